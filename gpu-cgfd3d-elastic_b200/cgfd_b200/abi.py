@@ -1,0 +1,307 @@
+"""ctypes mirror of include/cgfd_b200.h.
+
+`Problem` carries the inputs of drv_rk_curv_col_allstep (reference
+src/forward/drv_rk_curv_col.cu:28-50) as numpy arrays in the reference host layout
+[cmp][k][j][i] with 3 ghost points per side; `Simulation` owns the device state.
+"""
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+CGFD_MEDIUM_ELASTIC_ISO = 2
+CGFD_MEDIUM_ELASTIC_VTI = 3
+CGFD_MEDIUM_ELASTIC_ANISO = 4
+CGFD_PREC_FP32 = 0
+CGFD_PREC_BF16_COEF = 1
+CGFD_PREC_FP16_WAVE = 2
+# wavelet names of src_t.cu:873-903 -> ids
+WAVELETS = {"ricker": 0, "gaussian": 1, "ricker_deriv": 2, "gaussian_deriv": 3, "klauder": 4}
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+lib_path = os.path.join(os.path.dirname(_HERE), "_build", "libcgfd_b200.so")
+
+
+class CgfdError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"cgfd error {code}: {msg}")
+        self.code = code
+
+
+class PmlFace(C.Structure):
+    _fields_ = [("enable", C.c_int), ("num_layers", C.c_int), ("alpha_max", C.c_float),
+                ("beta_max", C.c_float), ("ref_vel", C.c_float)]
+
+
+class SourceDesc(C.Structure):
+    _fields_ = [("num", C.c_int), ("stf_given", C.c_int), ("stf_length", C.c_float),
+                ("stf_dt", C.c_float), ("stf_nt", C.c_int), ("cmp_type", C.c_int),
+                ("mechanism_type", C.c_int), ("loc_coord_type", C.c_int), ("loc_3dim", C.c_int),
+                ("loc", C.c_void_p), ("t_start", C.c_void_p), ("wavelet", C.c_void_p),
+                ("wavelet_coefs", C.c_void_p), ("cmp", C.c_void_p), ("cmp_values", C.c_void_p)]
+
+
+class StationDesc(C.Structure):
+    _fields_ = [("num", C.c_int), ("flag_coord", C.c_void_p), ("flag_depth", C.c_void_p),
+                ("loc", C.c_void_p)]
+
+
+class ProblemDesc(C.Structure):
+    _fields_ = [("ni", C.c_int), ("nj", C.c_int), ("nk", C.c_int), ("medium_type", C.c_int),
+                ("coord", C.c_void_p), ("metric", C.c_void_p), ("medium", C.c_void_p),
+                ("pml", (PmlFace * 2) * 3), ("free_top", C.c_int), ("dt", C.c_float),
+                ("t0", C.c_float), ("nt_total", C.c_int), ("src", SourceDesc),
+                ("sta", StationDesc), ("precision", C.c_int), ("device", C.c_int)]
+
+
+def medium_ncmp(medium_type):
+    return {CGFD_MEDIUM_ELASTIC_ISO: 3, CGFD_MEDIUM_ELASTIC_VTI: 6, CGFD_MEDIUM_ELASTIC_ANISO: 22}[medium_type]
+
+
+def ref_shape(ni, nj, nk):
+    """(nz, ny, nx) of one field in the reference layout."""
+    return (nk + 6, nj + 6, ni + 6)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+@dataclass
+class Sources:
+    """In-memory .src content (src_t.cu:205-611)."""
+    loc: np.ndarray                      # [n,3] float32, 0-based grid index
+    t_start: np.ndarray                  # [n]
+    wavelet: Optional[np.ndarray] = None  # [n] int32 ids
+    wavelet_coefs: Optional[np.ndarray] = None  # [n,10]
+    cmp: Optional[np.ndarray] = None     # [n,9] fx fy fz mxx myy mzz myz mxz mxy
+    cmp_values: Optional[np.ndarray] = None  # [n,nt,9]
+    stf_given: int = 0
+    stf_length: float = 0.0
+    stf_dt: float = 0.0
+    stf_nt: int = 0
+    cmp_type: int = 2
+    mechanism_type: int = 0
+    loc_coord_type: int = 0
+    loc_3dim: int = 0
+
+    @property
+    def num(self):
+        return int(self.loc.shape[0])
+
+
+@dataclass
+class Stations:
+    """In-memory station list (io_funcs.cu:52-80): 1-based x,y index; z per flag_depth."""
+    loc: np.ndarray                      # [n,3]
+    flag_depth: np.ndarray               # [n] int32
+    flag_coord: Optional[np.ndarray] = None
+    names: Optional[list] = None
+
+    @property
+    def num(self):
+        return int(self.loc.shape[0])
+
+
+@dataclass
+class Problem:
+    ni: int
+    nj: int
+    nk: int
+    medium_type: int
+    coord: Optional[np.ndarray]          # [3,nz,ny,nx] float32
+    metric: np.ndarray                   # [10,nz,ny,nx]
+    medium: np.ndarray                   # [ncmp,nz,ny,nx] (rho = density)
+    dt: float
+    nt_total: int
+    t0: float = 0.0
+    pml: list = field(default_factory=lambda: [[None, None], [None, None], [None, None]])
+    free_top: int = 1
+    src: Optional[Sources] = None
+    sta: Optional[Stations] = None
+    precision: int = CGFD_PREC_FP32
+    device: int = 0
+
+    def desc(self):
+        """Build the C description; the returned object keeps every array alive."""
+        keep = []
+
+        def arr(a, dt):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=dt)
+            keep.append(a)
+            return a
+
+        d = ProblemDesc()
+        d.ni, d.nj, d.nk = self.ni, self.nj, self.nk
+        d.medium_type = self.medium_type
+        d.coord = _ptr(arr(self.coord, np.float32))
+        d.metric = _ptr(arr(self.metric, np.float32))
+        d.medium = _ptr(arr(self.medium, np.float32))
+        for a in range(3):
+            for s in range(2):
+                f = self.pml[a][s]
+                if f:
+                    d.pml[a][s] = PmlFace(1, int(f["num_layers"]), float(f["alpha_max"]),
+                                          float(f["beta_max"]), float(f["ref_vel"]))
+        d.free_top = int(self.free_top)
+        d.dt, d.t0, d.nt_total = float(self.dt), float(self.t0), int(self.nt_total)
+        if self.src is not None and self.src.num > 0:
+            s = self.src
+            d.src.num = s.num
+            d.src.stf_given, d.src.stf_length = s.stf_given, s.stf_length
+            d.src.stf_dt, d.src.stf_nt = s.stf_dt, s.stf_nt
+            d.src.cmp_type, d.src.mechanism_type = s.cmp_type, s.mechanism_type
+            d.src.loc_coord_type, d.src.loc_3dim = s.loc_coord_type, s.loc_3dim
+            d.src.loc = _ptr(arr(s.loc, np.float32))
+            d.src.t_start = _ptr(arr(s.t_start, np.float32))
+            d.src.wavelet = _ptr(arr(s.wavelet, np.int32))
+            d.src.wavelet_coefs = _ptr(arr(s.wavelet_coefs, np.float32))
+            d.src.cmp = _ptr(arr(s.cmp, np.float32))
+            d.src.cmp_values = _ptr(arr(s.cmp_values, np.float32))
+        if self.sta is not None and self.sta.num > 0:
+            t = self.sta
+            d.sta.num = t.num
+            fc = t.flag_coord if t.flag_coord is not None else np.zeros(t.num, np.int32)
+            d.sta.flag_coord = _ptr(arr(fc, np.int32))
+            d.sta.flag_depth = _ptr(arr(t.flag_depth, np.int32))
+            d.sta.loc = _ptr(arr(t.loc, np.float32))
+        d.precision = int(self.precision)
+        d.device = int(self.device)
+        d._keep = keep
+        return d
+
+
+_lib = None
+
+
+def lib():
+    """Load libcgfd_b200.so from the package build folder; there is no fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(lib_path):
+        raise RuntimeError(f"{lib_path} is missing: build it with `make -C gpu-cgfd3d-elastic_b200` "
+                           "(or __graft_entry__.build())")
+    L = C.CDLL(lib_path)
+    P = C.c_void_p
+    sig = {
+        "cgfd_version": (C.c_int, []),
+        "cgfd_last_error": (C.c_char_p, []),
+        "cgfd_problem_create": (C.c_int, [C.POINTER(ProblemDesc), C.POINTER(P)]),
+        "cgfd_problem_destroy": (C.c_int, [P]),
+        "cgfd_run": (C.c_int, [P, C.c_int]),
+        "cgfd_enqueue_steps": (C.c_int, [P, C.c_int]),
+        "cgfd_synchronize": (C.c_int, [P]),
+        "cgfd_current_step": (C.c_int, [P]),
+        "cgfd_set_step": (C.c_int, [P, C.c_int]),
+        "cgfd_get_seismograms": (C.c_int, [P, P]),
+        "cgfd_num_stations": (C.c_int, [P]),
+        "cgfd_get_wavefield": (C.c_int, [P, P]),
+        "cgfd_set_wavefield": (C.c_int, [P, P]),
+        "cgfd_device_bytes": (C.c_size_t, [P]),
+        "cgfd_stream": (P, [P]),
+        "cgfd_set_graph_mode": (C.c_int, [P, C.c_int]),
+        "cgfd_set_zchunk": (C.c_int, [P, C.c_int]),
+        "cgfd_get_zchunk": (C.c_int, [P]),
+        "cgfd_fill_ghosts": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P]),
+        "cgfd_metric_calc": (C.c_int, [C.c_int, C.c_int, C.c_int, P, P]),
+        "cgfd_dt_estimate": (C.c_int, [C.POINTER(ProblemDesc), C.c_double, C.POINTER(C.c_double)]),
+        "cgfd_keep_three_digits": (C.c_double, [C.c_double]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def check(rc):
+    if rc != 0:
+        raise CgfdError(rc, lib().cgfd_last_error().decode())
+    return rc
+
+
+class Simulation:
+    """Device state of one forward simulation (cgfd_problem_create ... destroy)."""
+
+    def __init__(self, problem: Problem):
+        self.problem = problem
+        self._desc = problem.desc()
+        h = C.c_void_p()
+        check(lib().cgfd_problem_create(C.byref(self._desc), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().cgfd_problem_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, nsteps=-1):
+        check(lib().cgfd_run(self.h, int(nsteps)))
+
+    def enqueue(self, nsteps):
+        check(lib().cgfd_enqueue_steps(self.h, int(nsteps)))
+
+    def synchronize(self):
+        check(lib().cgfd_synchronize(self.h))
+
+    @property
+    def step(self):
+        return lib().cgfd_current_step(self.h)
+
+    def set_step(self, it):
+        check(lib().cgfd_set_step(self.h, int(it)))
+
+    @property
+    def num_stations(self):
+        return lib().cgfd_num_stations(self.h)
+
+    def seismograms(self):
+        n = self.num_stations
+        out = np.zeros((max(n, 0), 9, self.problem.nt_total), np.float32)
+        check(lib().cgfd_get_seismograms(self.h, out.ctypes.data))
+        return out
+
+    def wavefield(self):
+        p = self.problem
+        out = np.zeros((9,) + ref_shape(p.ni, p.nj, p.nk), np.float32)
+        check(lib().cgfd_get_wavefield(self.h, out.ctypes.data))
+        return out
+
+    def set_wavefield(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        check(lib().cgfd_set_wavefield(self.h, w.ctypes.data))
+
+    def device_bytes(self):
+        return int(lib().cgfd_device_bytes(self.h))
+
+    def set_graph_mode(self, on):
+        check(lib().cgfd_set_graph_mode(self.h, int(on)))
+
+    def set_zchunk(self, nzc):
+        check(lib().cgfd_set_zchunk(self.h, int(nzc)))
+
+    @property
+    def zchunk(self):
+        return lib().cgfd_get_zchunk(self.h)
+
+    @property
+    def stream(self):
+        return lib().cgfd_stream(self.h)

@@ -1,0 +1,488 @@
+// cgfd_api.cu -- host runtime and C ABI of the B200 CGFD3D time loop.
+//
+// A cgfd_problem holds everything drv_rk_curv_col_allstep() keeps on the device
+// (drv_rk_curv_col.cu:98-184) in a layout chosen for sm_100a:
+//   wavefield: 4 levels (w_pre/w_end pair that swaps every step + tmpA/tmpB ping-pong of
+//              the stage input) x 9 fields; no rhs level (the RHS lives in registers).
+//   fields:    [k][j][i] with 3 ghost planes in y/z and a 32-float ghost offset in x, so that
+//              every physical row starts on a 128-byte line.
+//   PML:       per enabled face, 3 levels (pre/end pair + tmp updated in place) x 9 fields.
+// One time step = station sampling, then per RK stage the bulk and surface-slab stage
+// kernels and the source kernel, then the step-counter advance. The 8 MacCormack pairs and
+// the 2 buffer parities give 8 distinct steps; each is captured once as a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "cgfd_b200.h"
+#include "cgfd_dev.cuh"
+#include "cgfd_launch.h"
+#include "cgfd_setup.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+void set_err(const std::string &m) { g_err = m; }
+
+#define CK(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess)                                                                       \
+      throw cgfd::Error(CGFD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+  } while (0)
+
+// 8 pairs of forward/backward flags (fd_t.cu:184-194), direction = (flag + stage) % 2
+const int kPairFlags[8][3] = {{0, 0, 0}, {1, 1, 0}, {1, 1, 1}, {0, 0, 1},
+                              {0, 1, 0}, {1, 0, 0}, {1, 0, 1}, {0, 1, 1}};
+const float kRkA[3] = {0.5f, 0.5f, 1.0f};                                          // fd_t.cu:35-37
+const float kRkB[4] = {1.0f / 6.0f, 1.0f / 3.0f, 1.0f / 3.0f, 1.0f / 6.0f};        // fd_t.cu:39-42
+
+template <typename T>
+T *dmalloc(size_t n, size_t &acc) {
+  void *p = nullptr;
+  if (n == 0) return nullptr;
+  cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    throw cgfd::Error(CGFD_ERR_NOMEM, "device allocation of " + std::to_string(n * sizeof(T)) + " bytes failed");
+  }
+  if (e != cudaSuccess) throw cgfd::Error(CGFD_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  acc += n * sizeof(T);
+  return (T *)p;
+}
+
+}  // namespace
+
+struct cgfd_problem {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int ni = 0, nj = 0, nk = 0, med = 0, ncoef = 0, nt_total = 0, free_top = 0;
+  float dt = 0.f;
+  long long sx = 0, sz = 0, sf = 0, off0 = 0;
+  size_t bytes = 0;
+  int nzc = 16;
+
+  float *wbuf[4] = {nullptr, nullptr, nullptr, nullptr};  // [0],[1]: pre/end by parity; [2],[3]: tmpA/tmpB
+  float *coef = nullptr, *jac = nullptr, *matx = nullptr, *maty = nullptr;
+
+  struct Face {
+    cgfd::PmlFaceHost h;
+    float *A = nullptr, *B = nullptr, *D = nullptr;
+    float *aux = nullptr;  // [3][9][n]
+    long long n = 0;
+  };
+  std::vector<Face> faces;
+
+  cgfd::SrcHost src;
+  int *d_it_begin = nullptr, *d_ext_num = nullptr;
+  long long *d_ext_idx = nullptr;
+  float *d_ext_wv = nullptr, *d_ext_wt = nullptr, *d_stf = nullptr;
+
+  cgfd::RecvHost rec;
+  long long *d_idx8 = nullptr;
+  float *d_w8 = nullptr, *d_seis = nullptr;
+
+  int *d_it = nullptr, *d_flag = nullptr;
+  int it = 0;
+
+  bool use_graph = true;
+  cudaGraphExec_t graph[8] = {};
+  bool graph_ok[8] = {};
+
+  long long didx(int i, int j, int k) const { return off0 + (long long)k * sz + (long long)j * sx + i; }
+
+  cgfd::StageP stage_params(int step, int stage) const {
+    cgfd::StageP p;
+    memset(&p, 0, sizeof(p));
+    p.ni = ni; p.nj = nj; p.nk = nk;
+    p.stage = stage;
+    int ipair = step % 8;
+    for (int a = 0; a < 3; a++) p.dir[a] = (kPairFlags[ipair][a] + stage) % 2;
+    p.sx = sx; p.sz = sz; p.sf = sf; p.off0 = off0;
+    float *pre = wbuf[step & 1], *end = wbuf[(step + 1) & 1];
+    float *tA = wbuf[2], *tB = wbuf[3];
+    const float *curs[4] = {pre, tA, tB, tA};
+    float *outs[4] = {tA, tB, tA, nullptr};
+    p.cur = curs[stage];
+    p.pre = pre;
+    p.tmp_out = outs[stage];
+    p.end = end;
+    p.ca = stage < 3 ? kRkA[stage] * dt : 0.f;
+    p.cb = kRkB[stage] * dt;
+    p.coef = coef; p.jac = jac; p.matx = matx; p.maty = maty;
+    p.free_top = free_top;
+    p.nbulk = free_top ? nk - cgfd::NSURF : nk;
+    p.nface = 0;
+    for (const Face &f : faces) {
+      cgfd::FaceP &o = p.face[p.nface++];
+      o.enable = 1;
+      o.axis = f.h.axis;
+      for (int b = 0; b < 3; b++) { o.lo[b] = f.h.lo[b]; o.hi[b] = f.h.hi[b]; }
+      o.nx = f.h.hi[0] - f.h.lo[0] + 1;
+      o.ny = f.h.hi[1] - f.h.lo[1] + 1;
+      o.n = f.n;
+      o.A = f.A; o.B = f.B; o.D = f.D;
+      float *apre = f.aux + (size_t)(step & 1) * 9 * f.n, *aend = f.aux + (size_t)((step + 1) & 1) * 9 * f.n;
+      float *atmp = f.aux + (size_t)2 * 9 * f.n;
+      o.aux_cur = stage == 0 ? apre : atmp;
+      o.aux_pre = apre;
+      o.aux_tmp = atmp;
+      o.aux_end = aend;
+    }
+    return p;
+  }
+
+  void enqueue_step(int step) {
+    cudaStream_t st = stream;
+    if (rec.n > 0) {
+      cgfd::RecvP r;
+      r.nsta = rec.n; r.nt_total = nt_total; r.idx8 = d_idx8; r.w8 = d_w8;
+      r.pre = wbuf[step & 1]; r.sf = sf; r.seis = d_seis; r.d_it = d_it; r.d_flag = d_flag;
+      cgfd::launch_recv(r, st);
+    }
+    for (int s = 0; s < 4; s++) {
+      cgfd::StageP p = stage_params(step, s);
+      cgfd::launch_stage(med, p, nzc, st);
+      if (src.nsrc > 0) {
+        cgfd::SrcP q;
+        q.nsrc = src.nsrc; q.max_ext = src.max_ext; q.max_nt = src.max_nt;
+        q.force = src.force; q.moment = src.moment; q.stage = s;
+        q.ca = p.ca; q.cb = p.cb;
+        q.it_begin = d_it_begin; q.ext_num = d_ext_num; q.ext_idx = d_ext_idx;
+        q.ext_wv = d_ext_wv; q.ext_wt = d_ext_wt; q.stf = d_stf;
+        q.tmp_out = p.tmp_out; q.end = p.end; q.sf = sf; q.d_it = d_it;
+        cgfd::launch_source(q, st);
+      }
+    }
+    cgfd::launch_advance(d_it, st);
+  }
+
+  void run_steps(int n) {
+    for (int s = 0; s < n; s++) {
+      int step = it;
+      int slot = step % 8;
+      if (use_graph) {
+        if (!graph_ok[slot]) {
+          cudaGraph_t g;
+          CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+          enqueue_step(step);
+          CK(cudaStreamEndCapture(stream, &g));
+          CK(cudaGraphInstantiate(&graph[slot], g, 0));
+          CK(cudaGraphDestroy(g));
+          graph_ok[slot] = true;
+        }
+        CK(cudaGraphLaunch(graph[slot], stream));
+      } else {
+        enqueue_step(step);
+        CK(cudaGetLastError());
+      }
+      it++;
+    }
+  }
+
+  void release() {
+    if (device >= 0) cudaSetDevice(device);
+    for (int s = 0; s < 8; s++)
+      if (graph_ok[s]) cudaGraphExecDestroy(graph[s]);
+    for (auto *p : wbuf) cudaFree(p);
+    cudaFree(coef); cudaFree(jac); cudaFree(matx); cudaFree(maty);
+    for (Face &f : faces) { cudaFree(f.A); cudaFree(f.B); cudaFree(f.D); cudaFree(f.aux); }
+    cudaFree(d_it_begin); cudaFree(d_ext_num); cudaFree(d_ext_idx); cudaFree(d_ext_wv); cudaFree(d_ext_wt);
+    cudaFree(d_stf); cudaFree(d_idx8); cudaFree(d_w8); cudaFree(d_seis); cudaFree(d_it); cudaFree(d_flag);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+template <typename Fn>
+int guarded(Fn fn) {
+  try {
+    fn();
+    return CGFD_OK;
+  } catch (cgfd::Error &e) {
+    set_err(e.what());
+    return e.code;
+  } catch (std::exception &e) {
+    set_err(e.what());
+    return CGFD_ERR_INVALID;
+  }
+}
+
+void upload_field(cgfd_problem *p, const float *host_ref, float *dst, float *stage_buf, int mode, int ghosts) {
+  size_t n = (size_t)(p->ni + 6) * (p->nj + 6) * (p->nk + 6);
+  CK(cudaMemcpyAsync(stage_buf, host_ref, n * sizeof(float), cudaMemcpyHostToDevice, p->stream));
+  cgfd::launch_repack_in(stage_buf, dst, p->ni, p->nj, p->nk, p->sx, p->sz, p->off0, mode, ghosts, p->stream);
+  CK(cudaGetLastError());
+}
+
+void build(cgfd_problem *p, const cgfd_problem_desc *d) {
+  cgfd::validate_desc(d);
+  if (d->precision != CGFD_PREC_FP32) throw cgfd::Error(CGFD_ERR_UNSUPPORTED, "only CGFD_PREC_FP32 in this build");
+  p->device = d->device;
+  CK(cudaSetDevice(p->device));
+  CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  p->ni = d->ni; p->nj = d->nj; p->nk = d->nk;
+  p->med = d->medium_type == CGFD_MEDIUM_ELASTIC_ISO ? cgfd::MED_ISO
+           : (d->medium_type == CGFD_MEDIUM_ELASTIC_VTI ? cgfd::MED_VTI : cgfd::MED_ANISO);
+  p->ncoef = p->med == cgfd::MED_ISO ? 12 : (p->med == cgfd::MED_VTI ? 15 : 31);
+  p->nt_total = d->nt_total;
+  p->dt = d->dt;
+  p->free_top = d->free_top ? 1 : 0;
+  if (p->free_top && p->nk < cgfd::NSURF + 4) throw cgfd::Error(CGFD_ERR_INVALID, "nk too small for the free surface");
+  // device layout
+  p->sx = ((cgfd::GX + p->ni + 3 + 31) / 32) * 32;
+  p->sz = p->sx * (p->nj + 6);
+  p->sf = ((p->sz * (p->nk + 6) + 63) / 64) * 64;
+  p->off0 = 3 * p->sz + 3 * p->sx + cgfd::GX;
+  // launch shape: enough z chunks to fill 148 SMs x 2 blocks a few times over
+  {
+    int nbulk = p->free_top ? p->nk - cgfd::NSURF : p->nk;
+    long long tiles = (long long)((p->ni + cgfd::TX - 1) / cgfd::TX) * ((p->nj + cgfd::TY - 1) / cgfd::TY);
+    long long want = 148 * 2 * 4;
+    int chunks = (int)std::max<long long>(1, std::min<long long>((want + tiles - 1) / tiles, std::max(1, nbulk / 12)));
+    p->nzc = (nbulk + chunks - 1) / chunks;
+    if (p->nzc < 1) p->nzc = 1;
+  }
+
+  size_t &B = p->bytes;
+  for (int l = 0; l < 4; l++) p->wbuf[l] = dmalloc<float>((size_t)9 * p->sf, B);
+  p->coef = dmalloc<float>((size_t)p->ncoef * p->sf, B);
+  p->jac = dmalloc<float>((size_t)p->sf, B);
+  for (int l = 0; l < 4; l++) CK(cudaMemsetAsync(p->wbuf[l], 0, sizeof(float) * 9 * p->sf, p->stream));
+  CK(cudaMemsetAsync(p->coef, 0, sizeof(float) * p->ncoef * p->sf, p->stream));
+  CK(cudaMemsetAsync(p->jac, 0, sizeof(float) * p->sf, p->stream));
+
+  // coefficients: metric (ghosts kept for the traction image), 1/rho, medium
+  cgfd::RefGrid g(p->ni, p->nj, p->nk);
+  float *stage_buf = dmalloc<float>(g.siz_icmp, B);
+  upload_field(p, d->metric, p->jac, stage_buf, 0, 1);
+  for (int c = 0; c < 9; c++) upload_field(p, d->metric + (size_t)(1 + c) * g.siz_icmp, p->coef + (size_t)c * p->sf, stage_buf, 0, 1);
+  upload_field(p, d->medium, p->coef + (size_t)cgfd::CF_SLW * p->sf, stage_buf, 1, 0);
+  int nmed = cgfd::medium_ncmp(d->medium_type) - 1;
+  for (int c = 0; c < nmed; c++)
+    upload_field(p, d->medium + (size_t)(1 + c) * g.siz_icmp, p->coef + (size_t)(cgfd::CF_MED + c) * p->sf, stage_buf, 0, 0);
+  CK(cudaStreamSynchronize(p->stream));
+  cudaFree(stage_buf);
+  B -= g.siz_icmp * sizeof(float);
+
+  // free surface
+  if (p->free_top) {
+    std::vector<float> mx, my;
+    cgfd::dvh2dvz(d, mx, my);
+    p->matx = dmalloc<float>(mx.size(), B);
+    p->maty = dmalloc<float>(my.size(), B);
+    CK(cudaMemcpy(p->matx, mx.data(), mx.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(p->maty, my.data(), my.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  // PML
+  cgfd::PmlFaceHost fh[3][2];
+  cgfd::pml_setup(d, fh);
+  for (int a = 0; a < 3; a++)
+    for (int s = 0; s < 2; s++) {
+      if (!fh[a][s].enable) continue;
+      cgfd_problem::Face f;
+      f.h = fh[a][s];
+      f.n = (long long)(f.h.hi[0] - f.h.lo[0] + 1) * (f.h.hi[1] - f.h.lo[1] + 1) * (f.h.hi[2] - f.h.lo[2] + 1);
+      size_t N1 = f.h.A.size();
+      f.A = dmalloc<float>(N1, B); f.B = dmalloc<float>(N1, B); f.D = dmalloc<float>(N1, B);
+      CK(cudaMemcpy(f.A, f.h.A.data(), N1 * sizeof(float), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(f.B, f.h.B.data(), N1 * sizeof(float), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(f.D, f.h.D.data(), N1 * sizeof(float), cudaMemcpyHostToDevice));
+      f.aux = dmalloc<float>((size_t)3 * 9 * f.n, B);
+      CK(cudaMemset(f.aux, 0, sizeof(float) * 3 * 9 * f.n));
+      p->faces.push_back(f);
+    }
+  // sources
+  cgfd::src_setup(d, p->src);
+  if (p->src.nsrc > 0) {
+    cgfd::SrcHost &s = p->src;
+    size_t ne = (size_t)s.nsrc * s.max_ext;
+    std::vector<long long> idx(ne, p->off0);
+    for (size_t e = 0; e < ne; e++) idx[e] = p->didx(s.ext_i[e], s.ext_j[e], s.ext_k[e]);
+    p->d_it_begin = dmalloc<int>(s.nsrc, B);
+    p->d_ext_num = dmalloc<int>(s.nsrc, B);
+    p->d_ext_idx = dmalloc<long long>(ne, B);
+    p->d_ext_wv = dmalloc<float>(ne, B);
+    p->d_ext_wt = dmalloc<float>(ne, B);
+    p->d_stf = dmalloc<float>(s.stf.size(), B);
+    CK(cudaMemcpy(p->d_it_begin, s.it_begin.data(), s.nsrc * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(p->d_ext_num, s.ext_num.data(), s.nsrc * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(p->d_ext_idx, idx.data(), ne * sizeof(long long), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(p->d_ext_wv, s.ext_wv.data(), ne * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(p->d_ext_wt, s.ext_wt.data(), ne * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(p->d_stf, s.stf.data(), s.stf.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  // stations
+  cgfd::recv_setup(d, p->rec);
+  if (p->rec.n > 0) {
+    std::vector<long long> idx8((size_t)p->rec.n * 8);
+    for (int r = 0; r < p->rec.n; r++)
+      for (int q = 0; q < 8; q++)
+        idx8[(size_t)r * 8 + q] = p->didx(p->rec.i[r] + (q & 1), p->rec.j[r] + ((q >> 1) & 1), p->rec.k[r] + ((q >> 2) & 1));
+    p->d_idx8 = dmalloc<long long>(idx8.size(), B);
+    p->d_w8 = dmalloc<float>(p->rec.w8.size(), B);
+    p->d_seis = dmalloc<float>((size_t)p->rec.n * 9 * p->nt_total, B);
+    CK(cudaMemcpy(p->d_idx8, idx8.data(), idx8.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(p->d_w8, p->rec.w8.data(), p->rec.w8.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemset(p->d_seis, 0, sizeof(float) * p->rec.n * 9 * p->nt_total));
+  }
+  p->d_it = dmalloc<int>(1, B);
+  p->d_flag = dmalloc<int>(1, B);
+  CK(cudaMemset(p->d_it, 0, sizeof(int)));
+  CK(cudaMemset(p->d_flag, 0, sizeof(int)));
+  CK(cudaDeviceSynchronize());
+}
+
+}  // namespace
+
+extern "C" {
+
+int cgfd_version(void) { return 100; }
+
+const char *cgfd_last_error(void) { return g_err.c_str(); }
+
+int cgfd_problem_create(const cgfd_problem_desc *desc, cgfd_problem **out) {
+  if (!out) { set_err("out is NULL"); return CGFD_ERR_INVALID; }
+  *out = nullptr;
+  cgfd_problem *p = new cgfd_problem;
+  int rc = guarded([&] { build(p, desc); });
+  if (rc != CGFD_OK) {
+    p->release();
+    delete p;
+    return rc;
+  }
+  *out = p;
+  return CGFD_OK;
+}
+
+int cgfd_problem_destroy(cgfd_problem *p) {
+  if (!p) return CGFD_OK;
+  p->release();
+  delete p;
+  return CGFD_OK;
+}
+
+int cgfd_enqueue_steps(cgfd_problem *p, int nsteps) {
+  if (!p) { set_err("problem is NULL"); return CGFD_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(p->device));
+    if (nsteps < 0) nsteps = p->nt_total - p->it;
+    p->run_steps(nsteps);
+  });
+}
+
+int cgfd_synchronize(cgfd_problem *p) {
+  if (!p) { set_err("problem is NULL"); return CGFD_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(p->device));
+    CK(cudaStreamSynchronize(p->stream));
+    int flag = 0;
+    CK(cudaMemcpy(&flag, p->d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) throw cgfd::Error(CGFD_ERR_NONFINITE, "non-finite value sampled at a station");
+  });
+}
+
+int cgfd_run(cgfd_problem *p, int nsteps) {
+  int rc = cgfd_enqueue_steps(p, nsteps);
+  if (rc) return rc;
+  return cgfd_synchronize(p);
+}
+
+int cgfd_current_step(const cgfd_problem *p) { return p ? p->it : -1; }
+
+int cgfd_set_step(cgfd_problem *p, int it) {
+  if (!p || it < 0) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(p->device));
+    CK(cudaStreamSynchronize(p->stream));
+    // the buffer roles follow the step parity: move w_pre / PML pre to the new parity
+    if ((it & 1) != (p->it & 1)) {
+      std::swap(p->wbuf[0], p->wbuf[1]);
+      for (auto &f : p->faces) {
+        size_t n = (size_t)9 * f.n;
+        CK(cudaMemcpyAsync(f.aux + n * 2, f.aux, n * sizeof(float), cudaMemcpyDeviceToDevice, p->stream));
+        CK(cudaMemcpyAsync(f.aux, f.aux + n, n * sizeof(float), cudaMemcpyDeviceToDevice, p->stream));
+        CK(cudaMemcpyAsync(f.aux + n, f.aux + n * 2, n * sizeof(float), cudaMemcpyDeviceToDevice, p->stream));
+      }
+      for (int s = 0; s < 8; s++)
+        if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }
+    }
+    p->it = it;
+    CK(cudaMemcpyAsync(p->d_it, &p->it, sizeof(int), cudaMemcpyHostToDevice, p->stream));
+    CK(cudaStreamSynchronize(p->stream));
+  });
+}
+
+int cgfd_num_stations(const cgfd_problem *p) { return p ? p->rec.n : -1; }
+
+int cgfd_get_seismograms(cgfd_problem *p, float *out) {
+  if (!p || !out) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(p->device));
+    CK(cudaStreamSynchronize(p->stream));
+    if (p->rec.n > 0)
+      CK(cudaMemcpy(out, p->d_seis, sizeof(float) * p->rec.n * 9 * p->nt_total, cudaMemcpyDeviceToHost));
+  });
+}
+
+int cgfd_get_wavefield(cgfd_problem *p, float *out) {
+  if (!p || !out) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(p->device));
+    cgfd::RefGrid g(p->ni, p->nj, p->nk);
+    size_t acc = 0;
+    float *tmp = dmalloc<float>(g.siz_icmp, acc);
+    const float *pre = p->wbuf[p->it & 1];
+    for (int c = 0; c < 9; c++) {
+      cgfd::launch_repack_out(pre + (size_t)c * p->sf, tmp, p->ni, p->nj, p->nk, p->sx, p->sz, p->off0, p->stream);
+      CK(cudaMemcpyAsync(out + (size_t)c * g.siz_icmp, tmp, g.siz_icmp * sizeof(float), cudaMemcpyDeviceToHost, p->stream));
+    }
+    CK(cudaStreamSynchronize(p->stream));
+    cudaFree(tmp);
+  });
+}
+
+int cgfd_set_wavefield(cgfd_problem *p, const float *in) {
+  if (!p || !in) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(p->device));
+    cgfd::RefGrid g(p->ni, p->nj, p->nk);
+    size_t acc = 0;
+    float *tmp = dmalloc<float>(g.siz_icmp, acc);
+    float *pre = p->wbuf[p->it & 1];
+    for (int c = 0; c < 9; c++) upload_field(p, in + (size_t)c * g.siz_icmp, pre + (size_t)c * p->sf, tmp, 0, 0);
+    CK(cudaStreamSynchronize(p->stream));
+    cudaFree(tmp);
+  });
+}
+
+size_t cgfd_device_bytes(const cgfd_problem *p) { return p ? p->bytes : 0; }
+
+void *cgfd_stream(cgfd_problem *p) { return p ? (void *)p->stream : nullptr; }
+
+/* Disable (0) or enable (1) CUDA-graph replay of the time steps. */
+int cgfd_set_graph_mode(cgfd_problem *p, int on) {
+  if (!p) return CGFD_ERR_INVALID;
+  p->use_graph = on != 0;
+  return CGFD_OK;
+}
+
+/* z planes per thread block of the bulk stage kernel (autotuner knob; graphs are rebuilt). */
+int cgfd_set_zchunk(cgfd_problem *p, int nzc) {
+  if (!p || nzc < 1) return CGFD_ERR_INVALID;
+  p->nzc = nzc;
+  for (int s = 0; s < 8; s++)
+    if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }
+  return CGFD_OK;
+}
+
+int cgfd_get_zchunk(const cgfd_problem *p) { return p ? p->nzc : -1; }
+
+}  // extern "C"

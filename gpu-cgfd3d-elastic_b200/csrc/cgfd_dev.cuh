@@ -1,0 +1,291 @@
+// cgfd_dev.cuh -- device-side building blocks of the fused RK-stage kernels.
+//
+// One RK stage of the reference (sv_curv_col_el_*_onestage + wav_update/wav_update_end,
+// drv_rk_curv_col.cu:263-491) becomes, per grid cell and in one pass over HBM:
+//   27 one-sided 5-point MacCormack derivatives (fd_t.cu:90-114 coefficients),
+//   momentum + Hooke (iso / VTI / 21-Cij), the CFS-PML correction and auxiliary-variable
+//   update of every face that contains the cell, and the RK4 combine of the wavefield and
+//   of the PML auxiliaries (tmp = pre + a*dt*rhs, end (+)= b*dt*rhs).
+// The RHS itself never reaches HBM.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cgfd {
+
+// Thread-block tile of the z-marching kernel (x fastest).
+constexpr int TX = 32;
+constexpr int TY = 8;
+// Ghost offset along x in the device layout: the physical row starts on a 128-byte line.
+constexpr int GX = 32;
+// Planes below the top processed by the surface-slab kernel when the free surface is on:
+// the traction image rewrites up to 4 layers, vlow 3 (sv_curv_col_el_iso_gpu.cu:212-249).
+constexpr int NSURF = 4;
+
+enum { MED_ISO = 0, MED_VTI = 1, MED_ANISO = 2 };
+
+// Coefficient fields in the device coefficient array, in this order:
+//   0..8  xi_x xi_y xi_z eta_x eta_y eta_z zeta_x zeta_y zeta_z
+//   9     1/rho
+//   10..  iso: lambda mu | vti: c11 c13 c33 c55 c66 | aniso: c11 c12 .. c66 (21, row-major upper)
+constexpr int CF_SLW = 9;
+constexpr int CF_MED = 10;
+template <int MED> struct MedInfo;
+template <> struct MedInfo<MED_ISO>   { static constexpr int NCOEF = 12; };
+template <> struct MedInfo<MED_VTI>   { static constexpr int NCOEF = 15; };
+template <> struct MedInfo<MED_ANISO> { static constexpr int NCOEF = 31; };
+
+// One CFS-PML face (bdry_t.cu:85-257): box [lo,hi] in physical indices, 1-D A/B/D along the
+// face normal, and the 9-component auxiliary variables (component stride n) at the levels
+// this stage reads and writes.
+struct FaceP {
+  int enable;
+  int axis;           // 0 x, 1 y, 2 z
+  int lo[3], hi[3];   // inclusive box, physical 0-based indices
+  int nx, ny;         // box extents along x, y
+  long long n;        // points in the box
+  const float *A, *B, *D;
+  const float *aux_cur;   // level read by the RHS (pre at stage 0, tmp otherwise)
+  const float *aux_pre;   // pre level (stages 1-2)
+  float *aux_tmp;         // tmp level written at stages 0-2 (== aux_cur at stages 1-2)
+  float *aux_end;         // end level
+};
+
+struct StageP {
+  int ni, nj, nk;
+  int stage;              // 0..3
+  int dir[3];             // 0 backward, 1 forward (fd_t.cu:184-235)
+  long long sx, sz, sf;   // row, plane and field strides of the device layout (floats)
+  long long off0;         // offset of physical point (0,0,0)
+  const float *cur;       // wavefield read by the stencils (9 fields)
+  const float *pre;       // w_pre (stages 1-2)
+  float *tmp_out;         // next stage input (stages 0-2)
+  float *end;             // accumulator (written at every stage)
+  float ca, cb;           // rk_a[stage]*dt, rk_b[stage]*dt
+  const float *coef;      // [ncoef][sf]
+  const float *jac;       // [sf]
+  const float *matx;      // free surface: [nj][ni][9] matVx2Vz (row-major 3x3)
+  const float *maty;      //                [nj][ni][9] matVy2Vz
+  int free_top;
+  int nbulk;              // planes [0, nbulk) belong to the bulk kernel
+  int nface;
+  FaceP face[6];
+};
+
+// ---------------------------------------------------------------------------------------
+// MacCormack DRP operator (fd_t.cu:90-93, 111-114): backward uses offsets -3..+1,
+// forward -1..+3. The 5 samples are passed in increasing position.
+// ---------------------------------------------------------------------------------------
+template <int DIR>
+__device__ __forceinline__ float drp5(float a0, float a1, float a2, float a3, float a4) {
+  if (DIR == 0)
+    return -0.041686285f * a0 + 0.333411808f * a1 - 1.250117713f * a2 + 0.666745142f * a3 + 0.291647047f * a4;
+  else
+    return -0.291647047f * a0 - 0.666745142f * a1 + 1.250117713f * a2 - 0.333411808f * a3 + 0.041686285f * a4;
+}
+__device__ __forceinline__ float drp5r(int dir, float a0, float a1, float a2, float a3, float a4) {
+  return dir ? drp5<1>(a0, a1, a2, a3, a4) : drp5<0>(a0, a1, a2, a3, a4);
+}
+// left extent of the operator
+__host__ __device__ constexpr int op_left(int dir) { return dir ? 1 : 3; }
+
+// Voigt index of (a,b): xx yy zz yz xz xy == wavefield components 3..8 minus 3.
+__host__ __device__ constexpr int voigt(int a, int b) {
+  return a == b ? a : (a + b == 3 ? 3 : (a + b == 2 ? 4 : 5));
+}
+
+// ---------------------------------------------------------------------------------------
+// Hooke's law from the velocity gradient G[vi][xj] = dV_vi/dx_j, per medium.
+// ---------------------------------------------------------------------------------------
+template <int MED>
+struct Medium;
+
+template <>
+struct Medium<MED_ISO> {
+  float lam, mu, lam2mu;
+  __device__ __forceinline__ void load(const float *coef, long long sf, long long idx) {
+    lam = __ldg(coef + (CF_MED + 0) * sf + idx);
+    mu = __ldg(coef + (CF_MED + 1) * sf + idx);
+    lam2mu = lam + 2.0f * mu;
+  }
+  __device__ __forceinline__ void hooke(const float G[3][3], float h[6]) const {
+    h[0] = lam2mu * G[0][0] + lam * (G[1][1] + G[2][2]);
+    h[1] = lam2mu * G[1][1] + lam * (G[0][0] + G[2][2]);
+    h[2] = lam2mu * G[2][2] + lam * (G[0][0] + G[1][1]);
+    h[3] = mu * (G[1][2] + G[2][1]);
+    h[4] = mu * (G[0][2] + G[2][0]);
+    h[5] = mu * (G[0][1] + G[1][0]);
+  }
+};
+
+template <>
+struct Medium<MED_VTI> {
+  float c11, c12, c13, c33, c55, c66;
+  __device__ __forceinline__ void load(const float *coef, long long sf, long long idx) {
+    c11 = __ldg(coef + (CF_MED + 0) * sf + idx);
+    c13 = __ldg(coef + (CF_MED + 1) * sf + idx);
+    c33 = __ldg(coef + (CF_MED + 2) * sf + idx);
+    c55 = __ldg(coef + (CF_MED + 3) * sf + idx);
+    c66 = __ldg(coef + (CF_MED + 4) * sf + idx);
+    c12 = c11 - 2.0f * c66;  // sv_curv_col_el_vti_gpu.cu:407
+  }
+  __device__ __forceinline__ void hooke(const float G[3][3], float h[6]) const {
+    h[0] = c11 * G[0][0] + c12 * G[1][1] + c13 * G[2][2];
+    h[1] = c12 * G[0][0] + c11 * G[1][1] + c13 * G[2][2];
+    h[2] = c13 * (G[0][0] + G[1][1]) + c33 * G[2][2];
+    h[3] = c55 * (G[1][2] + G[2][1]);
+    h[4] = c55 * (G[0][2] + G[2][0]);
+    h[5] = c66 * (G[0][1] + G[1][0]);
+  }
+};
+
+template <>
+struct Medium<MED_ANISO> {
+  float c[21];  // c11 c12 c13 c14 c15 c16 c22 .. c66 (upper triangle, row-major)
+  __device__ __forceinline__ void load(const float *coef, long long sf, long long idx) {
+#pragma unroll
+    for (int n = 0; n < 21; n++) c[n] = __ldg(coef + (CF_MED + n) * sf + idx);
+  }
+  __device__ __forceinline__ static constexpr int up(int a, int b) {
+    // index of C[a][b] (a<=b) in the packed upper triangle
+    return a * 6 - a * (a - 1) / 2 + (b - a);
+  }
+  __device__ __forceinline__ float C(int a, int b) const { return a <= b ? c[up(a, b)] : c[up(b, a)]; }
+  __device__ __forceinline__ void hooke(const float G[3][3], float h[6]) const {
+    float e[6] = {G[0][0], G[1][1], G[2][2], G[1][2] + G[2][1], G[0][2] + G[2][0], G[0][1] + G[1][0]};
+#pragma unroll
+    for (int I = 0; I < 6; I++) {
+      float s = C(I, 0) * e[0];
+#pragma unroll
+      for (int J = 1; J < 6; J++) s += C(I, J) * e[J];
+      h[I] = s;
+    }
+  }
+};
+
+// momentum of one axis: sum_j m[j] * dT_(vi,j) / d(axis)
+__device__ __forceinline__ void momentum_axis(const float m[3], const float dt[6], float mom[3]) {
+  mom[0] = m[0] * dt[0] + m[1] * dt[5] + m[2] * dt[4];
+  mom[1] = m[0] * dt[5] + m[1] * dt[1] + m[2] * dt[3];
+  mom[2] = m[0] * dt[4] + m[1] * dt[3] + m[2] * dt[2];
+}
+
+// ---------------------------------------------------------------------------------------
+// Per-cell state carried from the derivative phase to the store phase.
+// ---------------------------------------------------------------------------------------
+struct CellAcc {
+  float G[3][3];   // velocity gradient
+  float mom[3];    // divergence of stress (before 1/rho)
+  float hc[9];     // sum of PML corrections
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      mom[a] = 0.f;
+#pragma unroll
+      for (int b = 0; b < 3; b++) G[a][b] = 0.f;
+    }
+#pragma unroll
+    for (int c = 0; c < 9; c++) hc[c] = 0.f;
+  }
+  // accumulate the derivatives of one axis with metric row m
+  __device__ __forceinline__ void add_axis(const float m[3], const float dv[3], const float dt[6]) {
+#pragma unroll
+    for (int vi = 0; vi < 3; vi++)
+#pragma unroll
+      for (int xj = 0; xj < 3; xj++) G[vi][xj] += m[xj] * dv[vi];
+    float mm[3];
+    momentum_axis(m, dt, mm);
+    mom[0] += mm[0]; mom[1] += mm[1]; mom[2] += mm[2];
+  }
+};
+
+// RK combine of 9 values at one point (wav_update / wav_update_end, wav_t.cu:362-378).
+// cur_c: the stage input at the point (== pre at stage 0).
+__device__ __forceinline__ void rk_store(int stage, float ca, float cb, long long comp_stride, long long idx,
+                                         const float cur_c[9], const float h[9], const float *pre,
+                                         float *tmp_out, float *end) {
+  if (stage == 0) {
+#pragma unroll
+    for (int c = 0; c < 9; c++) {
+      tmp_out[c * comp_stride + idx] = cur_c[c] + ca * h[c];
+      end[c * comp_stride + idx] = cur_c[c] + cb * h[c];
+    }
+  } else if (stage < 3) {
+    float p[9], e[9];
+#pragma unroll
+    for (int c = 0; c < 9; c++) {
+      p[c] = __ldg(pre + c * comp_stride + idx);
+      e[c] = end[c * comp_stride + idx];
+    }
+#pragma unroll
+    for (int c = 0; c < 9; c++) {
+      tmp_out[c * comp_stride + idx] = p[c] + ca * h[c];
+      end[c * comp_stride + idx] = e[c] + cb * h[c];
+    }
+  } else {
+    float e[9];
+#pragma unroll
+    for (int c = 0; c < 9; c++) e[c] = end[c * comp_stride + idx];
+#pragma unroll
+    for (int c = 0; c < 9; c++) end[c * comp_stride + idx] = e[c] + cb * h[c];
+  }
+}
+
+// CFS-PML work of one face for one cell (sv_curv_col_el_iso_gpu.cu:680-1147):
+//   rhs_d = the 1-D terms of this axis; h += (B-1) rhs_d - B aux; aux' = D rhs_d - A aux,
+//   plus the free-surface-converted zeta terms on x/y faces at the top (surf != nullptr),
+//   followed by the RK combine of the auxiliary variables.
+template <int MED>
+__device__ __forceinline__ void pml_face(const StageP &p, const FaceP &f, int i, int j, int k,
+                                         const Medium<MED> &md, float slw, const float m[3],
+                                         const float dv[3], const float dt[6], const float *surf_mat,
+                                         const float zeta[3], float hc[9]) {
+  int ab = f.axis == 0 ? i - f.lo[0] : (f.axis == 1 ? j - f.lo[1] : k - f.lo[2]);
+  float cA = __ldg(f.A + ab), cB = __ldg(f.B + ab), cD = __ldg(f.D + ab);
+  float cB1 = cB - 1.0f;
+  long long ia = ((long long)(k - f.lo[2]) * f.ny + (j - f.lo[1])) * f.nx + (i - f.lo[0]);
+  float rhs[9];
+  momentum_axis(m, dt, rhs);
+  rhs[0] *= slw; rhs[1] *= slw; rhs[2] *= slw;
+  {
+    float Ga[3][3];
+#pragma unroll
+    for (int vi = 0; vi < 3; vi++)
+#pragma unroll
+      for (int xj = 0; xj < 3; xj++) Ga[vi][xj] = m[xj] * dv[vi];
+    md.hooke(Ga, rhs + 3);
+  }
+  float aux[9], arhs[9];
+#pragma unroll
+  for (int c = 0; c < 9; c++) {
+    aux[c] = f.aux_cur[c * f.n + ia];
+    hc[c] += cB1 * rhs[c] - cB * aux[c];
+    arhs[c] = cD * rhs[c] - cA * aux[c];
+  }
+  if (surf_mat) {
+    // dzV converted from this axis' derivative (sv_curv_col_el_iso_gpu.cu:855-915)
+    float dz[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) dz[r] = surf_mat[3 * r] * dv[0] + surf_mat[3 * r + 1] * dv[1] + surf_mat[3 * r + 2] * dv[2];
+    float Gs[3][3], hs[6];
+#pragma unroll
+    for (int vi = 0; vi < 3; vi++)
+#pragma unroll
+      for (int xj = 0; xj < 3; xj++) Gs[vi][xj] = zeta[xj] * dz[vi];
+    md.hooke(Gs, hs);
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+      hc[3 + c] += cB1 * hs[c];
+      arhs[3 + c] += cD * hs[c];
+    }
+  }
+  rk_store(p.stage, p.ca, p.cb, f.n, ia, aux, arhs, f.aux_pre, f.aux_tmp, f.aux_end);
+}
+
+// Index helpers for the device layout.
+__device__ __forceinline__ long long didx(const StageP &p, int i, int j, int k) {
+  return p.off0 + (long long)k * p.sz + (long long)j * p.sx + i;
+}
+
+}  // namespace cgfd

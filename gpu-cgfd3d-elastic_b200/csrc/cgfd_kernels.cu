@@ -1,0 +1,449 @@
+// cgfd_kernels.cu -- fused RK-stage kernels of the CGFD3D elastic path for sm_100a.
+//
+// k_stage_bulk: all planes below the surface slab. A thread block owns a TX x TY column
+//   tile and marches along z: the x-y tile of the current plane (with the 3/1-point halo of
+//   the one-sided MacCormack operators) sits in shared memory, double-buffered so that each
+//   plane needs one barrier, and the 5 planes the z operator needs sit in a per-thread
+//   register queue. Every wavefield value is read from HBM once per stage (halo re-reads hit
+//   L2), the RHS is combined into tmp/end in registers and never stored.
+//   Replaces sv_curv_col_el_{iso,vti,aniso}_rhs_inner_gpu, _rhs_cfspml_gpu and the
+//   wav_update/wav_update_end launches for these cells.
+// k_stage_surface: the top NSURF planes when the free surface is on: inner RHS, traction
+//   image (sv_curv_col_el_gpu.cu:19-221), vlow (sv_curv_col_el_iso_gpu.cu:462-603), PML
+//   with the free-surface terms, RK combine.
+// k_source: moment/force injection over the smoothed points (sv_curv_col_el_gpu.cu:227-301),
+//   applied to tmp/end with the stage's RK weights.
+// k_recv: trilinear station sampling of w_pre for all stations (io_funcs.cu:1624-1666).
+#include "cgfd_dev.cuh"
+#include "cgfd_launch.h"
+
+namespace cgfd {
+
+template <int MED, int DX, int DY, int DZ>
+__global__ void __launch_bounds__(TX *TY, 2) k_stage_bulk(const __grid_constant__ StageP p, int nzc) {
+  constexpr int LX = op_left(DX), LY = op_left(DY), LZ = op_left(DZ);
+  constexpr int SW = TX + 4, SH = TY + 4;
+  __shared__ float s[2][9][SH][SW];
+
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int bx = blockIdx.x, by = blockIdx.y;
+  const int i = bx * TX + tx, j = by * TY + ty;
+  const int kb = blockIdx.z * nzc;
+  const int ke = min(kb + nzc, p.nbulk);
+  if (kb >= ke) return;
+  const bool act = (i < p.ni) && (j < p.nj);
+  const long long sf = p.sf;
+  const float *__restrict__ cur = p.cur;
+
+  // halo slot of this thread (x halo: 4 columns per tile row, y halo: 4 rows per tile column)
+  int h_i = 0, h_j = 0, h_sx = 0, h_sy = 0;
+  bool h_on = false;
+  if (tid < 4 * TY) {
+    int row = tid >> 2, hh = tid & 3;
+    h_j = by * TY + row;
+    h_sy = row + LY;
+    if (hh < LX) { h_i = bx * TX - LX + hh; h_sx = hh; }
+    else { h_i = bx * TX + TX + (hh - LX); h_sx = TX + hh; }
+    h_on = true;
+  } else if (tid < 4 * TY + 4 * TX) {
+    int q = tid - 4 * TY;
+    int col = q % TX, hh = q / TX;
+    h_i = bx * TX + col;
+    h_sx = col + LX;
+    h_j = hh < LY ? by * TY - LY + hh : by * TY + TY + (hh - LY);
+    h_sy = LY + (h_j - by * TY);
+    h_on = true;
+  }
+  // points beyond the 3 ghost layers are never needed; they read as 0 without a load
+  const bool h_ld = h_on && h_i <= p.ni + 2 && h_j <= p.nj + 2;
+
+  // z register queue: q[f][n] holds plane k - LZ + n
+  float q[9][5];
+#pragma unroll
+  for (int f = 0; f < 9; f++)
+#pragma unroll
+    for (int n = 0; n < 5; n++) q[f][n] = 0.f;
+  if (act) {
+#pragma unroll
+    for (int n = 0; n < 4; n++) {
+      long long id = didx(p, i, j, kb - LZ + n);
+#pragma unroll
+      for (int f = 0; f < 9; f++) q[f][n] = __ldg(cur + f * sf + id);
+    }
+  }
+
+  for (int k = kb; k < ke; k++) {
+    const int buf = k & 1;
+    if (act) {
+      long long id = didx(p, i, j, k + 4 - LZ);
+#pragma unroll
+      for (int f = 0; f < 9; f++) q[f][4] = __ldg(cur + f * sf + id);
+    }
+#pragma unroll
+    for (int f = 0; f < 9; f++) s[buf][f][ty + LY][tx + LX] = q[f][LZ];
+    if (h_on) {
+      long long id = h_ld ? didx(p, h_i, h_j, k) : 0;
+#pragma unroll
+      for (int f = 0; f < 9; f++) s[buf][f][h_sy][h_sx] = h_ld ? __ldg(cur + f * sf + id) : 0.f;
+    }
+    __syncthreads();
+
+    if (act) {
+      const long long id = didx(p, i, j, k);
+      float m[3][3];
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) m[a][b] = __ldg(p.coef + (3 * a + b) * sf + id);
+      const float slw = __ldg(p.coef + CF_SLW * sf + id);
+      Medium<MED> md;
+      md.load(p.coef, sf, id);
+      CellAcc acc;
+      acc.zero();
+      // ---- x
+      {
+        float d[9];
+#pragma unroll
+        for (int f = 0; f < 9; f++) {
+          const float *r = &s[buf][f][ty + LY][tx];
+          d[f] = drp5<DX>(r[0], r[1], r[2], r[3], r[4]);
+        }
+        acc.add_axis(m[0], d, d + 3);
+        for (int fi = 0; fi < p.nface; fi++) {
+          const FaceP &fc = p.face[fi];
+          if (fc.axis == 0 && i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] && j <= fc.hi[1] && k >= fc.lo[2] &&
+              k <= fc.hi[2])
+            pml_face<MED>(p, fc, i, j, k, md, slw, m[0], d, d + 3, nullptr, nullptr, acc.hc);
+        }
+      }
+      // ---- y
+      {
+        float d[9];
+#pragma unroll
+        for (int f = 0; f < 9; f++)
+          d[f] = drp5<DY>(s[buf][f][ty][tx + LX], s[buf][f][ty + 1][tx + LX], s[buf][f][ty + 2][tx + LX],
+                          s[buf][f][ty + 3][tx + LX], s[buf][f][ty + 4][tx + LX]);
+        acc.add_axis(m[1], d, d + 3);
+        for (int fi = 0; fi < p.nface; fi++) {
+          const FaceP &fc = p.face[fi];
+          if (fc.axis == 1 && i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] && j <= fc.hi[1] && k >= fc.lo[2] &&
+              k <= fc.hi[2])
+            pml_face<MED>(p, fc, i, j, k, md, slw, m[1], d, d + 3, nullptr, nullptr, acc.hc);
+        }
+      }
+      // ---- z
+      {
+        float d[9];
+#pragma unroll
+        for (int f = 0; f < 9; f++) d[f] = drp5<DZ>(q[f][0], q[f][1], q[f][2], q[f][3], q[f][4]);
+        acc.add_axis(m[2], d, d + 3);
+        for (int fi = 0; fi < p.nface; fi++) {
+          const FaceP &fc = p.face[fi];
+          if (fc.axis == 2 && i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] && j <= fc.hi[1] && k >= fc.lo[2] &&
+              k <= fc.hi[2])
+            pml_face<MED>(p, fc, i, j, k, md, slw, m[2], d, d + 3, nullptr, nullptr, acc.hc);
+        }
+      }
+      float h[9];
+      h[0] = slw * acc.mom[0] + acc.hc[0];
+      h[1] = slw * acc.mom[1] + acc.hc[1];
+      h[2] = slw * acc.mom[2] + acc.hc[2];
+      md.hooke(acc.G, h + 3);
+#pragma unroll
+      for (int c = 3; c < 9; c++) h[c] += acc.hc[c];
+      float cc[9];
+#pragma unroll
+      for (int f = 0; f < 9; f++) cc[f] = q[f][LZ];
+      rk_store(p.stage, p.ca, p.cb, sf, id, cc, h, p.pre, p.tmp_out, p.end);
+    }
+#pragma unroll
+    for (int f = 0; f < 9; f++)
+#pragma unroll
+      for (int n = 0; n < 4; n++) q[f][n] = q[f][n + 1];
+  }
+}
+
+// -----------------------------------------------------------------------------------------
+// surface slab
+// -----------------------------------------------------------------------------------------
+__device__ __forceinline__ float ld5(int dir, const float *v, long long id, long long off, float (&o)[5]) {
+  int L = op_left(dir);
+#pragma unroll
+  for (int n = 0; n < 5; n++) o[n] = __ldg(v + id + (n - L) * off);
+  return 0.f;
+}
+
+template <int MED>
+__global__ void __launch_bounds__(128) k_stage_surface(const __grid_constant__ StageP p) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= p.ni || j >= p.nj) return;
+  const long long sf = p.sf;
+  const float *__restrict__ cur = p.cur;
+  const long long offs[3] = {1, p.sx, p.sz};
+  const int nk2 = p.nk - 1;
+
+  for (int k = p.nbulk; k < p.nk; k++) {
+    const long long id = didx(p, i, j, k);
+    float m[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int b = 0; b < 3; b++) m[a][b] = __ldg(p.coef + (3 * a + b) * sf + id);
+    const float slw = __ldg(p.coef + CF_SLW * sf + id);
+    Medium<MED> md;
+    md.load(p.coef, sf, id);
+
+    // normal derivatives of all 9 fields along the 3 axes
+    float dv[3][3], dtt[3][6];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+#pragma unroll
+      for (int f = 0; f < 9; f++) {
+        float v[5];
+        ld5(p.dir[a], cur + f * sf, id, offs[a], v);
+        float d = drp5r(p.dir[a], v[0], v[1], v[2], v[3], v[4]);
+        if (f < 3) dv[a][f] = d; else dtt[a][f - 3] = d;
+      }
+    }
+    float hc[9];
+#pragma unroll
+    for (int c = 0; c < 9; c++) hc[c] = 0.f;
+
+    // momentum: normal form, or the traction image near the free surface
+    float h[9];
+    {
+      float mom[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        float mm[3];
+        momentum_axis(m[a], dtt[a], mm);
+        mom[0] += mm[0]; mom[1] += mm[1]; mom[2] += mm[2];
+      }
+      h[0] = slw * mom[0]; h[1] = slw * mom[1]; h[2] = slw * mom[2];
+    }
+    const int dzr = p.dir[2];
+    if (p.free_top) {
+      const int idx_last = dzr ? 3 : 1, idx_first = dzr ? -1 : -3;
+      if (k >= nk2 - idx_last) {
+        // sv_curv_col_el_gpu.cu:53-217
+        const int n_free = nk2 - k - idx_first;
+        const float jc = __ldg(p.jac + id);
+        const float slwjac = slw / jc;
+        const int LXo = op_left(p.dir[0]), LYo = op_left(p.dir[1]), LZo = op_left(dzr);
+        // rows of the stress tensor: components (Txx,Txy,Txz), (Txy,Tyy,Tyz), (Txz,Tyz,Tzz)
+        const int tr[3][3] = {{3, 8, 7}, {8, 4, 6}, {7, 6, 5}};
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          const float *T1 = cur + tr[c][0] * sf, *T2 = cur + tr[c][1] * sf, *T3 = cur + tr[c][2] * sf;
+          float vx[5], vy[5], vz[5];
+#pragma unroll
+          for (int n = 0; n < 5; n++) {
+            long long q = id + (n - LXo);
+            vx[n] = __ldg(p.jac + q) * (__ldg(p.coef + 0 * sf + q) * __ldg(T1 + q) + __ldg(p.coef + 1 * sf + q) * __ldg(T2 + q) +
+                                        __ldg(p.coef + 2 * sf + q) * __ldg(T3 + q));
+            q = id + (long long)(n - LYo) * p.sx;
+            vy[n] = __ldg(p.jac + q) * (__ldg(p.coef + 3 * sf + q) * __ldg(T1 + q) + __ldg(p.coef + 4 * sf + q) * __ldg(T2 + q) +
+                                        __ldg(p.coef + 5 * sf + q) * __ldg(T3 + q));
+            int off;
+            float sgn;
+            if (n < n_free) { off = n - LZo; sgn = 1.f; }
+            else if (n == n_free) { off = 0; sgn = 0.f; }
+            else { off = (n - LZo) - 2 * (n - n_free); sgn = -1.f; }
+            q = id + (long long)off * p.sz;
+            float fz = __ldg(p.jac + q) * (__ldg(p.coef + 6 * sf + q) * __ldg(T1 + q) + __ldg(p.coef + 7 * sf + q) * __ldg(T2 + q) +
+                                           __ldg(p.coef + 8 * sf + q) * __ldg(T3 + q));
+            vz[n] = sgn * fz;
+          }
+          float DxTx = drp5r(p.dir[0], vx[0], vx[1], vx[2], vx[3], vx[4]);
+          float DyTy = drp5r(p.dir[1], vy[0], vy[1], vy[2], vy[3], vy[4]);
+          float DzTz = drp5r(dzr, vz[0], vz[1], vz[2], vz[3], vz[4]);
+          h[c] = (DxTx + DyTy + DzTz) * slwjac;
+        }
+      }
+    }
+    // Hooke: normal, or vlow with low-order / converted dzV in the top 3 layers
+    {
+      float dz[3] = {dv[2][0], dv[2][1], dv[2][2]};
+      if (p.free_top && k >= nk2 - 2) {
+        const int nl = nk2 - k;
+        if (nl == 0) {
+          const long long ij = ((long long)j * p.ni + i) * 9;
+#pragma unroll
+          for (int r = 0; r < 3; r++)
+            dz[r] = __ldg(p.matx + ij + 3 * r) * dv[0][0] + __ldg(p.matx + ij + 3 * r + 1) * dv[0][1] +
+                    __ldg(p.matx + ij + 3 * r + 2) * dv[0][2] + __ldg(p.maty + ij + 3 * r) * dv[1][0] +
+                    __ldg(p.maty + ij + 3 * r + 1) * dv[1][1] + __ldg(p.maty + ij + 3 * r + 2) * dv[1][2];
+        } else {
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            const float *v = cur + c * sf;
+            if (nl == 1) {  // 2nd order (fd_t.cu:82-85, 103-106)
+              dz[c] = dzr ? (-__ldg(v + id) + __ldg(v + id + p.sz)) : (-__ldg(v + id - p.sz) + __ldg(v + id));
+            } else {        // 4th order (fd_t.cu:86-89, 107-110)
+              dz[c] = dzr ? (-7.0f / 6.0f * __ldg(v + id) + 8.0f / 6.0f * __ldg(v + id + p.sz) -
+                             1.0f / 6.0f * __ldg(v + id + 2 * p.sz))
+                          : (1.0f / 6.0f * __ldg(v + id - 2 * p.sz) - 8.0f / 6.0f * __ldg(v + id - p.sz) +
+                             7.0f / 6.0f * __ldg(v + id));
+            }
+          }
+        }
+      }
+      float G[3][3];
+#pragma unroll
+      for (int vi = 0; vi < 3; vi++)
+#pragma unroll
+        for (int xj = 0; xj < 3; xj++) G[vi][xj] = m[0][xj] * dv[0][vi] + m[1][xj] * dv[1][vi] + m[2][xj] * dz[vi];
+      md.hooke(G, h + 3);
+    }
+    // CFS-PML faces, with the free-surface terms on x/y faces at the top layer
+    for (int fi = 0; fi < p.nface; fi++) {
+      const FaceP &fc = p.face[fi];
+      if (!(i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] && j <= fc.hi[1] && k >= fc.lo[2] && k <= fc.hi[2])) continue;
+      const int a = fc.axis;
+      const float *smat = nullptr;
+      if (p.free_top && a < 2 && k == nk2) smat = (a == 0 ? p.matx : p.maty) + ((long long)j * p.ni + i) * 9;
+      pml_face<MED>(p, fc, i, j, k, md, slw, m[a], dv[a], dtt[a], smat, m[2], hc);
+    }
+#pragma unroll
+    for (int c = 0; c < 9; c++) h[c] += hc[c];
+    float cc[9];
+#pragma unroll
+    for (int f = 0; f < 9; f++) cc[f] = __ldg(cur + f * sf + id);
+    rk_store(p.stage, p.ca, p.cb, sf, id, cc, h, p.pre, p.tmp_out, p.end);
+  }
+}
+
+// -----------------------------------------------------------------------------------------
+// sources, stations, step counter
+// -----------------------------------------------------------------------------------------
+__global__ void k_source(const __grid_constant__ SrcP s) {
+  const int is = blockIdx.y;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (is >= s.nsrc || e >= s.ext_num[is]) return;
+  const int it = *s.d_it;
+  const int ib = s.it_begin[is];
+  if (it < ib || it > ib + s.max_nt - 1) return;
+  const float *v = s.stf + (((long long)is * s.max_nt + (it - ib)) * 4 + s.stage) * 9;
+  const long long id = s.ext_idx[(long long)is * s.max_ext + e];
+  const float wv = s.ext_wv[(long long)is * s.max_ext + e];
+  const float wt = s.ext_wt[(long long)is * s.max_ext + e];
+  for (int c = 0; c < 9; c++) {
+    float h;
+    if (c < 3) { if (!s.force) continue; h = v[c] * wv; }
+    else { if (!s.moment) continue; h = -v[c] * wt; }
+    if (s.stage < 3) atomicAdd(s.tmp_out + c * s.sf + id, s.ca * h);
+    atomicAdd(s.end + c * s.sf + id, s.cb * h);
+  }
+}
+
+__global__ void k_recv(const __grid_constant__ RecvP r) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= r.nsta * 9) return;
+  const int it = *r.d_it;
+  if (it < 0 || it >= r.nt_total) return;
+  const int sidx = t / 9, c = t % 9;
+  float v = 0.f;
+#pragma unroll
+  for (int qn = 0; qn < 8; qn++) {
+    float w = r.w8[sidx * 8 + qn];
+    if (w != 0.f) v += w * __ldg(r.pre + c * r.sf + r.idx8[sidx * 8 + qn]);
+  }
+  if (!isfinite(v)) atomicOr(r.d_flag, 1);
+  r.seis[((long long)sidx * 9 + c) * r.nt_total + it] = v;
+}
+
+__global__ void k_advance(int *d_it) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *d_it += 1;
+}
+
+// Repack one field from the reference host layout (3 ghosts, nx = ni+6) into the device
+// layout. mode 1 converts density to 1/rho (md_rho_to_slow, md_t.cu:622-637).
+__global__ void k_repack_in(const float *__restrict__ src, float *__restrict__ dst, int ni, int nj, int nk,
+                            long long sx, long long sz, long long off0, int mode, int ghosts) {
+  const long long nxr = ni + 6, nyr = nj + 6;
+  const long long total = nxr * nyr * (nk + 6);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int ir = (int)(t % nxr), jr = (int)((t / nxr) % nyr), kr = (int)(t / (nxr * nyr));
+    int i = ir - 3, j = jr - 3, k = kr - 3;
+    bool inner = i >= 0 && i < ni && j >= 0 && j < nj && k >= 0 && k < nk;
+    if (!ghosts && !inner) continue;
+    float v = src[t];
+    if (mode == 1) v = v > 1e-10f ? 1.0f / v : 0.0f;
+    dst[off0 + (long long)k * sz + (long long)j * sx + i] = v;
+  }
+}
+
+__global__ void k_repack_out(const float *__restrict__ src, float *__restrict__ dst, int ni, int nj, int nk,
+                             long long sx, long long sz, long long off0) {
+  const long long nxr = ni + 6, nyr = nj + 6;
+  const long long total = nxr * nyr * (nk + 6);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int ir = (int)(t % nxr), jr = (int)((t / nxr) % nyr), kr = (int)(t / (nxr * nyr));
+    int i = ir - 3, j = jr - 3, k = kr - 3;
+    bool inner = i >= 0 && i < ni && j >= 0 && j < nj && k >= 0 && k < nk;
+    dst[t] = inner ? src[off0 + (long long)k * sz + (long long)j * sx + i] : 0.0f;
+  }
+}
+
+// -----------------------------------------------------------------------------------------
+// launch tables
+// -----------------------------------------------------------------------------------------
+typedef void (*BulkFn)(StageP, int);
+
+template <int MED>
+static void launch_bulk_med(const StageP &p, int nzc, dim3 grid, cudaStream_t st) {
+  const int code = p.dir[0] | (p.dir[1] << 1) | (p.dir[2] << 2);
+  dim3 block(TX, TY);
+  switch (code) {
+#define CASE(c)                                                                                   \
+  case c:                                                                                         \
+    k_stage_bulk<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1><<<grid, block, 0, st>>>(p, nzc); \
+    break;
+    CASE(0) CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7)
+#undef CASE
+  }
+}
+
+void launch_stage(int med, const StageP &p, int nzc, cudaStream_t st) {
+  if (p.nbulk > 0) {
+    dim3 grid((p.ni + TX - 1) / TX, (p.nj + TY - 1) / TY, (p.nbulk + nzc - 1) / nzc);
+    if (med == MED_ISO) launch_bulk_med<MED_ISO>(p, nzc, grid, st);
+    else if (med == MED_VTI) launch_bulk_med<MED_VTI>(p, nzc, grid, st);
+    else launch_bulk_med<MED_ANISO>(p, nzc, grid, st);
+  }
+  if (p.nbulk < p.nk) {
+    dim3 block(32, 4);
+    dim3 grid((p.ni + 31) / 32, (p.nj + 3) / 4);
+    if (med == MED_ISO) k_stage_surface<MED_ISO><<<grid, block, 0, st>>>(p);
+    else if (med == MED_VTI) k_stage_surface<MED_VTI><<<grid, block, 0, st>>>(p);
+    else k_stage_surface<MED_ANISO><<<grid, block, 0, st>>>(p);
+  }
+}
+
+void launch_source(const SrcP &s, cudaStream_t st) {
+  if (s.nsrc <= 0) return;
+  dim3 block(128);
+  dim3 grid((s.max_ext + 127) / 128, s.nsrc);
+  k_source<<<grid, block, 0, st>>>(s);
+}
+
+void launch_recv(const RecvP &r, cudaStream_t st) {
+  if (r.nsta <= 0) return;
+  int n = r.nsta * 9;
+  k_recv<<<(n + 127) / 128, 128, 0, st>>>(r);
+}
+
+void launch_advance(int *d_it, cudaStream_t st) { k_advance<<<1, 32, 0, st>>>(d_it); }
+
+void launch_repack_in(const float *src, float *dst, int ni, int nj, int nk, long long sx, long long sz, long long off0,
+                      int mode, int ghosts, cudaStream_t st) {
+  k_repack_in<<<1184, 256, 0, st>>>(src, dst, ni, nj, nk, sx, sz, off0, mode, ghosts);
+}
+
+void launch_repack_out(const float *src, float *dst, int ni, int nj, int nk, long long sx, long long sz, long long off0,
+                       cudaStream_t st) {
+  k_repack_out<<<1184, 256, 0, st>>>(src, dst, ni, nj, nk, sx, sz, off0);
+}
+
+}  // namespace cgfd

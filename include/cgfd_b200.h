@@ -1,0 +1,234 @@
+/*
+ * cgfd_b200.h -- C ABI of the B200-native CGFD3D elastic time-stepping path.
+ *
+ * The library (libcgfd_b200.so) replaces the time loop of hpc-lee/gpu-CGFD3D-elastic:
+ *   drv_rk_curv_col_allstep()          src/forward/drv_rk_curv_col.cu:28-567
+ *   sv_curv_col_el_{iso,vti,aniso}_onestage()  sv_curv_col_el_*_gpu.cu (RHS of one RK stage)
+ *   wav_update / wav_update_end         src/forward/wav_t.cu:362-378 (RK combine)
+ *   io_recv_keep                        src/forward/io_funcs.cu:1624-1666 (station sampling)
+ * together with the setup steps whose results that loop consumes (CFS-PML coefficients,
+ * free-surface velocity-gradient conversion matrices, source smoothing and source time
+ * functions, station location).
+ *
+ * Conventions shared with the reference:
+ *  - Host arrays use the reference layout var[cmp][k][j][i] with i fastest and CGFD_NGHOST
+ *    ghost points on every side: nx = ni+6, ny = nj+6, nz = nk+6 (gd_t.cu:1888-2043).
+ *  - Wavefield components are ordered Vx,Vy,Vz,Txx,Tyy,Tzz,Tyz,Txz,Txy (wav_t.cu:100-143).
+ *  - Metric components are ordered jac,xi_x,xi_y,xi_z,eta_x,eta_y,eta_z,zeta_x,zeta_y,zeta_z
+ *    (gd_t.cu:140-200, gd_curv_metric_init).
+ *  - Medium components are ordered as the media_*.nc variables (md_t.cu:16-268):
+ *      elastic_iso  : rho, lambda, mu
+ *      elastic_vti  : rho, c11, c13, c33, c55, c66
+ *      elastic_aniso: rho, c11,c12,c13,c14,c15,c16, c22,c23,c24,c25,c26, c33,c34,c35,c36,
+ *                     c44,c45,c46, c55,c56, c66
+ *    rho is the density; the library converts it to 1/rho like md_rho_to_slow (md_t.cu:622-637).
+ *
+ * Error convention: every entry point returns 0 on success and a negative CGFD_ERR_* code
+ * on failure; cgfd_last_error() then returns a message for the calling thread. Nothing in
+ * the library calls exit() or abort() (the reference aborts via MPI_Abort / exit).
+ */
+#ifndef CGFD_B200_H
+#define CGFD_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CGFD_NGHOST 3
+#define CGFD_NCMP   9
+
+/* medium ids: src/forward/constants.h:20-24 */
+#define CGFD_MEDIUM_ELASTIC_ISO   2
+#define CGFD_MEDIUM_ELASTIC_VTI   3
+#define CGFD_MEDIUM_ELASTIC_ANISO 4
+
+/* wavelet names accepted in .src files: src_t.cu:873-903 (src_cal_wavelet) */
+#define CGFD_WAVELET_RICKER         0
+#define CGFD_WAVELET_GAUSSIAN       1
+#define CGFD_WAVELET_RICKER_DERIV   2
+#define CGFD_WAVELET_GAUSSIAN_DERIV 3
+#define CGFD_WAVELET_KLAUDER        4
+
+/* storage precision of the device state (computation is always FP32) */
+#define CGFD_PREC_FP32       0  /* everything FP32 (the reference's arithmetic)            */
+#define CGFD_PREC_BF16_COEF  1  /* metrics/Jacobian/medium as scaled BF16, wavefield FP32   */
+#define CGFD_PREC_FP16_WAVE  2  /* scaled BF16 coefficients + FP16 wavefield with FP32 sum  */
+
+/* status codes */
+#define CGFD_OK               0
+#define CGFD_ERR_INVALID     -1   /* malformed description or argument                     */
+#define CGFD_ERR_CUDA        -2   /* CUDA runtime error                                     */
+#define CGFD_ERR_NOMEM       -3   /* device memory budget exceeded                          */
+#define CGFD_ERR_NONFINITE   -4   /* NaN/Inf detected in the wavefield                      */
+#define CGFD_ERR_UNSUPPORTED -5   /* option recognised but not implemented                  */
+#define CGFD_ERR_IO          -6   /* file could not be read or written                      */
+#define CGFD_ERR_BUSY        -7   /* serving queue full / request not finished              */
+
+/* One CFS-PML face (par_t.cu:230-371 "cfspml" block; bdry_t.cu:85-257 bdry_pml_set). */
+typedef struct cgfd_pml_face {
+  int   enable;       /* 1: CFS-PML on this face                                           */
+  int   num_layers;   /* N; the face box spans N+1 grid points (bdry_t.cu:138-155)          */
+  float alpha_max;
+  float beta_max;
+  float ref_vel;
+} cgfd_pml_face;
+
+/*
+ * Sources, as read from a .src file (src_t.cu:143-790, src_read_locate_file).
+ * Only grid-index locations (loc_coord_type 0) are accepted.
+ */
+typedef struct cgfd_source_desc {
+  int   num;              /* in_num_source                                                 */
+  int   stf_given;        /* 0: wavelet by name, 1: sampled values                         */
+  float stf_length;       /* stf_given 0: length of the source time function (s)           */
+  float stf_dt;           /* stf_given 1: sample interval                                  */
+  int   stf_nt;           /* stf_given 1: number of samples                                */
+  int   cmp_type;         /* 1 force, 2 moment, 3 force+moment (quirk kept: 3 = force only) */
+  int   mechanism_type;   /* 0 moment tensor, 1 strike/dip/rake + mu,D,A                   */
+  int   loc_coord_type;   /* 0 grid index (required)                                       */
+  int   loc_3dim;         /* 0: z is a grid index, 1: z counts down from the free surface  */
+  const float *loc;       /* [num][3] x,y,z (0-based index)                                */
+  const float *t_start;   /* [num] wavelet_tstart                                          */
+  const int   *wavelet;   /* [num] CGFD_WAVELET_* (stf_given 0)                             */
+  const float *wavelet_coefs; /* [num][10]                                                 */
+  const float *cmp;       /* stf_given 0: [num][9] = fx,fy,fz,mxx,myy,mzz,myz,mxz,mxy       */
+  const float *cmp_values;/* stf_given 1: [num][stf_nt][9], same order                      */
+} cgfd_source_desc;
+
+/* Stations, as read from a station list (io_funcs.cu:24-299, io_recv_read_locate). */
+typedef struct cgfd_station_desc {
+  int          num;
+  const int   *flag_coord; /* [num] 0: grid index (required)                               */
+  const int   *flag_depth; /* [num] 1: z counts down from the free surface                 */
+  const float *loc;        /* [num][3] x,y 1-based index, z per flag_depth                 */
+} cgfd_station_desc;
+
+/*
+ * Everything drv_rk_curv_col_allstep() consumes, in the reference's host layout.
+ */
+typedef struct cgfd_problem_desc {
+  int ni, nj, nk;           /* physical points incl. PML layers (ghosts excluded)          */
+  int medium_type;          /* CGFD_MEDIUM_ELASTIC_*                                        */
+  const float *coord;       /* [3][nz][ny][nx] x,y,z with ghosts filled; used for the PML
+                               length/spacing average (bdry_t.cu:334-451). May be NULL when
+                               no PML face is enabled.                                       */
+  const float *metric;      /* [10][nz][ny][nx]                                             */
+  const float *medium;      /* [ncmp][nz][ny][nx]                                           */
+  cgfd_pml_face pml[3][2];  /* [x,y,z][left/bottom, right/top]                              */
+  int   free_top;           /* 1: traction-image free surface at the top (z2)              */
+  float dt;
+  float t0;
+  int   nt_total;           /* number_of_time_steps + 1 (main_curv_col_el_3d.cu:589)        */
+  cgfd_source_desc  src;
+  cgfd_station_desc sta;
+  int   precision;          /* CGFD_PREC_*                                                  */
+  int   device;             /* CUDA device ordinal                                          */
+} cgfd_problem_desc;
+
+typedef struct cgfd_problem cgfd_problem;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int cgfd_version(void);
+
+/* Message for the last failed call on this thread ("" if none). */
+const char *cgfd_last_error(void);
+
+/*
+ * Build device-resident state for one forward simulation: the setup work that precedes
+ * drv_rk_curv_col_allstep() (bdry_pml_set, the dvh2dvz matrices, src_read_locate_file's
+ * smoothing and STF tables, io_recv_read_locate) plus the device mirrors of alloc.cu.
+ * Replaces: the init_*_device calls at drv_rk_curv_col.cu:109-117.
+ */
+int cgfd_problem_create(const cgfd_problem_desc *desc, cgfd_problem **out);
+
+/*
+ * Advance nsteps time steps (4 RK stages each), sampling the stations at the start of
+ * every step like io_recv_keep. nsteps < 0 runs to nt_total.
+ * Replaces: the time loop drv_rk_curv_col.cu:193-541.
+ */
+int cgfd_run(cgfd_problem *p, int nsteps);
+
+/* Index of the next time step to run (0 after create). */
+int cgfd_current_step(const cgfd_problem *p);
+
+/* Set the step counter (selects the MacCormack pair it%8 and the source time). */
+int cgfd_set_step(cgfd_problem *p, int it);
+
+/*
+ * Seismograms, [nsta][9][nt_total] in component order Vx..Txy; entries for steps not yet
+ * run are 0. Replaces: iorecv->recvone[r].seismo (io_funcs.cu:283-288, 1651-1659).
+ */
+int cgfd_get_seismograms(cgfd_problem *p, float *out);
+
+/* Number of stations located inside the grid (io_recv_read_locate's total_number). */
+int cgfd_num_stations(const cgfd_problem *p);
+
+/*
+ * Current wavefield w_pre in the reference layout [9][nz][ny][nx] (ghosts are 0), e.g.
+ * for a final snapshot. Replaces: the device-to-host copy of io_snap_nc_put.
+ */
+int cgfd_get_wavefield(cgfd_problem *p, float *out);
+
+/* Overwrite w_pre (physical points only; ghosts stay 0). */
+int cgfd_set_wavefield(cgfd_problem *p, const float *in);
+
+/* Device bytes held by the problem. */
+size_t cgfd_device_bytes(const cgfd_problem *p);
+
+/* Release all device and host state. Replaces: drv_rk_curv_col.cu:546-556. */
+int cgfd_problem_destroy(cgfd_problem *p);
+
+/*
+ * Stream the library launches on (a cudaStream_t, returned as void* so that the header
+ * needs no CUDA include).
+ */
+void *cgfd_stream(cgfd_problem *p);
+
+/*
+ * Enqueue n time steps on the problem's stream without synchronising (benchmarks and
+ * overlapping host work). cgfd_synchronize() waits and reports device-side errors.
+ */
+int cgfd_enqueue_steps(cgfd_problem *p, int nsteps);
+int cgfd_synchronize(cgfd_problem *p);
+
+/* ---- tuning knobs -------------------------------------------------------------------- */
+
+/* Disable (0) or enable (1, default) CUDA-graph replay of the time steps. */
+int cgfd_set_graph_mode(cgfd_problem *p, int on);
+
+/* z planes per thread block of the bulk stage kernel (autotuner knob). */
+int cgfd_set_zchunk(cgfd_problem *p, int nzc);
+int cgfd_get_zchunk(const cgfd_problem *p);
+
+/* ---- grid helpers (host, FP64) ------------------------------------------------------- */
+
+/*
+ * Fill the 3 ghost layers of ncmp fields [ncmp][nz][ny][nx] by linear extrapolation.
+ * Replaces: geometric_symmetry, gd_t.cu:404-502.
+ */
+int cgfd_fill_ghosts(int ni, int nj, int nk, int ncmp, float *v4d);
+
+/*
+ * Metrics from coordinates (ghosts filled), computed in FP64 with the 7-point centered
+ * operator and stored as float [10][nz][ny][nx].
+ * Replaces: gd_curv_metric_cal, gd_t.cu:209-314 (FP32 in the reference).
+ */
+int cgfd_metric_calc(int ni, int nj, int nk, const float *coord, float *metric);
+
+/*
+ * Largest stable time step (FP64): CFL * min distance to the 8 neighbour planes / Vp.
+ * Uses desc->coord and desc->medium (density form). The reference's CFL is 1.3.
+ * Replaces: blk_dt_esti_curv, blk_t.cu:673-763.
+ */
+int cgfd_dt_estimate(const cgfd_problem_desc *desc, double cfl, double *dtmax);
+
+/* Keep three significant digits. Replaces: blk_keep_three_digi, blk_t.cu:765-780. */
+double cgfd_keep_three_digits(double dt);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CGFD_B200_H */
