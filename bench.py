@@ -1,0 +1,347 @@
+#!/usr/bin/env python
+"""Benchmark of the CGFD3D elastic time loop on B200.
+
+Metric: Gcell-stage updates/s = ni*nj*nk (physical points incl. PML, ghosts excluded)
+x 4 RK stages x steps / time. One "step" is one time step (4 RK stages) of the plain FP32
+isotropic path on the 480x480x240 workload (50 m, CFS-PML 20, layered + 5% von Karman
+medium, one Ricker moment source fc=4 Hz, 400 surface stations), with every input resident
+in HBM. The wavefield (4 x 9 x 58 M floats) is far larger than L2, so no flush is needed.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference]
+
+Under torchrun each rank runs an independent replica on its own GPU (no collective on the
+data path); rank 0 prints one JSON line. --impl reference times the CPU restatement of the
+reference's time loop (the reference has no CPU solver of its own) on the host cores.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "gpu-cgfd3d-elastic_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "Gcell-stage updates/s"
+UNIT = "Gcell-stage/s"
+# algorithmic bytes per cell-stage of the fused RK4 stage (FP32): 36 wavefield accesses
+# (stage 0: 9 reads + 18 writes; stages 1-2: 27 + 18; stage 3: 18 + 9; averaged) plus the
+# coefficients read once per stage (iso 12, VTI 15, aniso 31).
+BYTES_PER_CELL_STAGE = {"iso": 36 * 4 + 12 * 4, "vti": 36 * 4 + 15 * 4, "aniso": 36 * 4 + 31 * 4}
+
+WORKLOADS = {
+    # name: (ni, nj, nk, dh, nsteps, npml, nsta_x, nsta_y, fc, perturb_std)
+    "480x480x240": (480, 480, 240, 50.0, 3000, 20, 20, 20, 4.0, 0.05),
+    "100x100x60": (100, 100, 60, 100.0, 500, 12, 5, 5, 2.0, 0.0),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", default="480x480x240", choices=sorted(WORKLOADS))
+    ap.add_argument("--grid", type=int, nargs=3, default=None, help="override ni nj nk (profiling)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--zchunk", type=int, default=0)
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def build_problem(args, device=0, nk_override=None):
+    from cgfd_b200 import synth
+    ni, nj, nk, dh, nsteps, npml, sx, sy, fc, pert = WORKLOADS[args.workload]
+    if args.grid:
+        ni, nj, nk = args.grid
+    if nk_override:
+        nk = nk_override
+    p = synth.make_problem(ni, nj, nk, dh, nsteps, dt=None, medium="iso", npml=npml, nsrc=1, sta_grid=(sx, sy),
+                           fc=fc, seed=2024, perturb_std=pert, corr=1000.0, hurst=0.3,
+                           src_depth=(2000.0, 2000.0), center_src=True)
+    p.device = device
+    return p
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(workload, cells_per_launch):
+    """DRAM bytes per bulk-kernel launch from the committed ncu summary, scaled by cells."""
+    path = os.path.join(ROOT, "profiles", "k_stage_bulk_iso.md")
+    try:
+        vals = {}
+        with open(path) as f:
+            for ln in f:
+                if ":" in ln and ln.strip().startswith("- "):
+                    k, v = ln.strip()[2:].split(":", 1)
+                    vals[k.strip()] = v.strip().split()[0]
+        b = float(vals["dram_bytes_per_launch"])
+        c = float(vals["cells_per_launch"])
+        return b * cells_per_launch / c
+    except Exception:
+        return None
+
+
+def cpu_baseline(args, threads):
+    """The oracle (FP32 CPU restatement, OpenMP on all host cores) on a sample of the workload."""
+    from oracle.oracle import Oracle
+    ni, nj, nk, *_ = WORKLOADS[args.workload]
+    if args.grid:
+        ni, nj, nk = args.grid
+    nk_s = max(16, min(nk, 24))
+    p = build_problem(args, nk_override=nk_s)
+    o = Oracle(p)
+    o.run(1)  # warm-up
+    t = time.perf_counter()
+    nst = 1
+    o.run(nst)
+    dt = time.perf_counter() - t
+    cells = p.ni * p.nj * p.nk * 4 * nst
+    return {"value": cells / dt / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{nst} time step (4 RK stages) of the {p.ni}x{p.nj}x{p.nk} slab of the workload "
+                      f"(same PML/free surface/source/stations), after 1 warm-up step; {dt:.2f} s"}
+
+
+def _oracle_rate(args, ni, nj, nk):
+    """cell-stages/s of the oracle on a small probe grid (1 warm-up + 1 timed step)."""
+    from oracle.oracle import Oracle
+    a = argparse.Namespace(**vars(args))
+    a.grid = [ni, nj, nk]
+    p = build_problem(a)
+    o = Oracle(p)
+    o.run(1)
+    t = time.perf_counter()
+    o.run(1)
+    return p.ni * p.nj * p.nk * 4 / (time.perf_counter() - t)
+
+
+def run_reference(args):
+    """--impl reference: the CPU restatement of the reference's time loop on host cores."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    threads = len(os.sched_getaffinity(0))
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    from oracle.oracle import Oracle
+    ni, nj, nk, *_ = WORKLOADS[args.workload]
+    if args.grid:
+        ni, nj, nk = args.grid
+    # bounded sample: a slab of the workload sized from a probe so that warm-up + steps
+    # finish in about two minutes on this host
+    rate = _oracle_rate(args, 64, 64, 16)
+    budget = 120.0
+    cells_per_step = rate * budget / max(1, args.steps + args.warmup) / 4.0
+    nk_s = max(16, min(nk, 24))
+    side = int(math.sqrt(max(cells_per_step / nk_s, 1.0)))
+    ni_s = max(48, min(ni, side))
+    nj_s = max(48, min(nj, side))
+    args_s = argparse.Namespace(**vars(args))
+    args_s.grid = [ni_s, nj_s, nk_s]
+    p = build_problem(args_s)
+    o = Oracle(p)
+    sample_steps = 1
+    for _ in range(args.warmup):
+        o.run(1)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        o.run(sample_steps)
+    el = time.perf_counter() - t
+    cells = p.ni * p.nj * p.nk * 4 * sample_steps * args.steps
+    v = cells / el / 1e9
+    out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": args.workload, "sample_grid": [p.ni, p.nj, p.nk], "medium": "elastic_iso"},
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                            "sample": f"each step = {sample_steps} time step(s) of the {p.ni}x{p.nj}x{p.nk} slab of "
+                                      "the workload by the oracle (the reference has no CPU solver)"},
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank, world, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from cgfd_b200 import Simulation
+
+    p = build_problem(args, device=local)
+    cells = p.ni * p.nj * p.nk
+    nbulk = p.nk - 4
+    sim = Simulation(p)
+    if args.zchunk:
+        sim.set_zchunk(args.zchunk)
+    st = torch.cuda.ExternalStream(sim.stream)
+    sim.enqueue(args.warmup)
+    sim.synchronize()
+    sim.set_timing(True)
+    sim.timing(reset=True)
+    sampler = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    sim.enqueue(args.steps)
+    e1.record(st)
+    e1.synchronize()
+    sim.synchronize()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    tim = sim.timing(reset=True)
+    sim.set_timing(False)
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * cells * 4 * args.steps / (ms * 1e-3) / 1e9
+
+    # roofline of the dominant kernel (bulk stage): algorithmic bytes per launch / duration
+    bulk_ms, bulk_n = tim["bulk"]
+    bpc = BYTES_PER_CELL_STAGE["iso"]
+    bulk_cells = p.ni * p.nj * nbulk
+    alg = bpc * bulk_cells
+    achieved = alg / (bulk_ms / bulk_n * 1e-3) / 1e9 if bulk_n else None
+    peak, peak_kind = measured_peak()
+    traffic = ncu_traffic(args.workload, bulk_cells)
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak if achieved else None, "traffic": traffic,
+            "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback",
+            "kernel": "k_stage_bulk<iso>", "bytes_per_cell_stage": bpc, "cells_per_launch": bulk_cells,
+            "kernel_ms": {k: (v[0] / v[1] if v[1] else None) for k, v in tim.items() if k != "launches"},
+            "kernel_share": {k: (v[0] / ms if ms else None) for k, v in tim.items() if k != "launches"}}
+    sim.close()
+    del sim
+
+    e2e = None
+    if not args.no_e2e:
+        # public API end to end: host arrays -> create (H2D + setup) -> K steps -> seismograms D2H
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t = time.perf_counter()
+        s2 = Simulation(p)
+        s2.enqueue(args.steps)
+        seis = s2.seismograms()
+        s2.synchronize()
+        t_e2e = time.perf_counter() - t
+        s2.close()
+        if dist:
+            tt = torch.tensor([t_e2e], device=f"cuda:{local}")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t_e2e = float(tt.item())
+        fld = (p.ni + 6) * (p.nj + 6) * (p.nk + 6) * 4
+        h2d = 13 * fld
+        e2e = {"value": world * cells * 4 * args.steps / t_e2e / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": seis.nbytes / args.steps,
+               "note": "cgfd_problem_create from host arrays (metric 10 + medium 3 fields) + K steps + "
+                       "seismogram read-back, wall clock"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = len(os.sched_getaffinity(0))
+        try:
+            cpu = cpu_baseline(args, threads)
+        except Exception as ex:  # report, do not fail the GPU measurement
+            cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": "port", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+               "config": {"workload": f"{p.ni}x{p.nj}x{p.nk}", "medium": "elastic_iso", "dh_m": 50.0,
+                          "pml_layers": 20, "free_surface": "timg", "sources": 1, "stations": 400,
+                          "dt": p.dt, "precision": "fp32", "parallelism": f"replicas x{world}",
+                          "l2": "inputs larger than L2 (wavefield 4x9x58M floats)"},
+               "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": tim["launches"],
+               "clocks": clocks}
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

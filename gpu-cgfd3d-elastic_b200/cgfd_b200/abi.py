@@ -207,6 +207,9 @@ def lib():
         "cgfd_set_graph_mode": (C.c_int, [P, C.c_int]),
         "cgfd_set_zchunk": (C.c_int, [P, C.c_int]),
         "cgfd_get_zchunk": (C.c_int, [P]),
+        "cgfd_set_timing": (C.c_int, [P, C.c_int]),
+        "cgfd_set_bulk_variant": (C.c_int, [P, C.c_int]),
+        "cgfd_get_timing": (C.c_int, [P, P, P, P, C.c_int]),
         "cgfd_fill_ghosts": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P]),
         "cgfd_metric_calc": (C.c_int, [C.c_int, C.c_int, C.c_int, P, P]),
         "cgfd_dt_estimate": (C.c_int, [C.POINTER(ProblemDesc), C.c_double, C.POINTER(C.c_double)]),
@@ -301,6 +304,23 @@ class Simulation:
     @property
     def zchunk(self):
         return lib().cgfd_get_zchunk(self.h)
+
+    def set_bulk_variant(self, tma):
+        check(lib().cgfd_set_bulk_variant(self.h, int(tma)))
+
+    def set_timing(self, on):
+        check(lib().cgfd_set_timing(self.h, int(on)))
+
+    def timing(self, reset=False):
+        """{kind: (total_ms, launches)} for bulk/surface/source/recv, plus total launches."""
+        ms = np.zeros(4, np.float64)
+        cnt = np.zeros(4, np.int64)
+        tot = C.c_longlong()
+        check(lib().cgfd_get_timing(self.h, ms.ctypes.data, cnt.ctypes.data, C.addressof(tot), int(reset)))
+        kinds = ("bulk", "surface", "source", "recv")
+        out = {k: (float(ms[n]), int(cnt[n])) for n, k in enumerate(kinds)}
+        out["launches"] = int(tot.value)
+        return out
 
     @property
     def stream(self):

@@ -10,6 +10,8 @@
 // One time step = station sampling, then per RK stage the bulk and surface-slab stage
 // kernels and the source kernel, then the step-counter advance. The 8 MacCormack pairs and
 // the 2 buffer parities give 8 distinct steps; each is captured once as a CUDA graph.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -57,6 +59,32 @@ T *dmalloc(size_t n, size_t &acc) {
   return (T *)p;
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void *ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !ptr)
+      throw cgfd::Error(CGFD_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+  }
+  return fn;
+}
+
+// 4-D map (x, y, z, field) over one device-layout array of nf fields.
+void make_map(CUtensorMap *m, const float *base, long long sx, long long ny, long long nz, int nf, long long sz,
+              long long sf, int boxx, int boxy, int boxf) {
+  cuuint64_t dims[4] = {(cuuint64_t)sx, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)nf};
+  cuuint64_t strides[3] = {(cuuint64_t)sx * 4, (cuuint64_t)sz * 4, (cuuint64_t)sf * 4};
+  cuuint32_t box[4] = {(cuuint32_t)boxx, (cuuint32_t)boxy, 1, (cuuint32_t)boxf};
+  cuuint32_t es[4] = {1, 1, 1, 1};
+  CUresult r = tensor_map_encoder()(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float *>(base), dims, strides,
+                                    box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw cgfd::Error(CGFD_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+}
+
 }  // namespace
 
 struct cgfd_problem {
@@ -92,8 +120,54 @@ struct cgfd_problem {
   int it = 0;
 
   bool use_graph = true;
+  bool use_tma = true;
+  CUtensorMap map_halo[4], map_ctr[4], map_coef;
   cudaGraphExec_t graph[8] = {};
   bool graph_ok[8] = {};
+  int graph_launches[8] = {};
+
+  // per-kernel CUDA-event timing (direct launches only): kind 0 bulk, 1 surface, 2 source, 3 recv
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_free;
+  struct TimedLaunch { int kind; cudaEvent_t a, b; };
+  std::vector<TimedLaunch> pending;
+  double t_ms[4] = {0, 0, 0, 0};
+  long long t_n[4] = {0, 0, 0, 0};
+  long long launches = 0;
+
+  cudaEvent_t get_event() {
+    if (ev_free.empty()) {
+      cudaEvent_t e;
+      CK(cudaEventCreate(&e));
+      return e;
+    }
+    cudaEvent_t e = ev_free.back();
+    ev_free.pop_back();
+    return e;
+  }
+
+  template <typename Fn>
+  int timed(int kind, Fn fn) {
+    if (!timing) return fn();
+    cudaEvent_t a = get_event(), b = get_event();
+    CK(cudaEventRecord(a, stream));
+    int n = fn();
+    CK(cudaEventRecord(b, stream));
+    pending.push_back({kind, a, b});
+    return n;
+  }
+
+  void collect_timing() {
+    for (auto &t : pending) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, t.a, t.b));
+      t_ms[t.kind] += ms;
+      t_n[t.kind] += 1;
+      ev_free.push_back(t.a);
+      ev_free.push_back(t.b);
+    }
+    pending.clear();
+  }
 
   long long didx(int i, int j, int k) const { return off0 + (long long)k * sz + (long long)j * sx + i; }
 
@@ -118,6 +192,7 @@ struct cgfd_problem {
     p.coef = coef; p.jac = jac; p.matx = matx; p.maty = maty;
     p.free_top = free_top;
     p.nbulk = free_top ? nk - cgfd::NSURF : nk;
+    p.err = d_flag;
     p.nface = 0;
     for (const Face &f : faces) {
       cgfd::FaceP &o = p.face[p.nface++];
@@ -138,17 +213,30 @@ struct cgfd_problem {
     return p;
   }
 
-  void enqueue_step(int step) {
+  int enqueue_step(int step) {
     cudaStream_t st = stream;
+    int n = 0;
     if (rec.n > 0) {
       cgfd::RecvP r;
       r.nsta = rec.n; r.nt_total = nt_total; r.idx8 = d_idx8; r.w8 = d_w8;
       r.pre = wbuf[step & 1]; r.sf = sf; r.seis = d_seis; r.d_it = d_it; r.d_flag = d_flag;
-      cgfd::launch_recv(r, st);
+      n += timed(3, [&] { return cgfd::launch_recv(r, st); });
     }
     for (int s = 0; s < 4; s++) {
       cgfd::StageP p = stage_params(step, s);
-      cgfd::launch_stage(med, p, nzc, st);
+      if (use_tma) {
+        cgfd::TmaP tm;
+        const int pre = step & 1, end = (step + 1) & 1;
+        const int curs[4] = {pre, 2, 3, 2};
+        tm.cur = map_halo[curs[s]];
+        tm.pre = map_ctr[pre];
+        tm.end = map_ctr[end];
+        tm.coef = map_coef;
+        n += timed(0, [&] { return cgfd::launch_stage_bulk_tma(med, p, tm, nzc, st); });
+      } else {
+        n += timed(0, [&] { return cgfd::launch_stage_bulk(med, p, nzc, st); });
+      }
+      n += timed(1, [&] { return cgfd::launch_stage_surface(med, p, st); });
       if (src.nsrc > 0) {
         cgfd::SrcP q;
         q.nsrc = src.nsrc; q.max_ext = src.max_ext; q.max_nt = src.max_nt;
@@ -157,29 +245,31 @@ struct cgfd_problem {
         q.it_begin = d_it_begin; q.ext_num = d_ext_num; q.ext_idx = d_ext_idx;
         q.ext_wv = d_ext_wv; q.ext_wt = d_ext_wt; q.stf = d_stf;
         q.tmp_out = p.tmp_out; q.end = p.end; q.sf = sf; q.d_it = d_it;
-        cgfd::launch_source(q, st);
+        n += timed(2, [&] { return cgfd::launch_source(q, st); });
       }
     }
-    cgfd::launch_advance(d_it, st);
+    n += cgfd::launch_advance(d_it, st);
+    return n;
   }
 
   void run_steps(int n) {
     for (int s = 0; s < n; s++) {
       int step = it;
       int slot = step % 8;
-      if (use_graph) {
+      if (use_graph && !timing) {
         if (!graph_ok[slot]) {
           cudaGraph_t g;
           CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-          enqueue_step(step);
+          graph_launches[slot] = enqueue_step(step);
           CK(cudaStreamEndCapture(stream, &g));
           CK(cudaGraphInstantiate(&graph[slot], g, 0));
           CK(cudaGraphDestroy(g));
           graph_ok[slot] = true;
         }
         CK(cudaGraphLaunch(graph[slot], stream));
+        launches += graph_launches[slot];
       } else {
-        enqueue_step(step);
+        launches += enqueue_step(step);
         CK(cudaGetLastError());
       }
       it++;
@@ -190,6 +280,8 @@ struct cgfd_problem {
     if (device >= 0) cudaSetDevice(device);
     for (int s = 0; s < 8; s++)
       if (graph_ok[s]) cudaGraphExecDestroy(graph[s]);
+    for (auto &t : pending) { ev_free.push_back(t.a); ev_free.push_back(t.b); }
+    for (auto e : ev_free) cudaEventDestroy(e);
     for (auto *p : wbuf) cudaFree(p);
     cudaFree(coef); cudaFree(jac); cudaFree(matx); cudaFree(maty);
     for (Face &f : faces) { cudaFree(f.A); cudaFree(f.B); cudaFree(f.D); cudaFree(f.aux); }
@@ -272,6 +364,16 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d) {
   cudaFree(stage_buf);
   B -= g.siz_icmp * sizeof(float);
 
+  // TMA tensor maps of the four wavefield levels and of the coefficients
+  {
+    int ty = cgfd::tma_tile_y(p->med);
+    for (int l = 0; l < 4; l++) {
+      make_map(&p->map_halo[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9, p->sz, p->sf, cgfd::TX + 8, ty + 6, 9);
+      make_map(&p->map_ctr[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9, p->sz, p->sf, cgfd::TX, ty, 9);
+    }
+    make_map(&p->map_coef, p->coef, p->sx, p->nj + 6, p->nk + 6, p->ncoef, p->sz, p->sf, cgfd::TX, ty, p->ncoef);
+    CK(cgfd::tma_prepare(p->med));
+  }
   // free surface
   if (p->free_top) {
     std::vector<float> mx, my;
@@ -383,8 +485,10 @@ int cgfd_synchronize(cgfd_problem *p) {
   return guarded([&] {
     CK(cudaSetDevice(p->device));
     CK(cudaStreamSynchronize(p->stream));
+    p->collect_timing();
     int flag = 0;
     CK(cudaMemcpy(&flag, p->d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag & 2) throw cgfd::Error(CGFD_ERR_CUDA, "a TMA pipeline wait timed out in the stage kernel");
     if (flag) throw cgfd::Error(CGFD_ERR_NONFINITE, "non-finite value sampled at a station");
   });
 }
@@ -405,6 +509,8 @@ int cgfd_set_step(cgfd_problem *p, int it) {
     // the buffer roles follow the step parity: move w_pre / PML pre to the new parity
     if ((it & 1) != (p->it & 1)) {
       std::swap(p->wbuf[0], p->wbuf[1]);
+      std::swap(p->map_halo[0], p->map_halo[1]);
+      std::swap(p->map_ctr[0], p->map_ctr[1]);
       for (auto &f : p->faces) {
         size_t n = (size_t)9 * f.n;
         CK(cudaMemcpyAsync(f.aux + n * 2, f.aux, n * sizeof(float), cudaMemcpyDeviceToDevice, p->stream));
@@ -484,5 +590,37 @@ int cgfd_set_zchunk(cgfd_problem *p, int nzc) {
 }
 
 int cgfd_get_zchunk(const cgfd_problem *p) { return p ? p->nzc : -1; }
+
+/* Bulk kernel variant: 1 = TMA-pipelined (default), 0 = direct loads. */
+int cgfd_set_bulk_variant(cgfd_problem *p, int tma) {
+  if (!p) return CGFD_ERR_INVALID;
+  p->use_tma = tma != 0;
+  for (int s = 0; s < 8; s++)
+    if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }
+  return CGFD_OK;
+}
+
+/* Per-kernel CUDA-event timing of subsequent steps (forces direct launches while on). */
+int cgfd_set_timing(cgfd_problem *p, int on) {
+  if (!p) return CGFD_ERR_INVALID;
+  p->timing = on != 0;
+  return CGFD_OK;
+}
+
+/* ms[4], count[4] accumulated since the last reset for kinds {bulk, surface, source, recv};
+   *launches = kernels launched by the library since the last reset. */
+int cgfd_get_timing(cgfd_problem *p, double *ms, long long *count, long long *launches, int reset) {
+  if (!p) return CGFD_ERR_INVALID;
+  for (int k = 0; k < 4; k++) {
+    if (ms) ms[k] = p->t_ms[k];
+    if (count) count[k] = p->t_n[k];
+  }
+  if (launches) *launches = p->launches;
+  if (reset) {
+    for (int k = 0; k < 4; k++) { p->t_ms[k] = 0; p->t_n[k] = 0; }
+    p->launches = 0;
+  }
+  return CGFD_OK;
+}
 
 }  // extern "C"

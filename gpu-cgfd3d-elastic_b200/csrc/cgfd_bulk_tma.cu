@@ -1,0 +1,313 @@
+// cgfd_bulk_tma.cu -- TMA-pipelined bulk RK-stage kernel for sm_100a.
+//
+// Each thread block owns a 32 x TYT column tile and marches along z through its chunk of
+// planes. Thread 0 streams, two planes ahead of the computation and with mbarrier
+// completion:
+//   - the stage input of one plane with its x-y halo, all 9 fields, as ONE 4-D TMA box
+//     (40 x (TYT+6) x 1 x 9) into a 3-slot ring (plane k for the x/y operators, plane k+-1
+//     for the z look-ahead, one in flight);
+//   - the coefficients (metrics, 1/rho, moduli) and, when the stage needs them, w_pre and
+//     w_end of the same plane (centre boxes) into a 2-slot ring.
+// The z march runs upwards for backward z operators and downwards for forward ones, so the
+// one-sided operator always needs exactly one plane ahead; the other 3 planes of the
+// 5-point z stencil live in a per-thread register queue. No thread computes an address
+// for a stencil or coefficient load; HBM sees every value once per stage.
+#include "cgfd_dev.cuh"
+#include "cgfd_launch.h"
+#include "cgfd_tma.cuh"
+
+namespace cgfd {
+
+template <int MED, int TYT>
+struct BulkSmem {
+  static constexpr int WX = TX + 8;   // x box [-4, 36) around the tile
+  static constexpr int WY = TYT + 6;  // y box [-3, TYT+3)
+  static constexpr int NC = MedInfo<MED>::NCOEF;
+  static constexpr int CELLS = TX * TYT;
+  static constexpr int WAVE_FLOATS = 9 * WY * WX;
+  static constexpr int WAVE_SLOT = ((WAVE_FLOATS * 4 + 127) / 128) * 128;  // bytes
+  static constexpr int COEF_BYTES = NC * CELLS * 4;
+  static constexpr int FLD_BYTES = 9 * CELLS * 4;
+  static constexpr int CPE_SLOT = COEF_BYTES + 2 * FLD_BYTES;
+  static constexpr int OFF_CPE = 3 * WAVE_SLOT;
+  static constexpr int OFF_BAR = OFF_CPE + 2 * CPE_SLOT;
+  static constexpr int BYTES = OFF_BAR + 8 * 8;
+};
+
+template <int MED>
+struct MediumS;
+template <>
+struct MediumS<MED_ISO> {
+  static __device__ __forceinline__ void load(Medium<MED_ISO> &m, const float *c, int stride) {
+    m.lam = c[(CF_MED + 0) * stride];
+    m.mu = c[(CF_MED + 1) * stride];
+    m.lam2mu = m.lam + 2.0f * m.mu;
+  }
+};
+template <>
+struct MediumS<MED_VTI> {
+  static __device__ __forceinline__ void load(Medium<MED_VTI> &m, const float *c, int stride) {
+    m.c11 = c[(CF_MED + 0) * stride];
+    m.c13 = c[(CF_MED + 1) * stride];
+    m.c33 = c[(CF_MED + 2) * stride];
+    m.c55 = c[(CF_MED + 3) * stride];
+    m.c66 = c[(CF_MED + 4) * stride];
+    m.c12 = m.c11 - 2.0f * m.c66;
+  }
+};
+template <>
+struct MediumS<MED_ANISO> {
+  static __device__ __forceinline__ void load(Medium<MED_ANISO> &m, const float *c, int stride) {
+#pragma unroll
+    for (int n = 0; n < 21; n++) m.c[n] = c[(CF_MED + n) * stride];
+  }
+};
+
+template <int MED, int DX, int DY, int DZ, int TYT>
+__global__ void __launch_bounds__(TX *TYT, 1)
+    k_stage_bulk_tma(const __grid_constant__ StageP p, const __grid_constant__ TmaP tm, int nzc) {
+  using S = BulkSmem<MED, TYT>;
+  constexpr int LX = op_left(DX), LY = op_left(DY);
+  constexpr int SD = DZ ? -1 : 1;  // march direction
+  extern __shared__ __align__(128) unsigned char smem[];
+  float *wave = reinterpret_cast<float *>(smem);
+  unsigned char *cpe = smem + S::OFF_CPE;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + S::OFF_BAR);  // 0..2 wave, 3..4 cpe
+
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int bx = blockIdx.x, by = blockIdx.y;
+  const int i = bx * TX + tx, j = by * TYT + ty;
+  const int kb = blockIdx.z * nzc;
+  const int ke = min(kb + nzc, p.nbulk);
+  if (kb >= ke) return;
+  const int n = ke - kb;
+  const bool act = i < p.ni && j < p.nj;
+  const int k0 = SD > 0 ? kb : ke - 1;
+  const long long sf = p.sf;
+  const int stage = p.stage;
+  const bool need_pre = stage == 1 || stage == 2;
+  const bool need_end = stage >= 1;
+  const uint32_t wave_bytes = S::WAVE_FLOATS * 4;
+  const uint32_t cpe_bytes = S::COEF_BYTES + (need_pre ? S::FLD_BYTES : 0) + (need_end ? S::FLD_BYTES : 0);
+  // box origins in device-layout coordinates (x multiple of 4: 16-byte aligned)
+  const int xw = GX + bx * TX - 4, yw = by * TYT;
+  const int xc = GX + bx * TX, yc = 3 + by * TYT;
+
+  if (tid == 0) {
+    for (int b = 0; b < 5; b++) mbar_init(&bar[b], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  auto issue_wave = [&](int m) {
+    const int kk = k0 + m * SD;
+    uint64_t *b = &bar[m % 3];
+    mbar_expect_tx(b, wave_bytes);
+    tma_load_4d(wave + (m % 3) * (S::WAVE_SLOT / 4), &tm.cur, xw, yw, kk + 3, 0, b);
+  };
+  auto issue_cpe = [&](int m) {
+    const int kk = k0 + m * SD;
+    const int sl = m & 1;
+    uint64_t *b = &bar[3 + sl];
+    unsigned char *base = cpe + sl * S::CPE_SLOT;
+    mbar_expect_tx(b, cpe_bytes);
+    tma_load_4d(base, &tm.coef, xc, yc, kk + 3, 0, b);
+    if (need_pre) tma_load_4d(base + S::COEF_BYTES, &tm.pre, xc, yc, kk + 3, 0, b);
+    if (need_end) tma_load_4d(base + S::COEF_BYTES + S::FLD_BYTES, &tm.end, xc, yc, kk + 3, 0, b);
+  };
+  if (tid == 0) {
+    issue_wave(0);
+    issue_wave(1);
+    issue_cpe(0);
+  }
+
+  // PML faces that intersect this block (uniform)
+  unsigned fmask = 0;
+  for (int fi = 0; fi < p.nface; fi++) {
+    const FaceP &f = p.face[fi];
+    const bool xo = f.lo[0] <= bx * TX + TX - 1 && f.hi[0] >= bx * TX;
+    const bool yo = f.lo[1] <= by * TYT + TYT - 1 && f.hi[1] >= by * TYT;
+    const bool zo = f.lo[2] <= ke - 1 && f.hi[2] >= kb;
+    if (xo && yo && zo) fmask |= 1u << fi;
+  }
+
+  // register queue in march order: q[f][n] = plane k + (n - 3) * SD
+  float q[9][5];
+#pragma unroll
+  for (int f = 0; f < 9; f++)
+#pragma unroll
+    for (int m = 0; m < 5; m++) q[f][m] = 0.f;
+  if (act) {
+#pragma unroll
+    for (int m = 0; m < 3; m++) {
+      const long long id = didx(p, i, j, k0 + (m - 3) * SD);
+#pragma unroll
+      for (int f = 0; f < 9; f++) q[f][m] = __ldg(p.cur + f * sf + id);
+    }
+  }
+  const int wc = (ty + 3) * S::WX + tx + 4;  // centre of this thread in a wave slot (per field)
+  mbar_wait(&bar[0], 0, p.err);
+#pragma unroll
+  for (int f = 0; f < 9; f++) q[f][3] = wave[f * S::WY * S::WX + wc];
+
+  const int cell = ty * TX + tx;
+  for (int m = 0; m < n; m++) {
+    const int k = k0 + m * SD;
+    if (tid == 0) {
+      if (m + 2 <= n) issue_wave(m + 2);
+      if (m + 1 < n) issue_cpe(m + 1);
+    }
+    const int ws = m % 3, wn = (m + 1) % 3, cs = m & 1;
+    mbar_wait(&bar[wn], ((m + 1) / 3) & 1, p.err);
+    mbar_wait(&bar[3 + cs], (m >> 1) & 1, p.err);
+    const float *W = wave + ws * (S::WAVE_SLOT / 4);
+    const float *Wn = wave + wn * (S::WAVE_SLOT / 4);
+#pragma unroll
+    for (int f = 0; f < 9; f++) q[f][4] = Wn[f * S::WY * S::WX + wc];
+
+    if (act) {
+      const float *Cc = reinterpret_cast<const float *>(cpe + cs * S::CPE_SLOT) + cell;
+      float mt[3][3];
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) mt[a][b] = Cc[(3 * a + b) * S::CELLS];
+      const float slw = Cc[CF_SLW * S::CELLS];
+      Medium<MED> md;
+      MediumS<MED>::load(md, Cc, S::CELLS);
+      CellAcc acc;
+      acc.zero();
+      // x
+      {
+        float d[9];
+#pragma unroll
+        for (int f = 0; f < 9; f++) {
+          const float *r = W + f * S::WY * S::WX + (ty + 3) * S::WX + tx + 4 - LX;
+          d[f] = drp5<DX>(r[0], r[1], r[2], r[3], r[4]);
+        }
+        acc.add_axis(mt[0], d, d + 3);
+        if (fmask)
+          for (int fi = 0; fi < p.nface; fi++) {
+            const FaceP &fc = p.face[fi];
+            if ((fmask >> fi & 1) && fc.axis == 0 && i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] &&
+                j <= fc.hi[1] && k >= fc.lo[2] && k <= fc.hi[2])
+              pml_face<MED>(p, fc, i, j, k, md, slw, mt[0], d, d + 3, nullptr, nullptr, acc.hc);
+          }
+      }
+      // y
+      {
+        float d[9];
+#pragma unroll
+        for (int f = 0; f < 9; f++) {
+          const float *r = W + f * S::WY * S::WX + (ty + 3 - LY) * S::WX + tx + 4;
+          d[f] = drp5<DY>(r[0], r[S::WX], r[2 * S::WX], r[3 * S::WX], r[4 * S::WX]);
+        }
+        acc.add_axis(mt[1], d, d + 3);
+        if (fmask)
+          for (int fi = 0; fi < p.nface; fi++) {
+            const FaceP &fc = p.face[fi];
+            if ((fmask >> fi & 1) && fc.axis == 1 && i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] &&
+                j <= fc.hi[1] && k >= fc.lo[2] && k <= fc.hi[2])
+              pml_face<MED>(p, fc, i, j, k, md, slw, mt[1], d, d + 3, nullptr, nullptr, acc.hc);
+          }
+      }
+      // z (queue in march order; the operator takes increasing k)
+      {
+        float d[9];
+#pragma unroll
+        for (int f = 0; f < 9; f++)
+          d[f] = SD > 0 ? drp5<DZ>(q[f][0], q[f][1], q[f][2], q[f][3], q[f][4])
+                        : drp5<DZ>(q[f][4], q[f][3], q[f][2], q[f][1], q[f][0]);
+        acc.add_axis(mt[2], d, d + 3);
+        if (fmask)
+          for (int fi = 0; fi < p.nface; fi++) {
+            const FaceP &fc = p.face[fi];
+            if ((fmask >> fi & 1) && fc.axis == 2 && i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] &&
+                j <= fc.hi[1] && k >= fc.lo[2] && k <= fc.hi[2])
+              pml_face<MED>(p, fc, i, j, k, md, slw, mt[2], d, d + 3, nullptr, nullptr, acc.hc);
+          }
+      }
+      float h[9];
+      h[0] = slw * acc.mom[0] + acc.hc[0];
+      h[1] = slw * acc.mom[1] + acc.hc[1];
+      h[2] = slw * acc.mom[2] + acc.hc[2];
+      md.hooke(acc.G, h + 3);
+#pragma unroll
+      for (int c = 3; c < 9; c++) h[c] += acc.hc[c];
+      // RK combine (wav_update / wav_update_end)
+      const long long id = didx(p, i, j, k);
+      const float *PR = reinterpret_cast<const float *>(cpe + cs * S::CPE_SLOT + S::COEF_BYTES) + cell;
+      const float *EN = PR + 9 * S::CELLS;
+      const float ca = p.ca, cb = p.cb;
+      if (stage == 0) {
+#pragma unroll
+        for (int f = 0; f < 9; f++) {
+          p.tmp_out[f * sf + id] = q[f][3] + ca * h[f];
+          p.end[f * sf + id] = q[f][3] + cb * h[f];
+        }
+      } else if (stage < 3) {
+#pragma unroll
+        for (int f = 0; f < 9; f++) {
+          p.tmp_out[f * sf + id] = PR[f * S::CELLS] + ca * h[f];
+          p.end[f * sf + id] = EN[f * S::CELLS] + cb * h[f];
+        }
+      } else {
+#pragma unroll
+        for (int f = 0; f < 9; f++) p.end[f * sf + id] = EN[f * S::CELLS] + cb * h[f];
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < 9; f++)
+#pragma unroll
+      for (int m2 = 0; m2 < 4; m2++) q[f][m2] = q[f][m2 + 1];
+    __syncthreads();
+  }
+}
+
+// -----------------------------------------------------------------------------------------
+template <int MED, int TYT>
+static void launch_tma_med(const StageP &p, const TmaP &tm, int nzc, cudaStream_t st) {
+  using S = BulkSmem<MED, TYT>;
+  const int code = p.dir[0] | (p.dir[1] << 1) | (p.dir[2] << 2);
+  dim3 block(TX, TYT);
+  dim3 grid((p.ni + TX - 1) / TX, (p.nj + TYT - 1) / TYT, (p.nbulk + nzc - 1) / nzc);
+  switch (code) {
+#define CASE(c)                                                                                            \
+  case c:                                                                                                  \
+    k_stage_bulk_tma<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, TYT><<<grid, block, S::BYTES, st>>>(p, tm, nzc); \
+    break;
+    CASE(0) CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7)
+#undef CASE
+  }
+}
+
+template <int MED, int TYT>
+static cudaError_t set_attr_med() {
+  using S = BulkSmem<MED, TYT>;
+  cudaError_t e = cudaSuccess;
+#define ATTR(c)                                                                                              \
+  if (e == cudaSuccess)                                                                                      \
+    e = cudaFuncSetAttribute(k_stage_bulk_tma<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, TYT>,           \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, S::BYTES);
+  ATTR(0) ATTR(1) ATTR(2) ATTR(3) ATTR(4) ATTR(5) ATTR(6) ATTR(7)
+#undef ATTR
+  return e;
+}
+
+int tma_tile_y(int med) { return med == MED_ISO ? 16 : 8; }
+
+cudaError_t tma_prepare(int med) {
+  if (med == MED_ISO) return set_attr_med<MED_ISO, 16>();
+  if (med == MED_VTI) return set_attr_med<MED_VTI, 8>();
+  return set_attr_med<MED_ANISO, 8>();
+}
+
+int launch_stage_bulk_tma(int med, const StageP &p, const TmaP &tm, int nzc, cudaStream_t st) {
+  if (p.nbulk <= 0) return 0;
+  if (med == MED_ISO) launch_tma_med<MED_ISO, 16>(p, tm, nzc, st);
+  else if (med == MED_VTI) launch_tma_med<MED_VTI, 8>(p, tm, nzc, st);
+  else launch_tma_med<MED_ANISO, 8>(p, tm, nzc, st);
+  return 1;
+}
+
+}  // namespace cgfd

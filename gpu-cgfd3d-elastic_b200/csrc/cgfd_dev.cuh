@@ -9,6 +9,7 @@
 // The RHS itself never reaches HBM.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -71,6 +72,13 @@ struct StageP {
   int nbulk;              // planes [0, nbulk) belong to the bulk kernel
   int nface;
   FaceP face[6];
+  int *err;               // device error word (bit 1: pipeline wait timed out)
+};
+
+// Tensor maps of the arrays one stage streams through TMA: the stage input (4-D box with
+// the x-y halo, all 9 fields), w_pre / w_end (centre boxes, 9 fields), coefficients.
+struct TmaP {
+  CUtensorMap cur, pre, end, coef;
 };
 
 // ---------------------------------------------------------------------------------------

@@ -405,36 +405,44 @@ static void launch_bulk_med(const StageP &p, int nzc, dim3 grid, cudaStream_t st
   }
 }
 
-void launch_stage(int med, const StageP &p, int nzc, cudaStream_t st) {
-  if (p.nbulk > 0) {
-    dim3 grid((p.ni + TX - 1) / TX, (p.nj + TY - 1) / TY, (p.nbulk + nzc - 1) / nzc);
-    if (med == MED_ISO) launch_bulk_med<MED_ISO>(p, nzc, grid, st);
-    else if (med == MED_VTI) launch_bulk_med<MED_VTI>(p, nzc, grid, st);
-    else launch_bulk_med<MED_ANISO>(p, nzc, grid, st);
-  }
-  if (p.nbulk < p.nk) {
-    dim3 block(32, 4);
-    dim3 grid((p.ni + 31) / 32, (p.nj + 3) / 4);
-    if (med == MED_ISO) k_stage_surface<MED_ISO><<<grid, block, 0, st>>>(p);
-    else if (med == MED_VTI) k_stage_surface<MED_VTI><<<grid, block, 0, st>>>(p);
-    else k_stage_surface<MED_ANISO><<<grid, block, 0, st>>>(p);
-  }
+int launch_stage_bulk(int med, const StageP &p, int nzc, cudaStream_t st) {
+  if (p.nbulk <= 0) return 0;
+  dim3 grid((p.ni + TX - 1) / TX, (p.nj + TY - 1) / TY, (p.nbulk + nzc - 1) / nzc);
+  if (med == MED_ISO) launch_bulk_med<MED_ISO>(p, nzc, grid, st);
+  else if (med == MED_VTI) launch_bulk_med<MED_VTI>(p, nzc, grid, st);
+  else launch_bulk_med<MED_ANISO>(p, nzc, grid, st);
+  return 1;
 }
 
-void launch_source(const SrcP &s, cudaStream_t st) {
-  if (s.nsrc <= 0) return;
+int launch_stage_surface(int med, const StageP &p, cudaStream_t st) {
+  if (p.nbulk >= p.nk) return 0;
+  dim3 block(32, 4);
+  dim3 grid((p.ni + 31) / 32, (p.nj + 3) / 4);
+  if (med == MED_ISO) k_stage_surface<MED_ISO><<<grid, block, 0, st>>>(p);
+  else if (med == MED_VTI) k_stage_surface<MED_VTI><<<grid, block, 0, st>>>(p);
+  else k_stage_surface<MED_ANISO><<<grid, block, 0, st>>>(p);
+  return 1;
+}
+
+int launch_source(const SrcP &s, cudaStream_t st) {
+  if (s.nsrc <= 0) return 0;
   dim3 block(128);
   dim3 grid((s.max_ext + 127) / 128, s.nsrc);
   k_source<<<grid, block, 0, st>>>(s);
+  return 1;
 }
 
-void launch_recv(const RecvP &r, cudaStream_t st) {
-  if (r.nsta <= 0) return;
+int launch_recv(const RecvP &r, cudaStream_t st) {
+  if (r.nsta <= 0) return 0;
   int n = r.nsta * 9;
   k_recv<<<(n + 127) / 128, 128, 0, st>>>(r);
+  return 1;
 }
 
-void launch_advance(int *d_it, cudaStream_t st) { k_advance<<<1, 32, 0, st>>>(d_it); }
+int launch_advance(int *d_it, cudaStream_t st) {
+  k_advance<<<1, 32, 0, st>>>(d_it);
+  return 1;
+}
 
 void launch_repack_in(const float *src, float *dst, int ni, int nj, int nk, long long sx, long long sz, long long off0,
                       int mode, int ghosts, cudaStream_t st) {

@@ -6,6 +6,7 @@
 namespace cgfd {
 
 struct StageP;
+struct TmaP;
 
 // Source injection of one stage (sv_curv_col_el_gpu.cu:227-301), applied to tmp/end.
 struct SrcP {
@@ -38,10 +39,16 @@ struct RecvP {
   int *d_flag;
 };
 
-void launch_stage(int med, const StageP &p, int nzc, cudaStream_t st);
-void launch_source(const SrcP &s, cudaStream_t st);
-void launch_recv(const RecvP &r, cudaStream_t st);
-void launch_advance(int *d_it, cudaStream_t st);
+// Each launcher returns the number of kernels it launched (0 or 1).
+int launch_stage_bulk(int med, const StageP &p, int nzc, cudaStream_t st);
+int launch_stage_surface(int med, const StageP &p, cudaStream_t st);
+// TMA-pipelined bulk kernel: tile height, one-time function attributes, launch.
+int tma_tile_y(int med);
+cudaError_t tma_prepare(int med);
+int launch_stage_bulk_tma(int med, const StageP &p, const TmaP &tm, int nzc, cudaStream_t st);
+int launch_source(const SrcP &s, cudaStream_t st);
+int launch_recv(const RecvP &r, cudaStream_t st);
+int launch_advance(int *d_it, cudaStream_t st);
 void launch_repack_in(const float *src, float *dst, int ni, int nj, int nk, long long sx, long long sz,
                       long long off0, int mode, int ghosts, cudaStream_t st);
 void launch_repack_out(const float *src, float *dst, int ni, int nj, int nk, long long sx, long long sz,

@@ -202,6 +202,19 @@ int cgfd_set_graph_mode(cgfd_problem *p, int on);
 int cgfd_set_zchunk(cgfd_problem *p, int nzc);
 int cgfd_get_zchunk(const cgfd_problem *p);
 
+/* Bulk stage kernel variant: 1 = TMA-pipelined (default), 0 = direct global loads. */
+int cgfd_set_bulk_variant(cgfd_problem *p, int tma);
+
+/* Per-kernel CUDA-event timing of subsequent steps (uses direct launches while on). */
+int cgfd_set_timing(cgfd_problem *p, int on);
+
+/*
+ * Accumulated kernel times (ms[4]) and launch counts (count[4]) for the kernel kinds
+ * {bulk stage, surface-slab stage, source, station}, and the number of kernels the library
+ * launched (*launches); reset != 0 clears them.
+ */
+int cgfd_get_timing(cgfd_problem *p, double *ms, long long *count, long long *launches, int reset);
+
 /* ---- grid helpers (host, FP64) ------------------------------------------------------- */
 
 /*
