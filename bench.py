@@ -290,7 +290,8 @@ def main():
             "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback",
             "kernel": "k_stage_bulk<iso>", "bytes_per_cell_stage": bpc, "cells_per_launch": bulk_cells,
             "kernel_ms": {k: (v[0] / v[1] if v[1] else None) for k, v in tim.items() if k != "launches"},
-            "kernel_share": {k: (v[0] / ms if ms else None) for k, v in tim.items() if k != "launches"}}
+            "kernel_share": {k: (v[0] / ms if ms else None) for k, v in tim.items()
+                             if k in ("bulk", "surface", "source", "recv")}}
     sim.close()
     del sim
 

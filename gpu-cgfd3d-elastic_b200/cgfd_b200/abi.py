@@ -312,13 +312,15 @@ class Simulation:
         check(lib().cgfd_set_timing(self.h, int(on)))
 
     def timing(self, reset=False):
-        """{kind: (total_ms, launches)} for bulk/surface/source/recv, plus total launches."""
-        ms = np.zeros(4, np.float64)
-        cnt = np.zeros(4, np.int64)
+        """{kind: (total_ms, launches)} per kernel kind plus "bulk" (all stages) and the
+        total number of library kernel launches."""
+        ms = np.zeros(8, np.float64)
+        cnt = np.zeros(8, np.int64)
         tot = C.c_longlong()
         check(lib().cgfd_get_timing(self.h, ms.ctypes.data, cnt.ctypes.data, C.addressof(tot), int(reset)))
-        kinds = ("bulk", "surface", "source", "recv")
+        kinds = ("bulk_s0", "bulk_s1", "bulk_s2", "bulk_s3", "surface", "source", "recv")
         out = {k: (float(ms[n]), int(cnt[n])) for n, k in enumerate(kinds)}
+        out["bulk"] = (float(ms[:4].sum()), int(cnt[:4].sum()))
         out["launches"] = int(tot.value)
         return out
 

@@ -126,13 +126,14 @@ struct cgfd_problem {
   bool graph_ok[8] = {};
   int graph_launches[8] = {};
 
-  // per-kernel CUDA-event timing (direct launches only): kind 0 bulk, 1 surface, 2 source, 3 recv
+  // per-kernel CUDA-event timing (direct launches only): kinds 0-3 bulk stage 0..3,
+  // 4 surface slab, 5 source, 6 stations
   bool timing = false;
   std::vector<cudaEvent_t> ev_free;
   struct TimedLaunch { int kind; cudaEvent_t a, b; };
   std::vector<TimedLaunch> pending;
-  double t_ms[4] = {0, 0, 0, 0};
-  long long t_n[4] = {0, 0, 0, 0};
+  double t_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  long long t_n[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   long long launches = 0;
 
   cudaEvent_t get_event() {
@@ -220,7 +221,7 @@ struct cgfd_problem {
       cgfd::RecvP r;
       r.nsta = rec.n; r.nt_total = nt_total; r.idx8 = d_idx8; r.w8 = d_w8;
       r.pre = wbuf[step & 1]; r.sf = sf; r.seis = d_seis; r.d_it = d_it; r.d_flag = d_flag;
-      n += timed(3, [&] { return cgfd::launch_recv(r, st); });
+      n += timed(6, [&] { return cgfd::launch_recv(r, st); });
     }
     for (int s = 0; s < 4; s++) {
       cgfd::StageP p = stage_params(step, s);
@@ -232,11 +233,11 @@ struct cgfd_problem {
         tm.pre = map_ctr[pre];
         tm.end = map_ctr[end];
         tm.coef = map_coef;
-        n += timed(0, [&] { return cgfd::launch_stage_bulk_tma(med, p, tm, nzc, st); });
+        n += timed(s, [&] { return cgfd::launch_stage_bulk_tma(med, p, tm, nzc, st); });
       } else {
-        n += timed(0, [&] { return cgfd::launch_stage_bulk(med, p, nzc, st); });
+        n += timed(s, [&] { return cgfd::launch_stage_bulk(med, p, nzc, st); });
       }
-      n += timed(1, [&] { return cgfd::launch_stage_surface(med, p, st); });
+      n += timed(4, [&] { return cgfd::launch_stage_surface(med, p, st); });
       if (src.nsrc > 0) {
         cgfd::SrcP q;
         q.nsrc = src.nsrc; q.max_ext = src.max_ext; q.max_nt = src.max_nt;
@@ -245,7 +246,7 @@ struct cgfd_problem {
         q.it_begin = d_it_begin; q.ext_num = d_ext_num; q.ext_idx = d_ext_idx;
         q.ext_wv = d_ext_wv; q.ext_wt = d_ext_wt; q.stf = d_stf;
         q.tmp_out = p.tmp_out; q.end = p.end; q.sf = sf; q.d_it = d_it;
-        n += timed(2, [&] { return cgfd::launch_source(q, st); });
+        n += timed(5, [&] { return cgfd::launch_source(q, st); });
       }
     }
     n += cgfd::launch_advance(d_it, st);
@@ -333,14 +334,12 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d) {
   p->sz = p->sx * (p->nj + 6);
   p->sf = ((p->sz * (p->nk + 6) + 63) / 64) * 64;
   p->off0 = 3 * p->sz + 3 * p->sx + cgfd::GX;
-  // launch shape: enough z chunks to fill 148 SMs x 2 blocks a few times over
+  // z planes per bulk block: ~32 keeps the per-chunk prologue (3 planes) small and gives
+  // enough blocks to fill 148 SMs many times over (cgfd_set_zchunk / the autotuner refine it)
   {
     int nbulk = p->free_top ? p->nk - cgfd::NSURF : p->nk;
-    long long tiles = (long long)((p->ni + cgfd::TX - 1) / cgfd::TX) * ((p->nj + cgfd::TY - 1) / cgfd::TY);
-    long long want = 148 * 2 * 4;
-    int chunks = (int)std::max<long long>(1, std::min<long long>((want + tiles - 1) / tiles, std::max(1, nbulk / 12)));
+    int chunks = std::max(1, (nbulk + 31) / 32);
     p->nzc = (nbulk + chunks - 1) / chunks;
-    if (p->nzc < 1) p->nzc = 1;
   }
 
   size_t &B = p->bytes;
@@ -607,17 +606,15 @@ int cgfd_set_timing(cgfd_problem *p, int on) {
   return CGFD_OK;
 }
 
-/* ms[4], count[4] accumulated since the last reset for kinds {bulk, surface, source, recv};
-   *launches = kernels launched by the library since the last reset. */
 int cgfd_get_timing(cgfd_problem *p, double *ms, long long *count, long long *launches, int reset) {
   if (!p) return CGFD_ERR_INVALID;
-  for (int k = 0; k < 4; k++) {
+  for (int k = 0; k < 8; k++) {
     if (ms) ms[k] = p->t_ms[k];
     if (count) count[k] = p->t_n[k];
   }
   if (launches) *launches = p->launches;
   if (reset) {
-    for (int k = 0; k < 4; k++) { p->t_ms[k] = 0; p->t_n[k] = 0; }
+    for (int k = 0; k < 8; k++) { p->t_ms[k] = 0; p->t_n[k] = 0; }
     p->launches = 0;
   }
   return CGFD_OK;

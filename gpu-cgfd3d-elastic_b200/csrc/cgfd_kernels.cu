@@ -183,7 +183,8 @@ __global__ void __launch_bounds__(128) k_stage_surface(const __grid_constant__ S
   const long long offs[3] = {1, p.sx, p.sz};
   const int nk2 = p.nk - 1;
 
-  for (int k = p.nbulk; k < p.nk; k++) {
+  {
+    const int k = p.nbulk + blockIdx.z;  // one thread per cell of the slab
     const long long id = didx(p, i, j, k);
     float m[3][3];
 #pragma unroll
@@ -417,7 +418,7 @@ int launch_stage_bulk(int med, const StageP &p, int nzc, cudaStream_t st) {
 int launch_stage_surface(int med, const StageP &p, cudaStream_t st) {
   if (p.nbulk >= p.nk) return 0;
   dim3 block(32, 4);
-  dim3 grid((p.ni + 31) / 32, (p.nj + 3) / 4);
+  dim3 grid((p.ni + 31) / 32, (p.nj + 3) / 4, p.nk - p.nbulk);
   if (med == MED_ISO) k_stage_surface<MED_ISO><<<grid, block, 0, st>>>(p);
   else if (med == MED_VTI) k_stage_surface<MED_VTI><<<grid, block, 0, st>>>(p);
   else k_stage_surface<MED_ANISO><<<grid, block, 0, st>>>(p);

@@ -209,9 +209,9 @@ int cgfd_set_bulk_variant(cgfd_problem *p, int tma);
 int cgfd_set_timing(cgfd_problem *p, int on);
 
 /*
- * Accumulated kernel times (ms[4]) and launch counts (count[4]) for the kernel kinds
- * {bulk stage, surface-slab stage, source, station}, and the number of kernels the library
- * launched (*launches); reset != 0 clears them.
+ * Accumulated kernel times (ms[8]) and launch counts (count[8]) for the kernel kinds
+ * {bulk stage of RK stage 0, 1, 2, 3, surface slab, source, stations, unused}, and the
+ * number of kernels the library launched (*launches); reset != 0 clears them.
  */
 int cgfd_get_timing(cgfd_problem *p, double *ms, long long *count, long long *launches, int reset);
 
