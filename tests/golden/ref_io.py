@@ -1,0 +1,43 @@
+"""I/O with the reference harness (oracle/_ref/ref_harness): writes a Problem in the
+reference's input formats and reads back the reference's outputs. Test infrastructure."""
+import os
+import subprocess
+
+import numpy as np
+
+from cgfd_b200 import formats
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+
+
+def write_inputs(p, d, nsteps):
+    os.makedirs(d, exist_ok=True)
+    with open(os.path.join(d, "params.txt"), "w") as f:
+        f.write(f"{p.ni} {p.nj} {p.nk} {p.medium_type} {p.nt_total} {nsteps} {int(p.free_top)} {p.dt:.9g} {p.t0:.9g}\n")
+        for a in range(3):
+            for s in range(2):
+                fc = p.pml[a][s]
+                if fc:
+                    f.write(f"1 {fc['num_layers']} {fc['alpha_max']:.9g} {fc['beta_max']:.9g} {fc['ref_vel']:.9g}\n")
+                else:
+                    f.write("0 0 0 0 0\n")
+    np.ascontiguousarray(p.coord, np.float32).tofile(os.path.join(d, "coord.bin"))
+    np.ascontiguousarray(p.medium, np.float32).tofile(os.path.join(d, "medium.bin"))
+    formats.write_src(os.path.join(d, "src.src"), p.src)
+    formats.write_station_list(os.path.join(d, "station.list"), p.sta)
+
+
+def run(p, d, nsteps, timeout=600):
+    write_inputs(p, d, nsteps)
+    r = subprocess.run([HARNESS, d], capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"ref_harness failed ({r.returncode}): {r.stderr[-2000:]}")
+    shp = (p.nk + 6, p.nj + 6, p.ni + 6)
+    info = dict(ln.split() for ln in open(os.path.join(d, "ref_info.txt")))
+    nrecv = int(info["nrecv"])
+    seis = np.fromfile(os.path.join(d, "ref_seismo.bin"), np.float32).reshape(nrecv, 9, p.nt_total)
+    wave = np.fromfile(os.path.join(d, "ref_wave.bin"), np.float32).reshape((9,) + shp)
+    metric = np.fromfile(os.path.join(d, "ref_metric.bin"), np.float32).reshape((10,) + shp)
+    return {"seismo": seis, "wave": wave, "metric": metric, "loop_ms": float(info["loop_ms"]),
+            "cell_stages": int(info["cell_stages"]), "nsrc": int(info["nsrc"])}

@@ -38,9 +38,14 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / den) if den > 0 else float(np.linalg.norm(a - b))
 
 
-def per_station_rel_l2(s, ref):
-    """max over stations of the relative L2 of the 9-component seismogram."""
-    out = []
-    for n in range(ref.shape[0]):
-        out.append(rel_l2(s[n], ref[n]))
-    return max(out) if out else 0.0
+def per_station_rel_l2(s, ref, floor=1e-3):
+    """max over stations of the relative L2 of the 9-component seismogram. The denominator
+    is floored at `floor` x the largest station norm so that a station the wave has not
+    reached yet (signal at rounding level) does not turn rounding noise into a large ratio."""
+    s = np.asarray(s, np.float64)
+    ref = np.asarray(ref, np.float64)
+    norms = [np.linalg.norm(ref[n]) for n in range(ref.shape[0])]
+    if not norms:
+        return 0.0
+    top = max(norms)
+    return max(float(np.linalg.norm(s[n] - ref[n]) / max(norms[n], floor * top, 1e-300)) for n in range(ref.shape[0]))

@@ -1,0 +1,52 @@
+"""Parity against the reference's OWN solver code run on the same GPU (oracle/_ref/ref_harness):
+pins the CPU oracle and checks the product. Tolerances (per-station relative L2, denominator
+floored at 1e-3 of the strongest station): oracle vs reference <= 2e-5 (same FP32 arithmetic,
+FMA contraction differs); product vs reference <= 1e-4."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from cgfd_b200 import Simulation
+from oracle.oracle import Oracle, metric_fp32
+from golden import ref_io
+from golden.cases import golden_problem
+from helpers import small_problem, per_station_rel_l2, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+needs_harness = pytest.mark.skipif(not os.path.exists(ref_io.HARNESS), reason="oracle/_ref/ref_harness not built")
+
+
+@needs_harness
+@pytest.mark.parametrize("name", ["iso_small", "vti_small", "aniso_small"])
+def test_oracle_and_product_match_reference(name):
+    p, nsteps = golden_problem(name)
+    with tempfile.TemporaryDirectory() as d:
+        ref = ref_io.run(p, d, nsteps)
+    # the reference's FP32 metrics equal the oracle's restatement of gd_curv_metric_cal
+    m_orc = metric_fp32(p.coord)
+    assert rel_l2(m_orc[:, 3:-3, 3:-3, 3:-3], ref["metric"][:, 3:-3, 3:-3, 3:-3]) < 1e-6
+    p.metric = ref["metric"]
+    orc = Oracle(p)
+    orc.run(nsteps)
+    sim = Simulation(p)
+    sim.run(nsteps)
+    rs = ref["seismo"][:, :, :nsteps]
+    assert rs.shape[0] == 9 and np.abs(rs).max() > 0
+    assert per_station_rel_l2(orc.seismograms()[:, :, :nsteps], rs) <= 2e-5
+    assert per_station_rel_l2(sim.seismograms()[:, :, :nsteps], rs) <= 1e-4
+    assert rel_l2(orc.wavefield(), ref["wave"]) <= 2e-5
+    assert rel_l2(sim.wavefield(), ref["wave"]) <= 1e-4
+
+
+@needs_harness
+def test_reference_kernels_timing_recorded():
+    """The reference's kernels run on this GPU: records Gcell-stage/s for the comparison."""
+    p = small_problem("iso", ni=96, nj=96, nk=64, nsteps=20, npml=8)
+    with tempfile.TemporaryDirectory() as d:
+        ref = ref_io.run(p, d, 20)
+    rate = ref["cell_stages"] / (ref["loop_ms"] * 1e-3) / 1e9
+    print(f"reference kernels: {rate:.3f} Gcell-stage/s on 96x96x64")
+    assert rate > 0
