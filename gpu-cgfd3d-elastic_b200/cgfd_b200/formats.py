@@ -68,14 +68,20 @@ def read_src(path) -> Sources:
         wav = np.zeros(n, np.int32)
         coefs = np.zeros((n, 10), np.float32)
         cmp = np.zeros((n, 9), np.float32)
+        # sscanf semantics of src_t.cu:491-507: values missing on a line keep what the previous
+        # source left in the same variables (0 before the first source)
+        prev_c = np.zeros(10, np.float32)
+        prev = np.zeros(9, np.float32)
         for s in range(n):
             w = next(it).split()
             t_start[s] = float(w[0])
             wav[s] = WAVELETS[w[1]]
             c = [float(x) for x in w[2:12]]
-            coefs[s, :len(c)] = c
-            v = [float(x) for x in next(it).split()]
-            cmp[s, sl] = v[: sl.stop - sl.start]
+            prev_c[:len(c)] = c
+            coefs[s] = prev_c
+            v = [float(x) for x in next(it).split()][: sl.stop - sl.start]
+            prev[sl.start:sl.start + len(v)] = v
+            cmp[s] = prev
         return Sources(loc=loc, t_start=t_start, wavelet=wav, wavelet_coefs=coefs, cmp=cmp, stf_given=0,
                        stf_length=stf_length, cmp_type=cmp_type, mechanism_type=mech, loc_coord_type=loc_coord,
                        loc_3dim=loc_3dim)
