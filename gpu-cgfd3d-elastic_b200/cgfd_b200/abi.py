@@ -200,6 +200,7 @@ def lib():
         "cgfd_set_step": (C.c_int, [P, C.c_int]),
         "cgfd_get_seismograms": (C.c_int, [P, P]),
         "cgfd_num_stations": (C.c_int, [P]),
+        "cgfd_station_info": (C.c_int, [P, P, P]),
         "cgfd_get_wavefield": (C.c_int, [P, P]),
         "cgfd_set_wavefield": (C.c_int, [P, P]),
         "cgfd_device_bytes": (C.c_size_t, [P]),

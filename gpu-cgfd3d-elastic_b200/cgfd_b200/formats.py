@@ -119,3 +119,91 @@ def read_station_list(path) -> Stations:
         loc.append([float(x) for x in w[3:6]])
     return Stations(loc=np.array(loc, np.float32), flag_depth=np.array(fd, np.int32),
                     flag_coord=np.array(fc, np.int32), names=names)
+
+
+# ---------------------------------------------------------------------------------------
+# Reference-format input sets and SAC files
+# ---------------------------------------------------------------------------------------
+def _write_nc(path, names, fields, ni, nj, nk, version=2):
+    """Physical points of reference-layout fields as float variables (k, j, i), with the
+    global attributes of gd_curv_coord_export (gd_t.cu:636-726). Uses scipy's NetCDF classic
+    writer, an implementation independent of the library's reader."""
+    from scipy.io import netcdf_file
+    f = netcdf_file(path, "w", version=version)
+    f.createDimension("i", ni)
+    f.createDimension("j", nj)
+    f.createDimension("k", nk)
+    for n, fld in zip(names, fields):
+        v = f.createVariable(n, "f4", ("k", "j", "i"))
+        v[:] = np.ascontiguousarray(fld[3:-3, 3:-3, 3:-3], np.float32)
+    setattr(f, "global_index_of_first_physical_points", np.array([0, 0, 0], np.int32))
+    setattr(f, "count_of_physical_points", np.array([ni, nj, nk], np.int32))
+    f.close()
+
+
+MEDIUM_NAMES = {
+    2: ["rho", "lambda", "mu"],
+    3: ["rho", "c11", "c13", "c33", "c55", "c66"],
+    4: ["rho"] + [f"c{a}{b}" for a in range(1, 7) for b in range(a, 7)],
+}
+MEDIUM_TYPES = {2: "elastic_iso", 3: "elastic_vti", 4: "elastic_aniso"}
+
+
+def write_case(d, p, nsteps, metric="calculate", check_stability=1):
+    """Writes a full reference-format input set for problem `p` into directory `d`:
+    par.json, grid/coord_px0_py0_pz0.nc, media/media_px0_py0_pz0.nc, src.src, station.list
+    (and grid/metric_px0_py0_pz0.nc when metric == "import"). Returns the par.json path."""
+    import json
+    import os
+    os.makedirs(os.path.join(d, "grid"), exist_ok=True)
+    os.makedirs(os.path.join(d, "media"), exist_ok=True)
+    _write_nc(os.path.join(d, "grid", "coord_px0_py0_pz0.nc"), ["x", "y", "z"], p.coord, p.ni, p.nj, p.nk)
+    if metric == "import":
+        _write_nc(os.path.join(d, "grid", "metric_px0_py0_pz0.nc"),
+                  ["jac", "xi_x", "xi_y", "xi_z", "eta_x", "eta_y", "eta_z", "zeta_x", "zeta_y", "zeta_z"],
+                  p.metric, p.ni, p.nj, p.nk)
+    _write_nc(os.path.join(d, "media", "media_px0_py0_pz0.nc"), MEDIUM_NAMES[p.medium_type], p.medium,
+              p.ni, p.nj, p.nk)
+    write_src(os.path.join(d, "src.src"), p.src)
+    write_station_list(os.path.join(d, "station.list"), p.sta)
+    names = [["boundary_x_left", "boundary_x_right"], ["boundary_y_front", "boundary_y_back"],
+             ["boundary_z_bottom", "boundary_z_top"]]
+    par = {
+        "number_of_total_grid_points_x": p.ni, "number_of_total_grid_points_y": p.nj,
+        "number_of_total_grid_points_z": p.nk, "number_of_mpiprocs_x": 1, "number_of_mpiprocs_y": 1,
+        "size_of_time_step": float(p.dt), "number_of_time_steps": int(nsteps), "check_stability": check_stability,
+        "grid_generation_method": {"import": os.path.join(d, "grid")},
+        "metric_calculation_method": ({"import": os.path.join(d, "grid")} if metric == "import" else {"calculate": 1}),
+        "medium": {"type": MEDIUM_TYPES[p.medium_type], "input_way": "import",
+                   "import": os.path.join(d, "media"), "#code": "func_name_here"},
+        "in_source_file": os.path.join(d, "src.src"),
+        "in_station_file": os.path.join(d, "station.list"),
+        "output_dir": os.path.join(d, "output"),
+        "check_nan_every_nummber_of_steps": 0, "output_all": 0,
+    }
+    for a in range(3):
+        for s in range(2):
+            f = p.pml[a][s]
+            if f:
+                par[names[a][s]] = {"cfspml": {"number_of_layers": f["num_layers"], "alpha_max": f["alpha_max"],
+                                               "beta_max": f["beta_max"], "ref_vel": f["ref_vel"]}}
+    if p.free_top:
+        par["boundary_z_top"] = {"free": "timg"}
+    path = os.path.join(d, "par.json")
+    with open(path, "w") as f:
+        json.dump(par, f, indent=2)
+    return path
+
+
+def read_sac(path):
+    """(header dict, data) of a SAC file written little-endian (the reference's native order)."""
+    raw = open(path, "rb").read()
+    fh = np.frombuffer(raw[:280], "<f4")
+    ih = np.frombuffer(raw[280:440], "<i4")
+    ch = raw[440:632]
+    hdr = {"delta": float(fh[0]), "b": float(fh[5]), "e": float(fh[6]), "stla": float(fh[31]),
+           "stlo": float(fh[32]), "stel": float(fh[33]), "stdp": float(fh[34]), "evla": float(fh[35]),
+           "nvhdr": int(ih[6]), "npts": int(ih[9]), "iftype": int(ih[15]), "leven": int(ih[35]),
+           "kstnm": ch[0:8], "kcmpnm": ch[160:168], "depmin": float(fh[1])}
+    data = np.frombuffer(raw[632:632 + 4 * hdr["npts"]], "<f4").copy()
+    return hdr, data

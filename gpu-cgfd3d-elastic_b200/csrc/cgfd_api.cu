@@ -527,6 +527,15 @@ int cgfd_set_step(cgfd_problem *p, int it) {
 
 int cgfd_num_stations(const cgfd_problem *p) { return p ? p->rec.n : -1; }
 
+int cgfd_station_info(const cgfd_problem *p, int *input_index, int *ijk) {
+  if (!p) { set_err("problem is NULL"); return CGFD_ERR_INVALID; }
+  for (int r = 0; r < p->rec.n; r++) {
+    if (input_index) input_index[r] = p->rec.input_index[r];
+    if (ijk) { ijk[3 * r] = p->rec.i[r]; ijk[3 * r + 1] = p->rec.j[r]; ijk[3 * r + 2] = p->rec.k[r]; }
+  }
+  return CGFD_OK;
+}
+
 int cgfd_get_seismograms(cgfd_problem *p, float *out) {
   if (!p || !out) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
   return guarded([&] {

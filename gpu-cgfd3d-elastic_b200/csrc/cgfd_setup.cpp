@@ -415,6 +415,7 @@ void recv_setup(const cgfd_problem_desc *d, RecvHost &r) {
     double dx = c[0] - ix, dy = c[1] - iy, dz = c[2] - iz;
     if (!(ix >= 0 && ix <= d->ni - 1 && iy >= 0 && iy <= d->nj - 1 && iz >= 0 && iz <= d->nk - 1)) continue;
     r.i.push_back(ix); r.j.push_back(iy); r.k.push_back(iz);
+    r.input_index.push_back(ir);
     double x1 = 1.0 - dx, y1 = 1.0 - dy, z1 = 1.0 - dz;
     double w[8] = {x1 * y1 * z1, dx * y1 * z1, x1 * dy * z1, dx * dy * z1,
                    0.0, x1 * y1 * dz + dx * y1 * dz, x1 * dy * dz, dx * dy * dz};

@@ -53,6 +53,7 @@ void src_setup(const cgfd_problem_desc *d, SrcHost &s);
 struct RecvHost {
   int n = 0;
   std::vector<int> i, j, k;               // corner 0, physical indices
+  std::vector<int> input_index;           // position in the station list
   std::vector<float> w8;                  // [n][8]
 };
 void recv_setup(const cgfd_problem_desc *d, RecvHost &r);

@@ -1,0 +1,286 @@
+// cgfd3d_b200.cpp -- drop-in command line driver: `cgfd3d_b200 <par.json> <gpu_id>`.
+//
+// Reproduces the observable behaviour of the reference's main (main_curv_col_el_3d.cu:22-853)
+// for the elastic time-loop path on one GPU: reads the same parameter file keys, grid /
+// metric / medium NetCDF files, .src source file and station list, checks the time step
+// (FP64), runs the B200 time loop through the C ABI and writes the same SAC files
+// (<output_dir>/<station>.<Vx..Txy>.sac, plus <station>.E**.sac strain for isotropic media).
+// Options outside this path (MPI decomposition, media discretisation, slices, ablexp,
+// acoustic / visco-elastic media) are rejected with a message.
+#include <sys/stat.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "cgfd_b200.h"
+#include "io/json.h"
+#include "io/ncclassic.h"
+#include "io/textfmt.h"
+
+using cgfd::json::Value;
+
+namespace {
+
+const char *kFnamePart = "px0_py0_pz0";  // blk_set_output (blk_t.cu:54) for one rank
+const char *kCmpNames[9] = {"Vx", "Vy", "Vz", "Txx", "Tyy", "Tzz", "Tyz", "Txz", "Txy"};
+
+[[noreturn]] void fail(const std::string &m) { throw std::runtime_error(m); }
+
+const Value &need(const Value &o, const char *key) {
+  const Value *v = o.get(key);
+  if (!v) fail(std::string("missing key '") + key + "'");
+  return *v;
+}
+
+struct Grid {
+  int ni, nj, nk;
+  size_t nx, ny, nz, siz;
+  size_t at(int i, int j, int k) const { return (size_t)(i + 3) + (size_t)(j + 3) * nx + (size_t)(k + 3) * nx * ny; }
+};
+
+// physical-point float variable [nk][nj][ni] -> reference layout field (ghosts untouched)
+void put_physical(const Grid &g, const std::vector<float> &v, float *field) {
+  if (v.size() != (size_t)g.ni * g.nj * g.nk) fail("variable size does not match the grid");
+  size_t n = 0;
+  for (int k = 0; k < g.nk; k++)
+    for (int j = 0; j < g.nj; j++)
+      for (int i = 0; i < g.ni; i++) field[g.at(i, j, k)] = v[n++];
+}
+
+void import_vars(const std::string &path, const Grid &g, const std::vector<std::string> &names, float *dst) {
+  cgfd::nc::File f = cgfd::nc::read_header(path);
+  for (size_t c = 0; c < names.size(); c++) {
+    std::vector<float> v = cgfd::nc::read_var(path, f, names[c]);
+    put_physical(g, v, dst + c * g.siz);
+  }
+}
+
+void mkdirs(const std::string &d) {
+  std::string cur;
+  for (size_t p = 0; p <= d.size(); p++) {
+    if (p == d.size() || d[p] == '/') {
+      if (!cur.empty()) mkdir(cur.c_str(), 0755);
+    }
+    if (p < d.size()) cur += d[p];
+  }
+}
+
+int run(int argc, char **argv) {
+  if (argc < 3) {
+    fprintf(stderr, "usage: cgfd3d_b200 <par_file> <gpu_id>\n");
+    return 1;
+  }
+  Value par = cgfd::json::parse_file(argv[1]);
+  int gpu = atoi(argv[2]);
+
+  Grid g;
+  g.ni = need(par, "number_of_total_grid_points_x").as_int();
+  g.nj = need(par, "number_of_total_grid_points_y").as_int();
+  g.nk = need(par, "number_of_total_grid_points_z").as_int();
+  g.nx = g.ni + 6; g.ny = g.nj + 6; g.nz = g.nk + 6;
+  g.siz = g.nx * g.ny * g.nz;
+  if (const Value *v = par.get("number_of_mpiprocs_x"))
+    if (v->as_int() != 1) fprintf(stderr, "note: number_of_mpiprocs_x ignored (one GPU, one block)\n");
+
+  // ---- time (par_t.cu:150-200)
+  double dt = -1.0, twin = -1.0, t0 = 0.0;
+  int nsteps = -1, check = 1;
+  if (const Value *v = par.get("size_of_time_step")) dt = v->as_num();
+  if (const Value *v = par.get("number_of_time_steps")) nsteps = v->as_int();
+  if (const Value *v = par.get("time_window_length")) twin = v->as_num();
+  if (const Value *v = par.get("time_start")) t0 = v->as_num();
+  if (const Value *v = par.get("check_stability")) check = v->as_int();
+  if (dt < 0.0 && twin < 0.0) fail("at least one of size_of_time_step / time_window_length must be > 0");
+  if (dt > 0.0) {
+    if (nsteps < 0 && twin < 0.0) fail("both number_of_time_steps and time_window_length are missing");
+    if (nsteps < 0) nsteps = (int)(twin / dt + 0.5);
+    twin = dt * nsteps;
+  }
+  int nt_total = nsteps + 1;
+
+  // ---- boundaries (par_t.cu:218-371)
+  cgfd_problem_desc d;
+  memset(&d, 0, sizeof(d));
+  const char *bnames[3][2] = {{"boundary_x_left", "boundary_x_right"},
+                              {"boundary_y_front", "boundary_y_back"},
+                              {"boundary_z_bottom", "boundary_z_top"}};
+  for (int a = 0; a < 3; a++)
+    for (int s = 0; s < 2; s++) {
+      const Value *b = par.get(bnames[a][s]);
+      if (!b) continue;
+      if (const Value *c = b->get("cfspml")) {
+        d.pml[a][s].enable = 1;
+        d.pml[a][s].num_layers = need(*c, "number_of_layers").as_int();
+        d.pml[a][s].alpha_max = (float)need(*c, "alpha_max").as_num();
+        d.pml[a][s].beta_max = (float)need(*c, "beta_max").as_num();
+        d.pml[a][s].ref_vel = (float)need(*c, "ref_vel").as_num();
+      }
+      if (b->get("ablexp")) fail(std::string(bnames[a][s]) + ": ablexp is not on this path (use cfspml)");
+      if (const Value *f = b->get("free")) {
+        if (!(a == 2 && s == 1)) fail("free surface is only implemented at the top");
+        if (f->as_str() != "timg") fail("free surface type must be \"timg\"");
+        d.free_top = 1;
+      }
+    }
+
+  // ---- grid (main:158-199)
+  std::vector<float> coord(3 * g.siz, 0.f);
+  const Value &gg = need(par, "grid_generation_method");
+  if (const Value *imp = gg.get("import")) {
+    std::string path = imp->as_str() + "/coord_" + kFnamePart + ".nc";
+    import_vars(path, g, {"x", "y", "z"}, coord.data());
+  } else if (const Value *cart = gg.get("cartesian")) {  // gd_curv_gen_cart, gd_t.cu:599-634
+    const Value &o = need(*cart, "origin"), &h = need(*cart, "inteval");
+    for (int k = -3; k < g.nk + 3; k++)
+      for (int j = -3; j < g.nj + 3; j++)
+        for (int i = -3; i < g.ni + 3; i++) {
+          size_t p = g.at(i, j, k);
+          coord[p] = (float)(o.arr.at(0).as_num() + i * h.arr.at(0).as_num());
+          coord[g.siz + p] = (float)(o.arr.at(1).as_num() + j * h.arr.at(1).as_num());
+          coord[2 * g.siz + p] = (float)(o.arr.at(2).as_num() + k * h.arr.at(2).as_num());
+        }
+  } else {
+    fail("grid_generation_method must be import or cartesian");
+  }
+  if (gg.get("import") && cgfd_fill_ghosts(g.ni, g.nj, g.nk, 3, coord.data())) fail(cgfd_last_error());
+
+  // ---- metrics (main:201-228)
+  std::vector<float> metric(10 * g.siz, 0.f);
+  const Value &mm = need(par, "metric_calculation_method");
+  if (const Value *imp = mm.get("import")) {
+    std::string path = imp->as_str() + "/metric_" + kFnamePart + ".nc";
+    import_vars(path, g, {"jac", "xi_x", "xi_y", "xi_z", "eta_x", "eta_y", "eta_z", "zeta_x", "zeta_y", "zeta_z"},
+                metric.data());
+    cgfd_fill_ghosts(g.ni, g.nj, g.nk, 10, metric.data());
+  } else {
+    if (cgfd_metric_calc(g.ni, g.nj, g.nk, coord.data(), metric.data())) fail(cgfd_last_error());
+  }
+
+  // ---- medium (par_t.cu:428-721, md_import md_t.cu:269-326)
+  const Value &md = need(par, "medium");
+  std::string type = need(md, "type").as_str();
+  std::vector<std::string> mnames;
+  if (type == "elastic_iso") { d.medium_type = CGFD_MEDIUM_ELASTIC_ISO; mnames = {"rho", "lambda", "mu"}; }
+  else if (type == "elastic_vti") { d.medium_type = CGFD_MEDIUM_ELASTIC_VTI; mnames = {"rho", "c11", "c13", "c33", "c55", "c66"}; }
+  else if (type == "elastic_aniso") {
+    d.medium_type = CGFD_MEDIUM_ELASTIC_ANISO;
+    mnames = {"rho"};
+    for (int a = 1; a <= 6; a++)
+      for (int b = a; b <= 6; b++) mnames.push_back("c" + std::to_string(a) + std::to_string(b));
+  } else fail("medium type '" + type + "' is not on this path (elastic_iso/vti/aniso)");
+  std::string way = need(md, "input_way").as_str();
+  if (way != "import") fail("medium input_way '" + way + "' is not on this path (import media_*.nc)");
+  std::vector<float> medium(mnames.size() * g.siz, 0.f);
+  import_vars(need(md, "import").as_str() + "/media_" + kFnamePart + ".nc", g, mnames, medium.data());
+
+  d.ni = g.ni; d.nj = g.nj; d.nk = g.nk;
+  d.coord = coord.data();
+  d.metric = metric.data();
+  d.medium = medium.data();
+
+  // ---- dt check in FP64 (main:591-648)
+  if (check == 1) {
+    double dtmax = 0.0;
+    if (cgfd_dt_estimate(&d, 1.3, &dtmax)) fail(cgfd_last_error());
+    printf("maximum allowed time step = %g\n", dtmax);
+    if (dtmax <= 0.0) fail("maximum dt <= 0");
+    if (dt < 0.0) {
+      dt = cgfd_keep_three_digits(dtmax);
+      nt_total = (int)(twin / dt + 0.5);  // main:621 (no +1 in this branch)
+      printf("-> set dt = %g, nt_total = %d\n", dt, nt_total);
+    }
+    if (dtmax < dt) fail("dt = " + std::to_string(dt) + " > dtmax = " + std::to_string(dtmax));
+  }
+  if (dt <= 0.0) fail("no time step");
+  d.dt = (float)dt;
+  d.t0 = (float)t0;
+  d.nt_total = nt_total;
+
+  // ---- sources and stations
+  cgfd::fmt::SourceFile sf = cgfd::fmt::read_source_file(need(par, "in_source_file").as_str());
+  d.src = sf.desc();
+  cgfd::fmt::StationFile stf;
+  bool have_sta = par.get("in_station_file") != nullptr;
+  if (have_sta) {
+    stf = cgfd::fmt::read_station_file(par.get("in_station_file")->as_str());
+    d.sta = stf.desc();
+  }
+  std::string out = par.get("output_dir") ? par.get("output_dir")->as_str() : std::string(".");
+  mkdirs(out);
+  d.precision = CGFD_PREC_FP32;
+  d.device = gpu;
+
+  // ---- run
+  cgfd_problem *p = nullptr;
+  if (cgfd_problem_create(&d, &p)) fail(std::string("create: ") + cgfd_last_error());
+  printf("grid %d x %d x %d, dt %g, nt_total %d, device %.2f GB\n", g.ni, g.nj, g.nk, dt, nt_total,
+         cgfd_device_bytes(p) / 1e9);
+  int step = 0;
+  while (step < nt_total) {
+    int n = std::min(100, nt_total - step);
+    int rc = cgfd_run(p, n);
+    if (rc) { std::string m = cgfd_last_error(); cgfd_problem_destroy(p); fail("run: " + m); }
+    step += n;
+    printf("-> it=%d\n", step);
+    fflush(stdout);
+  }
+
+  // ---- SAC output (io_recv_output_sac, io_funcs.cu:1775-1902)
+  int nsta = cgfd_num_stations(p);
+  std::vector<float> seis((size_t)std::max(nsta, 0) * 9 * nt_total);
+  std::vector<int> idx(std::max(nsta, 1)), ijk(3 * std::max(nsta, 1));
+  if (nsta > 0) {
+    cgfd_get_seismograms(p, seis.data());
+    cgfd_station_info(p, idx.data(), ijk.data());
+  }
+  cgfd_problem_destroy(p);
+  for (int r = 0; r < nsta; r++) {
+    size_t c0 = g.at(ijk[3 * r], ijk[3 * r + 1], ijk[3 * r + 2]);
+    float x = coord[c0], y = coord[g.siz + c0], z = coord[2 * g.siz + c0];
+    const std::string &name = stf.names[idx[r]];
+    float *tr = &seis[(size_t)r * 9 * nt_total];
+    for (int c = 0; c < 9; c++)
+      cgfd::fmt::write_sac(out + "/" + name + "." + kCmpNames[c] + ".sac", tr + (size_t)c * nt_total, nt_total,
+                           (float)dt, x, y, z, (float)dt);
+    if (d.medium_type == CGFD_MEDIUM_ELASTIC_ISO) {
+      // strain from stress in place (io_recv_output_sac_el_iso_strain, io_funcs.cu:1821-1902)
+      float lam = medium[g.siz + c0], mu = medium[2 * g.siz + c0];
+      float E1 = (float)((lam + mu) / (mu * (3.0 * lam + 2.0 * mu)));
+      float E2 = (float)(-lam / (2.0 * mu * (3.0 * lam + 2.0 * mu)));
+      float E3 = (float)(1.0 / mu);
+      float *T[6];
+      for (int c = 0; c < 6; c++) T[c] = tr + (size_t)(3 + c) * nt_total;
+      for (int t = 0; t < nt_total; t++) {
+        float E0 = E2 * (T[0][t] + T[1][t] + T[2][t]);
+        T[0][t] = E0 - (E2 - E1) * T[0][t];
+        T[1][t] = E0 - (E2 - E1) * T[1][t];
+        T[2][t] = E0 - (E2 - E1) * T[2][t];
+        T[3][t] = 0.5f * E3 * T[3][t];
+        T[4][t] = 0.5f * E3 * T[4][t];
+        T[5][t] = 0.5f * E3 * T[5][t];
+      }
+      const char *en[6] = {"Exx", "Eyy", "Ezz", "Eyz", "Exz", "Exy"};
+      for (int c = 0; c < 6; c++)
+        cgfd::fmt::write_sac(out + "/" + name + "." + en[c] + ".sac", T[c], nt_total, (float)dt, x, y, z, (float)dt);
+    }
+  }
+  printf("wrote %d stations to %s\n", nsta, out.c_str());
+  return 0;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+  try {
+    return run(argc, argv);
+  } catch (std::exception &e) {
+    fprintf(stderr, "cgfd3d_b200: %s\n", e.what());
+    return 1;
+  }
+}

@@ -1,0 +1,40 @@
+// textfmt.h -- the reference's text inputs (.src source file, station list) and the SAC
+// seismogram output, for the drop-in CLI.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "cgfd_b200.h"
+
+namespace cgfd {
+namespace fmt {
+
+// Parsed .src file (src_t.cu:205-611); desc() points into the owned arrays.
+struct SourceFile {
+  std::string evtnm;
+  cgfd_source_desc d{};
+  std::vector<float> loc, t_start, coefs, cmp, cmp_values;
+  std::vector<int> wavelet;
+  const cgfd_source_desc &desc();
+};
+SourceFile read_source_file(const std::string &path);
+
+// Parsed station list (io_funcs.cu:52-80).
+struct StationFile {
+  std::vector<std::string> names;
+  std::vector<int> flag_coord, flag_depth;
+  std::vector<float> loc;
+  cgfd_station_desc d{};
+  const cgfd_station_desc &desc();
+};
+StationFile read_station_file(const std::string &path);
+
+// One-component SAC file with the header fields the reference sets (sacLib.cu:8-100):
+// delta, b = 0, e = delta*(npts-1), npts, nvhdr = 6, iftype = ITIME, leven = 1, station
+// and event positions; every other field "undefined" (-12345).
+void write_sac(const std::string &path, const float *data, int npts, float delta, float stla, float stlo,
+               float stel, float stdp, float evla = 0.f, float evlo = 0.f, float evel = 0.f, float evdp = 0.f);
+
+}  // namespace fmt
+}  // namespace cgfd

@@ -166,6 +166,13 @@ int cgfd_get_seismograms(cgfd_problem *p, float *out);
 int cgfd_num_stations(const cgfd_problem *p);
 
 /*
+ * For each located station (seismogram order): its position in the input list
+ * (input_index[nsta], may be NULL) and the physical 0-based grid index of its interpolation
+ * corner 0 (ijk[nsta][3], may be NULL). Replaces: iorecv->recvone[r].i/j/k (io_funcs.cu:250-260).
+ */
+int cgfd_station_info(const cgfd_problem *p, int *input_index, int *ijk);
+
+/*
  * Current wavefield w_pre in the reference layout [9][nz][ny][nx] (ghosts are 0), e.g.
  * for a final snapshot. Replaces: the device-to-host copy of io_snap_nc_put.
  */

@@ -1,0 +1,60 @@
+"""The drop-in CLI on CPU: reads par.json, NetCDF grid/media (written by scipy, an independent
+NetCDF implementation), .src and station list, checks dt in FP64 - then stops at device
+creation because there is no GPU here."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from cgfd_b200 import formats, synth
+from helpers import small_problem
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "gpu-cgfd3d-elastic_b200", "_build", "cgfd3d_b200")
+
+
+def gpu_available():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the CPU-side stages only")
+@pytest.mark.parametrize("medium", ["iso", "vti", "aniso"])
+def test_cli_reads_reference_formats(tmp_path, medium):
+    p = small_problem(medium, nsteps=4)
+    par = formats.write_case(str(tmp_path), p, 4)
+    r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1
+    m = re.search(r"maximum allowed time step = ([0-9.eE+-]+)", r.stdout)
+    assert m, r.stdout + r.stderr
+    assert float(m.group(1)) == pytest.approx(synth.dt_estimate(p), rel=1e-5)
+    assert "create:" in r.stderr  # reached the device stage
+
+
+def test_cli_rejects_off_path_options(tmp_path):
+    p = small_problem("iso", nsteps=2)
+    par = formats.write_case(str(tmp_path), p, 2)
+    import json
+    cfg = json.load(open(par))
+    cfg["medium"]["input_way"] = "infile_layer"
+    json.dump(cfg, open(par, "w"))
+    r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "not on this path" in r.stderr
+    cfg["medium"]["input_way"] = "import"
+    cfg["boundary_x_left"] = {"ablexp": {"number_of_layers": 10}}
+    json.dump(cfg, open(par, "w"))
+    r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "ablexp" in r.stderr
+
+
+def test_cli_dt_check_rejects_unstable_step(tmp_path):
+    p = small_problem("iso", nsteps=2)
+    p.dt = 1.0
+    par = formats.write_case(str(tmp_path), p, 2)
+    r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "> dtmax" in r.stderr
