@@ -153,7 +153,8 @@ void write_sac(const std::string &path, const float *data, int npts, float delta
   char ch[192];
   for (float &x : fh) x = -12345.0f;
   for (int &x : ih) x = -12345;
-  for (int q = 0; q < 24; q++) {
+  // 23 text fields: kstnm(8) kevnm(16) and 21 more of 8 bytes
+  for (int q = 0; q < 23; q++) {
     int len = q == 1 ? 16 : 8;
     int off = q == 0 ? 0 : (q == 1 ? 8 : 24 + (q - 2) * 8);
     memset(ch + off, 0, len);
