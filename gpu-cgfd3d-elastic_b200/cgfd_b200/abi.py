@@ -135,6 +135,13 @@ class Problem:
             keep.append(a)
             return a
 
+        d = self._desc_no_src(arr)
+        if self.src is not None and self.src.num > 0:
+            _fill_src(d.src, self.src, arr)
+        d._keep = keep
+        return d
+
+    def _desc_no_src(self, arr):
         d = ProblemDesc()
         d.ni, d.nj, d.nk = self.ni, self.nj, self.nk
         d.medium_type = self.medium_type
@@ -149,19 +156,6 @@ class Problem:
                                           float(f["beta_max"]), float(f["ref_vel"]))
         d.free_top = int(self.free_top)
         d.dt, d.t0, d.nt_total = float(self.dt), float(self.t0), int(self.nt_total)
-        if self.src is not None and self.src.num > 0:
-            s = self.src
-            d.src.num = s.num
-            d.src.stf_given, d.src.stf_length = s.stf_given, s.stf_length
-            d.src.stf_dt, d.src.stf_nt = s.stf_dt, s.stf_nt
-            d.src.cmp_type, d.src.mechanism_type = s.cmp_type, s.mechanism_type
-            d.src.loc_coord_type, d.src.loc_3dim = s.loc_coord_type, s.loc_3dim
-            d.src.loc = _ptr(arr(s.loc, np.float32))
-            d.src.t_start = _ptr(arr(s.t_start, np.float32))
-            d.src.wavelet = _ptr(arr(s.wavelet, np.int32))
-            d.src.wavelet_coefs = _ptr(arr(s.wavelet_coefs, np.float32))
-            d.src.cmp = _ptr(arr(s.cmp, np.float32))
-            d.src.cmp_values = _ptr(arr(s.cmp_values, np.float32))
         if self.sta is not None and self.sta.num > 0:
             t = self.sta
             d.sta.num = t.num
@@ -171,8 +165,21 @@ class Problem:
             d.sta.loc = _ptr(arr(t.loc, np.float32))
         d.precision = int(self.precision)
         d.device = int(self.device)
-        d._keep = keep
         return d
+
+
+def _fill_src(ds, s, arr):
+    ds.num = s.num
+    ds.stf_given, ds.stf_length = s.stf_given, s.stf_length
+    ds.stf_dt, ds.stf_nt = s.stf_dt, s.stf_nt
+    ds.cmp_type, ds.mechanism_type = s.cmp_type, s.mechanism_type
+    ds.loc_coord_type, ds.loc_3dim = s.loc_coord_type, s.loc_3dim
+    ds.loc = _ptr(arr(s.loc, np.float32))
+    ds.t_start = _ptr(arr(s.t_start, np.float32))
+    ds.wavelet = _ptr(arr(s.wavelet, np.int32))
+    ds.wavelet_coefs = _ptr(arr(s.wavelet_coefs, np.float32))
+    ds.cmp = _ptr(arr(s.cmp, np.float32))
+    ds.cmp_values = _ptr(arr(s.cmp_values, np.float32))
 
 
 _lib = None
@@ -192,6 +199,10 @@ def lib():
         "cgfd_version": (C.c_int, []),
         "cgfd_last_error": (C.c_char_p, []),
         "cgfd_problem_create": (C.c_int, [C.POINTER(ProblemDesc), C.POINTER(P)]),
+        "cgfd_batch_create": (C.c_int, [C.POINTER(ProblemDesc), C.c_int, P, C.POINTER(P)]),
+        "cgfd_num_shots": (C.c_int, [P]),
+        "cgfd_get_wavefield_shot": (C.c_int, [P, C.c_int, P]),
+        "cgfd_set_wavefield_shot": (C.c_int, [P, C.c_int, P]),
         "cgfd_problem_destroy": (C.c_int, [P]),
         "cgfd_run": (C.c_int, [P, C.c_int]),
         "cgfd_enqueue_steps": (C.c_int, [P, C.c_int]),
@@ -231,13 +242,31 @@ def check(rc):
 
 
 class Simulation:
-    """Device state of one forward simulation (cgfd_problem_create ... destroy)."""
+    """Device state of one forward simulation (cgfd_problem_create ... destroy), or of a batch
+    of shots sharing one grid (cgfd_batch_create) when `shots` (list of Sources) is given."""
 
-    def __init__(self, problem: Problem):
+    def __init__(self, problem: Problem, shots=None):
         self.problem = problem
         self._desc = problem.desc()
         h = C.c_void_p()
-        check(lib().cgfd_problem_create(C.byref(self._desc), C.byref(h)))
+        self.nshot = 1
+        if shots is None:
+            check(lib().cgfd_problem_create(C.byref(self._desc), C.byref(h)))
+        else:
+            keep = []
+
+            def arr(a, dt):
+                if a is None:
+                    return None
+                a = np.ascontiguousarray(a, dtype=dt)
+                keep.append(a)
+                return a
+            sd = (SourceDesc * len(shots))()
+            for n, s in enumerate(shots):
+                _fill_src(sd[n], s, arr)
+            self._shots = (sd, keep)
+            self.nshot = len(shots)
+            check(lib().cgfd_batch_create(C.byref(self._desc), self.nshot, C.addressof(sd), C.byref(h)))
         self.h = h
 
     def close(self):
@@ -278,20 +307,21 @@ class Simulation:
         return lib().cgfd_num_stations(self.h)
 
     def seismograms(self):
+        """[nsta, 9, nt_total], or [nshot, nsta, 9, nt_total] for a batch."""
         n = self.num_stations
-        out = np.zeros((max(n, 0), 9, self.problem.nt_total), np.float32)
+        out = np.zeros((self.nshot, max(n, 0), 9, self.problem.nt_total), np.float32)
         check(lib().cgfd_get_seismograms(self.h, out.ctypes.data))
-        return out
+        return out[0] if self.nshot == 1 else out
 
-    def wavefield(self):
+    def wavefield(self, shot=0):
         p = self.problem
         out = np.zeros((9,) + ref_shape(p.ni, p.nj, p.nk), np.float32)
-        check(lib().cgfd_get_wavefield(self.h, out.ctypes.data))
+        check(lib().cgfd_get_wavefield_shot(self.h, int(shot), out.ctypes.data))
         return out
 
-    def set_wavefield(self, w):
+    def set_wavefield(self, w, shot=0):
         w = np.ascontiguousarray(w, np.float32)
-        check(lib().cgfd_set_wavefield(self.h, w.ctypes.data))
+        check(lib().cgfd_set_wavefield_shot(self.h, int(shot), w.ctypes.data))
 
     def device_bytes(self):
         return int(lib().cgfd_device_bytes(self.h))

@@ -91,6 +91,7 @@ struct cgfd_problem {
   int device = 0;
   cudaStream_t stream = nullptr;
   int ni = 0, nj = 0, nk = 0, med = 0, ncoef = 0, nt_total = 0, free_top = 0;
+  int nshot = 1;  // wavefields sharing the grid, coefficients and stations
   float dt = 0.f;
   long long sx = 0, sz = 0, sf = 0, off0 = 0;
   size_t bytes = 0;
@@ -108,7 +109,8 @@ struct cgfd_problem {
   std::vector<Face> faces;
 
   cgfd::SrcHost src;
-  int *d_it_begin = nullptr, *d_ext_num = nullptr;
+  std::vector<int> src_shot;
+  int *d_it_begin = nullptr, *d_ext_num = nullptr, *d_src_shot = nullptr;
   long long *d_ext_idx = nullptr;
   float *d_ext_wv = nullptr, *d_ext_wt = nullptr, *d_stf = nullptr;
 
@@ -194,6 +196,7 @@ struct cgfd_problem {
     p.free_top = free_top;
     p.nbulk = free_top ? nk - cgfd::NSURF : nk;
     p.err = d_flag;
+    p.nshot = nshot;
     p.nface = 0;
     for (const Face &f : faces) {
       cgfd::FaceP &o = p.face[p.nface++];
@@ -204,8 +207,9 @@ struct cgfd_problem {
       o.ny = f.h.hi[1] - f.h.lo[1] + 1;
       o.n = f.n;
       o.A = f.A; o.B = f.B; o.D = f.D;
-      float *apre = f.aux + (size_t)(step & 1) * 9 * f.n, *aend = f.aux + (size_t)((step + 1) & 1) * 9 * f.n;
-      float *atmp = f.aux + (size_t)2 * 9 * f.n;
+      const size_t L = (size_t)nshot * 9 * f.n;
+      float *apre = f.aux + (size_t)(step & 1) * L, *aend = f.aux + (size_t)((step + 1) & 1) * L;
+      float *atmp = f.aux + (size_t)2 * L;
       o.aux_cur = stage == 0 ? apre : atmp;
       o.aux_pre = apre;
       o.aux_tmp = atmp;
@@ -219,7 +223,7 @@ struct cgfd_problem {
     int n = 0;
     if (rec.n > 0) {
       cgfd::RecvP r;
-      r.nsta = rec.n; r.nt_total = nt_total; r.idx8 = d_idx8; r.w8 = d_w8;
+      r.nsta = rec.n; r.nshot = nshot; r.nt_total = nt_total; r.idx8 = d_idx8; r.w8 = d_w8;
       r.pre = wbuf[step & 1]; r.sf = sf; r.seis = d_seis; r.d_it = d_it; r.d_flag = d_flag;
       n += timed(6, [&] { return cgfd::launch_recv(r, st); });
     }
@@ -244,7 +248,7 @@ struct cgfd_problem {
         q.force = src.force; q.moment = src.moment; q.stage = s;
         q.ca = p.ca; q.cb = p.cb;
         q.it_begin = d_it_begin; q.ext_num = d_ext_num; q.ext_idx = d_ext_idx;
-        q.ext_wv = d_ext_wv; q.ext_wt = d_ext_wt; q.stf = d_stf;
+        q.ext_wv = d_ext_wv; q.ext_wt = d_ext_wt; q.stf = d_stf; q.src_shot = d_src_shot;
         q.tmp_out = p.tmp_out; q.end = p.end; q.sf = sf; q.d_it = d_it;
         n += timed(5, [&] { return cgfd::launch_source(q, st); });
       }
@@ -286,7 +290,7 @@ struct cgfd_problem {
     for (auto *p : wbuf) cudaFree(p);
     cudaFree(coef); cudaFree(jac); cudaFree(matx); cudaFree(maty);
     for (Face &f : faces) { cudaFree(f.A); cudaFree(f.B); cudaFree(f.D); cudaFree(f.aux); }
-    cudaFree(d_it_begin); cudaFree(d_ext_num); cudaFree(d_ext_idx); cudaFree(d_ext_wv); cudaFree(d_ext_wt);
+    cudaFree(d_it_begin); cudaFree(d_ext_num); cudaFree(d_src_shot); cudaFree(d_ext_idx); cudaFree(d_ext_wv); cudaFree(d_ext_wt);
     cudaFree(d_stf); cudaFree(d_idx8); cudaFree(d_w8); cudaFree(d_seis); cudaFree(d_it); cudaFree(d_flag);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -315,8 +319,10 @@ void upload_field(cgfd_problem *p, const float *host_ref, float *dst, float *sta
   CK(cudaGetLastError());
 }
 
-void build(cgfd_problem *p, const cgfd_problem_desc *d) {
+void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_source_desc *shots) {
   cgfd::validate_desc(d);
+  if (nshot < 1) throw cgfd::Error(CGFD_ERR_INVALID, "nshot must be >= 1");
+  p->nshot = nshot;
   if (d->precision != CGFD_PREC_FP32) throw cgfd::Error(CGFD_ERR_UNSUPPORTED, "only CGFD_PREC_FP32 in this build");
   p->device = d->device;
   CK(cudaSetDevice(p->device));
@@ -343,10 +349,10 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d) {
   }
 
   size_t &B = p->bytes;
-  for (int l = 0; l < 4; l++) p->wbuf[l] = dmalloc<float>((size_t)9 * p->sf, B);
+  for (int l = 0; l < 4; l++) p->wbuf[l] = dmalloc<float>((size_t)9 * p->sf * nshot, B);
   p->coef = dmalloc<float>((size_t)p->ncoef * p->sf, B);
   p->jac = dmalloc<float>((size_t)p->sf, B);
-  for (int l = 0; l < 4; l++) CK(cudaMemsetAsync(p->wbuf[l], 0, sizeof(float) * 9 * p->sf, p->stream));
+  for (int l = 0; l < 4; l++) CK(cudaMemsetAsync(p->wbuf[l], 0, sizeof(float) * 9 * p->sf * nshot, p->stream));
   CK(cudaMemsetAsync(p->coef, 0, sizeof(float) * p->ncoef * p->sf, p->stream));
   CK(cudaMemsetAsync(p->jac, 0, sizeof(float) * p->sf, p->stream));
 
@@ -367,8 +373,8 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d) {
   {
     int ty = cgfd::tma_tile_y(p->med);
     for (int l = 0; l < 4; l++) {
-      make_map(&p->map_halo[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9, p->sz, p->sf, cgfd::TX + 8, ty + 6, 9);
-      make_map(&p->map_ctr[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9, p->sz, p->sf, cgfd::TX, ty, 9);
+      make_map(&p->map_halo[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX + 8, ty + 6, 9);
+      make_map(&p->map_ctr[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX, ty, 9);
     }
     make_map(&p->map_coef, p->coef, p->sx, p->nj + 6, p->nk + 6, p->ncoef, p->sz, p->sf, cgfd::TX, ty, p->ncoef);
     CK(cgfd::tma_prepare(p->med));
@@ -396,12 +402,50 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d) {
       CK(cudaMemcpy(f.A, f.h.A.data(), N1 * sizeof(float), cudaMemcpyHostToDevice));
       CK(cudaMemcpy(f.B, f.h.B.data(), N1 * sizeof(float), cudaMemcpyHostToDevice));
       CK(cudaMemcpy(f.D, f.h.D.data(), N1 * sizeof(float), cudaMemcpyHostToDevice));
-      f.aux = dmalloc<float>((size_t)3 * 9 * f.n, B);
-      CK(cudaMemset(f.aux, 0, sizeof(float) * 3 * 9 * f.n));
+      f.aux = dmalloc<float>((size_t)3 * 9 * f.n * nshot, B);
+      CK(cudaMemset(f.aux, 0, sizeof(float) * 3 * 9 * f.n * nshot));
       p->faces.push_back(f);
     }
-  // sources
-  cgfd::src_setup(d, p->src);
+  // sources: one set per shot, concatenated (each source knows its shot)
+  if (!shots) {
+    cgfd::src_setup(d, p->src);
+    p->src_shot.assign(p->src.nsrc, 0);
+  } else {
+    cgfd::SrcHost &all = p->src;
+    all = cgfd::SrcHost();
+    std::vector<cgfd::SrcHost> per(nshot);
+    for (int sh = 0; sh < nshot; sh++) {
+      cgfd_problem_desc ds = *d;
+      ds.src = shots[sh];
+      cgfd::validate_desc(&ds);
+      cgfd::src_setup(&ds, per[sh]);
+      all.max_nt = std::max(all.max_nt, per[sh].max_nt);
+      all.max_ext = std::max(all.max_ext, per[sh].max_ext);
+      all.force |= per[sh].force;
+      all.moment |= per[sh].moment;
+    }
+    for (int sh = 0; sh < nshot; sh++) {
+      const cgfd::SrcHost &q = per[sh];
+      for (int is = 0; is < q.nsrc; is++) {
+        all.it_begin.push_back(q.it_begin[is]);
+        all.ext_num.push_back(q.ext_num[is]);
+        for (int e = 0; e < all.max_ext; e++) {
+          bool ok = e < q.max_ext;
+          size_t qe = (size_t)is * q.max_ext + e;
+          all.ext_i.push_back(ok ? q.ext_i[qe] : 0);
+          all.ext_j.push_back(ok ? q.ext_j[qe] : 0);
+          all.ext_k.push_back(ok ? q.ext_k[qe] : 0);
+          all.ext_wv.push_back(ok ? q.ext_wv[qe] : 0.f);
+          all.ext_wt.push_back(ok ? q.ext_wt[qe] : 0.f);
+        }
+        for (int t = 0; t < all.max_nt; t++)
+          for (int c = 0; c < 36; c++)
+            all.stf.push_back(t < q.max_nt ? q.stf[((size_t)is * q.max_nt + t) * 36 + c] : 0.f);
+        p->src_shot.push_back(sh);
+        all.nsrc++;
+      }
+    }
+  }
   if (p->src.nsrc > 0) {
     cgfd::SrcHost &s = p->src;
     size_t ne = (size_t)s.nsrc * s.max_ext;
@@ -413,6 +457,8 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d) {
     p->d_ext_wv = dmalloc<float>(ne, B);
     p->d_ext_wt = dmalloc<float>(ne, B);
     p->d_stf = dmalloc<float>(s.stf.size(), B);
+    p->d_src_shot = dmalloc<int>(s.nsrc, B);
+    CK(cudaMemcpy(p->d_src_shot, p->src_shot.data(), s.nsrc * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(p->d_it_begin, s.it_begin.data(), s.nsrc * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(p->d_ext_num, s.ext_num.data(), s.nsrc * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(p->d_ext_idx, idx.data(), ne * sizeof(long long), cudaMemcpyHostToDevice));
@@ -429,10 +475,10 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d) {
         idx8[(size_t)r * 8 + q] = p->didx(p->rec.i[r] + (q & 1), p->rec.j[r] + ((q >> 1) & 1), p->rec.k[r] + ((q >> 2) & 1));
     p->d_idx8 = dmalloc<long long>(idx8.size(), B);
     p->d_w8 = dmalloc<float>(p->rec.w8.size(), B);
-    p->d_seis = dmalloc<float>((size_t)p->rec.n * 9 * p->nt_total, B);
+    p->d_seis = dmalloc<float>((size_t)p->rec.n * 9 * p->nt_total * nshot, B);
     CK(cudaMemcpy(p->d_idx8, idx8.data(), idx8.size() * sizeof(long long), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(p->d_w8, p->rec.w8.data(), p->rec.w8.size() * sizeof(float), cudaMemcpyHostToDevice));
-    CK(cudaMemset(p->d_seis, 0, sizeof(float) * p->rec.n * 9 * p->nt_total));
+    CK(cudaMemset(p->d_seis, 0, sizeof(float) * p->rec.n * 9 * p->nt_total * nshot));
   }
   p->d_it = dmalloc<int>(1, B);
   p->d_flag = dmalloc<int>(1, B);
@@ -453,7 +499,7 @@ int cgfd_problem_create(const cgfd_problem_desc *desc, cgfd_problem **out) {
   if (!out) { set_err("out is NULL"); return CGFD_ERR_INVALID; }
   *out = nullptr;
   cgfd_problem *p = new cgfd_problem;
-  int rc = guarded([&] { build(p, desc); });
+  int rc = guarded([&] { build(p, desc, 1, nullptr); });
   if (rc != CGFD_OK) {
     p->release();
     delete p;
@@ -462,6 +508,22 @@ int cgfd_problem_create(const cgfd_problem_desc *desc, cgfd_problem **out) {
   *out = p;
   return CGFD_OK;
 }
+
+int cgfd_batch_create(const cgfd_problem_desc *desc, int nshot, const cgfd_source_desc *shots, cgfd_problem **out) {
+  if (!out || !shots) { set_err("out/shots is NULL"); return CGFD_ERR_INVALID; }
+  *out = nullptr;
+  cgfd_problem *p = new cgfd_problem;
+  int rc = guarded([&] { build(p, desc, nshot, shots); });
+  if (rc != CGFD_OK) {
+    p->release();
+    delete p;
+    return rc;
+  }
+  *out = p;
+  return CGFD_OK;
+}
+
+int cgfd_num_shots(const cgfd_problem *p) { return p ? p->nshot : -1; }
 
 int cgfd_problem_destroy(cgfd_problem *p) {
   if (!p) return CGFD_OK;
@@ -511,7 +573,7 @@ int cgfd_set_step(cgfd_problem *p, int it) {
       std::swap(p->map_halo[0], p->map_halo[1]);
       std::swap(p->map_ctr[0], p->map_ctr[1]);
       for (auto &f : p->faces) {
-        size_t n = (size_t)9 * f.n;
+        size_t n = (size_t)9 * f.n * p->nshot;
         CK(cudaMemcpyAsync(f.aux + n * 2, f.aux, n * sizeof(float), cudaMemcpyDeviceToDevice, p->stream));
         CK(cudaMemcpyAsync(f.aux, f.aux + n, n * sizeof(float), cudaMemcpyDeviceToDevice, p->stream));
         CK(cudaMemcpyAsync(f.aux + n, f.aux + n * 2, n * sizeof(float), cudaMemcpyDeviceToDevice, p->stream));
@@ -542,18 +604,18 @@ int cgfd_get_seismograms(cgfd_problem *p, float *out) {
     CK(cudaSetDevice(p->device));
     CK(cudaStreamSynchronize(p->stream));
     if (p->rec.n > 0)
-      CK(cudaMemcpy(out, p->d_seis, sizeof(float) * p->rec.n * 9 * p->nt_total, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(out, p->d_seis, sizeof(float) * p->rec.n * 9 * p->nt_total * p->nshot, cudaMemcpyDeviceToHost));
   });
 }
 
-int cgfd_get_wavefield(cgfd_problem *p, float *out) {
-  if (!p || !out) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
+int cgfd_get_wavefield_shot(cgfd_problem *p, int shot, float *out) {
+  if (!p || !out || shot < 0 || shot >= p->nshot) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
   return guarded([&] {
     CK(cudaSetDevice(p->device));
     cgfd::RefGrid g(p->ni, p->nj, p->nk);
     size_t acc = 0;
     float *tmp = dmalloc<float>(g.siz_icmp, acc);
-    const float *pre = p->wbuf[p->it & 1];
+    const float *pre = p->wbuf[p->it & 1] + (size_t)shot * 9 * p->sf;
     for (int c = 0; c < 9; c++) {
       cgfd::launch_repack_out(pre + (size_t)c * p->sf, tmp, p->ni, p->nj, p->nk, p->sx, p->sz, p->off0, p->stream);
       CK(cudaMemcpyAsync(out + (size_t)c * g.siz_icmp, tmp, g.siz_icmp * sizeof(float), cudaMemcpyDeviceToHost, p->stream));
@@ -563,19 +625,23 @@ int cgfd_get_wavefield(cgfd_problem *p, float *out) {
   });
 }
 
-int cgfd_set_wavefield(cgfd_problem *p, const float *in) {
-  if (!p || !in) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
+int cgfd_get_wavefield(cgfd_problem *p, float *out) { return cgfd_get_wavefield_shot(p, 0, out); }
+
+int cgfd_set_wavefield_shot(cgfd_problem *p, int shot, const float *in) {
+  if (!p || !in || shot < 0 || shot >= p->nshot) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
   return guarded([&] {
     CK(cudaSetDevice(p->device));
     cgfd::RefGrid g(p->ni, p->nj, p->nk);
     size_t acc = 0;
     float *tmp = dmalloc<float>(g.siz_icmp, acc);
-    float *pre = p->wbuf[p->it & 1];
+    float *pre = p->wbuf[p->it & 1] + (size_t)shot * 9 * p->sf;
     for (int c = 0; c < 9; c++) upload_field(p, in + (size_t)c * g.siz_icmp, pre + (size_t)c * p->sf, tmp, 0, 0);
     CK(cudaStreamSynchronize(p->stream));
     cudaFree(tmp);
   });
 }
+
+int cgfd_set_wavefield(cgfd_problem *p, const float *in) { return cgfd_set_wavefield_shot(p, 0, in); }
 
 size_t cgfd_device_bytes(const cgfd_problem *p) { return p ? p->bytes : 0; }
 
@@ -602,6 +668,7 @@ int cgfd_get_zchunk(const cgfd_problem *p) { return p ? p->nzc : -1; }
 /* Bulk kernel variant: 1 = TMA-pipelined (default), 0 = direct loads. */
 int cgfd_set_bulk_variant(cgfd_problem *p, int tma) {
   if (!p) return CGFD_ERR_INVALID;
+  if (!tma && p->nshot > 1) { set_err("the direct-load bulk kernel handles one shot"); return CGFD_ERR_UNSUPPORTED; }
   p->use_tma = tma != 0;
   for (int s = 0; s < 8; s++)
     if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }

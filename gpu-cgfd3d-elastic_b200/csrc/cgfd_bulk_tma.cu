@@ -75,7 +75,9 @@ __global__ void __launch_bounds__(TX *TYT, 1)
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + S::OFF_BAR);  // 0..2 wave, 3..4 cpe
 
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int bx = blockIdx.x, by = blockIdx.y;
+  // shots are the fastest block index: the nshot blocks of one tile run side by side and
+  // share the coefficient tiles through L2
+  const int shot = blockIdx.x % p.nshot, bx = blockIdx.x / p.nshot, by = blockIdx.y;
   const int i = bx * TX + tx, j = by * TYT + ty;
   const int kb = blockIdx.z * nzc;
   const int ke = min(kb + nzc, p.nbulk);
@@ -84,6 +86,10 @@ __global__ void __launch_bounds__(TX *TYT, 1)
   const bool act = i < p.ni && j < p.nj;
   const int k0 = SD > 0 ? kb : ke - 1;
   const long long sf = p.sf;
+  const long long woff = (long long)shot * 9 * sf;
+  const float *__restrict__ cur = p.cur + woff;
+  float *__restrict__ tmp_out = p.tmp_out + woff;
+  float *__restrict__ endw = p.end + woff;
   const int stage = p.stage;
   const bool need_pre = stage == 1 || stage == 2;
   const bool need_end = stage >= 1;
@@ -103,7 +109,7 @@ __global__ void __launch_bounds__(TX *TYT, 1)
     const int kk = k0 + m * SD;
     uint64_t *b = &bar[m % 3];
     mbar_expect_tx(b, wave_bytes);
-    tma_load_4d(wave + (m % 3) * (S::WAVE_SLOT / 4), &tm.cur, xw, yw, kk + 3, 0, b);
+    tma_load_4d(wave + (m % 3) * (S::WAVE_SLOT / 4), &tm.cur, xw, yw, kk + 3, 9 * shot, b);
   };
   auto issue_cpe = [&](int m) {
     const int kk = k0 + m * SD;
@@ -112,8 +118,8 @@ __global__ void __launch_bounds__(TX *TYT, 1)
     unsigned char *base = cpe + sl * S::CPE_SLOT;
     mbar_expect_tx(b, cpe_bytes);
     tma_load_4d(base, &tm.coef, xc, yc, kk + 3, 0, b);
-    if (need_pre) tma_load_4d(base + S::COEF_BYTES, &tm.pre, xc, yc, kk + 3, 0, b);
-    if (need_end) tma_load_4d(base + S::COEF_BYTES + S::FLD_BYTES, &tm.end, xc, yc, kk + 3, 0, b);
+    if (need_pre) tma_load_4d(base + S::COEF_BYTES, &tm.pre, xc, yc, kk + 3, 9 * shot, b);
+    if (need_end) tma_load_4d(base + S::COEF_BYTES + S::FLD_BYTES, &tm.end, xc, yc, kk + 3, 9 * shot, b);
   };
   if (tid == 0) {
     issue_wave(0);
@@ -142,7 +148,7 @@ __global__ void __launch_bounds__(TX *TYT, 1)
     for (int m = 0; m < 3; m++) {
       const long long id = didx(p, i, j, k0 + (m - 3) * SD);
 #pragma unroll
-      for (int f = 0; f < 9; f++) q[f][m] = __ldg(p.cur + f * sf + id);
+      for (int f = 0; f < 9; f++) q[f][m] = __ldg(cur + f * sf + id);
     }
   }
   const int wc = (ty + 3) * S::WX + tx + 4;  // centre of this thread in a wave slot (per field)
@@ -191,7 +197,7 @@ __global__ void __launch_bounds__(TX *TYT, 1)
             const FaceP &fc = p.face[fi];
             if ((fmask >> fi & 1) && fc.axis == 0 && i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] &&
                 j <= fc.hi[1] && k >= fc.lo[2] && k <= fc.hi[2])
-              pml_face<MED>(p, fc, i, j, k, md, slw, mt[0], d, d + 3, nullptr, nullptr, acc.hc);
+              pml_face<MED>(p, fc, i, j, k, md, slw, mt[0], d, d + 3, nullptr, nullptr, acc.hc, shot);
           }
       }
       // y
@@ -208,7 +214,7 @@ __global__ void __launch_bounds__(TX *TYT, 1)
             const FaceP &fc = p.face[fi];
             if ((fmask >> fi & 1) && fc.axis == 1 && i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] &&
                 j <= fc.hi[1] && k >= fc.lo[2] && k <= fc.hi[2])
-              pml_face<MED>(p, fc, i, j, k, md, slw, mt[1], d, d + 3, nullptr, nullptr, acc.hc);
+              pml_face<MED>(p, fc, i, j, k, md, slw, mt[1], d, d + 3, nullptr, nullptr, acc.hc, shot);
           }
       }
       // z (queue in march order; the operator takes increasing k)
@@ -224,7 +230,7 @@ __global__ void __launch_bounds__(TX *TYT, 1)
             const FaceP &fc = p.face[fi];
             if ((fmask >> fi & 1) && fc.axis == 2 && i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] &&
                 j <= fc.hi[1] && k >= fc.lo[2] && k <= fc.hi[2])
-              pml_face<MED>(p, fc, i, j, k, md, slw, mt[2], d, d + 3, nullptr, nullptr, acc.hc);
+              pml_face<MED>(p, fc, i, j, k, md, slw, mt[2], d, d + 3, nullptr, nullptr, acc.hc, shot);
           }
       }
       float h[9];
@@ -242,18 +248,18 @@ __global__ void __launch_bounds__(TX *TYT, 1)
       if (stage == 0) {
 #pragma unroll
         for (int f = 0; f < 9; f++) {
-          p.tmp_out[f * sf + id] = q[f][3] + ca * h[f];
-          p.end[f * sf + id] = q[f][3] + cb * h[f];
+          tmp_out[f * sf + id] = q[f][3] + ca * h[f];
+          endw[f * sf + id] = q[f][3] + cb * h[f];
         }
       } else if (stage < 3) {
 #pragma unroll
         for (int f = 0; f < 9; f++) {
-          p.tmp_out[f * sf + id] = PR[f * S::CELLS] + ca * h[f];
-          p.end[f * sf + id] = EN[f * S::CELLS] + cb * h[f];
+          tmp_out[f * sf + id] = PR[f * S::CELLS] + ca * h[f];
+          endw[f * sf + id] = EN[f * S::CELLS] + cb * h[f];
         }
       } else {
 #pragma unroll
-        for (int f = 0; f < 9; f++) p.end[f * sf + id] = EN[f * S::CELLS] + cb * h[f];
+        for (int f = 0; f < 9; f++) endw[f * sf + id] = EN[f * S::CELLS] + cb * h[f];
       }
     }
 #pragma unroll
@@ -270,7 +276,7 @@ static void launch_tma_med(const StageP &p, const TmaP &tm, int nzc, cudaStream_
   using S = BulkSmem<MED, TYT>;
   const int code = p.dir[0] | (p.dir[1] << 1) | (p.dir[2] << 2);
   dim3 block(TX, TYT);
-  dim3 grid((p.ni + TX - 1) / TX, (p.nj + TYT - 1) / TYT, (p.nbulk + nzc - 1) / nzc);
+  dim3 grid(((p.ni + TX - 1) / TX) * p.nshot, (p.nj + TYT - 1) / TYT, (p.nbulk + nzc - 1) / nzc);
   switch (code) {
 #define CASE(c)                                                                                            \
   case c:                                                                                                  \

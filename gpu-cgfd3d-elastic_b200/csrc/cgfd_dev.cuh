@@ -47,6 +47,7 @@ struct FaceP {
   int nx, ny;         // box extents along x, y
   long long n;        // points in the box
   const float *A, *B, *D;
+  // each level holds nshot x 9 components (shot stride 9 n)
   const float *aux_cur;   // level read by the RHS (pre at stage 0, tmp otherwise)
   const float *aux_pre;   // pre level (stages 1-2)
   float *aux_tmp;         // tmp level written at stages 0-2 (== aux_cur at stages 1-2)
@@ -73,6 +74,7 @@ struct StageP {
   int nface;
   FaceP face[6];
   int *err;               // device error word (bit 1: pipeline wait timed out)
+  int nshot;              // wavefields sharing this grid (batched sources); 1 = plain
 };
 
 // Tensor maps of the arrays one stage streams through TMA: the stage input (4-D box with
@@ -248,11 +250,11 @@ template <int MED>
 __device__ __forceinline__ void pml_face(const StageP &p, const FaceP &f, int i, int j, int k,
                                          const Medium<MED> &md, float slw, const float m[3],
                                          const float dv[3], const float dt[6], const float *surf_mat,
-                                         const float zeta[3], float hc[9]) {
+                                         const float zeta[3], float hc[9], int shot = 0) {
   int ab = f.axis == 0 ? i - f.lo[0] : (f.axis == 1 ? j - f.lo[1] : k - f.lo[2]);
   float cA = __ldg(f.A + ab), cB = __ldg(f.B + ab), cD = __ldg(f.D + ab);
   float cB1 = cB - 1.0f;
-  long long ia = ((long long)(k - f.lo[2]) * f.ny + (j - f.lo[1])) * f.nx + (i - f.lo[0]);
+  long long ia = (long long)shot * 9 * f.n + ((long long)(k - f.lo[2]) * f.ny + (j - f.lo[1])) * f.nx + (i - f.lo[0]);
   float rhs[9];
   momentum_axis(m, dt, rhs);
   rhs[0] *= slw; rhs[1] *= slw; rhs[2] *= slw;

@@ -179,12 +179,15 @@ __global__ void __launch_bounds__(128) k_stage_surface(const __grid_constant__ S
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= p.ni || j >= p.nj) return;
   const long long sf = p.sf;
-  const float *__restrict__ cur = p.cur;
+  const int nslab = p.nk - p.nbulk;
+  const int shot = blockIdx.z / nslab;
+  const long long woff = (long long)shot * 9 * sf;
+  const float *__restrict__ cur = p.cur + woff;
   const long long offs[3] = {1, p.sx, p.sz};
   const int nk2 = p.nk - 1;
 
   {
-    const int k = p.nbulk + blockIdx.z;  // one thread per cell of the slab
+    const int k = p.nbulk + blockIdx.z % nslab;  // one thread per cell of the slab
     const long long id = didx(p, i, j, k);
     float m[3][3];
 #pragma unroll
@@ -304,14 +307,14 @@ __global__ void __launch_bounds__(128) k_stage_surface(const __grid_constant__ S
       const int a = fc.axis;
       const float *smat = nullptr;
       if (p.free_top && a < 2 && k == nk2) smat = (a == 0 ? p.matx : p.maty) + ((long long)j * p.ni + i) * 9;
-      pml_face<MED>(p, fc, i, j, k, md, slw, m[a], dv[a], dtt[a], smat, m[2], hc);
+      pml_face<MED>(p, fc, i, j, k, md, slw, m[a], dv[a], dtt[a], smat, m[2], hc, shot);
     }
 #pragma unroll
     for (int c = 0; c < 9; c++) h[c] += hc[c];
     float cc[9];
 #pragma unroll
     for (int f = 0; f < 9; f++) cc[f] = __ldg(cur + f * sf + id);
-    rk_store(p.stage, p.ca, p.cb, sf, id, cc, h, p.pre, p.tmp_out, p.end);
+    rk_store(p.stage, p.ca, p.cb, sf, id, cc, h, p.pre + woff, p.tmp_out ? p.tmp_out + woff : nullptr, p.end + woff);
   }
 }
 
@@ -326,7 +329,7 @@ __global__ void k_source(const __grid_constant__ SrcP s) {
   const int ib = s.it_begin[is];
   if (it < ib || it > ib + s.max_nt - 1) return;
   const float *v = s.stf + (((long long)is * s.max_nt + (it - ib)) * 4 + s.stage) * 9;
-  const long long id = s.ext_idx[(long long)is * s.max_ext + e];
+  const long long id = s.ext_idx[(long long)is * s.max_ext + e] + (long long)s.src_shot[is] * 9 * s.sf;
   const float wv = s.ext_wv[(long long)is * s.max_ext + e];
   const float wt = s.ext_wt[(long long)is * s.max_ext + e];
   for (int c = 0; c < 9; c++) {
@@ -340,18 +343,19 @@ __global__ void k_source(const __grid_constant__ SrcP s) {
 
 __global__ void k_recv(const __grid_constant__ RecvP r) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= r.nsta * 9) return;
+  if (t >= r.nshot * r.nsta * 9) return;
   const int it = *r.d_it;
   if (it < 0 || it >= r.nt_total) return;
-  const int sidx = t / 9, c = t % 9;
+  const int shot = t / (r.nsta * 9), sidx = (t / 9) % r.nsta, c = t % 9;
+  const float *pre = r.pre + (long long)shot * 9 * r.sf;
   float v = 0.f;
 #pragma unroll
   for (int qn = 0; qn < 8; qn++) {
     float w = r.w8[sidx * 8 + qn];
-    if (w != 0.f) v += w * __ldg(r.pre + c * r.sf + r.idx8[sidx * 8 + qn]);
+    if (w != 0.f) v += w * __ldg(pre + c * r.sf + r.idx8[sidx * 8 + qn]);
   }
   if (!isfinite(v)) atomicOr(r.d_flag, 1);
-  r.seis[((long long)sidx * 9 + c) * r.nt_total + it] = v;
+  r.seis[(((long long)shot * r.nsta + sidx) * 9 + c) * r.nt_total + it] = v;
 }
 
 __global__ void k_advance(int *d_it) {
@@ -418,7 +422,7 @@ int launch_stage_bulk(int med, const StageP &p, int nzc, cudaStream_t st) {
 int launch_stage_surface(int med, const StageP &p, cudaStream_t st) {
   if (p.nbulk >= p.nk) return 0;
   dim3 block(32, 4);
-  dim3 grid((p.ni + 31) / 32, (p.nj + 3) / 4, p.nk - p.nbulk);
+  dim3 grid((p.ni + 31) / 32, (p.nj + 3) / 4, (p.nk - p.nbulk) * p.nshot);
   if (med == MED_ISO) k_stage_surface<MED_ISO><<<grid, block, 0, st>>>(p);
   else if (med == MED_VTI) k_stage_surface<MED_VTI><<<grid, block, 0, st>>>(p);
   else k_stage_surface<MED_ANISO><<<grid, block, 0, st>>>(p);
@@ -435,7 +439,7 @@ int launch_source(const SrcP &s, cudaStream_t st) {
 
 int launch_recv(const RecvP &r, cudaStream_t st) {
   if (r.nsta <= 0) return 0;
-  int n = r.nsta * 9;
+  int n = r.nshot * r.nsta * 9;
   k_recv<<<(n + 127) / 128, 128, 0, st>>>(r);
   return 1;
 }

@@ -20,6 +20,7 @@ struct SrcP {
   const float *ext_wv;         // [nsrc][max_ext] coef * (1/rho) / jac
   const float *ext_wt;         // [nsrc][max_ext] coef / jac
   const float *stf;            // [nsrc][max_nt][4][9]: fx fy fz mxx myy mzz myz mxz mxy
+  const int *src_shot;         // [nsrc] wavefield (shot) each source acts on
   float *tmp_out;
   float *end;
   long long sf;
@@ -29,12 +30,13 @@ struct SrcP {
 // Station sampling of w_pre (io_funcs.cu:1624-1666).
 struct RecvP {
   int nsta;
+  int nshot;                   // every shot is sampled at the same stations
   int nt_total;
   const long long *idx8;       // [nsta][8] device-layout corner index
   const float *w8;             // [nsta][8] trilinear weights (reference corner usage)
   const float *pre;
   long long sf;
-  float *seis;                 // [nsta][9][nt_total]
+  float *seis;                 // [nshot][nsta][9][nt_total]
   const int *d_it;
   int *d_flag;
 };

@@ -144,6 +144,18 @@ const char *cgfd_last_error(void);
 int cgfd_problem_create(const cgfd_problem_desc *desc, cgfd_problem **out);
 
 /*
+ * Batched sources on one grid: nshot independent wavefields share the grid, metrics,
+ * medium, boundaries and stations (desc->src is ignored); shots[s] holds the sources of
+ * wavefield s. One launch per kernel and RK stage covers every shot, with the shot as the
+ * fastest block index so that the coefficient tiles of a grid tile are read once from HBM
+ * for all shots. Seismograms come back as [nshot][nsta][9][nt_total].
+ * No counterpart in the reference (one source set per run there).
+ */
+int cgfd_batch_create(const cgfd_problem_desc *desc, int nshot, const cgfd_source_desc *shots,
+                      cgfd_problem **out);
+int cgfd_num_shots(const cgfd_problem *p);
+
+/*
  * Advance nsteps time steps (4 RK stages each), sampling the stations at the start of
  * every step like io_recv_keep. nsteps < 0 runs to nt_total.
  * Replaces: the time loop drv_rk_curv_col.cu:193-541.
@@ -157,8 +169,8 @@ int cgfd_current_step(const cgfd_problem *p);
 int cgfd_set_step(cgfd_problem *p, int it);
 
 /*
- * Seismograms, [nsta][9][nt_total] in component order Vx..Txy; entries for steps not yet
- * run are 0. Replaces: iorecv->recvone[r].seismo (io_funcs.cu:283-288, 1651-1659).
+ * Seismograms, [nshot][nsta][9][nt_total] in component order Vx..Txy (nshot = 1 unless
+ * created by cgfd_batch_create); entries for steps not yet run are 0. Replaces: iorecv->recvone[r].seismo (io_funcs.cu:283-288, 1651-1659).
  */
 int cgfd_get_seismograms(cgfd_problem *p, float *out);
 
@@ -180,6 +192,10 @@ int cgfd_get_wavefield(cgfd_problem *p, float *out);
 
 /* Overwrite w_pre (physical points only; ghosts stay 0). */
 int cgfd_set_wavefield(cgfd_problem *p, const float *in);
+
+/* Per-shot variants of cgfd_get_wavefield / cgfd_set_wavefield for batched problems. */
+int cgfd_get_wavefield_shot(cgfd_problem *p, int shot, float *out);
+int cgfd_set_wavefield_shot(cgfd_problem *p, int shot, const float *in);
 
 /* Device bytes held by the problem. */
 size_t cgfd_device_bytes(const cgfd_problem *p);
