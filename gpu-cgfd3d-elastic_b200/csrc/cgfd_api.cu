@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -72,14 +73,16 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-// 4-D map (x, y, z, field) over one device-layout array of nf fields.
-void make_map(CUtensorMap *m, const float *base, long long sx, long long ny, long long nz, int nf, long long sz,
-              long long sf, int boxx, int boxy, int boxf) {
+// 4-D map (x, y, z, field) over one device-layout array of nf fields of `esize`-byte elements
+// (4: FP32, 2: FP16 or BF16 as `dtype` says).
+void make_map(CUtensorMap *m, const void *base, long long sx, long long ny, long long nz, int nf, long long sz,
+              long long sf, int boxx, int boxy, int boxf, CUtensorMapDataType dtype = CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+              int esize = 4) {
   cuuint64_t dims[4] = {(cuuint64_t)sx, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)nf};
-  cuuint64_t strides[3] = {(cuuint64_t)sx * 4, (cuuint64_t)sz * 4, (cuuint64_t)sf * 4};
+  cuuint64_t strides[3] = {(cuuint64_t)(sx * esize), (cuuint64_t)(sz * esize), (cuuint64_t)(sf * esize)};
   cuuint32_t box[4] = {(cuuint32_t)boxx, (cuuint32_t)boxy, 1, (cuuint32_t)boxf};
   cuuint32_t es[4] = {1, 1, 1, 1};
-  CUresult r = tensor_map_encoder()(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float *>(base), dims, strides,
+  CUresult r = tensor_map_encoder()(m, dtype, 4, const_cast<void *>(base), dims, strides,
                                     box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) throw cgfd::Error(CGFD_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
@@ -99,6 +102,18 @@ struct cgfd_problem {
 
   float *wbuf[4] = {nullptr, nullptr, nullptr, nullptr};  // [0],[1]: pre/end by parity; [2],[3]: tmpA/tmpB
   float *coef = nullptr, *jac = nullptr, *matx = nullptr, *maty = nullptr;
+  // 16-bit coefficient storage (replaces `coef` when coef_type != COEF_F32):
+  // value = cscale[field] * stored + coffset[field]
+  int precision = CGFD_PREC_FP32;
+  int coef_type = cgfd::COEF_F32;
+  void *coef16 = nullptr;
+  float cscale[32] = {}, coffset[32] = {};
+  // FP16 stage levels (CGFD_PREC_FP16_WAVE): wbuf[2], wbuf[3] hold __half; per-step scale
+  // d_wsc[18] from d_amax[2] (max |w| of velocity / stress) and d_srcb[nt_total][2] (largest
+  // source increment of each step)
+  int wave16 = 0;
+  float *d_wsc = nullptr, *d_srcb = nullptr;
+  unsigned int *d_amax = nullptr;
 
   struct Face {
     cgfd::PmlFaceHost h;
@@ -192,11 +207,15 @@ struct cgfd_problem {
     p.end = end;
     p.ca = stage < 3 ? kRkA[stage] * dt : 0.f;
     p.cb = kRkB[stage] * dt;
-    p.coef = coef; p.jac = jac; p.matx = matx; p.maty = maty;
+    p.coef = coef_type == cgfd::COEF_F32 ? (const void *)coef : (const void *)coef16;
+    for (int c = 0; c < 32; c++) { p.cscale[c] = cscale[c]; p.coffset[c] = coffset[c]; }
+    p.jac = jac; p.matx = matx; p.maty = maty;
     p.free_top = free_top;
     p.nbulk = free_top ? nk - cgfd::NSURF : nk;
     p.err = d_flag;
     p.nshot = nshot;
+    p.wsc = d_wsc;
+    p.amax = d_amax;
     p.nface = 0;
     for (const Face &f : faces) {
       cgfd::FaceP &o = p.face[p.nface++];
@@ -227,6 +246,7 @@ struct cgfd_problem {
       r.pre = wbuf[step & 1]; r.sf = sf; r.seis = d_seis; r.d_it = d_it; r.d_flag = d_flag;
       n += timed(6, [&] { return cgfd::launch_recv(r, st); });
     }
+    if (wave16) n += timed(7, [&] { return cgfd::launch_wave_scale(d_amax, d_srcb, d_it, nt_total, d_wsc, st); });
     for (int s = 0; s < 4; s++) {
       cgfd::StageP p = stage_params(step, s);
       if (use_tma) {
@@ -237,11 +257,11 @@ struct cgfd_problem {
         tm.pre = map_ctr[pre];
         tm.end = map_ctr[end];
         tm.coef = map_coef;
-        n += timed(s, [&] { return cgfd::launch_stage_bulk_tma(med, p, tm, nzc, st); });
+        n += timed(s, [&] { return cgfd::launch_stage_bulk_tma(med, coef_type, wave16, p, tm, nzc, st); });
       } else {
         n += timed(s, [&] { return cgfd::launch_stage_bulk(med, p, nzc, st); });
       }
-      n += timed(4, [&] { return cgfd::launch_stage_surface(med, p, st); });
+      n += timed(4, [&] { return cgfd::launch_stage_surface(med, coef_type, wave16, p, st); });
       if (src.nsrc > 0) {
         cgfd::SrcP q;
         q.nsrc = src.nsrc; q.max_ext = src.max_ext; q.max_nt = src.max_nt;
@@ -250,6 +270,7 @@ struct cgfd_problem {
         q.it_begin = d_it_begin; q.ext_num = d_ext_num; q.ext_idx = d_ext_idx;
         q.ext_wv = d_ext_wv; q.ext_wt = d_ext_wt; q.stf = d_stf; q.src_shot = d_src_shot;
         q.tmp_out = p.tmp_out; q.end = p.end; q.sf = sf; q.d_it = d_it;
+        q.wave16 = wave16; q.wsc = d_wsc; q.amax = d_amax;
         n += timed(5, [&] { return cgfd::launch_source(q, st); });
       }
     }
@@ -288,9 +309,10 @@ struct cgfd_problem {
     for (auto &t : pending) { ev_free.push_back(t.a); ev_free.push_back(t.b); }
     for (auto e : ev_free) cudaEventDestroy(e);
     for (auto *p : wbuf) cudaFree(p);
-    cudaFree(coef); cudaFree(jac); cudaFree(matx); cudaFree(maty);
+    cudaFree(coef); cudaFree(coef16); cudaFree(jac); cudaFree(matx); cudaFree(maty);
     for (Face &f : faces) { cudaFree(f.A); cudaFree(f.B); cudaFree(f.D); cudaFree(f.aux); }
     cudaFree(d_it_begin); cudaFree(d_ext_num); cudaFree(d_src_shot); cudaFree(d_ext_idx); cudaFree(d_ext_wv); cudaFree(d_ext_wt);
+    cudaFree(d_wsc); cudaFree(d_srcb); cudaFree(d_amax);
     cudaFree(d_stf); cudaFree(d_idx8); cudaFree(d_w8); cudaFree(d_seis); cudaFree(d_it); cudaFree(d_flag);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -319,11 +341,96 @@ void upload_field(cgfd_problem *p, const float *host_ref, float *dst, float *sta
   CK(cudaGetLastError());
 }
 
+// Replace the FP32 coefficient array by a 16-bit copy (stochastically rounded), one
+// scale/offset per field chosen in FP64 from the field's exact extremes over the cells the
+// kernels read (physical box + 3 ghosts):
+//   FP16 / BF16: offset 0, power-of-two scale putting max |value| in [2^13, 2^14) (FP16
+//                keeps 11 significant bits for values down to 2^-27 of the maximum);
+//   U16 (fixed point): offset = min, scale = (max - min) / 65535, i.e. 16 bits across the
+//                field's range -- for the bounded ranges of metrics, 1/rho and moduli this
+//                is 20-30x finer than FP16.
+void to_16bit_coefficients(cgfd_problem *p) {
+  unsigned int *d_mm = dmalloc<unsigned int>(2 * p->ncoef, p->bytes);
+  std::vector<unsigned int> mm(2 * p->ncoef);
+  for (int c = 0; c < p->ncoef; c++) { mm[2 * c] = 0xffffffffu; mm[2 * c + 1] = 0u; }
+  CK(cudaMemcpyAsync(d_mm, mm.data(), sizeof(unsigned int) * mm.size(), cudaMemcpyHostToDevice, p->stream));
+  for (int c = 0; c < p->ncoef; c++)
+    cgfd::launch_coef_minmax(p->coef + (size_t)c * p->sf, p->ni, p->nj, p->nk, p->sx, p->sz, p->off0, d_mm + 2 * c,
+                             p->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(mm.data(), d_mm, sizeof(unsigned int) * mm.size(), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  cudaFree(d_mm);
+  p->bytes -= sizeof(unsigned int) * 2 * p->ncoef;
+  p->coef16 = dmalloc<uint16_t>((size_t)p->ncoef * p->sf, p->bytes);
+  for (int c = 0; c < p->ncoef; c++) {
+    const double lo = cgfd::coef_key_to_float(mm[2 * c]), hi = cgfd::coef_key_to_float(mm[2 * c + 1]);
+    if (!std::isfinite(lo) || !std::isfinite(hi))
+      throw cgfd::Error(CGFD_ERR_NONFINITE, "coefficient field " + std::to_string(c) + " is not finite");
+    double scale = 1.0, offset = 0.0;
+    if (p->coef_type == cgfd::COEF_U16) {
+      offset = lo;
+      scale = hi > lo ? (hi - lo) / 65535.0 : 1.0;
+    } else {
+      const double m = std::max(std::fabs(lo), std::fabs(hi));
+      if (m > 0.0) scale = std::ldexp(1.0, std::ilogb(m) - 13);
+    }
+    p->cscale[c] = (float)scale;
+    p->coffset[c] = (float)offset;
+    cgfd::launch_coef_to16(p->coef_type, p->coef + (size_t)c * p->sf, (uint16_t *)p->coef16 + (size_t)c * p->sf, p->sf,
+                           p->cscale[c], p->coffset[c], c, p->stream);
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(p->stream));
+  cudaFree(p->coef);
+  p->coef = nullptr;
+  p->bytes -= sizeof(float) * p->ncoef * p->sf;
+}
+
+// Largest source increment added to an RK stage input in each step, per group (velocity:
+// forces, stress: moments): max over sources, stages 0-2 and spread points of
+// |rk_a[s] dt * value * weight|. Part of the FP16 stage-level scale of that step.
+std::vector<float> source_bounds(const cgfd_problem *p) {
+  std::vector<float> sb((size_t)p->nt_total * 2, 0.f);
+  const cgfd::SrcHost &s = p->src;
+  for (int is = 0; is < s.nsrc; is++) {
+    float wv = 0.f, wt = 0.f;
+    for (int e = 0; e < s.ext_num[is]; e++) {
+      wv = std::max(wv, std::fabs(s.ext_wv[(size_t)is * s.max_ext + e]));
+      wt = std::max(wt, std::fabs(s.ext_wt[(size_t)is * s.max_ext + e]));
+    }
+    for (int t = 0; t < s.max_nt; t++) {
+      const int it = s.it_begin[is] + t;
+      if (it < 0 || it >= p->nt_total) continue;
+      for (int st = 0; st < 3; st++) {
+        const float ca = std::fabs(kRkA[st] * p->dt);
+        const float *v = &s.stf[(((size_t)is * s.max_nt + t) * 4 + st) * 9];
+        for (int c = 0; c < 9; c++) {
+          if (c < 3 && !s.force) continue;
+          if (c >= 3 && !s.moment) continue;
+          const float b = ca * std::fabs(v[c]) * (c < 3 ? wv : wt);
+          float &o = sb[(size_t)it * 2 + (c < 3 ? 0 : 1)];
+          o = std::max(o, b);
+        }
+      }
+    }
+  }
+  return sb;
+}
+
 void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_source_desc *shots) {
   cgfd::validate_desc(d);
   if (nshot < 1) throw cgfd::Error(CGFD_ERR_INVALID, "nshot must be >= 1");
   p->nshot = nshot;
-  if (d->precision != CGFD_PREC_FP32) throw cgfd::Error(CGFD_ERR_UNSUPPORTED, "only CGFD_PREC_FP32 in this build");
+  p->precision = d->precision;
+  switch (d->precision) {
+    case CGFD_PREC_BF16_COEF: p->coef_type = cgfd::COEF_BF16; break;
+    case CGFD_PREC_FP16_COEF: p->coef_type = cgfd::COEF_F16; break;
+    case CGFD_PREC_U16_COEF:
+    case CGFD_PREC_FP16_WAVE: p->coef_type = cgfd::COEF_U16; break;
+    default: p->coef_type = cgfd::COEF_F32;
+  }
+  p->wave16 = d->precision == CGFD_PREC_FP16_WAVE ? 1 : 0;
   p->device = d->device;
   CK(cudaSetDevice(p->device));
   CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
@@ -349,10 +456,13 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   }
 
   size_t &B = p->bytes;
-  for (int l = 0; l < 4; l++) p->wbuf[l] = dmalloc<float>((size_t)9 * p->sf * nshot, B);
+  // levels 0-1 (w_pre / w_end) FP32; 2-3 (RK stage inputs) FP32 or FP16
+  const size_t lev_bytes[4] = {4, 4, p->wave16 ? 2u : 4u, p->wave16 ? 2u : 4u};
+  for (int l = 0; l < 4; l++)
+    p->wbuf[l] = (float *)dmalloc<uint16_t>((size_t)9 * p->sf * nshot * (lev_bytes[l] / 2), B);
   p->coef = dmalloc<float>((size_t)p->ncoef * p->sf, B);
   p->jac = dmalloc<float>((size_t)p->sf, B);
-  for (int l = 0; l < 4; l++) CK(cudaMemsetAsync(p->wbuf[l], 0, sizeof(float) * 9 * p->sf * nshot, p->stream));
+  for (int l = 0; l < 4; l++) CK(cudaMemsetAsync(p->wbuf[l], 0, lev_bytes[l] * 9 * p->sf * nshot, p->stream));
   CK(cudaMemsetAsync(p->coef, 0, sizeof(float) * p->ncoef * p->sf, p->stream));
   CK(cudaMemsetAsync(p->jac, 0, sizeof(float) * p->sf, p->stream));
 
@@ -368,16 +478,31 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   CK(cudaStreamSynchronize(p->stream));
   cudaFree(stage_buf);
   B -= g.siz_icmp * sizeof(float);
+  if (p->coef_type != cgfd::COEF_F32) to_16bit_coefficients(p);
 
   // TMA tensor maps of the four wavefield levels and of the coefficients
   {
     int ty = cgfd::tma_tile_y(p->med);
     for (int l = 0; l < 4; l++) {
+      if (lev_bytes[l] == 2) {  // FP16 stage level: x halo of 8 elements keeps the box 16-byte aligned
+        make_map(&p->map_halo[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX + 16,
+                 ty + 6, 9, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2);
+        make_map(&p->map_ctr[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX, ty, 9,
+                 CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2);
+        continue;
+      }
       make_map(&p->map_halo[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX + 8, ty + 6, 9);
       make_map(&p->map_ctr[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX, ty, 9);
     }
-    make_map(&p->map_coef, p->coef, p->sx, p->nj + 6, p->nk + 6, p->ncoef, p->sz, p->sf, cgfd::TX, ty, p->ncoef);
-    CK(cgfd::tma_prepare(p->med));
+    if (p->coef_type == cgfd::COEF_F32)
+      make_map(&p->map_coef, p->coef, p->sx, p->nj + 6, p->nk + 6, p->ncoef, p->sz, p->sf, cgfd::TX, ty, p->ncoef);
+    else
+      make_map(&p->map_coef, p->coef16, p->sx, p->nj + 6, p->nk + 6, p->ncoef, p->sz, p->sf, cgfd::TX, ty, p->ncoef,
+               p->coef_type == cgfd::COEF_F16    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+               : p->coef_type == cgfd::COEF_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                 : CU_TENSOR_MAP_DATA_TYPE_UINT16,
+               2);
+    CK(cgfd::tma_prepare(p->med, p->coef_type, p->wave16));
   }
   // free surface
   if (p->free_top) {
@@ -484,7 +609,24 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   p->d_flag = dmalloc<int>(1, B);
   CK(cudaMemset(p->d_it, 0, sizeof(int)));
   CK(cudaMemset(p->d_flag, 0, sizeof(int)));
+  if (p->wave16) {
+    p->d_wsc = dmalloc<float>(18, B);
+    p->d_amax = dmalloc<unsigned int>(2, B);
+    CK(cudaMemset(p->d_wsc, 0, sizeof(float) * 18));
+    CK(cudaMemset(p->d_amax, 0, sizeof(unsigned int) * 2));  // the wavefield starts at zero
+    std::vector<float> sb = source_bounds(p);
+    p->d_srcb = dmalloc<float>(sb.size(), B);
+    CK(cudaMemcpy(p->d_srcb, sb.data(), sb.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
   CK(cudaDeviceSynchronize());
+}
+
+// FP16 stage levels: recompute max |w_pre| after the host replaced or re-labelled levels.
+void refresh_wave_max(cgfd_problem *p) {
+  if (!p->wave16) return;
+  CK(cudaMemsetAsync(p->d_amax, 0, sizeof(unsigned int) * 2, p->stream));
+  cgfd::launch_wave_absmax(p->wbuf[p->it & 1], p->sf, p->nshot, p->d_amax, p->stream);
+  CK(cudaGetLastError());
 }
 
 }  // namespace
@@ -583,6 +725,7 @@ int cgfd_set_step(cgfd_problem *p, int it) {
     }
     p->it = it;
     CK(cudaMemcpyAsync(p->d_it, &p->it, sizeof(int), cudaMemcpyHostToDevice, p->stream));
+    refresh_wave_max(p);
     CK(cudaStreamSynchronize(p->stream));
   });
 }
@@ -636,6 +779,7 @@ int cgfd_set_wavefield_shot(cgfd_problem *p, int shot, const float *in) {
     float *tmp = dmalloc<float>(g.siz_icmp, acc);
     float *pre = p->wbuf[p->it & 1] + (size_t)shot * 9 * p->sf;
     for (int c = 0; c < 9; c++) upload_field(p, in + (size_t)c * g.siz_icmp, pre + (size_t)c * p->sf, tmp, 0, 0);
+    refresh_wave_max(p);
     CK(cudaStreamSynchronize(p->stream));
     cudaFree(tmp);
   });
@@ -669,6 +813,10 @@ int cgfd_get_zchunk(const cgfd_problem *p) { return p ? p->nzc : -1; }
 int cgfd_set_bulk_variant(cgfd_problem *p, int tma) {
   if (!p) return CGFD_ERR_INVALID;
   if (!tma && p->nshot > 1) { set_err("the direct-load bulk kernel handles one shot"); return CGFD_ERR_UNSUPPORTED; }
+  if (!tma && p->precision != CGFD_PREC_FP32) {
+    set_err("the direct-load bulk kernel handles FP32 storage only");
+    return CGFD_ERR_UNSUPPORTED;
+  }
   p->use_tma = tma != 0;
   for (int s = 0; s < 8; s++)
     if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }

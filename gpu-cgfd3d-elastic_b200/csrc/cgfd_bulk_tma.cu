@@ -18,59 +18,51 @@
 
 namespace cgfd {
 
-template <int MED, int TYT>
+// Wave policies: stage input / next-stage output storage.
+//   WP 0: FP32 in, FP32 out (plain)      WP 1: FP32 in, FP16 out (stage 0 of FP16 mode)
+//   WP 2: FP16 in, FP16 out (stages 1-3 of FP16 mode; stage 3 has no stage output)
+template <int WP> struct WavePolicy {
+  using TW = typename std::conditional<WP == 2, __half, float>::type;
+  using TT = typename std::conditional<WP >= 1, __half, float>::type;
+};
+
+template <int MED, int TYT, typename TC, typename TW>
 struct BulkSmem {
-  static constexpr int WX = TX + 8;   // x box [-4, 36) around the tile
-  static constexpr int WY = TYT + 6;  // y box [-3, TYT+3)
+  static constexpr int XO = 16 / (int)sizeof(TW);  // x halo of the box: 16 bytes, TMA-aligned
+  static constexpr int WX = TX + 2 * XO;  // x box [-XO, 32+XO) around the tile
+  static constexpr int WY = TYT + 6;      // y box [-3, TYT+3)
   static constexpr int NC = MedInfo<MED>::NCOEF;
   static constexpr int CELLS = TX * TYT;
-  static constexpr int WAVE_FLOATS = 9 * WY * WX;
-  static constexpr int WAVE_SLOT = ((WAVE_FLOATS * 4 + 127) / 128) * 128;  // bytes
-  static constexpr int COEF_BYTES = NC * CELLS * 4;
+  static constexpr int WAVE_ELEMS = 9 * WY * WX;
+  static constexpr int WAVE_SLOT = ((WAVE_ELEMS * (int)sizeof(TW) + 127) / 128) * 128;  // bytes
+  static constexpr int COEF_BYTES = NC * CELLS * (int)sizeof(TC);  // multiple of 128 for every medium
   static constexpr int FLD_BYTES = 9 * CELLS * 4;
   static constexpr int CPE_SLOT = COEF_BYTES + 2 * FLD_BYTES;
   static constexpr int OFF_CPE = 3 * WAVE_SLOT;
   static constexpr int OFF_BAR = OFF_CPE + 2 * CPE_SLOT;
   static constexpr int BYTES = OFF_BAR + 8 * 8;
+  static_assert(COEF_BYTES % 128 == 0, "w_pre/w_end boxes must stay 128-byte aligned");
 };
 
-template <int MED>
-struct MediumS;
-template <>
-struct MediumS<MED_ISO> {
-  static __device__ __forceinline__ void load(Medium<MED_ISO> &m, const float *c, int stride) {
-    m.lam = c[(CF_MED + 0) * stride];
-    m.mu = c[(CF_MED + 1) * stride];
-    m.lam2mu = m.lam + 2.0f * m.mu;
-  }
-};
-template <>
-struct MediumS<MED_VTI> {
-  static __device__ __forceinline__ void load(Medium<MED_VTI> &m, const float *c, int stride) {
-    m.c11 = c[(CF_MED + 0) * stride];
-    m.c13 = c[(CF_MED + 1) * stride];
-    m.c33 = c[(CF_MED + 2) * stride];
-    m.c55 = c[(CF_MED + 3) * stride];
-    m.c66 = c[(CF_MED + 4) * stride];
-    m.c12 = m.c11 - 2.0f * m.c66;
-  }
-};
-template <>
-struct MediumS<MED_ANISO> {
-  static __device__ __forceinline__ void load(Medium<MED_ANISO> &m, const float *c, int stride) {
-#pragma unroll
-    for (int n = 0; n < 21; n++) m.c[n] = c[(CF_MED + n) * stride];
-  }
+// one cell's coefficients from a shared-memory tile (stride = cells per tile)
+template <typename TC, int STRIDE>
+struct CoefTile {
+  const TC *c;  // field 0 of this cell
+  const StageP &p;
+  __device__ __forceinline__ float operator()(int f) const { return coef_decode<TC>(c[f * STRIDE], p, f); }
 };
 
-template <int MED, int DX, int DY, int DZ, int TYT>
+template <int MED, int DX, int DY, int DZ, int TYT, typename TC, int WP>
 __global__ void __launch_bounds__(TX *TYT, 1)
     k_stage_bulk_tma(const __grid_constant__ StageP p, const __grid_constant__ TmaP tm, int nzc) {
-  using S = BulkSmem<MED, TYT>;
+  using TW = typename WavePolicy<WP>::TW;
+  using TT = typename WavePolicy<WP>::TT;
+  using S = BulkSmem<MED, TYT, TC, TW>;
   constexpr int LX = op_left(DX), LY = op_left(DY);
   constexpr int SD = DZ ? -1 : 1;  // march direction
   extern __shared__ __align__(128) unsigned char smem[];
-  float *wave = reinterpret_cast<float *>(smem);
+  __shared__ float s_wsc[18];  // FP16 stage levels: scale, inverse scale
+  TW *wave = reinterpret_cast<TW *>(smem);
   unsigned char *cpe = smem + S::OFF_CPE;
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + S::OFF_BAR);  // 0..2 wave, 3..4 cpe
 
@@ -87,21 +79,24 @@ __global__ void __launch_bounds__(TX *TYT, 1)
   const int k0 = SD > 0 ? kb : ke - 1;
   const long long sf = p.sf;
   const long long woff = (long long)shot * 9 * sf;
-  const float *__restrict__ cur = p.cur + woff;
-  float *__restrict__ tmp_out = p.tmp_out + woff;
+  const TW *__restrict__ cur = reinterpret_cast<const TW *>(p.cur) + woff;
+  TT *__restrict__ tmp_out = reinterpret_cast<TT *>(p.tmp_out) + woff;
   float *__restrict__ endw = p.end + woff;
   const int stage = p.stage;
   const bool need_pre = stage == 1 || stage == 2;
   const bool need_end = stage >= 1;
-  const uint32_t wave_bytes = S::WAVE_FLOATS * 4;
+  const uint32_t wave_bytes = S::WAVE_ELEMS * sizeof(TW);
   const uint32_t cpe_bytes = S::COEF_BYTES + (need_pre ? S::FLD_BYTES : 0) + (need_end ? S::FLD_BYTES : 0);
-  // box origins in device-layout coordinates (x multiple of 4: 16-byte aligned)
-  const int xw = GX + bx * TX - 4, yw = by * TYT;
+  // box origins in device-layout coordinates (x * element size a multiple of 16 bytes)
+  const int xw = GX + bx * TX - S::XO, yw = by * TYT;
   const int xc = GX + bx * TX, yc = 3 + by * TYT;
 
   if (tid == 0) {
     for (int b = 0; b < 5; b++) mbar_init(&bar[b], 1);
     fence_barrier_init();
+  }
+  if constexpr (WP != 0) {
+    if (tid < 18) s_wsc[tid] = p.wsc[tid];
   }
   __syncthreads();
 
@@ -109,7 +104,7 @@ __global__ void __launch_bounds__(TX *TYT, 1)
     const int kk = k0 + m * SD;
     uint64_t *b = &bar[m % 3];
     mbar_expect_tx(b, wave_bytes);
-    tma_load_4d(wave + (m % 3) * (S::WAVE_SLOT / 4), &tm.cur, xw, yw, kk + 3, 9 * shot, b);
+    tma_load_4d(wave + (m % 3) * (S::WAVE_SLOT / (int)sizeof(TW)), &tm.cur, xw, yw, kk + 3, 9 * shot, b);
   };
   auto issue_cpe = [&](int m) {
     const int kk = k0 + m * SD;
@@ -148,13 +143,14 @@ __global__ void __launch_bounds__(TX *TYT, 1)
     for (int m = 0; m < 3; m++) {
       const long long id = didx(p, i, j, k0 + (m - 3) * SD);
 #pragma unroll
-      for (int f = 0; f < 9; f++) q[f][m] = __ldg(cur + f * sf + id);
+      for (int f = 0; f < 9; f++) q[f][m] = to_f(__ldg(cur + f * sf + id));
     }
   }
-  const int wc = (ty + 3) * S::WX + tx + 4;  // centre of this thread in a wave slot (per field)
+  const int wc = (ty + 3) * S::WX + tx + S::XO;  // centre of this thread in a wave slot (per field)
   mbar_wait(&bar[0], 0, p.err);
 #pragma unroll
-  for (int f = 0; f < 9; f++) q[f][3] = wave[f * S::WY * S::WX + wc];
+  for (int f = 0; f < 9; f++) q[f][3] = to_f(wave[f * S::WY * S::WX + wc]);
+  float vmax = 0.f, smax = 0.f;  // FP16 mode, stage 3: max |w_end| of this thread
 
   const int cell = ty * TX + tx;
   for (int m = 0; m < n; m++) {
@@ -166,21 +162,21 @@ __global__ void __launch_bounds__(TX *TYT, 1)
     const int ws = m % 3, wn = (m + 1) % 3, cs = m & 1;
     mbar_wait(&bar[wn], ((m + 1) / 3) & 1, p.err);
     mbar_wait(&bar[3 + cs], (m >> 1) & 1, p.err);
-    const float *W = wave + ws * (S::WAVE_SLOT / 4);
-    const float *Wn = wave + wn * (S::WAVE_SLOT / 4);
+    const TW *W = wave + ws * (S::WAVE_SLOT / (int)sizeof(TW));
+    const TW *Wn = wave + wn * (S::WAVE_SLOT / (int)sizeof(TW));
 #pragma unroll
-    for (int f = 0; f < 9; f++) q[f][4] = Wn[f * S::WY * S::WX + wc];
+    for (int f = 0; f < 9; f++) q[f][4] = to_f(Wn[f * S::WY * S::WX + wc]);
 
     if (act) {
-      const float *Cc = reinterpret_cast<const float *>(cpe + cs * S::CPE_SLOT) + cell;
+      const CoefTile<TC, S::CELLS> Cc{reinterpret_cast<const TC *>(cpe + cs * S::CPE_SLOT) + cell, p};
       float mt[3][3];
 #pragma unroll
       for (int a = 0; a < 3; a++)
 #pragma unroll
-        for (int b = 0; b < 3; b++) mt[a][b] = Cc[(3 * a + b) * S::CELLS];
-      const float slw = Cc[CF_SLW * S::CELLS];
+        for (int b = 0; b < 3; b++) mt[a][b] = Cc(3 * a + b);
+      const float slw = Cc(CF_SLW);
       Medium<MED> md;
-      MediumS<MED>::load(md, Cc, S::CELLS);
+      md.load(Cc);
       CellAcc acc;
       acc.zero();
       // x
@@ -188,8 +184,9 @@ __global__ void __launch_bounds__(TX *TYT, 1)
         float d[9];
 #pragma unroll
         for (int f = 0; f < 9; f++) {
-          const float *r = W + f * S::WY * S::WX + (ty + 3) * S::WX + tx + 4 - LX;
-          d[f] = drp5<DX>(r[0], r[1], r[2], r[3], r[4]);
+          const TW *r = W + f * S::WY * S::WX + (ty + 3) * S::WX + tx + S::XO - LX;
+          d[f] = drp5<DX>(to_f(r[0]), to_f(r[1]), to_f(r[2]), to_f(r[3]), to_f(r[4]));
+          if constexpr (WP == 2) d[f] *= s_wsc[f];  // the operator is linear: scale once
         }
         acc.add_axis(mt[0], d, d + 3);
         if (fmask)
@@ -205,8 +202,9 @@ __global__ void __launch_bounds__(TX *TYT, 1)
         float d[9];
 #pragma unroll
         for (int f = 0; f < 9; f++) {
-          const float *r = W + f * S::WY * S::WX + (ty + 3 - LY) * S::WX + tx + 4;
-          d[f] = drp5<DY>(r[0], r[S::WX], r[2 * S::WX], r[3 * S::WX], r[4 * S::WX]);
+          const TW *r = W + f * S::WY * S::WX + (ty + 3 - LY) * S::WX + tx + S::XO;
+          d[f] = drp5<DY>(to_f(r[0]), to_f(r[S::WX]), to_f(r[2 * S::WX]), to_f(r[3 * S::WX]), to_f(r[4 * S::WX]));
+          if constexpr (WP == 2) d[f] *= s_wsc[f];
         }
         acc.add_axis(mt[1], d, d + 3);
         if (fmask)
@@ -221,9 +219,11 @@ __global__ void __launch_bounds__(TX *TYT, 1)
       {
         float d[9];
 #pragma unroll
-        for (int f = 0; f < 9; f++)
+        for (int f = 0; f < 9; f++) {
           d[f] = SD > 0 ? drp5<DZ>(q[f][0], q[f][1], q[f][2], q[f][3], q[f][4])
                         : drp5<DZ>(q[f][4], q[f][3], q[f][2], q[f][1], q[f][0]);
+          if constexpr (WP == 2) d[f] *= s_wsc[f];
+        }
         acc.add_axis(mt[2], d, d + 3);
         if (fmask)
           for (int fi = 0; fi < p.nface; fi++) {
@@ -248,18 +248,27 @@ __global__ void __launch_bounds__(TX *TYT, 1)
       if (stage == 0) {
 #pragma unroll
         for (int f = 0; f < 9; f++) {
-          tmp_out[f * sf + id] = q[f][3] + ca * h[f];
+          const float t = q[f][3] + ca * h[f];
+          tmp_out[f * sf + id] = from_f<TT>(WP != 0 ? t * s_wsc[9 + f] : t);
           endw[f * sf + id] = q[f][3] + cb * h[f];
         }
       } else if (stage < 3) {
 #pragma unroll
         for (int f = 0; f < 9; f++) {
-          tmp_out[f * sf + id] = PR[f * S::CELLS] + ca * h[f];
+          const float t = PR[f * S::CELLS] + ca * h[f];
+          tmp_out[f * sf + id] = from_f<TT>(WP != 0 ? t * s_wsc[9 + f] : t);
           endw[f * sf + id] = EN[f * S::CELLS] + cb * h[f];
         }
       } else {
 #pragma unroll
-        for (int f = 0; f < 9; f++) endw[f * sf + id] = EN[f * S::CELLS] + cb * h[f];
+        for (int f = 0; f < 9; f++) {
+          const float e = EN[f * S::CELLS] + cb * h[f];
+          endw[f * sf + id] = e;
+          if constexpr (WP == 2) {
+            if (f < 3) vmax = fmaxf(vmax, fabsf(e));
+            else smax = fmaxf(smax, fabsf(e));
+          }
+        }
       }
     }
 #pragma unroll
@@ -268,32 +277,44 @@ __global__ void __launch_bounds__(TX *TYT, 1)
       for (int m2 = 0; m2 < 4; m2++) q[f][m2] = q[f][m2 + 1];
     __syncthreads();
   }
+  if constexpr (WP == 2) {
+    if (stage == 3) {  // the next step's FP16 scale
+      for (int o = 16; o; o >>= 1) {
+        vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+        smax = fmaxf(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+      }
+      if (tx == 0) {
+        atomic_max_abs(&p.amax[0], vmax);
+        atomic_max_abs(&p.amax[1], smax);
+      }
+    }
+  }
 }
 
 // -----------------------------------------------------------------------------------------
-template <int MED, int TYT>
+template <int MED, int TYT, typename TC, int WP>
 static void launch_tma_med(const StageP &p, const TmaP &tm, int nzc, cudaStream_t st) {
-  using S = BulkSmem<MED, TYT>;
+  using S = BulkSmem<MED, TYT, TC, typename WavePolicy<WP>::TW>;
   const int code = p.dir[0] | (p.dir[1] << 1) | (p.dir[2] << 2);
   dim3 block(TX, TYT);
   dim3 grid(((p.ni + TX - 1) / TX) * p.nshot, (p.nj + TYT - 1) / TYT, (p.nbulk + nzc - 1) / nzc);
   switch (code) {
 #define CASE(c)                                                                                            \
   case c:                                                                                                  \
-    k_stage_bulk_tma<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, TYT><<<grid, block, S::BYTES, st>>>(p, tm, nzc); \
+    k_stage_bulk_tma<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, TYT, TC, WP><<<grid, block, S::BYTES, st>>>(p, tm, nzc); \
     break;
     CASE(0) CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7)
 #undef CASE
   }
 }
 
-template <int MED, int TYT>
+template <int MED, int TYT, typename TC, int WP>
 static cudaError_t set_attr_med() {
-  using S = BulkSmem<MED, TYT>;
+  using S = BulkSmem<MED, TYT, TC, typename WavePolicy<WP>::TW>;
   cudaError_t e = cudaSuccess;
 #define ATTR(c)                                                                                              \
   if (e == cudaSuccess)                                                                                      \
-    e = cudaFuncSetAttribute(k_stage_bulk_tma<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, TYT>,           \
+    e = cudaFuncSetAttribute(k_stage_bulk_tma<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, TYT, TC, WP>,   \
                              cudaFuncAttributeMaxDynamicSharedMemorySize, S::BYTES);
   ATTR(0) ATTR(1) ATTR(2) ATTR(3) ATTR(4) ATTR(5) ATTR(6) ATTR(7)
 #undef ATTR
@@ -302,17 +323,42 @@ static cudaError_t set_attr_med() {
 
 int tma_tile_y(int med) { return med == MED_ISO ? 16 : 8; }
 
-cudaError_t tma_prepare(int med) {
-  if (med == MED_ISO) return set_attr_med<MED_ISO, 16>();
-  if (med == MED_VTI) return set_attr_med<MED_VTI, 8>();
-  return set_attr_med<MED_ANISO, 8>();
+template <typename TC, int WP>
+static cudaError_t prepare_tc(int med) {
+  if (med == MED_ISO) return set_attr_med<MED_ISO, 16, TC, WP>();
+  if (med == MED_VTI) return set_attr_med<MED_VTI, 8, TC, WP>();
+  return set_attr_med<MED_ANISO, 8, TC, WP>();
 }
 
-int launch_stage_bulk_tma(int med, const StageP &p, const TmaP &tm, int nzc, cudaStream_t st) {
+cudaError_t tma_prepare(int med, int coef_type, int wave16) {
+  if (wave16) {
+    if (coef_type != COEF_U16) return cudaErrorInvalidValue;
+    cudaError_t e = prepare_tc<uint16_t, 1>(med);
+    return e == cudaSuccess ? prepare_tc<uint16_t, 2>(med) : e;
+  }
+  if (coef_type == COEF_U16) return prepare_tc<uint16_t, 0>(med);
+  if (coef_type == COEF_F16) return prepare_tc<__half, 0>(med);
+  if (coef_type == COEF_BF16) return prepare_tc<__nv_bfloat16, 0>(med);
+  return prepare_tc<float, 0>(med);
+}
+
+template <typename TC, int WP>
+static void launch_tc(int med, const StageP &p, const TmaP &tm, int nzc, cudaStream_t st) {
+  if (med == MED_ISO) launch_tma_med<MED_ISO, 16, TC, WP>(p, tm, nzc, st);
+  else if (med == MED_VTI) launch_tma_med<MED_VTI, 8, TC, WP>(p, tm, nzc, st);
+  else launch_tma_med<MED_ANISO, 8, TC, WP>(p, tm, nzc, st);
+}
+
+int launch_stage_bulk_tma(int med, int coef_type, int wave16, const StageP &p, const TmaP &tm, int nzc,
+                          cudaStream_t st) {
   if (p.nbulk <= 0) return 0;
-  if (med == MED_ISO) launch_tma_med<MED_ISO, 16>(p, tm, nzc, st);
-  else if (med == MED_VTI) launch_tma_med<MED_VTI, 8>(p, tm, nzc, st);
-  else launch_tma_med<MED_ANISO, 8>(p, tm, nzc, st);
+  if (wave16) {  // 16-bit fixed-point coefficients with FP16 stage levels
+    if (p.stage == 0) launch_tc<uint16_t, 1>(med, p, tm, nzc, st);
+    else launch_tc<uint16_t, 2>(med, p, tm, nzc, st);
+  } else if (coef_type == COEF_U16) launch_tc<uint16_t, 0>(med, p, tm, nzc, st);
+  else if (coef_type == COEF_F16) launch_tc<__half, 0>(med, p, tm, nzc, st);
+  else if (coef_type == COEF_BF16) launch_tc<__nv_bfloat16, 0>(med, p, tm, nzc, st);
+  else launch_tc<float, 0>(med, p, tm, nzc, st);
   return 1;
 }
 

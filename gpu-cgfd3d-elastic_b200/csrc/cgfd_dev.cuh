@@ -10,8 +10,12 @@
 #pragma once
 
 #include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <type_traits>
 
 namespace cgfd {
 
@@ -60,12 +64,15 @@ struct StageP {
   int dir[3];             // 0 backward, 1 forward (fd_t.cu:184-235)
   long long sx, sz, sf;   // row, plane and field strides of the device layout (floats)
   long long off0;         // offset of physical point (0,0,0)
-  const float *cur;       // wavefield read by the stencils (9 fields)
+  const float *cur;       // wavefield read by the stencils (9 fields); __half when the
+                          // FP16 stage levels are the input (stages 1-3)
   const float *pre;       // w_pre (stages 1-2)
-  float *tmp_out;         // next stage input (stages 0-2)
+  float *tmp_out;         // next stage input (stages 0-2); __half in FP16-stage mode
   float *end;             // accumulator (written at every stage)
   float ca, cb;           // rk_a[stage]*dt, rk_b[stage]*dt
-  const float *coef;      // [ncoef][sf]
+  const void *coef;       // [ncoef][sf] of float, __half or __nv_bfloat16
+  float cscale[32];       // 16-bit coefficients: value = cscale[f] * stored + coffset[f]
+  float coffset[32];
   const float *jac;       // [sf]
   const float *matx;      // free surface: [nj][ni][9] matVx2Vz (row-major 3x3)
   const float *maty;      //                [nj][ni][9] matVy2Vz
@@ -75,7 +82,15 @@ struct StageP {
   FaceP face[6];
   int *err;               // device error word (bit 1: pipeline wait timed out)
   int nshot;              // wavefields sharing this grid (batched sources); 1 = plain
+  // FP16 stage levels: wsc[0..8] scale (value = scale * stored), wsc[9..17] its inverse,
+  // fixed for one time step; amax[0..1] collects max |w| of the velocity / stress fields
+  // written at stage 3 (the next step's scale)
+  const float *wsc;
+  unsigned int *amax;
 };
+
+// max |w| groups of the FP16 stage levels: velocity (fields 0-2) and stress (3-8)
+__host__ __device__ constexpr int wgroup(int f) { return f < 3 ? 0 : 1; }
 
 // Tensor maps of the arrays one stage streams through TMA: the stage input (4-D box with
 // the x-y halo, all 9 fields), w_pre / w_end (centre boxes, 9 fields), coefficients.
@@ -114,9 +129,10 @@ struct Medium;
 template <>
 struct Medium<MED_ISO> {
   float lam, mu, lam2mu;
-  __device__ __forceinline__ void load(const float *coef, long long sf, long long idx) {
-    lam = __ldg(coef + (CF_MED + 0) * sf + idx);
-    mu = __ldg(coef + (CF_MED + 1) * sf + idx);
+  template <typename G>
+  __device__ __forceinline__ void load(G get) {  // get(c): coefficient field c at the cell
+    lam = get(CF_MED + 0);
+    mu = get(CF_MED + 1);
     lam2mu = lam + 2.0f * mu;
   }
   __device__ __forceinline__ void hooke(const float G[3][3], float h[6]) const {
@@ -132,12 +148,13 @@ struct Medium<MED_ISO> {
 template <>
 struct Medium<MED_VTI> {
   float c11, c12, c13, c33, c55, c66;
-  __device__ __forceinline__ void load(const float *coef, long long sf, long long idx) {
-    c11 = __ldg(coef + (CF_MED + 0) * sf + idx);
-    c13 = __ldg(coef + (CF_MED + 1) * sf + idx);
-    c33 = __ldg(coef + (CF_MED + 2) * sf + idx);
-    c55 = __ldg(coef + (CF_MED + 3) * sf + idx);
-    c66 = __ldg(coef + (CF_MED + 4) * sf + idx);
+  template <typename G>
+  __device__ __forceinline__ void load(G get) {
+    c11 = get(CF_MED + 0);
+    c13 = get(CF_MED + 1);
+    c33 = get(CF_MED + 2);
+    c55 = get(CF_MED + 3);
+    c66 = get(CF_MED + 4);
     c12 = c11 - 2.0f * c66;  // sv_curv_col_el_vti_gpu.cu:407
   }
   __device__ __forceinline__ void hooke(const float G[3][3], float h[6]) const {
@@ -153,9 +170,10 @@ struct Medium<MED_VTI> {
 template <>
 struct Medium<MED_ANISO> {
   float c[21];  // c11 c12 c13 c14 c15 c16 c22 .. c66 (upper triangle, row-major)
-  __device__ __forceinline__ void load(const float *coef, long long sf, long long idx) {
+  template <typename G>
+  __device__ __forceinline__ void load(G get) {
 #pragma unroll
-    for (int n = 0; n < 21; n++) c[n] = __ldg(coef + (CF_MED + n) * sf + idx);
+    for (int n = 0; n < 21; n++) c[n] = get(CF_MED + n);
   }
   __device__ __forceinline__ static constexpr int up(int a, int b) {
     // index of C[a][b] (a<=b) in the packed upper triangle
@@ -171,6 +189,42 @@ struct Medium<MED_ANISO> {
       for (int J = 1; J < 6; J++) s += C(I, J) * e[J];
       h[I] = s;
     }
+  }
+};
+
+// 16-bit storage: value = per-field scale x stored value (FP32 arithmetic)
+__device__ __forceinline__ float to_f(float x) { return x; }
+__device__ __forceinline__ float to_f(__half x) { return __half2float(x); }
+__device__ __forceinline__ float to_f(__nv_bfloat16 x) { return __bfloat162float(x); }
+__device__ __forceinline__ float to_f(uint16_t x) { return (float)x; }
+template <typename T>
+__device__ __forceinline__ T from_f(float x);
+template <>
+__device__ __forceinline__ float from_f<float>(float x) { return x; }
+template <>
+__device__ __forceinline__ __half from_f<__half>(float x) { return __float2half_rn(x); }
+
+// non-negative float maximum through the integer atomic (order of non-negative floats is
+// the order of their bit patterns)
+__device__ __forceinline__ void atomic_max_abs(unsigned int *a, float v) {
+  atomicMax(a, __float_as_uint(fabsf(v)));
+}
+
+// decode of one stored coefficient of field c
+template <typename TC>
+__device__ __forceinline__ float coef_decode(TC v, const StageP &p, int c) {
+  if constexpr (std::is_same<TC, float>::value) return v;
+  else return fmaf(p.cscale[c], to_f(v), p.coffset[c]);
+}
+
+template <typename TC>
+struct CoefView {
+  const TC *base;
+  long long stride;
+  const StageP &p;
+  __device__ __forceinline__ CoefView(const StageP &p_) : base(static_cast<const TC *>(p_.coef)), stride(p_.sf), p(p_) {}
+  __device__ __forceinline__ float operator()(int c, long long idx) const {
+    return coef_decode<TC>(__ldg(base + c * stride + idx), p, c);
   }
 };
 

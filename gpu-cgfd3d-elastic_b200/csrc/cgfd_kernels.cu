@@ -90,14 +90,15 @@ __global__ void __launch_bounds__(TX *TY, 2) k_stage_bulk(const __grid_constant_
 
     if (act) {
       const long long id = didx(p, i, j, k);
+      const CoefView<float> cv(p);
       float m[3][3];
 #pragma unroll
       for (int a = 0; a < 3; a++)
 #pragma unroll
-        for (int b = 0; b < 3; b++) m[a][b] = __ldg(p.coef + (3 * a + b) * sf + id);
-      const float slw = __ldg(p.coef + CF_SLW * sf + id);
+        for (int b = 0; b < 3; b++) m[a][b] = cv(3 * a + b, id);
+      const float slw = cv(CF_SLW, id);
       Medium<MED> md;
-      md.load(p.coef, sf, id);
+      md.load([&](int c) { return cv(c, id); });
       CellAcc acc;
       acc.zero();
       // ---- x
@@ -166,15 +167,33 @@ __global__ void __launch_bounds__(TX *TY, 2) k_stage_bulk(const __grid_constant_
 // -----------------------------------------------------------------------------------------
 // surface slab
 // -----------------------------------------------------------------------------------------
-__device__ __forceinline__ float ld5(int dir, const float *v, long long id, long long off, float (&o)[5]) {
+// Stage input of the surface kernel: FP32, or scaled FP16 (value = scale[f] * stored).
+template <typename TW>
+struct WaveIn {
+  const TW *w;
+  long long sf;
+  const float *sc;
+  __device__ __forceinline__ float operator()(int f, long long q) const {
+    const float v = to_f(__ldg(w + f * sf + q));
+    if constexpr (std::is_same<TW, float>::value) return v;
+    else return v * __ldg(sc + f);
+  }
+};
+
+template <typename TW>
+__device__ __forceinline__ void ld5(int dir, const WaveIn<TW> &cur, int f, long long id, long long off,
+                                    float (&o)[5]) {
   int L = op_left(dir);
 #pragma unroll
-  for (int n = 0; n < 5; n++) o[n] = __ldg(v + id + (n - L) * off);
-  return 0.f;
+  for (int n = 0; n < 5; n++) o[n] = cur(f, id + (n - L) * off);
 }
 
-template <int MED>
+// Surface slab: one thread per cell of the top NSURF planes. WP is the wave policy of the
+// bulk kernel (0 FP32 stage levels; 1 FP32 input, FP16 output; 2 FP16 input and output).
+template <int MED, typename TC, int WP>
 __global__ void __launch_bounds__(128) k_stage_surface(const __grid_constant__ StageP p) {
+  using TW = typename std::conditional<WP == 2, __half, float>::type;
+  using TT = typename std::conditional<WP >= 1, __half, float>::type;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= p.ni || j >= p.nj) return;
@@ -182,21 +201,22 @@ __global__ void __launch_bounds__(128) k_stage_surface(const __grid_constant__ S
   const int nslab = p.nk - p.nbulk;
   const int shot = blockIdx.z / nslab;
   const long long woff = (long long)shot * 9 * sf;
-  const float *__restrict__ cur = p.cur + woff;
+  const WaveIn<TW> cur{reinterpret_cast<const TW *>(p.cur) + woff, sf, p.wsc};
   const long long offs[3] = {1, p.sx, p.sz};
   const int nk2 = p.nk - 1;
 
   {
     const int k = p.nbulk + blockIdx.z % nslab;  // one thread per cell of the slab
     const long long id = didx(p, i, j, k);
+    const CoefView<TC> cv(p);
     float m[3][3];
 #pragma unroll
     for (int a = 0; a < 3; a++)
 #pragma unroll
-      for (int b = 0; b < 3; b++) m[a][b] = __ldg(p.coef + (3 * a + b) * sf + id);
-    const float slw = __ldg(p.coef + CF_SLW * sf + id);
+      for (int b = 0; b < 3; b++) m[a][b] = cv(3 * a + b, id);
+    const float slw = cv(CF_SLW, id);
     Medium<MED> md;
-    md.load(p.coef, sf, id);
+    md.load([&](int c) { return cv(c, id); });
 
     // normal derivatives of all 9 fields along the 3 axes
     float dv[3][3], dtt[3][6];
@@ -205,7 +225,7 @@ __global__ void __launch_bounds__(128) k_stage_surface(const __grid_constant__ S
 #pragma unroll
       for (int f = 0; f < 9; f++) {
         float v[5];
-        ld5(p.dir[a], cur + f * sf, id, offs[a], v);
+        ld5(p.dir[a], cur, f, id, offs[a], v);
         float d = drp5r(p.dir[a], v[0], v[1], v[2], v[3], v[4]);
         if (f < 3) dv[a][f] = d; else dtt[a][f - 3] = d;
       }
@@ -239,24 +259,21 @@ __global__ void __launch_bounds__(128) k_stage_surface(const __grid_constant__ S
         const int tr[3][3] = {{3, 8, 7}, {8, 4, 6}, {7, 6, 5}};
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-          const float *T1 = cur + tr[c][0] * sf, *T2 = cur + tr[c][1] * sf, *T3 = cur + tr[c][2] * sf;
+          const int f1 = tr[c][0], f2 = tr[c][1], f3 = tr[c][2];
           float vx[5], vy[5], vz[5];
 #pragma unroll
           for (int n = 0; n < 5; n++) {
             long long q = id + (n - LXo);
-            vx[n] = __ldg(p.jac + q) * (__ldg(p.coef + 0 * sf + q) * __ldg(T1 + q) + __ldg(p.coef + 1 * sf + q) * __ldg(T2 + q) +
-                                        __ldg(p.coef + 2 * sf + q) * __ldg(T3 + q));
+            vx[n] = __ldg(p.jac + q) * (cv(0, q) * cur(f1, q) + cv(1, q) * cur(f2, q) + cv(2, q) * cur(f3, q));
             q = id + (long long)(n - LYo) * p.sx;
-            vy[n] = __ldg(p.jac + q) * (__ldg(p.coef + 3 * sf + q) * __ldg(T1 + q) + __ldg(p.coef + 4 * sf + q) * __ldg(T2 + q) +
-                                        __ldg(p.coef + 5 * sf + q) * __ldg(T3 + q));
+            vy[n] = __ldg(p.jac + q) * (cv(3, q) * cur(f1, q) + cv(4, q) * cur(f2, q) + cv(5, q) * cur(f3, q));
             int off;
             float sgn;
             if (n < n_free) { off = n - LZo; sgn = 1.f; }
             else if (n == n_free) { off = 0; sgn = 0.f; }
             else { off = (n - LZo) - 2 * (n - n_free); sgn = -1.f; }
             q = id + (long long)off * p.sz;
-            float fz = __ldg(p.jac + q) * (__ldg(p.coef + 6 * sf + q) * __ldg(T1 + q) + __ldg(p.coef + 7 * sf + q) * __ldg(T2 + q) +
-                                           __ldg(p.coef + 8 * sf + q) * __ldg(T3 + q));
+            float fz = __ldg(p.jac + q) * (cv(6, q) * cur(f1, q) + cv(7, q) * cur(f2, q) + cv(8, q) * cur(f3, q));
             vz[n] = sgn * fz;
           }
           float DxTx = drp5r(p.dir[0], vx[0], vx[1], vx[2], vx[3], vx[4]);
@@ -281,14 +298,13 @@ __global__ void __launch_bounds__(128) k_stage_surface(const __grid_constant__ S
         } else {
 #pragma unroll
           for (int c = 0; c < 3; c++) {
-            const float *v = cur + c * sf;
             if (nl == 1) {  // 2nd order (fd_t.cu:82-85, 103-106)
-              dz[c] = dzr ? (-__ldg(v + id) + __ldg(v + id + p.sz)) : (-__ldg(v + id - p.sz) + __ldg(v + id));
+              dz[c] = dzr ? (-cur(c, id) + cur(c, id + p.sz)) : (-cur(c, id - p.sz) + cur(c, id));
             } else {        // 4th order (fd_t.cu:86-89, 107-110)
-              dz[c] = dzr ? (-7.0f / 6.0f * __ldg(v + id) + 8.0f / 6.0f * __ldg(v + id + p.sz) -
-                             1.0f / 6.0f * __ldg(v + id + 2 * p.sz))
-                          : (1.0f / 6.0f * __ldg(v + id - 2 * p.sz) - 8.0f / 6.0f * __ldg(v + id - p.sz) +
-                             7.0f / 6.0f * __ldg(v + id));
+              dz[c] = dzr ? (-7.0f / 6.0f * cur(c, id) + 8.0f / 6.0f * cur(c, id + p.sz) -
+                             1.0f / 6.0f * cur(c, id + 2 * p.sz))
+                          : (1.0f / 6.0f * cur(c, id - 2 * p.sz) - 8.0f / 6.0f * cur(c, id - p.sz) +
+                             7.0f / 6.0f * cur(c, id));
             }
           }
         }
@@ -311,10 +327,42 @@ __global__ void __launch_bounds__(128) k_stage_surface(const __grid_constant__ S
     }
 #pragma unroll
     for (int c = 0; c < 9; c++) h[c] += hc[c];
-    float cc[9];
+    if constexpr (WP == 0) {
+      float cc[9];
 #pragma unroll
-    for (int f = 0; f < 9; f++) cc[f] = __ldg(cur + f * sf + id);
-    rk_store(p.stage, p.ca, p.cb, sf, id, cc, h, p.pre + woff, p.tmp_out ? p.tmp_out + woff : nullptr, p.end + woff);
+      for (int f = 0; f < 9; f++) cc[f] = cur(f, id);
+      rk_store(p.stage, p.ca, p.cb, sf, id, cc, h, p.pre + woff, p.tmp_out ? p.tmp_out + woff : nullptr, p.end + woff);
+    } else {
+      // FP16 stage levels: the RK combine of rk_store with the stage output scaled to FP16
+      TT *tout = reinterpret_cast<TT *>(p.tmp_out) + woff;
+      float *endw = p.end + woff;
+      const float *prw = p.pre + woff;
+      if (p.stage == 0) {
+#pragma unroll
+        for (int f = 0; f < 9; f++) {
+          const float c0 = cur(f, id);
+          tout[f * sf + id] = from_f<TT>((c0 + p.ca * h[f]) * __ldg(p.wsc + 9 + f));
+          endw[f * sf + id] = c0 + p.cb * h[f];
+        }
+      } else if (p.stage < 3) {
+#pragma unroll
+        for (int f = 0; f < 9; f++) {
+          tout[f * sf + id] = from_f<TT>((__ldg(prw + f * sf + id) + p.ca * h[f]) * __ldg(p.wsc + 9 + f));
+          endw[f * sf + id] = endw[f * sf + id] + p.cb * h[f];
+        }
+      } else {
+        float vmax = 0.f, smax = 0.f;
+#pragma unroll
+        for (int f = 0; f < 9; f++) {
+          const float e = endw[f * sf + id] + p.cb * h[f];
+          endw[f * sf + id] = e;
+          if (f < 3) vmax = fmaxf(vmax, fabsf(e));
+          else smax = fmaxf(smax, fabsf(e));
+        }
+        atomic_max_abs(&p.amax[0], vmax);
+        atomic_max_abs(&p.amax[1], smax);
+      }
+    }
   }
 }
 
@@ -336,8 +384,12 @@ __global__ void k_source(const __grid_constant__ SrcP s) {
     float h;
     if (c < 3) { if (!s.force) continue; h = v[c] * wv; }
     else { if (!s.moment) continue; h = -v[c] * wt; }
-    if (s.stage < 3) atomicAdd(s.tmp_out + c * s.sf + id, s.ca * h);
-    atomicAdd(s.end + c * s.sf + id, s.cb * h);
+    if (s.stage < 3) {
+      if (s.wave16) atomicAdd(reinterpret_cast<__half *>(s.tmp_out) + c * s.sf + id, __float2half_rn(s.ca * h * s.wsc[9 + c]));
+      else atomicAdd(s.tmp_out + c * s.sf + id, s.ca * h);
+    }
+    const float old = atomicAdd(s.end + c * s.sf + id, s.cb * h);
+    if (s.wave16 && s.stage == 3) atomic_max_abs(&s.amax[wgroup(c)], old + s.cb * h);
   }
 }
 
@@ -419,14 +471,185 @@ int launch_stage_bulk(int med, const StageP &p, int nzc, cudaStream_t st) {
   return 1;
 }
 
-int launch_stage_surface(int med, const StageP &p, cudaStream_t st) {
+template <typename TC, int WP>
+static void launch_surface_tc(int med, const StageP &p, dim3 grid, dim3 block, cudaStream_t st) {
+  if (med == MED_ISO) k_stage_surface<MED_ISO, TC, WP><<<grid, block, 0, st>>>(p);
+  else if (med == MED_VTI) k_stage_surface<MED_VTI, TC, WP><<<grid, block, 0, st>>>(p);
+  else k_stage_surface<MED_ANISO, TC, WP><<<grid, block, 0, st>>>(p);
+}
+
+int launch_stage_surface(int med, int coef_type, int wave16, const StageP &p, cudaStream_t st) {
   if (p.nbulk >= p.nk) return 0;
   dim3 block(32, 4);
   dim3 grid((p.ni + 31) / 32, (p.nj + 3) / 4, (p.nk - p.nbulk) * p.nshot);
-  if (med == MED_ISO) k_stage_surface<MED_ISO><<<grid, block, 0, st>>>(p);
-  else if (med == MED_VTI) k_stage_surface<MED_VTI><<<grid, block, 0, st>>>(p);
-  else k_stage_surface<MED_ANISO><<<grid, block, 0, st>>>(p);
+  if (wave16) {
+    if (p.stage == 0) launch_surface_tc<uint16_t, 1>(med, p, grid, block, st);
+    else launch_surface_tc<uint16_t, 2>(med, p, grid, block, st);
+  } else if (coef_type == COEF_U16) launch_surface_tc<uint16_t, 0>(med, p, grid, block, st);
+  else if (coef_type == COEF_F16) launch_surface_tc<__half, 0>(med, p, grid, block, st);
+  else if (coef_type == COEF_BF16) launch_surface_tc<__nv_bfloat16, 0>(med, p, grid, block, st);
+  else launch_surface_tc<float, 0>(med, p, grid, block, st);
   return 1;
+}
+
+// Scale of the FP16 stage levels for this step: max |w| at the step's start (collected by
+// the last step's stage 3) and the largest source increment of this step, mapped by a power
+// of two into [2^12, 2^13); FP16 then holds 8x-16x growth within the step before its
+// largest finite value. Then clears the collector for this step's stage 3.
+__global__ void k_wave_scale(unsigned int *amax, const float *srcb, const int *d_it, int nt_total, float *wsc) {
+  const int g = threadIdx.x;
+  if (g >= 2) return;
+  const int it = *d_it;
+  float m = __uint_as_float(amax[g]);
+  if (srcb && it >= 0 && it < nt_total) m = fmaxf(m, srcb[2 * it + g]);
+  int e = 0;
+  if (m > 0.f && m <= 3.0e38f) {
+    e = (int)((__float_as_uint(m) >> 23) & 0xff) - 127 - 12;  // exponent of m (m normal)
+    if (m < 1.1754944e-38f) e = -126 - 12;
+  }
+  e = max(-100, min(100, e));
+  const float sc = __uint_as_float((unsigned)(e + 127) << 23), inv = __uint_as_float((unsigned)(127 - e) << 23);
+  for (int f = g ? 3 : 0; f < (g ? 9 : 3); f++) {
+    wsc[f] = sc;
+    wsc[9 + f] = inv;
+  }
+  amax[g] = 0u;
+}
+
+int launch_wave_scale(unsigned int *amax, const float *srcb, const int *d_it, int nt_total, float *wsc,
+                      cudaStream_t st) {
+  k_wave_scale<<<1, 32, 0, st>>>(amax, srcb, d_it, nt_total, wsc);
+  return 1;
+}
+
+__global__ void k_wave_absmax(const float *__restrict__ w, long long sf, int nshot, unsigned int *amax) {
+  const long long n = (long long)nshot * 9 * sf;
+  float vm = 0.f, sm = 0.f;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int f = (int)((t / sf) % 9);
+    if (f < 3) vm = fmaxf(vm, fabsf(w[t]));
+    else sm = fmaxf(sm, fabsf(w[t]));
+  }
+  for (int o = 16; o; o >>= 1) {
+    vm = fmaxf(vm, __shfl_xor_sync(0xffffffffu, vm, o));
+    sm = fmaxf(sm, __shfl_xor_sync(0xffffffffu, sm, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_abs(&amax[0], vm);
+    atomic_max_abs(&amax[1], sm);
+  }
+}
+
+void launch_wave_absmax(const float *w, long long sf, int nshot, unsigned int *amax, cudaStream_t st) {
+  k_wave_absmax<<<1184, 256, 0, st>>>(w, sf, nshot, amax);
+}
+
+// Convert one FP32 coefficient field to 16 bits (value = scale * stored + offset) by
+// stochastic rounding: each cell rounds up or down with the probabilities that make the
+// stored value exact on average, the draw a fixed hash of (field, cell). Round-to-nearest
+// would give every cell of a homogeneous layer the same error, i.e. a systematic shift of
+// the layer's wave speed whose phase error grows with travel time; stochastic rounding
+// leaves zero-mean cell-scale noise that the wave averages over a wavelength.
+__device__ __forceinline__ unsigned int mix32(unsigned int h) {  // murmur3 finaliser
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+
+template <typename TC>
+__global__ void k_coef_to16(const float *__restrict__ src, TC *__restrict__ dst, long long n, float scale,
+                            float offset, unsigned int field) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const unsigned int hsh = mix32((unsigned int)t ^ mix32((unsigned int)(t >> 32) + 0x9e3779b9u * (field + 1)));
+    const float u = (float)(hsh >> 8) * (1.0f / 16777216.0f);  // [0, 1)
+    if constexpr (std::is_same<TC, uint16_t>::value) {
+      // fixed point over the field's [min, max]; cells outside it (padding) clamp
+      const float q = (src[t] - offset) / scale;
+      float fl = floorf(q);
+      if (u < q - fl) fl += 1.f;
+      dst[t] = (uint16_t)fminf(fmaxf(fl, 0.f), 65535.f);
+    } else {
+      const float v = src[t] / scale;
+      TC lo;
+      if constexpr (std::is_same<TC, __half>::value) lo = __float2half_rz(v);
+      else lo = __float2bfloat16_rz(v);
+      const float flo = to_f(lo);
+      if (flo != v && isfinite(v)) {
+        TC hi;
+        unsigned short bits;
+        memcpy(&bits, &lo, 2);
+        bits += 1;  // next representable value away from zero (sign-magnitude)
+        memcpy(&hi, &bits, 2);
+        const float fhi = to_f(hi);
+        if (u < (v - flo) / (fhi - flo)) lo = hi;
+      }
+      dst[t] = lo;
+    }
+  }
+}
+
+// order-preserving key of a float (unsigned compare of keys = float compare)
+__device__ __forceinline__ unsigned int fkey(float f) {
+  const unsigned int b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+float coef_key_to_float(unsigned int k) {
+  unsigned int b = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+  float f;
+  memcpy(&f, &b, 4);
+  return f;
+}
+
+__global__ void k_coef_minmax(const float *__restrict__ src, int ni, int nj, int nk, long long sx, long long sz,
+                              long long off0, unsigned int *out) {
+  const int nx = ni + 6, ny = nj + 6;
+  const long long n = (long long)nx * ny * (nk + 6);
+  unsigned int mn = 0xffffffffu, mx = 0u;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nx) - 3, j = (int)((t / nx) % ny) - 3, k = (int)(t / ((long long)nx * ny)) - 3;
+    const unsigned int key = fkey(src[off0 + (long long)k * sz + (long long)j * sx + i]);
+    mn = min(mn, key);
+    mx = max(mx, key);
+  }
+  for (int o = 16; o; o >>= 1) {
+    mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&out[0], mn);
+    atomicMax(&out[1], mx);
+  }
+}
+
+void launch_coef_minmax(const float *src, int ni, int nj, int nk, long long sx, long long sz, long long off0,
+                        unsigned int *out, cudaStream_t st) {
+  k_coef_minmax<<<592, 256, 0, st>>>(src, ni, nj, nk, sx, sz, off0, out);
+}
+
+__global__ void k_absmax(const float *__restrict__ src, long long n, unsigned int *out) {
+  float m = 0.f;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    m = fmaxf(m, fabsf(src[t]));
+  for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));  // non-negative floats order as uints
+}
+
+void launch_absmax(const float *src, long long n, unsigned int *out, cudaStream_t st) {
+  k_absmax<<<592, 256, 0, st>>>(src, n, out);
+}
+
+void launch_coef_to16(int coef_type, const float *src, void *dst, long long n, float scale, float offset, int field,
+                      cudaStream_t st) {
+  if (coef_type == COEF_U16)
+    k_coef_to16<uint16_t><<<1184, 256, 0, st>>>(src, (uint16_t *)dst, n, scale, offset, field);
+  else if (coef_type == COEF_F16)
+    k_coef_to16<__half><<<1184, 256, 0, st>>>(src, (__half *)dst, n, scale, offset, field);
+  else
+    k_coef_to16<__nv_bfloat16><<<1184, 256, 0, st>>>(src, (__nv_bfloat16 *)dst, n, scale, offset, field);
 }
 
 int launch_source(const SrcP &s, cudaStream_t st) {

@@ -8,6 +8,10 @@ namespace cgfd {
 struct StageP;
 struct TmaP;
 
+// storage type of the coefficient array
+// (16-bit types: value = scale * stored + offset, one scale/offset per field)
+enum { COEF_F32 = 0, COEF_F16 = 1, COEF_BF16 = 2, COEF_U16 = 3 };
+
 // Source injection of one stage (sv_curv_col_el_gpu.cu:227-301), applied to tmp/end.
 struct SrcP {
   int nsrc, max_ext, max_nt;
@@ -21,10 +25,13 @@ struct SrcP {
   const float *ext_wt;         // [nsrc][max_ext] coef / jac
   const float *stf;            // [nsrc][max_nt][4][9]: fx fy fz mxx myy mzz myz mxz mxy
   const int *src_shot;         // [nsrc] wavefield (shot) each source acts on
-  float *tmp_out;
+  float *tmp_out;              // __half when wave16
   float *end;
   long long sf;
   const int *d_it;
+  int wave16;                  // FP16 stage levels: tmp_out holds scaled __half
+  const float *wsc;            // [18] scale / inverse scale of this step (wave16)
+  unsigned int *amax;          // [2] max |w_end| per group, collected at stage 3 (wave16)
 };
 
 // Station sampling of w_pre (io_funcs.cu:1624-1666).
@@ -43,11 +50,27 @@ struct RecvP {
 
 // Each launcher returns the number of kernels it launched (0 or 1).
 int launch_stage_bulk(int med, const StageP &p, int nzc, cudaStream_t st);
-int launch_stage_surface(int med, const StageP &p, cudaStream_t st);
+int launch_stage_surface(int med, int coef_type, int wave16, const StageP &p, cudaStream_t st);
 // TMA-pipelined bulk kernel: tile height, one-time function attributes, launch.
+// wave16: FP16 stage levels (requires COEF_F16).
 int tma_tile_y(int med);
-cudaError_t tma_prepare(int med);
-int launch_stage_bulk_tma(int med, const StageP &p, const TmaP &tm, int nzc, cudaStream_t st);
+cudaError_t tma_prepare(int med, int coef_type, int wave16);
+int launch_stage_bulk_tma(int med, int coef_type, int wave16, const StageP &p, const TmaP &tm, int nzc,
+                          cudaStream_t st);
+// FP16 stage levels: per-step scale from the last step's max |w| and the step's source bound
+int launch_wave_scale(unsigned int *amax, const float *srcb, const int *d_it, int nt_total, float *wsc,
+                      cudaStream_t st);
+// max |w| of the velocity / stress groups over `nshot` wavefields into amax[2]
+void launch_wave_absmax(const float *w, long long sf, int nshot, unsigned int *amax, cudaStream_t st);
+// 16-bit coefficient storage
+void launch_absmax(const float *src, long long n, unsigned int *out, cudaStream_t st);
+// min / max of one field over the cells any kernel reads (physical box + 3 ghosts per side),
+// as order-preserving keys out[0] (min), out[1] (max); decode with coef_key_to_float
+void launch_coef_minmax(const float *src, int ni, int nj, int nk, long long sx, long long sz, long long off0,
+                        unsigned int *out, cudaStream_t st);
+float coef_key_to_float(unsigned int key);
+void launch_coef_to16(int coef_type, const float *src, void *dst, long long n, float scale, float offset, int field,
+                      cudaStream_t st);
 int launch_source(const SrcP &s, cudaStream_t st);
 int launch_recv(const RecvP &r, cudaStream_t st);
 int launch_advance(int *d_it, cudaStream_t st);

@@ -51,10 +51,16 @@ extern "C" {
 #define CGFD_WAVELET_GAUSSIAN_DERIV 3
 #define CGFD_WAVELET_KLAUDER        4
 
-/* storage precision of the device state (computation is always FP32) */
-#define CGFD_PREC_FP32       0  /* everything FP32 (the reference's arithmetic)            */
-#define CGFD_PREC_BF16_COEF  1  /* metrics/Jacobian/medium as scaled BF16, wavefield FP32   */
-#define CGFD_PREC_FP16_WAVE  2  /* scaled BF16 coefficients + FP16 wavefield with FP32 sum  */
+/* Storage precision of the device state; arithmetic is FP32 in every mode. The 16-bit
+   coefficient modes store the 9 metric fields, 1/rho and the moduli (the Jacobian, read only
+   at the free surface, stays FP32) with one scale and offset per field, stochastically
+   rounded (zero-mean per-cell error, so a homogeneous layer keeps its wave speed). */
+#define CGFD_PREC_FP32       0  /* everything FP32 (the reference's arithmetic)              */
+#define CGFD_PREC_BF16_COEF  1  /* coefficients BF16 (power-of-two scale), wavefield FP32     */
+#define CGFD_PREC_FP16_COEF  2  /* coefficients FP16 (power-of-two scale), wavefield FP32     */
+#define CGFD_PREC_U16_COEF   3  /* coefficients 16-bit fixed point over each field's range    */
+#define CGFD_PREC_FP16_WAVE  4  /* U16 coefficients + RK stage wavefields FP16 (dynamic per-
+                                   step scale); the solution levels stay FP32                */
 
 /* status codes */
 #define CGFD_OK               0
