@@ -14,6 +14,8 @@ import numpy as np
 CGFD_MEDIUM_ELASTIC_ISO = 2
 CGFD_MEDIUM_ELASTIC_VTI = 3
 CGFD_MEDIUM_ELASTIC_ANISO = 4
+CGFD_ERR_BUSY = -7
+CGFD_ERR_NOMEM = -3
 CGFD_PREC_FP32 = 0
 CGFD_PREC_BF16_COEF = 1
 CGFD_PREC_FP16_COEF = 2
@@ -170,6 +172,43 @@ class Problem:
         return d
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("hbm_budget", C.c_size_t), ("max_active", C.c_int), ("max_batch", C.c_int),
+                ("steps_per_slice", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("failed", C.c_longlong),
+                ("pending", C.c_longlong), ("active", C.c_longlong), ("batches", C.c_longlong),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
+                ("cell_stages_per_s", C.c_double), ("source_steps_per_s", C.c_double),
+                ("hbm_budget", C.c_size_t), ("hbm_in_use", C.c_size_t), ("hbm_peak", C.c_size_t)]
+
+
+def problem_bytes(problem, shots=None):
+    """(resident, peak) device bytes a Simulation(problem, shots) will hold (no device call)."""
+    d = problem.desc()
+    keep = []
+
+    def arr(a, dt):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=dt)
+        keep.append(a)
+        return a
+    sd = None
+    n = 1
+    if shots is not None:
+        sd = (SourceDesc * len(shots))()
+        for k, s in enumerate(shots):
+            _fill_src(sd[k], s, arr)
+        n = len(shots)
+    r, pk = C.c_size_t(), C.c_size_t()
+    check(lib().cgfd_problem_bytes(C.byref(d), n, C.addressof(sd) if sd is not None else None, C.byref(r),
+                                   C.byref(pk)))
+    return int(r.value), int(pk.value)
+
+
 def _fill_src(ds, s, arr):
     ds.num = s.num
     ds.stf_given, ds.stf_length = s.stf_given, s.stf_length
@@ -228,6 +267,14 @@ def lib():
         "cgfd_metric_calc": (C.c_int, [C.c_int, C.c_int, C.c_int, P, P]),
         "cgfd_dt_estimate": (C.c_int, [C.POINTER(ProblemDesc), C.c_double, C.POINTER(C.c_double)]),
         "cgfd_keep_three_digits": (C.c_double, [C.c_double]),
+        "cgfd_problem_bytes": (C.c_int, [C.POINTER(ProblemDesc), C.c_int, P, C.POINTER(C.c_size_t),
+                                         C.POINTER(C.c_size_t)]),
+        "cgfd_server_create": (C.c_int, [C.POINTER(ServerOpts), C.POINTER(P)]),
+        "cgfd_server_submit": (C.c_int, [P, C.POINTER(ProblemDesc), C.POINTER(C.c_longlong)]),
+        "cgfd_server_poll": (C.c_int, [P, C.c_longlong, P, C.POINTER(C.c_int)]),
+        "cgfd_server_wait": (C.c_int, [P, C.c_longlong, C.c_double]),
+        "cgfd_server_get_stats": (C.c_int, [P, C.POINTER(ServerStats)]),
+        "cgfd_server_destroy": (C.c_int, [P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -360,3 +407,66 @@ class Simulation:
     @property
     def stream(self):
         return lib().cgfd_stream(self.h)
+
+
+class Server:
+    """Serving loop on one GPU (cgfd_server_*): submit problems, poll/wait for seismograms.
+    The model arrays of a submitted problem must stay alive until its request completes;
+    Server keeps a reference to each submitted description until its result is taken."""
+
+    def __init__(self, device=0, hbm_budget=0, max_active=4, max_batch=8, steps_per_slice=50):
+        o = ServerOpts(int(device), int(hbm_budget), int(max_active), int(max_batch), int(steps_per_slice))
+        h = C.c_void_p()
+        check(lib().cgfd_server_create(C.byref(o), C.byref(h)))
+        self.h = h
+        self._live = {}
+
+    def submit(self, problem):
+        d = problem.desc()
+        rid = C.c_longlong()
+        check(lib().cgfd_server_submit(self.h, C.byref(d), C.byref(rid)))
+        self._live[rid.value] = (d, problem)
+        return rid.value
+
+    def poll(self, rid):
+        """None while queued/running; the [nsta, 9, nt_total] seismograms once done."""
+        nsta = C.c_int()
+        rc = lib().cgfd_server_poll(self.h, rid, None, C.byref(nsta))
+        if rc == CGFD_ERR_BUSY:
+            return None
+        check(rc)
+        p = self._live[rid][1]
+        out = np.zeros((nsta.value, 9, p.nt_total), np.float32)
+        check(lib().cgfd_server_poll(self.h, rid, out.ctypes.data, C.byref(nsta)))
+        del self._live[rid]
+        return out
+
+    def wait(self, rid, timeout=-1.0):
+        rc = lib().cgfd_server_wait(self.h, rid, float(timeout))
+        if rc == CGFD_ERR_BUSY:
+            return None
+        check(rc)
+        return self.poll(rid)
+
+    def stats(self):
+        st = ServerStats()
+        check(lib().cgfd_server_get_stats(self.h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if self.h:
+            lib().cgfd_server_destroy(self.h)
+            self.h = None
+            self._live.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -246,7 +246,8 @@ struct cgfd_problem {
       r.pre = wbuf[step & 1]; r.sf = sf; r.seis = d_seis; r.d_it = d_it; r.d_flag = d_flag;
       n += timed(6, [&] { return cgfd::launch_recv(r, st); });
     }
-    if (wave16) n += timed(7, [&] { return cgfd::launch_wave_scale(d_amax, d_srcb, d_it, nt_total, d_wsc, st); });
+    if (wave16)
+      n += timed(7, [&] { return cgfd::launch_wave_scale(d_amax, d_srcb, d_it, nt_total, nshot, d_wsc, st); });
     for (int s = 0; s < 4; s++) {
       cgfd::StageP p = stage_params(step, s);
       if (use_tma) {
@@ -387,11 +388,69 @@ void to_16bit_coefficients(cgfd_problem *p) {
   p->bytes -= sizeof(float) * p->ncoef * p->sf;
 }
 
-// Largest source increment added to an RK stage input in each step, per group (velocity:
-// forces, stress: moments): max over sources, stages 0-2 and spread points of
-// |rk_a[s] dt * value * weight|. Part of the FP16 stage-level scale of that step.
+// Device layout [k][j][i] of one field: rows padded to 32 floats with the physical x origin
+// at GX (128-byte aligned rows), 3 ghost rows/planes in y/z, fields 256-byte aligned.
+void layout(int ni, int nj, int nk, long long &sx, long long &sz, long long &sf, long long &off0) {
+  sx = ((cgfd::GX + ni + 3 + 31) / 32) * 32;
+  sz = sx * (nj + 6);
+  sf = ((sz * (nk + 6) + 63) / 64) * 64;
+  off0 = 3 * sz + 3 * sx + cgfd::GX;
+}
+
+// Device bytes build() holds once done (*resident) and at its high-water mark (*peak), from
+// the description alone (host work only: PML, source and station setup).
+void problem_bytes(const cgfd_problem_desc *d, int nshot, const cgfd_source_desc *shots, size_t *resident,
+                   size_t *peak) {
+  cgfd::validate_desc(d);
+  if (nshot < 1) throw cgfd::Error(CGFD_ERR_INVALID, "nshot must be >= 1");
+  long long sx, sz, sf, off0;
+  layout(d->ni, d->nj, d->nk, sx, sz, sf, off0);
+  const int ncoef = d->medium_type == CGFD_MEDIUM_ELASTIC_ISO ? 12 : (d->medium_type == CGFD_MEDIUM_ELASTIC_VTI ? 15 : 31);
+  const bool c16 = d->precision != CGFD_PREC_FP32, w16 = d->precision == CGFD_PREC_FP16_WAVE;
+  const size_t F = sizeof(float);
+  const size_t waves = (size_t)9 * sf * nshot * (2 * F + 2 * (w16 ? 2 : F));
+  const size_t coef32 = (size_t)ncoef * sf * F, coef16 = (size_t)ncoef * sf * 2, jac = (size_t)sf * F;
+  const size_t stage_buf = (size_t)(d->ni + 6) * (d->nj + 6) * (d->nk + 6) * F;
+  size_t r = waves + (c16 ? coef16 : coef32) + jac;
+  const size_t high = waves + jac + coef32 + (c16 ? std::max(stage_buf, coef16 + 8 * (size_t)ncoef) : stage_buf);
+  if (d->free_top) r += (size_t)2 * 9 * d->ni * d->nj * F;
+  cgfd::PmlFaceHost fh[3][2];
+  cgfd::pml_setup(d, fh);
+  for (int a = 0; a < 3; a++)
+    for (int s = 0; s < 2; s++) {
+      if (!fh[a][s].enable) continue;
+      const cgfd::PmlFaceHost &h = fh[a][s];
+      const size_t n = (size_t)(h.hi[0] - h.lo[0] + 1) * (h.hi[1] - h.lo[1] + 1) * (h.hi[2] - h.lo[2] + 1);
+      r += 3 * h.A.size() * F + (size_t)3 * 9 * n * nshot * F;
+    }
+  size_t nsrc = 0, max_ext = 0, max_nt = 0;
+  for (int sh = 0; sh < (shots ? nshot : 1); sh++) {
+    cgfd_problem_desc ds = *d;
+    if (shots) ds.src = shots[sh];
+    cgfd::SrcHost q;
+    cgfd::validate_desc(&ds);
+    cgfd::src_setup(&ds, q);
+    nsrc += q.nsrc;
+    max_ext = std::max(max_ext, (size_t)q.max_ext);
+    max_nt = std::max(max_nt, (size_t)q.max_nt);
+  }
+  if (nsrc > 0) r += nsrc * 3 * sizeof(int) + nsrc * max_ext * (sizeof(long long) + 2 * F) + nsrc * max_nt * 36 * F;
+  cgfd::RecvHost rec;
+  cgfd::recv_setup(d, rec);
+  if (rec.n > 0)
+    r += (size_t)rec.n * 8 * (sizeof(long long) + F) + (size_t)rec.n * 9 * d->nt_total * nshot * F;
+  r += 2 * sizeof(int);
+  if (w16) r += (size_t)nshot * (18 * F + 2 * sizeof(unsigned int) + (size_t)d->nt_total * 2 * F);
+  if (resident) *resident = r;
+  if (peak) *peak = std::max(r, high);
+}
+
+// Largest source increment added to an RK stage input in each step, per shot and group
+// (velocity: forces, stress: moments): max over the shot's sources, stages 0-2 and spread
+// points of |rk_a[s] dt * value * weight|; [nt_total][nshot][2]. Part of the FP16
+// stage-level scale of that step.
 std::vector<float> source_bounds(const cgfd_problem *p) {
-  std::vector<float> sb((size_t)p->nt_total * 2, 0.f);
+  std::vector<float> sb((size_t)p->nt_total * p->nshot * 2, 0.f);
   const cgfd::SrcHost &s = p->src;
   for (int is = 0; is < s.nsrc; is++) {
     float wv = 0.f, wt = 0.f;
@@ -409,7 +468,7 @@ std::vector<float> source_bounds(const cgfd_problem *p) {
           if (c < 3 && !s.force) continue;
           if (c >= 3 && !s.moment) continue;
           const float b = ca * std::fabs(v[c]) * (c < 3 ? wv : wt);
-          float &o = sb[(size_t)it * 2 + (c < 3 ? 0 : 1)];
+          float &o = sb[((size_t)it * p->nshot + p->src_shot[is]) * 2 + (c < 3 ? 0 : 1)];
           o = std::max(o, b);
         }
       }
@@ -443,10 +502,7 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   p->free_top = d->free_top ? 1 : 0;
   if (p->free_top && p->nk < cgfd::NSURF + 4) throw cgfd::Error(CGFD_ERR_INVALID, "nk too small for the free surface");
   // device layout
-  p->sx = ((cgfd::GX + p->ni + 3 + 31) / 32) * 32;
-  p->sz = p->sx * (p->nj + 6);
-  p->sf = ((p->sz * (p->nk + 6) + 63) / 64) * 64;
-  p->off0 = 3 * p->sz + 3 * p->sx + cgfd::GX;
+  layout(p->ni, p->nj, p->nk, p->sx, p->sz, p->sf, p->off0);
   // z planes per bulk block: ~32 keeps the per-chunk prologue (3 planes) small and gives
   // enough blocks to fill 148 SMs many times over (cgfd_set_zchunk / the autotuner refine it)
   {
@@ -610,10 +666,10 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   CK(cudaMemset(p->d_it, 0, sizeof(int)));
   CK(cudaMemset(p->d_flag, 0, sizeof(int)));
   if (p->wave16) {
-    p->d_wsc = dmalloc<float>(18, B);
-    p->d_amax = dmalloc<unsigned int>(2, B);
-    CK(cudaMemset(p->d_wsc, 0, sizeof(float) * 18));
-    CK(cudaMemset(p->d_amax, 0, sizeof(unsigned int) * 2));  // the wavefield starts at zero
+    p->d_wsc = dmalloc<float>(18 * (size_t)nshot, B);
+    p->d_amax = dmalloc<unsigned int>(2 * (size_t)nshot, B);
+    CK(cudaMemset(p->d_wsc, 0, sizeof(float) * 18 * nshot));
+    CK(cudaMemset(p->d_amax, 0, sizeof(unsigned int) * 2 * nshot));  // the wavefield starts at zero
     std::vector<float> sb = source_bounds(p);
     p->d_srcb = dmalloc<float>(sb.size(), B);
     CK(cudaMemcpy(p->d_srcb, sb.data(), sb.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -624,18 +680,26 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
 // FP16 stage levels: recompute max |w_pre| after the host replaced or re-labelled levels.
 void refresh_wave_max(cgfd_problem *p) {
   if (!p->wave16) return;
-  CK(cudaMemsetAsync(p->d_amax, 0, sizeof(unsigned int) * 2, p->stream));
+  CK(cudaMemsetAsync(p->d_amax, 0, sizeof(unsigned int) * 2 * p->nshot, p->stream));
   cgfd::launch_wave_absmax(p->wbuf[p->it & 1], p->sf, p->nshot, p->d_amax, p->stream);
   CK(cudaGetLastError());
 }
 
 }  // namespace
 
+void cgfd::set_last_error(const std::string &m) { set_err(m); }
+
 extern "C" {
 
 int cgfd_version(void) { return 100; }
 
 const char *cgfd_last_error(void) { return g_err.c_str(); }
+
+int cgfd_problem_bytes(const cgfd_problem_desc *desc, int nshot, const cgfd_source_desc *shots, size_t *resident,
+                       size_t *peak) {
+  if (!desc) { set_err("desc is NULL"); return CGFD_ERR_INVALID; }
+  return guarded([&] { problem_bytes(desc, nshot, shots, resident, peak); });
+}
 
 int cgfd_problem_create(const cgfd_problem_desc *desc, cgfd_problem **out) {
   if (!out) { set_err("out is NULL"); return CGFD_ERR_INVALID; }

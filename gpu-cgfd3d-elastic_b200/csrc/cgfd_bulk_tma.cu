@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(TX *TYT, 1)
     fence_barrier_init();
   }
   if constexpr (WP != 0) {
-    if (tid < 18) s_wsc[tid] = p.wsc[tid];
+    if (tid < 18) s_wsc[tid] = p.wsc[shot * 18 + tid];  // this shot's scale
   }
   __syncthreads();
 
@@ -284,8 +284,8 @@ __global__ void __launch_bounds__(TX *TYT, 1)
         smax = fmaxf(smax, __shfl_xor_sync(0xffffffffu, smax, o));
       }
       if (tx == 0) {
-        atomic_max_abs(&p.amax[0], vmax);
-        atomic_max_abs(&p.amax[1], smax);
+        atomic_max_abs(&p.amax[2 * shot + 0], vmax);
+        atomic_max_abs(&p.amax[2 * shot + 1], smax);
       }
     }
   }

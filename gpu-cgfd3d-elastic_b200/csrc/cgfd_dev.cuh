@@ -82,9 +82,9 @@ struct StageP {
   FaceP face[6];
   int *err;               // device error word (bit 1: pipeline wait timed out)
   int nshot;              // wavefields sharing this grid (batched sources); 1 = plain
-  // FP16 stage levels: wsc[0..8] scale (value = scale * stored), wsc[9..17] its inverse,
-  // fixed for one time step; amax[0..1] collects max |w| of the velocity / stress fields
-  // written at stage 3 (the next step's scale)
+  // FP16 stage levels, per shot s: wsc[18s + 0..8] scale (value = scale * stored),
+  // wsc[18s + 9..17] its inverse, fixed for one time step; amax[2s + 0..1] collects max |w|
+  // of the velocity / stress fields written at stage 3 (the next step's scale)
   const float *wsc;
   unsigned int *amax;
 };

@@ -201,7 +201,8 @@ __global__ void __launch_bounds__(128) k_stage_surface(const __grid_constant__ S
   const int nslab = p.nk - p.nbulk;
   const int shot = blockIdx.z / nslab;
   const long long woff = (long long)shot * 9 * sf;
-  const WaveIn<TW> cur{reinterpret_cast<const TW *>(p.cur) + woff, sf, p.wsc};
+  const float *wsc = p.wsc + shot * 18;  // FP16 stage levels: this shot's scale
+  const WaveIn<TW> cur{reinterpret_cast<const TW *>(p.cur) + woff, sf, wsc};
   const long long offs[3] = {1, p.sx, p.sz};
   const int nk2 = p.nk - 1;
 
@@ -341,13 +342,13 @@ __global__ void __launch_bounds__(128) k_stage_surface(const __grid_constant__ S
 #pragma unroll
         for (int f = 0; f < 9; f++) {
           const float c0 = cur(f, id);
-          tout[f * sf + id] = from_f<TT>((c0 + p.ca * h[f]) * __ldg(p.wsc + 9 + f));
+          tout[f * sf + id] = from_f<TT>((c0 + p.ca * h[f]) * __ldg(wsc + 9 + f));
           endw[f * sf + id] = c0 + p.cb * h[f];
         }
       } else if (p.stage < 3) {
 #pragma unroll
         for (int f = 0; f < 9; f++) {
-          tout[f * sf + id] = from_f<TT>((__ldg(prw + f * sf + id) + p.ca * h[f]) * __ldg(p.wsc + 9 + f));
+          tout[f * sf + id] = from_f<TT>((__ldg(prw + f * sf + id) + p.ca * h[f]) * __ldg(wsc + 9 + f));
           endw[f * sf + id] = endw[f * sf + id] + p.cb * h[f];
         }
       } else {
@@ -359,8 +360,8 @@ __global__ void __launch_bounds__(128) k_stage_surface(const __grid_constant__ S
           if (f < 3) vmax = fmaxf(vmax, fabsf(e));
           else smax = fmaxf(smax, fabsf(e));
         }
-        atomic_max_abs(&p.amax[0], vmax);
-        atomic_max_abs(&p.amax[1], smax);
+        atomic_max_abs(&p.amax[2 * shot + 0], vmax);
+        atomic_max_abs(&p.amax[2 * shot + 1], smax);
       }
     }
   }
@@ -377,7 +378,8 @@ __global__ void k_source(const __grid_constant__ SrcP s) {
   const int ib = s.it_begin[is];
   if (it < ib || it > ib + s.max_nt - 1) return;
   const float *v = s.stf + (((long long)is * s.max_nt + (it - ib)) * 4 + s.stage) * 9;
-  const long long id = s.ext_idx[(long long)is * s.max_ext + e] + (long long)s.src_shot[is] * 9 * s.sf;
+  const int shot = s.src_shot[is];
+  const long long id = s.ext_idx[(long long)is * s.max_ext + e] + (long long)shot * 9 * s.sf;
   const float wv = s.ext_wv[(long long)is * s.max_ext + e];
   const float wt = s.ext_wt[(long long)is * s.max_ext + e];
   for (int c = 0; c < 9; c++) {
@@ -385,11 +387,12 @@ __global__ void k_source(const __grid_constant__ SrcP s) {
     if (c < 3) { if (!s.force) continue; h = v[c] * wv; }
     else { if (!s.moment) continue; h = -v[c] * wt; }
     if (s.stage < 3) {
-      if (s.wave16) atomicAdd(reinterpret_cast<__half *>(s.tmp_out) + c * s.sf + id, __float2half_rn(s.ca * h * s.wsc[9 + c]));
+      if (s.wave16)
+        atomicAdd(reinterpret_cast<__half *>(s.tmp_out) + c * s.sf + id, __float2half_rn(s.ca * h * s.wsc[18 * shot + 9 + c]));
       else atomicAdd(s.tmp_out + c * s.sf + id, s.ca * h);
     }
     const float old = atomicAdd(s.end + c * s.sf + id, s.cb * h);
-    if (s.wave16 && s.stage == 3) atomic_max_abs(&s.amax[wgroup(c)], old + s.cb * h);
+    if (s.wave16 && s.stage == 3) atomic_max_abs(&s.amax[2 * shot + wgroup(c)], old + s.cb * h);
   }
 }
 
@@ -496,12 +499,16 @@ int launch_stage_surface(int med, int coef_type, int wave16, const StageP &p, cu
 // the last step's stage 3) and the largest source increment of this step, mapped by a power
 // of two into [2^12, 2^13); FP16 then holds 8x-16x growth within the step before its
 // largest finite value. Then clears the collector for this step's stage 3.
-__global__ void k_wave_scale(unsigned int *amax, const float *srcb, const int *d_it, int nt_total, float *wsc) {
-  const int g = threadIdx.x;
-  if (g >= 2) return;
+// One scale per shot and group: shots of a batch round exactly as when run alone.
+__global__ void k_wave_scale(unsigned int *amax, const float *srcb, const int *d_it, int nt_total, int nshot,
+                             float *wsc_all) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 2 * nshot) return;
+  const int shot = t >> 1, g = t & 1;
+  float *wsc = wsc_all + 18 * shot;
   const int it = *d_it;
-  float m = __uint_as_float(amax[g]);
-  if (srcb && it >= 0 && it < nt_total) m = fmaxf(m, srcb[2 * it + g]);
+  float m = __uint_as_float(amax[t]);
+  if (srcb && it >= 0 && it < nt_total) m = fmaxf(m, srcb[((long long)it * nshot + shot) * 2 + g]);
   int e = 0;
   if (m > 0.f && m <= 3.0e38f) {
     e = (int)((__float_as_uint(m) >> 23) & 0xff) - 127 - 12;  // exponent of m (m normal)
@@ -513,17 +520,17 @@ __global__ void k_wave_scale(unsigned int *amax, const float *srcb, const int *d
     wsc[f] = sc;
     wsc[9 + f] = inv;
   }
-  amax[g] = 0u;
+  amax[t] = 0u;
 }
 
-int launch_wave_scale(unsigned int *amax, const float *srcb, const int *d_it, int nt_total, float *wsc,
+int launch_wave_scale(unsigned int *amax, const float *srcb, const int *d_it, int nt_total, int nshot, float *wsc,
                       cudaStream_t st) {
-  k_wave_scale<<<1, 32, 0, st>>>(amax, srcb, d_it, nt_total, wsc);
+  k_wave_scale<<<(2 * nshot + 127) / 128, 128, 0, st>>>(amax, srcb, d_it, nt_total, nshot, wsc);
   return 1;
 }
 
-__global__ void k_wave_absmax(const float *__restrict__ w, long long sf, int nshot, unsigned int *amax) {
-  const long long n = (long long)nshot * 9 * sf;
+__global__ void k_wave_absmax(const float *__restrict__ w, long long sf, unsigned int *amax) {
+  const long long n = 9 * sf;
   float vm = 0.f, sm = 0.f;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const int f = (int)((t / sf) % 9);
@@ -541,7 +548,7 @@ __global__ void k_wave_absmax(const float *__restrict__ w, long long sf, int nsh
 }
 
 void launch_wave_absmax(const float *w, long long sf, int nshot, unsigned int *amax, cudaStream_t st) {
-  k_wave_absmax<<<1184, 256, 0, st>>>(w, sf, nshot, amax);
+  for (int s = 0; s < nshot; s++) k_wave_absmax<<<1184, 256, 0, st>>>(w + (size_t)s * 9 * sf, sf, amax + 2 * s);
 }
 
 // Convert one FP32 coefficient field to 16 bits (value = scale * stored + offset) by

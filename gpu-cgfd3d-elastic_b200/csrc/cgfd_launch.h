@@ -30,8 +30,8 @@ struct SrcP {
   long long sf;
   const int *d_it;
   int wave16;                  // FP16 stage levels: tmp_out holds scaled __half
-  const float *wsc;            // [18] scale / inverse scale of this step (wave16)
-  unsigned int *amax;          // [2] max |w_end| per group, collected at stage 3 (wave16)
+  const float *wsc;            // [nshot][18] scale / inverse scale of this step (wave16)
+  unsigned int *amax;          // [nshot][2] max |w_end| per group, collected at stage 3 (wave16)
 };
 
 // Station sampling of w_pre (io_funcs.cu:1624-1666).
@@ -58,9 +58,9 @@ cudaError_t tma_prepare(int med, int coef_type, int wave16);
 int launch_stage_bulk_tma(int med, int coef_type, int wave16, const StageP &p, const TmaP &tm, int nzc,
                           cudaStream_t st);
 // FP16 stage levels: per-step scale from the last step's max |w| and the step's source bound
-int launch_wave_scale(unsigned int *amax, const float *srcb, const int *d_it, int nt_total, float *wsc,
+int launch_wave_scale(unsigned int *amax, const float *srcb, const int *d_it, int nt_total, int nshot, float *wsc,
                       cudaStream_t st);
-// max |w| of the velocity / stress groups over `nshot` wavefields into amax[2]
+// max |w| of the velocity / stress groups of each of `nshot` wavefields into amax[nshot][2]
 void launch_wave_absmax(const float *w, long long sf, int nshot, unsigned int *amax, cudaStream_t st);
 // 16-bit coefficient storage
 void launch_absmax(const float *src, long long n, unsigned int *out, cudaStream_t st);

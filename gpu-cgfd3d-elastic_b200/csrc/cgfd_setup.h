@@ -60,4 +60,7 @@ void recv_setup(const cgfd_problem_desc *d, RecvHost &r);
 
 void validate_desc(const cgfd_problem_desc *d);
 
+// message returned by cgfd_last_error() on this thread
+void set_last_error(const std::string &m);
+
 }  // namespace cgfd

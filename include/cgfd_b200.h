@@ -206,6 +206,15 @@ int cgfd_set_wavefield_shot(cgfd_problem *p, int shot, const float *in);
 /* Device bytes held by the problem. */
 size_t cgfd_device_bytes(const cgfd_problem *p);
 
+/*
+ * Device bytes cgfd_batch_create(desc, nshot, shots) (shots NULL and nshot 1: the plain
+ * cgfd_problem_create) will hold once built (*resident, = cgfd_device_bytes) and at its
+ * high-water mark during the build (*peak); host work only, no device call.
+ * No counterpart in the reference.
+ */
+int cgfd_problem_bytes(const cgfd_problem_desc *desc, int nshot, const cgfd_source_desc *shots,
+                       size_t *resident, size_t *peak);
+
 /* Release all device and host state. Replaces: drv_rk_curv_col.cu:546-556. */
 int cgfd_problem_destroy(cgfd_problem *p);
 
@@ -239,10 +248,57 @@ int cgfd_set_timing(cgfd_problem *p, int on);
 
 /*
  * Accumulated kernel times (ms[8]) and launch counts (count[8]) for the kernel kinds
- * {bulk stage of RK stage 0, 1, 2, 3, surface slab, source, stations, unused}, and the
+ * {bulk stage of RK stage 0, 1, 2, 3, surface slab, source, stations, FP16 stage scale}, and the
  * number of kernels the library launched (*launches); reset != 0 clears them.
  */
 int cgfd_get_timing(cgfd_problem *p, double *ms, long long *count, long long *launches, int reset);
+
+/* ---- serving ------------------------------------------------------------------------- */
+/*
+ * A request loop on one GPU (no counterpart in the reference, which runs one simulation per
+ * process). Requests are forward simulations of any grid size, medium type and precision,
+ * each with its own sources; a scheduler thread admits them in submission order whenever a
+ * slot and the HBM budget allow (sized by cgfd_problem_bytes), builds queued requests that
+ * share a grid (same coord/metric/medium arrays, boundaries, time stepping, stations and
+ * precision) as ONE batched problem, and advances every resident problem in slices of
+ * time steps on its own stream, so admitted work overlaps on the device and a new request
+ * starts while others are mid-run. Results are bitwise those of the request run alone.
+ * The caller's coord/metric/medium arrays must stay valid until the request completes
+ * (sources and stations are copied at submit).
+ */
+typedef struct cgfd_server cgfd_server;
+
+typedef struct cgfd_server_opts {
+  int    device;            /* CUDA device ordinal of every request                          */
+  size_t hbm_budget;        /* device bytes the server may hold; 0: 85% of free memory       */
+  int    max_active;        /* resident problems (streams) at once; <= 0: 4                  */
+  int    max_batch;         /* same-grid requests per batched problem; <= 0: 8               */
+  int    steps_per_slice;   /* time steps enqueued per problem per scheduling pass; <= 0: 50 */
+} cgfd_server_opts;
+
+typedef struct cgfd_server_stats {
+  long long submitted, completed, failed, pending, active, batches;
+  double    p50_ms, p99_ms, mean_ms;      /* submit -> results ready, completed requests      */
+  double    cell_stages_per_s;          /* completed grid-cell x RK-stage updates per second
+                                           between the first admission and the last result  */
+  double    source_steps_per_s;         /* completed source x time steps per second          */
+  size_t    hbm_budget, hbm_in_use, hbm_peak;
+} cgfd_server_stats;
+
+int cgfd_server_create(const cgfd_server_opts *opts, cgfd_server **out);
+/* Validate and queue one request; *request_id identifies it. */
+int cgfd_server_submit(cgfd_server *s, const cgfd_problem_desc *desc, long long *request_id);
+/*
+ * CGFD_ERR_BUSY while queued or running; CGFD_OK when done (*nsta stations; with seismo_out
+ * non-NULL the [nsta][9][nt_total] seismograms are copied there and the request's results are
+ * released); the request's error code if it failed (cgfd_last_error() says why).
+ */
+int cgfd_server_poll(cgfd_server *s, long long request_id, float *seismo_out, int *nsta);
+/* Block until the request finishes (timeout_s < 0: no limit); CGFD_ERR_BUSY on timeout. */
+int cgfd_server_wait(cgfd_server *s, long long request_id, double timeout_s);
+int cgfd_server_get_stats(cgfd_server *s, cgfd_server_stats *out);
+/* Stop the scheduler: queued requests fail with CGFD_ERR_BUSY, device state is released. */
+int cgfd_server_destroy(cgfd_server *s);
 
 /* ---- grid helpers (host, FP64) ------------------------------------------------------- */
 

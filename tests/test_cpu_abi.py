@@ -115,3 +115,30 @@ def test_null_arguments():
     assert L.cgfd_problem_create(None, None) == -1
     assert L.cgfd_run(None, 1) == -1
     assert L.cgfd_problem_destroy(None) == 0
+
+
+def test_problem_bytes_on_host():
+    """cgfd_problem_bytes needs no device: it grows with the batch and shrinks with 16-bit
+    storage."""
+    import dataclasses
+    from cgfd_b200 import problem_bytes, synth, CGFD_PREC_U16_COEF, CGFD_PREC_FP16_WAVE
+    p = small_problem("iso", nsrc=0)
+    rng = np.random.default_rng(0)
+    shots = [synth.dc_sources(p.coord, p.ni, p.nj, 1, rng, depth_range=(600.0, 1200.0), stf_length=p.nt_total * p.dt)
+             for _ in range(3)]
+    one, _ = problem_bytes(dataclasses.replace(p, src=shots[0]))
+    three, _ = problem_bytes(p, shots)
+    assert three > one
+    u16, _ = problem_bytes(dataclasses.replace(p, src=shots[0], precision=CGFD_PREC_U16_COEF))
+    w16, _ = problem_bytes(dataclasses.replace(p, src=shots[0], precision=CGFD_PREC_FP16_WAVE))
+    assert w16 < u16 < one
+
+
+def test_server_without_gpu_fails_cleanly():
+    from conftest import gpu_available
+    from cgfd_b200 import Server, CgfdError
+    if gpu_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(CgfdError) as e:
+        Server()
+    assert e.value.code == -2

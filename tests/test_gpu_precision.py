@@ -87,8 +87,8 @@ def test_precision_storage_sizes():
 
 
 def test_fp16_wave_batched_vs_fp64():
-    """The batched mixed-precision form: 3 shots in one FP16_WAVE batch, each against its own
-    FP64 oracle run."""
+    """The batched mixed-precision form: 3 shots in one FP16_WAVE batch, each bitwise equal to
+    its solo FP16_WAVE run and within the bar of its own FP64 oracle run."""
     p = small_problem("iso", ni=48, nj=44, nk=36, nsteps=200, npml=6, nsrc=0, sta_grid=(3, 3), seed=3)
     rng = np.random.default_rng(21)
     shots = [synth.dc_sources(p.coord, p.ni, p.nj, 1, rng, depth_range=(700.0, 1500.0), fc_range=(2.5, 4.0),
@@ -97,9 +97,13 @@ def test_fp16_wave_batched_vs_fp64():
     b = Simulation(p, shots=shots)
     b.run()
     bs = b.seismograms()
-    p.precision = CGFD_PREC_FP32
     for n, s in enumerate(shots):
         p.src = s
+        p.precision = CGFD_PREC_FP16_WAVE
+        solo = Simulation(p)  # per-shot FP16 scales: a shot rounds as it does alone
+        solo.run()
+        assert np.array_equal(solo.seismograms(), bs[n])
+        p.precision = CGFD_PREC_FP32
         o = Oracle(p, fp64=True)
         o.run()
         e = seismo_errors(bs[n], o.seismograms())
