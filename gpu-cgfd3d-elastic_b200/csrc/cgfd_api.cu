@@ -834,6 +834,81 @@ int cgfd_get_wavefield_shot(cgfd_problem *p, int shot, float *out) {
 
 int cgfd_get_wavefield(cgfd_problem *p, float *out) { return cgfd_get_wavefield_shot(p, 0, out); }
 
+}  // extern "C"
+
+// ---- wavefield read-back without device allocation -------------------------------------
+// cgfd_get_wavefield_shot stages the whole wavefield in a temporary device buffer
+// (cudaMalloc + cudaFree). Some callers cannot afford that: a serving process that keeps the
+// device filled to its memory budget with resident problems (the temporary may not fit, and
+// failing a snapshot for lack of memory is not acceptable), and a caller reading a snapshot
+// while other problems run on other streams (cudaFree waits for the whole device). This
+// variant stages through one fixed static device array instead, a few z planes at a time.
+namespace {
+
+constexpr size_t kNoAllocScratchFloats = (size_t)1 << 20;  // 4 MiB: one chunk of reference planes
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocScratchFloats];
+std::mutex g_noalloc_mu;
+float *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// planes [kr0, kr0 + nplanes) of one field in the reference layout (3 ghosts, 0 there)
+__global__ void k_repack_out_planes(const float *__restrict__ src, float *__restrict__ dst, int ni, int nj, int nk,
+                                    long long sx, long long sz, long long off0, int kr0, int nplanes) {
+  const long long nxr = ni + 6, nyr = nj + 6;
+  const long long total = nxr * nyr * nplanes;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int ir = (int)(t % nxr), jr = (int)((t / nxr) % nyr), kr = kr0 + (int)(t / (nxr * nyr));
+    const int i = ir - 3, j = jr - 3, k = kr - 3;
+    const bool inner = i >= 0 && i < ni && j >= 0 && j < nj && k >= 0 && k < nk;
+    dst[t] = inner ? src[off0 + (long long)k * sz + (long long)j * sx + i] : 0.0f;
+  }
+}
+
+// Device address of the scratch array on `device` (current): looked up once per device.
+float *noalloc_scratch(int device) {
+  if (device < 0 || device >= kNoAllocMaxDevices) throw cgfd::Error(CGFD_ERR_INVALID, "device ordinal out of range");
+  std::lock_guard<std::mutex> g(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    float *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr)
+      throw cgfd::Error(CGFD_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    g_noalloc_ptr[device] = ptr;
+  }
+  return g_noalloc_ptr[device];
+}
+
+}  // namespace
+
+extern "C" {
+
+int cgfd_get_wavefield_shot_noalloc(cgfd_problem *p, int shot, float *out) {
+  if (!p || !out || shot < 0 || shot >= p->nshot) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
+  return guarded([&] {
+    const size_t nxr = (size_t)p->ni + 6, nyr = (size_t)p->nj + 6, nzr = (size_t)p->nk + 6;
+    const size_t plane = nxr * nyr;
+    if (plane > kNoAllocScratchFloats)
+      throw cgfd::Error(CGFD_ERR_INVALID, "one reference-layout plane (" + std::to_string(plane) +
+                                              " floats) exceeds the no-allocation scratch of " +
+                                              std::to_string(kNoAllocScratchFloats) + " floats");
+    CK(cudaSetDevice(p->device));
+    float *scratch = noalloc_scratch(p->device);
+    const int per = (int)(kNoAllocScratchFloats / plane);
+    const float *pre = p->wbuf[p->it & 1] + (size_t)shot * 9 * p->sf;
+    for (int c = 0; c < 9; c++)
+      for (int k0 = 0; k0 < (int)nzr; k0 += per) {
+        const int np = std::min(per, (int)nzr - k0);
+        // stream order keeps the copy of one chunk ahead of the kernel that refills the scratch
+        k_repack_out_planes<<<592, 256, 0, p->stream>>>(pre + (size_t)c * p->sf, scratch, p->ni, p->nj, p->nk, p->sx,
+                                                         p->sz, p->off0, k0, np);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out + (size_t)c * plane * nzr + (size_t)k0 * plane, scratch, (size_t)np * plane * sizeof(float),
+                           cudaMemcpyDeviceToHost, p->stream));
+      }
+    CK(cudaStreamSynchronize(p->stream));
+  });
+}
+
 int cgfd_set_wavefield_shot(cgfd_problem *p, int shot, const float *in) {
   if (!p || !in || shot < 0 || shot >= p->nshot) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
   return guarded([&] {

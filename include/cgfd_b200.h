@@ -203,6 +203,21 @@ int cgfd_set_wavefield(cgfd_problem *p, const float *in);
 int cgfd_get_wavefield_shot(cgfd_problem *p, int shot, float *out);
 int cgfd_set_wavefield_shot(cgfd_problem *p, int shot, const float *in);
 
+/*
+ * Same result as cgfd_get_wavefield_shot, but allocates no device memory: the repack goes
+ * through one static 4 MiB device array (2^20 floats) shared by every call, a chunk of
+ * reference-layout z planes at a time. For callers that cannot allocate: a server holding the
+ * device at its memory budget, or a snapshot taken while other streams keep running (the
+ * temporary buffer's cudaFree would wait for the whole device). Limit: one plane,
+ * (ni+6)*(nj+6) floats, must fit the array; larger grids get CGFD_ERR_INVALID. Nothing in the
+ * array needs to start at zero (each chunk is fully written before it is copied). Calls that
+ * overlap on one device (other threads, other problems) race on the shared array and must
+ * be serialised by the caller. The first call on a device looks up the array's address there
+ * and should come before any stream capture starts.
+ * No counterpart in the reference.
+ */
+int cgfd_get_wavefield_shot_noalloc(cgfd_problem *p, int shot, float *out);
+
 /* Device bytes held by the problem. */
 size_t cgfd_device_bytes(const cgfd_problem *p);
 
