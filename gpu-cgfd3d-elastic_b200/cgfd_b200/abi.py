@@ -398,7 +398,7 @@ class Simulation:
         cnt = np.zeros(8, np.int64)
         tot = C.c_longlong()
         check(lib().cgfd_get_timing(self.h, ms.ctypes.data, cnt.ctypes.data, C.addressof(tot), int(reset)))
-        kinds = ("bulk_s0", "bulk_s1", "bulk_s2", "bulk_s3", "surface", "source", "recv")
+        kinds = ("bulk_s0", "bulk_s1", "bulk_s2", "bulk_s3", "surface", "source", "recv", "wave_scale")
         out = {k: (float(ms[n]), int(cnt[n])) for n, k in enumerate(kinds)}
         out["bulk"] = (float(ms[:4].sum()), int(cnt[:4].sum()))
         out["launches"] = int(tot.value)

@@ -112,6 +112,9 @@ struct cgfd_problem {
   // d_wsc[18] from d_amax[2] (max |w| of velocity / stress) and d_srcb[nt_total][2] (largest
   // source increment of each step)
   int wave16 = 0;
+  // TMA bulk kernel tile lists for the current z chunk (interior tiles, then PML tiles)
+  int *d_tiles = nullptr;
+  cgfd::BulkTiles tiles;
   float *d_wsc = nullptr, *d_srcb = nullptr;
   unsigned int *d_amax = nullptr;
 
@@ -144,7 +147,7 @@ struct cgfd_problem {
   int graph_launches[8] = {};
 
   // per-kernel CUDA-event timing (direct launches only): kinds 0-3 bulk stage 0..3,
-  // 4 surface slab, 5 source, 6 stations
+  // 4 surface slab, 5 source, 6 stations, 7 FP16 stage scale
   bool timing = false;
   std::vector<cudaEvent_t> ev_free;
   struct TimedLaunch { int kind; cudaEvent_t a, b; };
@@ -258,7 +261,7 @@ struct cgfd_problem {
         tm.pre = map_ctr[pre];
         tm.end = map_ctr[end];
         tm.coef = map_coef;
-        n += timed(s, [&] { return cgfd::launch_stage_bulk_tma(med, coef_type, wave16, p, tm, nzc, st); });
+        n += timed(s, [&] { return cgfd::launch_stage_bulk_tma(med, coef_type, wave16, p, tm, nzc, tiles, st); });
       } else {
         n += timed(s, [&] { return cgfd::launch_stage_bulk(med, p, nzc, st); });
       }
@@ -313,7 +316,7 @@ struct cgfd_problem {
     cudaFree(coef); cudaFree(coef16); cudaFree(jac); cudaFree(matx); cudaFree(maty);
     for (Face &f : faces) { cudaFree(f.A); cudaFree(f.B); cudaFree(f.D); cudaFree(f.aux); }
     cudaFree(d_it_begin); cudaFree(d_ext_num); cudaFree(d_src_shot); cudaFree(d_ext_idx); cudaFree(d_ext_wv); cudaFree(d_ext_wt);
-    cudaFree(d_wsc); cudaFree(d_srcb); cudaFree(d_amax);
+    cudaFree(d_wsc); cudaFree(d_srcb); cudaFree(d_amax); cudaFree(d_tiles);
     cudaFree(d_stf); cudaFree(d_idx8); cudaFree(d_w8); cudaFree(d_seis); cudaFree(d_it); cudaFree(d_flag);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -476,6 +479,8 @@ std::vector<float> source_bounds(const cgfd_problem *p) {
   }
   return sb;
 }
+
+void make_tiles(cgfd_problem *p);
 
 void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_source_desc *shots) {
   cgfd::validate_desc(d);
@@ -661,6 +666,7 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
     CK(cudaMemcpy(p->d_w8, p->rec.w8.data(), p->rec.w8.size() * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMemset(p->d_seis, 0, sizeof(float) * p->rec.n * 9 * p->nt_total * nshot));
   }
+  make_tiles(p);
   p->d_it = dmalloc<int>(1, B);
   p->d_flag = dmalloc<int>(1, B);
   CK(cudaMemset(p->d_it, 0, sizeof(int)));
@@ -675,6 +681,39 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
     CK(cudaMemcpy(p->d_srcb, sb.data(), sb.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
   CK(cudaDeviceSynchronize());
+}
+
+// Tile lists of the TMA bulk kernel for the current z chunk: (bx, by, chunk) with x fastest,
+// split by whether any CFS-PML face box meets the tile's 32 x TY x chunk volume.
+void make_tiles(cgfd_problem *p) {
+  const int ty = cgfd::tma_tile_y(p->med), nbulk = p->free_top ? p->nk - cgfd::NSURF : p->nk;
+  const int nbx = (p->ni + cgfd::TX - 1) / cgfd::TX, nby = (p->nj + ty - 1) / ty, nbz = (nbulk + p->nzc - 1) / p->nzc;
+  std::vector<int> in, pm;
+  for (int cz = 0; cz < nbz; cz++)
+    for (int by = 0; by < nby; by++)
+      for (int bx = 0; bx < nbx; bx++) {
+        const int kb = cz * p->nzc, ke = std::min(kb + p->nzc, nbulk);
+        bool touch = false;
+        for (const auto &f : p->faces) {
+          const bool xo = f.h.lo[0] <= bx * cgfd::TX + cgfd::TX - 1 && f.h.hi[0] >= bx * cgfd::TX;
+          const bool yo = f.h.lo[1] <= by * ty + ty - 1 && f.h.hi[1] >= by * ty;
+          const bool zo = f.h.lo[2] <= ke - 1 && f.h.hi[2] >= kb;
+          touch |= xo && yo && zo;
+        }
+        std::vector<int> &dst = touch ? pm : in;
+        dst.insert(dst.end(), {bx, by, cz});
+      }
+  cudaFree(p->d_tiles);
+  p->d_tiles = nullptr;
+  std::vector<int> all(in);
+  all.insert(all.end(), pm.begin(), pm.end());
+  size_t acc = 0;
+  p->d_tiles = dmalloc<int>(std::max<size_t>(all.size(), 3), acc);
+  if (!all.empty()) CK(cudaMemcpy(p->d_tiles, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice));
+  p->tiles.interior = p->d_tiles;
+  p->tiles.ninterior = (int)(in.size() / 3);
+  p->tiles.pml = p->d_tiles + in.size();
+  p->tiles.npml = (int)(pm.size() / 3);
 }
 
 // FP16 stage levels: recompute max |w_pre| after the host replaced or re-labelled levels.
@@ -940,10 +979,14 @@ int cgfd_set_graph_mode(cgfd_problem *p, int on) {
 /* z planes per thread block of the bulk stage kernel (autotuner knob; graphs are rebuilt). */
 int cgfd_set_zchunk(cgfd_problem *p, int nzc) {
   if (!p || nzc < 1) return CGFD_ERR_INVALID;
-  p->nzc = nzc;
-  for (int s = 0; s < 8; s++)
-    if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }
-  return CGFD_OK;
+  return guarded([&] {
+    CK(cudaSetDevice(p->device));
+    CK(cudaStreamSynchronize(p->stream));
+    p->nzc = nzc;
+    make_tiles(p);
+    for (int s = 0; s < 8; s++)
+      if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }
+  });
 }
 
 int cgfd_get_zchunk(const cgfd_problem *p) { return p ? p->nzc : -1; }

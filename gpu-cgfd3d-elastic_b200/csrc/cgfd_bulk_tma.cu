@@ -26,7 +26,18 @@ template <int WP> struct WavePolicy {
   using TT = typename std::conditional<WP >= 1, __half, float>::type;
 };
 
-template <int MED, int TYT, typename TC, typename TW>
+// Tile height and resident blocks per SM for interior tiles (MINB) and PML tiles (MINB_PML):
+// two 32x8 blocks per SM (two independent barrier domains hide each other's pipeline waits)
+// wherever registers (<= 128 per thread) and shared memory allow; the VTI face code and
+// everything aniso need more registers and run one.
+template <int MED> struct TileCfg { static constexpr int TYT = 8, MINB = 1, MINB_PML = 1; };
+template <> struct TileCfg<MED_ISO> { static constexpr int TYT = 8, MINB = 2, MINB_PML = 2; };
+template <> struct TileCfg<MED_VTI> { static constexpr int TYT = 8, MINB = 2, MINB_PML = 1; };
+template <int MED, bool PML> struct BlocksPerSm {
+  static constexpr int value = PML ? TileCfg<MED>::MINB_PML : TileCfg<MED>::MINB;
+};
+
+template <int MED, int TYT, typename TC, typename TW, int MINB = TileCfg<MED>::MINB>
 struct BulkSmem {
   static constexpr int XO = 16 / (int)sizeof(TW);  // x halo of the box: 16 bytes, TMA-aligned
   static constexpr int WX = TX + 2 * XO;  // x box [-XO, 32+XO) around the tile
@@ -37,11 +48,16 @@ struct BulkSmem {
   static constexpr int WAVE_SLOT = ((WAVE_ELEMS * (int)sizeof(TW) + 127) / 128) * 128;  // bytes
   static constexpr int COEF_BYTES = NC * CELLS * (int)sizeof(TC);  // multiple of 128 for every medium
   static constexpr int FLD_BYTES = 9 * CELLS * 4;
-  static constexpr int CPE_SLOT = COEF_BYTES + 2 * FLD_BYTES;
+  // w_pre staged by TMA unless that keeps MINB blocks from fitting one SM (then read directly)
+  static constexpr int FULL = 3 * WAVE_SLOT + 2 * (COEF_BYTES + 2 * FLD_BYTES) + 64;
+  static constexpr bool PT = MINB == 1 || FULL <= 113 * 1024;
+  static constexpr int OFF_END = COEF_BYTES + (PT ? FLD_BYTES : 0);  // within a cpe slot
+  static constexpr int CPE_SLOT = OFF_END + FLD_BYTES;
   static constexpr int OFF_CPE = 3 * WAVE_SLOT;
   static constexpr int OFF_BAR = OFF_CPE + 2 * CPE_SLOT;
   static constexpr int BYTES = OFF_BAR + 8 * 8;
   static_assert(COEF_BYTES % 128 == 0, "w_pre/w_end boxes must stay 128-byte aligned");
+  static_assert(MINB == 1 || MINB * (BYTES + 1024) <= 228 * 1024, "MINB blocks must fit one SM's shared memory");
 };
 
 // one cell's coefficients from a shared-memory tile (stride = cells per tile)
@@ -52,12 +68,16 @@ struct CoefTile {
   __device__ __forceinline__ float operator()(int f) const { return coef_decode<TC>(c[f * STRIDE], p, f); }
 };
 
-template <int MED, int DX, int DY, int DZ, int TYT, typename TC, int WP>
-__global__ void __launch_bounds__(TX *TYT, 1)
-    k_stage_bulk_tma(const __grid_constant__ StageP p, const __grid_constant__ TmaP tm, int nzc) {
+// Tiles come from a list (3 ints each: bx, by, z chunk): one list for the tiles that no
+// CFS-PML face touches (PML false: the face code is compiled out, fewer registers) and one
+// for the rest (PML true).
+template <int MED, int DX, int DY, int DZ, int TYT, typename TC, int WP, bool PML>
+__global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
+    k_stage_bulk_tma(const __grid_constant__ StageP p, const __grid_constant__ TmaP tm, int nzc,
+                     const int *__restrict__ tiles) {
   using TW = typename WavePolicy<WP>::TW;
   using TT = typename WavePolicy<WP>::TT;
-  using S = BulkSmem<MED, TYT, TC, TW>;
+  using S = BulkSmem<MED, TYT, TC, TW, BlocksPerSm<MED, PML>::value>;
   constexpr int LX = op_left(DX), LY = op_left(DY);
   constexpr int SD = DZ ? -1 : 1;  // march direction
   extern __shared__ __align__(128) unsigned char smem[];
@@ -69,9 +89,10 @@ __global__ void __launch_bounds__(TX *TYT, 1)
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   // shots are the fastest block index: the nshot blocks of one tile run side by side and
   // share the coefficient tiles through L2
-  const int shot = blockIdx.x % p.nshot, bx = blockIdx.x / p.nshot, by = blockIdx.y;
+  const int shot = blockIdx.x % p.nshot, tile = blockIdx.x / p.nshot;
+  const int bx = __ldg(tiles + 3 * tile), by = __ldg(tiles + 3 * tile + 1), cz = __ldg(tiles + 3 * tile + 2);
   const int i = bx * TX + tx, j = by * TYT + ty;
-  const int kb = blockIdx.z * nzc;
+  const int kb = cz * nzc;
   const int ke = min(kb + nzc, p.nbulk);
   if (kb >= ke) return;
   const int n = ke - kb;
@@ -86,7 +107,7 @@ __global__ void __launch_bounds__(TX *TYT, 1)
   const bool need_pre = stage == 1 || stage == 2;
   const bool need_end = stage >= 1;
   const uint32_t wave_bytes = S::WAVE_ELEMS * sizeof(TW);
-  const uint32_t cpe_bytes = S::COEF_BYTES + (need_pre ? S::FLD_BYTES : 0) + (need_end ? S::FLD_BYTES : 0);
+  const uint32_t cpe_bytes = S::COEF_BYTES + (need_pre && S::PT ? S::FLD_BYTES : 0) + (need_end ? S::FLD_BYTES : 0);
   // box origins in device-layout coordinates (x * element size a multiple of 16 bytes)
   const int xw = GX + bx * TX - S::XO, yw = by * TYT;
   const int xc = GX + bx * TX, yc = 3 + by * TYT;
@@ -113,8 +134,8 @@ __global__ void __launch_bounds__(TX *TYT, 1)
     unsigned char *base = cpe + sl * S::CPE_SLOT;
     mbar_expect_tx(b, cpe_bytes);
     tma_load_4d(base, &tm.coef, xc, yc, kk + 3, 0, b);
-    if (need_pre) tma_load_4d(base + S::COEF_BYTES, &tm.pre, xc, yc, kk + 3, 9 * shot, b);
-    if (need_end) tma_load_4d(base + S::COEF_BYTES + S::FLD_BYTES, &tm.end, xc, yc, kk + 3, 9 * shot, b);
+    if (S::PT && need_pre) tma_load_4d(base + S::COEF_BYTES, &tm.pre, xc, yc, kk + 3, 9 * shot, b);
+    if (need_end) tma_load_4d(base + S::OFF_END, &tm.end, xc, yc, kk + 3, 9 * shot, b);
   };
   if (tid == 0) {
     issue_wave(0);
@@ -124,7 +145,7 @@ __global__ void __launch_bounds__(TX *TYT, 1)
 
   // PML faces that intersect this block (uniform)
   unsigned fmask = 0;
-  for (int fi = 0; fi < p.nface; fi++) {
+  for (int fi = 0; PML && fi < p.nface; fi++) {
     const FaceP &f = p.face[fi];
     const bool xo = f.lo[0] <= bx * TX + TX - 1 && f.hi[0] >= bx * TX;
     const bool yo = f.lo[1] <= by * TYT + TYT - 1 && f.hi[1] >= by * TYT;
@@ -189,13 +210,14 @@ __global__ void __launch_bounds__(TX *TYT, 1)
           if constexpr (WP == 2) d[f] *= s_wsc[f];  // the operator is linear: scale once
         }
         acc.add_axis(mt[0], d, d + 3);
-        if (fmask)
-          for (int fi = 0; fi < p.nface; fi++) {
-            const FaceP &fc = p.face[fi];
-            if ((fmask >> fi & 1) && fc.axis == 0 && i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] &&
-                j <= fc.hi[1] && k >= fc.lo[2] && k <= fc.hi[2])
-              pml_face<MED>(p, fc, i, j, k, md, slw, mt[0], d, d + 3, nullptr, nullptr, acc.hc, shot);
-          }
+        if constexpr (PML) {
+          if (fmask)
+            for (int fi = 0; fi < p.nface; fi++) {
+              const FaceP &fc = p.face[fi];
+              if ((fmask >> fi & 1) && fc.axis == 0 && in_face(fc, i, j, k))
+                pml_face<MED>(p, fc, i, j, k, md, slw, mt[0], d, d + 3, nullptr, nullptr, acc.hc, shot);
+            }
+        }
       }
       // y
       {
@@ -207,13 +229,14 @@ __global__ void __launch_bounds__(TX *TYT, 1)
           if constexpr (WP == 2) d[f] *= s_wsc[f];
         }
         acc.add_axis(mt[1], d, d + 3);
-        if (fmask)
-          for (int fi = 0; fi < p.nface; fi++) {
-            const FaceP &fc = p.face[fi];
-            if ((fmask >> fi & 1) && fc.axis == 1 && i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] &&
-                j <= fc.hi[1] && k >= fc.lo[2] && k <= fc.hi[2])
-              pml_face<MED>(p, fc, i, j, k, md, slw, mt[1], d, d + 3, nullptr, nullptr, acc.hc, shot);
-          }
+        if constexpr (PML) {
+          if (fmask)
+            for (int fi = 0; fi < p.nface; fi++) {
+              const FaceP &fc = p.face[fi];
+              if ((fmask >> fi & 1) && fc.axis == 1 && in_face(fc, i, j, k))
+                pml_face<MED>(p, fc, i, j, k, md, slw, mt[1], d, d + 3, nullptr, nullptr, acc.hc, shot);
+            }
+        }
       }
       // z (queue in march order; the operator takes increasing k)
       {
@@ -225,13 +248,14 @@ __global__ void __launch_bounds__(TX *TYT, 1)
           if constexpr (WP == 2) d[f] *= s_wsc[f];
         }
         acc.add_axis(mt[2], d, d + 3);
-        if (fmask)
-          for (int fi = 0; fi < p.nface; fi++) {
-            const FaceP &fc = p.face[fi];
-            if ((fmask >> fi & 1) && fc.axis == 2 && i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] &&
-                j <= fc.hi[1] && k >= fc.lo[2] && k <= fc.hi[2])
-              pml_face<MED>(p, fc, i, j, k, md, slw, mt[2], d, d + 3, nullptr, nullptr, acc.hc, shot);
-          }
+        if constexpr (PML) {
+          if (fmask)
+            for (int fi = 0; fi < p.nface; fi++) {
+              const FaceP &fc = p.face[fi];
+              if ((fmask >> fi & 1) && fc.axis == 2 && in_face(fc, i, j, k))
+                pml_face<MED>(p, fc, i, j, k, md, slw, mt[2], d, d + 3, nullptr, nullptr, acc.hc, shot);
+            }
+        }
       }
       float h[9];
       h[0] = slw * acc.mom[0] + acc.hc[0];
@@ -243,7 +267,8 @@ __global__ void __launch_bounds__(TX *TYT, 1)
       // RK combine (wav_update / wav_update_end)
       const long long id = didx(p, i, j, k);
       const float *PR = reinterpret_cast<const float *>(cpe + cs * S::CPE_SLOT + S::COEF_BYTES) + cell;
-      const float *EN = PR + 9 * S::CELLS;
+      const float *EN = reinterpret_cast<const float *>(cpe + cs * S::CPE_SLOT + S::OFF_END) + cell;
+      const float *prg = p.pre + woff + id;  // w_pre in HBM when it is not staged
       const float ca = p.ca, cb = p.cb;
       if (stage == 0) {
 #pragma unroll
@@ -255,7 +280,7 @@ __global__ void __launch_bounds__(TX *TYT, 1)
       } else if (stage < 3) {
 #pragma unroll
         for (int f = 0; f < 9; f++) {
-          const float t = PR[f * S::CELLS] + ca * h[f];
+          const float t = (S::PT ? PR[f * S::CELLS] : __ldg(prg + f * sf)) + ca * h[f];
           tmp_out[f * sf + id] = from_f<TT>(WP != 0 ? t * s_wsc[9 + f] : t);
           endw[f * sf + id] = EN[f * S::CELLS] + cb * h[f];
         }
@@ -292,42 +317,60 @@ __global__ void __launch_bounds__(TX *TYT, 1)
 }
 
 // -----------------------------------------------------------------------------------------
-template <int MED, int TYT, typename TC, int WP>
-static void launch_tma_med(const StageP &p, const TmaP &tm, int nzc, cudaStream_t st) {
-  using S = BulkSmem<MED, TYT, TC, typename WavePolicy<WP>::TW>;
+template <int MED, int TYT, typename TC, int WP, bool PML>
+static void launch_tma_kind(const StageP &p, const TmaP &tm, int nzc, const int *tiles, int ntiles, cudaStream_t st) {
+  using S = BulkSmem<MED, TYT, TC, typename WavePolicy<WP>::TW, BlocksPerSm<MED, PML>::value>;
+  if (ntiles <= 0) return;
   const int code = p.dir[0] | (p.dir[1] << 1) | (p.dir[2] << 2);
   dim3 block(TX, TYT);
-  dim3 grid(((p.ni + TX - 1) / TX) * p.nshot, (p.nj + TYT - 1) / TYT, (p.nbulk + nzc - 1) / nzc);
+  dim3 grid(ntiles * p.nshot);
   switch (code) {
-#define CASE(c)                                                                                            \
-  case c:                                                                                                  \
-    k_stage_bulk_tma<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, TYT, TC, WP><<<grid, block, S::BYTES, st>>>(p, tm, nzc); \
+#define CASE(c)                                                                                              \
+  case c:                                                                                                    \
+    k_stage_bulk_tma<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, TYT, TC, WP, PML>                           \
+        <<<grid, block, S::BYTES, st>>>(p, tm, nzc, tiles);                                                  \
     break;
     CASE(0) CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7)
 #undef CASE
   }
 }
 
+// PML tiles first (the slower blocks start early), then the interior tiles.
 template <int MED, int TYT, typename TC, int WP>
-static cudaError_t set_attr_med() {
-  using S = BulkSmem<MED, TYT, TC, typename WavePolicy<WP>::TW>;
+static int launch_tma_med(const StageP &p, const TmaP &tm, int nzc, const BulkTiles &t, cudaStream_t st) {
+  launch_tma_kind<MED, TYT, TC, WP, true>(p, tm, nzc, t.pml, t.npml, st);
+  launch_tma_kind<MED, TYT, TC, WP, false>(p, tm, nzc, t.interior, t.ninterior, st);
+  return (t.npml > 0) + (t.ninterior > 0);
+}
+
+template <int MED, int TYT, typename TC, int WP, bool PML>
+static cudaError_t set_attr_kind() {
+  using S = BulkSmem<MED, TYT, TC, typename WavePolicy<WP>::TW, BlocksPerSm<MED, PML>::value>;
   cudaError_t e = cudaSuccess;
 #define ATTR(c)                                                                                              \
   if (e == cudaSuccess)                                                                                      \
-    e = cudaFuncSetAttribute(k_stage_bulk_tma<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, TYT, TC, WP>,   \
+    e = cudaFuncSetAttribute(k_stage_bulk_tma<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, TYT, TC, WP, PML>, \
                              cudaFuncAttributeMaxDynamicSharedMemorySize, S::BYTES);
   ATTR(0) ATTR(1) ATTR(2) ATTR(3) ATTR(4) ATTR(5) ATTR(6) ATTR(7)
 #undef ATTR
   return e;
 }
 
-int tma_tile_y(int med) { return med == MED_ISO ? 16 : 8; }
+template <int MED, int TYT, typename TC, int WP>
+static cudaError_t set_attr_med() {
+  cudaError_t e = set_attr_kind<MED, TYT, TC, WP, true>();
+  return e == cudaSuccess ? set_attr_kind<MED, TYT, TC, WP, false>() : e;
+}
+
+int tma_tile_y(int med) {
+  return med == MED_ISO ? TileCfg<MED_ISO>::TYT : (med == MED_VTI ? TileCfg<MED_VTI>::TYT : TileCfg<MED_ANISO>::TYT);
+}
 
 template <typename TC, int WP>
 static cudaError_t prepare_tc(int med) {
-  if (med == MED_ISO) return set_attr_med<MED_ISO, 16, TC, WP>();
-  if (med == MED_VTI) return set_attr_med<MED_VTI, 8, TC, WP>();
-  return set_attr_med<MED_ANISO, 8, TC, WP>();
+  if (med == MED_ISO) return set_attr_med<MED_ISO, TileCfg<MED_ISO>::TYT, TC, WP>();
+  if (med == MED_VTI) return set_attr_med<MED_VTI, TileCfg<MED_VTI>::TYT, TC, WP>();
+  return set_attr_med<MED_ANISO, TileCfg<MED_ANISO>::TYT, TC, WP>();
 }
 
 cudaError_t tma_prepare(int med, int coef_type, int wave16) {
@@ -343,23 +386,23 @@ cudaError_t tma_prepare(int med, int coef_type, int wave16) {
 }
 
 template <typename TC, int WP>
-static void launch_tc(int med, const StageP &p, const TmaP &tm, int nzc, cudaStream_t st) {
-  if (med == MED_ISO) launch_tma_med<MED_ISO, 16, TC, WP>(p, tm, nzc, st);
-  else if (med == MED_VTI) launch_tma_med<MED_VTI, 8, TC, WP>(p, tm, nzc, st);
-  else launch_tma_med<MED_ANISO, 8, TC, WP>(p, tm, nzc, st);
+static int launch_tc(int med, const StageP &p, const TmaP &tm, int nzc, const BulkTiles &t, cudaStream_t st) {
+  if (med == MED_ISO) return launch_tma_med<MED_ISO, TileCfg<MED_ISO>::TYT, TC, WP>(p, tm, nzc, t, st);
+  if (med == MED_VTI) return launch_tma_med<MED_VTI, TileCfg<MED_VTI>::TYT, TC, WP>(p, tm, nzc, t, st);
+  return launch_tma_med<MED_ANISO, TileCfg<MED_ANISO>::TYT, TC, WP>(p, tm, nzc, t, st);
 }
 
 int launch_stage_bulk_tma(int med, int coef_type, int wave16, const StageP &p, const TmaP &tm, int nzc,
-                          cudaStream_t st) {
+                          const BulkTiles &t, cudaStream_t st) {
   if (p.nbulk <= 0) return 0;
   if (wave16) {  // 16-bit fixed-point coefficients with FP16 stage levels
-    if (p.stage == 0) launch_tc<uint16_t, 1>(med, p, tm, nzc, st);
-    else launch_tc<uint16_t, 2>(med, p, tm, nzc, st);
-  } else if (coef_type == COEF_U16) launch_tc<uint16_t, 0>(med, p, tm, nzc, st);
-  else if (coef_type == COEF_F16) launch_tc<__half, 0>(med, p, tm, nzc, st);
-  else if (coef_type == COEF_BF16) launch_tc<__nv_bfloat16, 0>(med, p, tm, nzc, st);
-  else launch_tc<float, 0>(med, p, tm, nzc, st);
-  return 1;
+    if (p.stage == 0) return launch_tc<uint16_t, 1>(med, p, tm, nzc, t, st);
+    return launch_tc<uint16_t, 2>(med, p, tm, nzc, t, st);
+  }
+  if (coef_type == COEF_U16) return launch_tc<uint16_t, 0>(med, p, tm, nzc, t, st);
+  if (coef_type == COEF_F16) return launch_tc<__half, 0>(med, p, tm, nzc, t, st);
+  if (coef_type == COEF_BF16) return launch_tc<__nv_bfloat16, 0>(med, p, tm, nzc, t, st);
+  return launch_tc<float, 0>(med, p, tm, nzc, t, st);
 }
 
 }  // namespace cgfd

@@ -347,6 +347,11 @@ __device__ __forceinline__ void pml_face(const StageP &p, const FaceP &f, int i,
   rk_store(p.stage, p.ca, p.cb, f.n, ia, aux, arhs, f.aux_pre, f.aux_tmp, f.aux_end);
 }
 
+__device__ __forceinline__ bool in_face(const FaceP &f, int i, int j, int k) {
+  return i >= f.lo[0] && i <= f.hi[0] && j >= f.lo[1] && j <= f.hi[1] && k >= f.lo[2] && k <= f.hi[2];
+}
+
+
 // Index helpers for the device layout.
 __device__ __forceinline__ long long didx(const StageP &p, int i, int j, int k) {
   return p.off0 + (long long)k * p.sz + (long long)j * p.sx + i;
