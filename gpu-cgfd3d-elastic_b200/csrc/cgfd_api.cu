@@ -113,8 +113,11 @@ struct cgfd_problem {
   // source increment of each step)
   int wave16 = 0;
   // TMA bulk kernel tile lists for the current z chunk (interior tiles, then PML tiles)
-  int *d_tiles = nullptr;
+  int4 *d_tiles = nullptr;
   cgfd::BulkTiles tiles;
+  // PML tiles run on `side`, forked from and joined back into `stream` at every stage
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   float *d_wsc = nullptr, *d_srcb = nullptr;
   unsigned int *d_amax = nullptr;
 
@@ -261,7 +264,19 @@ struct cgfd_problem {
         tm.pre = map_ctr[pre];
         tm.end = map_ctr[end];
         tm.coef = map_coef;
-        n += timed(s, [&] { return cgfd::launch_stage_bulk_tma(med, coef_type, wave16, p, tm, nzc, tiles, st); });
+        n += timed(s, [&] {
+          const bool fork = tiles.npml > 0 && tiles.ninterior > 0;
+          if (fork) {
+            CK(cudaEventRecord(ev_fork, st));
+            CK(cudaStreamWaitEvent(side, ev_fork, 0));
+          }
+          const int k = cgfd::launch_stage_bulk_tma(med, coef_type, wave16, p, tm, tiles, st, fork ? side : st);
+          if (fork) {
+            CK(cudaEventRecord(ev_join, side));
+            CK(cudaStreamWaitEvent(st, ev_join, 0));
+          }
+          return k;
+        });
       } else {
         n += timed(s, [&] { return cgfd::launch_stage_bulk(med, p, nzc, st); });
       }
@@ -319,6 +334,9 @@ struct cgfd_problem {
     cudaFree(d_wsc); cudaFree(d_srcb); cudaFree(d_amax); cudaFree(d_tiles);
     cudaFree(d_stf); cudaFree(d_idx8); cudaFree(d_w8); cudaFree(d_seis); cudaFree(d_it); cudaFree(d_flag);
     if (stream) cudaStreamDestroy(stream);
+    if (side) cudaStreamDestroy(side);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
   }
 };
 
@@ -498,6 +516,9 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   p->device = d->device;
   CK(cudaSetDevice(p->device));
   CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
   p->ni = d->ni; p->nj = d->nj; p->nk = d->nk;
   p->med = d->medium_type == CGFD_MEDIUM_ELASTIC_ISO ? cgfd::MED_ISO
            : (d->medium_type == CGFD_MEDIUM_ELASTIC_VTI ? cgfd::MED_VTI : cgfd::MED_ANISO);
@@ -683,37 +704,49 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   CK(cudaDeviceSynchronize());
 }
 
-// Tile lists of the TMA bulk kernel for the current z chunk: (bx, by, chunk) with x fastest,
-// split by whether any CFS-PML face box meets the tile's 32 x TY x chunk volume.
+// Tile lists of the TMA bulk kernel: 32 x TY columns, split along z into chunks of about
+// nzc planes that never straddle a z-face boundary of the CFS-PML (so planes above the
+// bottom absorbing layer run as interior tiles), and sorted by whether any PML face box meets
+// the tile's volume. Entries (bx, by, first plane, end plane), x fastest.
 void make_tiles(cgfd_problem *p) {
   const int ty = cgfd::tma_tile_y(p->med), nbulk = p->free_top ? p->nk - cgfd::NSURF : p->nk;
-  const int nbx = (p->ni + cgfd::TX - 1) / cgfd::TX, nby = (p->nj + ty - 1) / ty, nbz = (nbulk + p->nzc - 1) / p->nzc;
-  std::vector<int> in, pm;
-  for (int cz = 0; cz < nbz; cz++)
+  const int nbx = (p->ni + cgfd::TX - 1) / cgfd::TX, nby = (p->nj + ty - 1) / ty;
+  std::vector<int> cuts = {0, nbulk};
+  for (const auto &f : p->faces)
+    if (f.h.axis == 2)
+      for (int c : {f.h.lo[2], f.h.hi[2] + 1})
+        if (c > 0 && c < nbulk) cuts.push_back(c);
+  std::sort(cuts.begin(), cuts.end());
+  cuts.erase(std::unique(cuts.begin(), cuts.end()), cuts.end());
+  std::vector<std::pair<int, int>> zr;
+  for (size_t s = 0; s + 1 < cuts.size(); s++) {
+    const int len = cuts[s + 1] - cuts[s], nch = std::max(1, (len + p->nzc - 1) / p->nzc);
+    for (int c = 0; c < nch; c++) zr.emplace_back(cuts[s] + len * c / nch, cuts[s] + len * (c + 1) / nch);
+  }
+  std::vector<int4> in, pm;
+  for (const auto &z : zr)
     for (int by = 0; by < nby; by++)
       for (int bx = 0; bx < nbx; bx++) {
-        const int kb = cz * p->nzc, ke = std::min(kb + p->nzc, nbulk);
         bool touch = false;
         for (const auto &f : p->faces) {
           const bool xo = f.h.lo[0] <= bx * cgfd::TX + cgfd::TX - 1 && f.h.hi[0] >= bx * cgfd::TX;
           const bool yo = f.h.lo[1] <= by * ty + ty - 1 && f.h.hi[1] >= by * ty;
-          const bool zo = f.h.lo[2] <= ke - 1 && f.h.hi[2] >= kb;
+          const bool zo = f.h.lo[2] <= z.second - 1 && f.h.hi[2] >= z.first;
           touch |= xo && yo && zo;
         }
-        std::vector<int> &dst = touch ? pm : in;
-        dst.insert(dst.end(), {bx, by, cz});
+        (touch ? pm : in).push_back(make_int4(bx, by, z.first, z.second));
       }
   cudaFree(p->d_tiles);
   p->d_tiles = nullptr;
-  std::vector<int> all(in);
+  std::vector<int4> all(in);
   all.insert(all.end(), pm.begin(), pm.end());
   size_t acc = 0;
-  p->d_tiles = dmalloc<int>(std::max<size_t>(all.size(), 3), acc);
-  if (!all.empty()) CK(cudaMemcpy(p->d_tiles, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice));
+  p->d_tiles = dmalloc<int4>(std::max<size_t>(all.size(), 1), acc);
+  if (!all.empty()) CK(cudaMemcpy(p->d_tiles, all.data(), all.size() * sizeof(int4), cudaMemcpyHostToDevice));
   p->tiles.interior = p->d_tiles;
-  p->tiles.ninterior = (int)(in.size() / 3);
+  p->tiles.ninterior = (int)in.size();
   p->tiles.pml = p->d_tiles + in.size();
-  p->tiles.npml = (int)(pm.size() / 3);
+  p->tiles.npml = (int)pm.size();
 }
 
 // FP16 stage levels: recompute max |w_pre| after the host replaced or re-labelled levels.

@@ -68,13 +68,13 @@ struct CoefTile {
   __device__ __forceinline__ float operator()(int f) const { return coef_decode<TC>(c[f * STRIDE], p, f); }
 };
 
-// Tiles come from a list (3 ints each: bx, by, z chunk): one list for the tiles that no
-// CFS-PML face touches (PML false: the face code is compiled out, fewer registers) and one
-// for the rest (PML true).
+// Tiles come from a list (4 ints each: bx, by, first plane, end plane): one list for the
+// tiles that no CFS-PML face touches (PML false: the face code is compiled out, fewer
+// registers) and one for the rest (PML true).
 template <int MED, int DX, int DY, int DZ, int TYT, typename TC, int WP, bool PML>
 __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
-    k_stage_bulk_tma(const __grid_constant__ StageP p, const __grid_constant__ TmaP tm, int nzc,
-                     const int *__restrict__ tiles) {
+    k_stage_bulk_tma(const __grid_constant__ StageP p, const __grid_constant__ TmaP tm,
+                     const int4 *__restrict__ tiles) {
   using TW = typename WavePolicy<WP>::TW;
   using TT = typename WavePolicy<WP>::TT;
   using S = BulkSmem<MED, TYT, TC, TW, BlocksPerSm<MED, PML>::value>;
@@ -90,10 +90,10 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
   // shots are the fastest block index: the nshot blocks of one tile run side by side and
   // share the coefficient tiles through L2
   const int shot = blockIdx.x % p.nshot, tile = blockIdx.x / p.nshot;
-  const int bx = __ldg(tiles + 3 * tile), by = __ldg(tiles + 3 * tile + 1), cz = __ldg(tiles + 3 * tile + 2);
+  const int4 tl = __ldg(tiles + tile);
+  const int bx = tl.x, by = tl.y;
   const int i = bx * TX + tx, j = by * TYT + ty;
-  const int kb = cz * nzc;
-  const int ke = min(kb + nzc, p.nbulk);
+  const int kb = tl.z, ke = tl.w;
   if (kb >= ke) return;
   const int n = ke - kb;
   const bool act = i < p.ni && j < p.nj;
@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
 
 // -----------------------------------------------------------------------------------------
 template <int MED, int TYT, typename TC, int WP, bool PML>
-static void launch_tma_kind(const StageP &p, const TmaP &tm, int nzc, const int *tiles, int ntiles, cudaStream_t st) {
+static void launch_tma_kind(const StageP &p, const TmaP &tm, const int4 *tiles, int ntiles, cudaStream_t st) {
   using S = BulkSmem<MED, TYT, TC, typename WavePolicy<WP>::TW, BlocksPerSm<MED, PML>::value>;
   if (ntiles <= 0) return;
   const int code = p.dir[0] | (p.dir[1] << 1) | (p.dir[2] << 2);
@@ -328,18 +328,18 @@ static void launch_tma_kind(const StageP &p, const TmaP &tm, int nzc, const int 
 #define CASE(c)                                                                                              \
   case c:                                                                                                    \
     k_stage_bulk_tma<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, TYT, TC, WP, PML>                           \
-        <<<grid, block, S::BYTES, st>>>(p, tm, nzc, tiles);                                                  \
+        <<<grid, block, S::BYTES, st>>>(p, tm, tiles);                                                       \
     break;
     CASE(0) CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7)
 #undef CASE
   }
 }
 
-// PML tiles first (the slower blocks start early), then the interior tiles.
+// PML tiles on st_pml, interior tiles on st (the caller forks and joins the two streams).
 template <int MED, int TYT, typename TC, int WP>
-static int launch_tma_med(const StageP &p, const TmaP &tm, int nzc, const BulkTiles &t, cudaStream_t st) {
-  launch_tma_kind<MED, TYT, TC, WP, true>(p, tm, nzc, t.pml, t.npml, st);
-  launch_tma_kind<MED, TYT, TC, WP, false>(p, tm, nzc, t.interior, t.ninterior, st);
+static int launch_tma_med(const StageP &p, const TmaP &tm, const BulkTiles &t, cudaStream_t st, cudaStream_t st_pml) {
+  launch_tma_kind<MED, TYT, TC, WP, true>(p, tm, t.pml, t.npml, st_pml);
+  launch_tma_kind<MED, TYT, TC, WP, false>(p, tm, t.interior, t.ninterior, st);
   return (t.npml > 0) + (t.ninterior > 0);
 }
 
@@ -386,23 +386,24 @@ cudaError_t tma_prepare(int med, int coef_type, int wave16) {
 }
 
 template <typename TC, int WP>
-static int launch_tc(int med, const StageP &p, const TmaP &tm, int nzc, const BulkTiles &t, cudaStream_t st) {
-  if (med == MED_ISO) return launch_tma_med<MED_ISO, TileCfg<MED_ISO>::TYT, TC, WP>(p, tm, nzc, t, st);
-  if (med == MED_VTI) return launch_tma_med<MED_VTI, TileCfg<MED_VTI>::TYT, TC, WP>(p, tm, nzc, t, st);
-  return launch_tma_med<MED_ANISO, TileCfg<MED_ANISO>::TYT, TC, WP>(p, tm, nzc, t, st);
+static int launch_tc(int med, const StageP &p, const TmaP &tm, const BulkTiles &t, cudaStream_t st,
+                     cudaStream_t st_pml) {
+  if (med == MED_ISO) return launch_tma_med<MED_ISO, TileCfg<MED_ISO>::TYT, TC, WP>(p, tm, t, st, st_pml);
+  if (med == MED_VTI) return launch_tma_med<MED_VTI, TileCfg<MED_VTI>::TYT, TC, WP>(p, tm, t, st, st_pml);
+  return launch_tma_med<MED_ANISO, TileCfg<MED_ANISO>::TYT, TC, WP>(p, tm, t, st, st_pml);
 }
 
-int launch_stage_bulk_tma(int med, int coef_type, int wave16, const StageP &p, const TmaP &tm, int nzc,
-                          const BulkTiles &t, cudaStream_t st) {
+int launch_stage_bulk_tma(int med, int coef_type, int wave16, const StageP &p, const TmaP &tm, const BulkTiles &t,
+                          cudaStream_t st, cudaStream_t st_pml) {
   if (p.nbulk <= 0) return 0;
   if (wave16) {  // 16-bit fixed-point coefficients with FP16 stage levels
-    if (p.stage == 0) return launch_tc<uint16_t, 1>(med, p, tm, nzc, t, st);
-    return launch_tc<uint16_t, 2>(med, p, tm, nzc, t, st);
+    if (p.stage == 0) return launch_tc<uint16_t, 1>(med, p, tm, t, st, st_pml);
+    return launch_tc<uint16_t, 2>(med, p, tm, t, st, st_pml);
   }
-  if (coef_type == COEF_U16) return launch_tc<uint16_t, 0>(med, p, tm, nzc, t, st);
-  if (coef_type == COEF_F16) return launch_tc<__half, 0>(med, p, tm, nzc, t, st);
-  if (coef_type == COEF_BF16) return launch_tc<__nv_bfloat16, 0>(med, p, tm, nzc, t, st);
-  return launch_tc<float, 0>(med, p, tm, nzc, t, st);
+  if (coef_type == COEF_U16) return launch_tc<uint16_t, 0>(med, p, tm, t, st, st_pml);
+  if (coef_type == COEF_F16) return launch_tc<__half, 0>(med, p, tm, t, st, st_pml);
+  if (coef_type == COEF_BF16) return launch_tc<__nv_bfloat16, 0>(med, p, tm, t, st, st_pml);
+  return launch_tc<float, 0>(med, p, tm, t, st, st_pml);
 }
 
 }  // namespace cgfd

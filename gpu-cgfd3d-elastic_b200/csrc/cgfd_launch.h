@@ -55,14 +55,15 @@ int launch_stage_surface(int med, int coef_type, int wave16, const StageP &p, cu
 // wave16: FP16 stage levels (requires COEF_F16).
 int tma_tile_y(int med);
 cudaError_t tma_prepare(int med, int coef_type, int wave16);
-// Tile lists of the TMA bulk kernel (device arrays, 3 ints per tile: bx, by, z chunk):
-// tiles no CFS-PML face touches, and the rest.
+// Tile lists of the TMA bulk kernel (device arrays, one int4 per tile: bx, by, first and
+// end z plane): tiles no CFS-PML face touches, and the rest.
 struct BulkTiles {
-  const int *interior = nullptr, *pml = nullptr;
+  const int4 *interior = nullptr, *pml = nullptr;
   int ninterior = 0, npml = 0;
 };
-int launch_stage_bulk_tma(int med, int coef_type, int wave16, const StageP &p, const TmaP &tm, int nzc,
-                          const BulkTiles &t, cudaStream_t st);
+// Interior tiles go to st, PML tiles to st_pml (may be st).
+int launch_stage_bulk_tma(int med, int coef_type, int wave16, const StageP &p, const TmaP &tm, const BulkTiles &t,
+                          cudaStream_t st, cudaStream_t st_pml);
 // FP16 stage levels: per-step scale from the last step's max |w| and the step's source bound
 int launch_wave_scale(unsigned int *amax, const float *srcb, const int *d_it, int nt_total, int nshot, float *wsc,
                       cudaStream_t st);
