@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--zchunk", type=int, default=0)
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched / mixed-precision section")
     return ap.parse_args()
 
 
@@ -150,6 +151,68 @@ def ncu_traffic(workload, cells_per_launch):
         return b * cells_per_launch / c
     except Exception:
         return None
+
+
+def _time_steps(sim, steps, warm=8):
+    """ms per step of `steps` graph-replayed steps after `warm` (>= 8 captures every graph)."""
+    import torch
+    st = torch.cuda.ExternalStream(sim.stream)
+    sim.enqueue(warm)
+    sim.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    sim.enqueue(steps)
+    e1.record(st)
+    e1.synchronize()
+    sim.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def batched_mixed(local, steps=16):
+    """Batched sources and storage precision on the 256x256x128 batch workload (50 m, CFS-PML
+    20, layered + 5% von Karman iso medium, 32 random double-couple sources at 1-6 km depth,
+    fc 2-5 Hz, 200 surface stations): source x time steps per second of the plain FP32 path
+    (one source per simulation) against batches of S shots in FP32, in 16-bit fixed-point
+    coefficients and in the mixed mode (16-bit coefficients + FP16 RK stage levels), and the
+    mixed mode's seismogram error against the plain FP32 path (which the tests hold within
+    1e-6 of the FP64 oracle)."""
+    import dataclasses
+    from cgfd_b200 import synth, Simulation, CGFD_PREC_FP32, CGFD_PREC_U16_COEF, CGFD_PREC_FP16_WAVE
+    ni, nj, nk, nsteps = 256, 256, 128, 1500
+    p = synth.make_problem(ni, nj, nk, 50.0, nsteps, dt=None, medium="iso", npml=20, nsrc=0, sta_grid=(20, 10),
+                           fc=3.0, seed=77, perturb_std=0.05, corr=1000.0, hurst=0.3)
+    p.device = local
+    rng = np.random.default_rng(78)
+    shots = [synth.dc_sources(p.coord, ni, nj, 1, rng, depth_range=(1000.0, 6000.0), fc_range=(2.0, 5.0),
+                              stf_length=p.nt_total * p.dt) for _ in range(32)]
+    out = {"workload": f"{ni}x{nj}x{nk}", "sources": 32, "stations": 200, "steps_timed": steps,
+           "unit": "source-steps/s"}
+    nacc = 400  # steps of the accuracy comparison (arrivals reach the stations)
+    one = Simulation(dataclasses.replace(p, src=shots[0]))
+    plain_ms = _time_steps(one, steps)
+    one.run(nacc - one.step)
+    ref = one.seismograms()[:, :, :nacc]
+    one.close()
+    out["plain_fp32"] = {"source_steps_per_s": 1e3 / plain_ms, "ms_per_step": plain_ms}
+    for name, prec in (("batched_fp32", CGFD_PREC_FP32), ("batched_u16coef", CGFD_PREC_U16_COEF),
+                       ("batched_mixed", CGFD_PREC_FP16_WAVE)):
+        for nshot in (8, 32):
+            q = dataclasses.replace(p, precision=prec)
+            b = Simulation(q, shots=shots[:nshot])
+            ms = _time_steps(b, steps)
+            rec = {"shots": nshot, "ms_per_step": ms, "source_steps_per_s": nshot * 1e3 / ms,
+                   "vs_plain": nshot * plain_ms / ms, "device_gb": b.device_bytes() / 1e9}
+            if prec != CGFD_PREC_FP32 and nshot == 8:
+                b.run(nacc - b.step)
+                s0 = b.seismograms()[0][:, :, :nacc]
+                den = float(np.linalg.norm(ref))
+                rec["seismo_rel_l2_vs_fp32"] = float(np.linalg.norm(s0 - ref) / den) if den > 0 else None
+                rec["seismo_steps_compared"] = nacc
+            b.close()
+            out[f"{name}_{nshot}"] = rec
+    out["note"] = ("Errors against the FP64 oracle on smaller grids (tests/test_gpu_precision.py): FP32 <= 7e-7, "
+                   "16-bit fixed-point coefficients <= 4e-5, mixed (plus FP16 stage levels) <= 5e-4 gather rel L2.")
+    return out
 
 
 def cpu_baseline(args, threads):
@@ -288,7 +351,8 @@ def main():
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "traffic": traffic,
             "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback",
-            "kernel": "k_stage_bulk<iso>", "bytes_per_cell_stage": bpc, "cells_per_launch": bulk_cells,
+            "kernel": "k_stage_bulk_tma<iso> (interior-tile and PML-tile launches of one RK stage)",
+            "bytes_per_cell_stage": bpc, "cells_per_launch": bulk_cells,
             "kernel_ms": {k: (v[0] / v[1] if v[1] else None) for k, v in tim.items() if k != "launches"},
             "kernel_share": {k: (v[0] / ms if ms else None) for k, v in tim.items()
                              if k in ("bulk", "surface", "source", "recv")}}
@@ -319,6 +383,13 @@ def main():
                "note": "cgfd_problem_create from host arrays (metric 10 + medium 3 fields) + K steps + "
                        "seismogram read-back, wall clock"}
 
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        try:
+            batched = batched_mixed(local)
+        except Exception as ex:  # report, do not fail the headline measurement
+            batched = {"error": str(ex)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = len(os.sched_getaffinity(0))
@@ -336,7 +407,7 @@ def main():
                           "dt": p.dt, "precision": "fp32", "parallelism": f"replicas x{world}",
                           "l2": "inputs larger than L2 (wavefield 4x9x58M floats)"},
                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": tim["launches"],
-               "clocks": clocks}
+               "clocks": clocks, "batched_mixed": batched}
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()
