@@ -58,6 +58,24 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(x, dist, device):
+    """Max of a per-rank float over all ranks (timings: the slowest rank sets the job time).
+    Every rank must call it at the same point; device is the tensor device of the backend
+    ("cuda:<n>" for nccl, "cpu" for gloo)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world, cells, steps, ms):
+    """Whole-job Gcell-stage/s: every rank advances its own replica of `cells` for `steps`
+    steps (4 RK stages each) within the max-over-ranks time `ms`."""
+    return world * cells * 4 * steps / (ms * 1e-3) / 1e9
+
+
 def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
@@ -334,11 +352,8 @@ def main():
     ms = e0.elapsed_time(e1)
     tim = sim.timing(reset=True)
     sim.set_timing(False)
-    if dist:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * cells * 4 * args.steps / (ms * 1e-3) / 1e9
+    ms = max_over_ranks(ms, dist, f"cuda:{local}")
+    value = job_value(world, cells, args.steps, ms)
 
     # roofline of the dominant kernel (bulk stage): algorithmic bytes per launch / duration
     bulk_ms, bulk_n = tim["bulk"]
@@ -372,10 +387,7 @@ def main():
         s2.synchronize()
         t_e2e = time.perf_counter() - t
         s2.close()
-        if dist:
-            tt = torch.tensor([t_e2e], device=f"cuda:{local}")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t_e2e = float(tt.item())
+        t_e2e = max_over_ranks(t_e2e, dist, f"cuda:{local}")
         fld = (p.ni + 6) * (p.nj + 6) * (p.nk + 6) * 4
         h2d = 13 * fld
         e2e = {"value": world * cells * 4 * args.steps / t_e2e / 1e9, "unit": UNIT,

@@ -248,6 +248,7 @@ def lib():
         "cgfd_run": (C.c_int, [P, C.c_int]),
         "cgfd_enqueue_steps": (C.c_int, [P, C.c_int]),
         "cgfd_synchronize": (C.c_int, [P]),
+        "cgfd_check_wait_bound": (C.c_int, [P]),
         "cgfd_current_step": (C.c_int, [P]),
         "cgfd_set_step": (C.c_int, [P, C.c_int]),
         "cgfd_get_seismograms": (C.c_int, [P, P]),
@@ -343,6 +344,12 @@ class Simulation:
 
     def synchronize(self):
         check(lib().cgfd_synchronize(self.h))
+
+    def check_wait_bound(self):
+        """cgfd_check_wait_bound: (status, message) of one device pipeline wait that nothing
+        completes; a working bound gives CGFD_ERR_CUDA and leaves the problem usable."""
+        rc = lib().cgfd_check_wait_bound(self.h)
+        return rc, lib().cgfd_last_error().decode()
 
     @property
     def step(self):

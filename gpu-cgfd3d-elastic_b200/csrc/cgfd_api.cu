@@ -832,6 +832,26 @@ int cgfd_synchronize(cgfd_problem *p) {
   });
 }
 
+int cgfd_check_wait_bound(cgfd_problem *p) {
+  if (!p) { set_err("problem is NULL"); return CGFD_ERR_INVALID; }
+  int rc = guarded([&] {
+    CK(cudaSetDevice(p->device));
+    CK(cudaStreamSynchronize(p->stream));
+    cgfd::launch_wait_bound_check(p->d_flag, 1 << 16, p->stream);
+    CK(cudaGetLastError());
+  });
+  if (rc != CGFD_OK) return rc;
+  rc = cgfd_synchronize(p);  // reports the timeout like a stage kernel's
+  std::string msg = g_err;
+  int zero = 0;
+  if (cudaMemcpy(p->d_flag, &zero, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+    set_err("could not clear the device error word");
+    return CGFD_ERR_CUDA;
+  }
+  set_err(msg);
+  return rc;
+}
+
 int cgfd_run(cgfd_problem *p, int nsteps) {
   int rc = cgfd_enqueue_steps(p, nsteps);
   if (rc) return rc;

@@ -16,6 +16,7 @@
 // k_recv: trilinear station sampling of w_pre for all stations (io_funcs.cu:1624-1666).
 #include "cgfd_dev.cuh"
 #include "cgfd_launch.h"
+#include "cgfd_tma.cuh"
 
 namespace cgfd {
 
@@ -545,6 +546,23 @@ __global__ void k_wave_absmax(const float *__restrict__ w, long long sf, unsigne
     atomic_max_abs(&amax[0], vm);
     atomic_max_abs(&amax[1], sm);
   }
+}
+
+// One mbarrier wait that no transfer completes, bounded by `polls`: the stage kernels' wait
+// path on a lost TMA transfer (records the pipeline-timeout bit in *err and returns).
+__global__ void k_wait_bound_check(int *err, int polls) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_wait(&bar, 0, err, polls);
+}
+
+int launch_wait_bound_check(int *err, int polls, cudaStream_t st) {
+  k_wait_bound_check<<<1, 32, 0, st>>>(err, polls);
+  return 1;
 }
 
 void launch_wave_absmax(const float *w, long long sf, int nshot, unsigned int *amax, cudaStream_t st) {

@@ -67,6 +67,8 @@ int launch_stage_bulk_tma(int med, int coef_type, int wave16, const StageP &p, c
 // FP16 stage levels: per-step scale from the last step's max |w| and the step's source bound
 int launch_wave_scale(unsigned int *amax, const float *srcb, const int *d_it, int nt_total, int nshot, float *wsc,
                       cudaStream_t st);
+// one bounded mbarrier wait that nothing completes (failure-path check)
+int launch_wait_bound_check(int *err, int polls, cudaStream_t st);
 // max |w| of the velocity / stress groups of each of `nshot` wavefields into amax[nshot][2]
 void launch_wave_absmax(const float *w, long long sf, int nshot, unsigned int *amax, cudaStream_t st);
 // 16-bit coefficient storage

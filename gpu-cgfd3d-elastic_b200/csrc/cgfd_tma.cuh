@@ -31,10 +31,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
-// Bounded wait on phase `parity`; returns false (and flags *err) on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
+// Bounded wait on phase `parity`; returns false (and flags *err) after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int limit = kWaitLimit) {
   const uint32_t a = smem_u32(bar);
-  for (int n = 0; n < kWaitLimit; ++n) {
+  for (int n = 0; n < limit; ++n) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred P;\n\t"

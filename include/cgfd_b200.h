@@ -246,6 +246,15 @@ void *cgfd_stream(cgfd_problem *p);
 int cgfd_enqueue_steps(cgfd_problem *p, int nsteps);
 int cgfd_synchronize(cgfd_problem *p);
 
+/*
+ * Failure-path check: runs, on the problem's stream, one device-side pipeline wait that no
+ * transfer completes, bounded like the stage kernels' waits (2^16 polls), and reports it the
+ * way a lost transfer in a stage would be reported: CGFD_ERR_CUDA with the pipeline-timeout
+ * message. The device error word is cleared afterwards, so the problem stays usable.
+ * No counterpart in the reference.
+ */
+int cgfd_check_wait_bound(cgfd_problem *p);
+
 /* ---- tuning knobs -------------------------------------------------------------------- */
 
 /* Disable (0) or enable (1, default) CUDA-graph replay of the time steps. */
