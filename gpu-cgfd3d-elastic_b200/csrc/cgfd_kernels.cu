@@ -191,8 +191,10 @@ __device__ __forceinline__ void ld5(int dir, const WaveIn<TW> &cur, int f, long 
 
 // Surface slab: one thread per cell of the top NSURF planes. WP is the wave policy of the
 // bulk kernel (0 FP32 stage levels; 1 FP32 input, FP16 output; 2 FP16 input and output).
+// The kernel is latency-bound on its many cached loads: registers are capped at 128 so that
+// 16 warps share each SM (a few spills are cheaper than 8 warps).
 template <int MED, typename TC, int WP>
-__global__ void __launch_bounds__(128) k_stage_surface(const __grid_constant__ StageP p) {
+__global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant__ StageP p) {
   using TW = typename std::conditional<WP == 2, __half, float>::type;
   using TT = typename std::conditional<WP >= 1, __half, float>::type;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
