@@ -255,6 +255,7 @@ def lib():
         "cgfd_num_stations": (C.c_int, [P]),
         "cgfd_station_info": (C.c_int, [P, P, P]),
         "cgfd_get_wavefield": (C.c_int, [P, P]),
+        "cgfd_get_peak_motion": (C.c_int, [P, C.c_int, P]),
         "cgfd_set_wavefield": (C.c_int, [P, P]),
         "cgfd_device_bytes": (C.c_size_t, [P]),
         "cgfd_stream": (P, [P]),
@@ -368,6 +369,13 @@ class Simulation:
         out = np.zeros((self.nshot, max(n, 0), 9, self.problem.nt_total), np.float32)
         check(lib().cgfd_get_seismograms(self.h, out.ctypes.data))
         return out[0] if self.nshot == 1 else out
+
+    def peak_motion(self, shot=0):
+        """[15, ny, nx] free-surface peak ground motion (PGV, PGVh, PGVx..z, PGA.., PGD..)."""
+        p = self.problem
+        out = np.zeros((15, p.nj + 6, p.ni + 6), np.float32)
+        check(lib().cgfd_get_peak_motion(self.h, int(shot), out.ctypes.data))
+        return out
 
     def wavefield(self, shot=0):
         p = self.problem

@@ -141,6 +141,8 @@ struct cgfd_problem {
 
   int *d_it = nullptr, *d_flag = nullptr;
   int it = 0;
+  // free-surface peak ground motion [nshot][15][nj][ni] and displacement [nshot][3][nj][ni]
+  float *d_pg = nullptr, *d_dis = nullptr;
 
   bool use_graph = true;
   bool use_tma = true;
@@ -293,6 +295,14 @@ struct cgfd_problem {
         n += timed(5, [&] { return cgfd::launch_source(q, st); });
       }
     }
+    if (free_top) {  // drv_rk_curv_col.cu:519-527: after the last stage, before the level swap
+      cgfd::PgP q;
+      q.ni = ni; q.nj = nj; q.nshot = nshot; q.sx = sx; q.sf = sf;
+      q.off_top = off0 + (long long)(nk - 1) * sz;
+      q.w_end = wbuf[(step + 1) & 1]; q.w_pre = wbuf[step & 1];
+      q.pg = d_pg; q.dis = d_dis; q.dt = dt;
+      n += cgfd::launch_peak_motion(q, st);
+    }
     n += cgfd::launch_advance(d_it, st);
     return n;
   }
@@ -331,7 +341,7 @@ struct cgfd_problem {
     cudaFree(coef); cudaFree(coef16); cudaFree(jac); cudaFree(matx); cudaFree(maty);
     for (Face &f : faces) { cudaFree(f.A); cudaFree(f.B); cudaFree(f.D); cudaFree(f.aux); }
     cudaFree(d_it_begin); cudaFree(d_ext_num); cudaFree(d_src_shot); cudaFree(d_ext_idx); cudaFree(d_ext_wv); cudaFree(d_ext_wt);
-    cudaFree(d_wsc); cudaFree(d_srcb); cudaFree(d_amax); cudaFree(d_tiles);
+    cudaFree(d_wsc); cudaFree(d_srcb); cudaFree(d_amax); cudaFree(d_tiles); cudaFree(d_pg); cudaFree(d_dis);
     cudaFree(d_stf); cudaFree(d_idx8); cudaFree(d_w8); cudaFree(d_seis); cudaFree(d_it); cudaFree(d_flag);
     if (stream) cudaStreamDestroy(stream);
     if (side) cudaStreamDestroy(side);
@@ -461,6 +471,7 @@ void problem_bytes(const cgfd_problem_desc *d, int nshot, const cgfd_source_desc
   if (rec.n > 0)
     r += (size_t)rec.n * 8 * (sizeof(long long) + F) + (size_t)rec.n * 9 * d->nt_total * nshot * F;
   r += 2 * sizeof(int);
+  if (d->free_top) r += (size_t)18 * d->ni * d->nj * nshot * F;
   if (w16) r += (size_t)nshot * (18 * F + 2 * sizeof(unsigned int) + (size_t)d->nt_total * 2 * F);
   if (resident) *resident = r;
   if (peak) *peak = std::max(r, high);
@@ -688,6 +699,13 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
     CK(cudaMemset(p->d_seis, 0, sizeof(float) * p->rec.n * 9 * p->nt_total * nshot));
   }
   make_tiles(p);
+  if (p->free_top) {
+    const size_t nij = (size_t)p->ni * p->nj * nshot;
+    p->d_pg = dmalloc<float>(15 * nij, B);
+    p->d_dis = dmalloc<float>(3 * nij, B);
+    CK(cudaMemset(p->d_pg, 0, sizeof(float) * 15 * nij));
+    CK(cudaMemset(p->d_dis, 0, sizeof(float) * 3 * nij));
+  }
   p->d_it = dmalloc<int>(1, B);
   p->d_flag = dmalloc<int>(1, B);
   CK(cudaMemset(p->d_it, 0, sizeof(int)));
@@ -925,6 +943,23 @@ int cgfd_get_wavefield_shot(cgfd_problem *p, int shot, float *out) {
 }
 
 int cgfd_get_wavefield(cgfd_problem *p, float *out) { return cgfd_get_wavefield_shot(p, 0, out); }
+
+int cgfd_get_peak_motion(cgfd_problem *p, int shot, float *out) {
+  if (!p || !out || shot < 0 || shot >= p->nshot) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
+  if (!p->free_top) { set_err("peak ground motion is computed at a free surface only"); return CGFD_ERR_UNSUPPORTED; }
+  return guarded([&] {
+    CK(cudaSetDevice(p->device));
+    CK(cudaStreamSynchronize(p->stream));
+    const size_t nij = (size_t)p->ni * p->nj, nx = p->ni + 6, ny = p->nj + 6;
+    std::vector<float> pg(15 * nij);
+    CK(cudaMemcpy(pg.data(), p->d_pg + (size_t)shot * 15 * nij, pg.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    std::fill(out, out + 15 * nx * ny, 0.f);  // ghost points stay 0 (PG_slice_output writes nx x ny)
+    for (int q = 0; q < 15; q++)
+      for (int j = 0; j < p->nj; j++)
+        memcpy(out + (size_t)q * nx * ny + (size_t)(j + 3) * nx + 3, pg.data() + (size_t)q * nij + (size_t)j * p->ni,
+               p->ni * sizeof(float));
+  });
+}
 
 }  // extern "C"
 

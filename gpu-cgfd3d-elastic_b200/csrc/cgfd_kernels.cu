@@ -416,6 +416,48 @@ __global__ void k_recv(const __grid_constant__ RecvP r) {
   r.seis[(((long long)shot * r.nsta + sidx) * 9 + c) * r.nt_total + it] = v;
 }
 
+// PG_calcu_gpu (wav_t.cu:281-360) on the top physical plane, every shot: acceleration from the
+// step difference of V, displacement accumulated by the trapezoid rule in double (the
+// reference's 0.5 literal), running maxima of the components and magnitudes.
+__global__ void k_peak_motion(const __grid_constant__ PgP q) {
+  const long long nij = (long long)q.ni * q.nj;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= nij * q.nshot) return;
+  const int shot = (int)(t / nij);
+  const long long ij = t % nij;
+  const int j = (int)(ij / q.ni), i = (int)(ij % q.ni);
+  const long long idx = (long long)shot * 9 * q.sf + q.off_top + (long long)j * q.sx + i;
+  float v1[3], v0[3], a[3], d[3];
+  float *dis = q.dis + (long long)shot * 3 * nij + ij;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    v1[c] = q.w_end[c * q.sf + idx];
+    v0[c] = q.w_pre[c * q.sf + idx];
+    a[c] = fabsf((v1[c] - v0[c]) / q.dt);
+    d[c] = (float)((double)dis[c * nij] + 0.5 * (double)(v1[c] + v0[c]) * (double)q.dt);
+    dis[c * nij] = d[c];
+  }
+  const float val[15] = {sqrtf(v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2]),
+                         sqrtf(v1[0] * v1[0] + v1[1] * v1[1]),
+                         fabsf(v1[0]), fabsf(v1[1]), fabsf(v1[2]),
+                         sqrtf(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]),
+                         sqrtf(a[0] * a[0] + a[1] * a[1]),
+                         a[0], a[1], a[2],
+                         sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]),
+                         sqrtf(d[0] * d[0] + d[1] * d[1]),
+                         fabsf(d[0]), fabsf(d[1]), fabsf(d[2])};
+  float *pg = q.pg + (long long)shot * 15 * nij + ij;
+#pragma unroll
+  for (int n = 0; n < 15; n++)
+    if (pg[n * nij] < val[n]) pg[n * nij] = val[n];
+}
+
+int launch_peak_motion(const PgP &q, cudaStream_t st) {
+  const long long n = (long long)q.ni * q.nj * q.nshot;
+  k_peak_motion<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(q);
+  return 1;
+}
+
 __global__ void k_advance(int *d_it) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *d_it += 1;
 }

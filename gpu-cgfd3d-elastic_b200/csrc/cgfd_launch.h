@@ -34,6 +34,17 @@ struct SrcP {
   unsigned int *amax;          // [nshot][2] max |w_end| per group, collected at stage 3 (wave16)
 };
 
+// Free-surface peak ground motion after each time step (PG_calcu_gpu, wav_t.cu:281-360).
+struct PgP {
+  int ni, nj, nshot;
+  long long sx, sf, off_top;   // off_top: device index of physical (0, 0, nk-1)
+  const float *w_end, *w_pre;  // the step's new and old state
+  float *pg;                   // [nshot][15][nj][ni]
+  float *dis;                  // [nshot][3][nj][ni] displacement accumulator
+  float dt;
+};
+int launch_peak_motion(const PgP &q, cudaStream_t st);
+
 // Station sampling of w_pre (io_funcs.cu:1624-1666).
 struct RecvP {
   int nsta;

@@ -4,7 +4,8 @@
 // for the elastic time-loop path on one GPU: reads the same parameter file keys, grid /
 // metric / medium NetCDF files, .src source file and station list, checks the time step
 // (FP64), runs the B200 time loop through the C ABI and writes the same SAC files
-// (<output_dir>/<station>.<Vx..Txy>.sac, plus <station>.E**.sac strain for isotropic media).
+// (<output_dir>/<station>.<Vx..Txy>.sac, plus <station>.E**.sac strain for isotropic media),
+// and with a free surface the peak ground motion file PG_V_A_D_px0_py0_pz0.nc.
 // Options outside this path (MPI decomposition, media discretisation, slices, ablexp,
 // acoustic / visco-elastic media) are rejected with a message.
 #include <sys/stat.h>
@@ -238,6 +239,29 @@ int run(int argc, char **argv) {
   if (nsta > 0) {
     cgfd_get_seismograms(p, seis.data());
     cgfd_station_info(p, idx.data(), ijk.data());
+  }
+  // free-surface peak ground motion (PG_slice_output, io_funcs.cu:2065-2124)
+  if (d.free_top) {
+    const size_t nx = g.ni + 6, ny = g.nj + 6;
+    std::vector<float> pg(15 * nx * ny);
+    if (cgfd_get_peak_motion(p, 0, pg.data())) fail(std::string("peak motion: ") + cgfd_last_error());
+    cgfd::nc::File f;
+    f.version = 1;  // NC_CLOBBER: classic format
+    f.dims = {{"j", ny}, {"i", nx}};
+    const char *names[15] = {"PGV", "PGVh", "PGVx", "PGVy", "PGVz", "PGA", "PGAh", "PGAx",
+                             "PGAy", "PGAz", "PGD", "PGDh", "PGDx", "PGDy", "PGDz"};
+    std::vector<const float *> data;
+    for (int q = 0; q < 15; q++) {
+      cgfd::nc::Var v;
+      v.name = names[q];
+      v.dimids = {0, 1};
+      f.vars.push_back(v);
+      data.push_back(pg.data() + (size_t)q * nx * ny);
+    }
+    f.gatts.push_back({"global_index_of_first_physical_points", cgfd::nc::INT, {0.0, 0.0}, ""});
+    f.gatts.push_back({"count_index_of_physical_points", cgfd::nc::INT, {(double)g.ni, (double)g.nj}, ""});
+    f.gatts.push_back({"coords_of_mpi_topo", cgfd::nc::INT, {0.0, 0.0, 0.0}, ""});
+    cgfd::nc::write(out + "/PG_V_A_D_px0_py0_pz0.nc", f, data);
   }
   cgfd_problem_destroy(p);
   for (int r = 0; r < nsta; r++) {

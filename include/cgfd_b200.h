@@ -199,6 +199,15 @@ int cgfd_get_wavefield(cgfd_problem *p, float *out);
 /* Overwrite w_pre (physical points only; ghosts stay 0). */
 int cgfd_set_wavefield(cgfd_problem *p, const float *in);
 
+/*
+ * Free-surface peak ground motion accumulated over the steps run so far, [15][ny][nx] in the
+ * order PGV, PGVh, PGVx, PGVy, PGVz, PGA, PGAh, PGAx, PGAy, PGAz, PGD, PGDh, PGDx, PGDy, PGDz
+ * (ghost points 0), i.e. the array PG_slice_output writes (io_funcs.cu:2065-2124), updated
+ * after every time step like PG_calcu_gpu (wav_t.cu:281-360, drv_rk_curv_col.cu:519-527).
+ * CGFD_ERR_UNSUPPORTED when the problem has no free surface.
+ */
+int cgfd_get_peak_motion(cgfd_problem *p, int shot, float *out);
+
 /* Per-shot variants of cgfd_get_wavefield / cgfd_set_wavefield for batched problems. */
 int cgfd_get_wavefield_shot(cgfd_problem *p, int shot, float *out);
 int cgfd_set_wavefield_shot(cgfd_problem *p, int shot, const float *in);

@@ -244,6 +244,10 @@ struct Oracle {
   std::vector<Recv> recv;
   std::vector<float> seismo;  // [nrecv][9][nt_total]
 
+  // free-surface peak ground motion (PG_calcu_gpu, wav_t.cu:281-360): [15][ny][nx] PGV, PGVh,
+  // PGVx..z, PGA, PGAh, PGAx..z, PGD, PGDh, PGDx..z, and the displacement accumulator [3][ny][nx]
+  std::vector<T> pg, dis;
+
   T *lev(int l) { return wave.data() + (size_t)l * 9 * g.siz_icmp; }
   const T *metric_c(int c) const { return metric.data() + (size_t)c * g.siz_icmp; }
   const T *med_c(int c) const { return med.data() + (size_t)c * g.siz_icmp; }
@@ -1015,6 +1019,45 @@ struct Oracle {
     }
   }
 
+  // PG_calcu_gpu, wav_t.cu:281-360: at the top physical plane, acceleration by the step
+  // difference of V, displacement by trapezoidal accumulation (double arithmetic from the
+  // 0.5 literal), and running maxima of components and magnitudes.
+  void pg_calcu(const T *w_end, const T *w_pre) {
+    if (pg.empty()) {
+      pg.assign((size_t)15 * g.siz_iz, (T)0);
+      dis.assign((size_t)3 * g.siz_iz, (T)0);
+    }
+    const T dtt = dt;
+    for (int iy = 0; iy < g.nj; iy++)
+      for (int ix = 0; ix < g.ni; ix++) {
+        const size_t iptr1 = (size_t)(ix + 3) + (size_t)(iy + 3) * g.siz_iy;
+        const size_t iptr = iptr1 + (size_t)g.nk2 * g.siz_iz;
+        T v1[3], v0[3], a[3];
+        for (int c = 0; c < 3; c++) {
+          v1[c] = w_end[c * g.siz_icmp + iptr];
+          v0[c] = w_pre[c * g.siz_icmp + iptr];
+          a[c] = std::fabs((v1[c] - v0[c]) / dtt);
+          T &d = dis[c * g.siz_iz + iptr1];
+          d = (T)((double)d + 0.5 * (double)(T)(v1[c] + v0[c]) * (double)dtt);
+        }
+        const T *D = &dis[0];
+        const T dx = D[iptr1], dy = D[g.siz_iz + iptr1], dz = D[2 * g.siz_iz + iptr1];
+        const T V = std::sqrt(v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2]);
+        const T Vh = std::sqrt(v1[0] * v1[0] + v1[1] * v1[1]);
+        const T A = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+        const T Ah = std::sqrt(a[0] * a[0] + a[1] * a[1]);
+        const T Dm = std::sqrt(dx * dx + dy * dy + dz * dz);
+        const T Dh = std::sqrt(dx * dx + dy * dy);
+        const T val[15] = {V, Vh, std::fabs(v1[0]), std::fabs(v1[1]), std::fabs(v1[2]),
+                           A, Ah, a[0], a[1], a[2],
+                           Dm, Dh, std::fabs(dx), std::fabs(dy), std::fabs(dz)};
+        for (int q = 0; q < 15; q++) {
+          T &m = pg[q * g.siz_iz + iptr1];
+          if (m < val[q]) m = val[q];
+        }
+      }
+  }
+
   // wav_update / wav_update_end, wav_t.cu:362-378
   static void update(size_t n, T coef, T *out, const T *in1, const T *in2) {
 #pragma omp parallel for schedule(static)
@@ -1087,6 +1130,7 @@ struct Oracle {
           });
         }
       }
+      if (free_top) pg_calcu(w_end, w_pre);  // drv_rk_curv_col.cu:519-527, before the level swap
       std::swap(lvl_pre, lvl_end);
       for_faces([&](Face &f) { std::swap(f.lvl_pre, f.lvl_end); });
       it_cur++;
@@ -1187,6 +1231,17 @@ int orc_get_seismograms(void *p, float *out) {
   Handle *h = (Handle *)p;
   const std::vector<float> &s = h->d ? h->d->seismo : h->f->seismo;
   memcpy(out, s.data(), s.size() * sizeof(float));
+  return 0;
+}
+
+// [15][ny][nx] peak ground motion (zeros before the first step or without a free surface)
+int orc_get_peak_motion(void *p, float *out) {
+  Handle *h = (Handle *)p;
+  auto copy = [&](auto *o) {
+    const size_t n = (size_t)15 * o->g.siz_iz;
+    for (size_t q = 0; q < n; q++) out[q] = o->pg.empty() ? 0.f : (float)o->pg[q];
+  };
+  if (h->d) copy(h->d); else copy(h->f);
   return 0;
 }
 

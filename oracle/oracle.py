@@ -35,6 +35,7 @@ def lib():
             ("orc_num_stations", C.c_int, [P]),
             ("orc_get_seismograms", C.c_int, [P, P]),
             ("orc_get_wavefield", C.c_int, [P, P]),
+            ("orc_get_peak_motion", C.c_int, [P, P]),
             ("orc_set_wavefield", C.c_int, [P, P]),
             ("orc_pml_coefs", C.c_int, [P, C.c_int, C.c_int, P, P, P]),
             ("orc_free_mats", C.c_int, [P, P, P]),
@@ -101,6 +102,13 @@ class Oracle:
     def seismograms(self):
         out = np.zeros((self.num_stations, 9, self.problem.nt_total), np.float32)
         lib().orc_get_seismograms(self.h, out.ctypes.data)
+        return out
+
+    def peak_motion(self):
+        """[15, ny, nx] free-surface peak ground motion (PGV, PGVh, PGVx..z, PGA.., PGD..)."""
+        p = self.problem
+        out = np.zeros((15, p.nj + 6, p.ni + 6), np.float32)
+        lib().orc_get_peak_motion(self.h, out.ctypes.data)
         return out
 
     def wavefield(self):

@@ -205,6 +205,13 @@ int main(int argc, char **argv) {
           x->end = x->var + x->siz_ilevel * 3;
         }
 
+  // free-surface peak ground motion, as drv_rk_curv_col.cu:174-186 allocates it
+  float *PG_d = nullptr, *Dis_accu_d = nullptr;
+  if (free_top) {
+    PG_d = init_PGVAD_device(&gd);
+    Dis_accu_d = init_Dis_accu_device(&gd);
+  }
+
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -266,6 +273,10 @@ int main(int argc, char **argv) {
         aux_update(2, cb);
       }
     }
+    if (free_top) {  // drv_rk_curv_col.cu:519-527
+      dim3 pb(8, 8), pgr((ni + 7) / 8, (nj + 7) / 8);
+      PG_calcu_gpu<<<pgr, pb>>>(w_end_d, w_pre_d, gd_d, PG_d, Dis_accu_d, dt);
+    }
     float *t = w_pre_d;
     w_pre_d = w_end_d;
     w_end_d = t;
@@ -298,6 +309,12 @@ int main(int argc, char **argv) {
   cudaMemcpy(w.data(), w_pre_d, sizeof(float) * w.size(), cudaMemcpyDeviceToHost);
   snprintf(path, sizeof(path), "%s/ref_wave.bin", dir);
   write_bin(path, w.data(), w.size());
+  if (free_top) {
+    std::vector<float> pg((size_t)15 * gd.nx * gd.ny);
+    cudaMemcpy(pg.data(), PG_d, sizeof(float) * pg.size(), cudaMemcpyDeviceToHost);
+    snprintf(path, sizeof(path), "%s/ref_pg.bin", dir);
+    write_bin(path, pg.data(), pg.size());
+  }
   snprintf(path, sizeof(path), "%s/ref_info.txt", dir);
   fp = fopen(path, "w");
   fprintf(fp, "nrecv %d\nnsrc %d\nloop_ms %.4f\ncell_stages %lld\n", iorecv.total_number, src.total_number, ms,

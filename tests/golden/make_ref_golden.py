@@ -3,8 +3,8 @@
 
     python tests/golden/make_ref_golden.py <out_dir>
 
-The fixtures hold the reference-computed metrics, seismograms and final wavefield of small
-seeded problems (tests/golden/cases.py); tests/test_cpu_golden.py checks the oracle against
+The fixtures hold the reference-computed metrics, seismograms, final wavefield and free-surface
+peak ground motion (PG_calcu_gpu) of small seeded problems (tests/golden/cases.py); tests/test_cpu_golden.py checks the oracle against
 them without a GPU.
 """
 import os
@@ -28,8 +28,9 @@ def main(out_dir):
         with tempfile.TemporaryDirectory() as d:
             r = ref_io.run(p, d, nsteps)
         sl = (slice(None), slice(3, -3), slice(3, -3), slice(3, -3))
+        extra = {"pg": r["pg"]} if r["pg"] is not None else {}
         np.savez_compressed(os.path.join(out_dir, f"ref_{name}.npz"), metric=r["metric"], seismo=r["seismo"],
-                            wave=r["wave"][sl], nsteps=nsteps)
+                            wave=r["wave"][sl], nsteps=nsteps, **extra)
         print(name, "stations", r["seismo"].shape[0], "max|seis|", float(np.abs(r["seismo"]).max()))
 
 

@@ -39,5 +39,7 @@ def run(p, d, nsteps, timeout=600):
     seis = np.fromfile(os.path.join(d, "ref_seismo.bin"), np.float32).reshape(nrecv, 9, p.nt_total)
     wave = np.fromfile(os.path.join(d, "ref_wave.bin"), np.float32).reshape((9,) + shp)
     metric = np.fromfile(os.path.join(d, "ref_metric.bin"), np.float32).reshape((10,) + shp)
-    return {"seismo": seis, "wave": wave, "metric": metric, "loop_ms": float(info["loop_ms"]),
+    pg_path = os.path.join(d, "ref_pg.bin")
+    pg = np.fromfile(pg_path, np.float32).reshape((15,) + shp[1:]) if os.path.exists(pg_path) else None
+    return {"seismo": seis, "wave": wave, "metric": metric, "pg": pg, "loop_ms": float(info["loop_ms"]),
             "cell_stages": int(info["cell_stages"]), "nsrc": int(info["nsrc"])}

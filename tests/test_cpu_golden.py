@@ -37,3 +37,9 @@ def test_oracle_matches_reference_golden(name):
     assert per_station_rel_l2(o.seismograms()[:, :, :nsteps], ref) <= 2e-5
     w = o.wavefield()[:, 3:-3, 3:-3, 3:-3]
     assert rel_l2(w, z["wave"]) <= 2e-5
+    # free-surface peak ground motion computed by the reference's PG_calcu_gpu
+    assert "pg" in z.files, "fixture lacks the peak ground motion (regenerate with make_ref_golden.py)"
+    pg = o.peak_motion()
+    for q in range(15):
+        assert np.abs(z["pg"][q]).max() > 0
+        assert rel_l2(pg[q], z["pg"][q]) <= 2e-5, q

@@ -42,3 +42,14 @@ def test_cli_sac_output_matches_oracle(tmp_path, medium, metric):
     if medium == "iso":
         hdr, exx = formats.read_sac(os.path.join(out, f"{p.sta.names[0]}.Exx.sac"))
         assert exx.shape[0] == p.nt_total and np.isfinite(exx).all()
+    # peak ground motion file (PG_slice_output): 15 variables (j, i) with ghosts, vs the oracle
+    from scipy.io import netcdf_file
+    with netcdf_file(os.path.join(out, "PG_V_A_D_px0_py0_pz0.nc"), "r", mmap=False) as f:
+        names = ["PGV", "PGVh", "PGVx", "PGVy", "PGVz", "PGA", "PGAh", "PGAx", "PGAy", "PGAz",
+                 "PGD", "PGDh", "PGDx", "PGDy", "PGDz"]
+        pg = np.stack([f.variables[n][:].copy() for n in names])
+        assert list(f.dimensions) == ["j", "i"] and pg.shape == (15, p.nj + 6, p.ni + 6)
+        assert list(f.count_index_of_physical_points) == [p.ni, p.nj]
+    opg = orc.peak_motion()
+    for q in range(15):
+        assert np.linalg.norm(pg[q] - opg[q]) <= 1e-4 * np.linalg.norm(opg[q]), q

@@ -105,3 +105,27 @@ def test_tma_and_direct_bulk_variants_agree(medium):
     for c in range(9):
         scale = float(np.abs(wb[c]).max())
         assert float(np.abs(wa[c] - wb[c]).max()) <= 1e-6 * max(scale, 1e-30)
+
+
+@pytest.mark.parametrize("medium", ["iso", "aniso"])
+def test_peak_motion_matches_oracle(medium):
+    """Free-surface PGV/PGA/PGD (PG_calcu_gpu) over a point-source run, every component."""
+    p = small_problem(medium, nsteps=60)
+    sim, orc = Simulation(p), Oracle(p)
+    sim.run()
+    orc.run()
+    a, b = sim.peak_motion(), orc.peak_motion()
+    assert a.shape == (15, p.nj + 6, p.ni + 6)
+    for q in range(15):
+        assert np.abs(b[q]).max() > 0
+        assert rel_l2(a[q], b[q]) <= 1e-4, q
+    assert not a[:, :3].any() and not a[:, :, :3].any()  # ghost points stay 0
+
+
+def test_peak_motion_needs_free_surface():
+    from cgfd_b200 import CgfdError
+    p = small_problem("iso", free_top=0, nsrc=0, sta_grid=None, nsteps=4)
+    sim = Simulation(p)
+    with pytest.raises(CgfdError) as e:
+        sim.peak_motion()
+    assert e.value.code == -5

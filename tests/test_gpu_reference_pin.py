@@ -39,6 +39,11 @@ def test_oracle_and_product_match_reference(name):
     assert per_station_rel_l2(sim.seismograms()[:, :, :nsteps], rs) <= 1e-4
     assert rel_l2(orc.wavefield(), ref["wave"]) <= 2e-5
     assert rel_l2(sim.wavefield(), ref["wave"]) <= 1e-4
+    # free-surface peak ground motion (PG_calcu_gpu): every component within the same bars
+    if ref["pg"] is not None:
+        for q in range(15):
+            assert rel_l2(orc.peak_motion()[q], ref["pg"][q]) <= 2e-5, q
+            assert rel_l2(sim.peak_motion()[q], ref["pg"][q]) <= 1e-4, q
 
 
 @needs_harness
