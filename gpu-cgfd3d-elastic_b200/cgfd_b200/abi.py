@@ -256,6 +256,7 @@ def lib():
         "cgfd_station_info": (C.c_int, [P, P, P]),
         "cgfd_get_wavefield": (C.c_int, [P, P]),
         "cgfd_get_peak_motion": (C.c_int, [P, C.c_int, P]),
+        "cgfd_get_wavefield_box": (C.c_int, [P, C.c_int, P, P, P, P]),
         "cgfd_set_wavefield": (C.c_int, [P, P]),
         "cgfd_device_bytes": (C.c_size_t, [P]),
         "cgfd_stream": (P, [P]),
@@ -369,6 +370,14 @@ class Simulation:
         out = np.zeros((self.nshot, max(n, 0), 9, self.problem.nt_total), np.float32)
         check(lib().cgfd_get_seismograms(self.h, out.ctypes.data))
         return out[0] if self.nshot == 1 else out
+
+    def wavefield_box(self, start, count, stride=(1, 1, 1), shot=0):
+        """[9, count_z, count_y, count_x] strided sub-box of w_pre (0-based physical indices)."""
+        a = [np.ascontiguousarray(v, np.int32) for v in (start, count, stride)]
+        out = np.zeros((9, int(count[2]), int(count[1]), int(count[0])), np.float32)
+        check(lib().cgfd_get_wavefield_box(self.h, int(shot), a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data,
+                                           out.ctypes.data))
+        return out
 
     def peak_motion(self, shot=0):
         """[15, ny, nx] free-surface peak ground motion (PGV, PGVh, PGVx..z, PGA.., PGD..)."""

@@ -149,7 +149,7 @@ MEDIUM_NAMES = {
 MEDIUM_TYPES = {2: "elastic_iso", 3: "elastic_vti", 4: "elastic_aniso"}
 
 
-def write_case(d, p, nsteps, metric="calculate", check_stability=1):
+def write_case(d, p, nsteps, metric="calculate", check_stability=1, snapshots=None):
     """Writes a full reference-format input set for problem `p` into directory `d`:
     par.json, grid/coord_px0_py0_pz0.nc, media/media_px0_py0_pz0.nc, src.src, station.list
     (and grid/metric_px0_py0_pz0.nc when metric == "import"). Returns the par.json path."""
@@ -189,6 +189,8 @@ def write_case(d, p, nsteps, metric="calculate", check_stability=1):
                                                "beta_max": f["beta_max"], "ref_vel": f["ref_vel"]}}
     if p.free_top:
         par["boundary_z_top"] = {"free": "timg"}
+    if snapshots:
+        par["snapshot"] = list(snapshots)  # entries in the par-file form (1-based grid_index_start)
     path = os.path.join(d, "par.json")
     with open(path, "w") as f:
         json.dump(par, f, indent=2)

@@ -143,6 +143,9 @@ struct cgfd_problem {
   int it = 0;
   // free-surface peak ground motion [nshot][15][nj][ni] and displacement [nshot][3][nj][ni]
   float *d_pg = nullptr, *d_dis = nullptr;
+  // staging buffer of cgfd_get_wavefield_box (grows to the largest box asked for)
+  float *d_box = nullptr;
+  size_t box_cap = 0;
 
   bool use_graph = true;
   bool use_tma = true;
@@ -341,7 +344,7 @@ struct cgfd_problem {
     cudaFree(coef); cudaFree(coef16); cudaFree(jac); cudaFree(matx); cudaFree(maty);
     for (Face &f : faces) { cudaFree(f.A); cudaFree(f.B); cudaFree(f.D); cudaFree(f.aux); }
     cudaFree(d_it_begin); cudaFree(d_ext_num); cudaFree(d_src_shot); cudaFree(d_ext_idx); cudaFree(d_ext_wv); cudaFree(d_ext_wt);
-    cudaFree(d_wsc); cudaFree(d_srcb); cudaFree(d_amax); cudaFree(d_tiles); cudaFree(d_pg); cudaFree(d_dis);
+    cudaFree(d_wsc); cudaFree(d_srcb); cudaFree(d_amax); cudaFree(d_tiles); cudaFree(d_pg); cudaFree(d_dis); cudaFree(d_box);
     cudaFree(d_stf); cudaFree(d_idx8); cudaFree(d_w8); cudaFree(d_seis); cudaFree(d_it); cudaFree(d_flag);
     if (stream) cudaStreamDestroy(stream);
     if (side) cudaStreamDestroy(side);
@@ -943,6 +946,38 @@ int cgfd_get_wavefield_shot(cgfd_problem *p, int shot, float *out) {
 }
 
 int cgfd_get_wavefield(cgfd_problem *p, float *out) { return cgfd_get_wavefield_shot(p, 0, out); }
+
+int cgfd_get_wavefield_box(cgfd_problem *p, int shot, const int *start, const int *count, const int *stride,
+                           float *out) {
+  if (!p || !out || !start || !count || !stride || shot < 0 || shot >= p->nshot) {
+    set_err("invalid argument");
+    return CGFD_ERR_INVALID;
+  }
+  const int n[3] = {p->ni, p->nj, p->nk};
+  for (int a = 0; a < 3; a++)
+    if (count[a] < 1 || stride[a] < 1 || start[a] < 0 || start[a] + (long long)(count[a] - 1) * stride[a] >= n[a]) {
+      set_err("box outside the physical grid");
+      return CGFD_ERR_INVALID;
+    }
+  return guarded([&] {
+    CK(cudaSetDevice(p->device));
+    const size_t cnt = (size_t)9 * count[0] * count[1] * count[2];
+    if (cnt > p->box_cap) {
+      CK(cudaStreamSynchronize(p->stream));
+      cudaFree(p->d_box);
+      p->d_box = nullptr;
+      p->box_cap = 0;
+      size_t acc = 0;
+      p->d_box = dmalloc<float>(cnt, acc);
+      p->box_cap = cnt;
+    }
+    const float *pre = p->wbuf[p->it & 1] + (size_t)shot * 9 * p->sf;
+    cgfd::launch_gather_box(pre, p->sf, p->sx, p->sz, p->off0, start, count, stride, p->d_box, p->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, p->d_box, cnt * sizeof(float), cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaStreamSynchronize(p->stream));
+  });
+}
 
 int cgfd_get_peak_motion(cgfd_problem *p, int shot, float *out) {
   if (!p || !out || shot < 0 || shot >= p->nshot) { set_err("invalid argument"); return CGFD_ERR_INVALID; }

@@ -458,6 +458,26 @@ int launch_peak_motion(const PgP &q, cudaStream_t st) {
   return 1;
 }
 
+__global__ void k_gather_box(const float *__restrict__ w, long long sf, long long sx, long long sz, long long off0,
+                             int3 start, int3 count, int3 stride, float *__restrict__ dst) {
+  const long long per = (long long)count.x * count.y * count.z;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 9 * per; t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t / per);
+    const long long r = t % per;
+    const int i = start.x + (int)(r % count.x) * stride.x;
+    const int j = start.y + (int)((r / count.x) % count.y) * stride.y;
+    const int k = start.z + (int)(r / ((long long)count.x * count.y)) * stride.z;
+    dst[t] = w[c * sf + off0 + (long long)k * sz + (long long)j * sx + i];
+  }
+}
+
+void launch_gather_box(const float *w, long long sf, long long sx, long long sz, long long off0, const int start[3],
+                       const int count[3], const int stride[3], float *dst, cudaStream_t st) {
+  k_gather_box<<<592, 256, 0, st>>>(w, sf, sx, sz, off0, make_int3(start[0], start[1], start[2]),
+                                    make_int3(count[0], count[1], count[2]),
+                                    make_int3(stride[0], stride[1], stride[2]), dst);
+}
+
 __global__ void k_advance(int *d_it) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *d_it += 1;
 }

@@ -34,6 +34,11 @@ struct SrcP {
   unsigned int *amax;          // [nshot][2] max |w_end| per group, collected at stage 3 (wave16)
 };
 
+// Strided sub-box of the 9 wavefield components into dst[9][count_k][count_j][count_i]
+// (io_snap_pack_buff, io_funcs.cu:1569-1595, all components in one launch).
+void launch_gather_box(const float *w, long long sf, long long sx, long long sz, long long off0, const int start[3],
+                       const int count[3], const int stride[3], float *dst, cudaStream_t st);
+
 // Free-surface peak ground motion after each time step (PG_calcu_gpu, wav_t.cu:281-360).
 struct PgP {
   int ni, nj, nshot;

@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <stdexcept>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -60,6 +61,119 @@ void import_vars(const std::string &path, const Grid &g, const std::vector<std::
     std::vector<float> v = cgfd::nc::read_var(path, f, names[c]);
     put_physical(g, v, dst + c * g.siz);
   }
+}
+
+// One "snapshot" entry of the par file, located in the grid like io_snapshot_locate
+// (io_funcs.cu:790-929): 1-based start in the file, indices outside the physical grid dropped.
+struct Snap {
+  std::string name;
+  int start[3], count[3], incre[3];   // 0-based first inner index, inner count, stride
+  int first_in_nc[3];                 // position of `start` in the requested index list
+  int it1, dit, vel, stress, strain;
+  std::unique_ptr<cgfd::nc::RecordWriter> w;
+};
+
+Snap parse_snapshot(const Value &e, const Grid &g) {
+  Snap s;
+  s.name = need(e, "name").as_str();
+  const Value &st = need(e, "grid_index_start"), &ct = need(e, "grid_index_count"), &ic = need(e, "grid_index_incre");
+  if (st.arr.size() != 3 || ct.arr.size() != 3 || ic.arr.size() != 3) fail("snapshot index arrays need 3 entries");
+  const int n[3] = {g.ni, g.nj, g.nk};
+  for (int a = 0; a < 3; a++) {
+    const int g1 = st.arr[a].as_int() - 1, cnt = ct.arr[a].as_int(), inc = ic.arr[a].as_int();
+    if (inc < 1) fail("snapshot " + s.name + ": grid_index_incre must be >= 1");
+    int first = -1, num = 0, pos = 0;
+    for (int q = 0; q < cnt; q++) {
+      const int gi = g1 + q * inc;
+      if (gi >= 0 && gi < n[a]) {
+        if (first < 0) { first = gi; pos = q; }
+        num++;
+      }
+      if (gi > n[a] - 1) break;
+    }
+    if (num == 0) fail("snapshot " + s.name + " lies outside the grid");
+    s.start[a] = first;
+    s.count[a] = num;
+    s.incre[a] = inc;
+    s.first_in_nc[a] = pos;
+  }
+  s.it1 = need(e, "time_index_start").as_int();
+  s.dit = need(e, "time_index_incre").as_int();
+  if (s.dit < 1) fail("snapshot " + s.name + ": time_index_incre must be >= 1");
+  s.vel = e.get("save_velocity") ? e.get("save_velocity")->as_int() : 0;
+  s.stress = e.get("save_stress") ? e.get("save_stress")->as_int() : 0;
+  s.strain = e.get("save_strain") ? e.get("save_strain")->as_int() : 0;
+  return s;
+}
+
+// io_snap_nc_create (io_funcs.cu:931-1047): time (unlimited), k, j, i; time, then the
+// requested groups Vx Vy Vz / Txx Tyy Tzz Txz Tyz Txy / Exx Eyy Ezz Exz Eyz Exy.
+void open_snapshot(Snap &s, const std::string &out) {
+  cgfd::nc::File f;
+  f.version = 1;
+  f.dims = {{"time", 0}, {"k", (uint64_t)s.count[2]}, {"j", (uint64_t)s.count[1]}, {"i", (uint64_t)s.count[0]}};
+  auto var = [&](const char *name, bool scalar) {
+    cgfd::nc::Var v;
+    v.name = name;
+    v.dimids = scalar ? std::vector<int>{0} : std::vector<int>{0, 1, 2, 3};
+    f.vars.push_back(v);
+  };
+  var("time", true);
+  if (s.vel == 1) for (const char *n : {"Vx", "Vy", "Vz"}) var(n, false);
+  if (s.stress == 1) for (const char *n : {"Txx", "Tyy", "Tzz", "Txz", "Tyz", "Txy"}) var(n, false);
+  if (s.strain == 1) for (const char *n : {"Exx", "Eyy", "Ezz", "Exz", "Eyz", "Exy"}) var(n, false);
+  f.gatts.push_back({"first_index_to_snapshot_output", cgfd::nc::INT,
+                     {(double)s.first_in_nc[0], (double)s.first_in_nc[1], (double)s.first_in_nc[2]}, ""});
+  f.gatts.push_back({"first_index_in_this_thread_with_ghosts", cgfd::nc::INT,
+                     {(double)s.start[0] + 3, (double)s.start[1] + 3, (double)s.start[2] + 3}, ""});
+  f.gatts.push_back({"index_stride_in_this_thread", cgfd::nc::INT,
+                     {(double)s.incre[0], (double)s.incre[1], (double)s.incre[2]}, ""});
+  f.gatts.push_back({"coords_of_mpi_topo", cgfd::nc::INT, {0.0, 0.0, 0.0}, ""});
+  s.w.reset(new cgfd::nc::RecordWriter(out + "/" + s.name + "_" + kFnamePart + ".nc", f));
+}
+
+// io_snap_nc_put (io_funcs.cu:1049-1256): at step it (state at the start of the step)
+bool snapshot_due(const Snap &s, int it, int nt_total) {
+  return it >= s.it1 && (it - s.it1) % s.dit == 0 && (it - s.it1) / s.dit <= (nt_total - s.it1) / s.dit;
+}
+
+void put_snapshot(Snap &s, cgfd_problem *p, const Grid &g, const std::vector<float> &medium, int iso, float time) {
+  const size_t n = (size_t)s.count[0] * s.count[1] * s.count[2];
+  std::vector<float> box(9 * n);
+  if (cgfd_get_wavefield_box(p, 0, s.start, s.count, s.incre, box.data()))
+    fail(std::string("snapshot: ") + cgfd_last_error());
+  // device component order Vx Vy Vz Txx Tyy Tzz Tyz Txz Txy; the file's stress order puts Txz
+  // before Tyz
+  const float *c[9];
+  for (int q = 0; q < 9; q++) c[q] = box.data() + q * n;
+  std::vector<const float *> data = {&time};
+  if (s.vel == 1) data.insert(data.end(), {c[0], c[1], c[2]});
+  if (s.stress == 1) data.insert(data.end(), {c[3], c[4], c[5], c[7], c[6], c[8]});
+  std::vector<float> E;
+  if (s.strain == 1) {
+    if (!iso) fail("snapshot strain is computed for elastic_iso media only (io_snap_stress_to_strain_eliso)");
+    // io_snap_stress_to_strain_eliso (io_funcs.cu:1462-1567)
+    E.resize(6 * n);
+    size_t m = 0;
+    for (int kk = 0; kk < s.count[2]; kk++)
+      for (int jj = 0; jj < s.count[1]; jj++)
+        for (int ii = 0; ii < s.count[0]; ii++, m++) {
+          const size_t at = g.at(s.start[0] + ii * s.incre[0], s.start[1] + jj * s.incre[1], s.start[2] + kk * s.incre[2]);
+          const float lam = medium[g.siz + at], mu = medium[2 * g.siz + at];
+          const float E1 = (float)((lam + mu) / (mu * (3.0 * lam + 2.0 * mu)));
+          const float E2 = (float)(-lam / (2.0 * mu * (3.0 * lam + 2.0 * mu)));
+          const float E3 = (float)(1.0 / mu);
+          const float E0 = E2 * (c[3][m] + c[4][m] + c[5][m]);
+          E[0 * n + m] = E0 - (E2 - E1) * c[3][m];
+          E[1 * n + m] = E0 - (E2 - E1) * c[4][m];
+          E[2 * n + m] = E0 - (E2 - E1) * c[5][m];
+          E[3 * n + m] = 0.5f * E3 * c[7][m];  // Exz
+          E[4 * n + m] = 0.5f * E3 * c[6][m];  // Eyz
+          E[5 * n + m] = 0.5f * E3 * c[8][m];  // Exy
+        }
+    for (int q = 0; q < 6; q++) data.push_back(E.data() + q * n);
+  }
+  s.w->append(data);
 }
 
 void mkdirs(const std::string &d) {
@@ -222,15 +336,37 @@ int run(int argc, char **argv) {
   if (cgfd_problem_create(&d, &p)) fail(std::string("create: ") + cgfd_last_error());
   printf("grid %d x %d x %d, dt %g, nt_total %d, device %.2f GB\n", g.ni, g.nj, g.nk, dt, nt_total,
          cgfd_device_bytes(p) / 1e9);
-  int step = 0;
+  // snapshots (io_snapshot_locate + io_snap_nc_create); taken at the start of a step
+  std::vector<Snap> snaps;
+  if (const Value *sv = par.get("snapshot"))
+    for (const Value &e : sv->arr) {
+      snaps.push_back(parse_snapshot(e, g));
+      open_snapshot(snaps.back(), out);
+    }
+  auto next_snapshot = [&](int from) {
+    int best = nt_total;
+    for (const Snap &s : snaps)
+      for (int it = std::max(from, s.it1); it < nt_total; it++)
+        if (snapshot_due(s, it, nt_total)) { best = std::min(best, it); break; }
+    return best;
+  };
+  int step = 0, last_print = 0;
   while (step < nt_total) {
-    int n = std::min(100, nt_total - step);
+    for (Snap &s : snaps)
+      if (snapshot_due(s, step, nt_total))
+        put_snapshot(s, p, g, medium, d.medium_type == CGFD_MEDIUM_ELASTIC_ISO,
+                     (float)step * d.dt + d.t0);  // t_cur = it * dt + t0 in float (drv_rk_curv_col.cu:195)
+    int n = std::min({100, nt_total - step, std::max(1, next_snapshot(step + 1) - step)});
     int rc = cgfd_run(p, n);
     if (rc) { std::string m = cgfd_last_error(); cgfd_problem_destroy(p); fail("run: " + m); }
     step += n;
-    printf("-> it=%d\n", step);
-    fflush(stdout);
+    if (step - last_print >= 100 || step == nt_total) {
+      printf("-> it=%d\n", step);
+      fflush(stdout);
+      last_print = step;
+    }
   }
+  snaps.clear();  // closes the snapshot files
 
   // ---- SAC output (io_recv_output_sac, io_funcs.cu:1775-1902)
   int nsta = cgfd_num_stations(p);

@@ -240,6 +240,53 @@ std::vector<float> read_var(const std::string &path, const File &f, const std::s
   return out;
 }
 
+namespace {
+
+std::vector<unsigned char> build_header(const File &f, const std::vector<uint64_t> &begins, uint32_t numrecs) {
+  Writer w;
+  w.b.insert(w.b.end(), {'C', 'D', 'F', (unsigned char)f.version});
+  w.u32(numrecs);
+  if (f.dims.empty()) { w.u32(0); w.u32(0); }
+  else {
+    w.u32(TAG_DIM);
+    w.u32((uint32_t)f.dims.size());
+    for (const Dim &d : f.dims) { w.name(d.name); w.u32((uint32_t)d.len); }
+  }
+  put_atts(w, f.gatts);
+  if (f.vars.empty()) { w.u32(0); w.u32(0); }
+  else {
+    w.u32(TAG_VAR);
+    w.u32((uint32_t)f.vars.size());
+    for (size_t v = 0; v < f.vars.size(); v++) {
+      const Var &var = f.vars[v];
+      w.name(var.name);
+      w.u32((uint32_t)var.dimids.size());
+      for (int d : var.dimids) w.u32((uint32_t)d);
+      put_atts(w, var.atts);
+      w.u32((uint32_t)var.type);
+      w.u32(var.vsize > 0xFFFFFFFCull ? 0xFFFFFFFFu : (uint32_t)var.vsize);
+      if (f.version == 1) w.u32((uint32_t)begins[v]);
+      else w.u64(begins[v]);
+    }
+  }
+  return w.b;
+}
+
+// big-endian copy of n floats
+void put_floats(std::vector<unsigned char> &tmp, const float *src, uint64_t n, uint64_t padded) {
+  tmp.assign(padded, 0);
+  for (uint64_t e = 0; e < n; e++) {
+    uint32_t u;
+    memcpy(&u, &src[e], 4);
+    tmp[4 * e] = (unsigned char)(u >> 24);
+    tmp[4 * e + 1] = (unsigned char)(u >> 16);
+    tmp[4 * e + 2] = (unsigned char)(u >> 8);
+    tmp[4 * e + 3] = (unsigned char)u;
+  }
+}
+
+}  // namespace
+
 void write(const std::string &path, File f, const std::vector<const float *> &data) {
   if (data.size() != f.vars.size()) throw std::runtime_error("netcdf write: one data array per variable");
   // sizes; all variables fixed-size float
@@ -248,64 +295,68 @@ void write(const std::string &path, File f, const std::vector<const float *> &da
     f.vars[v].type = FLOAT;
     uint64_t n = 1;
     for (int d : f.vars[v].dimids) {
-      if (f.dims[d].len == 0) throw std::runtime_error("netcdf write: record variables are not supported");
+      if (f.dims[d].len == 0) throw std::runtime_error("netcdf write: record variables go through RecordWriter");
       n *= f.dims[d].len;
     }
     nelem[v] = n;
     f.vars[v].vsize = pad4(n * 4);
   }
-  auto header = [&](const std::vector<uint64_t> &begins) {
-    Writer w;
-    w.b.insert(w.b.end(), {'C', 'D', 'F', (unsigned char)f.version});
-    w.u32(0);  // numrecs
-    if (f.dims.empty()) { w.u32(0); w.u32(0); }
-    else {
-      w.u32(TAG_DIM);
-      w.u32((uint32_t)f.dims.size());
-      for (const Dim &d : f.dims) { w.name(d.name); w.u32((uint32_t)d.len); }
-    }
-    put_atts(w, f.gatts);
-    if (f.vars.empty()) { w.u32(0); w.u32(0); }
-    else {
-      w.u32(TAG_VAR);
-      w.u32((uint32_t)f.vars.size());
-      for (size_t v = 0; v < f.vars.size(); v++) {
-        const Var &var = f.vars[v];
-        w.name(var.name);
-        w.u32((uint32_t)var.dimids.size());
-        for (int d : var.dimids) w.u32((uint32_t)d);
-        put_atts(w, var.atts);
-        w.u32((uint32_t)var.type);
-        w.u32(var.vsize > 0xFFFFFFFCull ? 0xFFFFFFFFu : (uint32_t)var.vsize);
-        if (f.version == 1) w.u32((uint32_t)begins[v]);
-        else w.u64(begins[v]);
-      }
-    }
-    return w.b;
-  };
   std::vector<uint64_t> begins(f.vars.size(), 0);
-  uint64_t hsize = header(begins).size();
-  uint64_t off = hsize;
+  uint64_t off = build_header(f, begins, 0).size();
   for (size_t v = 0; v < f.vars.size(); v++) { begins[v] = off; off += f.vars[v].vsize; }
   if (f.version == 1 && off > 0x7FFFFFFFull) throw std::runtime_error("netcdf write: file too large for CDF-1");
-  std::vector<unsigned char> h = header(begins);
+  std::vector<unsigned char> h = build_header(f, begins, 0);
   FILE *fp = fopen(path.c_str(), "wb");
   if (!fp) throw std::runtime_error("cannot create " + path);
   bool ok = fwrite(h.data(), 1, h.size(), fp) == h.size();
   std::vector<unsigned char> tmp;
   for (size_t v = 0; v < f.vars.size() && ok; v++) {
-    tmp.assign(f.vars[v].vsize, 0);
-    for (uint64_t e = 0; e < nelem[v]; e++) {
-      uint32_t u;
-      memcpy(&u, &data[v][e], 4);
-      tmp[4 * e] = (unsigned char)(u >> 24);
-      tmp[4 * e + 1] = (unsigned char)(u >> 16);
-      tmp[4 * e + 2] = (unsigned char)(u >> 8);
-      tmp[4 * e + 3] = (unsigned char)u;
-    }
+    put_floats(tmp, data[v], nelem[v], f.vars[v].vsize);
     ok = fwrite(tmp.data(), 1, tmp.size(), fp) == tmp.size();
   }
   if (fclose(fp) != 0 || !ok) throw std::runtime_error("netcdf write failed: " + path);
+}
+
+RecordWriter::RecordWriter(const std::string &path, File f) : path_(path) {
+  nelem_.resize(f.vars.size());
+  for (size_t v = 0; v < f.vars.size(); v++) {
+    Var &var = f.vars[v];
+    var.type = FLOAT;
+    if (var.dimids.empty() || f.dims[var.dimids[0]].len != 0)
+      throw std::runtime_error("netcdf record writer: every variable needs the record dimension first");
+    uint64_t n = 1;
+    for (size_t q = 1; q < var.dimids.size(); q++) n *= f.dims[var.dimids[q]].len;
+    nelem_[v] = n;
+    var.vsize = pad4(n * 4);  // per record
+  }
+  std::vector<uint64_t> begins(f.vars.size(), 0);
+  uint64_t off = build_header(f, begins, 0).size();
+  for (size_t v = 0; v < f.vars.size(); v++) { begins[v] = off; off += f.vars[v].vsize; }
+  std::vector<unsigned char> h = build_header(f, begins, 0);
+  fp_ = fopen(path.c_str(), "wb+");
+  if (!fp_) throw std::runtime_error("cannot create " + path);
+  if (fwrite(h.data(), 1, h.size(), fp_) != h.size()) throw std::runtime_error("netcdf write failed: " + path);
+  fflush(fp_);
+}
+
+void RecordWriter::append(const std::vector<const float *> &data) {
+  if (data.size() != nelem_.size()) throw std::runtime_error("netcdf append: one slab per variable");
+  if (fseek(fp_, 0, SEEK_END) != 0) throw std::runtime_error("netcdf append failed: " + path_);
+  std::vector<unsigned char> tmp;
+  bool ok = true;
+  for (size_t v = 0; v < nelem_.size() && ok; v++) {
+    put_floats(tmp, data[v], nelem_[v], pad4(nelem_[v] * 4));
+    ok = fwrite(tmp.data(), 1, tmp.size(), fp_) == tmp.size();
+  }
+  nrec_++;
+  unsigned char q[4] = {(unsigned char)(nrec_ >> 24), (unsigned char)(nrec_ >> 16), (unsigned char)(nrec_ >> 8),
+                        (unsigned char)nrec_};
+  ok = ok && fseek(fp_, 4, SEEK_SET) == 0 && fwrite(q, 1, 4, fp_) == 4 && fflush(fp_) == 0;
+  if (!ok) throw std::runtime_error("netcdf append failed: " + path_);
+}
+
+RecordWriter::~RecordWriter() {
+  if (fp_) fclose(fp_);
 }
 
 }  // namespace nc

@@ -5,6 +5,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstdio>
 #include <string>
 #include <vector>
 
@@ -55,6 +56,26 @@ std::vector<float> read_var(const std::string &path, const File &f, const std::s
 // Writes `f` (dims, global atts, fixed-size float variables) with the given data arrays,
 // one per variable in f.vars order. Throws on I/O errors.
 void write(const std::string &path, File f, const std::vector<const float *> &data);
+
+// A file of float record variables (every variable's first dimension is the record
+// dimension, length 0 in f.dims): the header goes out at construction, append() adds one
+// record (one slab per variable, f.vars order) and rewrites numrecs, so the file is valid
+// after every record (like nc_put_vara on an NC_UNLIMITED dimension).
+class RecordWriter {
+ public:
+  RecordWriter(const std::string &path, File f);
+  ~RecordWriter();
+  RecordWriter(const RecordWriter &) = delete;
+  RecordWriter &operator=(const RecordWriter &) = delete;
+  void append(const std::vector<const float *> &data);
+  uint64_t records() const { return nrec_; }
+
+ private:
+  FILE *fp_ = nullptr;
+  std::string path_;
+  std::vector<uint64_t> nelem_;
+  uint64_t nrec_ = 0;
+};
 
 }  // namespace nc
 }  // namespace cgfd

@@ -200,6 +200,15 @@ int cgfd_get_wavefield(cgfd_problem *p, float *out);
 int cgfd_set_wavefield(cgfd_problem *p, const float *in);
 
 /*
+ * Strided sub-box of the current wavefield w_pre (the state at the start of the next step),
+ * all 9 components: out[9][count[2]][count[1]][count[0]] with point (n0,n1,n2) at physical
+ * index start[a] + n_a * stride[a] (0-based, x,y,z order). Replaces: the per-component
+ * io_snap_pack_buff launches + copies of io_snap_nc_put (io_funcs.cu:1049-1256, 1569-1595).
+ */
+int cgfd_get_wavefield_box(cgfd_problem *p, int shot, const int *start, const int *count, const int *stride,
+                           float *out);
+
+/*
  * Free-surface peak ground motion accumulated over the steps run so far, [15][ny][nx] in the
  * order PGV, PGVh, PGVx, PGVy, PGVz, PGA, PGAh, PGAx, PGAy, PGAz, PGD, PGDh, PGDx, PGDy, PGDz
  * (ghost points 0), i.e. the array PG_slice_output writes (io_funcs.cu:2065-2124), updated

@@ -53,3 +53,58 @@ def test_cli_sac_output_matches_oracle(tmp_path, medium, metric):
     opg = orc.peak_motion()
     for q in range(15):
         assert np.linalg.norm(pg[q] - opg[q]) <= 1e-4 * np.linalg.norm(opg[q]), q
+
+
+def test_cli_snapshots_match_oracle(tmp_path):
+    """"snapshot" entries (io_snap_nc_create/put): a free-surface slice every 5 steps with
+    velocity, stress and strain, and a strided volume at the last step, as NetCDF record
+    variables, against the oracle's wavefield at the same steps."""
+    nsteps = 30
+    p = small_problem("iso", nsteps=nsteps)
+    snaps = [{"name": "surf", "grid_index_start": [1, 1, p.nk], "grid_index_count": [p.ni, p.nj, 1],
+              "grid_index_incre": [1, 1, 1], "time_index_start": 0, "time_index_incre": 5,
+              "save_velocity": 1, "save_stress": 1, "save_strain": 1},
+             {"name": "vol", "grid_index_start": [2, 1, 1], "grid_index_count": [p.ni, p.nj, p.nk],
+              "grid_index_incre": [2, 3, 2], "time_index_start": p.nt_total - 1, "time_index_incre": 1,
+              "save_velocity": 1, "save_stress": 0, "save_strain": 0}]
+    par = formats.write_case(str(tmp_path), p, nsteps, snapshots=snaps)
+    r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    from cgfd_b200 import synth
+    from scipy.io import netcdf_file
+    p.metric = synth.metrics(p.coord)
+    orc = Oracle(p)
+    states = {}
+    for it in range(p.nt_total):
+        states[it] = orc.wavefield()  # w_pre at the start of step it
+        orc.run(1)
+    out = os.path.join(str(tmp_path), "output")
+    lam, mu = p.medium[1], p.medium[2]
+    with netcdf_file(os.path.join(out, "surf_px0_py0_pz0.nc"), "r", mmap=False) as f:
+        assert list(f.dimensions) == ["time", "k", "j", "i"] and f.dimensions["time"] is None
+        t = f.variables["time"][:].copy()
+        steps = list(range(0, p.nt_total, 5))
+        assert len(t) == len(steps) and np.allclose(t, np.array(steps, np.float32) * np.float32(p.dt))
+        names = ["Vx", "Vy", "Vz", "Txx", "Tyy", "Tzz", "Txz", "Tyz", "Txy"]
+        comp = [0, 1, 2, 3, 4, 5, 7, 6, 8]
+        for n, it in enumerate(steps):
+            w = states[it][:, p.nk + 2:p.nk + 3, 3:-3, 3:-3]
+            for name, c in zip(names, comp):
+                got = f.variables[name][n]
+                assert np.linalg.norm(got - w[c]) <= 1e-4 * max(np.linalg.norm(w[c]), 1e-30), (name, it)
+            # isotropic strain from stress (io_snap_stress_to_strain_eliso)
+            l, m = lam[p.nk + 2:p.nk + 3, 3:-3, 3:-3], mu[p.nk + 2:p.nk + 3, 3:-3, 3:-3]
+            e1 = (l + m) / (m * (3 * l + 2 * m))
+            e2 = -l / (2 * m * (3 * l + 2 * m))
+            exx = e2 * (w[3] + w[4] + w[5]) - (e2 - e1) * w[3]
+            got = f.variables["Exx"][n]
+            assert np.linalg.norm(got - exx) <= 1e-4 * max(np.linalg.norm(exx), 1e-30)
+            got = f.variables["Exz"][n]
+            assert np.linalg.norm(got - 0.5 / m * w[7]) <= 1e-4 * max(np.linalg.norm(w[7] / m), 1e-30)
+        assert list(f.first_index_in_this_thread_with_ghosts) == [3, 3, p.nk + 2]
+    with netcdf_file(os.path.join(out, "vol_px0_py0_pz0.nc"), "r", mmap=False) as f:
+        vx = f.variables["Vx"][:].copy()
+        assert vx.shape == (1, (p.nk + 1) // 2, (p.nj + 2) // 3, p.ni // 2)
+        w = states[p.nt_total - 1][0, 3:-3:2, 3:-3:3, 4:-3:2]
+        assert np.linalg.norm(vx[0] - w) <= 1e-4 * np.linalg.norm(w)
+        assert list(f.index_stride_in_this_thread) == [2, 3, 2]
