@@ -514,6 +514,14 @@ std::vector<float> source_bounds(const cgfd_problem *p) {
 
 void make_tiles(cgfd_problem *p);
 
+// sources given by physical coordinates: located on the current device (nullptr otherwise)
+const cgfd::Located *locate_sources(const cgfd_problem_desc *d, cgfd::Located &out) {
+  if (d->src.num <= 0 || d->src.loc_coord_type != 1) return nullptr;
+  std::vector<int> depth(d->src.num, d->src.loc_3dim == 1 ? 1 : 0);
+  cgfd::locate_coords(d, d->src.num, d->src.loc, depth.data(), out);
+  return &out;
+}
+
 void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_source_desc *shots) {
   cgfd::validate_desc(d);
   if (nshot < 1) throw cgfd::Error(CGFD_ERR_INVALID, "nshot must be >= 1");
@@ -629,7 +637,8 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
     }
   // sources: one set per shot, concatenated (each source knows its shot)
   if (!shots) {
-    cgfd::src_setup(d, p->src);
+    cgfd::Located sl;
+    cgfd::src_setup(d, p->src, locate_sources(d, sl));
     p->src_shot.assign(p->src.nsrc, 0);
   } else {
     cgfd::SrcHost &all = p->src;
@@ -639,7 +648,8 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
       cgfd_problem_desc ds = *d;
       ds.src = shots[sh];
       cgfd::validate_desc(&ds);
-      cgfd::src_setup(&ds, per[sh]);
+      cgfd::Located sl;
+      cgfd::src_setup(&ds, per[sh], locate_sources(&ds, sl));
       all.max_nt = std::max(all.max_nt, per[sh].max_nt);
       all.max_ext = std::max(all.max_ext, per[sh].max_ext);
       all.force |= per[sh].force;
@@ -687,8 +697,34 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
     CK(cudaMemcpy(p->d_ext_wt, s.ext_wt.data(), ne * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(p->d_stf, s.stf.data(), s.stf.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
-  // stations
-  cgfd::recv_setup(d, p->rec);
+  // stations (those given by physical coordinates located on the device first)
+  {
+    const cgfd_station_desc &st = d->sta;
+    std::vector<int> which;
+    std::vector<float> xyz;
+    std::vector<int> depth;
+    for (int r = 0; r < st.num; r++)
+      if (st.flag_coord[r] == 1) {
+        which.push_back(r);
+        xyz.insert(xyz.end(), st.loc + 3 * r, st.loc + 3 * r + 3);
+        depth.push_back(st.flag_depth[r] == 1);
+      }
+    cgfd::Located rl;
+    if (!which.empty()) {
+      cgfd::Located part;
+      cgfd::locate_coords(d, (int)which.size(), xyz.data(), depth.data(), part);
+      rl.idx.assign(3 * (size_t)st.num, -1000);
+      rl.inc.assign(3 * (size_t)st.num, 0.f);
+      rl.xyz.assign(3 * (size_t)st.num, 0.f);
+      for (size_t w = 0; w < which.size(); w++)
+        for (int a = 0; a < 3; a++) {
+          rl.idx[3 * which[w] + a] = part.idx[3 * w + a];
+          rl.inc[3 * which[w] + a] = part.inc[3 * w + a];
+          rl.xyz[3 * which[w] + a] = part.xyz[3 * w + a];
+        }
+    }
+    cgfd::recv_setup(d, p->rec, which.empty() ? nullptr : &rl);
+  }
   if (p->rec.n > 0) {
     std::vector<long long> idx8((size_t)p->rec.n * 8);
     for (int r = 0; r < p->rec.n; r++)

@@ -43,8 +43,10 @@ void validate_desc(const cgfd_problem_desc *d) {
   if (d->src.num < 0 || d->sta.num < 0) throw Error(CGFD_ERR_INVALID, "negative source/station count");
   if (d->src.num > 0) {
     if (!d->src.loc || !d->src.t_start) throw Error(CGFD_ERR_INVALID, "source loc/t_start missing");
-    if (d->src.loc_coord_type != 0)
-      throw Error(CGFD_ERR_UNSUPPORTED, "sources located by physical coordinates are not supported");
+    if (d->src.loc_coord_type != 0 && d->src.loc_coord_type != 1)
+      throw Error(CGFD_ERR_INVALID, "loc_coord_type must be 0 (grid index) or 1 (physical coordinates)");
+    if (d->src.loc_coord_type == 1 && !d->coord)
+      throw Error(CGFD_ERR_INVALID, "coord is required to locate sources by physical coordinates");
     if (d->src.stf_given == 0 && (!d->src.wavelet || !d->src.wavelet_coefs || !d->src.cmp))
       throw Error(CGFD_ERR_INVALID, "wavelet source needs wavelet, wavelet_coefs and cmp");
     if (d->src.stf_given == 1 && (!d->src.cmp_values || d->src.stf_nt < 1 || !(d->src.stf_dt > 0)))
@@ -54,9 +56,12 @@ void validate_desc(const cgfd_problem_desc *d) {
   }
   if (d->sta.num > 0) {
     if (!d->sta.loc || !d->sta.flag_coord || !d->sta.flag_depth) throw Error(CGFD_ERR_INVALID, "station arrays missing");
-    for (int r = 0; r < d->sta.num; r++)
-      if (d->sta.flag_coord[r] != 0)
-        throw Error(CGFD_ERR_UNSUPPORTED, "stations located by physical coordinates are not supported");
+    for (int r = 0; r < d->sta.num; r++) {
+      if (d->sta.flag_coord[r] != 0 && d->sta.flag_coord[r] != 1)
+        throw Error(CGFD_ERR_INVALID, "station flag_coord must be 0 (grid index) or 1 (physical coordinates)");
+      if (d->sta.flag_coord[r] == 1 && !d->coord)
+        throw Error(CGFD_ERR_INVALID, "coord is required to locate stations by physical coordinates");
+    }
   }
 }
 
@@ -279,7 +284,7 @@ static double lag_interp(const std::vector<double> &t, const std::vector<double>
   return Li;
 }
 
-void src_setup(const cgfd_problem_desc *d, SrcHost &s) {
+void src_setup(const cgfd_problem_desc *d, SrcHost &s, const Located *loc) {
   s = SrcHost();
   const cgfd_source_desc &in = d->src;
   if (in.num <= 0) return;
@@ -295,15 +300,25 @@ void src_setup(const cgfd_problem_desc *d, SrcHost &s) {
   const double rk_time[4] = {0.0, 0.5, 0.5, 1.0};
   const int n[3] = {d->ni, d->nj, d->nk};
   for (int is = 0; is < in.num; is++) {
-    double c[3] = {in.loc[3 * is], in.loc[3 * is + 1], in.loc[3 * is + 2]};
-    if (in.loc_3dim == 1) c[2] = (d->nk - 1) - (float)c[2];
     int gi[3];
     double inc[3];
     bool outside = false;
-    for (int a = 0; a < 3; a++) {
-      gi[a] = (int)((float)c[a] + 0.5f);
-      inc[a] = (float)c[a] - gi[a];
-      if (gi[a] < 0 || gi[a] > n[a] - 1) outside = true;
+    if (in.loc_coord_type == 1) {
+      // located by coordinates: nearest grid point and shift (src_t.cu:341-398); without the
+      // location (sizing only) the source counts as inside
+      for (int a = 0; a < 3; a++) {
+        gi[a] = loc ? loc->idx[3 * is + a] : n[a] / 2;
+        inc[a] = loc ? loc->inc[3 * is + a] : 0.0f;
+        if (gi[a] < 0 || gi[a] > n[a] - 1) outside = true;
+      }
+    } else {
+      double c[3] = {in.loc[3 * is], in.loc[3 * is + 1], in.loc[3 * is + 2]};
+      if (in.loc_3dim == 1) c[2] = (d->nk - 1) - (float)c[2];
+      for (int a = 0; a < 3; a++) {
+        gi[a] = (int)((float)c[a] + 0.5f);
+        inc[a] = (float)c[a] - gi[a];
+        if (gi[a] < 0 || gi[a] > n[a] - 1) outside = true;
+      }
     }
     bool here = true;
     for (int a = 0; a < 3; a++)
@@ -404,15 +419,34 @@ void src_setup(const cgfd_problem_desc *d, SrcHost &s) {
 // Stations (io_funcs.cu:24-299, 1624-1666): 1-based grid index, floor location, trilinear
 // weights with the reference's corner usage (corner 5 counted twice, corner 4 never).
 // ---------------------------------------------------------------------------------------
-void recv_setup(const cgfd_problem_desc *d, RecvHost &r) {
+void recv_setup(const cgfd_problem_desc *d, RecvHost &r, const Located *loc) {
   r = RecvHost();
   const cgfd_station_desc &in = d->sta;
   for (int ir = 0; ir < in.num; ir++) {
-    float c[3] = {in.loc[3 * ir] - 1, in.loc[3 * ir + 1] - 1, in.loc[3 * ir + 2]};
-    if (in.flag_depth[ir] == 1) c[2] = (d->nk - 1) - c[2];
-    else c[2] -= 1;
-    int ix = (int)c[0], iy = (int)c[1], iz = (int)c[2];
-    double dx = c[0] - ix, dy = c[1] - iy, dz = c[2] - iz;
+    int ix, iy, iz;
+    double dx, dy, dz;
+    if (in.flag_coord[ir] == 1) {
+      // located by coordinates; a negative shift moves to the lower neighbour (io_funcs.cu:150-169)
+      int id[3];
+      float inc[3];
+      const int n[3] = {d->ni, d->nj, d->nk};
+      for (int a = 0; a < 3; a++) {
+        id[a] = loc ? loc->idx[3 * ir + a] : n[a] / 2;
+        inc[a] = loc ? loc->inc[3 * ir + a] : 0.0f;
+        if (id[a] != -1000 && inc[a] < 0.0) {
+          inc[a] = (float)(1.0 + inc[a]);
+          id[a] -= 1;
+        }
+      }
+      ix = id[0]; iy = id[1]; iz = id[2];
+      dx = inc[0]; dy = inc[1]; dz = inc[2];
+    } else {
+      float c[3] = {in.loc[3 * ir] - 1, in.loc[3 * ir + 1] - 1, in.loc[3 * ir + 2]};
+      if (in.flag_depth[ir] == 1) c[2] = (d->nk - 1) - c[2];
+      else c[2] -= 1;
+      ix = (int)c[0]; iy = (int)c[1]; iz = (int)c[2];
+      dx = c[0] - ix; dy = c[1] - iy; dz = c[2] - iz;
+    }
     if (!(ix >= 0 && ix <= d->ni - 1 && iy >= 0 && iy <= d->nj - 1 && iz >= 0 && iz <= d->nk - 1)) continue;
     r.i.push_back(ix); r.j.push_back(iy); r.k.push_back(iz);
     r.input_index.push_back(ir);

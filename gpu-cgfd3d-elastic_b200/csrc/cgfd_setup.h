@@ -41,6 +41,17 @@ void pml_setup(const cgfd_problem_desc *d, PmlFaceHost faces[3][2]);
 // [nj][ni][9] matVx2Vz / matVy2Vz at the top layer
 void dvh2dvz(const cgfd_problem_desc *d, std::vector<float> &matx, std::vector<float> &maty);
 
+// Points given by physical coordinates, located like the reference: global physical index
+// (-1000 when outside the grid), fractional shift, and the coordinates after a depth was
+// converted to z.
+struct Located {
+  std::vector<int> idx;
+  std::vector<float> inc;
+  std::vector<float> xyz;
+};
+// use_depth[q]: z of point q is a depth below the free surface. Runs on the current device.
+void locate_coords(const cgfd_problem_desc *d, int n, const float *xyz, const int *use_depth, Located &out);
+
 struct SrcHost {
   int nsrc = 0, max_ext = 0, max_nt = 0, force = 0, moment = 0;
   std::vector<int> it_begin, ext_num;
@@ -48,7 +59,9 @@ struct SrcHost {
   std::vector<float> ext_wv, ext_wt;      // coef*(1/rho)/jac, coef/jac
   std::vector<float> stf;                 // [nsrc][max_nt][4][9]
 };
-void src_setup(const cgfd_problem_desc *d, SrcHost &s);
+// loc: located coordinates of the sources (loc_coord_type 1); nullptr for grid indices, or
+// when only sizes are needed (every coordinate source is then taken as inside the grid)
+void src_setup(const cgfd_problem_desc *d, SrcHost &s, const Located *loc = nullptr);
 
 struct RecvHost {
   int n = 0;
@@ -56,7 +69,9 @@ struct RecvHost {
   std::vector<int> input_index;           // position in the station list
   std::vector<float> w8;                  // [n][8]
 };
-void recv_setup(const cgfd_problem_desc *d, RecvHost &r);
+// loc: located coordinates of the stations with flag_coord 1 (indexed like the input list);
+// nullptr when only sizes are needed (every such station is then taken as inside the grid)
+void recv_setup(const cgfd_problem_desc *d, RecvHost &r, const Located *loc = nullptr);
 
 void validate_desc(const cgfd_problem_desc *d);
 

@@ -35,6 +35,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <memory>
 #include <vector>
 #include <stdexcept>
 
@@ -202,6 +203,201 @@ inline int voigt(int a, int b) {
 
 // ---------------------------------------------------------------------------------------
 // The oracle state: reference structs flattened.
+// ---------------------------------------------------------------------------------------
+// Location by physical coordinates (gd_t.cu:949-1835, fdlib_math.cu:168-245), float
+// arithmetic as in the reference.
+// ---------------------------------------------------------------------------------------
+struct Locator {
+  const Grid &g;
+  const float *x, *y, *z;
+  float xmin, xmax, ymin, ymax, zmin, zmax;
+  int ts[3][4], te[3][4];
+  float tx0[4][4], tx1[4][4], ty0[4][4], ty1[4][4];
+
+  Locator(const Grid &g_, const float *coord) : g(g_), x(coord), y(coord + g_.siz_icmp), z(coord + 2 * g_.siz_icmp) {
+    xmin = xmax = x[0]; ymin = ymax = y[0]; zmin = zmax = z[0];
+    for (size_t t = 0; t < g.siz_icmp; t++) {  // gd_t.cu:952-969
+      xmin = xmin < x[t] ? xmin : x[t]; xmax = xmax > x[t] ? xmax : x[t];
+      ymin = ymin < y[t] ? ymin : y[t]; ymax = ymax > y[t] ? ymax : y[t];
+      zmin = zmin < z[t] ? zmin : z[t]; zmax = zmax > z[t] ? zmax : z[t];
+    }
+    const int n[3] = {g.ni, g.nj, g.nk};
+    for (int a = 0; a < 3; a++) {  // gd_t.cu:1034-1083
+      const int avg = n[a] / 4, left = n[a] % 4;
+      for (int t = 0; t < 4; t++) {
+        ts[a][t] = t == 0 ? NG : te[a][t - 1] + 1;
+        te[a][t] = ts[a][t] + avg - 1;
+        if (t < left) te[a][t] += 1;
+      }
+    }
+    for (int jt = 0; jt < 4; jt++)  // tiles of the top k-tile (the only ones depth_to_axis reads)
+      for (int it = 0; it < 4; it++) {
+        float a0 = 1.0e26f, a1 = -1.0e26f, b0 = 1.0e26f, b1 = -1.0e26f;
+        for (int k = ts[2][3]; k <= te[2][3]; k++)
+          for (int j = ts[1][jt]; j <= te[1][jt]; j++)
+            for (int i = ts[0][it]; i <= te[0][it]; i++) {
+              float c0, c1, d0, d1;
+              cell_xy(i, j, k, c0, c1, d0, d1);
+              a0 = a0 < c0 ? a0 : c0; a1 = a1 > c1 ? a1 : c1;
+              b0 = b0 < d0 ? b0 : d0; b1 = b1 > d1 ? b1 : d1;
+            }
+        tx0[jt][it] = a0; tx1[jt][it] = a1; ty0[jt][it] = b0; ty1[jt][it] = b1;
+      }
+  }
+  size_t at(int i, int j, int k) const { return i + j * g.siz_iy + k * g.siz_iz; }
+  // cell_xmin..ymax of gd_t.cu:990-1031 (8 corners)
+  void cell_xy(int i, int j, int k, float &a0, float &a1, float &b0, float &b1) const {
+    a0 = a1 = x[at(i, j, k)];
+    b0 = b1 = y[at(i, j, k)];
+    for (int n3 = 0; n3 < 2; n3++)
+      for (int n2 = 0; n2 < 2; n2++)
+        for (int n1 = 0; n1 < 2; n1++) {
+          size_t q = at(i + n1, j + n2, k + n3);
+          a0 = a0 < x[q] ? a0 : x[q]; a1 = a1 > x[q] ? a1 : x[q];
+          b0 = b0 < y[q] ? b0 : y[q]; b1 = b1 > y[q] ? b1 : y[q];
+        }
+  }
+  // fdlib_math_isPoint2InQuad
+  static bool in_quad(float px, float py, const float *vx0, const float *vy0) {
+    float vx[4] = {vx0[0], vx0[1], vx0[3], vx0[2]}, vy[4] = {vy0[0], vy0[1], vy0[3], vy0[2]};
+    for (int i = 0; i < 4; i++) {
+      float ex = i == 3 ? (vx[0] - vx[3]) : (vx[i + 1] - vx[i]);
+      float ey = i == 3 ? (vy[0] - vy[3]) : (vy[i + 1] - vy[i]);
+      float qx = px - vx[i], qy = py - vy[i];
+      float sg = ex * qy - ey * qx;
+      sg /= std::sqrt(ex * ex + ey * ey);
+      if (sg < -1e-6) return false;
+    }
+    return true;
+  }
+  // fdlib_math_rdinterp_2d for 4 points
+  static float rdinterp(float xx, float yy, const float *px, const float *py, const float *pv) {
+    float w[4] = {0, 0, 0, 0}, tot = 0.0f;
+    int atp = -1;
+    for (int i = 0; i < 4; i++) {
+      float dist = std::sqrt((xx - px[i]) * (xx - px[i]) + (yy - py[i]) * (yy - py[i]));
+      if (dist < 1e-9) atp = i;
+      else { w[i] = 1.0 / dist; tot += w[i]; }
+    }
+    if (atp > 0) { tot = 1.0; for (int i = 0; i < 4; i++) w[i] = 0.0; w[atp] = 1.0; }
+    float v = 0.0;
+    for (int i = 0; i < 4; i++) { w[i] *= 1.0 / tot; v += w[i] * pv[i]; }
+    return v;
+  }
+  // gd_curv_depth_to_axis
+  void depth_to_axis(float sx, float sy, float *sz) const {
+    if (sx < xmin || sx > xmax || sy < ymin || sy > ymax) return;
+    for (int jt = 0; jt < 4; jt++)
+      for (int it = 0; it < 4; it++) {
+        if (sx < tx0[jt][it] || sx > tx1[jt][it] || sy < ty0[jt][it] || sy > ty1[jt][it]) continue;
+        int k = te[2][3];
+        for (int j = ts[1][jt]; j <= te[1][jt]; j++)
+          for (int i = ts[0][it]; i <= te[0][it]; i++) {
+            float c0, c1, d0, d1;
+            cell_xy(i, j, k, c0, c1, d0, d1);
+            if (sx < c0 || sx > c1 || sy < d0 || sy > d1) continue;
+            float px[4], py[4], pz[4];
+            for (int n2 = 0; n2 < 2; n2++)
+              for (int n1 = 0; n1 < 2; n1++) {
+                size_t q = at(i + n1, j + n2, k);
+                px[n1 + n2 * 2] = x[q]; py[n1 + n2 * 2] = y[q]; pz[n1 + n2 * 2] = z[q];
+              }
+            if (in_quad(sx, sy, px, py)) {
+              float ztopo = rdinterp(sx, sy, px, py, pz);
+              *sz = ztopo - (*sz);
+              return;
+            }
+          }
+      }
+  }
+  static float dot(const float *a, const float *b) {
+    float r = 0.0;
+    for (int i = 0; i < 3; i++) r += a[i] * b[i];
+    return r;
+  }
+  // isPointInHexahedron_c + point2face + face_normal
+  static bool in_hexa(float px, float py, float pz, const float *vx, const float *vy, const float *vz) {
+    float pt[3] = {px, py, pz};
+    const int fc[6][3] = {{0, 4, 6}, {7, 5, 1}, {5, 4, 0}, {2, 6, 7}, {4, 5, 7}, {3, 1, 0}};
+    for (int f = 0; f < 6; f++) {
+      float h[3][3];
+      for (int c = 0; c < 3; c++) { h[c][0] = vx[fc[f][c]]; h[c][1] = vy[fc[f][c]]; h[c][2] = vz[fc[f][c]]; }
+      float p2f[3], A[3], B[3], nrm[3], un[3];
+      for (int i = 0; i < 3; i++) p2f[i] = h[0][i] - pt[i];
+      for (int i = 0; i < 3; i++) { A[i] = h[1][i] - h[0][i]; B[i] = h[2][i] - h[0][i]; }
+      nrm[0] = A[1] * B[2] - A[2] * B[1];
+      nrm[1] = A[2] * B[0] - A[0] * B[2];
+      nrm[2] = A[0] * B[1] - A[1] * B[0];
+      float len = std::sqrt(dot(nrm, nrm));
+      for (int i = 0; i < 3; i++) un[i] = nrm[i] / len;
+      float sg = dot(p2f, un);
+      float lp = std::sqrt(dot(p2f, p2f));
+      sg /= lp;
+      if (sg < 0.0) return false;
+    }
+    return true;
+  }
+  // gd_curv_coord_to_local_indx + gd_curv_coord2index_sample; returns false when not here
+  bool locate(float sx, float sy, float sz, int gidx[3], float inc[3]) const {
+    gidx[0] = gidx[1] = gidx[2] = -1000;
+    inc[0] = inc[1] = inc[2] = 0.0f;
+    if (sx < xmin || sx > xmax || sy < ymin || sy > ymax || sz < zmin || sz > zmax) return false;
+    float md = std::sqrt((sx - x[0]) * (sx - x[0]) + (sy - y[0]) * (sy - y[0]) + (sz - z[0]) * (sz - z[0]));
+    int mi = 0, mj = 0, mk = 0;
+    for (int k = 0; k < g.nz; k++)
+      for (int j = 0; j < g.ny; j++)
+        for (int i = 0; i < g.nx; i++) {
+          size_t q = at(i, j, k);
+          float dd = std::sqrt((sx - x[q]) * (sx - x[q]) + (sy - y[q]) * (sy - y[q]) + (sz - z[q]) * (sz - z[q]));
+          if (md > dd) { md = dd; mi = i; mj = j; mk = k; }
+        }
+    if (mi < g.ni1 || mi > g.ni2 || mj < g.nj1 || mj > g.nj2 || mk < g.nk1 || mk > g.nk2) return false;
+    gidx[0] = mi - NG; gidx[1] = mj - NG; gidx[2] = mk - NG;
+    for (int kk = 0; kk < 2; kk++)
+      for (int jj = 0; jj < 2; jj++)
+        for (int ii = 0; ii < 2; ii++) {
+          int ci = mi - 1 + ii, cj = mj - 1 + jj, ck = mk - 1 + kk;
+          float vx[8], vy[8], vz[8];
+          for (int n3 = 0; n3 < 2; n3++)
+            for (int n2 = 0; n2 < 2; n2++)
+              for (int n1 = 0; n1 < 2; n1++) {
+                size_t q = at(ci + n1, cj + n2, ck + n3);
+                int c = n1 + n2 * 2 + n3 * 4;
+                vx[c] = x[q]; vy[c] = y[q]; vz[c] = z[q];
+              }
+          if (!in_hexa(sx, sy, sz, vx, vy, vz)) continue;
+          const int ns = 100;
+          float m2 = std::sqrt((sx - vx[0]) * (sx - vx[0]) + (sy - vy[0]) * (sy - vy[0]) + (sz - vz[0]) * (sz - vz[0]));
+          int b1 = 0, b2 = 0, b3 = 0;
+          for (int n3 = 0; n3 < ns + 1; n3++) {
+            float Lz[2]; Lz[1] = (float)n3 / (float)ns; Lz[0] = 1.0 - Lz[1];
+            for (int n2 = 0; n2 < ns + 1; n2++) {
+              float Ly[2]; Ly[1] = (float)n2 / (float)ns; Ly[0] = 1.0 - Ly[1];
+              for (int n1 = 0; n1 < ns + 1; n1++) {
+                float Lx[2]; Lx[1] = (float)n1 / (float)ns; Lx[0] = 1.0 - Lx[1];
+                float xp = 0, yp = 0, zp = 0;
+                for (int k2 = 0; k2 < 2; k2++)
+                  for (int j2 = 0; j2 < 2; j2++)
+                    for (int i2 = 0; i2 < 2; i2++) {
+                      int c = i2 + j2 * 2 + k2 * 4;
+                      xp += Lx[i2] * Ly[j2] * Lz[k2] * vx[c];
+                      yp += Lx[i2] * Ly[j2] * Lz[k2] * vy[c];
+                      zp += Lx[i2] * Ly[j2] * Lz[k2] * vz[c];
+                    }
+                float dd = std::sqrt((sx - xp) * (sx - xp) + (sy - yp) * (sy - yp) + (sz - zp) * (sz - zp));
+                if (m2 > dd) { m2 = dd; b1 = n1; b2 = n2; b3 = n3; }
+              }
+            }
+          }
+          float si = (float)ci + (float)b1 / (float)ns, sj = (float)cj + (float)b2 / (float)ns,
+                sk = (float)ck + (float)b3 / (float)ns;
+          inc[0] = si - mi; inc[1] = sj - mj; inc[2] = sk - mk;
+          return true;
+        }
+    return true;  // in no surrounding cell: zero shift (gd_t.cu:1378-1386)
+  }
+};
+
 // ---------------------------------------------------------------------------------------
 template <typename T>
 struct Oracle {
@@ -605,20 +801,33 @@ struct Oracle {
     const cgfd_source_desc &s = d->src;
     nsrc = 0;
     if (s.num <= 0) return;
-    if (s.loc_coord_type != 0) throw std::runtime_error("source location by coordinate not supported");
+
     const int half = 3;  // fd->fdx_max_half_len
     const int len_ext = 2 * half + 1;
     max_ext = len_ext * len_ext * len_ext;
     std::vector<int> idx(3 * s.num), inthread(s.num, 0), outside(s.num, 0);
     std::vector<float> inc(3 * s.num);
     int gnk2 = g.nk - 1;
+    std::unique_ptr<Locator> lc;
+    if (s.loc_coord_type == 1) {
+      if (!d->coord) throw std::runtime_error("coord is required to locate sources");
+      lc.reset(new Locator(g, d->coord));
+    }
     for (int is = 0; is < s.num; is++) {
       float c[3] = {s.loc[3 * is], s.loc[3 * is + 1], s.loc[3 * is + 2]};
-      if (s.loc_3dim == 1) c[2] = gnk2 - c[2];
-      for (int a = 0; a < 3; a++) {
-        int gi = (int)(c[a] + 0.5);
-        inc[3 * is + a] = c[a] - gi;
-        idx[3 * is + a] = gi;
+      if (s.loc_coord_type == 1) {  // src_t.cu:341-398
+        if (s.loc_3dim == 1) lc->depth_to_axis(c[0], c[1], &c[2]);
+        int gi[3];
+        float fi[3];
+        lc->locate(c[0], c[1], c[2], gi, fi);
+        for (int a = 0; a < 3; a++) { idx[3 * is + a] = gi[a]; inc[3 * is + a] = fi[a]; }
+      } else {
+        if (s.loc_3dim == 1) c[2] = gnk2 - c[2];
+        for (int a = 0; a < 3; a++) {
+          int gi = (int)(c[a] + 0.5);
+          inc[3 * is + a] = c[a] - gi;
+          idx[3 * is + a] = gi;
+        }
       }
       // src_t.cu:296-307: an index outside the grid is replaced by -1000, which later
       // leaves the source without any smoothing point inside the grid.
@@ -736,16 +945,34 @@ struct Oracle {
     const cgfd_station_desc &s = d->sta;
     recv.clear();
     int gnk2 = g.nk - 1;
+    std::unique_ptr<Locator> lc;
     for (int ir = 0; ir < s.num; ir++) {
-      if (s.flag_coord[ir] != 0) throw std::runtime_error("station location by coordinate not supported");
-      float c[3] = {s.loc[3 * ir] - 1, s.loc[3 * ir + 1] - 1, s.loc[3 * ir + 2]};
-      if (s.flag_depth[ir] == 1) c[2] = gnk2 - c[2];
-      else c[2] -= 1;
-      int ix = (int)c[0], iy = (int)c[1], iz = (int)c[2];
-      float dx = c[0] - ix, dy = c[1] - iy, dz = c[2] - iz;
-      if (ix < 0 || ix > g.ni) ix = -1000;
-      if (iy < 0 || iy > g.nj) iy = -1000;
-      if (iz < 0 || iz > g.nk) iz = -1000;
+      int ix, iy, iz;
+      float dx, dy, dz;
+      if (s.flag_coord[ir] == 1) {  // io_funcs.cu:95-169
+        if (!lc) {
+          if (!d->coord) throw std::runtime_error("coord is required to locate stations");
+          lc.reset(new Locator(g, d->coord));
+        }
+        float c[3] = {s.loc[3 * ir], s.loc[3 * ir + 1], s.loc[3 * ir + 2]};
+        if (s.flag_depth[ir] == 1) lc->depth_to_axis(c[0], c[1], &c[2]);
+        int gi[3];
+        float fi[3];
+        lc->locate(c[0], c[1], c[2], gi, fi);
+        for (int a = 0; a < 3; a++)
+          if (fi[a] < 0.0) { fi[a] = 1.0 + fi[a]; gi[a] -= 1; }
+        ix = gi[0]; iy = gi[1]; iz = gi[2];
+        dx = fi[0]; dy = fi[1]; dz = fi[2];
+      } else {
+        float c[3] = {s.loc[3 * ir] - 1, s.loc[3 * ir + 1] - 1, s.loc[3 * ir + 2]};
+        if (s.flag_depth[ir] == 1) c[2] = gnk2 - c[2];
+        else c[2] -= 1;
+        ix = (int)c[0]; iy = (int)c[1]; iz = (int)c[2];
+        dx = c[0] - ix; dy = c[1] - iy; dz = c[2] - iz;
+        if (ix < 0 || ix > g.ni) ix = -1000;
+        if (iy < 0 || iy > g.nj) iy = -1000;
+        if (iz < 0 || iz > g.nk) iz = -1000;
+      }
       if (!(ix >= 0 && ix <= g.ni - 1 && iy >= 0 && iy <= g.nj - 1 && iz >= 0 && iz <= g.nk - 1)) continue;
       int il = ix + NG, jl = iy + NG, kl = iz + NG;
       Recv r;
@@ -1232,6 +1459,22 @@ int orc_get_seismograms(void *p, float *out) {
   const std::vector<float> &s = h->d ? h->d->seismo : h->f->seismo;
   memcpy(out, s.data(), s.size() * sizeof(float));
   return 0;
+}
+
+// Location of n points by physical coordinates (depth_flag: z is a depth below the surface):
+// global physical index (-1000 outside) and shift, as src_t.cu:341-398 uses them.
+int orc_locate_points(int ni, int nj, int nk, const float *coord, int n, const float *xyz, const int *depth_flag,
+                      int *idx, float *inc) {
+  return guarded([&] {
+    Grid g;
+    g.set(ni, nj, nk);
+    Locator lc(g, coord);
+    for (int q = 0; q < n; q++) {
+      float c[3] = {xyz[3 * q], xyz[3 * q + 1], xyz[3 * q + 2]};
+      if (depth_flag && depth_flag[q]) lc.depth_to_axis(c[0], c[1], &c[2]);
+      lc.locate(c[0], c[1], c[2], idx + 3 * q, inc + 3 * q);
+    }
+  });
 }
 
 // [15][ny][nx] peak ground motion (zeros before the first step or without a free surface)

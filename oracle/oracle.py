@@ -36,6 +36,7 @@ def lib():
             ("orc_get_seismograms", C.c_int, [P, P]),
             ("orc_get_wavefield", C.c_int, [P, P]),
             ("orc_get_peak_motion", C.c_int, [P, P]),
+            ("orc_locate_points", C.c_int, [C.c_int, C.c_int, C.c_int, P, C.c_int, P, P, P, P]),
             ("orc_set_wavefield", C.c_int, [P, P]),
             ("orc_pml_coefs", C.c_int, [P, C.c_int, C.c_int, P, P, P]),
             ("orc_free_mats", C.c_int, [P, P, P]),
@@ -58,6 +59,22 @@ def metric_fp32(coord):
     c = np.ascontiguousarray(coord, np.float32)
     lib().orc_metric_calc(nx - 6, ny - 6, nz - 6, c.ctypes.data, out.ctypes.data)
     return out
+
+
+def locate_points(coord, xyz, depth_flag=None):
+    """(idx [n,3] global physical index or -1000, inc [n,3] shift) of points given by physical
+    coordinates, located like the reference (nearest point, cell test, 101^3 sampling)."""
+    _, nz, ny, nx = coord.shape
+    c = np.ascontiguousarray(coord, np.float32)
+    q = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+    n = q.shape[0]
+    flags = np.ascontiguousarray(depth_flag if depth_flag is not None else np.zeros(n), np.int32)
+    idx = np.zeros((n, 3), np.int32)
+    inc = np.zeros((n, 3), np.float32)
+    if lib().orc_locate_points(nx - 6, ny - 6, nz - 6, c.ctypes.data, n, q.ctypes.data, flags.ctypes.data,
+                               idx.ctypes.data, inc.ctypes.data) != 0:
+        raise RuntimeError("oracle: " + lib().orc_error().decode())
+    return idx, inc
 
 
 def fill_ghosts(coord):

@@ -100,9 +100,9 @@ def test_invalid_descriptions_are_rejected():
     rc, msg = _create(d)
     assert rc == -1
     d = p.desc()
-    d.src.loc_coord_type = 1
+    d.src.loc_coord_type = 2
     rc, msg = _create(d)
-    assert rc == -5 and "coordinates" in msg
+    assert rc == -1 and "loc_coord_type" in msg
     d = p.desc()
     d.pml[2][1].enable = 1
     d.pml[2][1].num_layers = 3

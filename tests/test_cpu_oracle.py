@@ -128,3 +128,31 @@ def test_flat_free_surface_matrix_kat():
     # rows: dzVx, dzVy, dzVz; columns: dxVx, dxVy, dxVz (metric ratios are 1 on a cube grid)
     assert np.allclose(A, [[0, 0, -1], [0, 0, 0], [-r, 0, 0]], atol=1e-6)
     assert np.allclose(Bm, [[0, 0, 0], [0, 0, -1], [0, -r, 0]], atol=1e-6)
+
+
+def test_coordinate_location_recovers_cell_positions():
+    """The oracle's restatement of the reference's location (nearest point, containing cell,
+    101^3 sampling) returns the index + shift of points built by trilinear interpolation,
+    to the sampling step 0.01; a depth of 0 lands on the free surface."""
+    from oracle.oracle import locate_points
+    p = small_problem("iso", nsteps=4)
+    c = p.coord
+
+    def tri(i0, j0, k0, f):
+        out = np.zeros(3)
+        for kk in (0, 1):
+            for jj in (0, 1):
+                for ii in (0, 1):
+                    w = (f[0] if ii else 1 - f[0]) * (f[1] if jj else 1 - f[1]) * (f[2] if kk else 1 - f[2])
+                    out += w * c[:, k0 + 3 + kk, j0 + 3 + jj, i0 + 3 + ii]
+        return out
+    cases = [((10, 12, 8), (0.37, 0.61, 0.25)), ((20, 5, 15), (0.9, 0.1, 0.5)), ((3, 30, 2), (0.5, 0.5, 0.5))]
+    pts = np.array([tri(*a, f) for a, f in cases], np.float32)
+    idx, inc = locate_points(c, pts)
+    for (a, f), ix, fr in zip(cases, idx, inc):
+        assert np.allclose(ix + fr, np.array(a) + np.array(f), atol=0.0101)
+    top = c[:, p.nk + 2, 9 + 3, 7 + 3]
+    idx, inc = locate_points(c, np.array([[top[0], top[1], 0.0]], np.float32), [1])
+    assert tuple(idx[0]) == (7, 9, p.nk - 1) and np.allclose(inc[0], 0.0, atol=0.0101)
+    out, _ = locate_points(c, np.array([[1e9, 0.0, 0.0]], np.float32))
+    assert (out == -1000).all()
