@@ -82,8 +82,9 @@ typedef struct cgfd_pml_face {
 } cgfd_pml_face;
 
 /*
- * Sources, as read from a .src file (src_t.cu:143-790, src_read_locate_file).
- * Only grid-index locations (loc_coord_type 0) are accepted.
+ * Sources, as read from a .src file (src_t.cu:143-790, src_read_locate_file), located by grid
+ * index (loc_coord_type 0) or by physical coordinates (1; gd_curv_coord_to_glob_indx_gpu and
+ * gd_curv_depth_to_axis, gd_t.cu:1189-1500; desc->coord required).
  */
 typedef struct cgfd_source_desc {
   int   num;              /* in_num_source                                                 */
@@ -93,9 +94,10 @@ typedef struct cgfd_source_desc {
   int   stf_nt;           /* stf_given 1: number of samples                                */
   int   cmp_type;         /* 1 force, 2 moment, 3 force+moment (quirk kept: 3 = force only) */
   int   mechanism_type;   /* 0 moment tensor, 1 strike/dip/rake + mu,D,A                   */
-  int   loc_coord_type;   /* 0 grid index (required)                                       */
-  int   loc_3dim;         /* 0: z is a grid index, 1: z counts down from the free surface  */
-  const float *loc;       /* [num][3] x,y,z (0-based index)                                */
+  int   loc_coord_type;   /* 0 grid index, 1 physical coordinates                          */
+  int   loc_3dim;         /* 0: z is a grid index / coordinate, 1: z is the depth below the
+                             free surface (index count or length)                           */
+  const float *loc;       /* [num][3] x,y,z (0-based index, or coordinates)                */
   const float *t_start;   /* [num] wavelet_tstart                                          */
   const int   *wavelet;   /* [num] CGFD_WAVELET_* (stf_given 0)                             */
   const float *wavelet_coefs; /* [num][10]                                                 */
@@ -106,9 +108,9 @@ typedef struct cgfd_source_desc {
 /* Stations, as read from a station list (io_funcs.cu:24-299, io_recv_read_locate). */
 typedef struct cgfd_station_desc {
   int          num;
-  const int   *flag_coord; /* [num] 0: grid index (required)                               */
-  const int   *flag_depth; /* [num] 1: z counts down from the free surface                 */
-  const float *loc;        /* [num][3] x,y 1-based index, z per flag_depth                 */
+  const int   *flag_coord; /* [num] 0: grid index, 1: physical coordinates                 */
+  const int   *flag_depth; /* [num] 1: z is the depth below the free surface               */
+  const float *loc;        /* [num][3] x,y 1-based index (or coordinates), z per flags      */
 } cgfd_station_desc;
 
 /*
