@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--zchunk", type=int, default=0)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched / mixed-precision section")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
     return ap.parse_args()
 
 
@@ -233,6 +234,48 @@ def batched_mixed(local, steps=16):
     return out
 
 
+def serving_bench(local, nreq=24, mean_gap_s=0.02, seed=11):
+    """The serving loop under Poisson arrivals: nreq forward simulations on 4 models (iso /
+    VTI / aniso, 96x96x64 ... 160x160x96, CFS-PML 10, free surface, 300 steps each), 1-4
+    random double-couple sources per request, 16 surface stations; same-model requests batch.
+    Reports p50 / p99 latency (submit -> seismograms ready) and throughput."""
+    import dataclasses
+    from cgfd_b200 import synth, Server, Problem
+    rng = np.random.default_rng(seed)
+    shapes = [("iso", (96, 96, 64)), ("iso", (160, 160, 96)), ("vti", (128, 128, 64)), ("aniso", (96, 80, 64))]
+    weights = np.array([0.25, 0.25, 0.3, 0.2])
+    models = []
+    for n, (med, (ni, nj, nk)) in enumerate(shapes):
+        m = synth.make_problem(ni, nj, nk, 100.0, 299, dt=None, medium=med, npml=10, nsrc=0, sta_grid=(4, 4),
+                               fc=2.0, seed=100 + n)
+        m.device = local
+        models.append(m)
+    reqs = []
+    for r in range(nreq):
+        m = models[int(rng.choice(len(models), p=weights))]
+        src = synth.dc_sources(m.coord, m.ni, m.nj, int(rng.integers(1, 5)), rng, depth_range=(1500.0, 3000.0),
+                               fc_range=(1.5, 2.5), stf_length=m.nt_total * m.dt)
+        reqs.append(dataclasses.replace(m, src=src))
+    gaps = rng.exponential(mean_gap_s, nreq)
+    work = sum(q.ni * q.nj * q.nk * 4.0 * q.nt_total for q in reqs)
+    with Server(device=local, max_active=4, max_batch=4, steps_per_slice=50) as srv:
+        t0 = time.perf_counter()
+        ids = []
+        for q, g in zip(reqs, gaps):
+            time.sleep(float(g))
+            ids.append(srv.submit(q))
+        for i in ids:
+            if srv.wait(i, timeout=600) is None:
+                raise RuntimeError("serving request timed out")
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+    return {"requests": nreq, "models": [f"{m}:{a}x{b}x{c}" for m, (a, b, c) in shapes], "steps": 300,
+            "arrivals": f"Poisson, mean gap {mean_gap_s * 1e3:.0f} ms", "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "mean_ms": st["mean_ms"], "completed": st["completed"], "failed": st["failed"], "batches": st["batches"],
+            "cell_stages_per_s": st["cell_stages_per_s"], "source_steps_per_s": st["source_steps_per_s"],
+            "wall_s": wall, "offered_gcell_stages": work / 1e9, "hbm_peak_gb": st["hbm_peak"] / 1e9}
+
+
 def cpu_baseline(args, threads):
     """The oracle (FP32 CPU restatement, OpenMP on all host cores) on a sample of the workload."""
     from oracle.oracle import Oracle
@@ -402,6 +445,13 @@ def main():
         except Exception as ex:  # report, do not fail the headline measurement
             batched = {"error": str(ex)}
 
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        try:
+            serving = serving_bench(local)
+        except Exception as ex:  # report, do not fail the headline measurement
+            serving = {"error": str(ex)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = len(os.sched_getaffinity(0))
@@ -419,7 +469,7 @@ def main():
                           "dt": p.dt, "precision": "fp32", "parallelism": f"replicas x{world}",
                           "l2": "inputs larger than L2 (wavefield 4x9x58M floats)"},
                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": tim["launches"],
-               "clocks": clocks, "batched_mixed": batched}
+               "clocks": clocks, "batched_mixed": batched, "serving": serving}
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()

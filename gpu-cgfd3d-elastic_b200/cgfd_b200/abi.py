@@ -263,6 +263,7 @@ def lib():
         "cgfd_set_graph_mode": (C.c_int, [P, C.c_int]),
         "cgfd_set_zchunk": (C.c_int, [P, C.c_int]),
         "cgfd_get_zchunk": (C.c_int, [P]),
+        "cgfd_autotune": (C.c_int, [P, C.c_int, C.POINTER(C.c_int)]),
         "cgfd_set_timing": (C.c_int, [P, C.c_int]),
         "cgfd_set_bulk_variant": (C.c_int, [P, C.c_int]),
         "cgfd_get_timing": (C.c_int, [P, P, P, P, C.c_int]),
@@ -346,6 +347,12 @@ class Simulation:
 
     def synchronize(self):
         check(lib().cgfd_synchronize(self.h))
+
+    def autotune(self, steps=4):
+        """cgfd_autotune: fastest z-chunk length of this problem (state reset to step 0)."""
+        c = C.c_int()
+        check(lib().cgfd_autotune(self.h, int(steps), C.byref(c)))
+        return c.value
 
     def check_wait_bound(self):
         """cgfd_check_wait_bound: (status, message) of one device pipeline wait that nothing

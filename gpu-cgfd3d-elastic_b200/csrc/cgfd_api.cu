@@ -806,6 +806,27 @@ void make_tiles(cgfd_problem *p) {
   p->tiles.npml = (int)pm.size();
 }
 
+// Back to the state right after cgfd_problem_create: zero wavefield levels, PML auxiliaries,
+// seismograms, peak motion, scale collectors, error word; step 0.
+void reset_state(cgfd_problem *p) {
+  const size_t lev_bytes[4] = {4, 4, p->wave16 ? 2u : 4u, p->wave16 ? 2u : 4u};
+  for (int l = 0; l < 4; l++) CK(cudaMemsetAsync(p->wbuf[l], 0, lev_bytes[l] * 9 * p->sf * p->nshot, p->stream));
+  for (auto &f : p->faces) CK(cudaMemsetAsync(f.aux, 0, sizeof(float) * 3 * 9 * f.n * p->nshot, p->stream));
+  if (p->rec.n > 0)
+    CK(cudaMemsetAsync(p->d_seis, 0, sizeof(float) * p->rec.n * 9 * p->nt_total * p->nshot, p->stream));
+  if (p->d_pg) {
+    const size_t nij = (size_t)p->ni * p->nj * p->nshot;
+    CK(cudaMemsetAsync(p->d_pg, 0, sizeof(float) * 15 * nij, p->stream));
+    CK(cudaMemsetAsync(p->d_dis, 0, sizeof(float) * 3 * nij, p->stream));
+  }
+  if (p->d_amax) CK(cudaMemsetAsync(p->d_amax, 0, sizeof(unsigned int) * 2 * p->nshot, p->stream));
+  p->it = 0;
+  CK(cudaMemsetAsync(p->d_it, 0, sizeof(int), p->stream));
+  CK(cudaMemsetAsync(p->d_flag, 0, sizeof(int), p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  p->collect_timing();
+}
+
 // FP16 stage levels: recompute max |w_pre| after the host replaced or re-labelled levels.
 void refresh_wave_max(cgfd_problem *p) {
   if (!p->wave16) return;
@@ -1149,6 +1170,50 @@ int cgfd_set_zchunk(cgfd_problem *p, int nzc) {
 }
 
 int cgfd_get_zchunk(const cgfd_problem *p) { return p ? p->nzc : -1; }
+
+int cgfd_autotune(cgfd_problem *p, int steps, int *chosen) {
+  if (!p || steps < 1) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
+  if (p->it != 0) { set_err("autotuning runs on a problem that has not stepped yet (step 0)"); return CGFD_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(p->device));
+    const int nbulk = p->free_top ? p->nk - cgfd::NSURF : p->nk;
+    std::vector<int> cand;
+    for (int c : {8, 12, 16, 24, 32, 48, 64, 96, nbulk})
+      if (c >= 1 && c <= nbulk && std::find(cand.begin(), cand.end(), c) == cand.end()) cand.push_back(c);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    int best = p->nzc;
+    float best_ms = 1e30f;
+    const bool timing = p->timing;
+    p->timing = false;
+    for (int c : cand) {
+      CK(cudaStreamSynchronize(p->stream));
+      p->nzc = c;
+      make_tiles(p);
+      for (int s = 0; s < 8; s++)
+        if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }
+      p->run_steps(8);  // captures the 8 step graphs of this tiling
+      CK(cudaEventRecord(e0, p->stream));
+      p->run_steps(steps);
+      CK(cudaEventRecord(e1, p->stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best_ms) { best_ms = ms; best = c; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    p->timing = timing;
+    CK(cudaStreamSynchronize(p->stream));
+    p->nzc = best;
+    make_tiles(p);
+    for (int s = 0; s < 8; s++)
+      if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }
+    reset_state(p);
+    if (chosen) *chosen = best;
+  });
+}
 
 /* Bulk kernel variant: 1 = TMA-pipelined (default), 0 = direct loads. */
 int cgfd_set_bulk_variant(cgfd_problem *p, int tma) {

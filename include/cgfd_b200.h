@@ -284,6 +284,16 @@ int cgfd_set_graph_mode(cgfd_problem *p, int on);
 int cgfd_set_zchunk(cgfd_problem *p, int nzc);
 int cgfd_get_zchunk(const cgfd_problem *p);
 
+/*
+ * Autotuner of the bulk kernel's z-chunk length (planes per thread block column; the tile
+ * shape's free parameter): times `steps` graph-replayed time steps for each candidate
+ * (8, 12, 16, 24, 32, 48, 64, 96 and all bulk planes) on this problem, keeps the fastest
+ * (*chosen) and returns the problem to its freshly created state (zero wavefield, step 0).
+ * Only on a problem that has not stepped yet. Results do not depend on the chunk length.
+ * No counterpart in the reference.
+ */
+int cgfd_autotune(cgfd_problem *p, int steps, int *chosen);
+
 /* Bulk stage kernel variant: 1 = TMA-pipelined (default), 0 = direct global loads. */
 int cgfd_set_bulk_variant(cgfd_problem *p, int tma);
 

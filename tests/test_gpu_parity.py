@@ -129,3 +129,20 @@ def test_peak_motion_needs_free_surface():
     with pytest.raises(CgfdError) as e:
         sim.peak_motion()
     assert e.value.code == -5
+
+
+def test_autotune_picks_a_chunk_and_resets_state():
+    """cgfd_autotune times the z-chunk candidates on the problem itself, keeps the fastest and
+    returns the problem to step 0 with a zero wavefield: the following run equals a run of a
+    fresh problem bitwise (results do not depend on the chunk length)."""
+    p = small_problem("iso", nsteps=30)
+    a = Simulation(p)
+    c = a.autotune(2)
+    assert c in (8, 12, 16, 24, 32, 48, 64, 96, p.nk - 4) and a.zchunk == c and a.step == 0
+    a.run()
+    b = Simulation(p)
+    b.run()
+    assert np.array_equal(a.seismograms(), b.seismograms())
+    assert np.array_equal(a.wavefield(), b.wavefield())
+    with pytest.raises(Exception):
+        a.autotune(2)  # only before the first step
