@@ -261,6 +261,7 @@ struct cgfd_problem {
       n += timed(7, [&] { return cgfd::launch_wave_scale(d_amax, d_srcb, d_it, nt_total, nshot, d_wsc, st); });
     for (int s = 0; s < 4; s++) {
       cgfd::StageP p = stage_params(step, s);
+      bool surface_done = false;
       if (use_tma) {
         cgfd::TmaP tm;
         const int pre = step & 1, end = (step + 1) & 1;
@@ -269,13 +270,18 @@ struct cgfd_problem {
         tm.pre = map_ctr[pre];
         tm.end = map_ctr[end];
         tm.coef = map_coef;
+        const bool fork = tiles.npml > 0 && tiles.ninterior > 0;
+        // Outside per-kernel timing, the surface slab (latency-bound, top planes only) runs on
+        // the side stream behind the PML tiles, beside the interior tiles: it writes only the
+        // top planes of the stage outputs, which no bulk tile reads or writes in this stage.
+        surface_done = fork && !timing;
         n += timed(s, [&] {
-          const bool fork = tiles.npml > 0 && tiles.ninterior > 0;
           if (fork) {
             CK(cudaEventRecord(ev_fork, st));
             CK(cudaStreamWaitEvent(side, ev_fork, 0));
           }
-          const int k = cgfd::launch_stage_bulk_tma(med, coef_type, wave16, p, tm, tiles, st, fork ? side : st);
+          int k = cgfd::launch_stage_bulk_tma(med, coef_type, wave16, p, tm, tiles, st, fork ? side : st);
+          if (surface_done) k += cgfd::launch_stage_surface(med, coef_type, wave16, p, side);
           if (fork) {
             CK(cudaEventRecord(ev_join, side));
             CK(cudaStreamWaitEvent(st, ev_join, 0));
@@ -285,7 +291,7 @@ struct cgfd_problem {
       } else {
         n += timed(s, [&] { return cgfd::launch_stage_bulk(med, p, nzc, st); });
       }
-      n += timed(4, [&] { return cgfd::launch_stage_surface(med, coef_type, wave16, p, st); });
+      if (!surface_done) n += timed(4, [&] { return cgfd::launch_stage_surface(med, coef_type, wave16, p, st); });
       if (src.nsrc > 0) {
         cgfd::SrcP q;
         q.nsrc = src.nsrc; q.max_ext = src.max_ext; q.max_nt = src.max_nt;
@@ -590,12 +596,12 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
     for (int l = 0; l < 4; l++) {
       if (lev_bytes[l] == 2) {  // FP16 stage level: x halo of 8 elements keeps the box 16-byte aligned
         make_map(&p->map_halo[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX + 16,
-                 ty + 6, 9, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2);
+                 ty + 4, 9, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2);
         make_map(&p->map_ctr[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX, ty, 9,
                  CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2);
         continue;
       }
-      make_map(&p->map_halo[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX + 8, ty + 6, 9);
+      make_map(&p->map_halo[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX + 8, ty + 4, 9);
       make_map(&p->map_ctr[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX, ty, 9);
     }
     if (p->coef_type == cgfd::COEF_F32)

@@ -4,13 +4,16 @@
 // planes. Thread 0 streams, two planes ahead of the computation and with mbarrier
 // completion:
 //   - the stage input of one plane with its x-y halo, all 9 fields, as ONE 4-D TMA box
-//     (40 x (TYT+6) x 1 x 9) into a 3-slot ring (plane k for the x/y operators, plane k+-1
-//     for the z look-ahead, one in flight);
+//     (40 x (TYT+4) x 1 x 9) into a 3-slot ring (plane k for the x/y operators, plane k+-1
+//     for the z look-ahead, one in flight). The one-sided y operator of the stage reads one
+//     row on one side and three on the other, so the box holds rows [-1, TYT+3) for forward
+//     and [-3, TYT+1) for backward y operators; the x halo is 16 bytes on both sides (TMA
+//     alignment);
 //   - the coefficients (metrics, 1/rho, moduli) and, when the stage needs them, w_pre and
 //     w_end of the same plane (centre boxes) into a 2-slot ring.
 // The z march runs upwards for backward z operators and downwards for forward ones, so the
-// one-sided operator always needs exactly one plane ahead; the other 3 planes of the
-// 5-point z stencil live in a per-thread register queue. No thread computes an address
+// one-sided operator always needs exactly one plane ahead; the current plane and the one
+// ahead are read from the ring, the 3 planes behind live in a per-thread register queue. No thread computes an address
 // for a stencil or coefficient load; HBM sees every value once per stage.
 #include "cgfd_dev.cuh"
 #include "cgfd_launch.h"
@@ -41,7 +44,7 @@ template <int MED, int TYT, typename TC, typename TW, int MINB = TileCfg<MED>::M
 struct BulkSmem {
   static constexpr int XO = 16 / (int)sizeof(TW);  // x halo of the box: 16 bytes, TMA-aligned
   static constexpr int WX = TX + 2 * XO;  // x box [-XO, 32+XO) around the tile
-  static constexpr int WY = TYT + 6;      // y box [-3, TYT+3)
+  static constexpr int WY = TYT + 4;      // y box [-1, TYT+3) (forward) or [-3, TYT+1) (backward)
   static constexpr int NC = MedInfo<MED>::NCOEF;
   static constexpr int CELLS = TX * TYT;
   static constexpr int WAVE_ELEMS = 9 * WY * WX;
@@ -109,7 +112,7 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
   const uint32_t wave_bytes = S::WAVE_ELEMS * sizeof(TW);
   const uint32_t cpe_bytes = S::COEF_BYTES + (need_pre && S::PT ? S::FLD_BYTES : 0) + (need_end ? S::FLD_BYTES : 0);
   // box origins in device-layout coordinates (x * element size a multiple of 16 bytes)
-  const int xw = GX + bx * TX - S::XO, yw = by * TYT;
+  const int xw = GX + bx * TX - S::XO, yw = by * TYT + 3 - LY;  // box row r = tile row r - LY
   const int xc = GX + bx * TX, yc = 3 + by * TYT;
 
   if (tid == 0) {
@@ -153,12 +156,12 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
     if (xo && yo && zo) fmask |= 1u << fi;
   }
 
-  // register queue in march order: q[f][n] = plane k + (n - 3) * SD
-  float q[9][5];
+  // register queue of the planes behind, in march order: q[f][n] = plane k + (n - 3) * SD
+  float q[9][3];
 #pragma unroll
   for (int f = 0; f < 9; f++)
 #pragma unroll
-    for (int m = 0; m < 5; m++) q[f][m] = 0.f;
+    for (int m = 0; m < 3; m++) q[f][m] = 0.f;
   if (act) {
 #pragma unroll
     for (int m = 0; m < 3; m++) {
@@ -167,10 +170,8 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
       for (int f = 0; f < 9; f++) q[f][m] = to_f(__ldg(cur + f * sf + id));
     }
   }
-  const int wc = (ty + 3) * S::WX + tx + S::XO;  // centre of this thread in a wave slot (per field)
+  const int wc = (ty + LY) * S::WX + tx + S::XO;  // centre of this thread in a wave slot (per field)
   mbar_wait(&bar[0], 0, p.err);
-#pragma unroll
-  for (int f = 0; f < 9; f++) q[f][3] = to_f(wave[f * S::WY * S::WX + wc]);
   float vmax = 0.f, smax = 0.f;  // FP16 mode, stage 3: max |w_end| of this thread
 
   const int cell = ty * TX + tx;
@@ -185,8 +186,6 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
     mbar_wait(&bar[3 + cs], (m >> 1) & 1, p.err);
     const TW *W = wave + ws * (S::WAVE_SLOT / (int)sizeof(TW));
     const TW *Wn = wave + wn * (S::WAVE_SLOT / (int)sizeof(TW));
-#pragma unroll
-    for (int f = 0; f < 9; f++) q[f][4] = to_f(Wn[f * S::WY * S::WX + wc]);
 
     if (act) {
       const CoefTile<TC, S::CELLS> Cc{reinterpret_cast<const TC *>(cpe + cs * S::CPE_SLOT) + cell, p};
@@ -205,7 +204,7 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
         float d[9];
 #pragma unroll
         for (int f = 0; f < 9; f++) {
-          const TW *r = W + f * S::WY * S::WX + (ty + 3) * S::WX + tx + S::XO - LX;
+          const TW *r = W + f * S::WY * S::WX + (ty + LY) * S::WX + tx + S::XO - LX;
           d[f] = drp5<DX>(to_f(r[0]), to_f(r[1]), to_f(r[2]), to_f(r[3]), to_f(r[4]));
           if constexpr (WP == 2) d[f] *= s_wsc[f];  // the operator is linear: scale once
         }
@@ -224,7 +223,7 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
         float d[9];
 #pragma unroll
         for (int f = 0; f < 9; f++) {
-          const TW *r = W + f * S::WY * S::WX + (ty + 3 - LY) * S::WX + tx + S::XO;
+          const TW *r = W + f * S::WY * S::WX + ty * S::WX + tx + S::XO;
           d[f] = drp5<DY>(to_f(r[0]), to_f(r[S::WX]), to_f(r[2 * S::WX]), to_f(r[3 * S::WX]), to_f(r[4 * S::WX]));
           if constexpr (WP == 2) d[f] *= s_wsc[f];
         }
@@ -238,13 +237,13 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
             }
         }
       }
-      // z (queue in march order; the operator takes increasing k)
+      // z (queue, this plane and the one ahead in march order; the operator takes increasing k)
       {
         float d[9];
 #pragma unroll
         for (int f = 0; f < 9; f++) {
-          d[f] = SD > 0 ? drp5<DZ>(q[f][0], q[f][1], q[f][2], q[f][3], q[f][4])
-                        : drp5<DZ>(q[f][4], q[f][3], q[f][2], q[f][1], q[f][0]);
+          const float c0 = to_f(W[f * S::WY * S::WX + wc]), c1 = to_f(Wn[f * S::WY * S::WX + wc]);
+          d[f] = SD > 0 ? drp5<DZ>(q[f][0], q[f][1], q[f][2], c0, c1) : drp5<DZ>(c1, c0, q[f][2], q[f][1], q[f][0]);
           if constexpr (WP == 2) d[f] *= s_wsc[f];
         }
         acc.add_axis(mt[2], d, d + 3);
@@ -273,9 +272,10 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
       if (stage == 0) {
 #pragma unroll
         for (int f = 0; f < 9; f++) {
-          const float t = q[f][3] + ca * h[f];
+          const float c0 = to_f(W[f * S::WY * S::WX + wc]);  // stage input = w_pre at stage 0
+          const float t = c0 + ca * h[f];
           tmp_out[f * sf + id] = from_f<TT>(WP != 0 ? t * s_wsc[9 + f] : t);
-          endw[f * sf + id] = q[f][3] + cb * h[f];
+          endw[f * sf + id] = c0 + cb * h[f];
         }
       } else if (stage < 3) {
 #pragma unroll
@@ -297,9 +297,11 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
       }
     }
 #pragma unroll
-    for (int f = 0; f < 9; f++)
-#pragma unroll
-      for (int m2 = 0; m2 < 4; m2++) q[f][m2] = q[f][m2 + 1];
+    for (int f = 0; f < 9; f++) {
+      q[f][0] = q[f][1];
+      q[f][1] = q[f][2];
+      q[f][2] = to_f(W[f * S::WY * S::WX + wc]);
+    }
     __syncthreads();
   }
   if constexpr (WP == 2) {
