@@ -197,72 +197,69 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
       const float slw = Cc(CF_SLW);
       Medium<MED> md;
       md.load(Cc);
-      CellAcc acc;
-      acc.zero();
-      // x
-      {
-        float d[9];
+      // the 9 derivatives of the stage input along one axis at this cell
+      auto deriv_x = [&](float d[9]) {
 #pragma unroll
         for (int f = 0; f < 9; f++) {
           const TW *r = W + f * S::WY * S::WX + (ty + LY) * S::WX + tx + S::XO - LX;
           d[f] = drp5<DX>(to_f(r[0]), to_f(r[1]), to_f(r[2]), to_f(r[3]), to_f(r[4]));
           if constexpr (WP == 2) d[f] *= s_wsc[f];  // the operator is linear: scale once
         }
-        acc.add_axis(mt[0], d, d + 3);
-        if constexpr (PML) {
-          if (fmask)
-            for (int fi = 0; fi < p.nface; fi++) {
-              const FaceP &fc = p.face[fi];
-              if ((fmask >> fi & 1) && fc.axis == 0 && in_face(fc, i, j, k))
-                pml_face<MED>(p, fc, i, j, k, md, slw, mt[0], d, d + 3, nullptr, nullptr, acc.hc, shot);
-            }
-        }
-      }
-      // y
-      {
-        float d[9];
+      };
+      auto deriv_y = [&](float d[9]) {
 #pragma unroll
         for (int f = 0; f < 9; f++) {
           const TW *r = W + f * S::WY * S::WX + ty * S::WX + tx + S::XO;
           d[f] = drp5<DY>(to_f(r[0]), to_f(r[S::WX]), to_f(r[2 * S::WX]), to_f(r[3 * S::WX]), to_f(r[4 * S::WX]));
           if constexpr (WP == 2) d[f] *= s_wsc[f];
         }
-        acc.add_axis(mt[1], d, d + 3);
-        if constexpr (PML) {
-          if (fmask)
-            for (int fi = 0; fi < p.nface; fi++) {
-              const FaceP &fc = p.face[fi];
-              if ((fmask >> fi & 1) && fc.axis == 1 && in_face(fc, i, j, k))
-                pml_face<MED>(p, fc, i, j, k, md, slw, mt[1], d, d + 3, nullptr, nullptr, acc.hc, shot);
-            }
-        }
-      }
-      // z (queue, this plane and the one ahead in march order; the operator takes increasing k)
-      {
-        float d[9];
+      };
+      auto deriv_z = [&](float d[9]) {  // queue, this plane and the one ahead, in increasing k
 #pragma unroll
         for (int f = 0; f < 9; f++) {
           const float c0 = to_f(W[f * S::WY * S::WX + wc]), c1 = to_f(Wn[f * S::WY * S::WX + wc]);
           d[f] = SD > 0 ? drp5<DZ>(q[f][0], q[f][1], q[f][2], c0, c1) : drp5<DZ>(c1, c0, q[f][2], q[f][1], q[f][0]);
           if constexpr (WP == 2) d[f] *= s_wsc[f];
         }
+      };
+      CellAcc acc;
+      acc.zero();
+      {
+        float d[9];
+        deriv_x(d);
+        acc.add_axis(mt[0], d, d + 3);
+        deriv_y(d);
+        acc.add_axis(mt[1], d, d + 3);
+        deriv_z(d);
         acc.add_axis(mt[2], d, d + 3);
-        if constexpr (PML) {
-          if (fmask)
-            for (int fi = 0; fi < p.nface; fi++) {
-              const FaceP &fc = p.face[fi];
-              if ((fmask >> fi & 1) && fc.axis == 2 && in_face(fc, i, j, k))
-                pml_face<MED>(p, fc, i, j, k, md, slw, mt[2], d, d + 3, nullptr, nullptr, acc.hc, shot);
-            }
-        }
       }
       float h[9];
-      h[0] = slw * acc.mom[0] + acc.hc[0];
-      h[1] = slw * acc.mom[1] + acc.hc[1];
-      h[2] = slw * acc.mom[2] + acc.hc[2];
+      h[0] = slw * acc.mom[0];
+      h[1] = slw * acc.mom[1];
+      h[2] = slw * acc.mom[2];
       md.hooke(acc.G, h + 3);
-#pragma unroll
-      for (int c = 3; c < 9; c++) h[c] += acc.hc[c];
+      if constexpr (PML) {
+        // CFS-PML corrections added to the full right-hand side face by face, in face order
+        // (x1 x2 y1 y2 z1), as the reference applies its face kernels after the inner one;
+        // the face axis' derivatives are recomputed here, when the accumulators above are
+        // dead, to keep the face code's registers free
+        if (fmask)
+          for (int fi = 0; fi < p.nface; fi++) {
+            const FaceP &fc = p.face[fi];
+            if (!(fmask >> fi & 1) || !in_face(fc, i, j, k)) continue;
+            float d[9];
+            if (fc.axis == 0) {
+              deriv_x(d);
+              pml_face<MED>(p, fc, i, j, k, md, slw, mt[0], d, d + 3, nullptr, nullptr, h, shot);
+            } else if (fc.axis == 1) {
+              deriv_y(d);
+              pml_face<MED>(p, fc, i, j, k, md, slw, mt[1], d, d + 3, nullptr, nullptr, h, shot);
+            } else {
+              deriv_z(d);
+              pml_face<MED>(p, fc, i, j, k, md, slw, mt[2], d, d + 3, nullptr, nullptr, h, shot);
+            }
+          }
+      }
       // RK combine (wav_update / wav_update_end)
       const long long id = didx(p, i, j, k);
       const float *PR = reinterpret_cast<const float *>(cpe + cs * S::CPE_SLOT + S::COEF_BYTES) + cell;
