@@ -51,14 +51,16 @@ struct BulkSmem {
   static constexpr int WAVE_SLOT = ((WAVE_ELEMS * (int)sizeof(TW) + 127) / 128) * 128;  // bytes
   static constexpr int COEF_BYTES = NC * CELLS * (int)sizeof(TC);  // multiple of 128 for every medium
   static constexpr int FLD_BYTES = 9 * CELLS * 4;
-  // w_pre staged by TMA unless that keeps MINB blocks from fitting one SM (then read directly)
-  static constexpr int FULL = 3 * WAVE_SLOT + 2 * (COEF_BYTES + 2 * FLD_BYTES) + 64;
-  static constexpr bool PT = MINB == 1 || FULL <= 113 * 1024;
+  // w_pre staged by TMA at one block per SM; with two blocks per SM it is read directly
+  // (measured faster on 480x480x240: the smaller ring leaves the SM more L1)
+  static constexpr bool PT = MINB == 1;
   static constexpr int OFF_END = COEF_BYTES + (PT ? FLD_BYTES : 0);  // within a cpe slot
   static constexpr int CPE_SLOT = OFF_END + FLD_BYTES;
-  static constexpr int OFF_CPE = 3 * WAVE_SLOT;
+  static constexpr int NW = 3;  // wave ring slots: this plane, the one ahead, one in flight
+  static constexpr int OFF_CPE = NW * WAVE_SLOT;
   static constexpr int OFF_BAR = OFF_CPE + 2 * CPE_SLOT;
   static constexpr int BYTES = OFF_BAR + 8 * 8;
+  static_assert(NW + 2 <= 8, "mbarrier area");
   static_assert(COEF_BYTES % 128 == 0, "w_pre/w_end boxes must stay 128-byte aligned");
   static_assert(MINB == 1 || MINB * (BYTES + 1024) <= 228 * 1024, "MINB blocks must fit one SM's shared memory");
 };
@@ -87,7 +89,7 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
   __shared__ float s_wsc[18];  // FP16 stage levels: scale, inverse scale
   TW *wave = reinterpret_cast<TW *>(smem);
   unsigned char *cpe = smem + S::OFF_CPE;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + S::OFF_BAR);  // 0..2 wave, 3..4 cpe
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + S::OFF_BAR);  // NW wave, then 2 cpe
 
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   // shots are the fastest block index: the nshot blocks of one tile run side by side and
@@ -116,7 +118,7 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
   const int xc = GX + bx * TX, yc = 3 + by * TYT;
 
   if (tid == 0) {
-    for (int b = 0; b < 5; b++) mbar_init(&bar[b], 1);
+    for (int b = 0; b < S::NW + 2; b++) mbar_init(&bar[b], 1);
     fence_barrier_init();
   }
   if constexpr (WP != 0) {
@@ -126,14 +128,14 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
 
   auto issue_wave = [&](int m) {
     const int kk = k0 + m * SD;
-    uint64_t *b = &bar[m % 3];
+    uint64_t *b = &bar[m % S::NW];
     mbar_expect_tx(b, wave_bytes);
-    tma_load_4d(wave + (m % 3) * (S::WAVE_SLOT / (int)sizeof(TW)), &tm.cur, xw, yw, kk + 3, 9 * shot, b);
+    tma_load_4d(wave + (m % S::NW) * (S::WAVE_SLOT / (int)sizeof(TW)), &tm.cur, xw, yw, kk + 3, 9 * shot, b);
   };
   auto issue_cpe = [&](int m) {
     const int kk = k0 + m * SD;
     const int sl = m & 1;
-    uint64_t *b = &bar[3 + sl];
+    uint64_t *b = &bar[S::NW + sl];
     unsigned char *base = cpe + sl * S::CPE_SLOT;
     mbar_expect_tx(b, cpe_bytes);
     tma_load_4d(base, &tm.coef, xc, yc, kk + 3, 0, b);
@@ -141,8 +143,7 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
     if (need_end) tma_load_4d(base + S::OFF_END, &tm.end, xc, yc, kk + 3, 9 * shot, b);
   };
   if (tid == 0) {
-    issue_wave(0);
-    issue_wave(1);
+    for (int m = 0; m + 1 < S::NW && m <= n; m++) issue_wave(m);  // planes 0..n exist
     issue_cpe(0);
   }
 
@@ -178,12 +179,12 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
   for (int m = 0; m < n; m++) {
     const int k = k0 + m * SD;
     if (tid == 0) {
-      if (m + 2 <= n) issue_wave(m + 2);
+      if (m + S::NW - 1 <= n) issue_wave(m + S::NW - 1);
       if (m + 1 < n) issue_cpe(m + 1);
     }
-    const int ws = m % 3, wn = (m + 1) % 3, cs = m & 1;
-    mbar_wait(&bar[wn], ((m + 1) / 3) & 1, p.err);
-    mbar_wait(&bar[3 + cs], (m >> 1) & 1, p.err);
+    const int ws = m % S::NW, wn = (m + 1) % S::NW, cs = m & 1;
+    mbar_wait(&bar[wn], ((m + 1) / S::NW) & 1, p.err);
+    mbar_wait(&bar[S::NW + cs], (m >> 1) & 1, p.err);
     const TW *W = wave + ws * (S::WAVE_SLOT / (int)sizeof(TW));
     const TW *Wn = wave + wn * (S::WAVE_SLOT / (int)sizeof(TW));
 
