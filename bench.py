@@ -484,7 +484,7 @@ def main():
                "config": {"workload": f"{p.ni}x{p.nj}x{p.nk}", "medium": "elastic_iso", "dh_m": 50.0,
                           "pml_layers": 20, "free_surface": "timg", "sources": 1, "stations": 400,
                           "dt": p.dt, "precision": "fp32", "parallelism": f"replicas x{world}",
-                          "l2": "inputs larger than L2 (wavefield 4x9x58M floats)"},
+                          "l2": f"inputs larger than L2 (wavefield 4 levels x 9 x {(p.ni + 6) * (p.nj + 6) * (p.nk + 6) / 1e6:.1f}M floats)"},
                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                "clocks": clocks, "batched_mixed": batched, "serving": serving}
         print(json.dumps(out), flush=True)
