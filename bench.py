@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--zchunk", type=int, default=0)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched / mixed-precision section")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
+    ap.add_argument("--no-media", action="store_true", help="skip the VTI / aniso section")
     return ap.parse_args()
 
 
@@ -231,6 +232,40 @@ def batched_mixed(local, steps=16):
             out[f"{name}_{nshot}"] = rec
     out["note"] = ("Errors against the FP64 oracle on smaller grids (tests/test_gpu_precision.py): FP32 <= 7e-7, "
                    "16-bit fixed-point coefficients <= 4e-5, mixed (plus FP16 stage levels) <= 5e-4 gather rel L2.")
+    return out
+
+
+def media_bench(local, steps=20):
+    """The anisotropic media on the precision-study grid: 320x320x160 (50 m, CFS-PML 20, free
+    surface, layered Thomsen VTI and Bond-rotated tilted-TI 21-Cij media, one double-couple
+    source, 100 surface stations), FP32 and 16-bit fixed-point coefficients. Reports
+    Gcell-stage/s of graph-replayed steps and the bulk stage's algorithmic bytes (36 wavefield +
+    NCOEF coefficient accesses per cell-stage) per event-timed duration against the measured
+    HBM peak."""
+    from cgfd_b200 import synth, Simulation, CGFD_PREC_FP32, CGFD_PREC_U16_COEF
+    ni, nj, nk = 320, 320, 160
+    peak, _ = measured_peak()
+    out = {"workload": f"{ni}x{nj}x{nk}", "steps_timed": steps}
+    for med, ncoef in (("vti", 15), ("aniso", 31)):
+        p = synth.make_problem(ni, nj, nk, 50.0, 2000, dt=None, medium=med, npml=20, nsrc=1, sta_grid=(10, 10),
+                               fc=3.0, seed=31, src_depth=(2000.0, 2000.0), center_src=True)
+        p.device = local
+        for name, prec, cbytes in (("fp32", CGFD_PREC_FP32, 4), ("u16coef", CGFD_PREC_U16_COEF, 2)):
+            p.precision = prec
+            sim = Simulation(p)
+            ms = _time_steps(sim, steps)
+            sim.set_timing(True)
+            sim.timing(reset=True)
+            sim.enqueue(8)
+            sim.synchronize()
+            bulk_ms, bulk_n = sim.timing(reset=True)["bulk"]
+            sim.set_timing(False)
+            sim.close()
+            bpc = 36 * 4 + ncoef * cbytes
+            achieved = bpc * ni * nj * (nk - 4) / (bulk_ms / bulk_n * 1e-3) / 1e9
+            out[f"{med}_{name}"] = {"value": ni * nj * nk * 4 / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": ms,
+                                    "bulk_ms_per_stage": bulk_ms / bulk_n, "bytes_per_cell_stage": bpc,
+                                    "roofline_frac": achieved / peak}
     return out
 
 
@@ -462,6 +497,13 @@ def main():
         except Exception as ex:  # report, do not fail the headline measurement
             batched = {"error": str(ex)}
 
+    media = None
+    if rank == 0 and world == 1 and not args.no_media:
+        try:
+            media = media_bench(local)
+        except Exception as ex:  # report, do not fail the headline measurement
+            media = {"error": str(ex)}
+
     serving = None
     if rank == 0 and world == 1 and not args.no_serving:
         try:
@@ -486,7 +528,7 @@ def main():
                           "dt": p.dt, "precision": "fp32", "parallelism": f"replicas x{world}",
                           "l2": f"inputs larger than L2 (wavefield 4 levels x 9 x {(p.ni + 6) * (p.nj + 6) * (p.nk + 6) / 1e6:.1f}M floats)"},
                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-               "clocks": clocks, "batched_mixed": batched, "serving": serving}
+               "clocks": clocks, "batched_mixed": batched, "media": media, "serving": serving}
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()

@@ -193,8 +193,11 @@ __device__ __forceinline__ void ld5(int dir, const WaveIn<TW> &cur, int f, long 
 // bulk kernel (0 FP32 stage levels; 1 FP32 input, FP16 output; 2 FP16 input and output).
 // The kernel is latency-bound on its many cached loads: registers are capped at 128 so that
 // 16 warps share each SM (a few spills are cheaper than 8 warps).
-template <int MED, typename TC, int WP>
+// The operator directions of the stage (DX, DY, DZ: 0 backward, 1 forward) are template
+// parameters, so that every stencil offset is a compile-time constant.
+template <int MED, typename TC, int WP, int DX, int DY, int DZ>
 __global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant__ StageP p) {
+  constexpr int DIR[3] = {DX, DY, DZ};
   using TW = typename std::conditional<WP == 2, __half, float>::type;
   using TT = typename std::conditional<WP >= 1, __half, float>::type;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -229,8 +232,8 @@ __global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant_
 #pragma unroll
       for (int f = 0; f < 9; f++) {
         float v[5];
-        ld5(p.dir[a], cur, f, id, offs[a], v);
-        float d = drp5r(p.dir[a], v[0], v[1], v[2], v[3], v[4]);
+        ld5(DIR[a], cur, f, id, offs[a], v);
+        float d = drp5r(DIR[a], v[0], v[1], v[2], v[3], v[4]);
         if (f < 3) dv[a][f] = d; else dtt[a][f - 3] = d;
       }
     }
@@ -250,15 +253,15 @@ __global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant_
       }
       h[0] = slw * mom[0]; h[1] = slw * mom[1]; h[2] = slw * mom[2];
     }
-    const int dzr = p.dir[2];
+    constexpr int dzr = DZ;
     if (p.free_top) {
-      const int idx_last = dzr ? 3 : 1, idx_first = dzr ? -1 : -3;
+      constexpr int idx_last = dzr ? 3 : 1, idx_first = dzr ? -1 : -3;
       if (k >= nk2 - idx_last) {
         // sv_curv_col_el_gpu.cu:53-217
         const int n_free = nk2 - k - idx_first;
         const float jc = __ldg(p.jac + id);
         const float slwjac = slw / jc;
-        const int LXo = op_left(p.dir[0]), LYo = op_left(p.dir[1]), LZo = op_left(dzr);
+        constexpr int LXo = op_left(DX), LYo = op_left(DY), LZo = op_left(dzr);
         // rows of the stress tensor: components (Txx,Txy,Txz), (Txy,Tyy,Tyz), (Txz,Tyz,Tzz)
         const int tr[3][3] = {{3, 8, 7}, {8, 4, 6}, {7, 6, 5}};
 #pragma unroll
@@ -280,9 +283,9 @@ __global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant_
             float fz = __ldg(p.jac + q) * (cv(6, q) * cur(f1, q) + cv(7, q) * cur(f2, q) + cv(8, q) * cur(f3, q));
             vz[n] = sgn * fz;
           }
-          float DxTx = drp5r(p.dir[0], vx[0], vx[1], vx[2], vx[3], vx[4]);
-          float DyTy = drp5r(p.dir[1], vy[0], vy[1], vy[2], vy[3], vy[4]);
-          float DzTz = drp5r(dzr, vz[0], vz[1], vz[2], vz[3], vz[4]);
+          float DxTx = drp5<DX>(vx[0], vx[1], vx[2], vx[3], vx[4]);
+          float DyTy = drp5<DY>(vy[0], vy[1], vy[2], vy[3], vy[4]);
+          float DzTz = drp5<DZ>(vz[0], vz[1], vz[2], vz[3], vz[4]);
           h[c] = (DxTx + DyTy + DzTz) * slwjac;
         }
       }
@@ -539,11 +542,23 @@ int launch_stage_bulk(int med, const StageP &p, int nzc, cudaStream_t st) {
   return 1;
 }
 
+template <int MED, typename TC, int WP>
+static void launch_surface_med(const StageP &p, dim3 grid, dim3 block, cudaStream_t st) {
+  switch (p.dir[0] | (p.dir[1] << 1) | (p.dir[2] << 2)) {
+#define CASE(c)                                                                                          \
+  case c:                                                                                                \
+    k_stage_surface<MED, TC, WP, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1><<<grid, block, 0, st>>>(p);      \
+    break;
+    CASE(0) CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7)
+#undef CASE
+  }
+}
+
 template <typename TC, int WP>
 static void launch_surface_tc(int med, const StageP &p, dim3 grid, dim3 block, cudaStream_t st) {
-  if (med == MED_ISO) k_stage_surface<MED_ISO, TC, WP><<<grid, block, 0, st>>>(p);
-  else if (med == MED_VTI) k_stage_surface<MED_VTI, TC, WP><<<grid, block, 0, st>>>(p);
-  else k_stage_surface<MED_ANISO, TC, WP><<<grid, block, 0, st>>>(p);
+  if (med == MED_ISO) launch_surface_med<MED_ISO, TC, WP>(p, grid, block, st);
+  else if (med == MED_VTI) launch_surface_med<MED_VTI, TC, WP>(p, grid, block, st);
+  else launch_surface_med<MED_ANISO, TC, WP>(p, grid, block, st);
 }
 
 int launch_stage_surface(int med, int coef_type, int wave16, const StageP &p, cudaStream_t st) {
