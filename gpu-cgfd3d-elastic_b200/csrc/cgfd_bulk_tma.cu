@@ -31,11 +31,12 @@ template <int WP> struct WavePolicy {
 
 // Tile height and resident blocks per SM for interior tiles (MINB) and PML tiles (MINB_PML):
 // two 32x8 blocks per SM (two independent barrier domains hide each other's pipeline waits)
-// wherever registers (<= 128 per thread) and shared memory allow; the VTI face code and
-// everything aniso need more registers and run one.
-template <int MED> struct TileCfg { static constexpr int TYT = 8, MINB = 1, MINB_PML = 1; };
+// wherever registers (<= 128 per thread) and shared memory allow (iso and VTI, interior and
+// PML tiles); the 21-Cij medium's 31 coefficient fields do not fit twice at 32x8, so it runs
+// 32x4 tiles, three blocks per SM (12 warps instead of 8 of one 32x8 block).
+template <int MED> struct TileCfg { static constexpr int TYT = 4, MINB = 3, MINB_PML = 3; };
 template <> struct TileCfg<MED_ISO> { static constexpr int TYT = 8, MINB = 2, MINB_PML = 2; };
-template <> struct TileCfg<MED_VTI> { static constexpr int TYT = 8, MINB = 2, MINB_PML = 1; };
+template <> struct TileCfg<MED_VTI> { static constexpr int TYT = 8, MINB = 2, MINB_PML = 2; };
 template <int MED, bool PML> struct BlocksPerSm {
   static constexpr int value = PML ? TileCfg<MED>::MINB_PML : TileCfg<MED>::MINB;
 };
