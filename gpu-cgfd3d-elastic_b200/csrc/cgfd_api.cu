@@ -375,9 +375,60 @@ int guarded(Fn fn) {
   }
 }
 
-void upload_field(cgfd_problem *p, const float *host_ref, float *dst, float *stage_buf, int mode, int ghosts) {
+// Host -> device copies of the caller's model arrays (pageable memory) through two pinned
+// chunks: host threads fill one chunk while the copy engine drains the other, so the upload
+// runs at the slower of a parallel host memcpy and the host link instead of the driver's
+// serial pageable path.
+class PinnedStager {
+ public:
+  static constexpr size_t kChunk = size_t(64) << 20;
+  explicit PinnedStager(cudaStream_t st) : st_(st) {
+    for (int b = 0; b < 2; b++) {
+      CK(cudaHostAlloc(reinterpret_cast<void **>(&buf_[b]), kChunk, cudaHostAllocDefault));
+      CK(cudaEventCreateWithFlags(&done_[b], cudaEventDisableTiming));
+    }
+  }
+  ~PinnedStager() {
+    cudaStreamSynchronize(st_);
+    for (int b = 0; b < 2; b++) {
+      if (buf_[b]) cudaFreeHost(buf_[b]);
+      if (done_[b]) cudaEventDestroy(done_[b]);
+    }
+  }
+  PinnedStager(const PinnedStager &) = delete;
+  PinnedStager &operator=(const PinnedStager &) = delete;
+
+  void copy(void *dst, const void *src, size_t n) {
+    for (size_t o = 0; o < n; o += kChunk) {
+      const size_t m = std::min(kChunk, n - o);
+      const int b = next_;
+      next_ ^= 1;
+      CK(cudaEventSynchronize(done_[b]));  // the previous copy out of this chunk has finished
+      const char *in = static_cast<const char *>(src) + o;
+      const long long pieces = (long long)((m + kPiece - 1) / kPiece);
+#pragma omp parallel for schedule(static)
+      for (long long q = 0; q < pieces; q++) {
+        const size_t a = (size_t)q * kPiece;
+        std::memcpy(buf_[b] + a, in + a, std::min(kPiece, m - a));
+      }
+      CK(cudaMemcpyAsync(static_cast<char *>(dst) + o, buf_[b], m, cudaMemcpyHostToDevice, st_));
+      CK(cudaEventRecord(done_[b], st_));
+    }
+  }
+
+ private:
+  static constexpr size_t kPiece = size_t(1) << 20;
+  cudaStream_t st_;
+  char *buf_[2] = {nullptr, nullptr};
+  cudaEvent_t done_[2] = {nullptr, nullptr};
+  int next_ = 0;
+};
+
+void upload_field(cgfd_problem *p, const float *host_ref, float *dst, float *stage_buf, int mode, int ghosts,
+                  PinnedStager *ps = nullptr) {
   size_t n = (size_t)(p->ni + 6) * (p->nj + 6) * (p->nk + 6);
-  CK(cudaMemcpyAsync(stage_buf, host_ref, n * sizeof(float), cudaMemcpyHostToDevice, p->stream));
+  if (ps) ps->copy(stage_buf, host_ref, n * sizeof(float));
+  else CK(cudaMemcpyAsync(stage_buf, host_ref, n * sizeof(float), cudaMemcpyHostToDevice, p->stream));
   cgfd::launch_repack_in(stage_buf, dst, p->ni, p->nj, p->nk, p->sx, p->sz, p->off0, mode, ghosts, p->stream);
   CK(cudaGetLastError());
 }
@@ -579,12 +630,17 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   // coefficients: metric (ghosts kept for the traction image), 1/rho, medium
   cgfd::RefGrid g(p->ni, p->nj, p->nk);
   float *stage_buf = dmalloc<float>(g.siz_icmp, B);
-  upload_field(p, d->metric, p->jac, stage_buf, 0, 1);
-  for (int c = 0; c < 9; c++) upload_field(p, d->metric + (size_t)(1 + c) * g.siz_icmp, p->coef + (size_t)c * p->sf, stage_buf, 0, 1);
-  upload_field(p, d->medium, p->coef + (size_t)cgfd::CF_SLW * p->sf, stage_buf, 1, 0);
-  int nmed = cgfd::medium_ncmp(d->medium_type) - 1;
-  for (int c = 0; c < nmed; c++)
-    upload_field(p, d->medium + (size_t)(1 + c) * g.siz_icmp, p->coef + (size_t)(cgfd::CF_MED + c) * p->sf, stage_buf, 0, 0);
+  {
+    PinnedStager ps(p->stream);
+    upload_field(p, d->metric, p->jac, stage_buf, 0, 1, &ps);
+    for (int c = 0; c < 9; c++)
+      upload_field(p, d->metric + (size_t)(1 + c) * g.siz_icmp, p->coef + (size_t)c * p->sf, stage_buf, 0, 1, &ps);
+    upload_field(p, d->medium, p->coef + (size_t)cgfd::CF_SLW * p->sf, stage_buf, 1, 0, &ps);
+    int nmed = cgfd::medium_ncmp(d->medium_type) - 1;
+    for (int c = 0; c < nmed; c++)
+      upload_field(p, d->medium + (size_t)(1 + c) * g.siz_icmp, p->coef + (size_t)(cgfd::CF_MED + c) * p->sf,
+                   stage_buf, 0, 0, &ps);
+  }
   CK(cudaStreamSynchronize(p->stream));
   cudaFree(stage_buf);
   B -= g.siz_icmp * sizeof(float);
@@ -1142,7 +1198,10 @@ int cgfd_set_wavefield_shot(cgfd_problem *p, int shot, const float *in) {
     size_t acc = 0;
     float *tmp = dmalloc<float>(g.siz_icmp, acc);
     float *pre = p->wbuf[p->it & 1] + (size_t)shot * 9 * p->sf;
-    for (int c = 0; c < 9; c++) upload_field(p, in + (size_t)c * g.siz_icmp, pre + (size_t)c * p->sf, tmp, 0, 0);
+    {
+      PinnedStager ps(p->stream);
+      for (int c = 0; c < 9; c++) upload_field(p, in + (size_t)c * g.siz_icmp, pre + (size_t)c * p->sf, tmp, 0, 0, &ps);
+    }
     refresh_wave_max(p);
     CK(cudaStreamSynchronize(p->stream));
     cudaFree(tmp);
