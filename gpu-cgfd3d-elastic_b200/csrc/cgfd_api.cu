@@ -378,27 +378,28 @@ int guarded(Fn fn) {
 // Host -> device copies of the caller's model arrays (pageable memory) through two pinned
 // chunks: host threads fill one chunk while the copy engine drains the other, so the upload
 // runs at the slower of a parallel host memcpy and the host link instead of the driver's
-// serial pageable path.
+// serial pageable path. One stager per device, allocated on first use and kept for the life
+// of the process (2 x 64 MiB of pinned host memory): allocating and freeing pinned memory per
+// problem would synchronise the device under the serving loop's concurrent problems. Users
+// hold its lock for a whole upload; each chunk is refilled only after the copy out of it
+// has completed (per-chunk events), so no device-wide synchronisation is involved.
 class PinnedStager {
  public:
   static constexpr size_t kChunk = size_t(64) << 20;
-  explicit PinnedStager(cudaStream_t st) : st_(st) {
-    for (int b = 0; b < 2; b++) {
-      CK(cudaHostAlloc(reinterpret_cast<void **>(&buf_[b]), kChunk, cudaHostAllocDefault));
-      CK(cudaEventCreateWithFlags(&done_[b], cudaEventDisableTiming));
-    }
-  }
-  ~PinnedStager() {
-    cudaStreamSynchronize(st_);
-    for (int b = 0; b < 2; b++) {
-      if (buf_[b]) cudaFreeHost(buf_[b]);
-      if (done_[b]) cudaEventDestroy(done_[b]);
-    }
-  }
-  PinnedStager(const PinnedStager &) = delete;
-  PinnedStager &operator=(const PinnedStager &) = delete;
+  // fields below this size go through the plain pageable copy
+  static constexpr size_t kMinBytes = size_t(16) << 20;
 
-  void copy(void *dst, const void *src, size_t n) {
+  static PinnedStager &for_device(int device) {
+    static std::mutex mu;
+    static std::vector<PinnedStager *> all;
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)all.size() <= device) all.resize(device + 1, nullptr);
+    if (!all[device]) all[device] = new PinnedStager();  // device is current
+    return *all[device];
+  }
+  std::mutex &mutex() { return mu_; }
+
+  void copy(void *dst, const void *src, size_t n, cudaStream_t st) {
     for (size_t o = 0; o < n; o += kChunk) {
       const size_t m = std::min(kChunk, n - o);
       const int b = next_;
@@ -411,23 +412,31 @@ class PinnedStager {
         const size_t a = (size_t)q * kPiece;
         std::memcpy(buf_[b] + a, in + a, std::min(kPiece, m - a));
       }
-      CK(cudaMemcpyAsync(static_cast<char *>(dst) + o, buf_[b], m, cudaMemcpyHostToDevice, st_));
-      CK(cudaEventRecord(done_[b], st_));
+      CK(cudaMemcpyAsync(static_cast<char *>(dst) + o, buf_[b], m, cudaMemcpyHostToDevice, st));
+      CK(cudaEventRecord(done_[b], st));
     }
   }
 
  private:
+  PinnedStager() {
+    for (int b = 0; b < 2; b++) {
+      CK(cudaHostAlloc(reinterpret_cast<void **>(&buf_[b]), kChunk, cudaHostAllocPortable));
+      CK(cudaEventCreateWithFlags(&done_[b], cudaEventDisableTiming));
+    }
+  }
   static constexpr size_t kPiece = size_t(1) << 20;
-  cudaStream_t st_;
+  std::mutex mu_;
   char *buf_[2] = {nullptr, nullptr};
   cudaEvent_t done_[2] = {nullptr, nullptr};
   int next_ = 0;
 };
 
+// One model field (reference layout) into its device array, through stage_buf. ps: the
+// device's pinned stager, its lock held by the caller (nullptr: plain pageable copy).
 void upload_field(cgfd_problem *p, const float *host_ref, float *dst, float *stage_buf, int mode, int ghosts,
                   PinnedStager *ps = nullptr) {
   size_t n = (size_t)(p->ni + 6) * (p->nj + 6) * (p->nk + 6);
-  if (ps) ps->copy(stage_buf, host_ref, n * sizeof(float));
+  if (ps && n * sizeof(float) >= PinnedStager::kMinBytes) ps->copy(stage_buf, host_ref, n * sizeof(float), p->stream);
   else CK(cudaMemcpyAsync(stage_buf, host_ref, n * sizeof(float), cudaMemcpyHostToDevice, p->stream));
   cgfd::launch_repack_in(stage_buf, dst, p->ni, p->nj, p->nk, p->sx, p->sz, p->off0, mode, ghosts, p->stream);
   CK(cudaGetLastError());
@@ -631,7 +640,8 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   cgfd::RefGrid g(p->ni, p->nj, p->nk);
   float *stage_buf = dmalloc<float>(g.siz_icmp, B);
   {
-    PinnedStager ps(p->stream);
+    PinnedStager &ps = PinnedStager::for_device(p->device);
+    std::lock_guard<std::mutex> lk(ps.mutex());
     upload_field(p, d->metric, p->jac, stage_buf, 0, 1, &ps);
     for (int c = 0; c < 9; c++)
       upload_field(p, d->metric + (size_t)(1 + c) * g.siz_icmp, p->coef + (size_t)c * p->sf, stage_buf, 0, 1, &ps);
@@ -1199,7 +1209,8 @@ int cgfd_set_wavefield_shot(cgfd_problem *p, int shot, const float *in) {
     float *tmp = dmalloc<float>(g.siz_icmp, acc);
     float *pre = p->wbuf[p->it & 1] + (size_t)shot * 9 * p->sf;
     {
-      PinnedStager ps(p->stream);
+      PinnedStager &ps = PinnedStager::for_device(p->device);
+      std::lock_guard<std::mutex> lk(ps.mutex());
       for (int c = 0; c < 9; c++) upload_field(p, in + (size_t)c * g.siz_icmp, pre + (size_t)c * p->sf, tmp, 0, 0, &ps);
     }
     refresh_wave_max(p);
