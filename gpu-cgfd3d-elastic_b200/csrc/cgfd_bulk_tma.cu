@@ -9,12 +9,13 @@
 //     row on one side and three on the other, so the box holds rows [-1, TYT+3) for forward
 //     and [-3, TYT+1) for backward y operators; the x halo is 16 bytes on both sides (TMA
 //     alignment);
-//   - the coefficients (metrics, 1/rho, moduli) and, when the stage needs them, w_pre and
-//     w_end of the same plane (centre boxes) into a 2-slot ring.
+//   - the coefficients (metrics, 1/rho, moduli) and, when the stage needs them, w_end and
+//     (at one block per SM) w_pre of the same plane (centre boxes) into a 2-slot ring; with
+//     two blocks per SM w_pre is read directly by each thread.
 // The z march runs upwards for backward z operators and downwards for forward ones, so the
 // one-sided operator always needs exactly one plane ahead; the current plane and the one
-// ahead are read from the ring, the 3 planes behind live in a per-thread register queue. No thread computes an address
-// for a stencil or coefficient load; HBM sees every value once per stage.
+// ahead are read from the ring, the 3 planes behind live in a per-thread register queue.
+// No thread computes an address for a stencil or coefficient load.
 #include "cgfd_dev.cuh"
 #include "cgfd_launch.h"
 #include "cgfd_tma.cuh"
