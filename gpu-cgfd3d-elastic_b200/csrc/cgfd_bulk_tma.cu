@@ -302,6 +302,9 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
       q[f][1] = q[f][2];
       q[f][2] = to_f(W[f * S::WY * S::WX + wc]);
     }
+    // the slots read in this plane are refilled by TMA after the barrier: every read of them
+    // (the queue load above may still be in flight) must be ordered before those writes
+    fence_proxy_async_smem();
     __syncthreads();
   }
   if constexpr (WP == 2) {

@@ -27,6 +27,14 @@ __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// Orders this thread's earlier generic-proxy accesses to shared memory before later
+// async-proxy (TMA) accesses. A block barrier alone does not: a shared-memory load whose value
+// is not yet consumed can still be outstanding when the barrier completes, and a TMA load
+// issued after the barrier into the same buffer may then overwrite the data before it is read.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }

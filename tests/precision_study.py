@@ -1,0 +1,95 @@
+"""Long-run precision study: seismogram errors of every storage-precision mode against the FP64
+oracle (the CPU restatement instantiated in double, same inputs) on VTI and 21-Cij aniso media.
+
+The GPU test suite checks the modes over 240 steps on 56x52x40 grids; this study runs them long
+enough for phase errors to accumulate (default 2000 steps, the step count of the anisotropic
+precision workload) on the largest grid whose FP64 oracle run stays practical on a CPU
+(128x128x64, 50 m, CFS-PML 10, free surface, one double-couple source at 1.5 km, 16 surface
+stations; the full 320x320x160 workload would take the oracle days).
+
+Two stages, because the oracle runs on the host and the modes on a GPU:
+
+    python tests/precision_study.py oracle --cache DIR     # CPU: FP64 oracle seismograms
+    python tests/precision_study.py gpu --cache DIR        # GPU: every mode, error table
+
+Errors per mode (against FP64): relative L2 of the whole gather, largest per-station relative
+L2 (denominator floored at 1e-3 of the strongest station, as in the tests) and relative error
+of the peak amplitude.
+"""
+import argparse
+import json
+import os
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+for _p in (ROOT, os.path.join(ROOT, "gpu-cgfd3d-elastic_b200"), os.path.join(ROOT, "tests")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+MEDIA = ("vti", "aniso")
+
+
+def problem(medium, ni, nj, nk, nsteps):
+    from cgfd_b200 import synth
+    return synth.make_problem(ni, nj, nk, 50.0, nsteps, dt=None, medium=medium, npml=10, nsrc=1, sta_grid=(4, 4),
+                              fc=4.0, seed=41, src_depth=(1500.0, 1500.0), center_src=True)
+
+
+def stage_oracle(args):
+    from oracle.oracle import Oracle
+    os.makedirs(args.cache, exist_ok=True)
+    for med in MEDIA:
+        p = problem(med, args.ni, args.nj, args.nk, args.steps)
+        t = time.perf_counter()
+        o = Oracle(p, fp64=True)
+        o.run()
+        s = o.seismograms()
+        np.savez_compressed(os.path.join(args.cache, f"fp64_{med}.npz"), seis=s, dt=p.dt, steps=args.steps,
+                            shape=np.array([args.ni, args.nj, args.nk]))
+        print(f"{med}: FP64 oracle {time.perf_counter() - t:.0f} s, {s.shape[0]} stations", flush=True)
+
+
+def stage_gpu(args):
+    from cgfd_b200 import (Simulation, CGFD_PREC_FP32, CGFD_PREC_BF16_COEF, CGFD_PREC_FP16_COEF,
+                           CGFD_PREC_U16_COEF, CGFD_PREC_FP16_WAVE)
+    from helpers import rel_l2, per_station_rel_l2
+    modes = {"fp32": CGFD_PREC_FP32, "bf16_coef": CGFD_PREC_BF16_COEF, "fp16_coef": CGFD_PREC_FP16_COEF,
+             "u16_coef": CGFD_PREC_U16_COEF, "fp16_wave": CGFD_PREC_FP16_WAVE}
+    out = {"grid": f"{args.ni}x{args.nj}x{args.nk}", "steps": args.steps}
+    for med in MEDIA:
+        z = np.load(os.path.join(args.cache, f"fp64_{med}.npz"))
+        if int(z["steps"]) != args.steps or list(z["shape"]) != [args.ni, args.nj, args.nk]:
+            raise SystemExit(f"cache for {med} was made for another configuration")
+        ref = z["seis"]
+        peak = float(np.abs(ref).max())
+        p = problem(med, args.ni, args.nj, args.nk, args.steps)
+        for name, prec in modes.items():
+            p.precision = prec
+            sim = Simulation(p)
+            sim.run()
+            s = sim.seismograms()
+            sim.close()
+            out[f"{med}_{name}"] = {"gather_rel_l2": rel_l2(s, ref), "station_rel_l2": per_station_rel_l2(s, ref),
+                                    "peak_rel_err": abs(float(np.abs(s).max()) - peak) / peak}
+            e = out[f"{med}_{name}"]
+            print(f"{med:6s} {name:10s} gather {e['gather_rel_l2']:.2e}  station {e['station_rel_l2']:.2e}  "
+                  f"peak {e['peak_rel_err']:.2e}", flush=True)
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("stage", choices=["oracle", "gpu"])
+    ap.add_argument("--cache", required=True, help="directory of the FP64 oracle seismograms")
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--grid", type=int, nargs=3, default=(128, 128, 64))
+    args = ap.parse_args()
+    args.ni, args.nj, args.nk = args.grid
+    (stage_oracle if args.stage == "oracle" else stage_gpu)(args)
+
+
+if __name__ == "__main__":
+    main()
