@@ -12,6 +12,9 @@ Two stages, because the oracle runs on the host and the modes on a GPU:
     python tests/precision_study.py oracle --cache DIR     # CPU: FP64 oracle seismograms
     python tests/precision_study.py gpu --cache DIR        # GPU: every mode, error table
 
+`oracle --cache tests/golden` made the committed fixtures tests/golden/fp64_long_{vti,aniso}.npz
+that tests/test_gpu_precision_long.py checks the FP32, fixed-point and mixed modes against.
+
 Errors per mode (against FP64): relative L2 of the whole gather, largest per-station relative
 L2 (denominator floored at 1e-3 of the strongest station, as in the tests) and relative error
 of the peak amplitude.
@@ -47,7 +50,7 @@ def stage_oracle(args):
         o = Oracle(p, fp64=True)
         o.run()
         s = o.seismograms()
-        np.savez_compressed(os.path.join(args.cache, f"fp64_{med}.npz"), seis=s, dt=p.dt, steps=args.steps,
+        np.savez_compressed(os.path.join(args.cache, f"fp64_long_{med}.npz"), seis=s, dt=p.dt, steps=args.steps,
                             shape=np.array([args.ni, args.nj, args.nk]))
         print(f"{med}: FP64 oracle {time.perf_counter() - t:.0f} s, {s.shape[0]} stations", flush=True)
 
@@ -60,7 +63,7 @@ def stage_gpu(args):
              "u16_coef": CGFD_PREC_U16_COEF, "fp16_wave": CGFD_PREC_FP16_WAVE}
     out = {"grid": f"{args.ni}x{args.nj}x{args.nk}", "steps": args.steps}
     for med in MEDIA:
-        z = np.load(os.path.join(args.cache, f"fp64_{med}.npz"))
+        z = np.load(os.path.join(args.cache, f"fp64_long_{med}.npz"))
         if int(z["steps"]) != args.steps or list(z["shape"]) != [args.ni, args.nj, args.nk]:
             raise SystemExit(f"cache for {med} was made for another configuration")
         ref = z["seis"]

@@ -43,3 +43,15 @@ def test_oracle_matches_reference_golden(name):
     for q in range(15):
         assert np.abs(z["pg"][q]).max() > 0
         assert rel_l2(pg[q], z["pg"][q]) <= 2e-5, q
+
+
+@pytest.mark.parametrize("medium", ["vti", "aniso"])
+def test_long_run_fixture_matches_study_configuration(medium):
+    """The committed FP64 seismograms belong to the study's problem (same dt, stations, steps)."""
+    import precision_study
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", f"fp64_long_{medium}.npz"))
+    ni, nj, nk = [int(v) for v in z["shape"]]
+    p = precision_study.problem(medium, ni, nj, nk, int(z["steps"]))
+    assert abs(p.dt - float(z["dt"])) < 1e-9
+    assert z["seis"].shape == (p.sta.num, 9, p.nt_total)
+    assert np.isfinite(z["seis"]).all() and np.abs(z["seis"]).max() > 0
