@@ -497,19 +497,21 @@ def main():
         except Exception as ex:  # report, do not fail the headline measurement
             batched = {"error": str(ex)}
 
-    media = None
-    if rank == 0 and world == 1 and not args.no_media:
-        try:
-            media = media_bench(local)
-        except Exception as ex:  # report, do not fail the headline measurement
-            media = {"error": str(ex)}
-
     serving = None
     if rank == 0 and world == 1 and not args.no_serving:
         try:
             serving = serving_bench(local)
         except Exception as ex:  # report, do not fail the headline measurement
             serving = {"error": str(ex)}
+
+    # after serving: the large anisotropic models would otherwise sit in host memory while the
+    # serving loop's requests are built and uploaded
+    media = None
+    if rank == 0 and world == 1 and not args.no_media:
+        try:
+            media = media_bench(local)
+        except Exception as ex:  # report, do not fail the headline measurement
+            media = {"error": str(ex)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
