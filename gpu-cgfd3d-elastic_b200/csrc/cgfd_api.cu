@@ -46,18 +46,48 @@ const int kPairFlags[8][3] = {{0, 0, 0}, {1, 1, 0}, {1, 1, 1}, {0, 0, 1},
 const float kRkA[3] = {0.5f, 0.5f, 1.0f};                                          // fd_t.cu:35-37
 const float kRkB[4] = {1.0f / 6.0f, 1.0f / 3.0f, 1.0f / 3.0f, 1.0f / 6.0f};        // fd_t.cu:39-42
 
+// Device memory of a problem comes from the device's stream-ordered memory pool, allocated and
+// freed in the order of the problem's own stream: freeing a problem (cudaFreeAsync) does not
+// synchronise the device, so the serving loop retires one problem while others keep running
+// (cudaFree waits for all work on the device). The pool keeps freed memory for the next
+// problem (release threshold raised once per device).
+void keep_pool_memory(int device) {
+  static std::mutex mu;
+  static std::vector<int> done;
+  std::lock_guard<std::mutex> lk(mu);
+  if (std::find(done.begin(), done.end(), device) != done.end()) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    // reuse memory another stream freed only once that free has completed (no hidden
+    // dependency on the other problem's stream)
+    int no = 0;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
+  }
+  done.push_back(device);
+}
+
 template <typename T>
-T *dmalloc(size_t n, size_t &acc) {
+T *dmalloc(size_t n, size_t &acc, cudaStream_t st) {
   void *p = nullptr;
   if (n == 0) return nullptr;
-  cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+  cudaError_t e = cudaMallocAsync(&p, n * sizeof(T), st);
   if (e == cudaErrorMemoryAllocation) {
     cudaGetLastError();
     throw cgfd::Error(CGFD_ERR_NOMEM, "device allocation of " + std::to_string(n * sizeof(T)) + " bytes failed");
   }
-  if (e != cudaSuccess) throw cgfd::Error(CGFD_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  if (e != cudaSuccess) throw cgfd::Error(CGFD_ERR_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+  // the allocation is usable by the host's synchronous copies and by every stream from here on
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) throw cgfd::Error(CGFD_ERR_CUDA, std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e));
   acc += n * sizeof(T);
   return (T *)p;
+}
+
+// frees memory from dmalloc in the order of stream st (nullptr is ignored)
+inline void dfree(void *ptr, cudaStream_t st) {
+  if (ptr) cudaFreeAsync(ptr, st);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -346,12 +376,17 @@ struct cgfd_problem {
       if (graph_ok[s]) cudaGraphExecDestroy(graph[s]);
     for (auto &t : pending) { ev_free.push_back(t.a); ev_free.push_back(t.b); }
     for (auto e : ev_free) cudaEventDestroy(e);
-    for (auto *p : wbuf) cudaFree(p);
-    cudaFree(coef); cudaFree(coef16); cudaFree(jac); cudaFree(matx); cudaFree(maty);
-    for (Face &f : faces) { cudaFree(f.A); cudaFree(f.B); cudaFree(f.D); cudaFree(f.aux); }
-    cudaFree(d_it_begin); cudaFree(d_ext_num); cudaFree(d_src_shot); cudaFree(d_ext_idx); cudaFree(d_ext_wv); cudaFree(d_ext_wt);
-    cudaFree(d_wsc); cudaFree(d_srcb); cudaFree(d_amax); cudaFree(d_tiles); cudaFree(d_pg); cudaFree(d_dis); cudaFree(d_box);
-    cudaFree(d_stf); cudaFree(d_idx8); cudaFree(d_w8); cudaFree(d_seis); cudaFree(d_it); cudaFree(d_flag);
+    if (stream) {  // everything below was allocated in the order of this stream
+      const cudaStream_t st = stream;
+      for (auto *p : wbuf) dfree(p, st);
+      dfree(coef, st); dfree(coef16, st); dfree(jac, st); dfree(matx, st); dfree(maty, st);
+      for (Face &f : faces) { dfree(f.A, st); dfree(f.B, st); dfree(f.D, st); dfree(f.aux, st); }
+      dfree(d_it_begin, st); dfree(d_ext_num, st); dfree(d_src_shot, st); dfree(d_ext_idx, st); dfree(d_ext_wv, st);
+      dfree(d_ext_wt, st); dfree(d_wsc, st); dfree(d_srcb, st); dfree(d_amax, st); dfree(d_tiles, st); dfree(d_pg, st);
+      dfree(d_dis, st); dfree(d_box, st); dfree(d_stf, st); dfree(d_idx8, st); dfree(d_w8, st); dfree(d_seis, st);
+      dfree(d_it, st); dfree(d_flag, st);
+      cudaStreamSynchronize(st);
+    }
     if (stream) cudaStreamDestroy(stream);
     if (side) cudaStreamDestroy(side);
     if (ev_fork) cudaEventDestroy(ev_fork);
@@ -451,7 +486,7 @@ void upload_field(cgfd_problem *p, const float *host_ref, float *dst, float *sta
 //                field's range -- for the bounded ranges of metrics, 1/rho and moduli this
 //                is 20-30x finer than FP16.
 void to_16bit_coefficients(cgfd_problem *p) {
-  unsigned int *d_mm = dmalloc<unsigned int>(2 * p->ncoef, p->bytes);
+  unsigned int *d_mm = dmalloc<unsigned int>(2 * p->ncoef, p->bytes, p->stream);
   std::vector<unsigned int> mm(2 * p->ncoef);
   for (int c = 0; c < p->ncoef; c++) { mm[2 * c] = 0xffffffffu; mm[2 * c + 1] = 0u; }
   CK(cudaMemcpyAsync(d_mm, mm.data(), sizeof(unsigned int) * mm.size(), cudaMemcpyHostToDevice, p->stream));
@@ -461,9 +496,9 @@ void to_16bit_coefficients(cgfd_problem *p) {
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(mm.data(), d_mm, sizeof(unsigned int) * mm.size(), cudaMemcpyDeviceToHost, p->stream));
   CK(cudaStreamSynchronize(p->stream));
-  cudaFree(d_mm);
+  dfree(d_mm, p->stream);
   p->bytes -= sizeof(unsigned int) * 2 * p->ncoef;
-  p->coef16 = dmalloc<uint16_t>((size_t)p->ncoef * p->sf, p->bytes);
+  p->coef16 = dmalloc<uint16_t>((size_t)p->ncoef * p->sf, p->bytes, p->stream);
   for (int c = 0; c < p->ncoef; c++) {
     const double lo = cgfd::coef_key_to_float(mm[2 * c]), hi = cgfd::coef_key_to_float(mm[2 * c + 1]);
     if (!std::isfinite(lo) || !std::isfinite(hi))
@@ -483,7 +518,7 @@ void to_16bit_coefficients(cgfd_problem *p) {
   }
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(p->stream));
-  cudaFree(p->coef);
+  dfree(p->coef, p->stream);
   p->coef = nullptr;
   p->bytes -= sizeof(float) * p->ncoef * p->sf;
 }
@@ -603,6 +638,7 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   p->wave16 = d->precision == CGFD_PREC_FP16_WAVE ? 1 : 0;
   p->device = d->device;
   CK(cudaSetDevice(p->device));
+  keep_pool_memory(p->device);
   CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
@@ -629,16 +665,16 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   // levels 0-1 (w_pre / w_end) FP32; 2-3 (RK stage inputs) FP32 or FP16
   const size_t lev_bytes[4] = {4, 4, p->wave16 ? 2u : 4u, p->wave16 ? 2u : 4u};
   for (int l = 0; l < 4; l++)
-    p->wbuf[l] = (float *)dmalloc<uint16_t>((size_t)9 * p->sf * nshot * (lev_bytes[l] / 2), B);
-  p->coef = dmalloc<float>((size_t)p->ncoef * p->sf, B);
-  p->jac = dmalloc<float>((size_t)p->sf, B);
+    p->wbuf[l] = (float *)dmalloc<uint16_t>((size_t)9 * p->sf * nshot * (lev_bytes[l] / 2), B, p->stream);
+  p->coef = dmalloc<float>((size_t)p->ncoef * p->sf, B, p->stream);
+  p->jac = dmalloc<float>((size_t)p->sf, B, p->stream);
   for (int l = 0; l < 4; l++) CK(cudaMemsetAsync(p->wbuf[l], 0, lev_bytes[l] * 9 * p->sf * nshot, p->stream));
   CK(cudaMemsetAsync(p->coef, 0, sizeof(float) * p->ncoef * p->sf, p->stream));
   CK(cudaMemsetAsync(p->jac, 0, sizeof(float) * p->sf, p->stream));
 
   // coefficients: metric (ghosts kept for the traction image), 1/rho, medium
   cgfd::RefGrid g(p->ni, p->nj, p->nk);
-  float *stage_buf = dmalloc<float>(g.siz_icmp, B);
+  float *stage_buf = dmalloc<float>(g.siz_icmp, B, p->stream);
   {
     PinnedStager &ps = PinnedStager::for_device(p->device);
     std::lock_guard<std::mutex> lk(ps.mutex());
@@ -652,7 +688,7 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
                    stage_buf, 0, 0, &ps);
   }
   CK(cudaStreamSynchronize(p->stream));
-  cudaFree(stage_buf);
+  dfree(stage_buf, p->stream);
   B -= g.siz_icmp * sizeof(float);
   if (p->coef_type != cgfd::COEF_F32) to_16bit_coefficients(p);
 
@@ -684,8 +720,8 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   if (p->free_top) {
     std::vector<float> mx, my;
     cgfd::dvh2dvz(d, mx, my);
-    p->matx = dmalloc<float>(mx.size(), B);
-    p->maty = dmalloc<float>(my.size(), B);
+    p->matx = dmalloc<float>(mx.size(), B, p->stream);
+    p->maty = dmalloc<float>(my.size(), B, p->stream);
     CK(cudaMemcpy(p->matx, mx.data(), mx.size() * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(p->maty, my.data(), my.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
@@ -699,11 +735,11 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
       f.h = fh[a][s];
       f.n = (long long)(f.h.hi[0] - f.h.lo[0] + 1) * (f.h.hi[1] - f.h.lo[1] + 1) * (f.h.hi[2] - f.h.lo[2] + 1);
       size_t N1 = f.h.A.size();
-      f.A = dmalloc<float>(N1, B); f.B = dmalloc<float>(N1, B); f.D = dmalloc<float>(N1, B);
+      f.A = dmalloc<float>(N1, B, p->stream); f.B = dmalloc<float>(N1, B, p->stream); f.D = dmalloc<float>(N1, B, p->stream);
       CK(cudaMemcpy(f.A, f.h.A.data(), N1 * sizeof(float), cudaMemcpyHostToDevice));
       CK(cudaMemcpy(f.B, f.h.B.data(), N1 * sizeof(float), cudaMemcpyHostToDevice));
       CK(cudaMemcpy(f.D, f.h.D.data(), N1 * sizeof(float), cudaMemcpyHostToDevice));
-      f.aux = dmalloc<float>((size_t)3 * 9 * f.n * nshot, B);
+      f.aux = dmalloc<float>((size_t)3 * 9 * f.n * nshot, B, p->stream);
       CK(cudaMemset(f.aux, 0, sizeof(float) * 3 * 9 * f.n * nshot));
       p->faces.push_back(f);
     }
@@ -754,13 +790,13 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
     size_t ne = (size_t)s.nsrc * s.max_ext;
     std::vector<long long> idx(ne, p->off0);
     for (size_t e = 0; e < ne; e++) idx[e] = p->didx(s.ext_i[e], s.ext_j[e], s.ext_k[e]);
-    p->d_it_begin = dmalloc<int>(s.nsrc, B);
-    p->d_ext_num = dmalloc<int>(s.nsrc, B);
-    p->d_ext_idx = dmalloc<long long>(ne, B);
-    p->d_ext_wv = dmalloc<float>(ne, B);
-    p->d_ext_wt = dmalloc<float>(ne, B);
-    p->d_stf = dmalloc<float>(s.stf.size(), B);
-    p->d_src_shot = dmalloc<int>(s.nsrc, B);
+    p->d_it_begin = dmalloc<int>(s.nsrc, B, p->stream);
+    p->d_ext_num = dmalloc<int>(s.nsrc, B, p->stream);
+    p->d_ext_idx = dmalloc<long long>(ne, B, p->stream);
+    p->d_ext_wv = dmalloc<float>(ne, B, p->stream);
+    p->d_ext_wt = dmalloc<float>(ne, B, p->stream);
+    p->d_stf = dmalloc<float>(s.stf.size(), B, p->stream);
+    p->d_src_shot = dmalloc<int>(s.nsrc, B, p->stream);
     CK(cudaMemcpy(p->d_src_shot, p->src_shot.data(), s.nsrc * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(p->d_it_begin, s.it_begin.data(), s.nsrc * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(p->d_ext_num, s.ext_num.data(), s.nsrc * sizeof(int), cudaMemcpyHostToDevice));
@@ -802,9 +838,9 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
     for (int r = 0; r < p->rec.n; r++)
       for (int q = 0; q < 8; q++)
         idx8[(size_t)r * 8 + q] = p->didx(p->rec.i[r] + (q & 1), p->rec.j[r] + ((q >> 1) & 1), p->rec.k[r] + ((q >> 2) & 1));
-    p->d_idx8 = dmalloc<long long>(idx8.size(), B);
-    p->d_w8 = dmalloc<float>(p->rec.w8.size(), B);
-    p->d_seis = dmalloc<float>((size_t)p->rec.n * 9 * p->nt_total * nshot, B);
+    p->d_idx8 = dmalloc<long long>(idx8.size(), B, p->stream);
+    p->d_w8 = dmalloc<float>(p->rec.w8.size(), B, p->stream);
+    p->d_seis = dmalloc<float>((size_t)p->rec.n * 9 * p->nt_total * nshot, B, p->stream);
     CK(cudaMemcpy(p->d_idx8, idx8.data(), idx8.size() * sizeof(long long), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(p->d_w8, p->rec.w8.data(), p->rec.w8.size() * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMemset(p->d_seis, 0, sizeof(float) * p->rec.n * 9 * p->nt_total * nshot));
@@ -812,22 +848,22 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   make_tiles(p);
   if (p->free_top) {
     const size_t nij = (size_t)p->ni * p->nj * nshot;
-    p->d_pg = dmalloc<float>(15 * nij, B);
-    p->d_dis = dmalloc<float>(3 * nij, B);
+    p->d_pg = dmalloc<float>(15 * nij, B, p->stream);
+    p->d_dis = dmalloc<float>(3 * nij, B, p->stream);
     CK(cudaMemset(p->d_pg, 0, sizeof(float) * 15 * nij));
     CK(cudaMemset(p->d_dis, 0, sizeof(float) * 3 * nij));
   }
-  p->d_it = dmalloc<int>(1, B);
-  p->d_flag = dmalloc<int>(1, B);
+  p->d_it = dmalloc<int>(1, B, p->stream);
+  p->d_flag = dmalloc<int>(1, B, p->stream);
   CK(cudaMemset(p->d_it, 0, sizeof(int)));
   CK(cudaMemset(p->d_flag, 0, sizeof(int)));
   if (p->wave16) {
-    p->d_wsc = dmalloc<float>(18 * (size_t)nshot, B);
-    p->d_amax = dmalloc<unsigned int>(2 * (size_t)nshot, B);
+    p->d_wsc = dmalloc<float>(18 * (size_t)nshot, B, p->stream);
+    p->d_amax = dmalloc<unsigned int>(2 * (size_t)nshot, B, p->stream);
     CK(cudaMemset(p->d_wsc, 0, sizeof(float) * 18 * nshot));
     CK(cudaMemset(p->d_amax, 0, sizeof(unsigned int) * 2 * nshot));  // the wavefield starts at zero
     std::vector<float> sb = source_bounds(p);
-    p->d_srcb = dmalloc<float>(sb.size(), B);
+    p->d_srcb = dmalloc<float>(sb.size(), B, p->stream);
     CK(cudaMemcpy(p->d_srcb, sb.data(), sb.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
   CK(cudaDeviceSynchronize());
@@ -865,12 +901,12 @@ void make_tiles(cgfd_problem *p) {
         }
         (touch ? pm : in).push_back(make_int4(bx, by, z.first, z.second));
       }
-  cudaFree(p->d_tiles);
+  dfree(p->d_tiles, p->stream);
   p->d_tiles = nullptr;
   std::vector<int4> all(in);
   all.insert(all.end(), pm.begin(), pm.end());
   size_t acc = 0;
-  p->d_tiles = dmalloc<int4>(std::max<size_t>(all.size(), 1), acc);
+  p->d_tiles = dmalloc<int4>(std::max<size_t>(all.size(), 1), acc, p->stream);
   if (!all.empty()) CK(cudaMemcpy(p->d_tiles, all.data(), all.size() * sizeof(int4), cudaMemcpyHostToDevice));
   p->tiles.interior = p->d_tiles;
   p->tiles.ninterior = (int)in.size();
@@ -1063,14 +1099,14 @@ int cgfd_get_wavefield_shot(cgfd_problem *p, int shot, float *out) {
     CK(cudaSetDevice(p->device));
     cgfd::RefGrid g(p->ni, p->nj, p->nk);
     size_t acc = 0;
-    float *tmp = dmalloc<float>(g.siz_icmp, acc);
+    float *tmp = dmalloc<float>(g.siz_icmp, acc, p->stream);
     const float *pre = p->wbuf[p->it & 1] + (size_t)shot * 9 * p->sf;
     for (int c = 0; c < 9; c++) {
       cgfd::launch_repack_out(pre + (size_t)c * p->sf, tmp, p->ni, p->nj, p->nk, p->sx, p->sz, p->off0, p->stream);
       CK(cudaMemcpyAsync(out + (size_t)c * g.siz_icmp, tmp, g.siz_icmp * sizeof(float), cudaMemcpyDeviceToHost, p->stream));
     }
     CK(cudaStreamSynchronize(p->stream));
-    cudaFree(tmp);
+    dfree(tmp, p->stream);
   });
 }
 
@@ -1093,11 +1129,11 @@ int cgfd_get_wavefield_box(cgfd_problem *p, int shot, const int *start, const in
     const size_t cnt = (size_t)9 * count[0] * count[1] * count[2];
     if (cnt > p->box_cap) {
       CK(cudaStreamSynchronize(p->stream));
-      cudaFree(p->d_box);
+      dfree(p->d_box, p->stream);
       p->d_box = nullptr;
       p->box_cap = 0;
       size_t acc = 0;
-      p->d_box = dmalloc<float>(cnt, acc);
+      p->d_box = dmalloc<float>(cnt, acc, p->stream);
       p->box_cap = cnt;
     }
     const float *pre = p->wbuf[p->it & 1] + (size_t)shot * 9 * p->sf;
@@ -1206,7 +1242,7 @@ int cgfd_set_wavefield_shot(cgfd_problem *p, int shot, const float *in) {
     CK(cudaSetDevice(p->device));
     cgfd::RefGrid g(p->ni, p->nj, p->nk);
     size_t acc = 0;
-    float *tmp = dmalloc<float>(g.siz_icmp, acc);
+    float *tmp = dmalloc<float>(g.siz_icmp, acc, p->stream);
     float *pre = p->wbuf[p->it & 1] + (size_t)shot * 9 * p->sf;
     {
       PinnedStager &ps = PinnedStager::for_device(p->device);
@@ -1215,7 +1251,7 @@ int cgfd_set_wavefield_shot(cgfd_problem *p, int shot, const float *in) {
     }
     refresh_wave_max(p);
     CK(cudaStreamSynchronize(p->stream));
-    cudaFree(tmp);
+    dfree(tmp, p->stream);
   });
 }
 
