@@ -36,3 +36,19 @@ def test_repeated_runs_are_identical(medium, precision):
     assert np.abs(out[0][1]).max() > 0
     assert np.array_equal(out[0][0], out[1][0]), "final wavefields differ between identical runs"
     assert np.array_equal(out[0][1], out[1][1]), "seismograms differ between identical runs"
+
+
+def test_repeated_batched_runs_are_identical():
+    """A batch of 3 shots (shot-fastest block order, coefficient tiles shared through L2)."""
+    p = _problem("vti")
+    rng = np.random.default_rng(5)
+    shots = [synth.dc_sources(p.coord, p.ni, p.nj, 1, rng, depth_range=(800.0, 2000.0), fc_range=(3.0, 4.0),
+                              stf_length=p.nt_total * p.dt) for _ in range(3)]
+    out = []
+    for _ in range(2):
+        s = Simulation(p, shots=shots)
+        s.run()
+        out.append(s.seismograms())
+        s.close()
+    assert np.abs(out[0]).max() > 0
+    assert np.array_equal(out[0], out[1]), "batched seismograms differ between identical runs"
