@@ -15,7 +15,6 @@ reference's time loop (the reference has no CPU solver of its own) on the host c
 """
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -311,79 +310,86 @@ def serving_bench(local, nreq=24, mean_gap_s=0.02, seed=11):
             "wall_s": wall, "offered_gcell_stages": work / 1e9, "hbm_peak_gb": st["hbm_peak"] / 1e9}
 
 
-def cpu_baseline(args, threads):
-    """The oracle (FP32 CPU restatement, OpenMP on all host cores) on a sample of the workload."""
+def cpu_baseline(args, threads, p=None, steps=3):
+    """The oracle (FP32 CPU restatement, OpenMP on all host cores) on the full workload grid:
+    one warm-up time step, then `steps` timed time steps (each a full 4-stage step of every
+    cell, PML, free surface, source and stations), i.e. the same sample as each step of the
+    --impl reference arm."""
     from oracle.oracle import Oracle
-    ni, nj, nk, *_ = WORKLOADS[args.workload]
-    if args.grid:
-        ni, nj, nk = args.grid
-    nk_s = max(16, min(nk, 24))
-    p = build_problem(args, nk_override=nk_s)
+    if p is None:
+        p = build_problem(args)
     o = Oracle(p)
     o.run(1)  # warm-up
     t = time.perf_counter()
-    nst = 1
-    o.run(nst)
+    o.run(steps)
     dt = time.perf_counter() - t
-    cells = p.ni * p.nj * p.nk * 4 * nst
+    o.close()
+    cells = p.ni * p.nj * p.nk * 4 * steps
     return {"value": cells / dt / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{nst} time step (4 RK stages) of the {p.ni}x{p.nj}x{p.nk} slab of the workload "
-                      f"(same PML/free surface/source/stations), after 1 warm-up step; {dt:.2f} s"}
+            "sample": f"{steps} full time steps (4 RK stages each) of the {p.ni}x{p.nj}x{p.nk} workload grid after "
+                      f"1 warm-up step, {dt:.1f} s; the same per-step sample as --impl reference"}
 
 
-def _oracle_rate(args, ni, nj, nk):
-    """cell-stages/s of the oracle on a small probe grid (1 warm-up + 1 timed step)."""
-    from oracle.oracle import Oracle
-    a = argparse.Namespace(**vars(args))
-    a.grid = [ni, nj, nk]
-    p = build_problem(a)
-    o = Oracle(p)
-    o.run(1)
-    t = time.perf_counter()
-    o.run(1)
-    return p.ni * p.nj * p.nk * 4 / (time.perf_counter() - t)
+def reference_gpu_kernels(p, steps):
+    """The reference's own GPU solver code (oracle/_ref/ref_harness: its unmodified per-stage
+    kernels, RK-combine launches and per-station sampling, built for sm_100a) timed on the same
+    grid and step count on this B200; None when the harness was not built."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import tempfile
+    from golden import ref_io
+    if not os.path.exists(ref_io.HARNESS):
+        return None
+    with tempfile.TemporaryDirectory() as d:
+        r = ref_io.run(p, d, steps, timeout=1800)
+    rate = r["cell_stages"] / (r["loop_ms"] * 1e-3) / 1e9
+    return {"value": rate, "unit": UNIT, "steps": steps, "ms_per_step": r["loop_ms"] / steps,
+            "grid": [p.ni, p.nj, p.nk],
+            "note": "reference time loop (sv_curv_col_el_iso_onestage + wav_update + io_recv_keep per step) on the "
+                    "same B200, same grid, medium, PML, source and stations; device-synchronised loop time"}
 
 
 def run_reference(args):
-    """--impl reference: the CPU restatement of the reference's time loop on host cores."""
+    """--impl reference: the CPU restatement of the reference's time loop on host cores (the
+    reference has no CPU solver of its own), on the full workload grid: W warm-up time steps,
+    then K timed full time steps. If K + W full steps would take more than about four minutes
+    on this host, each step is a bounded z-slab sample of the workload instead (reported)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
     threads = len(os.sched_getaffinity(0))
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     from oracle.oracle import Oracle
-    ni, nj, nk, *_ = WORKLOADS[args.workload]
-    if args.grid:
-        ni, nj, nk = args.grid
-    # bounded sample: a slab of the workload sized from a probe so that warm-up + steps
-    # finish in about two minutes on this host
-    rate = _oracle_rate(args, 64, 64, 16)
-    budget = 120.0
-    cells_per_step = rate * budget / max(1, args.steps + args.warmup) / 4.0
-    nk_s = max(16, min(nk, 24))
-    side = int(math.sqrt(max(cells_per_step / nk_s, 1.0)))
-    ni_s = max(48, min(ni, side))
-    nj_s = max(48, min(nj, side))
-    args_s = argparse.Namespace(**vars(args))
-    args_s.grid = [ni_s, nj_s, nk_s]
-    p = build_problem(args_s)
+    p = build_problem(args)
     o = Oracle(p)
-    sample_steps = 1
-    for _ in range(args.warmup):
+    t = time.perf_counter()
+    o.run(1)  # probe step (also the first warm-up step)
+    t_step = time.perf_counter() - t
+    same = (args.steps + args.warmup) * t_step <= 240.0
+    if not same:
+        o.close()
+        nk_s = max(8, min(p.nk, int(p.nk * 240.0 / ((args.steps + args.warmup) * t_step))))
+        p = build_problem(args, nk_override=nk_s)
+        o = Oracle(p)
+        o.run(1)
+    for _ in range(max(0, args.warmup - 1)):
         o.run(1)
     t = time.perf_counter()
     for _ in range(args.steps):
-        o.run(sample_steps)
+        o.run(1)
     el = time.perf_counter() - t
-    cells = p.ni * p.nj * p.nk * 4 * sample_steps * args.steps
+    o.close()
+    cells = p.ni * p.nj * p.nk * 4 * args.steps
     v = cells / el / 1e9
+    sample = (f"each step = one full time step (4 RK stages) of the {p.ni}x{p.nj}x{p.nk} workload grid by the oracle"
+              if same else f"each step = one time step of a {p.ni}x{p.nj}x{p.nk} z-slab of the workload (full grid "
+                           f"would exceed the time bound: {t_step:.1f} s per step)")
     out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": args.workload, "sample_grid": [p.ni, p.nj, p.nk], "medium": "elastic_iso"},
-           "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                            "sample": f"each step = {sample_steps} time step(s) of the {p.ni}x{p.nj}x{p.nk} slab of "
-                                      "the workload by the oracle (the reference has no CPU solver)"},
+           "config": {"workload": f"{WORKLOADS[args.workload][0]}x{WORKLOADS[args.workload][1]}x"
+                                  f"{WORKLOADS[args.workload][2]}", "sample_grid": [p.ni, p.nj, p.nk],
+                      "medium": "elastic_iso", "same_grid_as_b200_arm": same},
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return 0
@@ -514,12 +520,17 @@ def main():
             media = {"error": str(ex)}
 
     cpu = None
+    ref_gpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = len(os.sched_getaffinity(0))
         try:
-            cpu = cpu_baseline(args, threads)
+            cpu = cpu_baseline(args, threads, p)
         except Exception as ex:  # report, do not fail the GPU measurement
             cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": "port", "sample": f"failed: {ex}"}
+        try:
+            ref_gpu = reference_gpu_kernels(p, args.steps)
+        except Exception as ex:  # report, do not fail the GPU measurement
+            ref_gpu = {"error": str(ex)}
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -529,7 +540,8 @@ def main():
                           "pml_layers": 20, "free_surface": "timg", "sources": 1, "stations": 400,
                           "dt": p.dt, "precision": "fp32", "parallelism": f"replicas x{world}",
                           "l2": f"inputs larger than L2 (wavefield 4 levels x 9 x {(p.ni + 6) * (p.nj + 6) * (p.nk + 6) / 1e6:.1f}M floats)"},
-               "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+               "roofline": roof, "cpu_baseline": cpu, "reference_gpu_kernels": ref_gpu, "e2e": e2e,
+               "gpu_launches": launches,
                "clocks": clocks, "batched_mixed": batched, "media": media, "serving": serving}
         print(json.dumps(out), flush=True)
     if dist:

@@ -26,6 +26,7 @@
 #include "cgfd_dev.cuh"
 #include "cgfd_launch.h"
 #include "cgfd_setup.h"
+#include "cgfd_tma.cuh"
 
 namespace {
 
@@ -614,6 +615,7 @@ std::vector<float> source_bounds(const cgfd_problem *p) {
 }
 
 void make_tiles(cgfd_problem *p);
+float *noalloc_scratch(int device);
 
 // sources given by physical coordinates: located on the current device (nullptr otherwise)
 const cgfd::Located *locate_sources(const cgfd_problem_desc *d, cgfd::Located &out) {
@@ -639,6 +641,9 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   p->device = d->device;
   CK(cudaSetDevice(p->device));
   keep_pool_memory(p->device);
+  // the no-allocation snapshot path's static scratch is loaded here, with the problem's own
+  // memory, so that cgfd_get_wavefield_shot_noalloc itself never takes device memory
+  noalloc_scratch(p->device);
   CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
@@ -1013,7 +1018,10 @@ int cgfd_synchronize(cgfd_problem *p) {
     p->collect_timing();
     int flag = 0;
     CK(cudaMemcpy(&flag, p->d_flag, sizeof(int), cudaMemcpyDeviceToHost));
-    if (flag & 2) throw cgfd::Error(CGFD_ERR_CUDA, "a TMA pipeline wait timed out in the stage kernel");
+    if (flag & cgfd::kErrPipelineTimeout)
+      throw cgfd::Error(CGFD_ERR_CUDA, "a TMA pipeline wait timed out in the stage kernel");
+    if (flag & cgfd::kErrWaveNonfinite)
+      throw cgfd::Error(CGFD_ERR_NONFINITE, "non-finite value in the wavefield (RK combine of stage 3)");
     if (flag) throw cgfd::Error(CGFD_ERR_NONFINITE, "non-finite value sampled at a station");
   });
 }
@@ -1127,13 +1135,13 @@ int cgfd_get_wavefield_box(cgfd_problem *p, int shot, const int *start, const in
   return guarded([&] {
     CK(cudaSetDevice(p->device));
     const size_t cnt = (size_t)9 * count[0] * count[1] * count[2];
-    if (cnt > p->box_cap) {
+    if (cnt > p->box_cap) {  // the staging buffer stays with the problem and counts in its bytes
       CK(cudaStreamSynchronize(p->stream));
       dfree(p->d_box, p->stream);
       p->d_box = nullptr;
+      p->bytes -= p->box_cap * sizeof(float);
       p->box_cap = 0;
-      size_t acc = 0;
-      p->d_box = dmalloc<float>(cnt, acc, p->stream);
+      p->d_box = dmalloc<float>(cnt, p->bytes, p->stream);
       p->box_cap = cnt;
     }
     const float *pre = p->wbuf[p->it & 1] + (size_t)shot * 9 * p->sf;
@@ -1164,12 +1172,13 @@ int cgfd_get_peak_motion(cgfd_problem *p, int shot, float *out) {
 }  // extern "C"
 
 // ---- wavefield read-back without device allocation -------------------------------------
-// cgfd_get_wavefield_shot stages the whole wavefield in a temporary device buffer
-// (cudaMalloc + cudaFree). Some callers cannot afford that: a serving process that keeps the
-// device filled to its memory budget with resident problems (the temporary may not fit, and
-// failing a snapshot for lack of memory is not acceptable), and a caller reading a snapshot
-// while other problems run on other streams (cudaFree waits for the whole device). This
-// variant stages through one fixed static device array instead, a few z planes at a time.
+// cgfd_get_wavefield_shot stages one wavefield component in a temporary device buffer taken
+// from the stream-ordered pool ((ni+6)(nj+6)(nk+6) floats for the call's duration). Some
+// callers cannot afford that: a serving process that keeps the device filled to its memory
+// budget with resident problems, where the temporary may not fit and a snapshot must not fail
+// for lack of memory. This variant stages through one fixed static device array instead, a
+// few z planes at a time. The array (and the repack kernel's code) is loaded when a problem
+// is created on the device, so the entry point itself takes no device memory.
 namespace {
 
 constexpr size_t kNoAllocScratchFloats = (size_t)1 << 20;  // 4 MiB: one chunk of reference planes
@@ -1191,7 +1200,9 @@ __global__ void k_repack_out_planes(const float *__restrict__ src, float *__rest
   }
 }
 
-// Device address of the scratch array on `device` (current): looked up once per device.
+// Device address of the scratch array on `device` (current): looked up once per device, by
+// the first problem created there. The lookup loads this file's device module (the 4 MiB array
+// and the repack kernel, whose code cudaFuncGetAttributes loads as well under lazy loading).
 float *noalloc_scratch(int device) {
   if (device < 0 || device >= kNoAllocMaxDevices) throw cgfd::Error(CGFD_ERR_INVALID, "device ordinal out of range");
   std::lock_guard<std::mutex> g(g_noalloc_mu);
@@ -1200,6 +1211,10 @@ float *noalloc_scratch(int device) {
     cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch);
     if (e != cudaSuccess || !ptr)
       throw cgfd::Error(CGFD_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, k_repack_out_planes);
+    if (e != cudaSuccess)
+      throw cgfd::Error(CGFD_ERR_CUDA, std::string("cudaFuncGetAttributes(repack): ") + cudaGetErrorString(e));
     g_noalloc_ptr[device] = ptr;
   }
   return g_noalloc_ptr[device];

@@ -176,6 +176,7 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
   const int wc = (ty + LY) * S::WX + tx + S::XO;  // centre of this thread in a wave slot (per field)
   mbar_wait(&bar[0], 0, p.err);
   float vmax = 0.f, smax = 0.f;  // FP16 mode, stage 3: max |w_end| of this thread
+  bool bad = false;              // stage 3: a new solution value is NaN/Inf
 
   const int cell = ty * TX + tx;
   for (int m = 0; m < n; m++) {
@@ -289,6 +290,7 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
         for (int f = 0; f < 9; f++) {
           const float e = EN[f * S::CELLS] + cb * h[f];
           endw[f * sf + id] = e;
+          bad |= nonfinite(e);
           if constexpr (WP == 2) {
             if (f < 3) vmax = fmaxf(vmax, fabsf(e));
             else smax = fmaxf(smax, fabsf(e));
@@ -307,6 +309,7 @@ __global__ void __launch_bounds__(TX *TYT, BlocksPerSm<MED, PML>::value)
     fence_proxy_async_smem();
     __syncthreads();
   }
+  if (bad) atomicOr(p.err, kErrWaveNonfinite);  // blow-up sentinel (drv_rk_curv_col.cu:507-510)
   if constexpr (WP == 2) {
     if (stage == 3) {  // the next step's FP16 scale
       for (int o = 16; o; o >>= 1) {

@@ -80,7 +80,7 @@ struct StageP {
   int nbulk;              // planes [0, nbulk) belong to the bulk kernel
   int nface;
   FaceP face[6];
-  int *err;               // device error word (bit 1: pipeline wait timed out)
+  int *err;               // device error word: kErrStationNonfinite, kErrPipelineTimeout, kErrWaveNonfinite
   int nshot;              // wavefields sharing this grid (batched sources); 1 = plain
   // FP16 stage levels, per shot s: wsc[18s + 0..8] scale (value = scale * stored),
   // wsc[18s + 9..17] its inverse, fixed for one time step; amax[2s + 0..1] collects max |w|
@@ -264,11 +264,20 @@ struct CellAcc {
   }
 };
 
+// Bits of the problem's device error word (reported by cgfd_synchronize).
+constexpr int kErrStationNonfinite = 1;  // a station sample is NaN/Inf
+constexpr int kErrWaveNonfinite = 4;     // the RK combine produced a NaN/Inf solution value
+
+// true when v is NaN or +-Inf (a NaN compares false)
+__device__ __forceinline__ bool nonfinite(float v) { return !(fabsf(v) <= 3.402823466e38f); }
+
 // RK combine of 9 values at one point (wav_update / wav_update_end, wav_t.cu:362-378).
-// cur_c: the stage input at the point (== pre at stage 0).
+// cur_c: the stage input at the point (== pre at stage 0). err (may be null): at stage 3,
+// a non-finite new solution value sets kErrWaveNonfinite there -- the blow-up sentinel the
+// reference leaves stubbed (drv_rk_curv_col.cu:507-510, wav_check_value wav_t.cu:260-279).
 __device__ __forceinline__ void rk_store(int stage, float ca, float cb, long long comp_stride, long long idx,
                                          const float cur_c[9], const float h[9], const float *pre,
-                                         float *tmp_out, float *end) {
+                                         float *tmp_out, float *end, int *err = nullptr) {
   if (stage == 0) {
 #pragma unroll
     for (int c = 0; c < 9; c++) {
@@ -289,10 +298,16 @@ __device__ __forceinline__ void rk_store(int stage, float ca, float cb, long lon
     }
   } else {
     float e[9];
+    bool bad = false;
 #pragma unroll
     for (int c = 0; c < 9; c++) e[c] = end[c * comp_stride + idx];
 #pragma unroll
-    for (int c = 0; c < 9; c++) end[c * comp_stride + idx] = e[c] + cb * h[c];
+    for (int c = 0; c < 9; c++) {
+      const float v = e[c] + cb * h[c];
+      end[c * comp_stride + idx] = v;
+      bad |= nonfinite(v);
+    }
+    if (err && bad) atomicOr(err, kErrWaveNonfinite);
   }
 }
 

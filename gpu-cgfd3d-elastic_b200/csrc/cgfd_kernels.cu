@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(TX *TY, 2) k_stage_bulk(const __grid_constant_
       float cc[9];
 #pragma unroll
       for (int f = 0; f < 9; f++) cc[f] = q[f][LZ];
-      rk_store(p.stage, p.ca, p.cb, sf, id, cc, h, p.pre, p.tmp_out, p.end);
+      rk_store(p.stage, p.ca, p.cb, sf, id, cc, h, p.pre, p.tmp_out, p.end, p.err);
     }
 #pragma unroll
     for (int f = 0; f < 9; f++)
@@ -338,7 +338,8 @@ __global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant_
       float cc[9];
 #pragma unroll
       for (int f = 0; f < 9; f++) cc[f] = cur(f, id);
-      rk_store(p.stage, p.ca, p.cb, sf, id, cc, h, p.pre + woff, p.tmp_out ? p.tmp_out + woff : nullptr, p.end + woff);
+      rk_store(p.stage, p.ca, p.cb, sf, id, cc, h, p.pre + woff, p.tmp_out ? p.tmp_out + woff : nullptr, p.end + woff,
+               p.err);
     } else {
       // FP16 stage levels: the RK combine of rk_store with the stage output scaled to FP16
       TT *tout = reinterpret_cast<TT *>(p.tmp_out) + woff;
@@ -359,13 +360,16 @@ __global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant_
         }
       } else {
         float vmax = 0.f, smax = 0.f;
+        bool bad = false;
 #pragma unroll
         for (int f = 0; f < 9; f++) {
           const float e = endw[f * sf + id] + p.cb * h[f];
           endw[f * sf + id] = e;
+          bad |= nonfinite(e);
           if (f < 3) vmax = fmaxf(vmax, fabsf(e));
           else smax = fmaxf(smax, fabsf(e));
         }
+        if (bad) atomicOr(p.err, kErrWaveNonfinite);
         atomic_max_abs(&p.amax[2 * shot + 0], vmax);
         atomic_max_abs(&p.amax[2 * shot + 1], smax);
       }
@@ -415,7 +419,7 @@ __global__ void k_recv(const __grid_constant__ RecvP r) {
     float w = r.w8[sidx * 8 + qn];
     if (w != 0.f) v += w * __ldg(pre + c * r.sf + r.idx8[sidx * 8 + qn]);
   }
-  if (!isfinite(v)) atomicOr(r.d_flag, 1);
+  if (nonfinite(v)) atomicOr(r.d_flag, kErrStationNonfinite);
   r.seis[(((long long)shot * r.nsta + sidx) * 9 + c) * r.nt_total + it] = v;
 }
 

@@ -226,19 +226,23 @@ int cgfd_set_wavefield_shot(cgfd_problem *p, int shot, const float *in);
 /*
  * Same result as cgfd_get_wavefield_shot, but allocates no device memory: the repack goes
  * through one static 4 MiB device array (2^20 floats) shared by every call, a chunk of
- * reference-layout z planes at a time. For callers that cannot allocate: a server holding the
- * device at its memory budget, or a snapshot taken while other streams keep running (the
- * temporary buffer's cudaFree would wait for the whole device). Limit: one plane,
- * (ni+6)*(nj+6) floats, must fit the array; larger grids get CGFD_ERR_INVALID. Nothing in the
- * array needs to start at zero (each chunk is fully written before it is copied). Calls that
- * overlap on one device (other threads, other problems) race on the shared array and must
- * be serialised by the caller. The first call on a device looks up the array's address there
- * and should come before any stream capture starts.
+ * reference-layout z planes at a time. For callers that cannot allocate: a server that holds
+ * the device at its memory budget with resident problems, where the temporary buffer of
+ * cgfd_get_wavefield_shot (one full wavefield component, (ni+6)(nj+6)(nk+6) floats, from the
+ * device's memory pool) may not fit and a snapshot must not fail for lack of memory.
+ * Limit: one plane, (ni+6)*(nj+6) floats, must fit the array; larger grids get
+ * CGFD_ERR_INVALID. The array and its repack kernel are loaded on a device when the first
+ * problem is created there (cgfd_problem_create / cgfd_batch_create look up the array's
+ * address, with that device current), and stay until the process exits; the call itself
+ * takes no device memory. Nothing in the array needs to start at zero (each chunk is fully
+ * written before it is copied). Calls that overlap on one device (other threads, other
+ * problems) race on the shared array and must be serialised by the caller.
  * No counterpart in the reference.
  */
 int cgfd_get_wavefield_shot_noalloc(cgfd_problem *p, int shot, float *out);
 
-/* Device bytes held by the problem. */
+/* Device bytes held by the problem (including the staging buffer of cgfd_get_wavefield_box
+   once it has been used: it grows to the largest box asked for and stays with the problem). */
 size_t cgfd_device_bytes(const cgfd_problem *p);
 
 /*
@@ -261,7 +265,11 @@ void *cgfd_stream(cgfd_problem *p);
 
 /*
  * Enqueue n time steps on the problem's stream without synchronising (benchmarks and
- * overlapping host work). cgfd_synchronize() waits and reports device-side errors.
+ * overlapping host work). cgfd_synchronize() waits and reports device-side errors:
+ * CGFD_ERR_NONFINITE when a step produced a NaN/Inf solution value anywhere in the grid
+ * (checked by the RK combine of the last stage of every step; the reference's check,
+ * drv_rk_curv_col.cu:507-510 / wav_check_value wav_t.cu:260-279, is stubbed out) or sampled
+ * one at a station; CGFD_ERR_CUDA when a stage kernel's pipeline wait timed out.
  */
 int cgfd_enqueue_steps(cgfd_problem *p, int nsteps);
 int cgfd_synchronize(cgfd_problem *p);

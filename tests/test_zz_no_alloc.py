@@ -53,6 +53,42 @@ def test_noalloc_chunks_over_many_planes():
     assert np.array_equal(out, ref)
 
 
+def _device_memory(device=0):
+    """(pool reserved bytes, pool used bytes, free device bytes) of `device` through the CUDA
+    driver API: the default memory pool the library allocates from, and cuMemGetInfo of the
+    primary context the library made current on this thread."""
+    cu = C.CDLL("libcuda.so.1")
+    dev = C.c_int()
+    assert cu.cuDeviceGet(C.byref(dev), device) == 0
+    pool = C.c_void_p()
+    assert cu.cuDeviceGetDefaultMemPool(C.byref(pool), dev) == 0
+    reserved, used = C.c_uint64(), C.c_uint64()
+    assert cu.cuMemPoolGetAttribute(pool, 5, C.byref(reserved)) == 0  # CU_MEMPOOL_ATTR_RESERVED_MEM_CURRENT
+    assert cu.cuMemPoolGetAttribute(pool, 7, C.byref(used)) == 0      # CU_MEMPOOL_ATTR_USED_MEM_CURRENT
+    free, total = C.c_size_t(), C.c_size_t()
+    assert cu.cuMemGetInfo_v2(C.byref(free), C.byref(total)) == 0
+    return reserved.value, used.value, free.value
+
+
+def test_noalloc_takes_no_device_memory():
+    """The property the entry point exists for: with a problem resident, further calls change
+    neither the memory pool's reserved / used bytes nor the device's free memory (the plain
+    cgfd_get_wavefield_shot takes a wavefield component from the pool for its duration)."""
+    p = small_problem("iso", ni=120, nj=100, nk=50, nsteps=6, npml=4, sta_grid=None, seed=5)
+    sim = Simulation(p)
+    sim.run(4)
+    ref = sim.wavefield()
+    out = np.zeros_like(ref)
+    fn = _noalloc()
+    assert fn(sim.h, 0, out.ctypes.data) == 0  # first call after create
+    for _ in range(2):
+        before = _device_memory(p.device)
+        assert fn(sim.h, 0, out.ctypes.data) == 0
+        after = _device_memory(p.device)
+        assert after == before, (before, after)
+        assert np.array_equal(out, ref)
+
+
 def test_noalloc_rejects_bad_arguments():
     p = small_problem("iso", nsteps=4, nsrc=0, sta_grid=None)
     sim = Simulation(p)
