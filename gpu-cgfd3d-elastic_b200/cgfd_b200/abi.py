@@ -21,6 +21,7 @@ CGFD_PREC_BF16_COEF = 1
 CGFD_PREC_FP16_COEF = 2
 CGFD_PREC_U16_COEF = 3
 CGFD_PREC_FP16_WAVE = 4
+CGFD_PREC_FP64 = 5
 # wavelet names of src_t.cu:873-903 -> ids
 WAVELETS = {"ricker": 0, "gaussian": 1, "ricker_deriv": 2, "gaussian_deriv": 3, "klauder": 4}
 

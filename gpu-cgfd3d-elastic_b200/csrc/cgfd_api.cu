@@ -126,12 +126,17 @@ struct cgfd_problem {
   cudaStream_t stream = nullptr;
   int ni = 0, nj = 0, nk = 0, med = 0, ncoef = 0, nt_total = 0, free_top = 0;
   int nshot = 1;  // wavefields sharing the grid, coefficients and stations
+  // FP64 build (CGFD_PREC_FP64): every real-typed device array below holds doubles (esz 8)
+  int fp64 = 0;
+  size_t esz = 4;
   float dt = 0.f;
   long long sx = 0, sz = 0, sf = 0, off0 = 0;
   size_t bytes = 0;
   int nzc = 16;
 
   float *wbuf[4] = {nullptr, nullptr, nullptr, nullptr};  // [0],[1]: pre/end by parity; [2],[3]: tmpA/tmpB
+  // (real-typed arrays -- wbuf, coef, jac, matx/maty, PML A/B/D/aux, d_dis -- are held as float*
+  // and hold doubles in the FP64 build; rptr() gives the typed, element-offset pointer)
   float *coef = nullptr, *jac = nullptr, *matx = nullptr, *maty = nullptr;
   // 16-bit coefficient storage (replaces `coef` when coef_type != COEF_F32):
   // value = cscale[field] * stored + coffset[field]
@@ -231,27 +236,40 @@ struct cgfd_problem {
 
   long long didx(int i, int j, int k) const { return off0 + (long long)k * sz + (long long)j * sx + i; }
 
-  cgfd::StageP stage_params(int step, int stage) const {
-    cgfd::StageP p;
+  // element `off` of a real-typed array held as float* (doubles in the FP64 build)
+  template <typename R>
+  static R *rptr(const float *base, size_t off = 0) {
+    return base ? reinterpret_cast<R *>(const_cast<float *>(base)) + off : nullptr;
+  }
+  void *rvoid(const float *base, size_t off) const {
+    return base ? (void *)((char *)base + off * esz) : nullptr;
+  }
+
+  cgfd::StageP stage_params(int step, int stage) const { return stage_params_t<float>(step, stage); }
+
+  template <typename R>
+  cgfd::StagePT<R> stage_params_t(int step, int stage) const {
+    cgfd::StagePT<R> p;
     memset(&p, 0, sizeof(p));
     p.ni = ni; p.nj = nj; p.nk = nk;
     p.stage = stage;
     int ipair = step % 8;
     for (int a = 0; a < 3; a++) p.dir[a] = (kPairFlags[ipair][a] + stage) % 2;
     p.sx = sx; p.sz = sz; p.sf = sf; p.off0 = off0;
-    float *pre = wbuf[step & 1], *end = wbuf[(step + 1) & 1];
-    float *tA = wbuf[2], *tB = wbuf[3];
-    const float *curs[4] = {pre, tA, tB, tA};
-    float *outs[4] = {tA, tB, tA, nullptr};
+    R *pre = rptr<R>(wbuf[step & 1]), *end = rptr<R>(wbuf[(step + 1) & 1]);
+    R *tA = rptr<R>(wbuf[2]), *tB = rptr<R>(wbuf[3]);
+    const R *curs[4] = {pre, tA, tB, tA};
+    R *outs[4] = {tA, tB, tA, nullptr};
     p.cur = curs[stage];
     p.pre = pre;
     p.tmp_out = outs[stage];
     p.end = end;
-    p.ca = stage < 3 ? kRkA[stage] * dt : 0.f;
-    p.cb = kRkB[stage] * dt;
+    // RK weights x dt: float as in the reference; in double from the same float constants
+    p.ca = stage < 3 ? R(kRkA[stage]) * R(dt) : R(0);
+    p.cb = R(kRkB[stage]) * R(dt);
     p.coef = coef_type == cgfd::COEF_F32 ? (const void *)coef : (const void *)coef16;
     for (int c = 0; c < 32; c++) { p.cscale[c] = cscale[c]; p.coffset[c] = coffset[c]; }
-    p.jac = jac; p.matx = matx; p.maty = maty;
+    p.jac = rptr<R>(jac); p.matx = rptr<R>(matx); p.maty = rptr<R>(maty);
     p.free_top = free_top;
     p.nbulk = free_top ? nk - cgfd::NSURF : nk;
     p.err = d_flag;
@@ -260,17 +278,17 @@ struct cgfd_problem {
     p.amax = d_amax;
     p.nface = 0;
     for (const Face &f : faces) {
-      cgfd::FaceP &o = p.face[p.nface++];
+      cgfd::FacePT<R> &o = p.face[p.nface++];
       o.enable = 1;
       o.axis = f.h.axis;
       for (int b = 0; b < 3; b++) { o.lo[b] = f.h.lo[b]; o.hi[b] = f.h.hi[b]; }
       o.nx = f.h.hi[0] - f.h.lo[0] + 1;
       o.ny = f.h.hi[1] - f.h.lo[1] + 1;
       o.n = f.n;
-      o.A = f.A; o.B = f.B; o.D = f.D;
+      o.A = rptr<R>(f.A); o.B = rptr<R>(f.B); o.D = rptr<R>(f.D);
       const size_t L = (size_t)nshot * 9 * f.n;
-      float *apre = f.aux + (size_t)(step & 1) * L, *aend = f.aux + (size_t)((step + 1) & 1) * L;
-      float *atmp = f.aux + (size_t)2 * L;
+      R *apre = rptr<R>(f.aux, (size_t)(step & 1) * L), *aend = rptr<R>(f.aux, (size_t)((step + 1) & 1) * L);
+      R *atmp = rptr<R>(f.aux, (size_t)2 * L);
       o.aux_cur = stage == 0 ? apre : atmp;
       o.aux_pre = apre;
       o.aux_tmp = atmp;
@@ -279,7 +297,47 @@ struct cgfd_problem {
     return p;
   }
 
+  // One time step of the FP64 build: the same kernels instantiated in double (direct-load bulk
+  // kernel, surface slab, sources, stations, peak motion), launched in the same order.
+  int enqueue_step64(int step) {
+    cudaStream_t st = stream;
+    int n = 0;
+    if (rec.n > 0) {
+      cgfd::RecvPT<double> r;
+      r.nsta = rec.n; r.nshot = nshot; r.nt_total = nt_total; r.idx8 = d_idx8; r.w8 = d_w8;
+      r.pre = rptr<double>(wbuf[step & 1]); r.sf = sf; r.seis = d_seis; r.d_it = d_it; r.d_flag = d_flag;
+      n += timed(6, [&] { return cgfd::launch_recv(r, st); });
+    }
+    for (int s = 0; s < 4; s++) {
+      const cgfd::StagePT<double> p = stage_params_t<double>(step, s);
+      n += timed(s, [&] { return cgfd::launch_stage_bulk(med, p, nzc, st); });
+      n += timed(4, [&] { return cgfd::launch_stage_surface64(med, p, st); });
+      if (src.nsrc > 0) {
+        cgfd::SrcPT<double> q;
+        memset(&q, 0, sizeof(q));
+        q.nsrc = src.nsrc; q.max_ext = src.max_ext; q.max_nt = src.max_nt;
+        q.force = src.force; q.moment = src.moment; q.stage = s;
+        q.ca = p.ca; q.cb = p.cb;
+        q.it_begin = d_it_begin; q.ext_num = d_ext_num; q.ext_idx = d_ext_idx;
+        q.ext_wv = d_ext_wv; q.ext_wt = d_ext_wt; q.stf = d_stf; q.src_shot = d_src_shot;
+        q.tmp_out = p.tmp_out; q.end = p.end; q.sf = sf; q.d_it = d_it;
+        n += timed(5, [&] { return cgfd::launch_source(q, st); });
+      }
+    }
+    if (free_top) {
+      cgfd::PgPT<double> q;
+      q.ni = ni; q.nj = nj; q.nshot = nshot; q.sx = sx; q.sf = sf;
+      q.off_top = off0 + (long long)(nk - 1) * sz;
+      q.w_end = rptr<double>(wbuf[(step + 1) & 1]); q.w_pre = rptr<double>(wbuf[step & 1]);
+      q.pg = d_pg; q.dis = rptr<double>(d_dis); q.dt = dt;
+      n += cgfd::launch_peak_motion(q, st);
+    }
+    n += cgfd::launch_advance(d_it, st);
+    return n;
+  }
+
   int enqueue_step(int step) {
+    if (fp64) return enqueue_step64(step);
     cudaStream_t st = stream;
     int n = 0;
     if (rec.n > 0) {
@@ -469,13 +527,32 @@ class PinnedStager {
 
 // One model field (reference layout) into its device array, through stage_buf. ps: the
 // device's pinned stager, its lock held by the caller (nullptr: plain pageable copy).
-void upload_field(cgfd_problem *p, const float *host_ref, float *dst, float *stage_buf, int mode, int ghosts,
+// dst: the device field (float, or double in the FP64 build).
+void upload_field(cgfd_problem *p, const float *host_ref, void *dst, float *stage_buf, int mode, int ghosts,
                   PinnedStager *ps = nullptr) {
   size_t n = (size_t)(p->ni + 6) * (p->nj + 6) * (p->nk + 6);
   if (ps && n * sizeof(float) >= PinnedStager::kMinBytes) ps->copy(stage_buf, host_ref, n * sizeof(float), p->stream);
   else CK(cudaMemcpyAsync(stage_buf, host_ref, n * sizeof(float), cudaMemcpyHostToDevice, p->stream));
-  cgfd::launch_repack_in(stage_buf, dst, p->ni, p->nj, p->nk, p->sx, p->sz, p->off0, mode, ghosts, p->stream);
+  if (p->fp64)
+    cgfd::launch_repack_in(stage_buf, (double *)dst, p->ni, p->nj, p->nk, p->sx, p->sz, p->off0, mode, ghosts, p->stream);
+  else
+    cgfd::launch_repack_in(stage_buf, (float *)dst, p->ni, p->nj, p->nk, p->sx, p->sz, p->off0, mode, ghosts, p->stream);
   CK(cudaGetLastError());
+}
+
+// a real-typed device array of n elements (doubles in the FP64 build), held as float*
+float *dalloc_real(cgfd_problem *p, size_t n, size_t &acc) {
+  return (float *)dmalloc<uint16_t>(n * p->esz / 2, acc, p->stream);
+}
+
+// host floats -> device real-typed array (converted to double in the FP64 build)
+void upload_real(cgfd_problem *p, float *dst, const std::vector<float> &v) {
+  if (p->fp64) {
+    std::vector<double> d(v.begin(), v.end());
+    CK(cudaMemcpy(dst, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice));
+  } else {
+    CK(cudaMemcpy(dst, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
 }
 
 // Replace the FP32 coefficient array by a 16-bit copy (stochastically rounded), one
@@ -542,11 +619,12 @@ void problem_bytes(const cgfd_problem_desc *d, int nshot, const cgfd_source_desc
   long long sx, sz, sf, off0;
   layout(d->ni, d->nj, d->nk, sx, sz, sf, off0);
   const int ncoef = d->medium_type == CGFD_MEDIUM_ELASTIC_ISO ? 12 : (d->medium_type == CGFD_MEDIUM_ELASTIC_VTI ? 15 : 31);
-  const bool c16 = d->precision != CGFD_PREC_FP32, w16 = d->precision == CGFD_PREC_FP16_WAVE;
-  const size_t F = sizeof(float);
+  const bool f64 = d->precision == CGFD_PREC_FP64;
+  const bool c16 = d->precision != CGFD_PREC_FP32 && !f64, w16 = d->precision == CGFD_PREC_FP16_WAVE;
+  const size_t F = f64 ? sizeof(double) : sizeof(float);  // real-typed arrays
   const size_t waves = (size_t)9 * sf * nshot * (2 * F + 2 * (w16 ? 2 : F));
   const size_t coef32 = (size_t)ncoef * sf * F, coef16 = (size_t)ncoef * sf * 2, jac = (size_t)sf * F;
-  const size_t stage_buf = (size_t)(d->ni + 6) * (d->nj + 6) * (d->nk + 6) * F;
+  const size_t stage_buf = (size_t)(d->ni + 6) * (d->nj + 6) * (d->nk + 6) * sizeof(float);
   size_t r = waves + (c16 ? coef16 : coef32) + jac;
   const size_t high = waves + jac + coef32 + (c16 ? std::max(stage_buf, coef16 + 8 * (size_t)ncoef) : stage_buf);
   if (d->free_top) r += (size_t)2 * 9 * d->ni * d->nj * F;
@@ -570,13 +648,15 @@ void problem_bytes(const cgfd_problem_desc *d, int nshot, const cgfd_source_desc
     max_ext = std::max(max_ext, (size_t)q.max_ext);
     max_nt = std::max(max_nt, (size_t)q.max_nt);
   }
-  if (nsrc > 0) r += nsrc * 3 * sizeof(int) + nsrc * max_ext * (sizeof(long long) + 2 * F) + nsrc * max_nt * 36 * F;
+  if (nsrc > 0)
+    r += nsrc * 3 * sizeof(int) + nsrc * max_ext * (sizeof(long long) + 2 * sizeof(float)) +
+         nsrc * max_nt * 36 * sizeof(float);
   cgfd::RecvHost rec;
   cgfd::recv_setup(d, rec);
   if (rec.n > 0)
-    r += (size_t)rec.n * 8 * (sizeof(long long) + F) + (size_t)rec.n * 9 * d->nt_total * nshot * F;
+    r += (size_t)rec.n * 8 * (sizeof(long long) + sizeof(float)) + (size_t)rec.n * 9 * d->nt_total * nshot * sizeof(float);
   r += 2 * sizeof(int);
-  if (d->free_top) r += (size_t)18 * d->ni * d->nj * nshot * F;
+  if (d->free_top) r += (size_t)(15 * sizeof(float) + 3 * F) * d->ni * d->nj * nshot;
   if (w16) r += (size_t)nshot * (18 * F + 2 * sizeof(unsigned int) + (size_t)d->nt_total * 2 * F);
   if (resident) *resident = r;
   if (peak) *peak = std::max(r, high);
@@ -638,6 +718,9 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
     default: p->coef_type = cgfd::COEF_F32;
   }
   p->wave16 = d->precision == CGFD_PREC_FP16_WAVE ? 1 : 0;
+  p->fp64 = d->precision == CGFD_PREC_FP64 ? 1 : 0;
+  p->esz = p->fp64 ? sizeof(double) : sizeof(float);
+  if (p->fp64) p->use_tma = false;  // the FP64 build runs the direct-load bulk kernel
   p->device = d->device;
   CK(cudaSetDevice(p->device));
   keep_pool_memory(p->device);
@@ -668,14 +751,15 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
 
   size_t &B = p->bytes;
   // levels 0-1 (w_pre / w_end) FP32; 2-3 (RK stage inputs) FP32 or FP16
-  const size_t lev_bytes[4] = {4, 4, p->wave16 ? 2u : 4u, p->wave16 ? 2u : 4u};
+  const size_t E = p->esz;
+  const size_t lev_bytes[4] = {E, E, p->wave16 ? 2u : E, p->wave16 ? 2u : E};
   for (int l = 0; l < 4; l++)
     p->wbuf[l] = (float *)dmalloc<uint16_t>((size_t)9 * p->sf * nshot * (lev_bytes[l] / 2), B, p->stream);
-  p->coef = dmalloc<float>((size_t)p->ncoef * p->sf, B, p->stream);
-  p->jac = dmalloc<float>((size_t)p->sf, B, p->stream);
+  p->coef = dalloc_real(p, (size_t)p->ncoef * p->sf, B);
+  p->jac = dalloc_real(p, (size_t)p->sf, B);
   for (int l = 0; l < 4; l++) CK(cudaMemsetAsync(p->wbuf[l], 0, lev_bytes[l] * 9 * p->sf * nshot, p->stream));
-  CK(cudaMemsetAsync(p->coef, 0, sizeof(float) * p->ncoef * p->sf, p->stream));
-  CK(cudaMemsetAsync(p->jac, 0, sizeof(float) * p->sf, p->stream));
+  CK(cudaMemsetAsync(p->coef, 0, E * p->ncoef * p->sf, p->stream));
+  CK(cudaMemsetAsync(p->jac, 0, E * p->sf, p->stream));
 
   // coefficients: metric (ghosts kept for the traction image), 1/rho, medium
   cgfd::RefGrid g(p->ni, p->nj, p->nk);
@@ -685,11 +769,12 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
     std::lock_guard<std::mutex> lk(ps.mutex());
     upload_field(p, d->metric, p->jac, stage_buf, 0, 1, &ps);
     for (int c = 0; c < 9; c++)
-      upload_field(p, d->metric + (size_t)(1 + c) * g.siz_icmp, p->coef + (size_t)c * p->sf, stage_buf, 0, 1, &ps);
-    upload_field(p, d->medium, p->coef + (size_t)cgfd::CF_SLW * p->sf, stage_buf, 1, 0, &ps);
+      upload_field(p, d->metric + (size_t)(1 + c) * g.siz_icmp, p->rvoid(p->coef, (size_t)c * p->sf), stage_buf, 0, 1,
+                   &ps);
+    upload_field(p, d->medium, p->rvoid(p->coef, (size_t)cgfd::CF_SLW * p->sf), stage_buf, 1, 0, &ps);
     int nmed = cgfd::medium_ncmp(d->medium_type) - 1;
     for (int c = 0; c < nmed; c++)
-      upload_field(p, d->medium + (size_t)(1 + c) * g.siz_icmp, p->coef + (size_t)(cgfd::CF_MED + c) * p->sf,
+      upload_field(p, d->medium + (size_t)(1 + c) * g.siz_icmp, p->rvoid(p->coef, (size_t)(cgfd::CF_MED + c) * p->sf),
                    stage_buf, 0, 0, &ps);
   }
   CK(cudaStreamSynchronize(p->stream));
@@ -698,7 +783,7 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   if (p->coef_type != cgfd::COEF_F32) to_16bit_coefficients(p);
 
   // TMA tensor maps of the four wavefield levels and of the coefficients
-  {
+  if (!p->fp64) {
     int ty = cgfd::tma_tile_y(p->med);
     for (int l = 0; l < 4; l++) {
       if (lev_bytes[l] == 2) {  // FP16 stage level: x halo of 8 elements keeps the box 16-byte aligned
@@ -725,10 +810,10 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   if (p->free_top) {
     std::vector<float> mx, my;
     cgfd::dvh2dvz(d, mx, my);
-    p->matx = dmalloc<float>(mx.size(), B, p->stream);
-    p->maty = dmalloc<float>(my.size(), B, p->stream);
-    CK(cudaMemcpy(p->matx, mx.data(), mx.size() * sizeof(float), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(p->maty, my.data(), my.size() * sizeof(float), cudaMemcpyHostToDevice));
+    p->matx = dalloc_real(p, mx.size(), B);
+    p->maty = dalloc_real(p, my.size(), B);
+    upload_real(p, p->matx, mx);
+    upload_real(p, p->maty, my);
   }
   // PML
   cgfd::PmlFaceHost fh[3][2];
@@ -740,12 +825,12 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
       f.h = fh[a][s];
       f.n = (long long)(f.h.hi[0] - f.h.lo[0] + 1) * (f.h.hi[1] - f.h.lo[1] + 1) * (f.h.hi[2] - f.h.lo[2] + 1);
       size_t N1 = f.h.A.size();
-      f.A = dmalloc<float>(N1, B, p->stream); f.B = dmalloc<float>(N1, B, p->stream); f.D = dmalloc<float>(N1, B, p->stream);
-      CK(cudaMemcpy(f.A, f.h.A.data(), N1 * sizeof(float), cudaMemcpyHostToDevice));
-      CK(cudaMemcpy(f.B, f.h.B.data(), N1 * sizeof(float), cudaMemcpyHostToDevice));
-      CK(cudaMemcpy(f.D, f.h.D.data(), N1 * sizeof(float), cudaMemcpyHostToDevice));
-      f.aux = dmalloc<float>((size_t)3 * 9 * f.n * nshot, B, p->stream);
-      CK(cudaMemset(f.aux, 0, sizeof(float) * 3 * 9 * f.n * nshot));
+      f.A = dalloc_real(p, N1, B); f.B = dalloc_real(p, N1, B); f.D = dalloc_real(p, N1, B);
+      upload_real(p, f.A, f.h.A);
+      upload_real(p, f.B, f.h.B);
+      upload_real(p, f.D, f.h.D);
+      f.aux = dalloc_real(p, (size_t)3 * 9 * f.n * nshot, B);
+      CK(cudaMemset(f.aux, 0, E * 3 * 9 * f.n * nshot));
       p->faces.push_back(f);
     }
   // sources: one set per shot, concatenated (each source knows its shot)
@@ -854,9 +939,9 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   if (p->free_top) {
     const size_t nij = (size_t)p->ni * p->nj * nshot;
     p->d_pg = dmalloc<float>(15 * nij, B, p->stream);
-    p->d_dis = dmalloc<float>(3 * nij, B, p->stream);
+    p->d_dis = dalloc_real(p, 3 * nij, B);
     CK(cudaMemset(p->d_pg, 0, sizeof(float) * 15 * nij));
-    CK(cudaMemset(p->d_dis, 0, sizeof(float) * 3 * nij));
+    CK(cudaMemset(p->d_dis, 0, E * 3 * nij));
   }
   p->d_it = dmalloc<int>(1, B, p->stream);
   p->d_flag = dmalloc<int>(1, B, p->stream);
@@ -922,15 +1007,16 @@ void make_tiles(cgfd_problem *p) {
 // Back to the state right after cgfd_problem_create: zero wavefield levels, PML auxiliaries,
 // seismograms, peak motion, scale collectors, error word; step 0.
 void reset_state(cgfd_problem *p) {
-  const size_t lev_bytes[4] = {4, 4, p->wave16 ? 2u : 4u, p->wave16 ? 2u : 4u};
+  const size_t E = p->esz;
+  const size_t lev_bytes[4] = {E, E, p->wave16 ? 2u : E, p->wave16 ? 2u : E};
   for (int l = 0; l < 4; l++) CK(cudaMemsetAsync(p->wbuf[l], 0, lev_bytes[l] * 9 * p->sf * p->nshot, p->stream));
-  for (auto &f : p->faces) CK(cudaMemsetAsync(f.aux, 0, sizeof(float) * 3 * 9 * f.n * p->nshot, p->stream));
+  for (auto &f : p->faces) CK(cudaMemsetAsync(f.aux, 0, E * 3 * 9 * f.n * p->nshot, p->stream));
   if (p->rec.n > 0)
     CK(cudaMemsetAsync(p->d_seis, 0, sizeof(float) * p->rec.n * 9 * p->nt_total * p->nshot, p->stream));
   if (p->d_pg) {
     const size_t nij = (size_t)p->ni * p->nj * p->nshot;
     CK(cudaMemsetAsync(p->d_pg, 0, sizeof(float) * 15 * nij, p->stream));
-    CK(cudaMemsetAsync(p->d_dis, 0, sizeof(float) * 3 * nij, p->stream));
+    CK(cudaMemsetAsync(p->d_dis, 0, p->esz * 3 * nij, p->stream));
   }
   if (p->d_amax) CK(cudaMemsetAsync(p->d_amax, 0, sizeof(unsigned int) * 2 * p->nshot, p->stream));
   p->it = 0;
@@ -1066,9 +1152,10 @@ int cgfd_set_step(cgfd_problem *p, int it) {
       std::swap(p->map_ctr[0], p->map_ctr[1]);
       for (auto &f : p->faces) {
         size_t n = (size_t)9 * f.n * p->nshot;
-        CK(cudaMemcpyAsync(f.aux + n * 2, f.aux, n * sizeof(float), cudaMemcpyDeviceToDevice, p->stream));
-        CK(cudaMemcpyAsync(f.aux, f.aux + n, n * sizeof(float), cudaMemcpyDeviceToDevice, p->stream));
-        CK(cudaMemcpyAsync(f.aux + n, f.aux + n * 2, n * sizeof(float), cudaMemcpyDeviceToDevice, p->stream));
+        void *l0 = p->rvoid(f.aux, 0), *l1 = p->rvoid(f.aux, n), *l2 = p->rvoid(f.aux, 2 * n);
+        CK(cudaMemcpyAsync(l2, l0, n * p->esz, cudaMemcpyDeviceToDevice, p->stream));
+        CK(cudaMemcpyAsync(l0, l1, n * p->esz, cudaMemcpyDeviceToDevice, p->stream));
+        CK(cudaMemcpyAsync(l1, l2, n * p->esz, cudaMemcpyDeviceToDevice, p->stream));
       }
       for (int s = 0; s < 8; s++)
         if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }
@@ -1108,9 +1195,14 @@ int cgfd_get_wavefield_shot(cgfd_problem *p, int shot, float *out) {
     cgfd::RefGrid g(p->ni, p->nj, p->nk);
     size_t acc = 0;
     float *tmp = dmalloc<float>(g.siz_icmp, acc, p->stream);
-    const float *pre = p->wbuf[p->it & 1] + (size_t)shot * 9 * p->sf;
     for (int c = 0; c < 9; c++) {
-      cgfd::launch_repack_out(pre + (size_t)c * p->sf, tmp, p->ni, p->nj, p->nk, p->sx, p->sz, p->off0, p->stream);
+      const size_t off = ((size_t)shot * 9 + c) * p->sf;
+      if (p->fp64)
+        cgfd::launch_repack_out(p->rptr<double>(p->wbuf[p->it & 1], off), tmp, p->ni, p->nj, p->nk, p->sx, p->sz,
+                                p->off0, p->stream);
+      else
+        cgfd::launch_repack_out(p->rptr<float>(p->wbuf[p->it & 1], off), tmp, p->ni, p->nj, p->nk, p->sx, p->sz,
+                                p->off0, p->stream);
       CK(cudaMemcpyAsync(out + (size_t)c * g.siz_icmp, tmp, g.siz_icmp * sizeof(float), cudaMemcpyDeviceToHost, p->stream));
     }
     CK(cudaStreamSynchronize(p->stream));
@@ -1144,8 +1236,13 @@ int cgfd_get_wavefield_box(cgfd_problem *p, int shot, const int *start, const in
       p->d_box = dmalloc<float>(cnt, p->bytes, p->stream);
       p->box_cap = cnt;
     }
-    const float *pre = p->wbuf[p->it & 1] + (size_t)shot * 9 * p->sf;
-    cgfd::launch_gather_box(pre, p->sf, p->sx, p->sz, p->off0, start, count, stride, p->d_box, p->stream);
+    const size_t off = (size_t)shot * 9 * p->sf;
+    if (p->fp64)
+      cgfd::launch_gather_box(p->rptr<double>(p->wbuf[p->it & 1], off), p->sf, p->sx, p->sz, p->off0, start, count,
+                              stride, p->d_box, p->stream);
+    else
+      cgfd::launch_gather_box(p->rptr<float>(p->wbuf[p->it & 1], off), p->sf, p->sx, p->sz, p->off0, start, count,
+                              stride, p->d_box, p->stream);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, p->d_box, cnt * sizeof(float), cudaMemcpyDeviceToHost, p->stream));
     CK(cudaStreamSynchronize(p->stream));
@@ -1188,7 +1285,8 @@ std::mutex g_noalloc_mu;
 float *g_noalloc_ptr[kNoAllocMaxDevices] = {};
 
 // planes [kr0, kr0 + nplanes) of one field in the reference layout (3 ghosts, 0 there)
-__global__ void k_repack_out_planes(const float *__restrict__ src, float *__restrict__ dst, int ni, int nj, int nk,
+template <typename R>
+__global__ void k_repack_out_planes(const R *__restrict__ src, float *__restrict__ dst, int ni, int nj, int nk,
                                     long long sx, long long sz, long long off0, int kr0, int nplanes) {
   const long long nxr = ni + 6, nyr = nj + 6;
   const long long total = nxr * nyr * nplanes;
@@ -1196,7 +1294,7 @@ __global__ void k_repack_out_planes(const float *__restrict__ src, float *__rest
     const int ir = (int)(t % nxr), jr = (int)((t / nxr) % nyr), kr = kr0 + (int)(t / (nxr * nyr));
     const int i = ir - 3, j = jr - 3, k = kr - 3;
     const bool inner = i >= 0 && i < ni && j >= 0 && j < nj && k >= 0 && k < nk;
-    dst[t] = inner ? src[off0 + (long long)k * sz + (long long)j * sx + i] : 0.0f;
+    dst[t] = inner ? (float)src[off0 + (long long)k * sz + (long long)j * sx + i] : 0.0f;
   }
 }
 
@@ -1212,7 +1310,8 @@ float *noalloc_scratch(int device) {
     if (e != cudaSuccess || !ptr)
       throw cgfd::Error(CGFD_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
     cudaFuncAttributes fa;
-    e = cudaFuncGetAttributes(&fa, k_repack_out_planes);
+    e = cudaFuncGetAttributes(&fa, k_repack_out_planes<float>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_repack_out_planes<double>);
     if (e != cudaSuccess)
       throw cgfd::Error(CGFD_ERR_CUDA, std::string("cudaFuncGetAttributes(repack): ") + cudaGetErrorString(e));
     g_noalloc_ptr[device] = ptr;
@@ -1236,13 +1335,17 @@ int cgfd_get_wavefield_shot_noalloc(cgfd_problem *p, int shot, float *out) {
     CK(cudaSetDevice(p->device));
     float *scratch = noalloc_scratch(p->device);
     const int per = (int)(kNoAllocScratchFloats / plane);
-    const float *pre = p->wbuf[p->it & 1] + (size_t)shot * 9 * p->sf;
     for (int c = 0; c < 9; c++)
       for (int k0 = 0; k0 < (int)nzr; k0 += per) {
         const int np = std::min(per, (int)nzr - k0);
+        const size_t off = ((size_t)shot * 9 + c) * p->sf;
         // stream order keeps the copy of one chunk ahead of the kernel that refills the scratch
-        k_repack_out_planes<<<592, 256, 0, p->stream>>>(pre + (size_t)c * p->sf, scratch, p->ni, p->nj, p->nk, p->sx,
-                                                         p->sz, p->off0, k0, np);
+        if (p->fp64)
+          k_repack_out_planes<<<592, 256, 0, p->stream>>>(p->rptr<double>(p->wbuf[p->it & 1], off), scratch, p->ni,
+                                                           p->nj, p->nk, p->sx, p->sz, p->off0, k0, np);
+        else
+          k_repack_out_planes<<<592, 256, 0, p->stream>>>(p->rptr<float>(p->wbuf[p->it & 1], off), scratch, p->ni,
+                                                           p->nj, p->nk, p->sx, p->sz, p->off0, k0, np);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(out + (size_t)c * plane * nzr + (size_t)k0 * plane, scratch, (size_t)np * plane * sizeof(float),
                            cudaMemcpyDeviceToHost, p->stream));
@@ -1258,11 +1361,12 @@ int cgfd_set_wavefield_shot(cgfd_problem *p, int shot, const float *in) {
     cgfd::RefGrid g(p->ni, p->nj, p->nk);
     size_t acc = 0;
     float *tmp = dmalloc<float>(g.siz_icmp, acc, p->stream);
-    float *pre = p->wbuf[p->it & 1] + (size_t)shot * 9 * p->sf;
     {
       PinnedStager &ps = PinnedStager::for_device(p->device);
       std::lock_guard<std::mutex> lk(ps.mutex());
-      for (int c = 0; c < 9; c++) upload_field(p, in + (size_t)c * g.siz_icmp, pre + (size_t)c * p->sf, tmp, 0, 0, &ps);
+      for (int c = 0; c < 9; c++)
+        upload_field(p, in + (size_t)c * g.siz_icmp, p->rvoid(p->wbuf[p->it & 1], ((size_t)shot * 9 + c) * p->sf), tmp, 0,
+                     0, &ps);
     }
     refresh_wave_max(p);
     CK(cudaStreamSynchronize(p->stream));
@@ -1346,7 +1450,11 @@ int cgfd_autotune(cgfd_problem *p, int steps, int *chosen) {
 int cgfd_set_bulk_variant(cgfd_problem *p, int tma) {
   if (!p) return CGFD_ERR_INVALID;
   if (!tma && p->nshot > 1) { set_err("the direct-load bulk kernel handles one shot"); return CGFD_ERR_UNSUPPORTED; }
-  if (!tma && p->precision != CGFD_PREC_FP32) {
+  if (tma && p->fp64) {
+    set_err("the FP64 build runs the direct-load bulk kernel");
+    return CGFD_ERR_UNSUPPORTED;
+  }
+  if (!tma && p->precision != CGFD_PREC_FP32 && !p->fp64) {
     set_err("the direct-load bulk kernel handles FP32 storage only");
     return CGFD_ERR_UNSUPPORTED;
   }

@@ -41,45 +41,51 @@ template <> struct MedInfo<MED_ISO>   { static constexpr int NCOEF = 12; };
 template <> struct MedInfo<MED_VTI>   { static constexpr int NCOEF = 15; };
 template <> struct MedInfo<MED_ANISO> { static constexpr int NCOEF = 31; };
 
+// Real type R of the stored solution, coefficients and arithmetic: float (the reference's
+// precision, every production mode) or double (the FP64 build, CGFD_PREC_FP64).
+
 // One CFS-PML face (bdry_t.cu:85-257): box [lo,hi] in physical indices, 1-D A/B/D along the
 // face normal, and the 9-component auxiliary variables (component stride n) at the levels
 // this stage reads and writes.
-struct FaceP {
+template <typename R>
+struct FacePT {
   int enable;
   int axis;           // 0 x, 1 y, 2 z
   int lo[3], hi[3];   // inclusive box, physical 0-based indices
   int nx, ny;         // box extents along x, y
   long long n;        // points in the box
-  const float *A, *B, *D;
+  const R *A, *B, *D;
   // each level holds nshot x 9 components (shot stride 9 n)
-  const float *aux_cur;   // level read by the RHS (pre at stage 0, tmp otherwise)
-  const float *aux_pre;   // pre level (stages 1-2)
-  float *aux_tmp;         // tmp level written at stages 0-2 (== aux_cur at stages 1-2)
-  float *aux_end;         // end level
+  const R *aux_cur;   // level read by the RHS (pre at stage 0, tmp otherwise)
+  const R *aux_pre;   // pre level (stages 1-2)
+  R *aux_tmp;         // tmp level written at stages 0-2 (== aux_cur at stages 1-2)
+  R *aux_end;         // end level
 };
+using FaceP = FacePT<float>;
 
-struct StageP {
+template <typename R>
+struct StagePT {
   int ni, nj, nk;
   int stage;              // 0..3
   int dir[3];             // 0 backward, 1 forward (fd_t.cu:184-235)
   long long sx, sz, sf;   // row, plane and field strides of the device layout (floats)
   long long off0;         // offset of physical point (0,0,0)
-  const float *cur;       // wavefield read by the stencils (9 fields); __half when the
+  const R *cur;           // wavefield read by the stencils (9 fields); __half when the
                           // FP16 stage levels are the input (stages 1-3)
-  const float *pre;       // w_pre (stages 1-2)
-  float *tmp_out;         // next stage input (stages 0-2); __half in FP16-stage mode
-  float *end;             // accumulator (written at every stage)
-  float ca, cb;           // rk_a[stage]*dt, rk_b[stage]*dt
-  const void *coef;       // [ncoef][sf] of float, __half or __nv_bfloat16
+  const R *pre;           // w_pre (stages 1-2)
+  R *tmp_out;             // next stage input (stages 0-2); __half in FP16-stage mode
+  R *end;                 // accumulator (written at every stage)
+  R ca, cb;               // rk_a[stage]*dt, rk_b[stage]*dt
+  const void *coef;       // [ncoef][sf] of R, __half, __nv_bfloat16 or uint16_t
   float cscale[32];       // 16-bit coefficients: value = cscale[f] * stored + coffset[f]
   float coffset[32];
-  const float *jac;       // [sf]
-  const float *matx;      // free surface: [nj][ni][9] matVx2Vz (row-major 3x3)
-  const float *maty;      //                [nj][ni][9] matVy2Vz
+  const R *jac;           // [sf]
+  const R *matx;          // free surface: [nj][ni][9] matVx2Vz (row-major 3x3)
+  const R *maty;          //                [nj][ni][9] matVy2Vz
   int free_top;
   int nbulk;              // planes [0, nbulk) belong to the bulk kernel
   int nface;
-  FaceP face[6];
+  FacePT<R> face[6];
   int *err;               // device error word: kErrStationNonfinite, kErrPipelineTimeout, kErrWaveNonfinite
   int nshot;              // wavefields sharing this grid (batched sources); 1 = plain
   // FP16 stage levels, per shot s: wsc[18s + 0..8] scale (value = scale * stored),
@@ -88,6 +94,7 @@ struct StageP {
   const float *wsc;
   unsigned int *amax;
 };
+using StageP = StagePT<float>;
 
 // max |w| groups of the FP16 stage levels: velocity (fields 0-2) and stress (3-8)
 __host__ __device__ constexpr int wgroup(int f) { return f < 3 ? 0 : 1; }
@@ -102,14 +109,18 @@ struct TmaP {
 // MacCormack DRP operator (fd_t.cu:90-93, 111-114): backward uses offsets -3..+1,
 // forward -1..+3. The 5 samples are passed in increasing position.
 // ---------------------------------------------------------------------------------------
-template <int DIR>
-__device__ __forceinline__ float drp5(float a0, float a1, float a2, float a3, float a4) {
+// (the coefficients are the reference's float values, in either real type)
+template <int DIR, typename R>
+__device__ __forceinline__ R drp5(R a0, R a1, R a2, R a3, R a4) {
   if (DIR == 0)
-    return -0.041686285f * a0 + 0.333411808f * a1 - 1.250117713f * a2 + 0.666745142f * a3 + 0.291647047f * a4;
+    return R(-0.041686285f) * a0 + R(0.333411808f) * a1 - R(1.250117713f) * a2 + R(0.666745142f) * a3 +
+           R(0.291647047f) * a4;
   else
-    return -0.291647047f * a0 - 0.666745142f * a1 + 1.250117713f * a2 - 0.333411808f * a3 + 0.041686285f * a4;
+    return R(-0.291647047f) * a0 - R(0.666745142f) * a1 + R(1.250117713f) * a2 - R(0.333411808f) * a3 +
+           R(0.041686285f) * a4;
 }
-__device__ __forceinline__ float drp5r(int dir, float a0, float a1, float a2, float a3, float a4) {
+template <typename R>
+__device__ __forceinline__ R drp5r(int dir, R a0, R a1, R a2, R a3, R a4) {
   return dir ? drp5<1>(a0, a1, a2, a3, a4) : drp5<0>(a0, a1, a2, a3, a4);
 }
 // left extent of the operator
@@ -123,19 +134,19 @@ __host__ __device__ constexpr int voigt(int a, int b) {
 // ---------------------------------------------------------------------------------------
 // Hooke's law from the velocity gradient G[vi][xj] = dV_vi/dx_j, per medium.
 // ---------------------------------------------------------------------------------------
-template <int MED>
+template <int MED, typename R = float>
 struct Medium;
 
-template <>
-struct Medium<MED_ISO> {
-  float lam, mu, lam2mu;
+template <typename R>
+struct Medium<MED_ISO, R> {
+  R lam, mu, lam2mu;
   template <typename G>
   __device__ __forceinline__ void load(G get) {  // get(c): coefficient field c at the cell
     lam = get(CF_MED + 0);
     mu = get(CF_MED + 1);
-    lam2mu = lam + 2.0f * mu;
+    lam2mu = lam + R(2) * mu;
   }
-  __device__ __forceinline__ void hooke(const float G[3][3], float h[6]) const {
+  __device__ __forceinline__ void hooke(const R G[3][3], R h[6]) const {
     h[0] = lam2mu * G[0][0] + lam * (G[1][1] + G[2][2]);
     h[1] = lam2mu * G[1][1] + lam * (G[0][0] + G[2][2]);
     h[2] = lam2mu * G[2][2] + lam * (G[0][0] + G[1][1]);
@@ -145,9 +156,9 @@ struct Medium<MED_ISO> {
   }
 };
 
-template <>
-struct Medium<MED_VTI> {
-  float c11, c12, c13, c33, c55, c66;
+template <typename R>
+struct Medium<MED_VTI, R> {
+  R c11, c12, c13, c33, c55, c66;
   template <typename G>
   __device__ __forceinline__ void load(G get) {
     c11 = get(CF_MED + 0);
@@ -155,9 +166,9 @@ struct Medium<MED_VTI> {
     c33 = get(CF_MED + 2);
     c55 = get(CF_MED + 3);
     c66 = get(CF_MED + 4);
-    c12 = c11 - 2.0f * c66;  // sv_curv_col_el_vti_gpu.cu:407
+    c12 = c11 - R(2) * c66;  // sv_curv_col_el_vti_gpu.cu:407
   }
-  __device__ __forceinline__ void hooke(const float G[3][3], float h[6]) const {
+  __device__ __forceinline__ void hooke(const R G[3][3], R h[6]) const {
     h[0] = c11 * G[0][0] + c12 * G[1][1] + c13 * G[2][2];
     h[1] = c12 * G[0][0] + c11 * G[1][1] + c13 * G[2][2];
     h[2] = c13 * (G[0][0] + G[1][1]) + c33 * G[2][2];
@@ -167,9 +178,9 @@ struct Medium<MED_VTI> {
   }
 };
 
-template <>
-struct Medium<MED_ANISO> {
-  float c[21];  // c11 c12 c13 c14 c15 c16 c22 .. c66 (upper triangle, row-major)
+template <typename R>
+struct Medium<MED_ANISO, R> {
+  R c[21];  // c11 c12 c13 c14 c15 c16 c22 .. c66 (upper triangle, row-major)
   template <typename G>
   __device__ __forceinline__ void load(G get) {
 #pragma unroll
@@ -179,12 +190,12 @@ struct Medium<MED_ANISO> {
     // index of C[a][b] (a<=b) in the packed upper triangle
     return a * 6 - a * (a - 1) / 2 + (b - a);
   }
-  __device__ __forceinline__ float C(int a, int b) const { return a <= b ? c[up(a, b)] : c[up(b, a)]; }
-  __device__ __forceinline__ void hooke(const float G[3][3], float h[6]) const {
-    float e[6] = {G[0][0], G[1][1], G[2][2], G[1][2] + G[2][1], G[0][2] + G[2][0], G[0][1] + G[1][0]};
+  __device__ __forceinline__ R C(int a, int b) const { return a <= b ? c[up(a, b)] : c[up(b, a)]; }
+  __device__ __forceinline__ void hooke(const R G[3][3], R h[6]) const {
+    R e[6] = {G[0][0], G[1][1], G[2][2], G[1][2] + G[2][1], G[0][2] + G[2][0], G[0][1] + G[1][0]};
 #pragma unroll
     for (int I = 0; I < 6; I++) {
-      float s = C(I, 0) * e[0];
+      R s = C(I, 0) * e[0];
 #pragma unroll
       for (int J = 1; J < 6; J++) s += C(I, J) * e[J];
       h[I] = s;
@@ -194,6 +205,7 @@ struct Medium<MED_ANISO> {
 
 // 16-bit storage: value = per-field scale x stored value (FP32 arithmetic)
 __device__ __forceinline__ float to_f(float x) { return x; }
+__device__ __forceinline__ double to_f(double x) { return x; }
 __device__ __forceinline__ float to_f(__half x) { return __half2float(x); }
 __device__ __forceinline__ float to_f(__nv_bfloat16 x) { return __bfloat162float(x); }
 __device__ __forceinline__ float to_f(uint16_t x) { return (float)x; }
@@ -210,26 +222,33 @@ __device__ __forceinline__ void atomic_max_abs(unsigned int *a, float v) {
   atomicMax(a, __float_as_uint(fabsf(v)));
 }
 
-// decode of one stored coefficient of field c
+// Real type the kernels compute in for coefficient storage TC: double for the FP64 build,
+// float otherwise.
 template <typename TC>
-__device__ __forceinline__ float coef_decode(TC v, const StageP &p, int c) {
-  if constexpr (std::is_same<TC, float>::value) return v;
+using real_of = typename std::conditional<std::is_same<TC, double>::value, double, float>::type;
+
+// decode of one stored coefficient of field c
+template <typename TC, typename P>
+__device__ __forceinline__ real_of<TC> coef_decode(TC v, const P &p, int c) {
+  if constexpr (std::is_same<TC, float>::value || std::is_same<TC, double>::value) return v;
   else return fmaf(p.cscale[c], to_f(v), p.coffset[c]);
 }
 
 template <typename TC>
 struct CoefView {
+  using P = StagePT<real_of<TC>>;
   const TC *base;
   long long stride;
-  const StageP &p;
-  __device__ __forceinline__ CoefView(const StageP &p_) : base(static_cast<const TC *>(p_.coef)), stride(p_.sf), p(p_) {}
-  __device__ __forceinline__ float operator()(int c, long long idx) const {
+  const P &p;
+  __device__ __forceinline__ CoefView(const P &p_) : base(static_cast<const TC *>(p_.coef)), stride(p_.sf), p(p_) {}
+  __device__ __forceinline__ real_of<TC> operator()(int c, long long idx) const {
     return coef_decode<TC>(__ldg(base + c * stride + idx), p, c);
   }
 };
 
 // momentum of one axis: sum_j m[j] * dT_(vi,j) / d(axis)
-__device__ __forceinline__ void momentum_axis(const float m[3], const float dt[6], float mom[3]) {
+template <typename R>
+__device__ __forceinline__ void momentum_axis(const R m[3], const R dt[6], R mom[3]) {
   mom[0] = m[0] * dt[0] + m[1] * dt[5] + m[2] * dt[4];
   mom[1] = m[0] * dt[5] + m[1] * dt[1] + m[2] * dt[3];
   mom[2] = m[0] * dt[4] + m[1] * dt[3] + m[2] * dt[2];
@@ -238,27 +257,28 @@ __device__ __forceinline__ void momentum_axis(const float m[3], const float dt[6
 // ---------------------------------------------------------------------------------------
 // Per-cell state carried from the derivative phase to the store phase.
 // ---------------------------------------------------------------------------------------
+template <typename R = float>
 struct CellAcc {
-  float G[3][3];   // velocity gradient
-  float mom[3];    // divergence of stress (before 1/rho)
-  float hc[9];     // sum of PML corrections
+  R G[3][3];   // velocity gradient
+  R mom[3];    // divergence of stress (before 1/rho)
+  R hc[9];     // sum of PML corrections
   __device__ __forceinline__ void zero() {
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      mom[a] = 0.f;
+      mom[a] = R(0);
 #pragma unroll
-      for (int b = 0; b < 3; b++) G[a][b] = 0.f;
+      for (int b = 0; b < 3; b++) G[a][b] = R(0);
     }
 #pragma unroll
-    for (int c = 0; c < 9; c++) hc[c] = 0.f;
+    for (int c = 0; c < 9; c++) hc[c] = R(0);
   }
   // accumulate the derivatives of one axis with metric row m
-  __device__ __forceinline__ void add_axis(const float m[3], const float dv[3], const float dt[6]) {
+  __device__ __forceinline__ void add_axis(const R m[3], const R dv[3], const R dt[6]) {
 #pragma unroll
     for (int vi = 0; vi < 3; vi++)
 #pragma unroll
       for (int xj = 0; xj < 3; xj++) G[vi][xj] += m[xj] * dv[vi];
-    float mm[3];
+    R mm[3];
     momentum_axis(m, dt, mm);
     mom[0] += mm[0]; mom[1] += mm[1]; mom[2] += mm[2];
   }
@@ -270,14 +290,16 @@ constexpr int kErrWaveNonfinite = 4;     // the RK combine produced a NaN/Inf so
 
 // true when v is NaN or +-Inf (a NaN compares false)
 __device__ __forceinline__ bool nonfinite(float v) { return !(fabsf(v) <= 3.402823466e38f); }
+__device__ __forceinline__ bool nonfinite(double v) { return !(fabs(v) <= 1.7976931348623157e308); }
 
 // RK combine of 9 values at one point (wav_update / wav_update_end, wav_t.cu:362-378).
 // cur_c: the stage input at the point (== pre at stage 0). err (may be null): at stage 3,
 // a non-finite new solution value sets kErrWaveNonfinite there -- the blow-up sentinel the
 // reference leaves stubbed (drv_rk_curv_col.cu:507-510, wav_check_value wav_t.cu:260-279).
-__device__ __forceinline__ void rk_store(int stage, float ca, float cb, long long comp_stride, long long idx,
-                                         const float cur_c[9], const float h[9], const float *pre,
-                                         float *tmp_out, float *end, int *err = nullptr) {
+template <typename R>
+__device__ __forceinline__ void rk_store(int stage, R ca, R cb, long long comp_stride, long long idx,
+                                         const R cur_c[9], const R h[9], const R *pre,
+                                         R *tmp_out, R *end, int *err = nullptr) {
   if (stage == 0) {
 #pragma unroll
     for (int c = 0; c < 9; c++) {
@@ -285,7 +307,7 @@ __device__ __forceinline__ void rk_store(int stage, float ca, float cb, long lon
       end[c * comp_stride + idx] = cur_c[c] + cb * h[c];
     }
   } else if (stage < 3) {
-    float p[9], e[9];
+    R p[9], e[9];
 #pragma unroll
     for (int c = 0; c < 9; c++) {
       p[c] = __ldg(pre + c * comp_stride + idx);
@@ -297,13 +319,13 @@ __device__ __forceinline__ void rk_store(int stage, float ca, float cb, long lon
       end[c * comp_stride + idx] = e[c] + cb * h[c];
     }
   } else {
-    float e[9];
+    R e[9];
     bool bad = false;
 #pragma unroll
     for (int c = 0; c < 9; c++) e[c] = end[c * comp_stride + idx];
 #pragma unroll
     for (int c = 0; c < 9; c++) {
-      const float v = e[c] + cb * h[c];
+      const R v = e[c] + cb * h[c];
       end[c * comp_stride + idx] = v;
       bad |= nonfinite(v);
     }
@@ -315,27 +337,29 @@ __device__ __forceinline__ void rk_store(int stage, float ca, float cb, long lon
 //   rhs_d = the 1-D terms of this axis; h += (B-1) rhs_d - B aux; aux' = D rhs_d - A aux,
 //   plus the free-surface-converted zeta terms on x/y faces at the top (surf != nullptr),
 //   followed by the RK combine of the auxiliary variables.
-template <int MED>
-__device__ __forceinline__ void pml_face(const StageP &p, const FaceP &f, int i, int j, int k,
-                                         const Medium<MED> &md, float slw, const float m[3],
-                                         const float dv[3], const float dt[6], const float *surf_mat,
-                                         const float zeta[3], float hc[9], int shot = 0) {
+template <typename T> struct nondeduced { using type = T; };  // keeps nullptr arguments out of deduction
+
+template <int MED, typename R>
+__device__ __forceinline__ void pml_face(const StagePT<R> &p, const FacePT<R> &f, int i, int j, int k,
+                                         const Medium<MED, R> &md, R slw, const R m[3],
+                                         const R dv[3], const R dt[6], const typename nondeduced<R>::type *surf_mat,
+                                         const typename nondeduced<R>::type *zeta, R hc[9], int shot = 0) {
   int ab = f.axis == 0 ? i - f.lo[0] : (f.axis == 1 ? j - f.lo[1] : k - f.lo[2]);
-  float cA = __ldg(f.A + ab), cB = __ldg(f.B + ab), cD = __ldg(f.D + ab);
-  float cB1 = cB - 1.0f;
+  R cA = __ldg(f.A + ab), cB = __ldg(f.B + ab), cD = __ldg(f.D + ab);
+  R cB1 = cB - R(1);
   long long ia = (long long)shot * 9 * f.n + ((long long)(k - f.lo[2]) * f.ny + (j - f.lo[1])) * f.nx + (i - f.lo[0]);
-  float rhs[9];
+  R rhs[9];
   momentum_axis(m, dt, rhs);
   rhs[0] *= slw; rhs[1] *= slw; rhs[2] *= slw;
   {
-    float Ga[3][3];
+    R Ga[3][3];
 #pragma unroll
     for (int vi = 0; vi < 3; vi++)
 #pragma unroll
       for (int xj = 0; xj < 3; xj++) Ga[vi][xj] = m[xj] * dv[vi];
     md.hooke(Ga, rhs + 3);
   }
-  float aux[9], arhs[9];
+  R aux[9], arhs[9];
 #pragma unroll
   for (int c = 0; c < 9; c++) {
     aux[c] = f.aux_cur[c * f.n + ia];
@@ -344,10 +368,10 @@ __device__ __forceinline__ void pml_face(const StageP &p, const FaceP &f, int i,
   }
   if (surf_mat) {
     // dzV converted from this axis' derivative (sv_curv_col_el_iso_gpu.cu:855-915)
-    float dz[3];
+    R dz[3];
 #pragma unroll
     for (int r = 0; r < 3; r++) dz[r] = surf_mat[3 * r] * dv[0] + surf_mat[3 * r + 1] * dv[1] + surf_mat[3 * r + 2] * dv[2];
-    float Gs[3][3], hs[6];
+    R Gs[3][3], hs[6];
 #pragma unroll
     for (int vi = 0; vi < 3; vi++)
 #pragma unroll
@@ -362,13 +386,15 @@ __device__ __forceinline__ void pml_face(const StageP &p, const FaceP &f, int i,
   rk_store(p.stage, p.ca, p.cb, f.n, ia, aux, arhs, f.aux_pre, f.aux_tmp, f.aux_end);
 }
 
-__device__ __forceinline__ bool in_face(const FaceP &f, int i, int j, int k) {
+template <typename R>
+__device__ __forceinline__ bool in_face(const FacePT<R> &f, int i, int j, int k) {
   return i >= f.lo[0] && i <= f.hi[0] && j >= f.lo[1] && j <= f.hi[1] && k >= f.lo[2] && k <= f.hi[2];
 }
 
 
 // Index helpers for the device layout.
-__device__ __forceinline__ long long didx(const StageP &p, int i, int j, int k) {
+template <typename R>
+__device__ __forceinline__ long long didx(const StagePT<R> &p, int i, int j, int k) {
   return p.off0 + (long long)k * p.sz + (long long)j * p.sx + i;
 }
 

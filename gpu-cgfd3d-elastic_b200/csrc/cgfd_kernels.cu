@@ -20,11 +20,16 @@
 
 namespace cgfd {
 
-template <int MED, int DX, int DY, int DZ>
-__global__ void __launch_bounds__(TX *TY, 2) k_stage_bulk(const __grid_constant__ StageP p, int nzc) {
+// Tile height of the direct-load kernel: 8 rows in FP32, 4 in FP64 (static shared memory).
+template <typename R> struct DirectTile { static constexpr int TYB = sizeof(R) == 8 ? 4 : TY; };
+
+template <int MED, int DX, int DY, int DZ, typename R = float>
+__global__ void __launch_bounds__(TX *DirectTile<R>::TYB, 2)
+    k_stage_bulk(const __grid_constant__ StagePT<R> p, int nzc) {
+  constexpr int TY = DirectTile<R>::TYB;
   constexpr int LX = op_left(DX), LY = op_left(DY), LZ = op_left(DZ);
   constexpr int SW = TX + 4, SH = TY + 4;
-  __shared__ float s[2][9][SH][SW];
+  __shared__ R s[2][9][SH][SW];
 
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int bx = blockIdx.x, by = blockIdx.y;
@@ -34,7 +39,7 @@ __global__ void __launch_bounds__(TX *TY, 2) k_stage_bulk(const __grid_constant_
   if (kb >= ke) return;
   const bool act = (i < p.ni) && (j < p.nj);
   const long long sf = p.sf;
-  const float *__restrict__ cur = p.cur;
+  const R *__restrict__ cur = p.cur;
 
   // halo slot of this thread (x halo: 4 columns per tile row, y halo: 4 rows per tile column)
   int h_i = 0, h_j = 0, h_sx = 0, h_sy = 0;
@@ -59,11 +64,11 @@ __global__ void __launch_bounds__(TX *TY, 2) k_stage_bulk(const __grid_constant_
   const bool h_ld = h_on && h_i <= p.ni + 2 && h_j <= p.nj + 2;
 
   // z register queue: q[f][n] holds plane k - LZ + n
-  float q[9][5];
+  R q[9][5];
 #pragma unroll
   for (int f = 0; f < 9; f++)
 #pragma unroll
-    for (int n = 0; n < 5; n++) q[f][n] = 0.f;
+    for (int n = 0; n < 5; n++) q[f][n] = R(0);
   if (act) {
 #pragma unroll
     for (int n = 0; n < 4; n++) {
@@ -85,34 +90,34 @@ __global__ void __launch_bounds__(TX *TY, 2) k_stage_bulk(const __grid_constant_
     if (h_on) {
       long long id = h_ld ? didx(p, h_i, h_j, k) : 0;
 #pragma unroll
-      for (int f = 0; f < 9; f++) s[buf][f][h_sy][h_sx] = h_ld ? __ldg(cur + f * sf + id) : 0.f;
+      for (int f = 0; f < 9; f++) s[buf][f][h_sy][h_sx] = h_ld ? __ldg(cur + f * sf + id) : R(0);
     }
     __syncthreads();
 
     if (act) {
       const long long id = didx(p, i, j, k);
-      const CoefView<float> cv(p);
-      float m[3][3];
+      const CoefView<R> cv(p);
+      R m[3][3];
 #pragma unroll
       for (int a = 0; a < 3; a++)
 #pragma unroll
         for (int b = 0; b < 3; b++) m[a][b] = cv(3 * a + b, id);
-      const float slw = cv(CF_SLW, id);
-      Medium<MED> md;
+      const R slw = cv(CF_SLW, id);
+      Medium<MED, R> md;
       md.load([&](int c) { return cv(c, id); });
-      CellAcc acc;
+      CellAcc<R> acc;
       acc.zero();
       // ---- x
       {
-        float d[9];
+        R d[9];
 #pragma unroll
         for (int f = 0; f < 9; f++) {
-          const float *r = &s[buf][f][ty + LY][tx];
+          const R *r = &s[buf][f][ty + LY][tx];
           d[f] = drp5<DX>(r[0], r[1], r[2], r[3], r[4]);
         }
         acc.add_axis(m[0], d, d + 3);
         for (int fi = 0; fi < p.nface; fi++) {
-          const FaceP &fc = p.face[fi];
+          const FacePT<R> &fc = p.face[fi];
           if (fc.axis == 0 && i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] && j <= fc.hi[1] && k >= fc.lo[2] &&
               k <= fc.hi[2])
             pml_face<MED>(p, fc, i, j, k, md, slw, m[0], d, d + 3, nullptr, nullptr, acc.hc);
@@ -120,14 +125,14 @@ __global__ void __launch_bounds__(TX *TY, 2) k_stage_bulk(const __grid_constant_
       }
       // ---- y
       {
-        float d[9];
+        R d[9];
 #pragma unroll
         for (int f = 0; f < 9; f++)
           d[f] = drp5<DY>(s[buf][f][ty][tx + LX], s[buf][f][ty + 1][tx + LX], s[buf][f][ty + 2][tx + LX],
                           s[buf][f][ty + 3][tx + LX], s[buf][f][ty + 4][tx + LX]);
         acc.add_axis(m[1], d, d + 3);
         for (int fi = 0; fi < p.nface; fi++) {
-          const FaceP &fc = p.face[fi];
+          const FacePT<R> &fc = p.face[fi];
           if (fc.axis == 1 && i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] && j <= fc.hi[1] && k >= fc.lo[2] &&
               k <= fc.hi[2])
             pml_face<MED>(p, fc, i, j, k, md, slw, m[1], d, d + 3, nullptr, nullptr, acc.hc);
@@ -135,25 +140,25 @@ __global__ void __launch_bounds__(TX *TY, 2) k_stage_bulk(const __grid_constant_
       }
       // ---- z
       {
-        float d[9];
+        R d[9];
 #pragma unroll
         for (int f = 0; f < 9; f++) d[f] = drp5<DZ>(q[f][0], q[f][1], q[f][2], q[f][3], q[f][4]);
         acc.add_axis(m[2], d, d + 3);
         for (int fi = 0; fi < p.nface; fi++) {
-          const FaceP &fc = p.face[fi];
+          const FacePT<R> &fc = p.face[fi];
           if (fc.axis == 2 && i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] && j <= fc.hi[1] && k >= fc.lo[2] &&
               k <= fc.hi[2])
             pml_face<MED>(p, fc, i, j, k, md, slw, m[2], d, d + 3, nullptr, nullptr, acc.hc);
         }
       }
-      float h[9];
+      R h[9];
       h[0] = slw * acc.mom[0] + acc.hc[0];
       h[1] = slw * acc.mom[1] + acc.hc[1];
       h[2] = slw * acc.mom[2] + acc.hc[2];
       md.hooke(acc.G, h + 3);
 #pragma unroll
       for (int c = 3; c < 9; c++) h[c] += acc.hc[c];
-      float cc[9];
+      R cc[9];
 #pragma unroll
       for (int f = 0; f < 9; f++) cc[f] = q[f][LZ];
       rk_store(p.stage, p.ca, p.cb, sf, id, cc, h, p.pre, p.tmp_out, p.end, p.err);
@@ -174,16 +179,16 @@ struct WaveIn {
   const TW *w;
   long long sf;
   const float *sc;
-  __device__ __forceinline__ float operator()(int f, long long q) const {
-    const float v = to_f(__ldg(w + f * sf + q));
-    if constexpr (std::is_same<TW, float>::value) return v;
+  __device__ __forceinline__ real_of<TW> operator()(int f, long long q) const {
+    const real_of<TW> v = to_f(__ldg(w + f * sf + q));
+    if constexpr (std::is_same<TW, float>::value || std::is_same<TW, double>::value) return v;
     else return v * __ldg(sc + f);
   }
 };
 
 template <typename TW>
 __device__ __forceinline__ void ld5(int dir, const WaveIn<TW> &cur, int f, long long id, long long off,
-                                    float (&o)[5]) {
+                                    real_of<TW> (&o)[5]) {
   int L = op_left(dir);
 #pragma unroll
   for (int n = 0; n < 5; n++) o[n] = cur(f, id + (n - L) * off);
@@ -196,10 +201,11 @@ __device__ __forceinline__ void ld5(int dir, const WaveIn<TW> &cur, int f, long 
 // The operator directions of the stage (DX, DY, DZ: 0 backward, 1 forward) are template
 // parameters, so that every stencil offset is a compile-time constant.
 template <int MED, typename TC, int WP, int DX, int DY, int DZ>
-__global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant__ StageP p) {
+__global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant__ StagePT<real_of<TC>> p) {
   constexpr int DIR[3] = {DX, DY, DZ};
-  using TW = typename std::conditional<WP == 2, __half, float>::type;
-  using TT = typename std::conditional<WP >= 1, __half, float>::type;
+  using R = real_of<TC>;  // double in the FP64 build (TC double, WP 0), float otherwise
+  using TW = typename std::conditional<WP == 2, __half, R>::type;
+  using TT = typename std::conditional<WP >= 1, __half, R>::type;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= p.ni || j >= p.nj) return;
@@ -216,38 +222,38 @@ __global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant_
     const int k = p.nbulk + blockIdx.z % nslab;  // one thread per cell of the slab
     const long long id = didx(p, i, j, k);
     const CoefView<TC> cv(p);
-    float m[3][3];
+    R m[3][3];
 #pragma unroll
     for (int a = 0; a < 3; a++)
 #pragma unroll
       for (int b = 0; b < 3; b++) m[a][b] = cv(3 * a + b, id);
-    const float slw = cv(CF_SLW, id);
-    Medium<MED> md;
+    const R slw = cv(CF_SLW, id);
+    Medium<MED, R> md;
     md.load([&](int c) { return cv(c, id); });
 
     // normal derivatives of all 9 fields along the 3 axes
-    float dv[3][3], dtt[3][6];
+    R dv[3][3], dtt[3][6];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
 #pragma unroll
       for (int f = 0; f < 9; f++) {
-        float v[5];
+        R v[5];
         ld5(DIR[a], cur, f, id, offs[a], v);
-        float d = drp5r(DIR[a], v[0], v[1], v[2], v[3], v[4]);
+        R d = drp5r(DIR[a], v[0], v[1], v[2], v[3], v[4]);
         if (f < 3) dv[a][f] = d; else dtt[a][f - 3] = d;
       }
     }
-    float hc[9];
+    R hc[9];
 #pragma unroll
-    for (int c = 0; c < 9; c++) hc[c] = 0.f;
+    for (int c = 0; c < 9; c++) hc[c] = R(0);
 
     // momentum: normal form, or the traction image near the free surface
-    float h[9];
+    R h[9];
     {
-      float mom[3] = {0.f, 0.f, 0.f};
+      R mom[3] = {R(0), R(0), R(0)};
 #pragma unroll
       for (int a = 0; a < 3; a++) {
-        float mm[3];
+        R mm[3];
         momentum_axis(m[a], dtt[a], mm);
         mom[0] += mm[0]; mom[1] += mm[1]; mom[2] += mm[2];
       }
@@ -259,15 +265,15 @@ __global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant_
       if (k >= nk2 - idx_last) {
         // sv_curv_col_el_gpu.cu:53-217
         const int n_free = nk2 - k - idx_first;
-        const float jc = __ldg(p.jac + id);
-        const float slwjac = slw / jc;
+        const R jc = __ldg(p.jac + id);
+        const R slwjac = slw / jc;
         constexpr int LXo = op_left(DX), LYo = op_left(DY), LZo = op_left(dzr);
         // rows of the stress tensor: components (Txx,Txy,Txz), (Txy,Tyy,Tyz), (Txz,Tyz,Tzz)
         const int tr[3][3] = {{3, 8, 7}, {8, 4, 6}, {7, 6, 5}};
 #pragma unroll
         for (int c = 0; c < 3; c++) {
           const int f1 = tr[c][0], f2 = tr[c][1], f3 = tr[c][2];
-          float vx[5], vy[5], vz[5];
+          R vx[5], vy[5], vz[5];
 #pragma unroll
           for (int n = 0; n < 5; n++) {
             long long q = id + (n - LXo);
@@ -275,24 +281,24 @@ __global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant_
             q = id + (long long)(n - LYo) * p.sx;
             vy[n] = __ldg(p.jac + q) * (cv(3, q) * cur(f1, q) + cv(4, q) * cur(f2, q) + cv(5, q) * cur(f3, q));
             int off;
-            float sgn;
-            if (n < n_free) { off = n - LZo; sgn = 1.f; }
-            else if (n == n_free) { off = 0; sgn = 0.f; }
-            else { off = (n - LZo) - 2 * (n - n_free); sgn = -1.f; }
+            R sgn;
+            if (n < n_free) { off = n - LZo; sgn = R(1); }
+            else if (n == n_free) { off = 0; sgn = R(0); }
+            else { off = (n - LZo) - 2 * (n - n_free); sgn = R(-1); }
             q = id + (long long)off * p.sz;
-            float fz = __ldg(p.jac + q) * (cv(6, q) * cur(f1, q) + cv(7, q) * cur(f2, q) + cv(8, q) * cur(f3, q));
+            R fz = __ldg(p.jac + q) * (cv(6, q) * cur(f1, q) + cv(7, q) * cur(f2, q) + cv(8, q) * cur(f3, q));
             vz[n] = sgn * fz;
           }
-          float DxTx = drp5<DX>(vx[0], vx[1], vx[2], vx[3], vx[4]);
-          float DyTy = drp5<DY>(vy[0], vy[1], vy[2], vy[3], vy[4]);
-          float DzTz = drp5<DZ>(vz[0], vz[1], vz[2], vz[3], vz[4]);
+          R DxTx = drp5<DX>(vx[0], vx[1], vx[2], vx[3], vx[4]);
+          R DyTy = drp5<DY>(vy[0], vy[1], vy[2], vy[3], vy[4]);
+          R DzTz = drp5<DZ>(vz[0], vz[1], vz[2], vz[3], vz[4]);
           h[c] = (DxTx + DyTy + DzTz) * slwjac;
         }
       }
     }
     // Hooke: normal, or vlow with low-order / converted dzV in the top 3 layers
     {
-      float dz[3] = {dv[2][0], dv[2][1], dv[2][2]};
+      R dz[3] = {dv[2][0], dv[2][1], dv[2][2]};
       if (p.free_top && k >= nk2 - 2) {
         const int nl = nk2 - k;
         if (nl == 0) {
@@ -316,7 +322,7 @@ __global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant_
           }
         }
       }
-      float G[3][3];
+      R G[3][3];
 #pragma unroll
       for (int vi = 0; vi < 3; vi++)
 #pragma unroll
@@ -325,17 +331,17 @@ __global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant_
     }
     // CFS-PML faces, with the free-surface terms on x/y faces at the top layer
     for (int fi = 0; fi < p.nface; fi++) {
-      const FaceP &fc = p.face[fi];
+      const FacePT<R> &fc = p.face[fi];
       if (!(i >= fc.lo[0] && i <= fc.hi[0] && j >= fc.lo[1] && j <= fc.hi[1] && k >= fc.lo[2] && k <= fc.hi[2])) continue;
       const int a = fc.axis;
-      const float *smat = nullptr;
+      const R *smat = nullptr;
       if (p.free_top && a < 2 && k == nk2) smat = (a == 0 ? p.matx : p.maty) + ((long long)j * p.ni + i) * 9;
       pml_face<MED>(p, fc, i, j, k, md, slw, m[a], dv[a], dtt[a], smat, m[2], hc, shot);
     }
 #pragma unroll
     for (int c = 0; c < 9; c++) h[c] += hc[c];
     if constexpr (WP == 0) {
-      float cc[9];
+      R cc[9];
 #pragma unroll
       for (int f = 0; f < 9; f++) cc[f] = cur(f, id);
       rk_store(p.stage, p.ca, p.cb, sf, id, cc, h, p.pre + woff, p.tmp_out ? p.tmp_out + woff : nullptr, p.end + woff,
@@ -380,7 +386,8 @@ __global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant_
 // -----------------------------------------------------------------------------------------
 // sources, stations, step counter
 // -----------------------------------------------------------------------------------------
-__global__ void k_source(const __grid_constant__ SrcP s) {
+template <typename R>
+__global__ void k_source(const __grid_constant__ SrcPT<R> s) {
   const int is = blockIdx.y;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (is >= s.nsrc || e >= s.ext_num[is]) return;
@@ -390,43 +397,51 @@ __global__ void k_source(const __grid_constant__ SrcP s) {
   const float *v = s.stf + (((long long)is * s.max_nt + (it - ib)) * 4 + s.stage) * 9;
   const int shot = s.src_shot[is];
   const long long id = s.ext_idx[(long long)is * s.max_ext + e] + (long long)shot * 9 * s.sf;
-  const float wv = s.ext_wv[(long long)is * s.max_ext + e];
-  const float wt = s.ext_wt[(long long)is * s.max_ext + e];
+  const R wv = s.ext_wv[(long long)is * s.max_ext + e];
+  const R wt = s.ext_wt[(long long)is * s.max_ext + e];
   for (int c = 0; c < 9; c++) {
-    float h;
-    if (c < 3) { if (!s.force) continue; h = v[c] * wv; }
-    else { if (!s.moment) continue; h = -v[c] * wt; }
+    R h;
+    if (c < 3) { if (!s.force) continue; h = R(v[c]) * wv; }
+    else { if (!s.moment) continue; h = -R(v[c]) * wt; }
     if (s.stage < 3) {
-      if (s.wave16)
-        atomicAdd(reinterpret_cast<__half *>(s.tmp_out) + c * s.sf + id, __float2half_rn(s.ca * h * s.wsc[18 * shot + 9 + c]));
-      else atomicAdd(s.tmp_out + c * s.sf + id, s.ca * h);
+      if constexpr (std::is_same<R, float>::value) {
+        if (s.wave16)
+          atomicAdd(reinterpret_cast<__half *>(s.tmp_out) + c * s.sf + id,
+                    __float2half_rn(s.ca * h * s.wsc[18 * shot + 9 + c]));
+        else atomicAdd(s.tmp_out + c * s.sf + id, s.ca * h);
+      } else {
+        atomicAdd(s.tmp_out + c * s.sf + id, s.ca * h);
+      }
     }
-    const float old = atomicAdd(s.end + c * s.sf + id, s.cb * h);
-    if (s.wave16 && s.stage == 3) atomic_max_abs(&s.amax[2 * shot + wgroup(c)], old + s.cb * h);
+    const R old = atomicAdd(s.end + c * s.sf + id, s.cb * h);
+    if constexpr (std::is_same<R, float>::value)
+      if (s.wave16 && s.stage == 3) atomic_max_abs(&s.amax[2 * shot + wgroup(c)], old + s.cb * h);
   }
 }
 
-__global__ void k_recv(const __grid_constant__ RecvP r) {
+template <typename R>
+__global__ void k_recv(const __grid_constant__ RecvPT<R> r) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= r.nshot * r.nsta * 9) return;
   const int it = *r.d_it;
   if (it < 0 || it >= r.nt_total) return;
   const int shot = t / (r.nsta * 9), sidx = (t / 9) % r.nsta, c = t % 9;
-  const float *pre = r.pre + (long long)shot * 9 * r.sf;
-  float v = 0.f;
+  const R *pre = r.pre + (long long)shot * 9 * r.sf;
+  R v = R(0);
 #pragma unroll
   for (int qn = 0; qn < 8; qn++) {
-    float w = r.w8[sidx * 8 + qn];
-    if (w != 0.f) v += w * __ldg(pre + c * r.sf + r.idx8[sidx * 8 + qn]);
+    const R w = r.w8[sidx * 8 + qn];
+    if (w != R(0)) v += w * __ldg(pre + c * r.sf + r.idx8[sidx * 8 + qn]);
   }
   if (nonfinite(v)) atomicOr(r.d_flag, kErrStationNonfinite);
-  r.seis[(((long long)shot * r.nsta + sidx) * 9 + c) * r.nt_total + it] = v;
+  r.seis[(((long long)shot * r.nsta + sidx) * 9 + c) * r.nt_total + it] = (float)v;
 }
 
 // PG_calcu_gpu (wav_t.cu:281-360) on the top physical plane, every shot: acceleration from the
 // step difference of V, displacement accumulated by the trapezoid rule in double (the
 // reference's 0.5 literal), running maxima of the components and magnitudes.
-__global__ void k_peak_motion(const __grid_constant__ PgP q) {
+template <typename R>
+__global__ void k_peak_motion(const __grid_constant__ PgPT<R> q) {
   const long long nij = (long long)q.ni * q.nj;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= nij * q.nshot) return;
@@ -434,38 +449,42 @@ __global__ void k_peak_motion(const __grid_constant__ PgP q) {
   const long long ij = t % nij;
   const int j = (int)(ij / q.ni), i = (int)(ij % q.ni);
   const long long idx = (long long)shot * 9 * q.sf + q.off_top + (long long)j * q.sx + i;
-  float v1[3], v0[3], a[3], d[3];
-  float *dis = q.dis + (long long)shot * 3 * nij + ij;
+  R v1[3], v0[3], a[3], d[3];
+  R *dis = q.dis + (long long)shot * 3 * nij + ij;
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     v1[c] = q.w_end[c * q.sf + idx];
     v0[c] = q.w_pre[c * q.sf + idx];
-    a[c] = fabsf((v1[c] - v0[c]) / q.dt);
-    d[c] = (float)((double)dis[c * nij] + 0.5 * (double)(v1[c] + v0[c]) * (double)q.dt);
+    a[c] = fabs((v1[c] - v0[c]) / R(q.dt));
+    d[c] = (R)((double)dis[c * nij] + 0.5 * (double)(v1[c] + v0[c]) * (double)q.dt);
     dis[c * nij] = d[c];
   }
-  const float val[15] = {sqrtf(v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2]),
-                         sqrtf(v1[0] * v1[0] + v1[1] * v1[1]),
-                         fabsf(v1[0]), fabsf(v1[1]), fabsf(v1[2]),
-                         sqrtf(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]),
-                         sqrtf(a[0] * a[0] + a[1] * a[1]),
-                         a[0], a[1], a[2],
-                         sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]),
-                         sqrtf(d[0] * d[0] + d[1] * d[1]),
-                         fabsf(d[0]), fabsf(d[1]), fabsf(d[2])};
+  const R val[15] = {sqrt(v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2]),
+                     sqrt(v1[0] * v1[0] + v1[1] * v1[1]),
+                     fabs(v1[0]), fabs(v1[1]), fabs(v1[2]),
+                     sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]),
+                     sqrt(a[0] * a[0] + a[1] * a[1]),
+                     a[0], a[1], a[2],
+                     sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]),
+                     sqrt(d[0] * d[0] + d[1] * d[1]),
+                     fabs(d[0]), fabs(d[1]), fabs(d[2])};
   float *pg = q.pg + (long long)shot * 15 * nij + ij;
 #pragma unroll
   for (int n = 0; n < 15; n++)
-    if (pg[n * nij] < val[n]) pg[n * nij] = val[n];
+    if (pg[n * nij] < (float)val[n]) pg[n * nij] = (float)val[n];
 }
 
-int launch_peak_motion(const PgP &q, cudaStream_t st) {
+template <typename R>
+int launch_peak_motion(const PgPT<R> &q, cudaStream_t st) {
   const long long n = (long long)q.ni * q.nj * q.nshot;
-  k_peak_motion<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(q);
+  k_peak_motion<R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(q);
   return 1;
 }
+template int launch_peak_motion<float>(const PgPT<float> &, cudaStream_t);
+template int launch_peak_motion<double>(const PgPT<double> &, cudaStream_t);
 
-__global__ void k_gather_box(const float *__restrict__ w, long long sf, long long sx, long long sz, long long off0,
+template <typename R>
+__global__ void k_gather_box(const R *__restrict__ w, long long sf, long long sx, long long sz, long long off0,
                              int3 start, int3 count, int3 stride, float *__restrict__ dst) {
   const long long per = (long long)count.x * count.y * count.z;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 9 * per; t += (long long)gridDim.x * blockDim.x) {
@@ -474,16 +493,21 @@ __global__ void k_gather_box(const float *__restrict__ w, long long sf, long lon
     const int i = start.x + (int)(r % count.x) * stride.x;
     const int j = start.y + (int)((r / count.x) % count.y) * stride.y;
     const int k = start.z + (int)(r / ((long long)count.x * count.y)) * stride.z;
-    dst[t] = w[c * sf + off0 + (long long)k * sz + (long long)j * sx + i];
+    dst[t] = (float)w[c * sf + off0 + (long long)k * sz + (long long)j * sx + i];
   }
 }
 
-void launch_gather_box(const float *w, long long sf, long long sx, long long sz, long long off0, const int start[3],
+template <typename R>
+void launch_gather_box(const R *w, long long sf, long long sx, long long sz, long long off0, const int start[3],
                        const int count[3], const int stride[3], float *dst, cudaStream_t st) {
-  k_gather_box<<<592, 256, 0, st>>>(w, sf, sx, sz, off0, make_int3(start[0], start[1], start[2]),
-                                    make_int3(count[0], count[1], count[2]),
-                                    make_int3(stride[0], stride[1], stride[2]), dst);
+  k_gather_box<R><<<592, 256, 0, st>>>(w, sf, sx, sz, off0, make_int3(start[0], start[1], start[2]),
+                                       make_int3(count[0], count[1], count[2]),
+                                       make_int3(stride[0], stride[1], stride[2]), dst);
 }
+template void launch_gather_box<float>(const float *, long long, long long, long long, long long, const int[3],
+                                       const int[3], const int[3], float *, cudaStream_t);
+template void launch_gather_box<double>(const double *, long long, long long, long long, long long, const int[3],
+                                        const int[3], const int[3], float *, cudaStream_t);
 
 __global__ void k_advance(int *d_it) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *d_it += 1;
@@ -491,7 +515,8 @@ __global__ void k_advance(int *d_it) {
 
 // Repack one field from the reference host layout (3 ghosts, nx = ni+6) into the device
 // layout. mode 1 converts density to 1/rho (md_rho_to_slow, md_t.cu:622-637).
-__global__ void k_repack_in(const float *__restrict__ src, float *__restrict__ dst, int ni, int nj, int nk,
+template <typename R>
+__global__ void k_repack_in(const float *__restrict__ src, R *__restrict__ dst, int ni, int nj, int nk,
                             long long sx, long long sz, long long off0, int mode, int ghosts) {
   const long long nxr = ni + 6, nyr = nj + 6;
   const long long total = nxr * nyr * (nk + 6);
@@ -501,12 +526,13 @@ __global__ void k_repack_in(const float *__restrict__ src, float *__restrict__ d
     bool inner = i >= 0 && i < ni && j >= 0 && j < nj && k >= 0 && k < nk;
     if (!ghosts && !inner) continue;
     float v = src[t];
-    if (mode == 1) v = v > 1e-10f ? 1.0f / v : 0.0f;
-    dst[off0 + (long long)k * sz + (long long)j * sx + i] = v;
+    if (mode == 1) v = v > 1e-10f ? 1.0f / v : 0.0f;  // 1/rho in float, as md_rho_to_slow
+    dst[off0 + (long long)k * sz + (long long)j * sx + i] = (R)v;
   }
 }
 
-__global__ void k_repack_out(const float *__restrict__ src, float *__restrict__ dst, int ni, int nj, int nk,
+template <typename R>
+__global__ void k_repack_out(const R *__restrict__ src, float *__restrict__ dst, int ni, int nj, int nk,
                              long long sx, long long sz, long long off0) {
   const long long nxr = ni + 6, nyr = nj + 6;
   const long long total = nxr * nyr * (nk + 6);
@@ -514,40 +540,42 @@ __global__ void k_repack_out(const float *__restrict__ src, float *__restrict__ 
     int ir = (int)(t % nxr), jr = (int)((t / nxr) % nyr), kr = (int)(t / (nxr * nyr));
     int i = ir - 3, j = jr - 3, k = kr - 3;
     bool inner = i >= 0 && i < ni && j >= 0 && j < nj && k >= 0 && k < nk;
-    dst[t] = inner ? src[off0 + (long long)k * sz + (long long)j * sx + i] : 0.0f;
+    dst[t] = inner ? (float)src[off0 + (long long)k * sz + (long long)j * sx + i] : 0.0f;
   }
 }
 
 // -----------------------------------------------------------------------------------------
 // launch tables
 // -----------------------------------------------------------------------------------------
-typedef void (*BulkFn)(StageP, int);
-
-template <int MED>
-static void launch_bulk_med(const StageP &p, int nzc, dim3 grid, cudaStream_t st) {
+template <int MED, typename R>
+static void launch_bulk_med(const StagePT<R> &p, int nzc, dim3 grid, cudaStream_t st) {
   const int code = p.dir[0] | (p.dir[1] << 1) | (p.dir[2] << 2);
-  dim3 block(TX, TY);
+  dim3 block(TX, DirectTile<R>::TYB);
   switch (code) {
-#define CASE(c)                                                                                   \
-  case c:                                                                                         \
-    k_stage_bulk<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1><<<grid, block, 0, st>>>(p, nzc); \
+#define CASE(c)                                                                                      \
+  case c:                                                                                            \
+    k_stage_bulk<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, R><<<grid, block, 0, st>>>(p, nzc); \
     break;
     CASE(0) CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7)
 #undef CASE
   }
 }
 
-int launch_stage_bulk(int med, const StageP &p, int nzc, cudaStream_t st) {
+template <typename R>
+int launch_stage_bulk(int med, const StagePT<R> &p, int nzc, cudaStream_t st) {
   if (p.nbulk <= 0) return 0;
-  dim3 grid((p.ni + TX - 1) / TX, (p.nj + TY - 1) / TY, (p.nbulk + nzc - 1) / nzc);
+  constexpr int ty = DirectTile<R>::TYB;
+  dim3 grid((p.ni + TX - 1) / TX, (p.nj + ty - 1) / ty, (p.nbulk + nzc - 1) / nzc);
   if (med == MED_ISO) launch_bulk_med<MED_ISO>(p, nzc, grid, st);
   else if (med == MED_VTI) launch_bulk_med<MED_VTI>(p, nzc, grid, st);
   else launch_bulk_med<MED_ANISO>(p, nzc, grid, st);
   return 1;
 }
+template int launch_stage_bulk<float>(int, const StagePT<float> &, int, cudaStream_t);
+template int launch_stage_bulk<double>(int, const StagePT<double> &, int, cudaStream_t);
 
 template <int MED, typename TC, int WP>
-static void launch_surface_med(const StageP &p, dim3 grid, dim3 block, cudaStream_t st) {
+static void launch_surface_med(const StagePT<real_of<TC>> &p, dim3 grid, dim3 block, cudaStream_t st) {
   switch (p.dir[0] | (p.dir[1] << 1) | (p.dir[2] << 2)) {
 #define CASE(c)                                                                                          \
   case c:                                                                                                \
@@ -559,7 +587,7 @@ static void launch_surface_med(const StageP &p, dim3 grid, dim3 block, cudaStrea
 }
 
 template <typename TC, int WP>
-static void launch_surface_tc(int med, const StageP &p, dim3 grid, dim3 block, cudaStream_t st) {
+static void launch_surface_tc(int med, const StagePT<real_of<TC>> &p, dim3 grid, dim3 block, cudaStream_t st) {
   if (med == MED_ISO) launch_surface_med<MED_ISO, TC, WP>(p, grid, block, st);
   else if (med == MED_VTI) launch_surface_med<MED_VTI, TC, WP>(p, grid, block, st);
   else launch_surface_med<MED_ANISO, TC, WP>(p, grid, block, st);
@@ -576,6 +604,14 @@ int launch_stage_surface(int med, int coef_type, int wave16, const StageP &p, cu
   else if (coef_type == COEF_F16) launch_surface_tc<__half, 0>(med, p, grid, block, st);
   else if (coef_type == COEF_BF16) launch_surface_tc<__nv_bfloat16, 0>(med, p, grid, block, st);
   else launch_surface_tc<float, 0>(med, p, grid, block, st);
+  return 1;
+}
+
+int launch_stage_surface64(int med, const StagePT<double> &p, cudaStream_t st) {
+  if (p.nbulk >= p.nk) return 0;
+  dim3 block(32, 4);
+  dim3 grid((p.ni + 31) / 32, (p.nj + 3) / 4, (p.nk - p.nbulk) * p.nshot);
+  launch_surface_tc<double, 0>(med, p, grid, block, st);
   return 1;
 }
 
@@ -760,34 +796,50 @@ void launch_coef_to16(int coef_type, const float *src, void *dst, long long n, f
     k_coef_to16<__nv_bfloat16><<<1184, 256, 0, st>>>(src, (__nv_bfloat16 *)dst, n, scale, offset, field);
 }
 
-int launch_source(const SrcP &s, cudaStream_t st) {
+template <typename R>
+int launch_source(const SrcPT<R> &s, cudaStream_t st) {
   if (s.nsrc <= 0) return 0;
   dim3 block(128);
   dim3 grid((s.max_ext + 127) / 128, s.nsrc);
-  k_source<<<grid, block, 0, st>>>(s);
+  k_source<R><<<grid, block, 0, st>>>(s);
   return 1;
 }
+template int launch_source<float>(const SrcPT<float> &, cudaStream_t);
+template int launch_source<double>(const SrcPT<double> &, cudaStream_t);
 
-int launch_recv(const RecvP &r, cudaStream_t st) {
+template <typename R>
+int launch_recv(const RecvPT<R> &r, cudaStream_t st) {
   if (r.nsta <= 0) return 0;
   int n = r.nshot * r.nsta * 9;
-  k_recv<<<(n + 127) / 128, 128, 0, st>>>(r);
+  k_recv<R><<<(n + 127) / 128, 128, 0, st>>>(r);
   return 1;
 }
+template int launch_recv<float>(const RecvPT<float> &, cudaStream_t);
+template int launch_recv<double>(const RecvPT<double> &, cudaStream_t);
 
 int launch_advance(int *d_it, cudaStream_t st) {
   k_advance<<<1, 32, 0, st>>>(d_it);
   return 1;
 }
 
-void launch_repack_in(const float *src, float *dst, int ni, int nj, int nk, long long sx, long long sz, long long off0,
+template <typename R>
+void launch_repack_in(const float *src, R *dst, int ni, int nj, int nk, long long sx, long long sz, long long off0,
                       int mode, int ghosts, cudaStream_t st) {
-  k_repack_in<<<1184, 256, 0, st>>>(src, dst, ni, nj, nk, sx, sz, off0, mode, ghosts);
+  k_repack_in<R><<<1184, 256, 0, st>>>(src, dst, ni, nj, nk, sx, sz, off0, mode, ghosts);
 }
+template void launch_repack_in<float>(const float *, float *, int, int, int, long long, long long, long long, int, int,
+                                      cudaStream_t);
+template void launch_repack_in<double>(const float *, double *, int, int, int, long long, long long, long long, int,
+                                       int, cudaStream_t);
 
-void launch_repack_out(const float *src, float *dst, int ni, int nj, int nk, long long sx, long long sz, long long off0,
+template <typename R>
+void launch_repack_out(const R *src, float *dst, int ni, int nj, int nk, long long sx, long long sz, long long off0,
                        cudaStream_t st) {
-  k_repack_out<<<1184, 256, 0, st>>>(src, dst, ni, nj, nk, sx, sz, off0);
+  k_repack_out<R><<<1184, 256, 0, st>>>(src, dst, ni, nj, nk, sx, sz, off0);
 }
+template void launch_repack_out<float>(const float *, float *, int, int, int, long long, long long, long long,
+                                       cudaStream_t);
+template void launch_repack_out<double>(const double *, float *, int, int, int, long long, long long, long long,
+                                        cudaStream_t);
 
 }  // namespace cgfd

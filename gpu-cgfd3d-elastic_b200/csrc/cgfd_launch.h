@@ -5,7 +5,8 @@
 
 namespace cgfd {
 
-struct StageP;
+template <typename R> struct StagePT;
+using StageP = StagePT<float>;
 struct TmaP;
 
 // storage type of the coefficient array
@@ -13,11 +14,13 @@ struct TmaP;
 enum { COEF_F32 = 0, COEF_F16 = 1, COEF_BF16 = 2, COEF_U16 = 3 };
 
 // Source injection of one stage (sv_curv_col_el_gpu.cu:227-301), applied to tmp/end.
-struct SrcP {
+// R: real type of the wavefield levels (float; double in the FP64 build).
+template <typename R>
+struct SrcPT {
   int nsrc, max_ext, max_nt;
   int force, moment;
   int stage;
-  float ca, cb;
+  R ca, cb;
   const int *it_begin;         // [nsrc]
   const int *ext_num;          // [nsrc]
   const long long *ext_idx;    // [nsrc][max_ext] device-layout index
@@ -25,48 +28,58 @@ struct SrcP {
   const float *ext_wt;         // [nsrc][max_ext] coef / jac
   const float *stf;            // [nsrc][max_nt][4][9]: fx fy fz mxx myy mzz myz mxz mxy
   const int *src_shot;         // [nsrc] wavefield (shot) each source acts on
-  float *tmp_out;              // __half when wave16
-  float *end;
+  R *tmp_out;                  // __half when wave16
+  R *end;
   long long sf;
   const int *d_it;
   int wave16;                  // FP16 stage levels: tmp_out holds scaled __half
   const float *wsc;            // [nshot][18] scale / inverse scale of this step (wave16)
   unsigned int *amax;          // [nshot][2] max |w_end| per group, collected at stage 3 (wave16)
 };
+using SrcP = SrcPT<float>;
 
 // Strided sub-box of the 9 wavefield components into dst[9][count_k][count_j][count_i]
 // (io_snap_pack_buff, io_funcs.cu:1569-1595, all components in one launch).
-void launch_gather_box(const float *w, long long sf, long long sx, long long sz, long long off0, const int start[3],
+template <typename R>
+void launch_gather_box(const R *w, long long sf, long long sx, long long sz, long long off0, const int start[3],
                        const int count[3], const int stride[3], float *dst, cudaStream_t st);
 
 // Free-surface peak ground motion after each time step (PG_calcu_gpu, wav_t.cu:281-360).
-struct PgP {
+template <typename R>
+struct PgPT {
   int ni, nj, nshot;
   long long sx, sf, off_top;   // off_top: device index of physical (0, 0, nk-1)
-  const float *w_end, *w_pre;  // the step's new and old state
+  const R *w_end, *w_pre;      // the step's new and old state
   float *pg;                   // [nshot][15][nj][ni]
-  float *dis;                  // [nshot][3][nj][ni] displacement accumulator
+  R *dis;                      // [nshot][3][nj][ni] displacement accumulator
   float dt;
 };
-int launch_peak_motion(const PgP &q, cudaStream_t st);
+using PgP = PgPT<float>;
+template <typename R>
+int launch_peak_motion(const PgPT<R> &q, cudaStream_t st);
 
 // Station sampling of w_pre (io_funcs.cu:1624-1666).
-struct RecvP {
+template <typename R>
+struct RecvPT {
   int nsta;
   int nshot;                   // every shot is sampled at the same stations
   int nt_total;
   const long long *idx8;       // [nsta][8] device-layout corner index
   const float *w8;             // [nsta][8] trilinear weights (reference corner usage)
-  const float *pre;
+  const R *pre;
   long long sf;
   float *seis;                 // [nshot][nsta][9][nt_total]
   const int *d_it;
   int *d_flag;
 };
+using RecvP = RecvPT<float>;
 
 // Each launcher returns the number of kernels it launched (0 or 1).
-int launch_stage_bulk(int med, const StageP &p, int nzc, cudaStream_t st);
+template <typename R>
+int launch_stage_bulk(int med, const StagePT<R> &p, int nzc, cudaStream_t st);
 int launch_stage_surface(int med, int coef_type, int wave16, const StageP &p, cudaStream_t st);
+// FP64 build: the surface slab with double storage and arithmetic
+int launch_stage_surface64(int med, const StagePT<double> &p, cudaStream_t st);
 // TMA-pipelined bulk kernel: tile height, one-time function attributes, launch.
 // wave16: FP16 stage levels (requires COEF_F16).
 int tma_tile_y(int med);
@@ -96,12 +109,17 @@ void launch_coef_minmax(const float *src, int ni, int nj, int nk, long long sx, 
 float coef_key_to_float(unsigned int key);
 void launch_coef_to16(int coef_type, const float *src, void *dst, long long n, float scale, float offset, int field,
                       cudaStream_t st);
-int launch_source(const SrcP &s, cudaStream_t st);
-int launch_recv(const RecvP &r, cudaStream_t st);
+template <typename R>
+int launch_source(const SrcPT<R> &s, cudaStream_t st);
+template <typename R>
+int launch_recv(const RecvPT<R> &r, cudaStream_t st);
 int launch_advance(int *d_it, cudaStream_t st);
-void launch_repack_in(const float *src, float *dst, int ni, int nj, int nk, long long sx, long long sz,
+// reference layout (float, 3 ghosts) -> device layout of real type R, and back
+template <typename R>
+void launch_repack_in(const float *src, R *dst, int ni, int nj, int nk, long long sx, long long sz,
                       long long off0, int mode, int ghosts, cudaStream_t st);
-void launch_repack_out(const float *src, float *dst, int ni, int nj, int nk, long long sx, long long sz,
+template <typename R>
+void launch_repack_out(const R *src, float *dst, int ni, int nj, int nk, long long sx, long long sz,
                        long long off0, cudaStream_t st);
 
 }  // namespace cgfd

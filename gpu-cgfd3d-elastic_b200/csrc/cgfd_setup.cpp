@@ -29,7 +29,7 @@ void validate_desc(const cgfd_problem_desc *d) {
   if (!d->metric || !d->medium) throw Error(CGFD_ERR_INVALID, "metric and medium arrays are required");
   if (!(d->dt > 0.0f)) throw Error(CGFD_ERR_INVALID, "dt must be > 0");
   if (d->nt_total < 1) throw Error(CGFD_ERR_INVALID, "nt_total must be >= 1");
-  if (d->precision < CGFD_PREC_FP32 || d->precision > CGFD_PREC_FP16_WAVE)
+  if (d->precision < CGFD_PREC_FP32 || d->precision > CGFD_PREC_FP64)
     throw Error(CGFD_ERR_INVALID, "unknown precision");
   if (d->free_top && d->pml[2][1].enable) throw Error(CGFD_ERR_INVALID, "the top face cannot be both free and PML");
   for (int a = 0; a < 3; a++)

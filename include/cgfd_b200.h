@@ -61,6 +61,10 @@ extern "C" {
 #define CGFD_PREC_U16_COEF   3  /* coefficients 16-bit fixed point over each field's range    */
 #define CGFD_PREC_FP16_WAVE  4  /* U16 coefficients + RK stage wavefields FP16 (dynamic per-
                                    step scale); the solution levels stay FP32                */
+#define CGFD_PREC_FP64       5  /* FP64 build of the same kernels: wavefield, coefficients, PML
+                                   auxiliaries and all arithmetic in double (the reference
+                                   each precision mode's seismogram error is measured against;
+                                   direct-load bulk kernel, not a production mode)            */
 
 /* status codes */
 #define CGFD_OK               0
