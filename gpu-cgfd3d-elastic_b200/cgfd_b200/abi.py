@@ -257,6 +257,10 @@ def lib():
         "cgfd_station_info": (C.c_int, [P, P, P]),
         "cgfd_get_wavefield": (C.c_int, [P, P]),
         "cgfd_get_peak_motion": (C.c_int, [P, C.c_int, P]),
+        "cgfd_set_line_receivers": (C.c_int, [P, C.c_int, P]),
+        "cgfd_get_line_seismograms": (C.c_int, [P, P]),
+        "cgfd_set_slices": (C.c_int, [P, C.c_int, P, C.c_int, P, C.c_int, P, C.c_int]),
+        "cgfd_get_slices": (C.c_int, [P, C.c_int, C.c_int, P]),
         "cgfd_get_wavefield_box": (C.c_int, [P, C.c_int, P, P, P, P]),
         "cgfd_set_wavefield": (C.c_int, [P, P]),
         "cgfd_device_bytes": (C.c_size_t, [P]),
@@ -386,6 +390,37 @@ class Simulation:
         check(lib().cgfd_get_wavefield_box(self.h, int(shot), a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data,
                                            out.ctypes.data))
         return out
+
+    def set_line_receivers(self, ijk):
+        """cgfd_set_line_receivers: grid points [n, 3] (physical 0-based i, j, k)."""
+        a = np.ascontiguousarray(np.asarray(ijk, np.int32).reshape(-1, 3))
+        self._line_n = a.shape[0]
+        check(lib().cgfd_set_line_receivers(self.h, int(a.shape[0]), a.ctypes.data))
+
+    def line_seismograms(self):
+        """[npts, 9, nt_total], or [nshot, npts, 9, nt_total] for a batch."""
+        n = getattr(self, "_line_n", 0)
+        out = np.zeros((self.nshot, n, 9, self.problem.nt_total), np.float32)
+        check(lib().cgfd_get_line_seismograms(self.h, out.ctypes.data))
+        return out[0] if self.nshot == 1 else out
+
+    def set_slices(self, ix=(), iy=(), iz=(), ring_steps=16):
+        """cgfd_set_slices: x / y / z plane indices (physical 0-based), device ring of steps."""
+        a = [np.ascontiguousarray(np.asarray(v, np.int32)) for v in (ix, iy, iz)]
+        self._slices = tuple(len(v) for v in a)
+        check(lib().cgfd_set_slices(self.h, len(a[0]), a[0].ctypes.data, len(a[1]), a[1].ctypes.data,
+                                    len(a[2]), a[2].ctypes.data, int(ring_steps)))
+
+    def slices(self, it, shot=0):
+        """(x [nx, 9, nk, nj], y [ny, 9, nk, ni], z [nz, 9, nj, ni]) planes of step `it`."""
+        p = self.problem
+        nx, ny, nz = self._slices
+        sizes = [nx * 9 * p.nk * p.nj, ny * 9 * p.nk * p.ni, nz * 9 * p.nj * p.ni]
+        out = np.zeros(sum(sizes), np.float32)
+        check(lib().cgfd_get_slices(self.h, int(shot), int(it), out.ctypes.data))
+        a, b = sizes[0], sizes[0] + sizes[1]
+        return (out[:a].reshape(nx, 9, p.nk, p.nj), out[a:b].reshape(ny, 9, p.nk, p.ni),
+                out[b:].reshape(nz, 9, p.nj, p.ni))
 
     def peak_motion(self, shot=0):
         """[15, ny, nx] free-surface peak ground motion (PGV, PGVh, PGVx..z, PGA.., PGD..)."""

@@ -149,10 +149,11 @@ MEDIUM_NAMES = {
 MEDIUM_TYPES = {2: "elastic_iso", 3: "elastic_vti", 4: "elastic_aniso"}
 
 
-def write_case(d, p, nsteps, metric="calculate", check_stability=1, snapshots=None):
+def write_case(d, p, nsteps, metric="calculate", check_stability=1, snapshots=None, extra=None):
     """Writes a full reference-format input set for problem `p` into directory `d`:
     par.json, grid/coord_px0_py0_pz0.nc, media/media_px0_py0_pz0.nc, src.src, station.list
-    (and grid/metric_px0_py0_pz0.nc when metric == "import"). Returns the par.json path."""
+    (and grid/metric_px0_py0_pz0.nc when metric == "import"); `extra` adds par-file entries
+    (e.g. "receiver_line", "slice"). Returns the par.json path."""
     import json
     import os
     os.makedirs(os.path.join(d, "grid"), exist_ok=True)
@@ -191,6 +192,8 @@ def write_case(d, p, nsteps, metric="calculate", check_stability=1, snapshots=No
         par["boundary_z_top"] = {"free": "timg"}
     if snapshots:
         par["snapshot"] = list(snapshots)  # entries in the par-file form (1-based grid_index_start)
+    if extra:
+        par.update(extra)
     path = os.path.join(d, "par.json")
     with open(path, "w") as f:
         json.dump(par, f, indent=2)

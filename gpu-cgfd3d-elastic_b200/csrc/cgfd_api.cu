@@ -174,6 +174,15 @@ struct cgfd_problem {
   cgfd::RecvHost rec;
   long long *d_idx8 = nullptr;
   float *d_w8 = nullptr, *d_seis = nullptr;
+  // line receivers (grid points sampled like stations, weight 1 at corner 0)
+  int nline = 0;
+  long long *d_line_idx8 = nullptr;
+  float *d_line_w8 = nullptr, *d_line_seis = nullptr;
+  // slices: plane indices (x, then y, then z), device ring of ring steps
+  int nslx = 0, nsly = 0, nslz = 0, slice_ring = 0;
+  long long slice_per_shot = 0;
+  int *d_slice_idx = nullptr;
+  float *d_slices = nullptr;
 
   int *d_it = nullptr, *d_flag = nullptr;
   int it = 0;
@@ -297,6 +306,29 @@ struct cgfd_problem {
     return p;
   }
 
+  // Line receivers and slices: samples of w_pre at the start of the step, after the stations
+  // (io_line_keep and io_slice_nc_put follow io_recv_keep, drv_rk_curv_col.cu:199-206).
+  template <typename R>
+  int enqueue_outputs(int step) {
+    int n = 0;
+    if (nline > 0) {
+      cgfd::RecvPT<R> r;
+      r.nsta = nline; r.nshot = nshot; r.nt_total = nt_total; r.idx8 = d_line_idx8; r.w8 = d_line_w8;
+      r.pre = rptr<R>(wbuf[step & 1]); r.sf = sf; r.seis = d_line_seis; r.d_it = d_it; r.d_flag = d_flag;
+      n += timed(6, [&] { return cgfd::launch_recv(r, stream); });
+    }
+    if (slice_per_shot > 0) {
+      cgfd::SliceP<R> q;
+      q.ni = ni; q.nj = nj; q.nk = nk; q.nshot = nshot;
+      q.sx = sx; q.sz = sz; q.sf = sf; q.off0 = off0;
+      q.pre = rptr<R>(wbuf[step & 1]);
+      q.nxs = nslx; q.nys = nsly; q.nzs = nslz; q.idx = d_slice_idx;
+      q.ring = d_slices; q.ring_steps = slice_ring; q.per_shot = slice_per_shot; q.d_it = d_it;
+      n += timed(6, [&] { return cgfd::launch_slices(q, stream); });
+    }
+    return n;
+  }
+
   // One time step of the FP64 build: the same kernels instantiated in double (direct-load bulk
   // kernel, surface slab, sources, stations, peak motion), launched in the same order.
   int enqueue_step64(int step) {
@@ -308,6 +340,7 @@ struct cgfd_problem {
       r.pre = rptr<double>(wbuf[step & 1]); r.sf = sf; r.seis = d_seis; r.d_it = d_it; r.d_flag = d_flag;
       n += timed(6, [&] { return cgfd::launch_recv(r, st); });
     }
+    n += enqueue_outputs<double>(step);
     for (int s = 0; s < 4; s++) {
       const cgfd::StagePT<double> p = stage_params_t<double>(step, s);
       n += timed(s, [&] { return cgfd::launch_stage_bulk(med, p, nzc, st); });
@@ -346,6 +379,7 @@ struct cgfd_problem {
       r.pre = wbuf[step & 1]; r.sf = sf; r.seis = d_seis; r.d_it = d_it; r.d_flag = d_flag;
       n += timed(6, [&] { return cgfd::launch_recv(r, st); });
     }
+    n += enqueue_outputs<float>(step);
     if (wave16)
       n += timed(7, [&] { return cgfd::launch_wave_scale(d_amax, d_srcb, d_it, nt_total, nshot, d_wsc, st); });
     for (int s = 0; s < 4; s++) {
@@ -443,6 +477,7 @@ struct cgfd_problem {
       dfree(d_it_begin, st); dfree(d_ext_num, st); dfree(d_src_shot, st); dfree(d_ext_idx, st); dfree(d_ext_wv, st);
       dfree(d_ext_wt, st); dfree(d_wsc, st); dfree(d_srcb, st); dfree(d_amax, st); dfree(d_tiles, st); dfree(d_pg, st);
       dfree(d_dis, st); dfree(d_box, st); dfree(d_stf, st); dfree(d_idx8, st); dfree(d_w8, st); dfree(d_seis, st);
+      dfree(d_line_idx8, st); dfree(d_line_w8, st); dfree(d_line_seis, st); dfree(d_slice_idx, st); dfree(d_slices, st);
       dfree(d_it, st); dfree(d_flag, st);
       cudaStreamSynchronize(st);
     }
@@ -1013,6 +1048,8 @@ void reset_state(cgfd_problem *p) {
   for (auto &f : p->faces) CK(cudaMemsetAsync(f.aux, 0, E * 3 * 9 * f.n * p->nshot, p->stream));
   if (p->rec.n > 0)
     CK(cudaMemsetAsync(p->d_seis, 0, sizeof(float) * p->rec.n * 9 * p->nt_total * p->nshot, p->stream));
+  if (p->nline > 0)
+    CK(cudaMemsetAsync(p->d_line_seis, 0, sizeof(float) * p->nline * 9 * p->nt_total * p->nshot, p->stream));
   if (p->d_pg) {
     const size_t nij = (size_t)p->ni * p->nj * p->nshot;
     CK(cudaMemsetAsync(p->d_pg, 0, sizeof(float) * 15 * nij, p->stream));
@@ -1351,6 +1388,108 @@ int cgfd_get_wavefield_shot_noalloc(cgfd_problem *p, int shot, float *out) {
                            cudaMemcpyDeviceToHost, p->stream));
       }
     CK(cudaStreamSynchronize(p->stream));
+  });
+}
+
+int cgfd_set_line_receivers(cgfd_problem *p, int npts, const int *ijk) {
+  if (!p || npts < 0 || (npts > 0 && !ijk)) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
+  for (int r = 0; r < npts; r++)
+    if (ijk[3 * r] < 0 || ijk[3 * r] >= p->ni || ijk[3 * r + 1] < 0 || ijk[3 * r + 1] >= p->nj || ijk[3 * r + 2] < 0 ||
+        ijk[3 * r + 2] >= p->nk) {
+      set_err("line receiver " + std::to_string(r) + " lies outside the physical grid");
+      return CGFD_ERR_INVALID;
+    }
+  return guarded([&] {
+    CK(cudaSetDevice(p->device));
+    CK(cudaStreamSynchronize(p->stream));
+    dfree(p->d_line_idx8, p->stream); dfree(p->d_line_w8, p->stream); dfree(p->d_line_seis, p->stream);
+    p->d_line_idx8 = nullptr; p->d_line_w8 = nullptr; p->d_line_seis = nullptr;
+    p->bytes -= (size_t)p->nline * (8 * (sizeof(long long) + sizeof(float)) + 9 * p->nt_total * p->nshot * sizeof(float));
+    p->nline = 0;
+    if (npts > 0) {
+      std::vector<long long> idx((size_t)npts * 8);
+      std::vector<float> w((size_t)npts * 8, 0.f);
+      for (int r = 0; r < npts; r++) {
+        const long long id = p->didx(ijk[3 * r], ijk[3 * r + 1], ijk[3 * r + 2]);
+        for (int q = 0; q < 8; q++) idx[(size_t)r * 8 + q] = id;
+        w[(size_t)r * 8] = 1.f;
+      }
+      p->d_line_idx8 = dmalloc<long long>(idx.size(), p->bytes, p->stream);
+      p->d_line_w8 = dmalloc<float>(w.size(), p->bytes, p->stream);
+      p->d_line_seis = dmalloc<float>((size_t)npts * 9 * p->nt_total * p->nshot, p->bytes, p->stream);
+      CK(cudaMemcpy(p->d_line_idx8, idx.data(), idx.size() * sizeof(long long), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(p->d_line_w8, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice));
+      CK(cudaMemset(p->d_line_seis, 0, sizeof(float) * npts * 9 * p->nt_total * p->nshot));
+      p->nline = npts;
+    }
+    for (int s = 0; s < 8; s++)
+      if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }
+  });
+}
+
+int cgfd_get_line_seismograms(cgfd_problem *p, float *out) {
+  if (!p || !out) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(p->device));
+    CK(cudaStreamSynchronize(p->stream));
+    if (p->nline > 0)
+      CK(cudaMemcpy(out, p->d_line_seis, sizeof(float) * p->nline * 9 * p->nt_total * p->nshot, cudaMemcpyDeviceToHost));
+  });
+}
+
+int cgfd_set_slices(cgfd_problem *p, int nx, const int *ix, int ny, const int *iy, int nz, const int *iz,
+                    int ring_steps) {
+  if (!p || nx < 0 || ny < 0 || nz < 0 || (nx && !ix) || (ny && !iy) || (nz && !iz) ||
+      (nx + ny + nz > 0 && ring_steps < 1)) {
+    set_err("invalid argument");
+    return CGFD_ERR_INVALID;
+  }
+  for (int s = 0; s < nx; s++)
+    if (ix[s] < 0 || ix[s] >= p->ni) { set_err("x slice index outside the physical grid"); return CGFD_ERR_INVALID; }
+  for (int s = 0; s < ny; s++)
+    if (iy[s] < 0 || iy[s] >= p->nj) { set_err("y slice index outside the physical grid"); return CGFD_ERR_INVALID; }
+  for (int s = 0; s < nz; s++)
+    if (iz[s] < 0 || iz[s] >= p->nk) { set_err("z slice index outside the physical grid"); return CGFD_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(p->device));
+    CK(cudaStreamSynchronize(p->stream));
+    dfree(p->d_slice_idx, p->stream); dfree(p->d_slices, p->stream);
+    p->d_slice_idx = nullptr; p->d_slices = nullptr;
+    p->bytes -= (size_t)(p->nslx + p->nsly + p->nslz) * sizeof(int) +
+                (size_t)p->slice_ring * p->nshot * p->slice_per_shot * sizeof(float);
+    p->nslx = p->nsly = p->nslz = p->slice_ring = 0;
+    p->slice_per_shot = 0;
+    const long long per = 9LL * ((long long)nx * p->nk * p->nj + (long long)ny * p->nk * p->ni + (long long)nz * p->nj * p->ni);
+    if (per > 0) {
+      std::vector<int> idx;
+      idx.insert(idx.end(), ix, ix + nx);
+      idx.insert(idx.end(), iy, iy + ny);
+      idx.insert(idx.end(), iz, iz + nz);
+      p->d_slice_idx = dmalloc<int>(idx.size(), p->bytes, p->stream);
+      CK(cudaMemcpy(p->d_slice_idx, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice));
+      p->d_slices = dmalloc<float>((size_t)ring_steps * p->nshot * per, p->bytes, p->stream);
+      p->nslx = nx; p->nsly = ny; p->nslz = nz;
+      p->slice_ring = ring_steps;
+      p->slice_per_shot = per;
+    }
+    for (int s = 0; s < 8; s++)
+      if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }
+  });
+}
+
+int cgfd_get_slices(cgfd_problem *p, int shot, int it, float *out) {
+  if (!p || !out || shot < 0 || shot >= p->nshot) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
+  if (p->slice_per_shot <= 0) { set_err("no slices are set"); return CGFD_ERR_INVALID; }
+  if (it < 0 || it >= p->it || it < p->it - p->slice_ring) {
+    set_err("step " + std::to_string(it) + " is not in the slice ring (steps " +
+            std::to_string(std::max(0, p->it - p->slice_ring)) + " .. " + std::to_string(p->it - 1) + ")");
+    return CGFD_ERR_INVALID;
+  }
+  return guarded([&] {
+    CK(cudaSetDevice(p->device));
+    CK(cudaStreamSynchronize(p->stream));
+    const size_t off = ((size_t)(it % p->slice_ring) * p->nshot + shot) * p->slice_per_shot;
+    CK(cudaMemcpy(out, p->d_slices + off, sizeof(float) * p->slice_per_shot, cudaMemcpyDeviceToHost));
   });
 }
 

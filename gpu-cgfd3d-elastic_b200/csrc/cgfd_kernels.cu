@@ -14,6 +14,8 @@
 // k_source: moment/force injection over the smoothed points (sv_curv_col_el_gpu.cu:227-301),
 //   applied to tmp/end with the stage's RK weights.
 // k_recv: trilinear station sampling of w_pre for all stations (io_funcs.cu:1624-1666).
+#include <algorithm>
+
 #include "cgfd_dev.cuh"
 #include "cgfd_launch.h"
 #include "cgfd_tma.cuh"
@@ -508,6 +510,56 @@ template void launch_gather_box<float>(const float *, long long, long long, long
                                        const int[3], const int[3], float *, cudaStream_t);
 template void launch_gather_box<double>(const double *, long long, long long, long long, long long, const int[3],
                                         const int[3], const int[3], float *, cudaStream_t);
+
+template <typename R>
+__global__ void k_slices(const __grid_constant__ SliceP<R> q) {
+  const int it = *q.d_it;
+  const long long total = q.per_shot * q.nshot;
+  const long long px = (long long)q.nk * q.nj, py = (long long)q.nk * q.ni, pz = (long long)q.nj * q.ni;
+  const long long ex = 9 * px * q.nxs, ey = 9 * py * q.nys;
+  float *out = q.ring + (long long)(it % q.ring_steps) * total;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int shot = (int)(t / q.per_shot);
+    long long r = t % q.per_shot;
+    int i, j, k, c;
+    if (r < ex) {  // x slice: [s][c][k][j]
+      const int s = (int)(r / (9 * px));
+      r %= 9 * px;
+      c = (int)(r / px);
+      k = (int)((r % px) / q.nj);
+      j = (int)(r % q.nj);
+      i = q.idx[s];
+    } else if (r < ex + ey) {  // y slice: [s][c][k][i]
+      r -= ex;
+      const int s = (int)(r / (9 * py));
+      r %= 9 * py;
+      c = (int)(r / py);
+      k = (int)((r % py) / q.ni);
+      i = (int)(r % q.ni);
+      j = q.idx[q.nxs + s];
+    } else {  // z slice: [s][c][j][i]
+      r -= ex + ey;
+      const int s = (int)(r / (9 * pz));
+      r %= 9 * pz;
+      c = (int)(r / pz);
+      j = (int)((r % pz) / q.ni);
+      i = (int)(r % q.ni);
+      k = q.idx[q.nxs + q.nys + s];
+    }
+    out[t] = (float)q.pre[((long long)shot * 9 + c) * q.sf + q.off0 + (long long)k * q.sz + (long long)j * q.sx + i];
+  }
+}
+
+template <typename R>
+int launch_slices(const SliceP<R> &q, cudaStream_t st) {
+  if (q.per_shot <= 0) return 0;
+  const long long total = q.per_shot * q.nshot;
+  const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 8);
+  k_slices<R><<<blocks, 256, 0, st>>>(q);
+  return 1;
+}
+template int launch_slices<float>(const SliceP<float> &, cudaStream_t);
+template int launch_slices<double>(const SliceP<double> &, cudaStream_t);
 
 __global__ void k_advance(int *d_it) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *d_it += 1;

@@ -74,6 +74,26 @@ struct RecvPT {
 };
 using RecvP = RecvPT<float>;
 
+// Slices: full x / y / z planes of the 9 components of w_pre at the start of every step
+// (io_slice_nc_put, io_funcs.cu:667-788, pack kernels io_funcs.cu:1528-1567), written into a
+// device ring of ring_steps steps: ring[(it % ring_steps) * nshot + shot][per_shot] with, per
+// shot, the x slices [nxs][9][nk][nj], then the y slices [nys][9][nk][ni], then the z slices
+// [nzs][9][nj][ni] (physical points only).
+template <typename R>
+struct SliceP {
+  int ni, nj, nk, nshot;
+  long long sx, sz, sf, off0;
+  const R *pre;
+  int nxs, nys, nzs;
+  const int *idx;              // [nxs + nys + nzs] physical 0-based plane index
+  float *ring;
+  int ring_steps;
+  long long per_shot;          // 9 * (nxs nk nj + nys nk ni + nzs nj ni)
+  const int *d_it;
+};
+template <typename R>
+int launch_slices(const SliceP<R> &q, cudaStream_t st);
+
 // Each launcher returns the number of kernels it launched (0 or 1).
 template <typename R>
 int launch_stage_bulk(int med, const StagePT<R> &p, int nzc, cudaStream_t st);

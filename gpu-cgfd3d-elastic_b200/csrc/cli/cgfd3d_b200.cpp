@@ -176,6 +176,95 @@ void put_snapshot(Snap &s, cgfd_problem *p, const Grid &g, const std::vector<flo
   s.w->append(data);
 }
 
+// One receiver of a "receiver_line" entry inside the grid (io_line_locate, io_funcs.cu:300-414):
+// point `seq` of the line at physical index start + seq * incre.
+struct LinePoint {
+  std::string line;
+  int seq, i, j, k;
+};
+
+std::vector<LinePoint> parse_lines(const Value *lv, const Grid &g) {
+  std::vector<LinePoint> pts;
+  if (!lv) return pts;
+  for (const Value &e : lv->arr) {
+    const std::string name = need(e, "name").as_str();
+    const Value &st = need(e, "grid_index_start"), &ic = need(e, "grid_index_incre");
+    if (st.arr.size() != 3 || ic.arr.size() != 3) fail("receiver_line " + name + ": index arrays need 3 entries");
+    const int cnt = need(e, "grid_index_count").as_int();
+    for (int n = 0; n < cnt; n++) {
+      int q[3];
+      for (int a = 0; a < 3; a++) q[a] = st.arr[a].as_int() - 1 + n * ic.arr[a].as_int();  // 1-based in the file
+      if (q[0] >= 0 && q[0] < g.ni && q[1] >= 0 && q[1] < g.nj && q[2] >= 0 && q[2] < g.nk)
+        pts.push_back({name, n, q[0], q[1], q[2]});
+    }
+  }
+  return pts;
+}
+
+// The x / y / z slices of the "slice" entry inside the grid (io_slice_locate,
+// io_funcs.cu:418-528), each a NetCDF file of record variables on an unlimited time dimension
+// (io_slice_nc_create, io_funcs.cu:531-664): slicex_i<gi+1>_<part>.nc with dims (time, k, j),
+// slicey_j<gj+1> (time, k, i), slicez_k<gk+1> (time, j, i); variable "time" and the 9 components.
+struct Slices {
+  std::vector<int> idx[3];
+  std::vector<std::unique_ptr<cgfd::nc::RecordWriter>> files[3];
+};
+
+Slices open_slices(const Value *sv, const Grid &g, const std::string &out) {
+  Slices S;
+  if (!sv) return S;
+  const char *keys[3] = {"x_index", "y_index", "z_index"};
+  const int n[3] = {g.ni, g.nj, g.nk};
+  const char *tag[3] = {"slicex_i", "slicey_j", "slicez_k"};
+  const char *att[3] = {"i_index_with_ghosts_in_this_thread", "j_index_with_ghosts_in_this_thread",
+                        "k_index_with_ghosts_in_this_thread"};
+  for (int a = 0; a < 3; a++) {
+    const Value *v = sv->get(keys[a]);
+    if (!v) continue;
+    for (const Value &e : v->arr) {
+      const int gi = e.as_int() - 1;
+      if (gi < 0 || gi >= n[a]) continue;
+      S.idx[a].push_back(gi);
+      cgfd::nc::File f;
+      f.version = 1;  // NC_CLOBBER: classic format
+      const std::string d1 = a == 2 ? "j" : "k", d2 = a == 0 ? "j" : "i";
+      f.dims = {{"time", 0}, {d1, (uint64_t)(a == 2 ? g.nj : g.nk)}, {d2, (uint64_t)(a == 0 ? g.nj : g.ni)}};
+      cgfd::nc::Var tv;
+      tv.name = "time";
+      tv.dimids = {0};
+      f.vars.push_back(tv);
+      for (int c = 0; c < 9; c++) {
+        cgfd::nc::Var v3;
+        v3.name = kCmpNames[c];
+        v3.dimids = {0, 1, 2};
+        f.vars.push_back(v3);
+      }
+      f.gatts.push_back({att[a], cgfd::nc::INT, {(double)(gi + 3)}, ""});
+      f.gatts.push_back({"coords_of_mpi_topo", cgfd::nc::INT, {0.0, 0.0, 0.0}, ""});
+      S.files[a].emplace_back(new cgfd::nc::RecordWriter(
+          out + "/" + tag[a] + std::to_string(gi + 1) + "_" + kFnamePart + ".nc", f));
+    }
+  }
+  return S;
+}
+
+// Appends the slices of step `it` (io_slice_nc_put: time = it * dt + t0, then each component).
+void put_slices(Slices &S, cgfd_problem *p, const Grid &g, int it, float time, std::vector<float> &buf) {
+  const size_t plane[3] = {(size_t)g.nk * g.nj, (size_t)g.nk * g.ni, (size_t)g.nj * g.ni};
+  size_t total = 0;
+  for (int a = 0; a < 3; a++) total += S.idx[a].size() * 9 * plane[a];
+  buf.resize(total);
+  if (cgfd_get_slices(p, 0, it, buf.data())) fail(std::string("slices: ") + cgfd_last_error());
+  size_t off = 0;
+  for (int a = 0; a < 3; a++)
+    for (size_t s = 0; s < S.idx[a].size(); s++) {
+      std::vector<const float *> data = {&time};
+      for (int c = 0; c < 9; c++) data.push_back(buf.data() + off + c * plane[a]);
+      S.files[a][s]->append(data);
+      off += 9 * plane[a];
+    }
+}
+
 void mkdirs(const std::string &d) {
   std::string cur;
   for (size_t p = 0; p <= d.size(); p++) {
@@ -343,6 +432,27 @@ int run(int argc, char **argv) {
       snaps.push_back(parse_snapshot(e, g));
       open_snapshot(snaps.back(), out);
     }
+  // line receivers and slices, sampled on the device at the start of every step
+  std::vector<LinePoint> lines = parse_lines(par.get("receiver_line"), g);
+  if (!lines.empty()) {
+    std::vector<int> ijk;
+    for (const LinePoint &l : lines) ijk.insert(ijk.end(), {l.i, l.j, l.k});
+    if (cgfd_set_line_receivers(p, (int)lines.size(), ijk.data())) fail(std::string("lines: ") + cgfd_last_error());
+  }
+  Slices slices = open_slices(par.get("slice"), g, out);
+  int ring = 100;  // steps per run chunk; the slice ring holds one chunk (at most ~512 MB)
+  {
+    const size_t per = 9 * sizeof(float) *
+                       (slices.idx[0].size() * g.nk * g.nj + slices.idx[1].size() * g.nk * g.ni +
+                        slices.idx[2].size() * g.nj * g.ni);
+    if (per > 0) {
+      ring = (int)std::max<size_t>(1, std::min<size_t>(100, (size_t(512) << 20) / per));
+      if (cgfd_set_slices(p, (int)slices.idx[0].size(), slices.idx[0].data(), (int)slices.idx[1].size(),
+                          slices.idx[1].data(), (int)slices.idx[2].size(), slices.idx[2].data(), ring))
+        fail(std::string("slices: ") + cgfd_last_error());
+    }
+  }
+  std::vector<float> slice_buf;
   auto next_snapshot = [&](int from) {
     int best = nt_total;
     for (const Snap &s : snaps)
@@ -356,9 +466,11 @@ int run(int argc, char **argv) {
       if (snapshot_due(s, step, nt_total))
         put_snapshot(s, p, g, medium, d.medium_type == CGFD_MEDIUM_ELASTIC_ISO,
                      (float)step * d.dt + d.t0);  // t_cur = it * dt + t0 in float (drv_rk_curv_col.cu:195)
-    int n = std::min({100, nt_total - step, std::max(1, next_snapshot(step + 1) - step)});
+    int n = std::min({ring, nt_total - step, std::max(1, next_snapshot(step + 1) - step)});
     int rc = cgfd_run(p, n);
     if (rc) { std::string m = cgfd_last_error(); cgfd_problem_destroy(p); fail("run: " + m); }
+    for (int it = step; it < step + n && !slices.idx[0].empty() + !slices.idx[1].empty() + !slices.idx[2].empty(); it++)
+      put_slices(slices, p, g, it, (float)it * d.dt + d.t0, slice_buf);
     step += n;
     if (step - last_print >= 100 || step == nt_total) {
       printf("-> it=%d\n", step);
@@ -367,6 +479,21 @@ int run(int argc, char **argv) {
     }
   }
   snaps.clear();  // closes the snapshot files
+  for (auto &f : slices.files) f.clear();  // closes the slice files
+  // line receivers (io_line_output_sac, io_funcs.cu:1943-1985): <line>.no<seq>.<cmp>.sac
+  if (!lines.empty()) {
+    std::vector<float> ls(lines.size() * 9 * (size_t)nt_total);
+    if (cgfd_get_line_seismograms(p, ls.data())) fail(std::string("lines: ") + cgfd_last_error());
+    for (size_t r = 0; r < lines.size(); r++) {
+      const LinePoint &l = lines[r];
+      const size_t c0 = g.at(l.i, l.j, l.k);
+      for (int c = 0; c < 9; c++)
+        cgfd::fmt::write_sac(out + "/" + l.line + ".no" + std::to_string(l.seq) + "." + kCmpNames[c] + ".sac",
+                             &ls[(r * 9 + c) * nt_total], nt_total, (float)dt, coord[c0], coord[g.siz + c0],
+                             coord[2 * g.siz + c0], (float)dt);
+    }
+    printf("wrote %zu line receivers\n", lines.size());
+  }
 
   // ---- SAC output (io_recv_output_sac, io_funcs.cu:1775-1902)
   int nsta = cgfd_num_stations(p);

@@ -223,6 +223,33 @@ int cgfd_get_wavefield_box(cgfd_problem *p, int shot, const int *start, const in
  */
 int cgfd_get_peak_motion(cgfd_problem *p, int shot, float *out);
 
+/*
+ * Line receivers: the 9 components of w_pre at grid points (no interpolation) at the start of
+ * every step, like io_line_keep (io_funcs.cu:1669-1700) on the points io_line_locate
+ * (io_funcs.cu:300-414) builds from the "receiver_line" entries (point n of a line at
+ * start + n * incre; the caller drops points outside the grid as io_line_locate does, this
+ * call refuses them). ijk[npts][3] are physical 0-based indices. Replaces the receiver set of
+ * any earlier call; steps run before the call hold zeros. Samples go to a device buffer and
+ * come back with cgfd_get_line_seismograms as [nshot][npts][9][nt_total] (the array
+ * io_line_output_sac writes, io_funcs.cu:1943-1985). The buffers count in cgfd_device_bytes.
+ */
+int cgfd_set_line_receivers(cgfd_problem *p, int npts, const int *ijk);
+int cgfd_get_line_seismograms(cgfd_problem *p, float *out);
+
+/*
+ * Slices: the full x, y and z planes (physical 0-based indices ix[nx], iy[ny], iz[nz]) of the
+ * 9 components of w_pre at the start of every step, like io_slice_nc_put
+ * (io_funcs.cu:667-788, called every step at drv_rk_curv_col.cu:206) on the planes
+ * io_slice_locate (io_funcs.cu:418-528) keeps. The planes are packed on the device into a ring
+ * of ring_steps steps (no host round trip inside the time loop); cgfd_get_slices returns the
+ * planes of one step `it` still in the ring (current_step - ring_steps <= it < current_step)
+ * as the x slices [nx][9][nk][nj], then the y slices [ny][9][nk][ni], then the z slices
+ * [nz][9][nj][ni]. Replaces any earlier slice set; the ring counts in cgfd_device_bytes.
+ */
+int cgfd_set_slices(cgfd_problem *p, int nx, const int *ix, int ny, const int *iy, int nz, const int *iz,
+                    int ring_steps);
+int cgfd_get_slices(cgfd_problem *p, int shot, int it, float *out);
+
 /* Per-shot variants of cgfd_get_wavefield / cgfd_set_wavefield for batched problems. */
 int cgfd_get_wavefield_shot(cgfd_problem *p, int shot, float *out);
 int cgfd_set_wavefield_shot(cgfd_problem *p, int shot, const float *in);
