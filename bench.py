@@ -304,46 +304,55 @@ def media_bench(local, steps=2000):
     return out
 
 
-def serving_bench(local, nreq=24, mean_gap_s=0.02, seed=11):
-    """The serving loop under Poisson arrivals: nreq forward simulations on 4 models (iso /
-    VTI / aniso, 96x96x64 ... 160x160x96, CFS-PML 10, free surface, 300 steps each), 1-4
-    random double-couple sources per request, 16 surface stations; same-model requests batch.
-    Reports p50 / p99 latency (submit -> seismograms ready) and throughput."""
+def serving_bench(local, nreq=40, nmodels=8, mean_gap_s=1.5, seed=11):
+    """The serving loop on a stream shaped like the serving workload: `nmodels` seeded models
+    with grid sizes drawn uniformly between 64^3 and 320x320x160 (x, y in [64, 320], z in
+    [64, 160]) and media 50% iso / 30% VTI / 20% 21-Cij aniso (each with its own topography and
+    medium, 100 m, CFS-PML 10, free surface, 16 surface stations); `nreq` requests with Poisson
+    arrivals (mean gap `mean_gap_s`), each on a random model with 1-8 random double-couple
+    sources and 500-2000 steps (drawn in steps of 500, so that same-grid requests can batch).
+    The full workload's 500 requests would hold the GPU for about ten minutes; the stream keeps
+    its size, media and step distributions at `nreq` requests. Reports p50 / p99 latency (submit
+    -> seismograms ready), completed cell-stages/s and the largest device memory held."""
     import dataclasses
-    from cgfd_b200 import synth, Server, Problem
+    from cgfd_b200 import synth, Server
     rng = np.random.default_rng(seed)
-    shapes = [("iso", (96, 96, 64)), ("iso", (160, 160, 96)), ("vti", (128, 128, 64)), ("aniso", (96, 80, 64))]
-    weights = np.array([0.25, 0.25, 0.3, 0.2])
+    kinds = rng.choice(["iso", "vti", "aniso"], size=nmodels, p=[0.5, 0.3, 0.2])
     models = []
-    for n, (med, (ni, nj, nk)) in enumerate(shapes):
-        m = synth.make_problem(ni, nj, nk, 100.0, 299, dt=None, medium=med, npml=10, nsrc=0, sta_grid=(4, 4),
-                               fc=2.0, seed=100 + n)
+    for n in range(nmodels):
+        ni, nj = (int(v) for v in rng.integers(8, 41, 2) * 8)
+        nk = int(rng.integers(8, 21) * 8)
+        m = synth.make_problem(ni, nj, nk, 100.0, 500, dt=None, medium=str(kinds[n]), npml=10, nsrc=0,
+                               sta_grid=(4, 4), fc=2.0, seed=300 + n)
         m.device = local
         models.append(m)
     reqs = []
     for r in range(nreq):
-        m = models[int(rng.choice(len(models), p=weights))]
-        src = synth.dc_sources(m.coord, m.ni, m.nj, int(rng.integers(1, 5)), rng, depth_range=(1500.0, 3000.0),
-                               fc_range=(1.5, 2.5), stf_length=m.nt_total * m.dt)
-        reqs.append(dataclasses.replace(m, src=src))
+        m = models[int(rng.integers(nmodels))]
+        steps = int(rng.integers(1, 5)) * 500
+        src = synth.dc_sources(m.coord, m.ni, m.nj, int(rng.integers(1, 9)), rng, depth_range=(1500.0, 4000.0),
+                               fc_range=(1.5, 2.5), stf_length=(steps + 1) * m.dt)
+        reqs.append(dataclasses.replace(m, src=src, nt_total=steps + 1))
     gaps = rng.exponential(mean_gap_s, nreq)
     work = sum(q.ni * q.nj * q.nk * 4.0 * q.nt_total for q in reqs)
-    with Server(device=local, max_active=4, max_batch=4, steps_per_slice=50) as srv:
+    with Server(device=local, max_active=4, max_batch=8, steps_per_slice=100) as srv:
         t0 = time.perf_counter()
         ids = []
         for q, g in zip(reqs, gaps):
             time.sleep(float(g))
             ids.append(srv.submit(q))
         for i in ids:
-            if srv.wait(i, timeout=600) is None:
+            if srv.wait(i, timeout=1800) is None:
                 raise RuntimeError("serving request timed out")
         wall = time.perf_counter() - t0
         st = srv.stats()
-    return {"requests": nreq, "models": [f"{m}:{a}x{b}x{c}" for m, (a, b, c) in shapes], "steps": 300,
+    return {"requests": nreq, "models": [f"{m.medium_type}:{m.ni}x{m.nj}x{m.nk}" for m in models],
+            "steps": "500-2000 (multiples of 500)", "sources": "1-8",
             "arrivals": f"Poisson, mean gap {mean_gap_s * 1e3:.0f} ms", "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
             "mean_ms": st["mean_ms"], "completed": st["completed"], "failed": st["failed"], "batches": st["batches"],
             "cell_stages_per_s": st["cell_stages_per_s"], "source_steps_per_s": st["source_steps_per_s"],
-            "wall_s": wall, "offered_gcell_stages": work / 1e9, "hbm_peak_gb": st["hbm_peak"] / 1e9}
+            "wall_s": wall, "offered_gcell_stages": work / 1e9, "hbm_peak_gb": st["hbm_peak"] / 1e9,
+            "hbm_budget_gb": st["hbm_budget"] / 1e9}
 
 
 def cpu_baseline(args, threads, p=None, steps=3):

@@ -22,16 +22,21 @@
 
 namespace cgfd {
 
-// Tile height of the direct-load kernel: 8 rows in FP32, 4 in FP64 (static shared memory).
-template <typename R> struct DirectTile { static constexpr int TYB = sizeof(R) == 8 ? 4 : TY; };
+// Shared memory of the direct-load kernel: the double-buffered x-y tile with its halo, 9 fields
+// (31 KB in FP32; 62 KB in the FP64 build, one block per SM).
+template <typename R> struct DirectTile {
+  static constexpr int SW = TX + 4, SH = TY + 4;
+  static constexpr int BYTES = 2 * 9 * SH * SW * (int)sizeof(R);
+  static constexpr int MINB = sizeof(R) == 8 ? 1 : 2;
+};
 
 template <int MED, int DX, int DY, int DZ, typename R = float>
-__global__ void __launch_bounds__(TX *DirectTile<R>::TYB, 2)
+__global__ void __launch_bounds__(TX *TY, DirectTile<R>::MINB)
     k_stage_bulk(const __grid_constant__ StagePT<R> p, int nzc) {
-  constexpr int TY = DirectTile<R>::TYB;
   constexpr int LX = op_left(DX), LY = op_left(DY), LZ = op_left(DZ);
-  constexpr int SW = TX + 4, SH = TY + 4;
-  __shared__ R s[2][9][SH][SW];
+  constexpr int SW = DirectTile<R>::SW, SH = DirectTile<R>::SH;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  R(*s)[9][SH][SW] = reinterpret_cast<R(*)[9][SH][SW]>(dsm);
 
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int bx = blockIdx.x, by = blockIdx.y;
@@ -602,11 +607,19 @@ __global__ void k_repack_out(const R *__restrict__ src, float *__restrict__ dst,
 template <int MED, typename R>
 static void launch_bulk_med(const StagePT<R> &p, int nzc, dim3 grid, cudaStream_t st) {
   const int code = p.dir[0] | (p.dir[1] << 1) | (p.dir[2] << 2);
-  dim3 block(TX, DirectTile<R>::TYB);
+  dim3 block(TX, TY);
+  constexpr int B = DirectTile<R>::BYTES;
+  // above 48 KB of dynamic shared memory each instantiation needs the opt-in once
+  static bool attr_done[8] = {};
   switch (code) {
-#define CASE(c)                                                                                      \
-  case c:                                                                                            \
-    k_stage_bulk<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, R><<<grid, block, 0, st>>>(p, nzc); \
+#define CASE(c)                                                                                          \
+  case c:                                                                                                \
+    if (B > 48 * 1024 && !attr_done[c]) {                                                                \
+      cudaFuncSetAttribute(k_stage_bulk<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, R>,                  \
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, B);                              \
+      attr_done[c] = true;                                                                               \
+    }                                                                                                    \
+    k_stage_bulk<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, R><<<grid, block, B, st>>>(p, nzc);       \
     break;
     CASE(0) CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7)
 #undef CASE
@@ -616,8 +629,7 @@ static void launch_bulk_med(const StagePT<R> &p, int nzc, dim3 grid, cudaStream_
 template <typename R>
 int launch_stage_bulk(int med, const StagePT<R> &p, int nzc, cudaStream_t st) {
   if (p.nbulk <= 0) return 0;
-  constexpr int ty = DirectTile<R>::TYB;
-  dim3 grid((p.ni + TX - 1) / TX, (p.nj + ty - 1) / ty, (p.nbulk + nzc - 1) / nzc);
+  dim3 grid((p.ni + TX - 1) / TX, (p.nj + TY - 1) / TY, (p.nbulk + nzc - 1) / nzc);
   if (med == MED_ISO) launch_bulk_med<MED_ISO>(p, nzc, grid, st);
   else if (med == MED_VTI) launch_bulk_med<MED_VTI>(p, nzc, grid, st);
   else launch_bulk_med<MED_ANISO>(p, nzc, grid, st);

@@ -1,11 +1,16 @@
 // cgfd_server.cpp -- serving loop: continuous admission of forward simulations onto one GPU.
 //
 // Requests (problem descriptions with their own sources) are queued by cgfd_server_submit from
-// any thread. One scheduler thread owns every CUDA call:
-//   - admission, in submission order, whenever a slot and HBM budget are free: the request at
-//     the head of the queue is grouped with the queued requests on the SAME grid (same model
-//     arrays and run parameters; only the sources differ), up to max_batch, and built as one
-//     batched problem (cgfd_batch_create) sized beforehand by cgfd_problem_bytes;
+// any thread. Two threads own the CUDA calls:
+//   - admission (scheduler thread), in submission order, whenever a slot and HBM budget are
+//     free: the request at the head of the queue is grouped with the queued requests on the
+//     SAME grid (same model arrays and run parameters; only the sources differ), up to
+//     max_batch, sized beforehand by cgfd_problem_bytes (its build high-water mark is reserved
+//     from the budget) and handed to the builder thread;
+//   - build (builder thread): cgfd_batch_create, i.e. the model upload and setup, which takes
+//     tens to hundreds of milliseconds for a large grid; the ready problem goes back to the
+//     scheduler. The scheduler never waits for a build, so resident problems keep their
+//     slices queued while a new grid uploads;
 //   - progress: every resident problem gets its time steps in slices of steps_per_slice, at
 //     most two slices queued on its own stream, so problems of different grids and media run
 //     side by side on the device and a newly admitted one starts while others are mid-run;
@@ -73,7 +78,8 @@ struct Slot {
   cgfd_problem *p = nullptr;
   std::vector<std::shared_ptr<Request>> reqs;
   int nt_total = 0, enqueued = 0;
-  size_t bytes = 0;
+  size_t bytes = 0;     // resident bytes once built
+  size_t reserved = 0;  // budget held while building (the build's high-water mark)
   std::deque<std::pair<cudaEvent_t, int>> inflight;  // (event after a slice, steps up to it)
   int done_steps = 0;
 };
@@ -91,7 +97,11 @@ struct cgfd_server {
   std::thread th;
   // scheduler-owned
   std::vector<Slot> slots;
-  size_t in_use = 0;
+  size_t in_use = 0;       // budget held by resident and building problems
+  int building = 0;        // problems handed to the builder and not yet back
+  // builder hand-off (under mu): groups to build, built problems (or failures) to take back
+  std::deque<Slot> to_build, built;
+  std::thread builder;
   // statistics (under mu)
   size_t peak = 0;
   long long batches = 0, completed = 0, failed = 0;
@@ -113,7 +123,7 @@ struct cgfd_server {
 
   // admit queued requests while a slot and budget are free (scheduler thread)
   void admit() {
-    while ((int)slots.size() < opts.max_active) {
+    while ((int)slots.size() + building < opts.max_active) {
       std::vector<std::shared_ptr<Request>> group;
       {
         std::lock_guard<std::mutex> g(mu);
@@ -132,7 +142,7 @@ struct cgfd_server {
         continue;
       }
       if (in_use + peak_b > opts.hbm_budget) {
-        if (!slots.empty()) return;  // wait for memory to free up (order kept)
+        if (!slots.empty() || building > 0) return;  // wait for memory to free up (order kept)
         if (group.size() > 1) {      // try the head alone
           group.resize(1);
           shots.resize(1);
@@ -147,23 +157,62 @@ struct cgfd_server {
       }
       remove_pending(group);
       Slot s;
-      rc = cgfd_batch_create(&group[0]->desc, (int)group.size(), shots.data(), &s.p);
-      if (rc != CGFD_OK) {
-        std::string m = cgfd_last_error();
-        for (auto &r : group) fail(r, rc, m);
-        continue;
-      }
       s.reqs = group;
       s.nt_total = group[0]->desc.nt_total;
-      s.bytes = cgfd_device_bytes(s.p);
-      in_use += s.bytes;
+      s.reserved = peak_b;
+      in_use += peak_b;
+      building++;
       {
         std::lock_guard<std::mutex> g(mu);
         for (auto &r : group) r->state = RUNNING;
         batches++;
-        peak = std::max(peak, in_use + (peak_b - resident));
+        peak = std::max(peak, in_use);
         if (!any_start) { any_start = true; t_first = Clock::now(); }
+        to_build.push_back(std::move(s));
       }
+      cv.notify_all();
+    }
+  }
+
+  // builder thread: one batched problem at a time, off the scheduler's path
+  void build_loop() {
+    cudaSetDevice(opts.device);
+    for (;;) {
+      Slot s;
+      {
+        std::unique_lock<std::mutex> g(mu);
+        cv.wait(g, [&] { return stop || !to_build.empty(); });
+        if (stop) return;
+        s = std::move(to_build.front());
+        to_build.pop_front();
+      }
+      std::vector<cgfd_source_desc> shots;
+      for (auto &r : s.reqs) shots.push_back(r->desc.src);
+      const int rc = cgfd_batch_create(&s.reqs[0]->desc, (int)s.reqs.size(), shots.data(), &s.p);
+      if (rc != CGFD_OK) {
+        const std::string m = cgfd_last_error();
+        for (auto &r : s.reqs) fail(r, rc, m);
+        s.p = nullptr;
+      } else {
+        s.bytes = cgfd_device_bytes(s.p);
+      }
+      std::lock_guard<std::mutex> g(mu);
+      built.push_back(std::move(s));
+    }
+  }
+
+  // scheduler: take built problems back (the reservation becomes the resident size)
+  void collect_built() {
+    std::deque<Slot> ready;
+    {
+      std::lock_guard<std::mutex> g(mu);
+      ready.swap(built);
+    }
+    for (Slot &s : ready) {
+      building--;
+      in_use -= s.reserved;
+      if (!s.p) continue;  // failed build: its requests were failed by the builder
+      in_use += s.bytes;
       slots.push_back(std::move(s));
     }
   }
@@ -257,7 +306,7 @@ struct cgfd_server {
       {
         std::unique_lock<std::mutex> g(mu);
         if (stop) break;
-        if (slots.empty() && pending.empty()) cv.wait_for(g, std::chrono::milliseconds(20));
+        if (slots.empty() && pending.empty() && built.empty()) cv.wait_for(g, std::chrono::milliseconds(20));
         if (stop) break;
         if (!fatal.empty()) {
           for (auto &r : pending) { r->state = FAILED; r->rc = CGFD_ERR_CUDA; r->err = fatal; failed++; }
@@ -266,10 +315,13 @@ struct cgfd_server {
           continue;
         }
       }
+      collect_built();
       admit();
       if (!progress()) std::this_thread::sleep_for(std::chrono::microseconds(200));
     }
     // shutdown: finish nothing further, release device state
+    if (builder.joinable()) builder.join();
+    collect_built();
     for (auto &s : slots) {
       for (auto &ev : s.inflight) cudaEventDestroy(ev.first);
       cgfd_synchronize(s.p);
@@ -308,6 +360,7 @@ int cgfd_server_create(const cgfd_server_opts *opts, cgfd_server **out) {
   }
   cgfd_server *s = new cgfd_server;
   s->opts = o;
+  s->builder = std::thread([s] { s->build_loop(); });
   s->th = std::thread([s] { s->loop(); });
   *out = s;
   return CGFD_OK;
@@ -437,9 +490,13 @@ int cgfd_server_destroy(cgfd_server *s) {
     s->stop = true;
     for (auto &r : s->pending) { r->state = FAILED; r->rc = CGFD_ERR_BUSY; r->err = "server destroyed"; }
     s->pending.clear();
+    for (auto &b : s->to_build)
+      for (auto &r : b.reqs) { r->state = FAILED; r->rc = CGFD_ERR_BUSY; r->err = "server destroyed"; }
+    s->to_build.clear();
     s->cv.notify_all();
   }
   if (s->th.joinable()) s->th.join();
+  if (s->builder.joinable()) s->builder.join();
   delete s;
   return CGFD_OK;
 }
