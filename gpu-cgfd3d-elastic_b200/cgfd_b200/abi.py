@@ -274,6 +274,7 @@ def lib():
         "cgfd_get_timing": (C.c_int, [P, P, P, P, C.c_int]),
         "cgfd_fill_ghosts": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P]),
         "cgfd_metric_calc": (C.c_int, [C.c_int, C.c_int, C.c_int, P, P]),
+        "cgfd_metric_calc_gpu": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, P]),
         "cgfd_dt_estimate": (C.c_int, [C.POINTER(ProblemDesc), C.c_double, C.POINTER(C.c_double)]),
         "cgfd_keep_three_digits": (C.c_double, [C.c_double]),
         "cgfd_problem_bytes": (C.c_int, [C.POINTER(ProblemDesc), C.c_int, P, C.POINTER(C.c_size_t),

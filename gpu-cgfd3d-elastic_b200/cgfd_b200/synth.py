@@ -75,6 +75,17 @@ def metrics(coord):
     return out
 
 
+def metrics_gpu(coord, device=0):
+    """FP64 metrics [10, nz, ny, nx] computed on the GPU via cgfd_metric_calc_gpu."""
+    _, nz, ny, nx = coord.shape
+    out = np.zeros((10, nz, ny, nx), np.float32)
+    c = np.ascontiguousarray(coord, np.float32)
+    rc = lib().cgfd_metric_calc_gpu(int(device), nx - 6, ny - 6, nz - 6, c.ctypes.data, out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(lib().cgfd_last_error().decode())
+    return out
+
+
 def von_karman(shape, dh, corr=1000.0, hurst=0.3, std=0.05, seed=1):
     """Seeded 3-D von Karman random field (zero mean, given std) on `shape` (nk, nj, ni)."""
     rng = np.random.default_rng(seed)

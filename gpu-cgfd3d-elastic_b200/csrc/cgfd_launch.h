@@ -94,6 +94,11 @@ struct SliceP {
 template <typename R>
 int launch_slices(const SliceP<R> &q, cudaStream_t st);
 
+// Grid metrics in FP64 from coordinates x, y, z (ghosts filled) into out[10] (jac, xi_x ..
+// zeta_z), all in one layout (off0 + k sz + j sx + i), ghosts by linear extrapolation.
+void launch_metric(const float *x, const float *y, const float *z, float *const out[10], int ni, int nj, int nk,
+                   long long sx, long long sz, long long off0, cudaStream_t st);
+
 // Each launcher returns the number of kernels it launched (0 or 1).
 template <typename R>
 int launch_stage_bulk(int med, const StagePT<R> &p, int nzc, cudaStream_t st);

@@ -354,16 +354,15 @@ int run(int argc, char **argv) {
   }
   if (gg.get("import") && cgfd_fill_ghosts(g.ni, g.nj, g.nk, 3, coord.data())) fail(cgfd_last_error());
 
-  // ---- metrics (main:201-228)
+  // ---- metrics (main:201-228): imported here, or calculated on the GPU after the dt check
   std::vector<float> metric(10 * g.siz, 0.f);
   const Value &mm = need(par, "metric_calculation_method");
-  if (const Value *imp = mm.get("import")) {
-    std::string path = imp->as_str() + "/metric_" + kFnamePart + ".nc";
+  const bool metric_import = mm.get("import") != nullptr;
+  if (metric_import) {
+    std::string path = mm.get("import")->as_str() + "/metric_" + kFnamePart + ".nc";
     import_vars(path, g, {"jac", "xi_x", "xi_y", "xi_z", "eta_x", "eta_y", "eta_z", "zeta_x", "zeta_y", "zeta_z"},
                 metric.data());
     cgfd_fill_ghosts(g.ni, g.nj, g.nk, 10, metric.data());
-  } else {
-    if (cgfd_metric_calc(g.ni, g.nj, g.nk, coord.data(), metric.data())) fail(cgfd_last_error());
   }
 
   // ---- medium (par_t.cu:428-721, md_import md_t.cu:269-326)
@@ -402,6 +401,9 @@ int run(int argc, char **argv) {
     if (dtmax < dt) fail("dt = " + std::to_string(dt) + " > dtmax = " + std::to_string(dtmax));
   }
   if (dt <= 0.0) fail("no time step");
+  // FP64 metrics on the GPU (equal to the host FP64 calculation bitwise)
+  if (!metric_import && cgfd_metric_calc_gpu(gpu, g.ni, g.nj, g.nk, coord.data(), metric.data()))
+    fail(std::string("metrics on the GPU: ") + cgfd_last_error());
   d.dt = (float)dt;
   d.t0 = (float)t0;
   d.nt_total = nt_total;

@@ -409,6 +409,15 @@ int cgfd_fill_ghosts(int ni, int nj, int nk, int ncmp, float *v4d);
 int cgfd_metric_calc(int ni, int nj, int nk, const float *coord, float *metric);
 
 /*
+ * The same metrics computed on the GPU `device` (FP64 arithmetic without fused multiply-add,
+ * so the result equals cgfd_metric_calc bitwise): host arrays in and out, one thread per
+ * point, ghost layers by linear extrapolation on the device (the host version is one pass of
+ * OpenMP threads over the grid; a large model's setup no longer waits on it).
+ * Replaces: gd_curv_metric_cal + geometric_symmetry, gd_t.cu:209-314, 404-502.
+ */
+int cgfd_metric_calc_gpu(int device, int ni, int nj, int nk, const float *coord, float *metric);
+
+/*
  * Largest stable time step (FP64): CFL * min distance to the 8 neighbour planes / Vp.
  * Uses desc->coord and desc->medium (density form). The reference's CFL is 1.3.
  * Replaces: blk_dt_esti_curv, blk_t.cu:673-763.

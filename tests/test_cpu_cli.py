@@ -33,7 +33,7 @@ def test_cli_reads_reference_formats(tmp_path, medium):
     m = re.search(r"maximum allowed time step = ([0-9.eE+-]+)", r.stdout)
     assert m, r.stdout + r.stderr
     assert float(m.group(1)) == pytest.approx(synth.dt_estimate(p), rel=1e-5)
-    assert "create:" in r.stderr  # reached the device stage
+    assert "metrics on the GPU:" in r.stderr  # reached the device stage (GPU metric calculation)
 
 
 def test_cli_rejects_off_path_options(tmp_path):
