@@ -56,7 +56,54 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched / mixed-precision section")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
     ap.add_argument("--no-media", action="store_true", help="skip the VTI / aniso section")
+    # profiling case (no JSON line): K steps of direct launches on the chosen grid, for ncu
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="run this many directly launched steps of the profiling case and exit")
+    ap.add_argument("--pml-faces", default="x1,x2,y1,y2,z1",
+                    help="profiling case: CFS-PML faces (comma list of x1,x2,y1,y2,z1, or none)")
+    ap.add_argument("--pml-layers", type=int, default=0, help="profiling case: layers per face (0: workload's)")
+    ap.add_argument("--shots", type=int, default=1, help="profiling case: shots of a batched problem")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "u16coef", "fp16wave", "fp64"],
+                    help="profiling case: storage precision")
     return ap.parse_args()
+
+
+def profile_run(args):
+    """Profiling case for ncu: the workload (or --grid) with the chosen CFS-PML faces and width,
+    shots and precision, `--profile-steps` steps launched directly (one launch per kernel, no
+    graph). Prints the face points and the kernels' cell counts."""
+    import dataclasses
+    from cgfd_b200 import synth, Simulation, CGFD_PREC_FP32, CGFD_PREC_U16_COEF, CGFD_PREC_FP16_WAVE, CGFD_PREC_FP64
+    p = build_problem(args)
+    nl = args.pml_layers or WORKLOADS[args.workload][5]
+    face = dict(p.pml[0][0], num_layers=nl)
+    names = [f for f in args.pml_faces.split(",") if f and f != "none"]
+    slots = {"x1": (0, 0), "x2": (0, 1), "y1": (1, 0), "y2": (1, 1), "z1": (2, 0)}
+    p.pml = [[None, None], [None, None], [None, None]]
+    for f in names:
+        a, sd = slots[f]
+        p.pml[a][sd] = face
+    p.precision = {"fp32": CGFD_PREC_FP32, "u16coef": CGFD_PREC_U16_COEF, "fp16wave": CGFD_PREC_FP16_WAVE,
+                   "fp64": CGFD_PREC_FP64}[args.precision]
+    if args.shots > 1:
+        rng = np.random.default_rng(78)
+        shots = [synth.dc_sources(p.coord, p.ni, p.nj, 1, rng, depth_range=(1000.0, 3000.0), fc_range=(2.0, 5.0),
+                                  stf_length=p.nt_total * p.dt) for _ in range(args.shots)]
+        sim = Simulation(p, shots=shots)
+    else:
+        sim = Simulation(p)
+    sim.set_graph_mode(0)
+    sim.run(args.profile_steps)
+    pts = 0
+    for f in names:
+        n = [p.ni, p.nj, p.nk]
+        n[slots[f][0]] = nl + 1
+        pts += n[0] * n[1] * n[2]
+    print(f"profile case {p.ni}x{p.nj}x{p.nk} faces={names or 'none'} layers={nl} shots={args.shots} "
+          f"precision={args.precision}: {args.profile_steps} steps, face points {pts}, "
+          f"bulk cells {p.ni * p.nj * (p.nk - 4)}", flush=True)
+    sim.close()
+    return 0
 
 
 def max_over_ranks(x, dist, device):
@@ -444,6 +491,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_steps > 0:
+        return profile_run(args)
     rank, world, local = dist_env()
     import torch
     torch.cuda.set_device(local)

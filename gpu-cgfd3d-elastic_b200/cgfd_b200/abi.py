@@ -173,6 +173,36 @@ class Problem:
         return d
 
 
+class LayerModelDesc(C.Structure):
+    """cgfd_layer_model: a layered elastic-isotropic model (the reference's interface file)."""
+    _fields_ = [("num_interfaces", C.c_int), ("nx", C.c_int), ("ny", C.c_int),
+                ("x0", C.c_float), ("y0", C.c_float), ("dx", C.c_float), ("dy", C.c_float)] + \
+        [(n, C.c_void_p) for n in ("elevation", "rho", "rho_grad", "rho_pow", "vp", "vp_grad", "vp_pow",
+                                   "vs", "vs_grad", "vs_pow")]
+
+
+CGFD_MEDIA_LOC, CGFD_MEDIA_HAR, CGFD_MEDIA_ARI = 0, 1, 2
+
+
+def media_layer_gpu(coord, model, method=CGFD_MEDIA_LOC, device=0):
+    """cgfd_media_layer_el_iso_gpu: medium [3, nz, ny, nx] (rho, lambda, mu) of the layered
+    model (formats.LayerModel) on the grid coord [3, nz, ny, nx]."""
+    _, nz, ny, nx = coord.shape
+    keep = []
+
+    def arr(a):
+        a = np.ascontiguousarray(a, np.float32)
+        keep.append(a)
+        return a.ctypes.data
+    d = LayerModelDesc(int(model.elevation.shape[0]), int(model.nx), int(model.ny), float(model.x0), float(model.y0),
+                       float(model.dx), float(model.dy), *[arr(getattr(model, n)) for n in model.FIELDS])
+    c = np.ascontiguousarray(coord, np.float32)
+    out = np.zeros((3, nz, ny, nx), np.float32)
+    check(lib().cgfd_media_layer_el_iso_gpu(int(device), nx - 6, ny - 6, nz - 6, c.ctypes.data, C.byref(d), int(method),
+                                            out.ctypes.data))
+    return out
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("device", C.c_int), ("hbm_budget", C.c_size_t), ("max_active", C.c_int), ("max_batch", C.c_int),
                 ("steps_per_slice", C.c_int)]
@@ -275,6 +305,7 @@ def lib():
         "cgfd_fill_ghosts": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P]),
         "cgfd_metric_calc": (C.c_int, [C.c_int, C.c_int, C.c_int, P, P]),
         "cgfd_metric_calc_gpu": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, P]),
+        "cgfd_media_layer_el_iso_gpu": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, P, C.c_int, P]),
         "cgfd_dt_estimate": (C.c_int, [C.POINTER(ProblemDesc), C.c_double, C.POINTER(C.c_double)]),
         "cgfd_keep_three_digits": (C.c_double, [C.c_double]),
         "cgfd_problem_bytes": (C.c_int, [C.POINTER(ProblemDesc), C.c_int, P, C.POINTER(C.c_size_t),

@@ -212,3 +212,32 @@ def read_sac(path):
            "kstnm": ch[0:8], "kcmpnm": ch[160:168], "depmin": float(fh[1])}
     data = np.frombuffer(raw[632:632 + 4 * hdr["npts"]], "<f4").copy()
     return hdr, data
+
+
+class LayerModel:
+    """A layered elastic-isotropic model, the contents of the reference's "elastic_isotropic"
+    interface file (read_interface_file, src/media/media_read_file.cpp:22-210): interfaces top
+    first on a uniform nx x ny mesh; per interface the elevation and the value / gradient /
+    power of rho, vp, vs of the layer below it, each [num_interfaces, ny, nx]."""
+
+    FIELDS = ("elevation", "rho", "rho_grad", "rho_pow", "vp", "vp_grad", "vp_pow", "vs", "vs_grad", "vs_pow")
+
+    def __init__(self, x0, y0, dx, dy, **fields):
+        self.x0, self.y0, self.dx, self.dy = float(x0), float(y0), float(dx), float(dy)
+        for n in self.FIELDS:
+            setattr(self, n, np.ascontiguousarray(fields[n], np.float32))
+        self.ny, self.nx = self.elevation.shape[1:]
+
+
+def write_layer_file(path, m: LayerModel):
+    """The interface file in the reference's format: media type, number of interfaces, the mesh
+    "NX NY MINX MINY DX DY", then one line per interface and mesh point (x fastest) with the
+    elevation and value, gradient, power of rho, vp, vs (values written so that they read back
+    exactly as float)."""
+    ni = m.elevation.shape[0]
+    with open(path, "w") as f:
+        f.write("# layered elastic-isotropic model\nelastic_isotropic\n")
+        f.write(f"{ni}\n{m.nx} {m.ny} {m.x0:.9g} {m.y0:.9g} {m.dx:.9g} {m.dy:.9g}\n")
+        cols = np.stack([getattr(m, n) for n in LayerModel.FIELDS], axis=-1).reshape(-1, len(LayerModel.FIELDS))
+        for row in cols:
+            f.write(" ".join(f"{v:.9g}" for v in row) + "\n")

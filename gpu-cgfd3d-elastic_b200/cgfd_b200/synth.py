@@ -133,6 +133,35 @@ def layered_iso(coord, layers=LAYERS_3, interfaces=INTERFACES_3, perturb=None):
     return med
 
 
+def layer_model(coord, seed=5, layers=LAYERS_3, depths=(-1500.0, -3500.0), relief=150.0, grad=True):
+    """A layered elastic-isotropic model (formats.LayerModel) over the grid's horizontal extent:
+    a free top interface above the topography, then undulating interfaces around the given
+    depths (seeded sinusoidal relief), each layer with vp / vs / rho of `layers` and, with
+    `grad`, a small depth gradient (power 1)."""
+    from .formats import LayerModel
+    rng = np.random.default_rng(seed)
+    x, y = coord[0], coord[1]
+    x0, x1 = float(x.min()) - 100.0, float(x.max()) + 100.0
+    y0, y1 = float(y.min()) - 100.0, float(y.max()) + 100.0
+    nx, ny = 41, 37
+    dx, dy = (x1 - x0) / (nx - 1), (y1 - y0) / (ny - 1)
+    X, Y = np.meshgrid(x0 + dx * np.arange(nx), y0 + dy * np.arange(ny))
+    top = np.full((ny, nx), float(coord[2].max()) + 1000.0)
+    elev = [top]
+    for d in depths:
+        kx, ky, ph = rng.uniform(0.5, 2.0), rng.uniform(0.5, 2.0), rng.uniform(0, 6.3)
+        elev.append(d + relief * np.sin(kx * 2 * np.pi * (X - x0) / (x1 - x0) + ph) *
+                    np.cos(ky * 2 * np.pi * (Y - y0) / (y1 - y0)))
+    ni = len(elev)
+    f = {"elevation": np.stack(elev)}
+    for q, name in enumerate(("vp", "vs", "rho")):
+        vals = np.array([lay[q] for lay in layers], np.float32)
+        f[name] = np.repeat(vals[:, None, None], ny, 1).repeat(nx, 2)
+        f[name + "_grad"] = np.full((ni, ny, nx), (0.05 if grad else 0.0) * (q < 2), np.float32)
+        f[name + "_pow"] = np.ones((ni, ny, nx), np.float32)
+    return LayerModel(x0, y0, dx, dy, **f)
+
+
 def thomsen_vti(coord, seed=2, layers=LAYERS_3, interfaces=INTERFACES_3):
     """VTI medium [6, ...] (rho, c11, c13, c33, c55, c66) from layered Thomsen parameters
     eps in [0, 0.2], delta in [-0.1, 0.1], gamma in [0, 0.15] (seeded per layer)."""

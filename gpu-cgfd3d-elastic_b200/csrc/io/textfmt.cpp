@@ -145,6 +145,40 @@ StationFile read_station_file(const std::string &path) {
   return s;
 }
 
+LayerFile read_layer_file(const std::string &path) {
+  std::ifstream in(path);
+  if (!in) throw std::runtime_error("cannot open " + path);
+  std::stringstream body;
+  std::string ln;
+  while (std::getline(in, ln)) {
+    if (ln.empty() || ln[0] == '#' || ln[0] == '\r') continue;
+    body << ln << "\n";
+  }
+  LayerFile L;
+  std::string type;
+  if (!(body >> type)) throw std::runtime_error(path + ": no media type");
+  if (type != "elastic_isotropic")
+    throw std::runtime_error(path + ": media type '" + type + "' is not on this path (elastic_isotropic)");
+  if (!(body >> L.ni) || L.ni < 1) throw std::runtime_error(path + ": number of interfaces missing or < 1");
+  if (!(body >> L.nx >> L.ny >> L.x0 >> L.y0 >> L.dx >> L.dy) || L.nx < 2 || L.ny < 2)
+    throw std::runtime_error(path + ": interface mesh line must be NX NY MINX MINY DX DY with NX, NY >= 2");
+  const size_t n = (size_t)L.ni * L.nx * L.ny;
+  for (auto &v : L.f) v.resize(n);
+  for (size_t p = 0; p < n; p++)
+    for (int q = 0; q < 10; q++)
+      if (!(body >> L.f[q][p])) throw std::runtime_error(path + ": insufficient data");
+  return L;
+}
+
+const cgfd_layer_model &LayerFile::desc() {
+  d.num_interfaces = ni; d.nx = nx; d.ny = ny;
+  d.x0 = x0; d.y0 = y0; d.dx = dx; d.dy = dy;
+  const float **dst[10] = {&d.elevation, &d.rho, &d.rho_grad, &d.rho_pow, &d.vp, &d.vp_grad, &d.vp_pow,
+                           &d.vs, &d.vs_grad, &d.vs_pow};
+  for (int q = 0; q < 10; q++) *dst[q] = f[q].data();
+  return d;
+}
+
 void write_sac(const std::string &path, const float *data, int npts, float delta, float stla, float stlo, float stel,
                float stdp, float evla, float evlo, float evel, float evdp) {
   // SAC binary header: 70 floats, 40 ints (incl. 5 logicals), 192 bytes of text (632 bytes)

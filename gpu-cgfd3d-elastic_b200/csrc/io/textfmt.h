@@ -30,6 +30,19 @@ struct StationFile {
 };
 StationFile read_station_file(const std::string &path);
 
+// Layered elastic-isotropic model file (read_interface_file, src/media/media_read_file.cpp:22-210;
+// lines starting with '#' and empty lines skipped, then whitespace-separated tokens): media type
+// elastic_isotropic, number of interfaces, "NX NY MINX MINY DX DY", then per interface and mesh
+// point the elevation and value / gradient / power of rho, vp, vs. desc() points into the arrays.
+struct LayerFile {
+  int ni = 0, nx = 0, ny = 0;
+  float x0 = 0, y0 = 0, dx = 0, dy = 0;
+  std::vector<float> f[10];  // elevation, rho, rho_grad, rho_pow, vp, vp_grad, vp_pow, vs, vs_grad, vs_pow
+  cgfd_layer_model d{};
+  const cgfd_layer_model &desc();
+};
+LayerFile read_layer_file(const std::string &path);
+
 // One-component SAC file with the header fields the reference sets (sacLib.cu:8-100):
 // delta, b = 0, e = delta*(npts-1), npts, nvhdr = 6, iftype = ITIME, leven = 1, station
 // and event positions; every other field "undefined" (-12345).

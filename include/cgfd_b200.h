@@ -418,6 +418,42 @@ int cgfd_metric_calc(int ni, int nj, int nk, const float *coord, float *metric);
 int cgfd_metric_calc_gpu(int device, int ni, int nj, int nk, const float *coord, float *metric);
 
 /*
+ * Layered elastic-isotropic model: the contents of the reference's "elastic_isotropic"
+ * interface file (read_interface_file, src/media/media_read_file.cpp:22-210; the par-file
+ * medium input_way "infile_layer"). num_interfaces interfaces, each on a uniform mesh of
+ * nx * ny points at x0 + i dx, y0 + j dy, top interface first; per interface and mesh point the
+ * elevation and, for the layer below it, rho, vp, vs as value, gradient and power
+ * (v(z) = value + (elevation - z)^power * gradient). Arrays [num_interfaces][ny][nx].
+ */
+typedef struct cgfd_layer_model {
+  int   num_interfaces, nx, ny;
+  float x0, y0, dx, dy;
+  const float *elevation;
+  const float *rho, *rho_grad, *rho_pow;
+  const float *vp, *vp_grad, *vp_pow;
+  const float *vs, *vs_grad, *vs_pow;
+} cgfd_layer_model;
+
+/* equivalent_medium_method of the par file */
+#define CGFD_MEDIA_LOC 0  /* the layer at each grid point                                   */
+#define CGFD_MEDIA_HAR 1  /* volume averaging at interfaces: rho arithmetic, kappa and mu
+                             harmonic                                                        */
+#define CGFD_MEDIA_ARI 2  /* volume averaging at interfaces: rho, lambda and mu arithmetic    */
+
+/*
+ * Media discretisation on the GPU `device`: samples the layered model onto the curvilinear
+ * grid coord [3][nz][ny][nx] (ghosts filled) at every point, ghosts included, into
+ * medium [3][nz][ny][nx] = rho, lambda, mu (the cgfd_problem_desc medium of elastic_iso).
+ * One thread per grid point; at interfaces the har / ari methods average 9^3 sample points of
+ * the surrounding half-grid cell. CGFD_ERR_INVALID when a grid point lies outside the
+ * interface mesh or vp <= sqrt(2) vs (the reference exits there).
+ * Replaces: media_layer2model_el_iso, src/media/media_layer2model.cpp:121-170 with
+ * parametrization_layer_el_iso_loc / _har / _ari (:1313-1355 and the averaging loops).
+ */
+int cgfd_media_layer_el_iso_gpu(int device, int ni, int nj, int nk, const float *coord, const cgfd_layer_model *model,
+                                int method, float *medium);
+
+/*
  * Largest stable time step (FP64): CFL * min distance to the 8 neighbour planes / Vp.
  * Uses desc->coord and desc->medium (density form). The reference's CFL is 1.3.
  * Replaces: blk_dt_esti_curv, blk_t.cu:673-763.
