@@ -142,6 +142,7 @@ struct cgfd_problem {
   // (real-typed arrays -- wbuf, coef, jac, matx/maty, PML A/B/D/aux, d_dis -- are held as float*
   // and hold doubles in the FP64 build; rptr() gives the typed, element-offset pointer)
   float *coef = nullptr, *jac = nullptr, *matx = nullptr, *maty = nullptr;
+  float *d_flux = nullptr;  // traction-image fluxes of the current stage input (free surface)
   // 16-bit coefficient storage (replaces `coef` when coef_type != COEF_F32):
   // value = cscale[field] * stored + coffset[field]
   int precision = CGFD_PREC_FP32;
@@ -283,6 +284,7 @@ struct cgfd_problem {
     p.coef = coef_type == cgfd::COEF_F32 ? (const void *)coef : (const void *)coef16;
     for (int c = 0; c < 32; c++) { p.cscale[c] = cscale[c]; p.coffset[c] = coffset[c]; }
     p.jac = rptr<R>(jac); p.matx = rptr<R>(matx); p.maty = rptr<R>(maty);
+    p.flux = rptr<R>(d_flux);
     p.free_top = free_top;
     p.nbulk = free_top ? nk - cgfd::NSURF : nk;
     p.err = d_flag;
@@ -348,7 +350,7 @@ struct cgfd_problem {
     for (int s = 0; s < 4; s++) {
       const cgfd::StagePT<double> p = stage_params_t<double>(step, s);
       n += timed(s, [&] { return cgfd::launch_stage_bulk(med, p, nzc, st); });
-      n += timed(4, [&] { return cgfd::launch_stage_surface64(med, p, st); });
+      n += timed(4, [&] { return cgfd::launch_timg_flux64(p, st) + cgfd::launch_stage_surface64(med, p, st); });
       if (src.nsrc > 0) {
         cgfd::SrcPT<double> q;
         memset(&q, 0, sizeof(q));
@@ -408,7 +410,9 @@ struct cgfd_problem {
             CK(cudaStreamWaitEvent(side, ev_fork, 0));
           }
           int k = cgfd::launch_stage_bulk_tma(med, coef_type, wave16, p, tm, tiles, st, fork ? side : st);
-          if (surface_done) k += cgfd::launch_stage_surface(med, coef_type, wave16, p, side);
+          if (surface_done)
+            k += cgfd::launch_timg_flux(coef_type, wave16, p, side) +
+                 cgfd::launch_stage_surface(med, coef_type, wave16, p, side);
           if (fork) {
             CK(cudaEventRecord(ev_join, side));
             CK(cudaStreamWaitEvent(st, ev_join, 0));
@@ -418,7 +422,11 @@ struct cgfd_problem {
       } else {
         n += timed(s, [&] { return cgfd::launch_stage_bulk(med, p, nzc, st); });
       }
-      if (!surface_done) n += timed(4, [&] { return cgfd::launch_stage_surface(med, coef_type, wave16, p, st); });
+      if (!surface_done)
+        n += timed(4, [&] {
+          return cgfd::launch_timg_flux(coef_type, wave16, p, st) +
+                 cgfd::launch_stage_surface(med, coef_type, wave16, p, st);
+        });
       if (src.nsrc > 0) {
         cgfd::SrcP q;
         q.nsrc = src.nsrc; q.max_ext = src.max_ext; q.max_nt = src.max_nt;
@@ -476,7 +484,7 @@ struct cgfd_problem {
     if (stream) {  // everything below was allocated in the order of this stream
       const cudaStream_t st = stream;
       for (auto *p : wbuf) dfree(p, st);
-      dfree(coef, st); dfree(coef16, st); dfree(jac, st); dfree(matx, st); dfree(maty, st);
+      dfree(coef, st); dfree(coef16, st); dfree(jac, st); dfree(matx, st); dfree(maty, st); dfree(d_flux, st);
       for (Face &f : faces) { dfree(f.A, st); dfree(f.B, st); dfree(f.D, st); dfree(f.aux, st); }
       dfree(d_it_begin, st); dfree(d_ext_num, st); dfree(d_src_shot, st); dfree(d_ext_idx, st); dfree(d_ext_wv, st);
       dfree(d_ext_wt, st); dfree(d_wsc, st); dfree(d_srcb, st); dfree(d_amax, st); dfree(d_tiles, st); dfree(d_pg, st);
@@ -666,7 +674,8 @@ void problem_bytes(const cgfd_problem_desc *d, int nshot, const cgfd_source_desc
   const size_t stage_buf = (size_t)(d->ni + 6) * (d->nj + 6) * (d->nk + 6) * sizeof(float);
   size_t r = waves + (c16 ? coef16 : coef32) + jac;
   const size_t high = waves + jac + coef32 + (c16 ? std::max(stage_buf, coef16 + 8 * (size_t)ncoef) : stage_buf);
-  if (d->free_top) r += (size_t)2 * 9 * d->ni * d->nj * F;
+  if (d->free_top)
+    r += (size_t)2 * 9 * d->ni * d->nj * F + (size_t)9 * cgfd::kFluxPlanes * (d->ni + 6) * (d->nj + 6) * nshot * F;
   cgfd::PmlFaceHost fh[3][2];
   cgfd::pml_setup(d, fh);
   for (int a = 0; a < 3; a++)
@@ -853,6 +862,7 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
     p->maty = dalloc_real(p, my.size(), B);
     upload_real(p, p->matx, mx);
     upload_real(p, p->maty, my);
+    p->d_flux = dalloc_real(p, (size_t)9 * cgfd::kFluxPlanes * (p->ni + 6) * (p->nj + 6) * nshot, B);
   }
   // PML
   cgfd::PmlFaceHost fh[3][2];

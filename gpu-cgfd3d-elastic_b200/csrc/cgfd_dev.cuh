@@ -19,6 +19,10 @@
 
 namespace cgfd {
 
+// Planes below the top whose traction-image fluxes the surface slab reads (the image's z
+// stencil reaches 4 planes below the top one).
+constexpr int kFluxPlanes = 5;
+
 // Thread-block tile of the z-marching kernel (x fastest).
 constexpr int TX = 32;
 constexpr int TY = 8;
@@ -83,6 +87,10 @@ struct StagePT {
   const R *matx;          // free surface: [nj][ni][9] matVx2Vz (row-major 3x3)
   const R *maty;          //                [nj][ni][9] matVy2Vz
   int free_top;
+  // traction-image fluxes of the stage input (free surface): flux[shot][9][kFluxPlanes][nj+6][ni+6],
+  // component 3c + a = jac (metric row a . stress row c) at planes nk-kFluxPlanes .. nk-1,
+  // ghost columns included
+  R *flux;
   int nbulk;              // planes [0, nbulk) belong to the bulk kernel
   int nface;
   FacePT<R> face[6];

@@ -207,6 +207,39 @@ __device__ __forceinline__ void ld5(int dir, const WaveIn<TW> &cur, int f, long 
 // 16 warps share each SM (a few spills are cheaper than 8 warps).
 // The operator directions of the stage (DX, DY, DZ: 0 backward, 1 forward) are template
 // parameters, so that every stencil offset is a compile-time constant.
+// Traction-image fluxes of the stage input at the top kFluxPlanes planes, every column of the
+// extended x-y range (ghosts give 0: the wavefield is 0 there): for stress row c (Txx Txy Txz /
+// Txy Tyy Tyz / Txz Tyz Tzz) and metric row a (xi, eta, zeta), jac (m_a . T_c) -- the
+// J (grad xi_a . T) terms sv_curv_col_el_gpu.cu:53-217 differentiates. Computed once per point
+// here instead of once per stencil use in the surface slab.
+template <typename TC, int WP>
+__global__ void __launch_bounds__(256) k_timg_flux(const __grid_constant__ StagePT<real_of<TC>> p) {
+  using R = real_of<TC>;
+  using TW = typename std::conditional<WP == 2, __half, R>::type;
+  const int nxe = p.ni + 6, nye = p.nj + 6;
+  const long long plane = (long long)nxe * nye, per_shot = 9 * kFluxPlanes * plane;
+  const long long total = plane * kFluxPlanes * p.nshot;
+  const CoefView<TC> cv(p);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int ii = (int)(t % nxe), jj = (int)((t / nxe) % nye);
+    const int pl = (int)((t / plane) % kFluxPlanes), shot = (int)(t / (plane * kFluxPlanes));
+    const int k = p.nk - kFluxPlanes + pl;
+    const long long q = didx(p, ii - 3, jj - 3, k);
+    const WaveIn<TW> cur{reinterpret_cast<const TW *>(p.cur) + (long long)shot * 9 * p.sf, p.sf,
+                         p.wsc + shot * 18};
+    const int tr[3][3] = {{3, 8, 7}, {8, 4, 6}, {7, 6, 5}};
+    const R jc = __ldg(p.jac + q);
+    R *out = p.flux + shot * per_shot + (long long)pl * plane + (long long)jj * nxe + ii;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const R t1 = cur(tr[c][0], q), t2 = cur(tr[c][1], q), t3 = cur(tr[c][2], q);
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+        out[(3 * c + a) * kFluxPlanes * plane] = jc * (cv(3 * a, q) * t1 + cv(3 * a + 1, q) * t2 + cv(3 * a + 2, q) * t3);
+    }
+  }
+}
+
 template <int MED, typename TC, int WP, int DX, int DY, int DZ>
 __global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant__ StagePT<real_of<TC>> p) {
   constexpr int DIR[3] = {DX, DY, DZ};
@@ -270,31 +303,30 @@ __global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant_
     if (p.free_top) {
       constexpr int idx_last = dzr ? 3 : 1, idx_first = dzr ? -1 : -3;
       if (k >= nk2 - idx_last) {
-        // sv_curv_col_el_gpu.cu:53-217
+        // sv_curv_col_el_gpu.cu:53-217, on the fluxes k_timg_flux computed for this stage
         const int n_free = nk2 - k - idx_first;
         const R jc = __ldg(p.jac + id);
         const R slwjac = slw / jc;
         constexpr int LXo = op_left(DX), LYo = op_left(DY), LZo = op_left(dzr);
-        // rows of the stress tensor: components (Txx,Txy,Txz), (Txy,Tyy,Tyz), (Txz,Tyz,Tzz)
-        const int tr[3][3] = {{3, 8, 7}, {8, 4, 6}, {7, 6, 5}};
+        const int nxe = p.ni + 6;
+        const long long fpl = (long long)nxe * (p.nj + 6), fcs = kFluxPlanes * fpl;
+        const R *F = p.flux + (long long)shot * 9 * fcs + (long long)(j + 3) * nxe + (i + 3);
+        const int pk = k - (p.nk - kFluxPlanes);  // flux plane of this cell
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-          const int f1 = tr[c][0], f2 = tr[c][1], f3 = tr[c][2];
           R vx[5], vy[5], vz[5];
+          const R *Fx = F + (3 * c + 0) * fcs + pk * fpl, *Fy = F + (3 * c + 1) * fcs + pk * fpl;
+          const R *Fz = F + (3 * c + 2) * fcs;
 #pragma unroll
           for (int n = 0; n < 5; n++) {
-            long long q = id + (n - LXo);
-            vx[n] = __ldg(p.jac + q) * (cv(0, q) * cur(f1, q) + cv(1, q) * cur(f2, q) + cv(2, q) * cur(f3, q));
-            q = id + (long long)(n - LYo) * p.sx;
-            vy[n] = __ldg(p.jac + q) * (cv(3, q) * cur(f1, q) + cv(4, q) * cur(f2, q) + cv(5, q) * cur(f3, q));
+            vx[n] = __ldg(Fx + (n - LXo));
+            vy[n] = __ldg(Fy + (long long)(n - LYo) * nxe);
             int off;
             R sgn;
             if (n < n_free) { off = n - LZo; sgn = R(1); }
             else if (n == n_free) { off = 0; sgn = R(0); }
             else { off = (n - LZo) - 2 * (n - n_free); sgn = R(-1); }
-            q = id + (long long)off * p.sz;
-            R fz = __ldg(p.jac + q) * (cv(6, q) * cur(f1, q) + cv(7, q) * cur(f2, q) + cv(8, q) * cur(f3, q));
-            vz[n] = sgn * fz;
+            vz[n] = sgn * __ldg(Fz + (long long)(pk + off) * fpl);
           }
           R DxTx = drp5<DX>(vx[0], vx[1], vx[2], vx[3], vx[4]);
           R DyTy = drp5<DY>(vy[0], vy[1], vy[2], vy[3], vy[4]);
@@ -655,6 +687,31 @@ static void launch_surface_tc(int med, const StagePT<real_of<TC>> &p, dim3 grid,
   if (med == MED_ISO) launch_surface_med<MED_ISO, TC, WP>(p, grid, block, st);
   else if (med == MED_VTI) launch_surface_med<MED_VTI, TC, WP>(p, grid, block, st);
   else launch_surface_med<MED_ANISO, TC, WP>(p, grid, block, st);
+}
+
+template <typename TC, int WP>
+static void launch_flux_tc(const StagePT<real_of<TC>> &p, cudaStream_t st) {
+  const long long total = (long long)(p.ni + 6) * (p.nj + 6) * kFluxPlanes * p.nshot;
+  const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 8);
+  k_timg_flux<TC, WP><<<blocks, 256, 0, st>>>(p);
+}
+
+int launch_timg_flux(int coef_type, int wave16, const StageP &p, cudaStream_t st) {
+  if (!p.free_top || !p.flux) return 0;
+  if (wave16) {
+    if (p.stage == 0) launch_flux_tc<uint16_t, 1>(p, st);
+    else launch_flux_tc<uint16_t, 2>(p, st);
+  } else if (coef_type == COEF_U16) launch_flux_tc<uint16_t, 0>(p, st);
+  else if (coef_type == COEF_F16) launch_flux_tc<__half, 0>(p, st);
+  else if (coef_type == COEF_BF16) launch_flux_tc<__nv_bfloat16, 0>(p, st);
+  else launch_flux_tc<float, 0>(p, st);
+  return 1;
+}
+
+int launch_timg_flux64(const StagePT<double> &p, cudaStream_t st) {
+  if (!p.free_top || !p.flux) return 0;
+  launch_flux_tc<double, 0>(p, st);
+  return 1;
 }
 
 int launch_stage_surface(int med, int coef_type, int wave16, const StageP &p, cudaStream_t st) {

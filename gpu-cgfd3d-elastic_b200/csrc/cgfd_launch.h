@@ -105,6 +105,9 @@ int launch_stage_bulk(int med, const StagePT<R> &p, int nzc, cudaStream_t st);
 int launch_stage_surface(int med, int coef_type, int wave16, const StageP &p, cudaStream_t st);
 // FP64 build: the surface slab with double storage and arithmetic
 int launch_stage_surface64(int med, const StagePT<double> &p, cudaStream_t st);
+// traction-image fluxes of the stage input for the surface slab (before it, same stream)
+int launch_timg_flux(int coef_type, int wave16, const StageP &p, cudaStream_t st);
+int launch_timg_flux64(const StagePT<double> &p, cudaStream_t st);
 // TMA-pipelined bulk kernel: tile height, one-time function attributes, launch.
 // wave16: FP16 stage levels (requires COEF_F16).
 int tma_tile_y(int med);

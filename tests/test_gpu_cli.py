@@ -108,3 +108,35 @@ def test_cli_snapshots_match_oracle(tmp_path):
         w = states[p.nt_total - 1][0, 3:-3:2, 3:-3:3, 4:-3:2]
         assert np.linalg.norm(vx[0] - w) <= 1e-4 * np.linalg.norm(w)
         assert list(f.index_stride_in_this_thread) == [2, 3, 2]
+
+
+def test_cli_layered_medium_matches_oracle(tmp_path):
+    """medium input_way "infile_layer" with the har equivalent medium: the CLI discretises the
+    layered model on the GPU; its seismograms equal the oracle's run on the medium the
+    reference's own media code builds from the same file (per-station rel L2 <= 1e-4)."""
+    import media_ref
+    if not media_ref.available():
+        pytest.skip("oracle/_ref/libref_media.so not built")
+    from cgfd_b200 import synth
+    nsteps = 60
+    p = small_problem("iso", nsteps=nsteps)
+    model = synth.layer_model(p.coord, seed=4, depths=(-1200.0, -2200.0))
+    lay = os.path.join(str(tmp_path), "model.lay")
+    formats.write_layer_file(lay, model)
+    extra = {"medium": {"type": "elastic_iso", "input_way": "infile_layer", "infile_layer": lay,
+                        "equivalent_medium_method": "har"}}
+    par = formats.write_case(str(tmp_path), p, nsteps, extra=extra)
+    r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    p.metric = synth.metrics(p.coord)
+    p.medium = media_ref.layer2model_el_iso(p.coord, model, 1)
+    orc = Oracle(p)
+    orc.run()
+    ref = orc.seismograms()
+    out = os.path.join(str(tmp_path), "output")
+    got = np.zeros_like(ref)
+    for n, name in enumerate(p.sta.names):
+        for c, cn in enumerate(CMPS):
+            got[n, c] = formats.read_sac(os.path.join(out, f"{name}.{cn}.sac"))[1]
+    assert np.abs(ref).max() > 0
+    assert per_station_rel_l2(got, ref) <= 1e-4
