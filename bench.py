@@ -351,7 +351,7 @@ def media_bench(local, steps=2000):
     return out
 
 
-def serving_bench(local, nreq=40, nmodels=8, mean_gap_s=1.5, seed=11):
+def serving_bench(local, nreq=40, nmodels=8, mean_gap_s=2.5, seed=11):
     """The serving loop on a stream shaped like the serving workload: `nmodels` seeded models
     with grid sizes drawn uniformly between 64^3 and 320x320x160 (x, y in [64, 320], z in
     [64, 160]) and media 50% iso / 30% VTI / 20% 21-Cij aniso (each with its own topography and
