@@ -11,6 +11,7 @@ Two stages, because the oracle runs on the host and the modes on a GPU:
 
     python tests/precision_study.py oracle --cache DIR     # CPU: FP64 oracle seismograms
     python tests/precision_study.py gpu --cache DIR        # GPU: every mode, error table
+    python tests/precision_study.py fp16sol --steps 1500   # GPU: FP16 solution-level bound
 
 `oracle --cache tests/golden` made the committed fixtures tests/golden/fp64_long_{vti,aniso}.npz
 that tests/test_gpu_precision_long.py checks the FP32, fixed-point and mixed modes against.
@@ -83,15 +84,59 @@ def stage_gpu(args):
     print(json.dumps(out))
 
 
+def round_fp16_scaled(w):
+    """FP16 storage of a wavefield with one power-of-two scale per group (velocity, stress),
+    max |w| mapped into [2^12, 2^13) as the FP16 stage levels do: the value read back."""
+    out = np.empty_like(w)
+    for sl in (slice(0, 3), slice(3, 9)):
+        m = float(np.abs(w[sl]).max())
+        if m == 0.0:
+            out[sl] = w[sl]
+            continue
+        e = int(np.floor(np.log2(m))) - 12
+        sc = 2.0 ** e
+        out[sl] = (w[sl].astype(np.float64) / sc).astype(np.float16).astype(np.float64) * sc
+    return out.astype(np.float32)
+
+
+def stage_fp16sol(args):
+    """Lower bound of the error of FP16 solution levels: the FP64 build of the kernels, its
+    solution level w_pre rounded to scaled FP16 after every time step (through
+    cgfd_get_wavefield / cgfd_set_wavefield), against the same FP64 run without rounding. A
+    real FP16-solution mode rounds at least this often (every RK stage's accumulator too), so
+    an error above the bar here rules it out."""
+    from cgfd_b200 import Simulation, CGFD_PREC_FP64
+    from helpers import rel_l2, per_station_rel_l2
+    out = {"grid": f"{args.ni}x{args.nj}x{args.nk}", "steps": args.steps}
+    for med in MEDIA:
+        p = problem(med, args.ni, args.nj, args.nk, args.steps)
+        p.precision = CGFD_PREC_FP64
+        ref = Simulation(p)
+        ref.run(args.steps)
+        r = ref.seismograms()[:, :, :args.steps]
+        ref.close()
+        sim = Simulation(p)
+        for it in range(args.steps):
+            sim.run(1)
+            sim.set_wavefield(round_fp16_scaled(sim.wavefield()))
+        s = sim.seismograms()[:, :, :args.steps]
+        sim.close()
+        e = {"gather_rel_l2": rel_l2(s, r), "station_rel_l2": per_station_rel_l2(s, r)}
+        out[med] = e
+        print(f"{med:6s} FP16 solution level (per-step rounding) gather {e['gather_rel_l2']:.2e}  "
+              f"station {e['station_rel_l2']:.2e}", flush=True)
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("stage", choices=["oracle", "gpu"])
-    ap.add_argument("--cache", required=True, help="directory of the FP64 oracle seismograms")
+    ap.add_argument("stage", choices=["oracle", "gpu", "fp16sol"])
+    ap.add_argument("--cache", default=None, help="directory of the FP64 oracle seismograms (oracle, gpu)")
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--grid", type=int, nargs=3, default=(128, 128, 64))
     args = ap.parse_args()
     args.ni, args.nj, args.nk = args.grid
-    (stage_oracle if args.stage == "oracle" else stage_gpu)(args)
+    {"oracle": stage_oracle, "gpu": stage_gpu, "fp16sol": stage_fp16sol}[args.stage](args)
 
 
 if __name__ == "__main__":
