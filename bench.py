@@ -52,7 +52,8 @@ def parse():
     ap.add_argument("--grid", type=int, nargs=3, default=None, help="override ni nj nk (profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--zchunk", type=int, default=0)
+    ap.add_argument("--zchunk", type=int, default=0, help="fixed z chunk (skips the autotuner)")
+    ap.add_argument("--no-autotune", action="store_true", help="default tile shape and z chunk")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched / mixed-precision section")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
     ap.add_argument("--no-media", action="store_true", help="skip the VTI / aniso section")
@@ -507,8 +508,15 @@ def main():
     cells = p.ni * p.nj * p.nk
     nbulk = p.nk - 4
     sim = Simulation(p)
+    tuned = None
     if args.zchunk:
         sim.set_zchunk(args.zchunk)
+    elif not args.no_autotune:
+        # cgfd_autotune: both tile shapes x the z-chunk candidates timed on this problem (4 steps
+        # each), before the warm-up; the state is reset to step 0 afterwards
+        t = time.perf_counter()
+        sim.autotune(4)
+        tuned = {"tile_shape": sim.tile_shape, "zchunk": sim.zchunk, "tuning_s": time.perf_counter() - t}
     st = torch.cuda.ExternalStream(sim.stream)
     # warm-up: W steps, at least 8 so that the CUDA graph of every step of the 8-step
     # operator-pair cycle is captured before the timed region
@@ -633,7 +641,8 @@ def main():
                "config": {"workload": f"{p.ni}x{p.nj}x{p.nk}", "medium": "elastic_iso", "dh_m": 50.0,
                           "pml_layers": 20, "free_surface": "timg", "sources": 1, "stations": 400,
                           "dt": p.dt, "precision": "fp32", "parallelism": f"replicas x{world}",
-                          "l2": f"inputs larger than L2 (wavefield 4 levels x 9 x {(p.ni + 6) * (p.nj + 6) * (p.nk + 6) / 1e6:.1f}M floats)"},
+                          "l2": f"inputs larger than L2 (wavefield 4 levels x 9 x {(p.ni + 6) * (p.nj + 6) * (p.nk + 6) / 1e6:.1f}M floats)",
+                          "autotuned": tuned},
                "roofline": roof, "cpu_baseline": cpu, "reference_gpu_kernels": ref_gpu, "e2e": e2e,
                "gpu_launches": launches,
                "clocks": clocks, "batched_mixed": batched, "media": media, "serving": serving}

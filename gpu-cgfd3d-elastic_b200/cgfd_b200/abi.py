@@ -288,6 +288,8 @@ def lib():
         "cgfd_get_wavefield": (C.c_int, [P, P]),
         "cgfd_get_peak_motion": (C.c_int, [P, C.c_int, P]),
         "cgfd_set_line_receivers": (C.c_int, [P, C.c_int, P]),
+        "cgfd_set_tile_shape": (C.c_int, [P, C.c_int]),
+        "cgfd_get_tile_shape": (C.c_int, [P]),
         "cgfd_get_line_seismograms": (C.c_int, [P, P]),
         "cgfd_set_slices": (C.c_int, [P, C.c_int, P, C.c_int, P, C.c_int, P, C.c_int]),
         "cgfd_get_slices": (C.c_int, [P, C.c_int, C.c_int, P]),
@@ -483,6 +485,13 @@ class Simulation:
     @property
     def zchunk(self):
         return lib().cgfd_get_zchunk(self.h)
+
+    def set_tile_shape(self, shape):
+        check(lib().cgfd_set_tile_shape(self.h, int(shape)))
+
+    @property
+    def tile_shape(self):
+        return lib().cgfd_get_tile_shape(self.h)
 
     def set_bulk_variant(self, tma):
         check(lib().cgfd_set_bulk_variant(self.h, int(tma)))

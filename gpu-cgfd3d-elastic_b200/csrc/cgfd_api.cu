@@ -137,6 +137,7 @@ struct cgfd_problem {
   long long sx = 0, sz = 0, sf = 0, off0 = 0;
   size_t bytes = 0;
   int nzc = 16;
+  int shape = 0;  // tile shape of the bulk kernel (0 default, 1 alternative; cgfd_set_tile_shape)
 
   float *wbuf[4] = {nullptr, nullptr, nullptr, nullptr};  // [0],[1]: pre/end by parity; [2],[3]: tmpA/tmpB
   // (real-typed arrays -- wbuf, coef, jac, matx/maty, PML A/B/D/aux, d_dis -- are held as float*
@@ -409,7 +410,7 @@ struct cgfd_problem {
             CK(cudaEventRecord(ev_fork, st));
             CK(cudaStreamWaitEvent(side, ev_fork, 0));
           }
-          int k = cgfd::launch_stage_bulk_tma(med, coef_type, wave16, p, tm, tiles, st, fork ? side : st);
+          int k = cgfd::launch_stage_bulk_tma(med, coef_type, wave16, shape, p, tm, tiles, st, fork ? side : st);
           if (surface_done)
             k += cgfd::launch_timg_flux(coef_type, wave16, p, side) +
                  cgfd::launch_stage_surface(med, coef_type, wave16, p, side);
@@ -743,6 +744,7 @@ std::vector<float> source_bounds(const cgfd_problem *p) {
 }
 
 void make_tiles(cgfd_problem *p);
+void make_maps(cgfd_problem *p);
 float *noalloc_scratch(int device);
 
 // sources given by physical coordinates: located on the current device (nullptr otherwise)
@@ -831,29 +833,7 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   if (p->coef_type != cgfd::COEF_F32) to_16bit_coefficients(p);
 
   // TMA tensor maps of the four wavefield levels and of the coefficients
-  if (!p->fp64) {
-    int ty = cgfd::tma_tile_y(p->med);
-    for (int l = 0; l < 4; l++) {
-      if (lev_bytes[l] == 2) {  // FP16 stage level: x halo of 8 elements keeps the box 16-byte aligned
-        make_map(&p->map_halo[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX + 16,
-                 ty + 4, 9, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2);
-        make_map(&p->map_ctr[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX, ty, 9,
-                 CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2);
-        continue;
-      }
-      make_map(&p->map_halo[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX + 8, ty + 4, 9);
-      make_map(&p->map_ctr[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX, ty, 9);
-    }
-    if (p->coef_type == cgfd::COEF_F32)
-      make_map(&p->map_coef, p->coef, p->sx, p->nj + 6, p->nk + 6, p->ncoef, p->sz, p->sf, cgfd::TX, ty, p->ncoef);
-    else
-      make_map(&p->map_coef, p->coef16, p->sx, p->nj + 6, p->nk + 6, p->ncoef, p->sz, p->sf, cgfd::TX, ty, p->ncoef,
-               p->coef_type == cgfd::COEF_F16    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
-               : p->coef_type == cgfd::COEF_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
-                                                 : CU_TENSOR_MAP_DATA_TYPE_UINT16,
-               2);
-    CK(cgfd::tma_prepare(p->med, p->coef_type, p->wave16));
-  }
+  if (!p->fp64) make_maps(p);
   // free surface
   if (p->free_top) {
     std::vector<float> mx, my;
@@ -1008,12 +988,41 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   CK(cudaDeviceSynchronize());
 }
 
+// TMA tensor maps of the four wavefield levels and of the coefficients for the current tile
+// shape (box heights follow the tile), and the bulk kernels' shared-memory attributes.
+void make_maps(cgfd_problem *p) {
+  const int nshot = p->nshot;
+  {
+    const int ty = cgfd::tma_tile_y(p->med, p->shape);
+    for (int l = 0; l < 4; l++) {
+      if (p->wave16 && l >= 2) {  // FP16 stage level: x halo of 8 elements keeps the box 16-byte aligned
+        make_map(&p->map_halo[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX + 16,
+                 ty + 4, 9, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2);
+        make_map(&p->map_ctr[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX, ty, 9,
+                 CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2);
+        continue;
+      }
+      make_map(&p->map_halo[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX + 8, ty + 4, 9);
+      make_map(&p->map_ctr[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX, ty, 9);
+    }
+    if (p->coef_type == cgfd::COEF_F32)
+      make_map(&p->map_coef, p->coef, p->sx, p->nj + 6, p->nk + 6, p->ncoef, p->sz, p->sf, cgfd::TX, ty, p->ncoef);
+    else
+      make_map(&p->map_coef, p->coef16, p->sx, p->nj + 6, p->nk + 6, p->ncoef, p->sz, p->sf, cgfd::TX, ty, p->ncoef,
+               p->coef_type == cgfd::COEF_F16    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+               : p->coef_type == cgfd::COEF_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                 : CU_TENSOR_MAP_DATA_TYPE_UINT16,
+               2);
+    CK(cgfd::tma_prepare(p->med, p->coef_type, p->wave16, p->shape));
+  }
+}
+
 // Tile lists of the TMA bulk kernel: 32 x TY columns, split along z into chunks of about
 // nzc planes that never straddle a z-face boundary of the CFS-PML (so planes above the
 // bottom absorbing layer run as interior tiles), and sorted by whether any PML face box meets
 // the tile's volume. Entries (bx, by, first plane, end plane), x fastest.
 void make_tiles(cgfd_problem *p) {
-  const int ty = cgfd::tma_tile_y(p->med), nbulk = p->free_top ? p->nk - cgfd::NSURF : p->nk;
+  const int ty = cgfd::tma_tile_y(p->med, p->shape), nbulk = p->free_top ? p->nk - cgfd::NSURF : p->nk;
   const int nbx = (p->ni + cgfd::TX - 1) / cgfd::TX, nby = (p->nj + ty - 1) / ty;
   std::vector<int> cuts = {0, nbulk};
   for (const auto &f : p->faces)
@@ -1555,24 +1564,49 @@ int cgfd_set_zchunk(cgfd_problem *p, int nzc) {
 
 int cgfd_get_zchunk(const cgfd_problem *p) { return p ? p->nzc : -1; }
 
+/* Tile shape of the TMA bulk kernel (0 default, 1 alternative); maps, tiles and graphs are rebuilt. */
+int cgfd_set_tile_shape(cgfd_problem *p, int shape) {
+  if (!p || shape < 0 || shape > 1) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
+  if (!p->use_tma) { set_err("tile shapes belong to the TMA bulk kernel"); return CGFD_ERR_UNSUPPORTED; }
+  return guarded([&] {
+    CK(cudaSetDevice(p->device));
+    CK(cudaStreamSynchronize(p->stream));
+    p->shape = shape;
+    make_maps(p);
+    make_tiles(p);
+    for (int s = 0; s < 8; s++)
+      if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }
+  });
+}
+
+int cgfd_get_tile_shape(const cgfd_problem *p) { return p ? p->shape : -1; }
+
 int cgfd_autotune(cgfd_problem *p, int steps, int *chosen) {
   if (!p || steps < 1) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
   if (p->it != 0) { set_err("autotuning runs on a problem that has not stepped yet (step 0)"); return CGFD_ERR_INVALID; }
   return guarded([&] {
     CK(cudaSetDevice(p->device));
     const int nbulk = p->free_top ? p->nk - cgfd::NSURF : p->nk;
-    std::vector<int> cand;
+    std::vector<int> zc;
     for (int c : {8, 12, 16, 24, 32, 48, 64, 96, nbulk})
-      if (c >= 1 && c <= nbulk && std::find(cand.begin(), cand.end(), c) == cand.end()) cand.push_back(c);
+      if (c >= 1 && c <= nbulk && std::find(zc.begin(), zc.end(), c) == zc.end()) zc.push_back(c);
+    std::vector<std::pair<int, int>> cand;  // (tile shape, z chunk); the FP64 build has no TMA kernel
+    for (int sh = 0; sh < (p->use_tma ? 2 : 1); sh++)
+      for (int c : zc) cand.emplace_back(sh, c);
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    int best = p->nzc;
+    int best = p->nzc, best_shape = p->shape;
     float best_ms = 1e30f;
     const bool timing = p->timing;
     p->timing = false;
-    for (int c : cand) {
+    for (const auto &sc : cand) {
+      const int c = sc.second;
       CK(cudaStreamSynchronize(p->stream));
+      if (p->use_tma && sc.first != p->shape) {
+        p->shape = sc.first;
+        make_maps(p);
+      }
       p->nzc = c;
       make_tiles(p);
       for (int s = 0; s < 8; s++)
@@ -1584,12 +1618,16 @@ int cgfd_autotune(cgfd_problem *p, int steps, int *chosen) {
       CK(cudaEventSynchronize(e1));
       float ms = 0.f;
       CK(cudaEventElapsedTime(&ms, e0, e1));
-      if (ms < best_ms) { best_ms = ms; best = c; }
+      if (ms < best_ms) { best_ms = ms; best = c; best_shape = sc.first; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     p->timing = timing;
     CK(cudaStreamSynchronize(p->stream));
+    if (p->use_tma && best_shape != p->shape) {
+      p->shape = best_shape;
+      make_maps(p);
+    }
     p->nzc = best;
     make_tiles(p);
     for (int s = 0; s < 8; s++)

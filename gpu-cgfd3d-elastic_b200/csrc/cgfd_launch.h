@@ -110,8 +110,9 @@ int launch_timg_flux(int coef_type, int wave16, const StageP &p, cudaStream_t st
 int launch_timg_flux64(const StagePT<double> &p, cudaStream_t st);
 // TMA-pipelined bulk kernel: tile height, one-time function attributes, launch.
 // wave16: FP16 stage levels (requires COEF_F16).
-int tma_tile_y(int med);
-cudaError_t tma_prepare(int med, int coef_type, int wave16);
+// shape: tile shape index (0 default, 1 the alternative; cgfd_bulk_tma.cuh TileShape)
+int tma_tile_y(int med, int shape);
+cudaError_t tma_prepare(int med, int coef_type, int wave16, int shape);
 // Tile lists of the TMA bulk kernel (device arrays, one int4 per tile: bx, by, first and
 // end z plane): tiles no CFS-PML face touches, and the rest.
 struct BulkTiles {
@@ -119,7 +120,8 @@ struct BulkTiles {
   int ninterior = 0, npml = 0;
 };
 // Interior tiles go to st, PML tiles to st_pml (may be st).
-int launch_stage_bulk_tma(int med, int coef_type, int wave16, const StageP &p, const TmaP &tm, const BulkTiles &t,
+int launch_stage_bulk_tma(int med, int coef_type, int wave16, int shape, const StageP &p, const TmaP &tm,
+                          const BulkTiles &t,
                           cudaStream_t st, cudaStream_t st_pml);
 // FP16 stage levels: per-step scale from the last step's max |w| and the step's source bound
 int launch_wave_scale(unsigned int *amax, const float *srcb, const int *d_it, int nt_total, int nshot, float *wsc,

@@ -324,12 +324,21 @@ int cgfd_set_zchunk(cgfd_problem *p, int nzc);
 int cgfd_get_zchunk(const cgfd_problem *p);
 
 /*
- * Autotuner of the bulk kernel's z-chunk length (planes per thread block column; the tile
- * shape's free parameter): times `steps` graph-replayed time steps for each candidate
- * (8, 12, 16, 24, 32, 48, 64, 96 and all bulk planes) on this problem, keeps the fastest
- * (*chosen) and returns the problem to its freshly created state (zero wavefield, step 0).
- * Only on a problem that has not stepped yet. Results do not depend on the chunk length.
- * No counterpart in the reference.
+ * Tile shape of the TMA bulk kernel: 0 (default) or 1 (the alternative), per medium
+ *   iso, VTI: 32x8 columns at two blocks per SM | 32x4 at three blocks per SM
+ *   21-Cij:   32x4 at three blocks per SM      | 32x8 at one block per SM (w_pre staged too).
+ * Results do not depend on the shape (the per-cell arithmetic is the same).
+ */
+int cgfd_set_tile_shape(cgfd_problem *p, int shape);
+int cgfd_get_tile_shape(const cgfd_problem *p);
+
+/*
+ * Autotuner of the bulk kernel's tile: times `steps` graph-replayed time steps for each tile
+ * shape (cgfd_set_tile_shape) and z-chunk length (planes per thread block column: 8, 12, 16,
+ * 24, 32, 48, 64, 96 and all bulk planes) on this problem, keeps the fastest pair (*chosen:
+ * the z chunk; cgfd_get_tile_shape: the shape) and returns the problem to its freshly created
+ * state (zero wavefield, step 0). Only on a problem that has not stepped yet. Results do not
+ * depend on the choice. No counterpart in the reference.
  */
 int cgfd_autotune(cgfd_problem *p, int steps, int *chosen);
 
