@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--zchunk", type=int, default=0, help="fixed z chunk (skips the autotuner)")
+    ap.add_argument("--tile-shape", type=int, default=-1, help="fixed bulk tile shape 0/1 (with --zchunk: no autotuner)")
     ap.add_argument("--no-autotune", action="store_true", help="default tile shape and z chunk")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched / mixed-precision section")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
@@ -509,6 +510,8 @@ def main():
     nbulk = p.nk - 4
     sim = Simulation(p)
     tuned = None
+    if args.tile_shape >= 0:
+        sim.set_tile_shape(args.tile_shape)
     if args.zchunk:
         sim.set_zchunk(args.zchunk)
     elif not args.no_autotune:

@@ -216,16 +216,24 @@ int main(int argc, char **argv) {
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0);
-  for (int it = 0; it < nsteps; it++) {
-    io_recv_keep(&iorecv, w_pre_d, w_buff, it, wav.ncmp, wav.siz_icmp);
-    int ipair = it % fd.num_of_pairs;
-    for (int istage = 0; istage < fd.num_rk_stages; istage++) {
-      w_cur_d = istage == 0 ? w_pre_d : w_tmp_d;
+  // Statement by statement against drv_rk_curv_col.cu (line numbers of that file). Left out:
+  // io_line_keep / io_slice_nc_put / io_snap_nc_put (:203-215; outputs the harness does not
+  // write), the MPI message pack / start / wait / unpack (:336, :353-355, :407-408, :461-462,
+  // :492-501; one rank, no neighbours), the acoustic and visco-elastic branches (:265-276,
+  // :317-331, :479-490), the stubbed NaN check (:507-510) and the exponential sponge (:513-515,
+  // not enabled by the cases). The per-stage cudaDeviceSynchronize (:333) is implied by the
+  // default stream's ordering.
+  for (int it = 0; it < nsteps; it++) {  // :193
+    io_recv_keep(&iorecv, w_pre_d, w_buff, it, wav.ncmp, wav.siz_icmp);  // :200
+    int ipair = it % fd.num_of_pairs;                                     // :221
+    for (int istage = 0; istage < fd.num_rk_stages; istage++) {         // :224
+      w_cur_d = istage == 0 ? w_pre_d : w_tmp_d;                          // :237-257
       if (bdrypml_d.is_enable_pml == 1)
         for (int a = 0; a < CONST_NDIM; a++)
           for (int s = 0; s < 2; s++)
             bdrypml_d.auxvar[a][s].cur = istage == 0 ? bdrypml_d.auxvar[a][s].pre : bdrypml_d.auxvar[a][s].tmp;
-      src_set_time(&src_d, it, istage);
+      src_set_time(&src_d, it, istage);  // :260
+      // :263-315, the three elastic media
       if (md_d.medium_type == CONST_MEDIUM_ELASTIC_ISO)
         sv_curv_col_el_iso_onestage(w_cur_d, w_rhs_d, wav_d, fd_wav_d, gd_d, metric_d, md_d, bdrypml_d, bdryfree_d, src_d,
                                     fd.num_of_fdx_op, fd.pair_fdx_op[ipair][istage], fd.num_of_fdy_op,
@@ -255,32 +263,32 @@ int main(int argc, char **argv) {
               else wav_update_end<<<g2, block>>>(x->siz_ilevel, coef, x->end, x->rhs);
             }
       };
-      if (istage == 0) {
+      if (istage == 0) {  // :339-395
         float ca = fd.rk_a[istage] * dt, cb = fd.rk_b[istage] * dt;
-        wav_update<<<grid, block>>>(wav_d.siz_ilevel, ca, w_tmp_d, w_pre_d, w_rhs_d);
-        aux_update(0, ca);
-        wav_update<<<grid, block>>>(wav_d.siz_ilevel, cb, w_end_d, w_pre_d, w_rhs_d);
-        aux_update(1, cb);
-      } else if (istage < fd.num_rk_stages - 1) {
+        wav_update<<<grid, block>>>(wav_d.siz_ilevel, ca, w_tmp_d, w_pre_d, w_rhs_d);  // :349
+        aux_update(0, ca);                                                              // :358-372
+        wav_update<<<grid, block>>>(wav_d.siz_ilevel, cb, w_end_d, w_pre_d, w_rhs_d);  // :378
+        aux_update(1, cb);                                                              // :381-395
+      } else if (istage < fd.num_rk_stages - 1) {  // :396-447
         float ca = fd.rk_a[istage] * dt, cb = fd.rk_b[istage] * dt;
-        wav_update<<<grid, block>>>(wav_d.siz_ilevel, ca, w_tmp_d, w_pre_d, w_rhs_d);
-        aux_update(0, ca);
-        wav_update_end<<<grid, block>>>(wav_d.siz_ilevel, cb, w_end_d, w_rhs_d);
-        aux_update(2, cb);
-      } else {
+        wav_update<<<grid, block>>>(wav_d.siz_ilevel, ca, w_tmp_d, w_pre_d, w_rhs_d);  // :403
+        aux_update(0, ca);                                                              // :410-424
+        wav_update_end<<<grid, block>>>(wav_d.siz_ilevel, cb, w_end_d, w_rhs_d);       // :430
+        aux_update(2, cb);                                                              // :433-447
+      } else {  // :448-478
         float cb = fd.rk_b[istage] * dt;
-        wav_update_end<<<grid, block>>>(wav_d.siz_ilevel, cb, w_end_d, w_rhs_d);
-        aux_update(2, cb);
+        wav_update_end<<<grid, block>>>(wav_d.siz_ilevel, cb, w_end_d, w_rhs_d);  // :456
+        aux_update(2, cb);                                                         // :464-478
       }
     }
     if (free_top) {  // drv_rk_curv_col.cu:519-527
       dim3 pb(8, 8), pgr((ni + 7) / 8, (nj + 7) / 8);
       PG_calcu_gpu<<<pgr, pb>>>(w_end_d, w_pre_d, gd_d, PG_d, Dis_accu_d, dt);
     }
-    float *t = w_pre_d;
+    float *t = w_pre_d;  // :529
     w_pre_d = w_end_d;
     w_end_d = t;
-    if (bdrypml_d.is_enable_pml == 1)
+    if (bdrypml_d.is_enable_pml == 1)  // :531-541
       for (int a = 0; a < CONST_NDIM; a++)
         for (int s = 0; s < 2; s++) {
           bdrypml_auxvar_t *x = &(bdrypml_d.auxvar[a][s]);
