@@ -204,8 +204,9 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(workload, cells_per_launch):
-    """DRAM bytes per bulk-kernel launch from the committed ncu summary, scaled by cells."""
+def ncu_traffic(workload, cells_per_launch, shape, zchunk):
+    """DRAM bytes per bulk-kernel launch (one RK stage) from the committed ncu summary of the
+    same tile shape and z chunk, scaled by cells; None when no capture of that choice exists."""
     path = os.path.join(ROOT, "profiles", "k_stage_bulk_iso.md")
     try:
         vals = {}
@@ -214,7 +215,7 @@ def ncu_traffic(workload, cells_per_launch):
                 if ":" in ln and ln.strip().startswith("- "):
                     k, v = ln.strip()[2:].split(":", 1)
                     vals[k.strip()] = v.strip().split()[0]
-        b = float(vals["dram_bytes_per_launch"])
+        b = float(vals[f"dram_bytes_per_launch_shape{shape}_zchunk{zchunk}"])
         c = float(vals["cells_per_launch"])
         return b * cells_per_launch / c
     except Exception:
@@ -520,6 +521,7 @@ def main():
         t = time.perf_counter()
         sim.autotune(4)
         tuned = {"tile_shape": sim.tile_shape, "zchunk": sim.zchunk, "tuning_s": time.perf_counter() - t}
+    shape_used, zchunk_used = sim.tile_shape, sim.zchunk
     st = torch.cuda.ExternalStream(sim.stream)
     # warm-up: W steps, at least 8 so that the CUDA graph of every step of the 8-step
     # operator-pair cycle is captured before the timed region
@@ -567,7 +569,7 @@ def main():
     alg = bpc * bulk_cells
     achieved = alg / (bulk_ms / bulk_n * 1e-3) / 1e9 if bulk_n else None
     peak, peak_kind = measured_peak()
-    traffic = ncu_traffic(args.workload, bulk_cells)
+    traffic = ncu_traffic(args.workload, bulk_cells, shape_used, zchunk_used)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "traffic": traffic,
             "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback",
