@@ -243,7 +243,8 @@ def batched_mixed(local, steps=16):
     fc 2-5 Hz, 200 surface stations): source x time steps per second of the plain FP32 path
     (one source per simulation) against batches of S shots in FP32, in 16-bit fixed-point
     coefficients and in the mixed mode (16-bit coefficients + FP16 RK stage levels), each with
-    its seismogram error against the FP64 build of the same kernels."""
+    its seismogram error against the FP64 build of the same kernels. Every problem is autotuned
+    (tile shape, z chunk and, for batches, the shot group) before it is timed."""
     import dataclasses
     from cgfd_b200 import synth, Simulation, CGFD_PREC_FP32, CGFD_PREC_U16_COEF, CGFD_PREC_FP16_WAVE
     ni, nj, nk, nsteps = 256, 256, 128, 1500
@@ -265,20 +266,25 @@ def batched_mixed(local, steps=16):
     ref = s64.seismograms()[:, :, :nacc]
     s64.close()
     one = Simulation(dataclasses.replace(p, src=shots[0]))
+    one.autotune(4)
+    plain_tuned = {"tile_shape": one.tile_shape, "zchunk": one.zchunk}
     plain_ms = _time_steps(one, steps)
     one.run(nacc - one.step)
     plain_err = rel_l2(one.seismograms()[:, :, :nacc], ref)
     one.close()
     out["plain_fp32"] = {"source_steps_per_s": 1e3 / plain_ms, "ms_per_step": plain_ms,
-                         "seismo_rel_l2_vs_fp64": plain_err, "seismo_steps_compared": nacc}
+                         "seismo_rel_l2_vs_fp64": plain_err, "seismo_steps_compared": nacc,
+                         "autotuned": plain_tuned}
     for name, prec in (("batched_fp32", CGFD_PREC_FP32), ("batched_u16coef", CGFD_PREC_U16_COEF),
                        ("batched_mixed", CGFD_PREC_FP16_WAVE)):
         for nshot in (8, 32):
             q = dataclasses.replace(p, precision=prec)
             b = Simulation(q, shots=shots[:nshot])
+            b.autotune(2)
             ms = _time_steps(b, steps)
             rec = {"shots": nshot, "ms_per_step": ms, "source_steps_per_s": nshot * 1e3 / ms,
-                   "vs_plain": nshot * plain_ms / ms, "device_gb": b.device_bytes() / 1e9}
+                   "vs_plain": nshot * plain_ms / ms, "device_gb": b.device_bytes() / 1e9,
+                   "autotuned": {"tile_shape": b.tile_shape, "zchunk": b.zchunk, "shot_group": b.shot_group}}
             if nshot == 8:
                 b.run(nacc - b.step)
                 rec["seismo_rel_l2_vs_fp64"] = rel_l2(b.seismograms()[0][:, :, :nacc], ref)

@@ -290,6 +290,8 @@ def lib():
         "cgfd_set_line_receivers": (C.c_int, [P, C.c_int, P]),
         "cgfd_set_tile_shape": (C.c_int, [P, C.c_int]),
         "cgfd_get_tile_shape": (C.c_int, [P]),
+        "cgfd_set_shot_group": (C.c_int, [P, C.c_int]),
+        "cgfd_get_shot_group": (C.c_int, [P]),
         "cgfd_get_line_seismograms": (C.c_int, [P, P]),
         "cgfd_set_slices": (C.c_int, [P, C.c_int, P, C.c_int, P, C.c_int, P, C.c_int]),
         "cgfd_get_slices": (C.c_int, [P, C.c_int, C.c_int, P]),
@@ -492,6 +494,13 @@ class Simulation:
     @property
     def tile_shape(self):
         return lib().cgfd_get_tile_shape(self.h)
+
+    def set_shot_group(self, group):
+        check(lib().cgfd_set_shot_group(self.h, int(group)))
+
+    @property
+    def shot_group(self):
+        return lib().cgfd_get_shot_group(self.h)
 
     def set_bulk_variant(self, tma):
         check(lib().cgfd_set_bulk_variant(self.h, int(tma)))

@@ -130,6 +130,7 @@ struct cgfd_problem {
   cudaStream_t stream = nullptr;
   int ni = 0, nj = 0, nk = 0, med = 0, ncoef = 0, nt_total = 0, free_top = 0;
   int nshot = 1;  // wavefields sharing the grid, coefficients and stations
+  int shot_group = 8;  // bulk kernel: shots per block group of a batch (cgfd_set_shot_group)
   // FP64 build (CGFD_PREC_FP64): every real-typed device array below holds doubles (esz 8)
   int fp64 = 0;
   size_t esz = 4;
@@ -155,8 +156,8 @@ struct cgfd_problem {
   // source increment of each step)
   int wave16 = 0;
   // TMA bulk kernel tile lists for the current z chunk (interior tiles, then PML tiles)
-  int4 *d_tiles = nullptr;
-  cgfd::BulkTiles tiles;
+  int4 *d_tiles = nullptr, *d_tiles_dn = nullptr;
+  cgfd::BulkTiles tiles, tiles_dn;  // z layers upwards (backward z operators) / downwards
   // PML tiles run on `side`, forked from and joined back into `stream` at every stage
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -410,7 +411,8 @@ struct cgfd_problem {
             CK(cudaEventRecord(ev_fork, st));
             CK(cudaStreamWaitEvent(side, ev_fork, 0));
           }
-          int k = cgfd::launch_stage_bulk_tma(med, coef_type, wave16, shape, p, tm, tiles, st, fork ? side : st);
+          int k = cgfd::launch_stage_bulk_tma(med, coef_type, wave16, shape, p, tm, p.dir[2] ? tiles_dn : tiles, st,
+                                              fork ? side : st);
           if (surface_done)
             k += cgfd::launch_timg_flux(coef_type, wave16, p, side) +
                  cgfd::launch_stage_surface(med, coef_type, wave16, p, side);
@@ -488,7 +490,8 @@ struct cgfd_problem {
       dfree(coef, st); dfree(coef16, st); dfree(jac, st); dfree(matx, st); dfree(maty, st); dfree(d_flux, st);
       for (Face &f : faces) { dfree(f.A, st); dfree(f.B, st); dfree(f.D, st); dfree(f.aux, st); }
       dfree(d_it_begin, st); dfree(d_ext_num, st); dfree(d_src_shot, st); dfree(d_ext_idx, st); dfree(d_ext_wv, st);
-      dfree(d_ext_wt, st); dfree(d_wsc, st); dfree(d_srcb, st); dfree(d_amax, st); dfree(d_tiles, st); dfree(d_pg, st);
+      dfree(d_ext_wt, st); dfree(d_wsc, st); dfree(d_srcb, st); dfree(d_amax, st); dfree(d_tiles, st);
+      dfree(d_tiles_dn, st); dfree(d_pg, st);
       dfree(d_dis, st); dfree(d_box, st); dfree(d_stf, st); dfree(d_idx8, st); dfree(d_w8, st); dfree(d_seis, st);
       dfree(d_line_idx8, st); dfree(d_line_w8, st); dfree(d_line_seis, st); dfree(d_slice_idx, st); dfree(d_slices, st);
       dfree(d_it, st); dfree(d_flag, st);
@@ -663,7 +666,7 @@ void layout(int ni, int nj, int nk, long long &sx, long long &sz, long long &sf,
 void problem_bytes(const cgfd_problem_desc *d, int nshot, const cgfd_source_desc *shots, size_t *resident,
                    size_t *peak) {
   cgfd::validate_desc(d);
-  if (nshot < 1) throw cgfd::Error(CGFD_ERR_INVALID, "nshot must be >= 1");
+  if (nshot < 1 || nshot > 32767) throw cgfd::Error(CGFD_ERR_INVALID, "nshot must be in [1, 32767]");
   long long sx, sz, sf, off0;
   layout(d->ni, d->nj, d->nk, sx, sz, sf, off0);
   const int ncoef = d->medium_type == CGFD_MEDIUM_ELASTIC_ISO ? 12 : (d->medium_type == CGFD_MEDIUM_ELASTIC_VTI ? 15 : 31);
@@ -757,7 +760,7 @@ const cgfd::Located *locate_sources(const cgfd_problem_desc *d, cgfd::Located &o
 
 void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_source_desc *shots) {
   cgfd::validate_desc(d);
-  if (nshot < 1) throw cgfd::Error(CGFD_ERR_INVALID, "nshot must be >= 1");
+  if (nshot < 1 || nshot > 32767) throw cgfd::Error(CGFD_ERR_INVALID, "nshot must be in [1, 32767]");
   p->nshot = nshot;
   p->precision = d->precision;
   switch (d->precision) {
@@ -1021,6 +1024,12 @@ void make_maps(cgfd_problem *p) {
 // nzc planes that never straddle a z-face boundary of the CFS-PML (so planes above the
 // bottom absorbing layer run as interior tiles), and sorted by whether any PML face box meets
 // the tile's volume. Entries (bx, by, first plane, end plane), x fastest.
+// Order: strips of tile rows, each strip z layer by z layer. A strip's layer holds about as
+// many blocks as the GPU keeps resident, so that a tile's x-y neighbours run beside it at the
+// same planes (their halo rows are read from DRAM once), and the tile's next chunk starts as
+// this one ends (the 3 planes its register queue starts from are still in L2). The layers run
+// in the march direction of the stage's z operator: upwards for backward operators (tiles),
+// downwards for forward ones (tiles_dn).
 void make_tiles(cgfd_problem *p) {
   const int ty = cgfd::tma_tile_y(p->med, p->shape), nbulk = p->free_top ? p->nk - cgfd::NSURF : p->nk;
   const int nbx = (p->ni + cgfd::TX - 1) / cgfd::TX, nby = (p->nj + ty - 1) / ty;
@@ -1036,30 +1045,56 @@ void make_tiles(cgfd_problem *p) {
     const int len = cuts[s + 1] - cuts[s], nch = std::max(1, (len + p->nzc - 1) / p->nzc);
     for (int c = 0; c < nch; c++) zr.emplace_back(cuts[s] + len * c / nch, cuts[s] + len * (c + 1) / nch);
   }
-  std::vector<int4> in, pm;
-  for (const auto &z : zr)
-    for (int by = 0; by < nby; by++)
-      for (int bx = 0; bx < nbx; bx++) {
-        bool touch = false;
-        for (const auto &f : p->faces) {
-          const bool xo = f.h.lo[0] <= bx * cgfd::TX + cgfd::TX - 1 && f.h.hi[0] >= bx * cgfd::TX;
-          const bool yo = f.h.lo[1] <= by * ty + ty - 1 && f.h.hi[1] >= by * ty;
-          const bool zo = f.h.lo[2] <= z.second - 1 && f.h.hi[2] >= z.first;
-          touch |= xo && yo && zo;
-        }
-        (touch ? pm : in).push_back(make_int4(bx, by, z.first, z.second));
+  int nsm = 148;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, p->device));
+  const int group = std::max(1, std::min(p->shot_group, p->nshot));
+  const long long resident = (long long)nsm * cgfd::tma_blocks_per_sm(p->med, p->shape);
+  const int strip = (int)std::max<long long>(1, (resident + (long long)nbx * group - 1) / ((long long)nbx * group));
+  for (int dn = 0; dn < 2; dn++) {
+    std::vector<int4> in, pm;
+    for (int s0 = 0; s0 < nby; s0 += strip)
+      for (size_t zi = 0; zi < zr.size(); zi++) {
+        const auto &z = zr[dn ? zr.size() - 1 - zi : zi];
+        for (int by = s0; by < std::min(nby, s0 + strip); by++)
+          for (int bx = 0; bx < nbx; bx++) {
+            bool touch = false;
+            for (const auto &f : p->faces) {
+              const bool xo = f.h.lo[0] <= bx * cgfd::TX + cgfd::TX - 1 && f.h.hi[0] >= bx * cgfd::TX;
+              const bool yo = f.h.lo[1] <= by * ty + ty - 1 && f.h.hi[1] >= by * ty;
+              const bool zo = f.h.lo[2] <= z.second - 1 && f.h.hi[2] >= z.first;
+              touch |= xo && yo && zo;
+            }
+            (touch ? pm : in).push_back(make_int4(bx, by, z.first, z.second));
+          }
       }
-  dfree(p->d_tiles, p->stream);
-  p->d_tiles = nullptr;
-  std::vector<int4> all(in);
-  all.insert(all.end(), pm.begin(), pm.end());
-  size_t acc = 0;
-  p->d_tiles = dmalloc<int4>(std::max<size_t>(all.size(), 1), acc, p->stream);
-  if (!all.empty()) CK(cudaMemcpy(p->d_tiles, all.data(), all.size() * sizeof(int4), cudaMemcpyHostToDevice));
-  p->tiles.interior = p->d_tiles;
-  p->tiles.ninterior = (int)in.size();
-  p->tiles.pml = p->d_tiles + in.size();
-  p->tiles.npml = (int)pm.size();
+    // batches: one entry per tile and shot, the shots in groups of `group`; a group's entries
+    // cover every tile before the next group's, the shot fastest within a group (the group's
+    // blocks of one tile share its coefficient tiles through L2, and a tile's x-y neighbours of
+    // the same shot stay resident beside it)
+    if (p->nshot > 1)
+      for (auto *lst : {&in, &pm}) {
+        std::vector<int4> ex;
+        ex.reserve(lst->size() * p->nshot);
+        for (int g0 = 0; g0 < p->nshot; g0 += group)
+          for (const int4 &e : *lst)
+            for (int sh = g0; sh < std::min(p->nshot, g0 + group); sh++)
+              ex.push_back(make_int4(e.x + (sh << 16), e.y, e.z, e.w));
+        lst->swap(ex);
+      }
+    int4 *&dt = dn ? p->d_tiles_dn : p->d_tiles;
+    cgfd::BulkTiles &tl = dn ? p->tiles_dn : p->tiles;
+    dfree(dt, p->stream);
+    dt = nullptr;
+    std::vector<int4> all(in);
+    all.insert(all.end(), pm.begin(), pm.end());
+    size_t acc = 0;
+    dt = dmalloc<int4>(std::max<size_t>(all.size(), 1), acc, p->stream);
+    if (!all.empty()) CK(cudaMemcpy(dt, all.data(), all.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    tl.interior = dt;
+    tl.ninterior = (int)in.size();
+    tl.pml = dt + in.size();
+    tl.npml = (int)pm.size();
+  }
 }
 
 // Back to the state right after cgfd_problem_create: zero wavefield levels, PML auxiliaries,
@@ -1581,6 +1616,21 @@ int cgfd_set_tile_shape(cgfd_problem *p, int shape) {
 
 int cgfd_get_tile_shape(const cgfd_problem *p) { return p ? p->shape : -1; }
 
+/* Shots per block group of a batch's bulk kernel; graphs are rebuilt. */
+int cgfd_set_shot_group(cgfd_problem *p, int group) {
+  if (!p || group < 1) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(p->device));
+    CK(cudaStreamSynchronize(p->stream));
+    p->shot_group = group;
+    if (p->use_tma) make_tiles(p);  // the strip height follows the group
+    for (int s = 0; s < 8; s++)
+      if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }
+  });
+}
+
+int cgfd_get_shot_group(const cgfd_problem *p) { return p ? std::max(1, std::min(p->shot_group, p->nshot)) : -1; }
+
 int cgfd_autotune(cgfd_problem *p, int steps, int *chosen) {
   if (!p || steps < 1) { set_err("invalid argument"); return CGFD_ERR_INVALID; }
   if (p->it != 0) { set_err("autotuning runs on a problem that has not stepped yet (step 0)"); return CGFD_ERR_INVALID; }
@@ -1600,6 +1650,19 @@ int cgfd_autotune(cgfd_problem *p, int steps, int *chosen) {
     float best_ms = 1e30f;
     const bool timing = p->timing;
     p->timing = false;
+    // graph-replayed steps of the current choice, after the 8 captures
+    auto time_choice = [&]() {
+      for (int s = 0; s < 8; s++)
+        if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }
+      p->run_steps(8);
+      CK(cudaEventRecord(e0, p->stream));
+      p->run_steps(steps);
+      CK(cudaEventRecord(e1, p->stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      return ms;
+    };
     for (const auto &sc : cand) {
       const int c = sc.second;
       CK(cudaStreamSynchronize(p->stream));
@@ -1609,20 +1672,9 @@ int cgfd_autotune(cgfd_problem *p, int steps, int *chosen) {
       }
       p->nzc = c;
       make_tiles(p);
-      for (int s = 0; s < 8; s++)
-        if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }
-      p->run_steps(8);  // captures the 8 step graphs of this tiling
-      CK(cudaEventRecord(e0, p->stream));
-      p->run_steps(steps);
-      CK(cudaEventRecord(e1, p->stream));
-      CK(cudaEventSynchronize(e1));
-      float ms = 0.f;
-      CK(cudaEventElapsedTime(&ms, e0, e1));
+      const float ms = time_choice();
       if (ms < best_ms) { best_ms = ms; best = c; best_shape = sc.first; }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    p->timing = timing;
     CK(cudaStreamSynchronize(p->stream));
     if (p->use_tma && best_shape != p->shape) {
       p->shape = best_shape;
@@ -1630,6 +1682,27 @@ int cgfd_autotune(cgfd_problem *p, int steps, int *chosen) {
     }
     p->nzc = best;
     make_tiles(p);
+    // batches: the shot group at the chosen tiling (4, 8, 16 or every shot)
+    if (p->use_tma && p->nshot > 1) {
+      int best_g = std::max(1, std::min(p->shot_group, p->nshot));
+      float best_gms = 1e30f;
+      std::vector<int> gc;
+      for (int g : {4, 8, 16, p->nshot})
+        if (g <= p->nshot && std::find(gc.begin(), gc.end(), g) == gc.end()) gc.push_back(g);
+      for (int g : gc) {
+        CK(cudaStreamSynchronize(p->stream));
+        p->shot_group = g;
+        make_tiles(p);
+        const float ms = time_choice();
+        if (ms < best_gms) { best_gms = ms; best_g = g; }
+      }
+      CK(cudaStreamSynchronize(p->stream));
+      p->shot_group = best_g;
+      make_tiles(p);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    p->timing = timing;
     for (int s = 0; s < 8; s++)
       if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }
     reset_state(p);

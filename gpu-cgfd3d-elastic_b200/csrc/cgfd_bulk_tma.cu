@@ -20,6 +20,12 @@ int tma_tile_y(int med, int shape) {
   return shape ? TileShape<MED_ANISO, 1>::TYT : TileShape<MED_ANISO, 0>::TYT;
 }
 
+int tma_blocks_per_sm(int med, int shape) {
+  if (med == MED_ISO) return shape ? TileShape<MED_ISO, 1>::MINB : TileShape<MED_ISO, 0>::MINB;
+  if (med == MED_VTI) return shape ? TileShape<MED_VTI, 1>::MINB : TileShape<MED_VTI, 0>::MINB;
+  return shape ? TileShape<MED_ANISO, 1>::MINB : TileShape<MED_ANISO, 0>::MINB;
+}
+
 cudaError_t tma_prepare(int med, int coef_type, int wave16, int shape) {
   if (med == MED_ISO) return prepare_bulk_tma_med<MED_ISO>(coef_type, wave16, shape);
   if (med == MED_VTI) return prepare_bulk_tma_med<MED_VTI>(coef_type, wave16, shape);

@@ -80,9 +80,9 @@ struct CoefTile {
   __device__ __forceinline__ float operator()(int f) const { return coef_decode<TC>(c[f * STRIDE], p, f); }
 };
 
-// Tiles come from a list (4 ints each: bx, by, first plane, end plane): one list for the
-// tiles that no CFS-PML face touches (PML false: the face code is compiled out, fewer
-// registers) and one for the rest (PML true).
+// Tiles come from a list (4 ints each: bx + (shot << 16), by, first plane, end plane), one
+// block per entry in list order: one list for the tiles that no CFS-PML face touches (PML
+// false: the face code is compiled out, fewer registers) and one for the rest (PML true).
 template <int MED, int DX, int DY, int DZ, int TYT, int MINB, typename TC, int WP, bool PML>
 __global__ void __launch_bounds__(TX *TYT, MINB)
     k_stage_bulk_tma(const __grid_constant__ StageP p, const __grid_constant__ TmaP tm,
@@ -99,11 +99,9 @@ __global__ void __launch_bounds__(TX *TYT, MINB)
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + S::OFF_BAR);  // NW wave, then 2 cpe
 
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  // shots are the fastest block index: the nshot blocks of one tile run side by side and
-  // share the coefficient tiles through L2
-  const int shot = blockIdx.x % p.nshot, tile = blockIdx.x / p.nshot;
-  const int4 tl = __ldg(tiles + tile);
-  const int bx = tl.x, by = tl.y;
+  // one block per list entry, in list order: x = bx + (shot << 16), y = by, z / w = planes
+  const int4 tl = __ldg(tiles + blockIdx.x);
+  const int bx = tl.x & 0xffff, by = tl.y, shot = tl.x >> 16;
   const int i = bx * TX + tx, j = by * TYT + ty;
   const int kb = tl.z, ke = tl.w;
   if (kb >= ke) return;
@@ -338,7 +336,7 @@ static void launch_tma_kind(const StageP &p, const TmaP &tm, const int4 *tiles, 
   if (ntiles <= 0) return;
   const int code = p.dir[0] | (p.dir[1] << 1) | (p.dir[2] << 2);
   dim3 block(TX, TYT);
-  dim3 grid(ntiles * p.nshot);
+  dim3 grid(ntiles);
   switch (code) {
 #define CASE(c)                                                                                              \
   case c:                                                                                                    \

@@ -201,10 +201,11 @@ __device__ __forceinline__ void ld5(int dir, const WaveIn<TW> &cur, int f, long 
   for (int n = 0; n < 5; n++) o[n] = cur(f, id + (n - L) * off);
 }
 
-// Surface slab: one thread per cell of the top NSURF planes. WP is the wave policy of the
-// bulk kernel (0 FP32 stage levels; 1 FP32 input, FP16 output; 2 FP16 input and output).
-// The kernel is latency-bound on its many cached loads: registers are capped at 128 so that
-// 16 warps share each SM (a few spills are cheaper than 8 warps).
+// Surface slab: one thread per cell of the top NSURF planes; a block holds the NSURF planes of
+// 32 x 2 columns, so that the z-stencil loads of one column hit in the SM's L1. WP is the wave
+// policy of the bulk kernel (0 FP32 stage levels; 1 FP32 input, FP16 output; 2 FP16 input and
+// output). The kernel is latency-bound on its many cached loads: registers are capped at 128 so
+// that 16 warps share each SM (a few spills are cheaper than 8 warps).
 // The operator directions of the stage (DX, DY, DZ: 0 backward, 1 forward) are template
 // parameters, so that every stencil offset is a compile-time constant.
 // Traction-image fluxes of the stage input at the top kFluxPlanes planes, every column of the
@@ -241,7 +242,7 @@ __global__ void __launch_bounds__(256) k_timg_flux(const __grid_constant__ Stage
 }
 
 template <int MED, typename TC, int WP, int DX, int DY, int DZ>
-__global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant__ StagePT<real_of<TC>> p) {
+__global__ void __launch_bounds__(32 * 2 * NSURF, 2) k_stage_surface(const __grid_constant__ StagePT<real_of<TC>> p) {
   constexpr int DIR[3] = {DX, DY, DZ};
   using R = real_of<TC>;  // double in the FP64 build (TC double, WP 0), float otherwise
   using TW = typename std::conditional<WP == 2, __half, R>::type;
@@ -250,8 +251,7 @@ __global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant_
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= p.ni || j >= p.nj) return;
   const long long sf = p.sf;
-  const int nslab = p.nk - p.nbulk;
-  const int shot = blockIdx.z / nslab;
+  const int shot = blockIdx.z;
   const long long woff = (long long)shot * 9 * sf;
   const float *wsc = p.wsc + shot * 18;  // FP16 stage levels: this shot's scale
   const WaveIn<TW> cur{reinterpret_cast<const TW *>(p.cur) + woff, sf, wsc};
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(128, 4) k_stage_surface(const __grid_constant_
   const int nk2 = p.nk - 1;
 
   {
-    const int k = p.nbulk + blockIdx.z % nslab;  // one thread per cell of the slab
+    const int k = p.nbulk + threadIdx.z;  // one thread per cell of the slab (nk - nbulk == NSURF)
     const long long id = didx(p, i, j, k);
     const CoefView<TC> cv(p);
     R m[3][3];
@@ -716,8 +716,8 @@ int launch_timg_flux64(const StagePT<double> &p, cudaStream_t st) {
 
 int launch_stage_surface(int med, int coef_type, int wave16, const StageP &p, cudaStream_t st) {
   if (p.nbulk >= p.nk) return 0;
-  dim3 block(32, 4);
-  dim3 grid((p.ni + 31) / 32, (p.nj + 3) / 4, (p.nk - p.nbulk) * p.nshot);
+  dim3 block(32, 2, NSURF);
+  dim3 grid((p.ni + 31) / 32, (p.nj + 1) / 2, p.nshot);
   if (wave16) {
     if (p.stage == 0) launch_surface_tc<uint16_t, 1>(med, p, grid, block, st);
     else launch_surface_tc<uint16_t, 2>(med, p, grid, block, st);
@@ -730,8 +730,8 @@ int launch_stage_surface(int med, int coef_type, int wave16, const StageP &p, cu
 
 int launch_stage_surface64(int med, const StagePT<double> &p, cudaStream_t st) {
   if (p.nbulk >= p.nk) return 0;
-  dim3 block(32, 4);
-  dim3 grid((p.ni + 31) / 32, (p.nj + 3) / 4, (p.nk - p.nbulk) * p.nshot);
+  dim3 block(32, 2, NSURF);
+  dim3 grid((p.ni + 31) / 32, (p.nj + 1) / 2, p.nshot);
   launch_surface_tc<double, 0>(med, p, grid, block, st);
   return 1;
 }

@@ -112,6 +112,7 @@ int launch_timg_flux64(const StagePT<double> &p, cudaStream_t st);
 // wave16: FP16 stage levels (requires COEF_F16).
 // shape: tile shape index (0 default, 1 the alternative; cgfd_bulk_tma.cuh TileShape)
 int tma_tile_y(int med, int shape);
+int tma_blocks_per_sm(int med, int shape);  // resident blocks per SM the tile shape is built for
 cudaError_t tma_prepare(int med, int coef_type, int wave16, int shape);
 // Tile lists of the TMA bulk kernel (device arrays, one int4 per tile: bx, by, first and
 // end z plane): tiles no CFS-PML face touches, and the rest.

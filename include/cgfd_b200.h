@@ -156,11 +156,11 @@ const char *cgfd_last_error(void);
 int cgfd_problem_create(const cgfd_problem_desc *desc, cgfd_problem **out);
 
 /*
- * Batched sources on one grid: nshot independent wavefields share the grid, metrics,
- * medium, boundaries and stations (desc->src is ignored); shots[s] holds the sources of
- * wavefield s. One launch per kernel and RK stage covers every shot, with the shot as the
- * fastest block index so that the coefficient tiles of a grid tile are read once from HBM
- * for all shots. Seismograms come back as [nshot][nsta][9][nt_total].
+ * Batched sources on one grid: nshot (1..32767) independent wavefields share the grid,
+ * metrics, medium, boundaries and stations (desc->src is ignored); shots[s] holds the sources
+ * of wavefield s. One launch per kernel and RK stage covers every shot; the shots of a group
+ * (cgfd_set_shot_group) run side by side, so that the coefficient tiles of a grid tile are
+ * read once from HBM for the group. Seismograms come back as [nshot][nsta][9][nt_total].
  * No counterpart in the reference (one source set per run there).
  */
 int cgfd_batch_create(const cgfd_problem_desc *desc, int nshot, const cgfd_source_desc *shots,
@@ -333,12 +333,25 @@ int cgfd_set_tile_shape(cgfd_problem *p, int shape);
 int cgfd_get_tile_shape(const cgfd_problem *p);
 
 /*
+ * Block order of a batch's bulk kernel: the shots come in groups of `group` (default 8; values
+ * above the batch's shot count mean every shot), each group's blocks cover every tile before
+ * the next group's start, and within a group the shot is the fastest block index. The blocks
+ * of one tile then share its coefficient tiles through L2 while a tile's x-y neighbours of the
+ * same shot stay resident beside it. Results do not depend on the group. Graphs are rebuilt.
+ * cgfd_get_shot_group returns the group in effect (at most the shot count). No counterpart in
+ * the reference.
+ */
+int cgfd_set_shot_group(cgfd_problem *p, int group);
+int cgfd_get_shot_group(const cgfd_problem *p);
+
+/*
  * Autotuner of the bulk kernel's tile: times `steps` graph-replayed time steps for each tile
  * shape (cgfd_set_tile_shape) and z-chunk length (planes per thread block column: 8, 12, 16,
  * 24, 32, 48, 64, 96 and all bulk planes) on this problem, keeps the fastest pair (*chosen:
  * the z chunk; cgfd_get_tile_shape: the shape) and returns the problem to its freshly created
- * state (zero wavefield, step 0). Only on a problem that has not stepped yet. Results do not
- * depend on the choice. No counterpart in the reference.
+ * state (zero wavefield, step 0). For a batch it then times the shot groups 4, 8, 16 and every
+ * shot at the chosen pair and keeps the fastest (cgfd_get_shot_group). Only on a problem that
+ * has not stepped yet. Results do not depend on the choice. No counterpart in the reference.
  */
 int cgfd_autotune(cgfd_problem *p, int steps, int *chosen);
 

@@ -43,3 +43,32 @@ def test_batch_validation():
     s = Simulation(p, shots=shots)
     with pytest.raises(Exception):
         s.set_bulk_variant(0)
+
+
+def test_shot_groups_agree_and_autotune_picks_one():
+    """The block order of a batch (shot groups of 1, 2 or every shot; strips of tile rows
+    sized by the group) changes no result: every group gives the same seismograms and final
+    wavefields bitwise. The autotuner then picks a group and returns the batch to step 0."""
+    p = small_problem("iso", nsteps=30, nsrc=0)
+    shots = _shots(p, 5, 9)
+    ref = None
+    for g in (5, 1, 2):
+        b = Simulation(p, shots=shots)
+        b.set_shot_group(g)
+        assert b.shot_group == g
+        b.run()
+        out = (b.seismograms(), [b.wavefield(n) for n in range(5)])
+        b.close()
+        if ref is None:
+            ref = out
+        else:
+            assert np.array_equal(out[0], ref[0])
+            for n in range(5):
+                assert np.array_equal(out[1][n], ref[1][n])
+    b = Simulation(p, shots=shots)
+    b.autotune(2)
+    assert b.shot_group in (4, 5)
+    assert b.step == 0
+    b.run()
+    assert np.array_equal(b.seismograms(), ref[0])
+    b.close()
