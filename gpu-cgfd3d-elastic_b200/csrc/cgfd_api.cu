@@ -106,10 +106,13 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 // 4-D map (x, y, z, field) over one device-layout array of nf fields of `esize`-byte elements
 // (4: FP32, 2: FP16 or BF16 as `dtype` says).
-void make_map(CUtensorMap *m, const void *base, long long sx, long long ny, long long nz, int nf, long long sz,
-              long long sf, int boxx, int boxy, int boxf, CUtensorMapDataType dtype = CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-              int esize = 4) {
-  cuuint64_t dims[4] = {(cuuint64_t)sx, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)nf};
+// 4-D map (x, y, z, field) of extents nx, ny, nz, nf over rows of sx, planes of sz and fields of
+// sf elements from `base`; a box that reaches beyond an extent reads zeros there without
+// touching memory.
+void make_map(CUtensorMap *m, const void *base, long long nx, long long ny, long long nz, int nf, long long sx,
+              long long sz, long long sf, int boxx, int boxy, int boxf,
+              CUtensorMapDataType dtype = CU_TENSOR_MAP_DATA_TYPE_FLOAT32, int esize = 4) {
+  cuuint64_t dims[4] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)nf};
   cuuint64_t strides[3] = {(cuuint64_t)(sx * esize), (cuuint64_t)(sz * esize), (cuuint64_t)(sf * esize)};
   cuuint32_t box[4] = {(cuuint32_t)boxx, (cuuint32_t)boxy, 1, (cuuint32_t)boxf};
   cuuint32_t es[4] = {1, 1, 1, 1};
@@ -997,21 +1000,29 @@ void make_maps(cgfd_problem *p) {
   const int nshot = p->nshot;
   {
     const int ty = cgfd::tma_tile_y(p->med, p->shape);
+    // The stage-input (halo) maps cover the physical cells only, from (0, 0, 0): the halo columns,
+    // rows and planes beyond the grid, which hold zeros in memory, come as the boxes' zero fill
+    // instead of as DRAM lines of row padding and ghost cells. The centre-box maps cover the
+    // whole allocation (padded coordinates).
+    const long long nx = p->ni, ny = p->nj, nz = p->nk;
     for (int l = 0; l < 4; l++) {
       if (p->wave16 && l >= 2) {  // FP16 stage level: x halo of 8 elements keeps the box 16-byte aligned
-        make_map(&p->map_halo[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX + 16,
-                 ty + 4, 9, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2);
-        make_map(&p->map_ctr[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX, ty, 9,
-                 CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2);
+        make_map(&p->map_halo[l], reinterpret_cast<const __half *>(p->wbuf[l]) + p->off0, nx, ny, nz, 9 * nshot, p->sx,
+                 p->sz, p->sf, cgfd::TX + 16, ty + 4, 9, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2);
+        make_map(&p->map_ctr[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sx, p->sz, p->sf, cgfd::TX, ty,
+                 9, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2);
         continue;
       }
-      make_map(&p->map_halo[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX + 8, ty + 4, 9);
-      make_map(&p->map_ctr[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sz, p->sf, cgfd::TX, ty, 9);
+      make_map(&p->map_halo[l], p->wbuf[l] + p->off0, nx, ny, nz, 9 * nshot, p->sx, p->sz, p->sf, cgfd::TX + 8, ty + 4,
+               9);
+      make_map(&p->map_ctr[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sx, p->sz, p->sf, cgfd::TX, ty, 9);
     }
     if (p->coef_type == cgfd::COEF_F32)
-      make_map(&p->map_coef, p->coef, p->sx, p->nj + 6, p->nk + 6, p->ncoef, p->sz, p->sf, cgfd::TX, ty, p->ncoef);
+      make_map(&p->map_coef, p->coef, p->sx, p->nj + 6, p->nk + 6, p->ncoef, p->sx, p->sz, p->sf, cgfd::TX, ty,
+               p->ncoef);
     else
-      make_map(&p->map_coef, p->coef16, p->sx, p->nj + 6, p->nk + 6, p->ncoef, p->sz, p->sf, cgfd::TX, ty, p->ncoef,
+      make_map(&p->map_coef, p->coef16, p->sx, p->nj + 6, p->nk + 6, p->ncoef, p->sx, p->sz, p->sf, cgfd::TX, ty,
+               p->ncoef,
                p->coef_type == cgfd::COEF_F16    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
                : p->coef_type == cgfd::COEF_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
                                                  : CU_TENSOR_MAP_DATA_TYPE_UINT16,

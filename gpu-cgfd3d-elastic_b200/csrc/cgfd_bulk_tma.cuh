@@ -118,8 +118,10 @@ __global__ void __launch_bounds__(TX *TYT, MINB)
   const bool need_end = stage >= 1;
   const uint32_t wave_bytes = S::WAVE_ELEMS * sizeof(TW);
   const uint32_t cpe_bytes = S::COEF_BYTES + (need_pre && S::PT ? S::FLD_BYTES : 0) + (need_end ? S::FLD_BYTES : 0);
-  // box origins in device-layout coordinates (x * element size a multiple of 16 bytes)
-  const int xw = GX + bx * TX - S::XO, yw = by * TYT + 3 - LY;  // box row r = tile row r - LY
+  // box origins (x * element size a multiple of 16 bytes): the stage-input map counts physical
+  // cells from (0, 0, 0), so the halo beyond the grid is zero fill; the centre-box maps count
+  // device-layout (padded) coordinates
+  const int xw = bx * TX - S::XO, yw = by * TYT - LY;  // box row r = tile row r - LY
   const int xc = GX + bx * TX, yc = 3 + by * TYT;
 
   if (tid == 0) {
@@ -135,7 +137,7 @@ __global__ void __launch_bounds__(TX *TYT, MINB)
     const int kk = k0 + m * SD;
     uint64_t *b = &bar[m % S::NW];
     mbar_expect_tx(b, wave_bytes);
-    tma_load_4d(wave + (m % S::NW) * (S::WAVE_SLOT / (int)sizeof(TW)), &tm.cur, xw, yw, kk + 3, 9 * shot, b);
+    tma_load_4d(wave + (m % S::NW) * (S::WAVE_SLOT / (int)sizeof(TW)), &tm.cur, xw, yw, kk, 9 * shot, b);
   };
   auto issue_cpe = [&](int m) {
     const int kk = k0 + m * SD;
