@@ -161,7 +161,8 @@ struct cgfd_problem {
   // TMA bulk kernel tile lists for the current z chunk (interior tiles, then PML tiles)
   int4 *d_tiles = nullptr, *d_tiles_dn = nullptr;
   cgfd::BulkTiles tiles, tiles_dn;  // z layers upwards (backward z operators) / downwards
-  // PML tiles run on `side`, forked from and joined back into `stream` at every stage
+  // the flux pass and surface slab run on `side`, forked from and joined back into `stream`
+  // at every stage
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   float *d_wsc = nullptr, *d_srcb = nullptr;
@@ -404,18 +405,17 @@ struct cgfd_problem {
         tm.pre = map_ctr[pre];
         tm.end = map_ctr[end];
         tm.coef = map_coef;
-        const bool fork = tiles.npml > 0 && tiles.ninterior > 0;
-        // Outside per-kernel timing, the surface slab (latency-bound, top planes only) runs on
-        // the side stream behind the PML tiles, beside the interior tiles: it writes only the
-        // top planes of the stage outputs, which no bulk tile reads or writes in this stage.
-        surface_done = fork && !timing;
+        // Outside per-kernel timing, the flux pass and the surface slab (latency-bound, top
+        // planes only) run on a side stream beside the bulk tiles: they write only the top
+        // planes of the stage outputs, which no bulk tile reads or writes in this stage.
+        const bool fork = free_top && tiles.n > 0 && !timing;
+        surface_done = fork;
         n += timed(s, [&] {
           if (fork) {
             CK(cudaEventRecord(ev_fork, st));
             CK(cudaStreamWaitEvent(side, ev_fork, 0));
           }
-          int k = cgfd::launch_stage_bulk_tma(med, coef_type, wave16, shape, p, tm, p.dir[2] ? tiles_dn : tiles, st,
-                                              fork ? side : st);
+          int k = cgfd::launch_stage_bulk_tma(med, coef_type, wave16, shape, p, tm, p.dir[2] ? tiles_dn : tiles, st);
           if (surface_done)
             k += cgfd::launch_timg_flux(coef_type, wave16, p, side) +
                  cgfd::launch_stage_surface(med, coef_type, wave16, p, side);
@@ -1033,17 +1033,18 @@ void make_maps(cgfd_problem *p) {
 
 // Tile lists of the TMA bulk kernel: 32 x TY columns, split along z into chunks of about
 // nzc planes that never straddle a z-face boundary of the CFS-PML (so planes above the
-// bottom absorbing layer run as interior tiles), and sorted by whether any PML face box meets
-// the tile's volume. Entries (bx, by, first plane, end plane), x fastest.
-// Order: strips of tile rows, each strip z layer by z layer. A strip's layer holds about as
-// many blocks as the GPU keeps resident, so that a tile's x-y neighbours run beside it at the
-// same planes (their halo rows are read from DRAM once), and the tile's next chunk starts as
-// this one ends (the 3 planes its register queue starts from are still in L2). The layers run
-// in the march direction of the stage's z operator: upwards for backward operators (tiles),
-// downwards for forward ones (tiles_dn).
+// bottom absorbing layer run as tiles without face code); a tile that any PML face box meets
+// carries the kTilePml flag. Entries (bx [+ kTilePml] [+ shot << 16], by, first plane, end plane).
+// Order: strips of tile rows, each strip z layer by z layer, x fastest. A strip's layer holds
+// about as many blocks as the GPU keeps resident, so that a tile's x-y neighbours run beside it
+// at the same planes (their halo lines are read from DRAM once), and the tile's next chunk
+// starts as this one ends (the 3 planes its register queue starts from are still in L2). The
+// layers run in the march direction of the stage's z operator: upwards for backward operators
+// (tiles), downwards for forward ones (tiles_dn).
 void make_tiles(cgfd_problem *p) {
   const int ty = cgfd::tma_tile_y(p->med, p->shape), nbulk = p->free_top ? p->nk - cgfd::NSURF : p->nk;
   const int nbx = (p->ni + cgfd::TX - 1) / cgfd::TX, nby = (p->nj + ty - 1) / ty;
+  if (nbx > cgfd::kTileBxMask + 1) throw cgfd::Error(CGFD_ERR_INVALID, "grid too wide for the bulk tile list");
   std::vector<int> cuts = {0, nbulk};
   for (const auto &f : p->faces)
     if (f.h.axis == 2)
@@ -1062,7 +1063,8 @@ void make_tiles(cgfd_problem *p) {
   const long long resident = (long long)nsm * cgfd::tma_blocks_per_sm(p->med, p->shape);
   const int strip = (int)std::max<long long>(1, (resident + (long long)nbx * group - 1) / ((long long)nbx * group));
   for (int dn = 0; dn < 2; dn++) {
-    std::vector<int4> in, pm;
+    std::vector<int4> list;
+    int npml = 0;
     for (int s0 = 0; s0 < nby; s0 += strip)
       for (size_t zi = 0; zi < zr.size(); zi++) {
         const auto &z = zr[dn ? zr.size() - 1 - zi : zi];
@@ -1075,36 +1077,34 @@ void make_tiles(cgfd_problem *p) {
               const bool zo = f.h.lo[2] <= z.second - 1 && f.h.hi[2] >= z.first;
               touch |= xo && yo && zo;
             }
-            (touch ? pm : in).push_back(make_int4(bx, by, z.first, z.second));
+            npml += touch;
+            list.push_back(make_int4(bx + (touch ? cgfd::kTilePml : 0), by, z.first, z.second));
           }
       }
     // batches: one entry per tile and shot, the shots in groups of `group`; a group's entries
     // cover every tile before the next group's, the shot fastest within a group (the group's
     // blocks of one tile share its coefficient tiles through L2, and a tile's x-y neighbours of
     // the same shot stay resident beside it)
-    if (p->nshot > 1)
-      for (auto *lst : {&in, &pm}) {
-        std::vector<int4> ex;
-        ex.reserve(lst->size() * p->nshot);
-        for (int g0 = 0; g0 < p->nshot; g0 += group)
-          for (const int4 &e : *lst)
-            for (int sh = g0; sh < std::min(p->nshot, g0 + group); sh++)
-              ex.push_back(make_int4(e.x + (sh << 16), e.y, e.z, e.w));
-        lst->swap(ex);
-      }
+    if (p->nshot > 1) {
+      std::vector<int4> ex;
+      ex.reserve(list.size() * p->nshot);
+      for (int g0 = 0; g0 < p->nshot; g0 += group)
+        for (const int4 &e : list)
+          for (int sh = g0; sh < std::min(p->nshot, g0 + group); sh++)
+            ex.push_back(make_int4(e.x + (sh << 16), e.y, e.z, e.w));
+      list.swap(ex);
+      npml *= p->nshot;
+    }
     int4 *&dt = dn ? p->d_tiles_dn : p->d_tiles;
     cgfd::BulkTiles &tl = dn ? p->tiles_dn : p->tiles;
     dfree(dt, p->stream);
     dt = nullptr;
-    std::vector<int4> all(in);
-    all.insert(all.end(), pm.begin(), pm.end());
     size_t acc = 0;
-    dt = dmalloc<int4>(std::max<size_t>(all.size(), 1), acc, p->stream);
-    if (!all.empty()) CK(cudaMemcpy(dt, all.data(), all.size() * sizeof(int4), cudaMemcpyHostToDevice));
-    tl.interior = dt;
-    tl.ninterior = (int)in.size();
-    tl.pml = dt + in.size();
-    tl.npml = (int)pm.size();
+    dt = dmalloc<int4>(std::max<size_t>(list.size(), 1), acc, p->stream);
+    if (!list.empty()) CK(cudaMemcpy(dt, list.data(), list.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    tl.list = dt;
+    tl.n = (int)list.size();
+    tl.npml = npml;
   }
 }
 

@@ -5,11 +5,11 @@
 namespace cgfd {
 
 extern template int launch_bulk_tma_med<MED_ISO>(int, int, int, const StageP &, const TmaP &, const BulkTiles &,
-                                                 cudaStream_t, cudaStream_t);
+                                                 cudaStream_t);
 extern template int launch_bulk_tma_med<MED_VTI>(int, int, int, const StageP &, const TmaP &, const BulkTiles &,
-                                                 cudaStream_t, cudaStream_t);
+                                                 cudaStream_t);
 extern template int launch_bulk_tma_med<MED_ANISO>(int, int, int, const StageP &, const TmaP &, const BulkTiles &,
-                                                   cudaStream_t, cudaStream_t);
+                                                 cudaStream_t);
 extern template cudaError_t prepare_bulk_tma_med<MED_ISO>(int, int, int);
 extern template cudaError_t prepare_bulk_tma_med<MED_VTI>(int, int, int);
 extern template cudaError_t prepare_bulk_tma_med<MED_ANISO>(int, int, int);
@@ -33,11 +33,11 @@ cudaError_t tma_prepare(int med, int coef_type, int wave16, int shape) {
 }
 
 int launch_stage_bulk_tma(int med, int coef_type, int wave16, int shape, const StageP &p, const TmaP &tm,
-                          const BulkTiles &t, cudaStream_t st, cudaStream_t st_pml) {
+                          const BulkTiles &t, cudaStream_t st) {
   if (p.nbulk <= 0) return 0;
-  if (med == MED_ISO) return launch_bulk_tma_med<MED_ISO>(coef_type, wave16, shape, p, tm, t, st, st_pml);
-  if (med == MED_VTI) return launch_bulk_tma_med<MED_VTI>(coef_type, wave16, shape, p, tm, t, st, st_pml);
-  return launch_bulk_tma_med<MED_ANISO>(coef_type, wave16, shape, p, tm, t, st, st_pml);
+  if (med == MED_ISO) return launch_bulk_tma_med<MED_ISO>(coef_type, wave16, shape, p, tm, t, st);
+  if (med == MED_VTI) return launch_bulk_tma_med<MED_VTI>(coef_type, wave16, shape, p, tm, t, st);
+  return launch_bulk_tma_med<MED_ANISO>(coef_type, wave16, shape, p, tm, t, st);
 }
 
 }  // namespace cgfd

@@ -80,13 +80,10 @@ struct CoefTile {
   __device__ __forceinline__ float operator()(int f) const { return coef_decode<TC>(c[f * STRIDE], p, f); }
 };
 
-// Tiles come from a list (4 ints each: bx + (shot << 16), by, first plane, end plane), one
-// block per entry in list order: one list for the tiles that no CFS-PML face touches (PML
-// false: the face code is compiled out, fewer registers) and one for the rest (PML true).
+// One tile (a block) of the stage; PML false: the tile meets no CFS-PML face and the face code
+// is compiled out.
 template <int MED, int DX, int DY, int DZ, int TYT, int MINB, typename TC, int WP, bool PML>
-__global__ void __launch_bounds__(TX *TYT, MINB)
-    k_stage_bulk_tma(const __grid_constant__ StageP p, const __grid_constant__ TmaP tm,
-                     const int4 *__restrict__ tiles) {
+__device__ __forceinline__ void bulk_tile(const StageP &p, const TmaP &tm, const int4 tl) {
   using TW = typename WavePolicy<WP>::TW;
   using TT = typename WavePolicy<WP>::TT;
   using S = BulkSmem<MED, TYT, TC, TW, MINB>;
@@ -99,9 +96,7 @@ __global__ void __launch_bounds__(TX *TYT, MINB)
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + S::OFF_BAR);  // NW wave, then 2 cpe
 
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  // one block per list entry, in list order: x = bx + (shot << 16), y = by, z / w = planes
-  const int4 tl = __ldg(tiles + blockIdx.x);
-  const int bx = tl.x & 0xffff, by = tl.y, shot = tl.x >> 16;
+  const int bx = tl.x & kTileBxMask, by = tl.y, shot = tl.x >> 16;
   const int i = bx * TX + tx, j = by * TYT + ty;
   const int kb = tl.z, ke = tl.w;
   if (kb >= ke) return;
@@ -330,58 +325,57 @@ __global__ void __launch_bounds__(TX *TYT, MINB)
 }
 
 
+// The bulk stage: one block per tile-list entry, in list order. An entry is (bx + PML flag
+// (kTilePml) + (shot << 16), by, first plane, end plane); a PML tile runs the face code, the
+// others its compiled-out form. Both kinds in one launch keep a tile's x-y neighbours, PML or
+// not, resident beside it, so that the halo lines they share are read from DRAM once.
+template <int MED, int DX, int DY, int DZ, int TYT, int MINB, typename TC, int WP>
+__global__ void __launch_bounds__(TX *TYT, MINB)
+    k_stage_bulk_tma(const __grid_constant__ StageP p, const __grid_constant__ TmaP tm,
+                     const int4 *__restrict__ tiles) {
+  const int4 tl = __ldg(tiles + blockIdx.x);
+  if (tl.x & kTilePml) bulk_tile<MED, DX, DY, DZ, TYT, MINB, TC, WP, true>(p, tm, tl);
+  else bulk_tile<MED, DX, DY, DZ, TYT, MINB, TC, WP, false>(p, tm, tl);
+}
+
 // -----------------------------------------------------------------------------------------
-template <int MED, int SH, typename TC, int WP, bool PML>
-static void launch_tma_kind(const StageP &p, const TmaP &tm, const int4 *tiles, int ntiles, cudaStream_t st) {
+template <int MED, int SH, typename TC, int WP>
+static int launch_tma_shape(const StageP &p, const TmaP &tm, const BulkTiles &t, cudaStream_t st) {
   constexpr int TYT = TileShape<MED, SH>::TYT, MINB = TileShape<MED, SH>::MINB;
   using S = BulkSmem<MED, TYT, TC, typename WavePolicy<WP>::TW, MINB>;
-  if (ntiles <= 0) return;
+  if (t.n <= 0) return 0;
   const int code = p.dir[0] | (p.dir[1] << 1) | (p.dir[2] << 2);
   dim3 block(TX, TYT);
-  dim3 grid(ntiles);
+  dim3 grid(t.n);
   switch (code) {
 #define CASE(c)                                                                                              \
   case c:                                                                                                    \
-    k_stage_bulk_tma<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, TYT, MINB, TC, WP, PML>                     \
-        <<<grid, block, S::BYTES, st>>>(p, tm, tiles);                                                       \
+    k_stage_bulk_tma<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, TYT, MINB, TC, WP>                          \
+        <<<grid, block, S::BYTES, st>>>(p, tm, t.list);                                                      \
     break;
     CASE(0) CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7)
 #undef CASE
   }
+  return 1;
 }
 
-// PML tiles on st_pml, interior tiles on st (the caller forks and joins the two streams).
 template <int MED, int SH, typename TC, int WP>
-static int launch_tma_shape(const StageP &p, const TmaP &tm, const BulkTiles &t, cudaStream_t st, cudaStream_t st_pml) {
-  launch_tma_kind<MED, SH, TC, WP, true>(p, tm, t.pml, t.npml, st_pml);
-  launch_tma_kind<MED, SH, TC, WP, false>(p, tm, t.interior, t.ninterior, st);
-  return (t.npml > 0) + (t.ninterior > 0);
-}
-
-template <int MED, int SH, typename TC, int WP, bool PML>
-static cudaError_t set_attr_kind() {
+static cudaError_t set_attr_shape() {
   constexpr int TYT = TileShape<MED, SH>::TYT, MINB = TileShape<MED, SH>::MINB;
   using S = BulkSmem<MED, TYT, TC, typename WavePolicy<WP>::TW, MINB>;
   cudaError_t e = cudaSuccess;
 #define ATTR(c)                                                                                               \
   if (e == cudaSuccess)                                                                                       \
-    e = cudaFuncSetAttribute(k_stage_bulk_tma<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, TYT, MINB, TC, WP, PML>, \
+    e = cudaFuncSetAttribute(k_stage_bulk_tma<MED, (c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1, TYT, MINB, TC, WP>,     \
                              cudaFuncAttributeMaxDynamicSharedMemorySize, S::BYTES);
   ATTR(0) ATTR(1) ATTR(2) ATTR(3) ATTR(4) ATTR(5) ATTR(6) ATTR(7)
 #undef ATTR
   return e;
 }
 
-template <int MED, int SH, typename TC, int WP>
-static cudaError_t set_attr_shape() {
-  cudaError_t e = set_attr_kind<MED, SH, TC, WP, true>();
-  return e == cudaSuccess ? set_attr_kind<MED, SH, TC, WP, false>() : e;
-}
-
 template <int MED, typename TC, int WP>
-static int launch_tc(int shape, const StageP &p, const TmaP &tm, const BulkTiles &t, cudaStream_t st,
-                     cudaStream_t st_pml) {
-  return shape ? launch_tma_shape<MED, 1, TC, WP>(p, tm, t, st, st_pml) : launch_tma_shape<MED, 0, TC, WP>(p, tm, t, st, st_pml);
+static int launch_tc(int shape, const StageP &p, const TmaP &tm, const BulkTiles &t, cudaStream_t st) {
+  return shape ? launch_tma_shape<MED, 1, TC, WP>(p, tm, t, st) : launch_tma_shape<MED, 0, TC, WP>(p, tm, t, st);
 }
 
 template <int MED, typename TC, int WP>
@@ -392,15 +386,15 @@ static cudaError_t prepare_tc(int shape) {
 // One medium: every coefficient storage type and wave policy, both tile shapes.
 template <int MED>
 int launch_bulk_tma_med(int coef_type, int wave16, int shape, const StageP &p, const TmaP &tm, const BulkTiles &t,
-                        cudaStream_t st, cudaStream_t st_pml) {
+                        cudaStream_t st) {
   if (wave16) {  // 16-bit fixed-point coefficients with FP16 stage levels
-    if (p.stage == 0) return launch_tc<MED, uint16_t, 1>(shape, p, tm, t, st, st_pml);
-    return launch_tc<MED, uint16_t, 2>(shape, p, tm, t, st, st_pml);
+    if (p.stage == 0) return launch_tc<MED, uint16_t, 1>(shape, p, tm, t, st);
+    return launch_tc<MED, uint16_t, 2>(shape, p, tm, t, st);
   }
-  if (coef_type == COEF_U16) return launch_tc<MED, uint16_t, 0>(shape, p, tm, t, st, st_pml);
-  if (coef_type == COEF_F16) return launch_tc<MED, __half, 0>(shape, p, tm, t, st, st_pml);
-  if (coef_type == COEF_BF16) return launch_tc<MED, __nv_bfloat16, 0>(shape, p, tm, t, st, st_pml);
-  return launch_tc<MED, float, 0>(shape, p, tm, t, st, st_pml);
+  if (coef_type == COEF_U16) return launch_tc<MED, uint16_t, 0>(shape, p, tm, t, st);
+  if (coef_type == COEF_F16) return launch_tc<MED, __half, 0>(shape, p, tm, t, st);
+  if (coef_type == COEF_BF16) return launch_tc<MED, __nv_bfloat16, 0>(shape, p, tm, t, st);
+  return launch_tc<MED, float, 0>(shape, p, tm, t, st);
 }
 
 template <int MED>

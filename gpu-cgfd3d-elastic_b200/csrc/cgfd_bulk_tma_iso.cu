@@ -3,7 +3,7 @@
 #include "cgfd_bulk_tma.cuh"
 
 namespace cgfd {
-template int launch_bulk_tma_med<MED_ISO>(int, int, int, const StageP &, const TmaP &, const BulkTiles &, cudaStream_t,
+template int launch_bulk_tma_med<MED_ISO>(int, int, int, const StageP &, const TmaP &, const BulkTiles &,
                                          cudaStream_t);
 template cudaError_t prepare_bulk_tma_med<MED_ISO>(int, int, int);
 }  // namespace cgfd

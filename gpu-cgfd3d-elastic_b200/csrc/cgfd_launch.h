@@ -114,16 +114,16 @@ int launch_timg_flux64(const StagePT<double> &p, cudaStream_t st);
 int tma_tile_y(int med, int shape);
 int tma_blocks_per_sm(int med, int shape);  // resident blocks per SM the tile shape is built for
 cudaError_t tma_prepare(int med, int coef_type, int wave16, int shape);
-// Tile lists of the TMA bulk kernel (device arrays, one int4 per tile: bx, by, first and
-// end z plane): tiles no CFS-PML face touches, and the rest.
+// Tile list of the TMA bulk kernel (device array, one int4 per block in launch order:
+// bx + kTilePml if a CFS-PML face meets the tile + (shot << 16), by, first and end z plane).
+constexpr int kTilePml = 0x8000;     // bit 15 of x
+constexpr int kTileBxMask = 0x7fff;  // bits 0-14 of x: bx (bits 16-30: the shot)
 struct BulkTiles {
-  const int4 *interior = nullptr, *pml = nullptr;
-  int ninterior = 0, npml = 0;
+  const int4 *list = nullptr;
+  int n = 0, npml = 0;  // entries, of which PML tiles
 };
-// Interior tiles go to st, PML tiles to st_pml (may be st).
 int launch_stage_bulk_tma(int med, int coef_type, int wave16, int shape, const StageP &p, const TmaP &tm,
-                          const BulkTiles &t,
-                          cudaStream_t st, cudaStream_t st_pml);
+                          const BulkTiles &t, cudaStream_t st);
 // FP16 stage levels: per-step scale from the last step's max |w| and the step's source bound
 int launch_wave_scale(unsigned int *amax, const float *srcb, const int *d_it, int nt_total, int nshot, float *wsc,
                       cudaStream_t st);
