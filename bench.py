@@ -205,8 +205,9 @@ def measured_peak():
 
 
 def ncu_traffic(workload, cells_per_launch, shape, zchunk):
-    """DRAM bytes per bulk-kernel launch (one RK stage) from the committed ncu summary of the
-    same tile shape and z chunk, scaled by cells; None when no capture of that choice exists."""
+    """DRAM bytes per bulk-kernel launch (one RK stage) from the committed ncu summary, scaled
+    by cells: the capture of the same tile shape with the nearest z chunk (the tile choice it
+    was taken with is returned beside it); (None, None) when that shape has no capture."""
     path = os.path.join(ROOT, "profiles", "k_stage_bulk_iso.md")
     try:
         vals = {}
@@ -215,11 +216,12 @@ def ncu_traffic(workload, cells_per_launch, shape, zchunk):
                 if ":" in ln and ln.strip().startswith("- "):
                     k, v = ln.strip()[2:].split(":", 1)
                     vals[k.strip()] = v.strip().split()[0]
-        b = float(vals[f"dram_bytes_per_launch_shape{shape}_zchunk{zchunk}"])
-        c = float(vals["cells_per_launch"])
-        return b * cells_per_launch / c
+        pre = f"dram_bytes_per_launch_shape{shape}_zchunk"
+        caps = {int(k[len(pre):]): float(v) for k, v in vals.items() if k.startswith(pre)}
+        z = min(caps, key=lambda c: abs(c - zchunk))
+        return caps[z] * cells_per_launch / float(vals["cells_per_launch"]), f"tile shape {shape}, z chunk {z}"
     except Exception:
-        return None
+        return None, None
 
 
 def _time_steps(sim, steps, warm=8):
@@ -305,7 +307,8 @@ def media_bench(local, steps=2000):
     (relative L2 of the gather, largest per-station relative L2 with the tests' 1e-3 floor,
     relative error of the peak amplitude). FP32 and 16-bit fixed-point coefficients also report
     the bulk stage's algorithmic bytes (36 wavefield + NCOEF coefficient accesses per
-    cell-stage) per event-timed duration against the measured HBM peak."""
+    cell-stage) per event-timed duration against the measured HBM peak. Each mode's problem is
+    autotuned (tile shape, z chunk) before it runs."""
     import torch
     from cgfd_b200 import (synth, Simulation, CGFD_PREC_FP32, CGFD_PREC_U16_COEF, CGFD_PREC_FP16_WAVE,
                            CGFD_PREC_FP16_COEF, CGFD_PREC_BF16_COEF, CGFD_PREC_FP64)
@@ -332,6 +335,8 @@ def media_bench(local, steps=2000):
         for name, prec, cbytes in modes:
             p.precision = prec
             sim = Simulation(p)
+            sim.autotune(4)  # tile shape and z chunk for this medium and storage mode
+            tuned = {"tile_shape": sim.tile_shape, "zchunk": sim.zchunk}
             st = torch.cuda.ExternalStream(sim.stream)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(st)
@@ -343,7 +348,7 @@ def media_bench(local, steps=2000):
             s = sim.seismograms()[:, :, :steps]
             rec = {"value": ni * nj * nk * 4 / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": ms,
                    "gather_rel_l2_vs_fp64": rel_l2(s, ref), "station_rel_l2_vs_fp64": per_station_rel_l2(s, ref),
-                   "peak_rel_err_vs_fp64": abs(float(np.abs(s).max()) - pk) / pk}
+                   "peak_rel_err_vs_fp64": abs(float(np.abs(s).max()) - pk) / pk, "autotuned": tuned}
             if name in ("fp32", "u16coef"):
                 sim.set_timing(True)
                 sim.timing(reset=True)
@@ -522,10 +527,10 @@ def main():
     if args.zchunk:
         sim.set_zchunk(args.zchunk)
     elif not args.no_autotune:
-        # cgfd_autotune: both tile shapes x the z-chunk candidates timed on this problem (4 steps
+        # cgfd_autotune: both tile shapes x the z-chunk candidates timed on this problem (8 steps
         # each), before the warm-up; the state is reset to step 0 afterwards
         t = time.perf_counter()
-        sim.autotune(4)
+        sim.autotune(8)
         tuned = {"tile_shape": sim.tile_shape, "zchunk": sim.zchunk, "tuning_s": time.perf_counter() - t}
     shape_used, zchunk_used = sim.tile_shape, sim.zchunk
     st = torch.cuda.ExternalStream(sim.stream)
@@ -575,9 +580,9 @@ def main():
     alg = bpc * bulk_cells
     achieved = alg / (bulk_ms / bulk_n * 1e-3) / 1e9 if bulk_n else None
     peak, peak_kind = measured_peak()
-    traffic = ncu_traffic(args.workload, bulk_cells, shape_used, zchunk_used)
+    traffic, traffic_capture = ncu_traffic(args.workload, bulk_cells, shape_used, zchunk_used)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak if achieved else None, "traffic": traffic,
+            "frac": achieved / peak if achieved else None, "traffic": traffic, "traffic_capture": traffic_capture,
             "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback",
             "kernel": "k_stage_bulk_tma<iso> (interior-tile and PML-tile launches of one RK stage)",
             "bytes_per_cell_stage": bpc, "cells_per_launch": bulk_cells,

@@ -1649,7 +1649,7 @@ int cgfd_autotune(cgfd_problem *p, int steps, int *chosen) {
     CK(cudaSetDevice(p->device));
     const int nbulk = p->free_top ? p->nk - cgfd::NSURF : p->nk;
     std::vector<int> zc;
-    for (int c : {8, 12, 16, 24, 32, 48, 64, 96, nbulk})
+    for (int c : {8, 10, 12, 14, 16, 20, 24, 32, 48, 64, 96, nbulk})
       if (c >= 1 && c <= nbulk && std::find(zc.begin(), zc.end(), c) == zc.end()) zc.push_back(c);
     std::vector<std::pair<int, int>> cand;  // (tile shape, z chunk); the FP64 build has no TMA kernel
     for (int sh = 0; sh < (p->use_tma ? 2 : 1); sh++)
