@@ -141,7 +141,7 @@ struct cgfd_problem {
   long long sx = 0, sz = 0, sf = 0, off0 = 0;
   size_t bytes = 0;
   int nzc = 16;
-  int shape = 0;  // tile shape of the bulk kernel (0 default, 1 alternative; cgfd_set_tile_shape)
+  int shape = 0;  // tile shape of the bulk kernel (cgfd_set_tile_shape; set per medium at creation)
 
   float *wbuf[4] = {nullptr, nullptr, nullptr, nullptr};  // [0],[1]: pre/end by parity; [2],[3]: tmpA/tmpB
   // (real-typed arrays -- wbuf, coef, jac, matx/maty, PML A/B/D/aux, d_dis -- are held as float*
@@ -797,11 +797,14 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   if (p->free_top && p->nk < cgfd::NSURF + 4) throw cgfd::Error(CGFD_ERR_INVALID, "nk too small for the free surface");
   // device layout
   layout(p->ni, p->nj, p->nk, p->sx, p->sz, p->sf, p->off0);
-  // z planes per bulk block: ~32 keeps the per-chunk prologue (3 planes) small and gives
-  // enough blocks to fill 148 SMs many times over (cgfd_set_zchunk / the autotuner refine it)
+  // default tiling (cgfd_set_tile_shape / cgfd_set_zchunk / the autotuner refine it): 32x4
+  // tiles at three blocks per SM for iso media, the shape-0 tiles otherwise, and z chunks of
+  // about 12 planes (with strip-ordered tile lists a chunk's 3-plane prologue comes from L2, and
+  // short chunks keep the resident blocks on neighbouring planes)
+  p->shape = p->med == cgfd::MED_ISO ? 1 : 0;
   {
     int nbulk = p->free_top ? p->nk - cgfd::NSURF : p->nk;
-    int chunks = std::max(1, (nbulk + 31) / 32);
+    int chunks = std::max(1, (nbulk + 11) / 12);
     p->nzc = (nbulk + chunks - 1) / chunks;
   }
 

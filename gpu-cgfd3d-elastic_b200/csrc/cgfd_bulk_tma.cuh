@@ -34,7 +34,7 @@ template <int WP> struct WavePolicy {
 };
 
 // Tile shapes (columns x rows of one thread block, resident blocks per SM), two per medium; the
-// autotuner (cgfd_autotune) picks one per problem. Shape 0 is the default:
+// autotuner (cgfd_autotune) picks one per problem (default: shape 1 for iso, 0 otherwise):
 //   iso, VTI: 32x8 at two blocks per SM (two independent barrier domains hide each other's
 //             pipeline waits; <= 128 registers), or 32x4 at three blocks per SM;
 //   21-Cij:   32x4 at three blocks per SM (its 31 coefficient fields do not fit twice at 32x8),

@@ -86,12 +86,17 @@ void pml_setup(const cgfd_problem_desc *d, PmlFaceHost faces[3][2]) {
       for (int b = 0; b < 3; b++) { f.lo[b] = 0; f.hi[b] = n[b] - 1; }
       if (s == 0) f.hi[a] = N;
       else f.lo[a] = n[a] - 1 - N;
-      // average spacing along the normal over the face box
+      // average spacing along the normal over the face box: one partial sum per line of the
+      // outer axis (threads take lines), added in line order, so the result does not depend on
+      // the thread count
       const float *x = d->coord, *y = d->coord + g.siz_icmp, *z = d->coord + 2 * g.siz_icmp;
-      int a1 = a == 0 ? 1 : 0, a2 = a == 2 ? 1 : 2;
-      double L = 0.0;
-      long long num = 0;
-      for (int o2 = f.lo[a2]; o2 <= f.hi[a2]; o2++)
+      const int a1 = a == 0 ? 1 : 0, a2 = a == 2 ? 1 : 2;
+      const int n2 = f.hi[a2] - f.lo[a2] + 1;
+      std::vector<double> part(n2, 0.0);
+#pragma omp parallel for schedule(static)
+      for (int q = 0; q < n2; q++) {
+        const int o2 = f.lo[a2] + q;
+        double Lq = 0.0;
         for (int o1 = f.lo[a1]; o1 <= f.hi[a1]; o1++) {
           int ijk[3];
           ijk[a1] = o1; ijk[a2] = o2; ijk[a] = f.lo[a];
@@ -100,11 +105,15 @@ void pml_setup(const cgfd_problem_desc *d, PmlFaceHost faces[3][2]) {
             ijk[a] = m;
             size_t p1 = g.at(ijk[0], ijk[1], ijk[2]);
             double dx = (double)x[p1] - x[p0], dy = (double)y[p1] - y[p0], dz = (double)z[p1] - z[p0];
-            L += std::sqrt(dx * dx + dy * dy + dz * dz);
+            Lq += std::sqrt(dx * dx + dy * dy + dz * dz);
             p0 = p1;
-            num++;
           }
         }
+        part[q] = Lq;
+      }
+      double L = 0.0;
+      for (double v : part) L += v;
+      const long long num = (long long)n2 * (f.hi[a1] - f.lo[a1] + 1) * (f.hi[a] - f.lo[a]);
       double dh = L / (double)num;
       double L0 = dh * N;
       double Rpp = std::pow(10.0, -((std::log10((double)N) - 1.0) / std::log10(2.0) + 4.0));
@@ -170,6 +179,9 @@ void dvh2dvz(const cgfd_problem_desc *d, std::vector<float> &matx, std::vector<f
   matx.assign((size_t)d->ni * d->nj * 9, 0.f);
   maty.assign((size_t)d->ni * d->nj * 9, 0.f);
   const int k = d->nk - 1;
+  int singular = 0;
+  // one independent 3x3 solve per surface column
+#pragma omp parallel for schedule(static) reduction(| : singular)
   for (int j = 0; j < d->nj; j++)
     for (int i = 0; i < d->ni; i++) {
       size_t iptr = g.at(i, j, k);
@@ -202,7 +214,10 @@ void dvh2dvz(const cgfd_problem_desc *d, std::vector<float> &matx, std::vector<f
       inv[2][1] = A[2][0] * A[0][1] - A[0][0] * A[2][1];
       inv[2][2] = A[0][0] * A[1][1] - A[0][1] * A[1][0];
       double det = inv[0][0] * A[0][0] + inv[0][1] * A[1][0] + inv[0][2] * A[2][0];
-      if (det == 0.0 || !std::isfinite(det)) throw Error(CGFD_ERR_INVALID, "singular free-surface traction matrix");
+      if (det == 0.0 || !std::isfinite(det)) {
+        singular = 1;
+        continue;
+      }
       for (int a = 0; a < 3; a++)
         for (int b = 0; b < 3; b++) inv[a][b] /= det;
       size_t ij = ((size_t)j * d->ni + i) * 9;
@@ -214,6 +229,7 @@ void dvh2dvz(const cgfd_problem_desc *d, std::vector<float> &matx, std::vector<f
           maty[ij + r * 3 + c] = (float)(-ac);
         }
     }
+  if (singular) throw Error(CGFD_ERR_INVALID, "singular free-surface traction matrix");
 }
 
 // ---------------------------------------------------------------------------------------

@@ -324,10 +324,11 @@ int cgfd_set_zchunk(cgfd_problem *p, int nzc);
 int cgfd_get_zchunk(const cgfd_problem *p);
 
 /*
- * Tile shape of the TMA bulk kernel: 0 (default) or 1 (the alternative), per medium
+ * Tile shape of the TMA bulk kernel, 0 or 1, per medium
  *   iso, VTI: 32x8 columns at two blocks per SM | 32x4 at three blocks per SM
  *   21-Cij:   32x4 at three blocks per SM      | 32x8 at one block per SM (w_pre staged too).
- * Results do not depend on the shape (the per-cell arithmetic is the same).
+ * Default: 1 for iso media, 0 otherwise (with z chunks of about 12 planes). Results do not
+ * depend on the shape (the per-cell arithmetic is the same).
  */
 int cgfd_set_tile_shape(cgfd_problem *p, int shape);
 int cgfd_get_tile_shape(const cgfd_problem *p);
