@@ -17,7 +17,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -547,6 +549,32 @@ class PinnedStager {
   }
   std::mutex &mutex() { return mu_; }
 
+  // device -> caller's (pageable) host memory, the reverse pipeline: the copy engine fills one
+  // chunk while host threads empty the other
+  void copy_out(void *dst, const void *src, size_t n, cudaStream_t st) {
+    const size_t nch = (n + kChunk - 1) / kChunk;
+    auto issue = [&](size_t c) {
+      const size_t o = c * kChunk, m = std::min(kChunk, n - o);
+      CK(cudaEventSynchronize(done_[c & 1]));
+      CK(cudaMemcpyAsync(buf_[c & 1], static_cast<const char *>(src) + o, m, cudaMemcpyDeviceToHost, st));
+      CK(cudaEventRecord(done_[c & 1], st));
+    };
+    if (nch > 0) issue(0);
+    for (size_t c = 0; c < nch; c++) {
+      if (c + 1 < nch) issue(c + 1);
+      CK(cudaEventSynchronize(done_[c & 1]));
+      const size_t o = c * kChunk, m = std::min(kChunk, n - o);
+      char *out = static_cast<char *>(dst) + o;
+      const long long pieces = (long long)((m + kPiece - 1) / kPiece);
+#pragma omp parallel for schedule(static)
+      for (long long q = 0; q < pieces; q++) {
+        const size_t a = (size_t)q * kPiece;
+        std::memcpy(out + a, buf_[c & 1] + a, std::min(kPiece, m - a));
+      }
+    }
+    next_ = (int)(nch & 1);
+  }
+
   void copy(void *dst, const void *src, size_t n, cudaStream_t st) {
     for (size_t o = 0; o < n; o += kChunk) {
       const size_t m = std::min(kChunk, n - o);
@@ -592,6 +620,43 @@ void upload_field(cgfd_problem *p, const float *host_ref, void *dst, float *stag
   else
     cgfd::launch_repack_in(stage_buf, (float *)dst, p->ni, p->nj, p->nk, p->sx, p->sz, p->off0, mode, ghosts, p->stream);
   CK(cudaGetLastError());
+}
+
+// Metrics computed on the device from the caller's coordinates (desc->metric NULL): the FP64
+// kernel of cgfd_metric_calc_gpu (bitwise equal to cgfd_metric_calc, ghosts included) in the
+// reference layout, each field then repacked into the problem's layout like an uploaded
+// metric. `view` (host, 10 fields in the reference layout, zero-initialised) receives what the
+// host-side setup reads: the Jacobian (source weights) and the top plane of the other fields
+// (free-surface matrices). ps: the device's pinned stager, its lock held by the caller.
+void metric_from_coords(cgfd_problem *p, const cgfd_problem_desc *d, PinnedStager &ps, float *view) {
+  cgfd::RefGrid g(p->ni, p->nj, p->nk);
+  const size_t siz = g.siz_icmp;
+  size_t acc = 0;
+  float *dc = dmalloc<float>(3 * siz, acc, p->stream);
+  float *dm = dmalloc<float>(10 * siz, acc, p->stream);
+  for (int c = 0; c < 3; c++) ps.copy(dc + c * siz, d->coord + c * siz, siz * sizeof(float), p->stream);
+  CK(cudaMemsetAsync(dm, 0, 10 * siz * sizeof(float), p->stream));
+  const long long sx = g.nx, sz = (long long)g.nx * g.ny, off0 = 3 + 3 * sx + 3 * sz;
+  float *out[10];
+  for (int f = 0; f < 10; f++) out[f] = dm + f * siz;
+  cgfd::launch_metric(dc, dc + siz, dc + 2 * siz, out, p->ni, p->nj, p->nk, sx, sz, off0, p->stream);
+  CK(cudaGetLastError());
+  for (int f = 0; f < 10; f++) {
+    void *dst = f == 0 ? (void *)p->jac : p->rvoid(p->coef, (size_t)(f - 1) * p->sf);
+    if (p->fp64)
+      cgfd::launch_repack_in(out[f], (double *)dst, p->ni, p->nj, p->nk, p->sx, p->sz, p->off0, 0, 1, p->stream);
+    else
+      cgfd::launch_repack_in(out[f], (float *)dst, p->ni, p->nj, p->nk, p->sx, p->sz, p->off0, 0, 1, p->stream);
+  }
+  CK(cudaGetLastError());
+  ps.copy_out(view, dm, siz * sizeof(float), p->stream);
+  const size_t top = (size_t)(p->nk - 1 + 3) * g.nx * g.ny, plane = (size_t)g.nx * g.ny;
+  for (int f = 1; f < 10; f++)
+    CK(cudaMemcpyAsync(view + f * siz + top, dm + f * siz + top, plane * sizeof(float), cudaMemcpyDeviceToHost,
+                       p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  dfree(dc, p->stream);
+  dfree(dm, p->stream);
 }
 
 // a real-typed device array of n elements (doubles in the FP64 build), held as float*
@@ -680,7 +745,10 @@ void problem_bytes(const cgfd_problem_desc *d, int nshot, const cgfd_source_desc
   const size_t coef32 = (size_t)ncoef * sf * F, coef16 = (size_t)ncoef * sf * 2, jac = (size_t)sf * F;
   const size_t stage_buf = (size_t)(d->ni + 6) * (d->nj + 6) * (d->nk + 6) * sizeof(float);
   size_t r = waves + (c16 ? coef16 : coef32) + jac;
-  const size_t high = waves + jac + coef32 + (c16 ? std::max(stage_buf, coef16 + 8 * (size_t)ncoef) : stage_buf);
+  // metric computed on the device (no metric given): coordinates and the 10 metric fields in the
+  // reference layout are held beside the staging buffer while the metric is repacked
+  const size_t upload = stage_buf * (d->metric ? 1 : 14);
+  const size_t high = waves + jac + coef32 + (c16 ? std::max(upload, coef16 + 8 * (size_t)ncoef) : upload);
   if (d->free_top)
     r += (size_t)2 * 9 * d->ni * d->nj * F + (size_t)9 * cgfd::kFluxPlanes * (d->ni + 6) * (d->nj + 6) * nshot * F;
   cgfd::PmlFaceHost fh[3][2];
@@ -823,13 +891,26 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   // coefficients: metric (ghosts kept for the traction image), 1/rho, medium
   cgfd::RefGrid g(p->ni, p->nj, p->nk);
   float *stage_buf = dmalloc<float>(g.siz_icmp, B, p->stream);
+  // desc->metric NULL: metrics computed on the device from the coordinates; the host-side
+  // setup below then reads the description with `view` as its metric
+  std::unique_ptr<float, void (*)(void *)> view(nullptr, std::free);
+  cgfd_problem_desc dv;
   {
     PinnedStager &ps = PinnedStager::for_device(p->device);
     std::lock_guard<std::mutex> lk(ps.mutex());
-    upload_field(p, d->metric, p->jac, stage_buf, 0, 1, &ps);
-    for (int c = 0; c < 9; c++)
-      upload_field(p, d->metric + (size_t)(1 + c) * g.siz_icmp, p->rvoid(p->coef, (size_t)c * p->sf), stage_buf, 0, 1,
-                   &ps);
+    if (d->metric) {
+      upload_field(p, d->metric, p->jac, stage_buf, 0, 1, &ps);
+      for (int c = 0; c < 9; c++)
+        upload_field(p, d->metric + (size_t)(1 + c) * g.siz_icmp, p->rvoid(p->coef, (size_t)c * p->sf), stage_buf, 0,
+                     1, &ps);
+    } else {
+      view.reset(static_cast<float *>(std::calloc((size_t)10 * g.siz_icmp, sizeof(float))));
+      if (!view) throw cgfd::Error(CGFD_ERR_NOMEM, "host memory for the metric view");
+      metric_from_coords(p, d, ps, view.get());
+      dv = *d;
+      dv.metric = view.get();
+      d = &dv;
+    }
     upload_field(p, d->medium, p->rvoid(p->coef, (size_t)cgfd::CF_SLW * p->sf), stage_buf, 1, 0, &ps);
     int nmed = cgfd::medium_ncmp(d->medium_type) - 1;
     for (int c = 0; c < nmed; c++)

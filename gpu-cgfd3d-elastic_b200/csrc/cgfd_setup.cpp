@@ -26,7 +26,8 @@ void validate_desc(const cgfd_problem_desc *d) {
   if (!d) throw Error(CGFD_ERR_INVALID, "desc is NULL");
   if (d->ni < 8 || d->nj < 8 || d->nk < 8) throw Error(CGFD_ERR_INVALID, "grid must have at least 8 points per axis");
   if (medium_ncmp(d->medium_type) < 0) throw Error(CGFD_ERR_UNSUPPORTED, "medium_type must be elastic iso/vti/aniso");
-  if (!d->metric || !d->medium) throw Error(CGFD_ERR_INVALID, "metric and medium arrays are required");
+  if (!d->medium) throw Error(CGFD_ERR_INVALID, "the medium array is required");
+  if (!d->metric && !d->coord) throw Error(CGFD_ERR_INVALID, "coordinates are required when no metric is given");
   if (!(d->dt > 0.0f)) throw Error(CGFD_ERR_INVALID, "dt must be > 0");
   if (d->nt_total < 1) throw Error(CGFD_ERR_INVALID, "nt_total must be >= 1");
   if (d->precision < CGFD_PREC_FP32 || d->precision > CGFD_PREC_FP64)
@@ -388,7 +389,8 @@ void src_setup(const cgfd_problem_desc *d, SrcHost &s, const Located *loc) {
             if (i < 0 || i >= d->ni || j < 0 || j >= d->nj || k < 0 || k >= d->nk) continue;
             double w = delt[(ii + half) + len * (jj + half) + len * len * (kk + half)] / sum;
             size_t p = g.at(i, j, k);
-            double jac = d->metric[p];
+            // (no metric: only the sizes are wanted, cgfd_problem_bytes before the metric exists)
+            double jac = d->metric ? (double)d->metric[p] : 1.0;
             double rho = d->medium[p];
             double slw = rho > 1e-10 ? 1.0 / rho : 0.0;
             size_t e = (size_t)is_local * s.max_ext + ne;

@@ -125,8 +125,12 @@ typedef struct cgfd_problem_desc {
   int medium_type;          /* CGFD_MEDIUM_ELASTIC_*                                        */
   const float *coord;       /* [3][nz][ny][nx] x,y,z with ghosts filled; used for the PML
                                length/spacing average (bdry_t.cu:334-451). May be NULL when
-                               no PML face is enabled.                                       */
-  const float *metric;      /* [10][nz][ny][nx]                                             */
+                               no PML face is enabled and metric is given.                   */
+  const float *metric;      /* [10][nz][ny][nx] jac, xi_x..zeta_z with ghosts filled; or
+                               NULL: computed on the device from coord (the "calculate"
+                               metric method: gd_curv_metric_cal + geometric_symmetry, here
+                               in FP64, equal to cgfd_metric_calc bitwise), so that only the
+                               coordinates cross the host link                               */
   const float *medium;      /* [ncmp][nz][ny][nx]                                           */
   cgfd_pml_face pml[3][2];  /* [x,y,z][left/bottom, right/top]                              */
   int   free_top;           /* 1: traction-image free surface at the top (z2)              */

@@ -25,3 +25,28 @@ def test_gpu_metric_rejects_bad_sizes():
     from cgfd_b200 import lib
     out = np.zeros(10, np.float32)
     assert lib().cgfd_metric_calc_gpu(0, 2, 2, 2, out.ctypes.data, out.ctypes.data) == -1
+
+
+@pytest.mark.parametrize("medium,precision", [("iso", 0), ("vti", 3), ("aniso", 5)])
+def test_problem_without_metric_equals_host_metric(medium, precision):
+    """A description without a metric (desc.metric NULL): the problem computes it on the device
+    from the coordinates. Its run equals the run given the host FP64 metric (cgfd_metric_calc)
+    bitwise, seismograms and final wavefield: the metric itself is bitwise equal, and so are the
+    host-side setups that read it (source weights from the Jacobian, free-surface matrices from
+    the top plane). FP32, 16-bit fixed-point coefficients and the FP64 build."""
+    import dataclasses
+    from cgfd_b200 import Simulation
+    p = synth.make_problem(52, 44, 36, 100.0, 40, dt=None, medium=medium, npml=6, nsrc=1, sta_grid=(3, 3),
+                           seed=5, src_depth=(800.0, 800.0), center_src=True)
+    p.precision = precision
+    q = dataclasses.replace(p, metric=None)
+    a = Simulation(p)
+    a.run()
+    b = Simulation(q)
+    b.run()
+    assert np.abs(a.seismograms()).max() > 0
+    assert np.array_equal(a.seismograms(), b.seismograms())
+    assert np.array_equal(a.wavefield(), b.wavefield())
+    assert a.device_bytes() == b.device_bytes()
+    a.close()
+    b.close()
