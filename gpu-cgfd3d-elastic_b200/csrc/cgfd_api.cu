@@ -1758,18 +1758,32 @@ int cgfd_autotune(cgfd_problem *p, int steps, int *chosen) {
       CK(cudaEventElapsedTime(&ms, e0, e1));
       return ms;
     };
-    for (const auto &sc : cand) {
-      const int c = sc.second;
+    auto use = [&](const std::pair<int, int> &sc) {
       CK(cudaStreamSynchronize(p->stream));
       if (p->use_tma && sc.first != p->shape) {
         p->shape = sc.first;
         make_maps(p);
       }
-      p->nzc = c;
+      p->nzc = sc.second;
       make_tiles(p);
-      const float ms = time_choice();
-      if (ms < best_ms) { best_ms = ms; best = c; best_shape = sc.first; }
+    };
+    // every candidate once, then the three fastest again over three times the steps (close
+    // candidates differ by less than a short run's spread)
+    std::vector<std::pair<float, std::pair<int, int>>> timed;
+    for (const auto &sc : cand) {
+      use(sc);
+      timed.emplace_back(time_choice(), sc);
     }
+    std::stable_sort(timed.begin(), timed.end(),
+                     [](const auto &a, const auto &b) { return a.first < b.first; });
+    const int steps1 = steps;
+    steps = 3 * steps1;
+    for (size_t r = 0; r < std::min<size_t>(3, timed.size()); r++) {
+      use(timed[r].second);
+      const float ms = time_choice();
+      if (ms < best_ms) { best_ms = ms; best = timed[r].second.second; best_shape = timed[r].second.first; }
+    }
+    steps = steps1;
     CK(cudaStreamSynchronize(p->stream));
     if (p->use_tma && best_shape != p->shape) {
       p->shape = best_shape;

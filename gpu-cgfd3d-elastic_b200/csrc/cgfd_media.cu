@@ -17,6 +17,7 @@
 #include <cfloat>
 #include <cuda_runtime.h>
 
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -34,6 +35,7 @@ struct LayerDev {
   float x0, y0, dx, dy;
   const float *elev;                       // [NI][ny][nx]
   const float *p[9];                       // rho, rho_grad, rho_pow, vp, vp_grad, vp_pow, vs, vs_grad, vs_pow
+  const float *par;                        // general files: [npar][value, grad, pow][NI][ny][nx]
 };
 
 struct P3 {
@@ -279,6 +281,256 @@ __global__ void k_media_avg(const __grid_constant__ LayerDev m, const __grid_con
   }
 }
 
+
+// -----------------------------------------------------------------------------------------
+// VTI, TTI and 21-Cij layer files (media_layer2model_el_vti / _el_aniso,
+// src/media/media_layer2model.cpp:173-398). The parameters of a file type, in the file's order:
+//   22 vti_prem     rho vph vpv vsh vsv eta            25 tti_thomsen rho vp0 vs0 epsilon delta gamma azimuth dip
+//   23 vti_thomsen  rho vp0 vs0 epsilon delta gamma    26 tti_bond    rho c11 c33 c55 c66 c13 azimuth dip
+//   24 vti_cij      rho c11 c33 c55 c66 c13            27 aniso_cij   rho c11 c12 ... c66 (21)
+// Every parameter is value + dz^pow * grad of its layer (CalPointValue_layer,
+// media_layer2model.cpp:454-1216), averaged with the layer above on an interface; para2vti /
+// para2tti (media_utility.cpp:620-831) turn them into the stiffness: 6 fields (rho c11 c33 c55
+// c66 c13) for the VTI files, 22 (rho c11 c12 ... c66) for the others. The har / ari
+// averages take c_ij harmonically / arithmetically over the 9^3 sub-points, rho arithmetically.
+template <int T> struct LayerFile;
+template <> struct LayerFile<22> { static constexpr int NPAR = 6, NOUT = 6; };
+template <> struct LayerFile<23> { static constexpr int NPAR = 6, NOUT = 6; };
+template <> struct LayerFile<24> { static constexpr int NPAR = 6, NOUT = 6; };
+template <> struct LayerFile<25> { static constexpr int NPAR = 8, NOUT = 22; };
+template <> struct LayerFile<26> { static constexpr int NPAR = 8, NOUT = 22; };
+template <> struct LayerFile<27> { static constexpr int NPAR = 22, NOUT = 22; };
+
+// value + dz^pow * grad of parameter q of layer mi at (x, y)
+__device__ float layer_val_par(const LayerDev &m, int q, int mi, float x, float y, float dz) {
+  const size_t sl = (size_t)m.nx * m.ny, lv = sl * m.ni_;
+  const float *b = m.par + (size_t)q * 3 * lv + (size_t)mi * sl;
+  const float v = bilinear(m, b, x, y);
+  const float g = bilinear(m, b + lv, x, y);
+  const float pw = bilinear(m, b + 2 * lv, x, y);
+  return (float)__dadd_rn((double)v, __dmul_rn(pow((double)dz, (double)pw), (double)g));
+}
+
+// AssignLayerMediaPara2Point + CalPointValue_layer for the general files; 1: outside the mesh
+template <int NPAR>
+__device__ int point_params(const LayerDev &m, P3 a, float var[NPAR]) {
+  const float maxx = __fadd_rn(m.x0, __fmul_rn(m.dx, (float)(m.nx - 1)));
+  const float maxy = __fadd_rn(m.y0, __fmul_rn(m.dy, (float)(m.ny - 1)));
+  if (a.x < m.x0 || a.x > maxx || a.y < m.y0 || a.y > maxy) return 1;
+  float e[kMaxInterfaces];
+  const size_t sl = (size_t)m.nx * m.ny, lv = sl * m.ni_;
+  for (int n = 0; n < m.ni_; n++) e[n] = bilinear(m, m.elev + n * sl, a.x, a.y);
+  int mi = last_ge(a.z, e, m.ni_);
+  if (mi == -1) {  // above the top interface: the top layer's values
+    mi = last_ge(e[0], e, m.ni_);
+    for (int q = 0; q < NPAR; q++) var[q] = bilinear(m, m.par + (size_t)q * 3 * lv + (size_t)mi * sl, a.x, a.y);
+    return 0;
+  }
+  float dz = __fsub_rn(e[mi], a.z);
+  for (int q = 0; q < NPAR; q++) var[q] = layer_val_par(m, q, mi, a.x, a.y, dz);
+  if ((int)dz == 0) {  // on an interface (the reference's integer-abs test)
+    const int mt = first_ge(a.z, e, m.ni_) - 1;
+    if (mt >= 0) {
+      dz = __fsub_rn(e[mt], a.z);
+      for (int q = 0; q < NPAR; q++) {
+        const float top = layer_val_par(m, q, mt, a.x, a.y, dz);
+        var[q] = (float)__ddiv_rn((double)__fadd_rn(var[q], top), 2.0);
+      }
+    }
+  }
+  return 0;
+}
+
+// sqrt(2 delta c33 (c33 - cs) + (c33 - cs)^2) - cs: Thomsen's c13 (the reference's expression,
+// double with the float square of the float difference)
+__device__ float thomsen_c13(float delta, float c33, float cs) {
+  const float dcs = __fsub_rn(c33, cs);
+  const double t = __dadd_rn(__dmul_rn(__dmul_rn(__dmul_rn(2.0, (double)delta), (double)c33), (double)dcs),
+                             (double)__fmul_rn(dcs, dcs));
+  return (float)__dsub_rn(__dsqrt_rn(t), (double)cs);
+}
+
+// 2.0 x a * c + c (double, stored float)
+__device__ float thomsen_scale(float a, float c) {
+  return (float)__dadd_rn(__dmul_rn(__dmul_rn(2.0, (double)a), (double)c), (double)c);
+}
+
+// para2vti: o = rho c11 c33 c55 c66 c13
+template <int T>
+__device__ void para2vti(const float *v, float *o) {
+  if constexpr (T == 22) {  // rho vph vpv vsh vsv eta
+    const float rho = v[0];
+    o[1] = __fmul_rn(__fmul_rn(v[1], v[1]), rho);
+    o[2] = __fmul_rn(__fmul_rn(v[2], v[2]), rho);
+    o[4] = __fmul_rn(__fmul_rn(v[3], v[3]), rho);
+    o[3] = __fmul_rn(__fmul_rn(v[4], v[4]), rho);
+    o[0] = rho;
+    o[5] = (float)__dmul_rn((double)v[5], __dsub_rn((double)o[1], __dmul_rn(2.0, (double)o[3])));
+  } else if constexpr (T == 23) {  // rho vp0 vs0 epsilon delta gamma
+    const float rho = v[0];
+    const float c33 = __fmul_rn(__fmul_rn(v[1], v[1]), rho), c55 = __fmul_rn(__fmul_rn(v[2], v[2]), rho);
+    o[0] = rho;
+    o[2] = c33;
+    o[3] = c55;
+    o[4] = thomsen_scale(v[5], c55);
+    o[1] = thomsen_scale(v[3], c33);
+    o[5] = thomsen_c13(v[4], c33, c55);
+  } else {  // rho c11 c33 c55 c66 c13
+    for (int q = 0; q < 6; q++) o[q] = v[q];
+  }
+}
+
+// BondTransform (media_utility.cpp:683-724): C = R C0 R^T for dip theta and azimuth phi
+// (degrees), float matrix products summed in index order. Kept alike on purpose: row 5 of R
+// holds a11 a31 + a12 a31 in its last column, as the reference's table does.
+__device__ void bond(const float c0[6][6], float theta, float phi, float *o) {
+  const double pi = 3.14159265358979311600;  // acos(-1) in double
+  theta = (float)__dmul_rn((double)theta, __ddiv_rn(pi, 180.0));
+  phi = (float)__dmul_rn((double)phi, __ddiv_rn(pi, 180.0));
+  const float ct = cosf(theta), st = sinf(theta), cp = cosf(phi), sp = sinf(phi);
+  const float a11 = __fmul_rn(ct, sp), a12 = cp, a13 = __fmul_rn(st, sp);
+  const float a21 = -__fmul_rn(ct, cp), a22 = sp, a23 = -__fmul_rn(st, cp);
+  const float a31 = -st, a32 = 0.f, a33 = ct;
+  auto m2 = [](float a, float b) { return __fmul_rn(__fmul_rn(2.f, a), b); };
+  const float R[6][6] = {
+      {__fmul_rn(a11, a11), __fmul_rn(a12, a12), __fmul_rn(a13, a13), m2(a12, a13), m2(a13, a11), m2(a11, a12)},
+      {__fmul_rn(a21, a21), __fmul_rn(a22, a22), __fmul_rn(a23, a23), m2(a22, a23), m2(a23, a21), m2(a21, a22)},
+      {__fmul_rn(a31, a31), __fmul_rn(a32, a32), __fmul_rn(a33, a33), m2(a32, a33), m2(a33, a31), m2(a31, a32)},
+      {__fmul_rn(a21, a31), __fmul_rn(a22, a32), __fmul_rn(a23, a33), __fadd_rn(__fmul_rn(a22, a33), __fmul_rn(a23, a32)),
+       __fadd_rn(__fmul_rn(a21, a33), __fmul_rn(a23, a31)), __fadd_rn(__fmul_rn(a22, a31), __fmul_rn(a21, a32))},
+      {__fmul_rn(a31, a11), __fmul_rn(a32, a12), __fmul_rn(a33, a13), __fadd_rn(__fmul_rn(a12, a33), __fmul_rn(a13, a32)),
+       __fadd_rn(__fmul_rn(a13, a31), __fmul_rn(a11, a33)), __fadd_rn(__fmul_rn(a11, a31), __fmul_rn(a12, a31))},
+      {__fmul_rn(a11, a21), __fmul_rn(a12, a22), __fmul_rn(a13, a23), __fadd_rn(__fmul_rn(a12, a23), __fmul_rn(a13, a22)),
+       __fadd_rn(__fmul_rn(a13, a21), __fmul_rn(a11, a23)), __fadd_rn(__fmul_rn(a11, a22), __fmul_rn(a12, a21))}};
+  float RC[6][6];
+  for (int i = 0; i < 6; i++)
+    for (int j = 0; j < 6; j++) {
+      float s = 0.f;
+      for (int k = 0; k < 6; k++) s = __fadd_rn(s, __fmul_rn(R[i][k], c0[k][j]));
+      RC[i][j] = s;
+    }
+  int n = 1;
+  for (int i = 0; i < 6; i++)
+    for (int j = i; j < 6; j++) {
+      float s = 0.f;
+      for (int k = 0; k < 6; k++) s = __fadd_rn(s, __fmul_rn(RC[i][k], R[j][k]));
+      o[n++] = s;
+    }
+}
+
+// para2tti: o = rho c11 c12 c13 c14 c15 c16 c22 c23 c24 c25 c26 c33 c34 c35 c36 c44 c45 c46 c55 c56 c66
+template <int T>
+__device__ void para2tti(const float *v, float *o) {
+  if constexpr (T == 27) {
+    for (int q = 0; q < 22; q++) o[q] = v[q];
+  } else {
+    float c11, c33, c44, c66, c13;
+    if constexpr (T == 25) {  // rho vp0 vs0 epsilon delta gamma azimuth dip
+      c33 = __fmul_rn(__fmul_rn(v[1], v[1]), v[0]);
+      c44 = __fmul_rn(__fmul_rn(v[2], v[2]), v[0]);
+      c66 = thomsen_scale(v[5], c44);
+      c11 = thomsen_scale(v[3], c33);
+      c13 = thomsen_c13(v[4], c33, c44);
+    } else {  // rho c11 c33 c55 c66 c13 azimuth dip
+      c11 = v[1]; c33 = v[2]; c44 = v[3]; c66 = v[4]; c13 = v[5];
+    }
+    o[0] = v[0];
+    const float c12 = __fsub_rn(c11, __fmul_rn(2.f, c66));
+    const float c0[6][6] = {{c11, c12, c13, 0.f, 0.f, 0.f}, {c12, c11, c13, 0.f, 0.f, 0.f}, {c13, c13, c33, 0.f, 0.f, 0.f},
+                            {0.f, 0.f, 0.f, c44, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f, c44, 0.f}, {0.f, 0.f, 0.f, 0.f, 0.f, c66}};
+    bond(c0, v[7], v[6], o);
+  }
+}
+
+template <int T>
+__device__ void para2out(const float *v, float *o) {
+  if constexpr (LayerFile<T>::NOUT == 6) para2vti<T>(v, o);
+  else para2tti<T>(v, o);
+}
+
+struct OutDev {
+  long long n;
+  float *f;  // [NOUT][n]
+  int *err;
+};
+
+template <int T>
+__global__ void k_media_loc_gen(const __grid_constant__ LayerDev m, const __grid_constant__ GridDev g,
+                                const __grid_constant__ OutDev out) {
+  constexpr int NP = LayerFile<T>::NPAR, NO = LayerFile<T>::NOUT;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < out.n; t += (long long)gridDim.x * blockDim.x) {
+    float var[NP], o[NO];
+    if (point_params<NP>(m, P3{g.x[t], g.y[t], g.z[t]}, var)) {
+      atomicOr(out.err, 1);
+      continue;
+    }
+    para2out<T>(var, o);
+    for (int q = 0; q < NO; q++) out.f[q * out.n + t] = o[q];
+  }
+}
+
+// the har / ari equivalent medium of the general files (parametrization_layer_el_vti_har /
+// _ari, _el_aniso_har / _ari, media_layer2model.cpp:2176-2793)
+template <int T, bool HAR>
+__global__ void k_media_avg_gen(const __grid_constant__ LayerDev m, const __grid_constant__ GridDev g,
+                                const __grid_constant__ OutDev out) {
+  constexpr int NP = LayerFile<T>::NPAR, NO = LayerFile<T>::NOUT;
+  const long long sl = g.nx, ss = (long long)g.nx * g.ny;
+  const long long n = (long long)(g.nx - 2) * (g.ny - 2) * (g.nz - 2);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(t % (g.nx - 2)), j = 1 + (int)((t / (g.nx - 2)) % (g.ny - 2));
+    const int k = 1 + (int)(t / ((long long)(g.nx - 2) * (g.ny - 2)));
+    const long long indx = i + j * sl + k * ss;
+    const long long c[8] = {indx - 1 - sl - ss, indx - sl - ss, indx - ss, indx - 1 - ss,
+                            indx - 1 - sl,      indx - sl,      indx,      indx - 1};
+    bool above = false, mixed = false;
+    for (int q = 0; q < 8; q++) {
+      const int v = g.mat[c[q]];
+      if (v == -1) above = true;
+      if (v != g.mat[c[0]]) mixed = true;
+    }
+    if (above || !mixed) continue;
+    P3 M[8];
+    for (int q = 0; q < 8; q++) M[q] = P3{g.hx[c[q]], g.hy[c[q]], g.hz[c[q]]};
+    float acc[NO];
+    for (int q = 0; q < NO; q++) acc[q] = 0.f;
+    int bad = 0;
+    auto lerp = [](P3 a, P3 b, int s) {
+      return P3{__fadd_rn(a.x, __fmul_rn(__fdiv_rn(__fsub_rn(b.x, a.x), (float)kSub), (float)s)),
+                __fadd_rn(a.y, __fmul_rn(__fdiv_rn(__fsub_rn(b.y, a.y), (float)kSub), (float)s)),
+                __fadd_rn(a.z, __fmul_rn(__fdiv_rn(__fsub_rn(b.z, a.z), (float)kSub), (float)s))};
+    };
+    for (int kk = 0; kk <= kSub; kk++)
+      for (int jj = 0; jj <= kSub; jj++)
+        for (int ii = 0; ii <= kSub; ii++) {
+          const P3 lx00 = lerp(M[0], M[1], ii), lx10 = lerp(M[3], M[2], ii);
+          const P3 lx01 = lerp(M[4], M[5], ii), lx11 = lerp(M[7], M[6], ii);
+          const P3 lxy0 = lerp(lx00, lx10, jj), lxy1 = lerp(lx01, lx11, jj);
+          float var[NP], o[NO];
+          if (point_params<NP>(m, lerp(lxy0, lxy1, kk), var)) { bad = 1; continue; }
+          para2out<T>(var, o);
+          acc[0] = __fadd_rn(acc[0], o[0]);
+          for (int q = 1; q < NO; q++)
+            acc[q] = HAR ? (float)__dadd_rn((double)acc[q], __ddiv_rn(1.0, (double)o[q])) : __fadd_rn(acc[q], o[q]);
+        }
+    if (bad) { atomicOr(out.err, 1); continue; }
+    constexpr int nsg = (kSub + 1) * (kSub + 1) * (kSub + 1);
+    out.f[indx] = __fdiv_rn(acc[0], (float)nsg);
+    for (int q = 1; q < NO; q++)
+      out.f[q * out.n + indx] = HAR ? (float)__ddiv_rn((double)nsg, (double)acc[q]) : __fdiv_rn(acc[q], (float)nsg);
+  }
+}
+
+template <int T>
+void launch_media_gen(const LayerDev &m, const GridDev &g, const OutDev &o, int method, cudaStream_t st) {
+  k_media_loc_gen<T><<<148 * 8, 256, 0, st>>>(m, g, o);
+  if (method == CGFD_MEDIA_LOC) return;
+  k_half_grid<<<148 * 8, 256, 0, st>>>(g);
+  k_mark<<<148 * 8, 256, 0, st>>>(m, g);
+  if (method == CGFD_MEDIA_HAR) k_media_avg_gen<T, true><<<148 * 8, 128, 0, st>>>(m, g, o);
+  else k_media_avg_gen<T, false><<<148 * 8, 128, 0, st>>>(m, g, o);
+}
+
 }  // namespace
 }  // namespace cgfd
 
@@ -370,6 +622,156 @@ extern "C" int cgfd_media_layer_el_iso_gpu(int device, int ni, int nj, int nk, c
     set_last_error((herr & 1) ? "a grid point lies outside the interface mesh"
                               : "vp must be larger than sqrt(2) vs in every layer");
     return CGFD_ERR_INVALID;
+  }
+  return CGFD_OK;
+}
+
+extern "C" int cgfd_media_layer_gpu(int device, int ni, int nj, int nk, const float *coord, const cgfd_layer_media *lm,
+                                    int medium_type, int method, float *medium) {
+  using namespace cgfd;
+  if (!coord || !lm || !medium || !lm->elevation || !lm->param || ni < 4 || nj < 4 || nk < 4 ||
+      method < CGFD_MEDIA_LOC || method > CGFD_MEDIA_ARI) {
+    set_last_error("invalid argument");
+    return CGFD_ERR_INVALID;
+  }
+  if (lm->num_interfaces < 1 || lm->num_interfaces > kMaxInterfaces || lm->nx < 2 || lm->ny < 2) {
+    set_last_error("layer model: 1 to 64 interfaces on a mesh of at least 2 x 2 points are required");
+    return CGFD_ERR_INVALID;
+  }
+  const int T = lm->type;
+  // the file types each target medium accepts (media_layer2model_el_iso / _el_vti / _el_aniso)
+  const bool ok = (medium_type == CGFD_MEDIUM_ELASTIC_ISO && T == CGFD_LAYER_ELASTIC_ISO) ||
+                  (medium_type == CGFD_MEDIUM_ELASTIC_VTI && T >= CGFD_LAYER_VTI_PREM && T <= CGFD_LAYER_VTI_CIJ) ||
+                  (medium_type == CGFD_MEDIUM_ELASTIC_ANISO && T >= CGFD_LAYER_ELASTIC_ISO && T <= CGFD_LAYER_ANISO_CIJ);
+  if (!ok) {
+    set_last_error("layer file type not usable for this medium type");
+    return CGFD_ERR_INVALID;
+  }
+  const size_t nx = ni + 6, ny = nj + 6, nz = nk + 6, n = nx * ny * nz;
+  const size_t lv = (size_t)lm->num_interfaces * lm->nx * lm->ny;
+  const int nout_med = medium_type == CGFD_MEDIUM_ELASTIC_ISO ? 3 : (medium_type == CGFD_MEDIUM_ELASTIC_VTI ? 6 : 22);
+  auto M = [&](int f) { return medium + (size_t)f * n; };  // field f of the output, desc order
+
+  // the family's fields on the device: iso (rho lambda mu), VTI (rho c11 c33 c55 c66 c13), 22 Cij
+  std::vector<float> fam;
+  int nfam = 0;
+  if (T == CGFD_LAYER_ELASTIC_ISO) {
+    cgfd_layer_model m{};
+    m.num_interfaces = lm->num_interfaces; m.nx = lm->nx; m.ny = lm->ny;
+    m.x0 = lm->x0; m.y0 = lm->y0; m.dx = lm->dx; m.dy = lm->dy;
+    m.elevation = lm->elevation;
+    const float **pp[9] = {&m.rho, &m.rho_grad, &m.rho_pow, &m.vp, &m.vp_grad, &m.vp_pow, &m.vs, &m.vs_grad, &m.vs_pow};
+    for (int q = 0; q < 9; q++) *pp[q] = lm->param + (size_t)q * lv;
+    if (medium_type == CGFD_MEDIUM_ELASTIC_ISO)
+      return cgfd_media_layer_el_iso_gpu(device, ni, nj, nk, coord, &m, method, medium);
+    fam.resize(3 * n);
+    nfam = 3;
+    const int rc = cgfd_media_layer_el_iso_gpu(device, ni, nj, nk, coord, &m, method, fam.data());
+    if (rc) return rc;
+  } else {
+    nfam = T <= CGFD_LAYER_VTI_CIJ ? 6 : 22;
+    const int npar = T <= CGFD_LAYER_VTI_CIJ ? 6 : (T == CGFD_LAYER_ANISO_CIJ ? 22 : 8);
+    std::vector<void *> owned;
+    cudaStream_t st = nullptr;
+    auto cleanup = [&] {
+      for (void *q : owned) cudaFree(q);
+      if (st) cudaStreamDestroy(st);
+    };
+    auto fail = [&](cudaError_t e, const char *what) {
+      cleanup();
+      set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+      return e == cudaErrorMemoryAllocation ? CGFD_ERR_NOMEM : CGFD_ERR_CUDA;
+    };
+    auto dalloc = [&](size_t bytes, void **out) {
+      cudaError_t e = cudaMalloc(out, bytes);
+      if (e == cudaSuccess) owned.push_back(*out);
+      return e;
+    };
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(e, "cudaSetDevice");
+    if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "cudaStreamCreate");
+    LayerDev m{};
+    m.ni_ = lm->num_interfaces; m.nx = lm->nx; m.ny = lm->ny;
+    m.x0 = lm->x0; m.y0 = lm->y0; m.dx = lm->dx; m.dy = lm->dy;
+    float *dm = nullptr, *dc = nullptr, *dout = nullptr, *dh = nullptr;
+    int *derr = nullptr, *dmat = nullptr;
+    if ((e = dalloc((1 + 3 * (size_t)npar) * lv * sizeof(float), (void **)&dm)) != cudaSuccess) return fail(e, "cudaMalloc");
+    if ((e = cudaMemcpyAsync(dm, lm->elevation, lv * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(dm + lv, lm->param, 3 * (size_t)npar * lv * sizeof(float), cudaMemcpyHostToDevice, st)) !=
+            cudaSuccess)
+      return fail(e, "cudaMemcpy");
+    m.elev = dm;
+    m.par = dm + lv;
+    if ((e = dalloc(3 * n * sizeof(float), (void **)&dc)) != cudaSuccess) return fail(e, "cudaMalloc");
+    if ((e = dalloc((size_t)nfam * n * sizeof(float), (void **)&dout)) != cudaSuccess) return fail(e, "cudaMalloc");
+    if ((e = dalloc(sizeof(int), (void **)&derr)) != cudaSuccess) return fail(e, "cudaMalloc");
+    if ((e = cudaMemcpyAsync(dc, coord, 3 * n * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+      return fail(e, "cudaMemcpy");
+    cudaMemsetAsync(derr, 0, sizeof(int), st);
+    GridDev g{};
+    g.nx = (int)nx; g.ny = (int)ny; g.nz = (int)nz;
+    g.x = dc; g.y = dc + n; g.z = dc + 2 * n;
+    if (method != CGFD_MEDIA_LOC) {
+      if ((e = dalloc(3 * n * sizeof(float), (void **)&dh)) != cudaSuccess) return fail(e, "cudaMalloc");
+      if ((e = dalloc(n * sizeof(int), (void **)&dmat)) != cudaSuccess) return fail(e, "cudaMalloc");
+      g.hx = dh; g.hy = dh + n; g.hz = dh + 2 * n;
+      g.mat = dmat;
+    }
+    OutDev o{(long long)n, dout, derr};
+    switch (T) {
+      case CGFD_LAYER_VTI_PREM: launch_media_gen<22>(m, g, o, method, st); break;
+      case CGFD_LAYER_VTI_THOMSEN: launch_media_gen<23>(m, g, o, method, st); break;
+      case CGFD_LAYER_VTI_CIJ: launch_media_gen<24>(m, g, o, method, st); break;
+      case CGFD_LAYER_TTI_THOMSEN: launch_media_gen<25>(m, g, o, method, st); break;
+      case CGFD_LAYER_TTI_BOND: launch_media_gen<26>(m, g, o, method, st); break;
+      default: launch_media_gen<27>(m, g, o, method, st); break;
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "media kernels");
+    int herr = 0;
+    fam.resize((size_t)nfam * n);
+    if ((e = cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(fam.data(), dout, (size_t)nfam * n * sizeof(float), cudaMemcpyDeviceToHost, st)) !=
+            cudaSuccess)
+      return fail(e, "cudaMemcpy");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail(e, "cudaStreamSynchronize");
+    cleanup();
+    if (herr) {
+      set_last_error("a grid point lies outside the interface mesh");
+      return CGFD_ERR_INVALID;
+    }
+  }
+  auto F = [&](int f) { return fam.data() + (size_t)f * n; };
+  if (medium_type == CGFD_MEDIUM_ELASTIC_VTI) {  // rho c11 c33 c55 c66 c13 -> rho c11 c13 c33 c55 c66
+    const int from[6] = {0, 1, 5, 2, 3, 4};
+    for (int f = 0; f < 6; f++) std::memcpy(M(f), F(from[f]), n * sizeof(float));
+    return CGFD_OK;
+  }
+  // 21-Cij medium (desc order rho c11 c12 c13 c14 c15 c16 c22 c23 c24 c25 c26 c33 c34 c35 c36 c44
+  // c45 c46 c55 c56 c66)
+  if (nfam == 22) {
+    std::memcpy(medium, fam.data(), 22 * n * sizeof(float));
+    return CGFD_OK;
+  }
+  std::memset(medium, 0, (size_t)nout_med * n * sizeof(float));
+  enum { RHO = 0, C11 = 1, C12 = 2, C13 = 3, C22 = 7, C23 = 8, C33 = 12, C44 = 16, C55 = 19, C66 = 21 };
+  const bool iso = nfam == 3;
+#pragma omp parallel for schedule(static)
+  for (long long t = 0; t < (long long)n; t++) {
+    if (iso) {  // el_aniso's elastic_isotropic branch: lambda -> c13, mu -> c44
+      const float c13 = F(1)[t], c44 = F(2)[t];
+      const float c11 = (float)((double)c13 + 2.0 * (double)c44);
+      M(RHO)[t] = F(0)[t];
+      M(C11)[t] = c11; M(C22)[t] = c11; M(C33)[t] = c11;
+      M(C12)[t] = c13; M(C13)[t] = c13; M(C23)[t] = c13;
+      M(C44)[t] = c44; M(C55)[t] = c44; M(C66)[t] = c44;
+    } else {  // its VTI branch
+      const float c11 = F(1)[t], c33 = F(2)[t], c55 = F(3)[t], c66 = F(4)[t], c13 = F(5)[t];
+      M(RHO)[t] = F(0)[t];
+      M(C11)[t] = c11; M(C22)[t] = c11; M(C33)[t] = c33;
+      M(C12)[t] = (float)((double)c11 - 2.0 * (double)c66);
+      M(C13)[t] = c13; M(C23)[t] = c13;
+      M(C44)[t] = c55; M(C55)[t] = c55; M(C66)[t] = c66;
+    }
   }
   return CGFD_OK;
 }

@@ -352,7 +352,8 @@ int cgfd_get_shot_group(const cgfd_problem *p);
 /*
  * Autotuner of the bulk kernel's tile: times `steps` graph-replayed time steps for each tile
  * shape (cgfd_set_tile_shape) and z-chunk length (planes per thread block column: 8, 10, 12,
- * 14, 16, 20, 24, 32, 48, 64, 96 and all bulk planes) on this problem, keeps the fastest pair (*chosen:
+ * 14, 16, 20, 24, 32, 48, 64, 96 and all bulk planes) on this problem, times the three fastest
+ * again over 3 x `steps` steps and keeps the fastest pair (*chosen:
  * the z chunk; cgfd_get_tile_shape: the shape) and returns the problem to its freshly created
  * state (zero wavefield, step 0). For a batch it then times the shot groups 4, 8, 16 and every
  * shot at the chosen pair and keeps the fastest (cgfd_get_shot_group). Only on a problem that
@@ -479,6 +480,43 @@ typedef struct cgfd_layer_model {
  */
 int cgfd_media_layer_el_iso_gpu(int device, int ni, int nj, int nk, const float *coord, const cgfd_layer_model *model,
                                 int method, float *medium);
+
+/*
+ * Layer files of every elastic media type (read_interface_file, media_read_file.cpp:22-560),
+ * by the reference's type numbers; the parameters of each, in the file's order:
+ */
+#define CGFD_LAYER_ELASTIC_ISO   21  /* rho vp vs                                              */
+#define CGFD_LAYER_VTI_PREM      22  /* rho vph vpv vsh vsv eta                                */
+#define CGFD_LAYER_VTI_THOMSEN   23  /* rho vp0 vs0 epsilon delta gamma                        */
+#define CGFD_LAYER_VTI_CIJ       24  /* rho c11 c33 c55 c66 c13                                */
+#define CGFD_LAYER_TTI_THOMSEN   25  /* rho vp0 vs0 epsilon delta gamma azimuth dip (degrees)  */
+#define CGFD_LAYER_TTI_BOND      26  /* rho c11 c33 c55 c66 c13 azimuth dip (degrees)          */
+#define CGFD_LAYER_ANISO_CIJ     27  /* rho c11 c12 c13 c14 c15 c16 c22 c23 c24 c25 c26 c33 c34
+                                        c35 c36 c44 c45 c46 c55 c56 c66                        */
+typedef struct cgfd_layer_media {
+  int   type;                    /* CGFD_LAYER_*                                            */
+  int   num_interfaces, nx, ny;  /* as cgfd_layer_model                                     */
+  float x0, y0, dx, dy;
+  const float *elevation;        /* [num_interfaces][ny][nx]                                */
+  const float *param;            /* [npar][3][num_interfaces][ny][nx]: value, gradient and
+                                    power of each parameter of the type, in the order above  */
+} cgfd_layer_media;
+
+/*
+ * Media discretisation of any layer file on the GPU `device` into the cgfd_problem_desc medium
+ * of medium_type (CGFD_MEDIUM_ELASTIC_*): iso from an elastic_isotropic file (as
+ * cgfd_media_layer_el_iso_gpu); VTI [rho c11 c13 c33 c55 c66] from the three VTI files; 21-Cij
+ * [rho c11 c12 ... c66] from any of the seven (iso and VTI files expanded to the full tensor).
+ * method CGFD_MEDIA_LOC / _HAR / _ARI; har and ari average every c_ij harmonically /
+ * arithmetically over the 9^3 sub-points of a half-grid cell an interface crosses (rho
+ * arithmetically), the VTI files' in VTI form before the expansion. CGFD_ERR_INVALID for a
+ * file type the medium type does not take or a grid point outside the interface mesh.
+ * Replaces: media_layer2model_el_vti / _el_aniso (src/media/media_layer2model.cpp:173-398) with
+ * parametrization_layer_el_{vti,aniso}_{loc,har,ari} (:1365-1492, 2176-2793), para2vti,
+ * BondTransform, para2tti (src/media/media_utility.cpp:620-831).
+ */
+int cgfd_media_layer_gpu(int device, int ni, int nj, int nk, const float *coord, const cgfd_layer_media *model,
+                         int medium_type, int method, float *medium);
 
 /*
  * Largest stable time step (FP64): CFL * min distance to the 8 neighbour planes / Vp.

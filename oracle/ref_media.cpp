@@ -1,6 +1,6 @@
 // ref_media.cpp -- C entry to the reference's own media discretisation code (src/media/, built
 // unmodified from the reference tree by oracle/Makefile.ref into oracle/_ref/libref_media.so).
-// TEST INFRASTRUCTURE: the checker of cgfd_media_layer_el_iso_gpu; nothing in the product
+// TEST INFRASTRUCTURE: the checker of cgfd_media_layer_el_iso_gpu and cgfd_media_layer_gpu; nothing in the product
 // links it.
 #include <cstddef>
 
@@ -11,4 +11,23 @@ extern "C" int ref_media_layer2model_el_iso(float *lam3d, float *mu3d, float *rh
                                             const char *in_3lay_file, const char *method) {
   // the curvilinear grid type, as main_curv_col_el_3d.cu:307-313 passes it; rank 1 prints nothing
   return media_layer2model_el_iso(lam3d, mu3d, rho3d, x3d, y3d, z3d, nx, ny, nz, GRID_CURV, in_3lay_file, method, 1);
+}
+
+// media_layer2model_el_vti (media_layer2model.cpp:173-228): rho, c11, c33, c55, c66, c13
+extern "C" int ref_media_layer2model_el_vti(float *rho, float *c11, float *c33, float *c55, float *c66, float *c13,
+                                            const float *x3d, const float *y3d, const float *z3d, size_t nx,
+                                            size_t ny, size_t nz, const char *in_3lay_file, const char *method) {
+  return media_layer2model_el_vti(rho, c11, c33, c55, c66, c13, x3d, y3d, z3d, nx, ny, nz, GRID_CURV, in_3lay_file,
+                                  method, 1);
+}
+
+// media_layer2model_el_aniso (media_layer2model.cpp:230-398): out[0] rho, out[1..21] c11 c12 c13 c14 c15 c16
+// c22 c23 c24 c25 c26 c33 c34 c35 c36 c44 c45 c46 c55 c56 c66
+extern "C" int ref_media_layer2model_el_aniso(float *const *out, const float *x3d, const float *y3d, const float *z3d,
+                                              size_t nx, size_t ny, size_t nz, const char *in_3lay_file,
+                                              const char *method) {
+  return media_layer2model_el_aniso(out[0], out[1], out[2], out[3], out[4], out[5], out[6], out[7], out[8], out[9],
+                                    out[10], out[11], out[12], out[13], out[14], out[15], out[16], out[17], out[18],
+                                    out[19], out[20], out[21], x3d, y3d, z3d, nx, ny, nz, GRID_CURV, in_3lay_file,
+                                    method, 1);
 }
