@@ -203,6 +203,30 @@ def media_layer_gpu(coord, model, method=CGFD_MEDIA_LOC, device=0):
     return out
 
 
+class LayerMediaDesc(C.Structure):
+    """cgfd_layer_media: a layer file of any elastic type."""
+    _fields_ = [("type", C.c_int), ("num_interfaces", C.c_int), ("nx", C.c_int), ("ny", C.c_int),
+                ("x0", C.c_float), ("y0", C.c_float), ("dx", C.c_float), ("dy", C.c_float),
+                ("elevation", C.c_void_p), ("param", C.c_void_p)]
+
+
+def media_layer_any_gpu(coord, model, medium_type, method=CGFD_MEDIA_LOC, device=0):
+    """cgfd_media_layer_gpu: the medium of medium_type (CGFD_MEDIUM_ELASTIC_*: [3 | 6 | 22, nz, ny,
+    nx] in the problem description's order) from the layer file model (formats.LayerMedia) on the
+    grid coord [3, nz, ny, nx]."""
+    _, nz, ny, nx = coord.shape
+    el = np.ascontiguousarray(model.elevation, np.float32)
+    pa = np.ascontiguousarray(model.param, np.float32)
+    d = LayerMediaDesc(int(model.type), int(el.shape[0]), int(model.nx), int(model.ny), float(model.x0),
+                       float(model.y0), float(model.dx), float(model.dy), el.ctypes.data, pa.ctypes.data)
+    c = np.ascontiguousarray(coord, np.float32)
+    nf = {2: 3, 3: 6, 4: 22}[int(medium_type)]
+    out = np.zeros((nf, nz, ny, nx), np.float32)
+    check(lib().cgfd_media_layer_gpu(int(device), nx - 6, ny - 6, nz - 6, c.ctypes.data, C.byref(d), int(medium_type),
+                                     int(method), out.ctypes.data))
+    return out
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("device", C.c_int), ("hbm_budget", C.c_size_t), ("max_active", C.c_int), ("max_batch", C.c_int),
                 ("steps_per_slice", C.c_int)]
@@ -310,6 +334,7 @@ def lib():
         "cgfd_metric_calc": (C.c_int, [C.c_int, C.c_int, C.c_int, P, P]),
         "cgfd_metric_calc_gpu": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, P]),
         "cgfd_media_layer_el_iso_gpu": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, P, C.c_int, P]),
+        "cgfd_media_layer_gpu": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, P, C.c_int, C.c_int, P]),
         "cgfd_dt_estimate": (C.c_int, [C.POINTER(ProblemDesc), C.c_double, C.POINTER(C.c_double)]),
         "cgfd_keep_three_digits": (C.c_double, [C.c_double]),
         "cgfd_problem_bytes": (C.c_int, [C.POINTER(ProblemDesc), C.c_int, P, C.POINTER(C.c_size_t),

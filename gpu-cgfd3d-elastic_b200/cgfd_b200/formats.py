@@ -241,3 +241,48 @@ def write_layer_file(path, m: LayerModel):
         cols = np.stack([getattr(m, n) for n in LayerModel.FIELDS], axis=-1).reshape(-1, len(LayerModel.FIELDS))
         for row in cols:
             f.write(" ".join(f"{v:.9g}" for v in row) + "\n")
+
+
+# Layer file types (the reference's media type numbers) and their parameters in file order
+LAYER_TYPES = {
+    21: ("elastic_isotropic", ("rho", "vp", "vs")),
+    22: ("elastic_vti_prem", ("rho", "vph", "vpv", "vsh", "vsv", "eta")),
+    23: ("elastic_vti_thomsen", ("rho", "vp0", "vs0", "epsilon", "delta", "gamma")),
+    24: ("elastic_vti_cij", ("rho", "c11", "c33", "c55", "c66", "c13")),
+    25: ("elastic_tti_thomsen", ("rho", "vp0", "vs0", "epsilon", "delta", "gamma", "azimuth", "dip")),
+    26: ("elastic_tti_bond", ("rho", "c11", "c33", "c55", "c66", "c13", "azimuth", "dip")),
+    27: ("elastic_aniso_cij", ("rho", "c11", "c12", "c13", "c14", "c15", "c16", "c22", "c23", "c24", "c25", "c26",
+                               "c33", "c34", "c35", "c36", "c44", "c45", "c46", "c55", "c56", "c66")),
+}
+
+
+class LayerMedia:
+    """A layer file of any elastic type (read_interface_file, src/media/media_read_file.cpp:22-700):
+    interfaces top first on a uniform nx x ny mesh; `elevation` [num_interfaces, ny, nx] and
+    `param` [npar, 3, num_interfaces, ny, nx]: value, gradient and power of each parameter of
+    LAYER_TYPES[type], in the file's order, for the layer below each interface."""
+
+    def __init__(self, type, x0, y0, dx, dy, elevation, param):
+        self.type = int(type)
+        self.x0, self.y0, self.dx, self.dy = float(x0), float(y0), float(dx), float(dy)
+        self.elevation = np.ascontiguousarray(elevation, np.float32)
+        self.param = np.ascontiguousarray(param, np.float32)
+        self.ny, self.nx = self.elevation.shape[1:]
+        assert self.param.shape == (len(LAYER_TYPES[self.type][1]), 3) + self.elevation.shape
+
+
+def write_layer_media_file(path, m: LayerMedia):
+    """The interface file of m in the reference's format: the type name, number of interfaces,
+    "NX NY MINX MINY DX DY", then per interface and mesh point (x fastest) the elevation and
+    value, gradient, power of every parameter (values written so that they read back exactly)."""
+    ni = m.elevation.shape[0]
+    name = LAYER_TYPES[m.type][0]
+    with open(path, "w") as f:
+        f.write(f"# layered {name} model\n{name}\n")
+        f.write(f"{ni}\n{m.nx} {m.ny} {m.x0:.9g} {m.y0:.9g} {m.dx:.9g} {m.dy:.9g}\n")
+        cols = [m.elevation.reshape(-1)]
+        for q in range(m.param.shape[0]):
+            for c in range(3):
+                cols.append(m.param[q, c].reshape(-1))
+        for row in np.stack(cols, axis=-1):
+            f.write(" ".join(f"{v:.9g}" for v in row) + "\n")

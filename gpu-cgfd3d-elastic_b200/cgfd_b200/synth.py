@@ -162,6 +162,57 @@ def layer_model(coord, seed=5, layers=LAYERS_3, depths=(-1500.0, -3500.0), relie
     return LayerModel(x0, y0, dx, dy, **f)
 
 
+def layer_media(coord, type, seed=5, depths=(-1500.0, -3500.0), relief=150.0, grad=True):
+    """A layer file of media type `type` (formats.LAYER_TYPES) over the grid's horizontal extent,
+    with the interfaces of layer_model (a free top interface, undulating interfaces around the
+    given depths) and seeded per-layer parameters: speeds of LAYERS_3 with Thomsen epsilon in
+    [0, 0.2], delta in [-0.1, 0.1], gamma in [0, 0.15], PREM-style vph / vsh a few percent above
+    vpv / vsv and eta near 1, stiffnesses from those (Cij files), and with `grad` a small depth
+    gradient (power 1) on the speeds and the stiffnesses. The tilt (azimuth in [0, 360), dip in
+    [10, 60] degrees) and the extra terms of the 21-Cij file are the same in every layer, so
+    that no c_ij changes sign across an interface (the harmonic average of a c_ij that does is
+    ill-conditioned)."""
+    from .formats import LayerMedia, LAYER_TYPES
+    base = layer_model(coord, seed=seed, depths=depths, relief=relief, grad=False)
+    rng = np.random.default_rng(seed + 100)
+    ni, ny, nx = base.elevation.shape
+    names = LAYER_TYPES[type][1]
+    az, dip = rng.uniform(0.0, 360.0), rng.uniform(10.0, 60.0)
+    E0 = rng.normal(0.0, 0.02, (6, 6))
+    E0 = (E0 + E0.T) / 2
+    per = []  # per layer: parameter values
+    for n in range(ni):
+        vp, vs, rho = LAYERS_3[min(n, len(LAYERS_3) - 1)]
+        eps, dlt, gam = rng.uniform(0.0, 0.2), rng.uniform(-0.1, 0.1), rng.uniform(0.0, 0.15)
+        c33, c55 = rho * vp * vp, rho * vs * vs
+        c11, c66 = c33 * (1 + 2 * eps), c55 * (1 + 2 * gam)
+        c13 = np.sqrt(2 * dlt * c33 * (c33 - c55) + (c33 - c55) ** 2) - c55
+        v = {"rho": rho, "vp": vp, "vs": vs, "vph": vp * 1.03, "vpv": vp, "vsh": vs * 1.04, "vsv": vs,
+             "eta": rng.uniform(0.9, 1.0), "vp0": vp, "vs0": vs, "epsilon": eps, "delta": dlt, "gamma": gam,
+             "azimuth": az, "dip": dip, "c11": c11, "c33": c33, "c55": c55, "c66": c66, "c13": c13}
+        if type == 27:  # a rotated TI tensor with small extra terms
+            C = np.zeros((6, 6))
+            C[0, 0] = C[1, 1] = c11
+            C[2, 2] = c33
+            C[0, 1] = C[1, 0] = c11 - 2 * c66
+            C[0, 2] = C[2, 0] = C[1, 2] = C[2, 1] = c13
+            C[3, 3] = C[4, 4] = c55
+            C[5, 5] = c66
+            C = C + E0 * c55
+            for a in range(6):
+                for b in range(a, 6):
+                    v["c%d%d" % (a + 1, b + 1)] = C[a, b]
+        per.append(v)
+    param = np.zeros((len(names), 3, ni, ny, nx), np.float32)
+    for q, nm in enumerate(names):
+        for n in range(ni):
+            param[q, 0, n] = per[n][nm]
+            speed_or_stiff = nm.startswith("v") or nm.startswith("c")
+            param[q, 1, n] = (0.05 if nm.startswith("v") else 5e3) if (grad and speed_or_stiff) else 0.0
+            param[q, 2, n] = 1.0
+    return LayerMedia(type, base.x0, base.y0, base.dx, base.dy, base.elevation, param)
+
+
 def thomsen_vti(coord, seed=2, layers=LAYERS_3, interfaces=INTERFACES_3):
     """VTI medium [6, ...] (rho, c11, c13, c33, c55, c66) from layered Thomsen parameters
     eps in [0, 0.2], delta in [-0.1, 0.1], gamma in [0, 0.15] (seeded per layer)."""

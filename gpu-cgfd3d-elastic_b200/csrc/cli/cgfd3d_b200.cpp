@@ -381,18 +381,17 @@ int run(int argc, char **argv) {
   std::vector<float> medium(mnames.size() * g.siz, 0.f);
   if (way == "import") {
     import_vars(need(md, "import").as_str() + "/media_" + kFnamePart + ".nc", g, mnames, medium.data());
-  } else if (way == "infile_layer" && d.medium_type == CGFD_MEDIUM_ELASTIC_ISO) {
-    // layered model discretised on the GPU (media_layer2model_el_iso, main_curv_col_el_3d.cu:301-313)
+  } else if (way == "infile_layer") {
+    // layer model discretised on the GPU (media_layer2model_el_iso / _el_vti / _el_aniso,
+    // main_curv_col_el_3d.cu:301-336), into the medium order of the medium type
     cgfd::fmt::LayerFile lf = cgfd::fmt::read_layer_file(need(md, "infile_layer").as_str());
     const std::string em = md.get("equivalent_medium_method") ? md.get("equivalent_medium_method")->as_str() : "loc";
     const int method = em == "loc" ? CGFD_MEDIA_LOC : em == "har" ? CGFD_MEDIA_HAR : em == "ari" ? CGFD_MEDIA_ARI : -1;
     if (method < 0) fail("equivalent_medium_method '" + em + "' must be loc, har or ari");
-    std::vector<float> rlm(3 * g.siz);
-    if (cgfd_media_layer_el_iso_gpu(gpu, g.ni, g.nj, g.nk, coord.data(), &lf.desc(), method, rlm.data()))
+    if (cgfd_media_layer_gpu(gpu, g.ni, g.nj, g.nk, coord.data(), &lf.media(), d.medium_type, method, medium.data()))
       fail(std::string("media on the GPU: ") + cgfd_last_error());
-    medium = rlm;  // rho, lambda, mu: the medium order of elastic_iso
   } else {
-    fail("medium input_way '" + way + "' is not on this path (import media_*.nc, or infile_layer for elastic_iso)");
+    fail("medium input_way '" + way + "' is not on this path (import media_*.nc, or infile_layer)");
   }
 
   d.ni = g.ni; d.nj = g.nj; d.nk = g.nk;

@@ -157,26 +157,46 @@ LayerFile read_layer_file(const std::string &path) {
   LayerFile L;
   std::string type;
   if (!(body >> type)) throw std::runtime_error(path + ": no media type");
-  if (type != "elastic_isotropic")
-    throw std::runtime_error(path + ": media type '" + type + "' is not on this path (elastic_isotropic)");
+  static const struct { const char *name; int type, npar; } kTypes[] = {
+      {"elastic_isotropic", CGFD_LAYER_ELASTIC_ISO, 3},  {"elastic_vti_prem", CGFD_LAYER_VTI_PREM, 6},
+      {"elastic_vti_thomsen", CGFD_LAYER_VTI_THOMSEN, 6}, {"elastic_vti_cij", CGFD_LAYER_VTI_CIJ, 6},
+      {"elastic_tti_thomsen", CGFD_LAYER_TTI_THOMSEN, 8}, {"elastic_tti_bond", CGFD_LAYER_TTI_BOND, 8},
+      {"elastic_aniso_cij", CGFD_LAYER_ANISO_CIJ, 22}};
+  for (const auto &t : kTypes)
+    if (type == t.name) { L.type = t.type; L.npar = t.npar; }
+  if (!L.type)
+    throw std::runtime_error(path + ": media type '" + type + "' is not on this path (the elastic types)");
   if (!(body >> L.ni) || L.ni < 1) throw std::runtime_error(path + ": number of interfaces missing or < 1");
   if (!(body >> L.nx >> L.ny >> L.x0 >> L.y0 >> L.dx >> L.dy) || L.nx < 2 || L.ny < 2)
     throw std::runtime_error(path + ": interface mesh line must be NX NY MINX MINY DX DY with NX, NY >= 2");
   const size_t n = (size_t)L.ni * L.nx * L.ny;
-  for (auto &v : L.f) v.resize(n);
-  for (size_t p = 0; p < n; p++)
-    for (int q = 0; q < 10; q++)
-      if (!(body >> L.f[q][p])) throw std::runtime_error(path + ": insufficient data");
+  L.elevation.resize(n);
+  L.param.resize((size_t)L.npar * 3 * n);
+  for (size_t p = 0; p < n; p++) {
+    if (!(body >> L.elevation[p])) throw std::runtime_error(path + ": insufficient data");
+    for (int q = 0; q < 3 * L.npar; q++)
+      if (!(body >> L.param[(size_t)q * n + p])) throw std::runtime_error(path + ": insufficient data");
+  }
   return L;
 }
 
 const cgfd_layer_model &LayerFile::desc() {
+  const size_t n = (size_t)ni * nx * ny;
   d.num_interfaces = ni; d.nx = nx; d.ny = ny;
   d.x0 = x0; d.y0 = y0; d.dx = dx; d.dy = dy;
-  const float **dst[10] = {&d.elevation, &d.rho, &d.rho_grad, &d.rho_pow, &d.vp, &d.vp_grad, &d.vp_pow,
-                           &d.vs, &d.vs_grad, &d.vs_pow};
-  for (int q = 0; q < 10; q++) *dst[q] = f[q].data();
+  d.elevation = elevation.data();
+  const float **dst[9] = {&d.rho, &d.rho_grad, &d.rho_pow, &d.vp, &d.vp_grad, &d.vp_pow, &d.vs, &d.vs_grad, &d.vs_pow};
+  for (int q = 0; q < 9 && q < 3 * npar; q++) *dst[q] = param.data() + (size_t)q * n;
   return d;
+}
+
+const cgfd_layer_media &LayerFile::media() {
+  m.type = type;
+  m.num_interfaces = ni; m.nx = nx; m.ny = ny;
+  m.x0 = x0; m.y0 = y0; m.dx = dx; m.dy = dy;
+  m.elevation = elevation.data();
+  m.param = param.data();
+  return m;
 }
 
 void write_sac(const std::string &path, const float *data, int npts, float delta, float stla, float stlo, float stel,

@@ -30,16 +30,23 @@ struct StationFile {
 };
 StationFile read_station_file(const std::string &path);
 
-// Layered elastic-isotropic model file (read_interface_file, src/media/media_read_file.cpp:22-210;
-// lines starting with '#' and empty lines skipped, then whitespace-separated tokens): media type
-// elastic_isotropic, number of interfaces, "NX NY MINX MINY DX DY", then per interface and mesh
-// point the elevation and value / gradient / power of rho, vp, vs. desc() points into the arrays.
+// Layer model file of any elastic media type (read_interface_file,
+// src/media/media_read_file.cpp:22-700; lines starting with '#' and empty lines skipped, then
+// whitespace-separated tokens): the media type name (elastic_isotropic, elastic_vti_prem,
+// elastic_vti_thomsen, elastic_vti_cij, elastic_tti_thomsen, elastic_tti_bond,
+// elastic_aniso_cij), number of interfaces, "NX NY MINX MINY DX DY", then per interface and
+// mesh point the elevation and value / gradient / power of every parameter of the type.
+// media() (every type) and desc() (elastic_isotropic) point into the arrays.
 struct LayerFile {
-  int ni = 0, nx = 0, ny = 0;
+  int type = 0;  // CGFD_LAYER_*
+  int ni = 0, nx = 0, ny = 0, npar = 0;
   float x0 = 0, y0 = 0, dx = 0, dy = 0;
-  std::vector<float> f[10];  // elevation, rho, rho_grad, rho_pow, vp, vp_grad, vp_pow, vs, vs_grad, vs_pow
+  std::vector<float> elevation;  // [ni][ny][nx]
+  std::vector<float> param;      // [npar][3][ni][ny][nx]
   cgfd_layer_model d{};
+  cgfd_layer_media m{};
   const cgfd_layer_model &desc();
+  const cgfd_layer_media &media();
 };
 LayerFile read_layer_file(const std::string &path);
 

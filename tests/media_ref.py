@@ -33,3 +33,42 @@ def layer2model_el_iso(coord, model, method=0):
                 c[2].ctypes.data, nx, ny, nz, path.encode(), METHODS[method])
     assert rc == 0
     return np.stack([rho, lam, mu])
+
+
+def layer2model(coord, model, medium_type, method=0):
+    """The medium of medium_type (2 iso [rho lambda mu], 3 VTI [rho c11 c13 c33 c55 c66], 4 21-Cij
+    [rho c11 ... c66]) from the layer file model (formats.LayerMedia) by the reference's
+    media_layer2model_el_iso / _el_vti / _el_aniso on the grid coord."""
+    L = C.CDLL(LIB)
+    _, nz, ny, nx = coord.shape
+    c = np.ascontiguousarray(coord, np.float32)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "model.lay")
+        formats.write_layer_media_file(path, model)
+        if medium_type == 2:
+            fn = L.ref_media_layer2model_el_iso
+            fn.restype = C.c_int
+            fn.argtypes = [C.c_void_p] * 6 + [C.c_size_t] * 3 + [C.c_char_p, C.c_char_p]
+            lam, mu, rho = (np.zeros((nz, ny, nx), np.float32) for _ in range(3))
+            rc = fn(lam.ctypes.data, mu.ctypes.data, rho.ctypes.data, c[0].ctypes.data, c[1].ctypes.data,
+                    c[2].ctypes.data, nx, ny, nz, path.encode(), METHODS[method])
+            out = np.stack([rho, lam, mu])
+        elif medium_type == 3:
+            fn = L.ref_media_layer2model_el_vti
+            fn.restype = C.c_int
+            fn.argtypes = [C.c_void_p] * 9 + [C.c_size_t] * 3 + [C.c_char_p, C.c_char_p]
+            f = [np.zeros((nz, ny, nx), np.float32) for _ in range(6)]  # rho c11 c33 c55 c66 c13
+            rc = fn(*[a.ctypes.data for a in f], c[0].ctypes.data, c[1].ctypes.data, c[2].ctypes.data, nx, ny, nz,
+                    path.encode(), METHODS[method])
+            out = np.stack([f[0], f[1], f[5], f[2], f[3], f[4]])
+        else:
+            fn = L.ref_media_layer2model_el_aniso
+            fn.restype = C.c_int
+            fn.argtypes = [C.c_void_p] * 4 + [C.c_size_t] * 3 + [C.c_char_p, C.c_char_p]
+            f = [np.zeros((nz, ny, nx), np.float32) for _ in range(22)]
+            ptrs = (C.c_void_p * 22)(*[a.ctypes.data for a in f])
+            rc = fn(ptrs, c[0].ctypes.data, c[1].ctypes.data, c[2].ctypes.data, nx, ny, nz, path.encode(),
+                    METHODS[method])
+            out = np.stack(f)
+    assert rc == 0
+    return out

@@ -1,5 +1,6 @@
-"""Media discretisation on the GPU (cgfd_media_layer_el_iso_gpu) against the reference's own
-host code (media_layer2model_el_iso from the reference's src/media, oracle/_ref/libref_media.so)
+"""Media discretisation on the GPU (cgfd_media_layer_el_iso_gpu, cgfd_media_layer_gpu) against the
+reference's own host code (media_layer2model_el_iso / _el_vti / _el_aniso from the reference's
+src/media, oracle/_ref/libref_media.so)
 on the same curvilinear grid and layered model with undulating interfaces and depth gradients,
 for the three methods (loc, har, ari). Bar: every value equal to the reference's within 1e-6
 relative (both evaluate the same float / double expressions in the same order; the one
@@ -34,4 +35,52 @@ def test_gpu_media_rejects_points_outside_the_mesh():
     model.x0 += 500.0  # the mesh no longer covers the grid's first columns
     with pytest.raises(CgfdError) as e:
         media_layer_gpu(coord, model, 0)
+    assert e.value.code == -1
+
+
+# (layer file type, target medium type): VTI files into VTI media, every file type into 21-Cij
+CASES = [(22, 3), (23, 3), (24, 3), (21, 4), (23, 4), (25, 4), (26, 4), (27, 4)]
+
+
+@pytest.mark.parametrize("method", [0, 1, 2])
+@pytest.mark.parametrize("ftype,medium", CASES)
+def test_gpu_layer_media_matches_reference(ftype, medium, method):
+    """cgfd_media_layer_gpu against the reference's media_layer2model_el_vti / _el_aniso on the
+    same grid and layer file: every field within 1e-6 of its largest magnitude, and at least 99%
+    of the values bitwise equal, for the files without a rotation. The Bond-rotated TTI files
+    take their sines and cosines from another math library (last-ulp differences): 2e-5, and
+    under the harmonic average the c_ij whose values change sign from layer to layer (c14, c36,
+    c45 of this model) are left out: their harmonic mean divides by sums near zero, where the
+    reference's own value is arbitrary in the last digits (it reaches 100-4000 times the c_ij's
+    largest layer value)."""
+    from cgfd_b200 import media_layer_any_gpu
+    coord = synth.curvilinear_grid(40, 36, 32, 100.0, seed=7)
+    model = synth.layer_media(coord, ftype, seed=9)
+    ref = media_ref.layer2model(coord, model, medium, method)
+    got = media_layer_any_gpu(coord, model, medium, method)
+    assert got.shape == ref.shape and np.isfinite(ref).all() and (ref[0] > 0).all()
+    rotated = ftype in (25, 26)
+    tol = 2e-5 if rotated else 1e-6
+    loc = media_ref.layer2model(coord, model, medium, 0) if method else ref
+    for f in range(ref.shape[0]):
+        if rotated and method == 1 and (loc[f] > 0).any() and (loc[f] < 0).any():
+            assert np.isfinite(got[f]).all()
+            continue
+        scale = float(np.abs(ref[f]).max())
+        if scale == 0.0:
+            assert not got[f].any(), f
+            continue
+        err = float(np.abs(got[f].astype(np.float64) - ref[f]).max())
+        assert err <= tol * scale, (f, err, scale)
+    if not rotated:
+        assert (got == ref).mean() >= 0.99
+    if method:
+        assert (ref != loc).any()
+
+
+def test_gpu_layer_media_rejects_wrong_file_type():
+    from cgfd_b200 import media_layer_any_gpu
+    coord = synth.curvilinear_grid(24, 24, 20, 100.0, seed=7)
+    with pytest.raises(CgfdError) as e:
+        media_layer_any_gpu(coord, synth.layer_media(coord, 25, seed=9), 3, 0)  # a TTI file into a VTI medium
     assert e.value.code == -1
