@@ -293,13 +293,17 @@ __global__ void k_media_avg(const __grid_constant__ LayerDev m, const __grid_con
 // para2tti (media_utility.cpp:620-831) turn them into the stiffness: 6 fields (rho c11 c33 c55
 // c66 c13) for the VTI files, 22 (rho c11 c12 ... c66) for the others. The har / ari
 // averages take c_ij harmonically / arithmetically over the 9^3 sub-points, rho arithmetically.
+// NEWDZ: on an interface, the layer above is evaluated at the point's depth below that layer's
+// own interface (PREM and Thomsen VTI files, media_layer2model.cpp:596, 669), or, kept alike
+// on purpose, at the depth below the point's own interface, as the reference does for the
+// VTI-Cij, TTI and 21-Cij files (:721-757, 805-850, 967-1082, 1129-1174 reuse dz).
 template <int T> struct LayerFile;
-template <> struct LayerFile<22> { static constexpr int NPAR = 6, NOUT = 6; };
-template <> struct LayerFile<23> { static constexpr int NPAR = 6, NOUT = 6; };
-template <> struct LayerFile<24> { static constexpr int NPAR = 6, NOUT = 6; };
-template <> struct LayerFile<25> { static constexpr int NPAR = 8, NOUT = 22; };
-template <> struct LayerFile<26> { static constexpr int NPAR = 8, NOUT = 22; };
-template <> struct LayerFile<27> { static constexpr int NPAR = 22, NOUT = 22; };
+template <> struct LayerFile<22> { static constexpr int NPAR = 6, NOUT = 6; static constexpr bool NEWDZ = true; };
+template <> struct LayerFile<23> { static constexpr int NPAR = 6, NOUT = 6; static constexpr bool NEWDZ = true; };
+template <> struct LayerFile<24> { static constexpr int NPAR = 6, NOUT = 6; static constexpr bool NEWDZ = false; };
+template <> struct LayerFile<25> { static constexpr int NPAR = 8, NOUT = 22; static constexpr bool NEWDZ = false; };
+template <> struct LayerFile<26> { static constexpr int NPAR = 8, NOUT = 22; static constexpr bool NEWDZ = false; };
+template <> struct LayerFile<27> { static constexpr int NPAR = 22, NOUT = 22; static constexpr bool NEWDZ = false; };
 
 // value + dz^pow * grad of parameter q of layer mi at (x, y)
 __device__ float layer_val_par(const LayerDev &m, int q, int mi, float x, float y, float dz) {
@@ -312,7 +316,7 @@ __device__ float layer_val_par(const LayerDev &m, int q, int mi, float x, float 
 }
 
 // AssignLayerMediaPara2Point + CalPointValue_layer for the general files; 1: outside the mesh
-template <int NPAR>
+template <int NPAR, bool NEWDZ>
 __device__ int point_params(const LayerDev &m, P3 a, float var[NPAR]) {
   const float maxx = __fadd_rn(m.x0, __fmul_rn(m.dx, (float)(m.nx - 1)));
   const float maxy = __fadd_rn(m.y0, __fmul_rn(m.dy, (float)(m.ny - 1)));
@@ -331,7 +335,7 @@ __device__ int point_params(const LayerDev &m, P3 a, float var[NPAR]) {
   if ((int)dz == 0) {  // on an interface (the reference's integer-abs test)
     const int mt = first_ge(a.z, e, m.ni_) - 1;
     if (mt >= 0) {
-      dz = __fsub_rn(e[mt], a.z);
+      if (NEWDZ) dz = __fsub_rn(e[mt], a.z);
       for (int q = 0; q < NPAR; q++) {
         const float top = layer_val_par(m, q, mt, a.x, a.y, dz);
         var[q] = (float)__ddiv_rn((double)__fadd_rn(var[q], top), 2.0);
@@ -460,7 +464,7 @@ __global__ void k_media_loc_gen(const __grid_constant__ LayerDev m, const __grid
   constexpr int NP = LayerFile<T>::NPAR, NO = LayerFile<T>::NOUT;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < out.n; t += (long long)gridDim.x * blockDim.x) {
     float var[NP], o[NO];
-    if (point_params<NP>(m, P3{g.x[t], g.y[t], g.z[t]}, var)) {
+    if (point_params<NP, LayerFile<T>::NEWDZ>(m, P3{g.x[t], g.y[t], g.z[t]}, var)) {
       atomicOr(out.err, 1);
       continue;
     }
@@ -507,7 +511,7 @@ __global__ void k_media_avg_gen(const __grid_constant__ LayerDev m, const __grid
           const P3 lx01 = lerp(M[4], M[5], ii), lx11 = lerp(M[7], M[6], ii);
           const P3 lxy0 = lerp(lx00, lx10, jj), lxy1 = lerp(lx01, lx11, jj);
           float var[NP], o[NO];
-          if (point_params<NP>(m, lerp(lxy0, lxy1, kk), var)) { bad = 1; continue; }
+          if (point_params<NP, LayerFile<T>::NEWDZ>(m, lerp(lxy0, lxy1, kk), var)) { bad = 1; continue; }
           para2out<T>(var, o);
           acc[0] = __fadd_rn(acc[0], o[0]);
           for (int q = 1; q < NO; q++)
