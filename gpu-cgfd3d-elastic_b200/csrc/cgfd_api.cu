@@ -1735,9 +1735,12 @@ int cgfd_autotune(cgfd_problem *p, int steps, int *chosen) {
     std::vector<int> zc;
     for (int c : {8, 10, 12, 14, 16, 20, 24, 32, 48, 64, 96, nbulk})
       if (c >= 1 && c <= nbulk && std::find(zc.begin(), zc.end(), c) == zc.end()) zc.push_back(c);
-    std::vector<std::pair<int, int>> cand;  // (tile shape, z chunk); the FP64 build has no TMA kernel
-    for (int sh = 0; sh < (p->use_tma ? 2 : 1); sh++)
-      for (int c : zc) cand.emplace_back(sh, c);
+    // (tile shape, z chunk), the shapes interleaved so that a clock drifting during the tuning
+    // (power cap, temperature) does not favour one of them; the FP64 build has no TMA kernel
+    std::vector<std::pair<int, int>> cand;
+    for (int c : zc)
+      for (int sh = 0; sh < (p->use_tma ? 2 : 1); sh++) cand.emplace_back(sh, c);
+    const std::pair<int, int> dflt(p->shape, p->nzc);
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -1767,7 +1770,9 @@ int cgfd_autotune(cgfd_problem *p, int steps, int *chosen) {
       p->nzc = sc.second;
       make_tiles(p);
     };
-    // every candidate once, then the three fastest again over three times the steps (close
+    // every candidate once; then the three fastest and the default tiling again, twice each
+    // over twice the steps in a palindromic order (a b c d d c b a: a clock drifting linearly
+    // during the tuning adds the same to every finalist), keeping the lowest mean (close
     // candidates differ by less than a short run's spread)
     std::vector<std::pair<float, std::pair<int, int>>> timed;
     for (const auto &sc : cand) {
@@ -1776,14 +1781,21 @@ int cgfd_autotune(cgfd_problem *p, int steps, int *chosen) {
     }
     std::stable_sort(timed.begin(), timed.end(),
                      [](const auto &a, const auto &b) { return a.first < b.first; });
+    std::vector<std::pair<int, int>> fin;
+    for (size_t r = 0; r < std::min<size_t>(3, timed.size()); r++) fin.push_back(timed[r].second);
+    if (std::find(fin.begin(), fin.end(), dflt) == fin.end()) fin.push_back(dflt);
+    std::vector<float> sum(fin.size(), 0.f);
     const int steps1 = steps;
-    steps = 3 * steps1;
-    for (size_t r = 0; r < std::min<size_t>(3, timed.size()); r++) {
-      use(timed[r].second);
-      const float ms = time_choice();
-      if (ms < best_ms) { best_ms = ms; best = timed[r].second.second; best_shape = timed[r].second.first; }
-    }
+    steps = 2 * steps1;
+    for (int pass = 0; pass < 2; pass++)
+      for (size_t r = 0; r < fin.size(); r++) {
+        const size_t q = pass ? fin.size() - 1 - r : r;
+        use(fin[q]);
+        sum[q] += time_choice();
+      }
     steps = steps1;
+    for (size_t q = 0; q < fin.size(); q++)
+      if (sum[q] < best_ms) { best_ms = sum[q]; best = fin[q].second; best_shape = fin[q].first; }
     CK(cudaStreamSynchronize(p->stream));
     if (p->use_tma && best_shape != p->shape) {
       p->shape = best_shape;

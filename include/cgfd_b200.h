@@ -352,8 +352,9 @@ int cgfd_get_shot_group(const cgfd_problem *p);
 /*
  * Autotuner of the bulk kernel's tile: times `steps` graph-replayed time steps for each tile
  * shape (cgfd_set_tile_shape) and z-chunk length (planes per thread block column: 8, 10, 12,
- * 14, 16, 20, 24, 32, 48, 64, 96 and all bulk planes) on this problem, times the three fastest
- * again over 3 x `steps` steps and keeps the fastest pair (*chosen:
+ * 14, 16, 20, 24, 32, 48, 64, 96 and all bulk planes; the shapes interleaved) on this problem,
+ * times the three fastest and the default tiling twice more over 2 x `steps` steps in a
+ * palindromic order and keeps the pair of lowest mean (*chosen:
  * the z chunk; cgfd_get_tile_shape: the shape) and returns the problem to its freshly created
  * state (zero wavefield, step 0). For a batch it then times the shot groups 4, 8, 16 and every
  * shot at the chosen pair and keeps the fastest (cgfd_get_shot_group). Only on a problem that

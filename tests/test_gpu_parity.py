@@ -161,8 +161,10 @@ def test_autotune_picks_a_chunk_and_resets_state():
     equals a run of a fresh problem (bitwise when the default shape won)."""
     p = small_problem("iso", nsteps=30)
     a = Simulation(p)
-    c = a.autotune(2)  # both tile shapes x the z-chunk candidates
-    assert c in (8, 10, 12, 14, 16, 20, 24, 32, 48, 64, 96, p.nk - 4) and a.zchunk == c and a.step == 0
+    default_chunk = a.zchunk
+    c = a.autotune(2)  # both tile shapes x the z-chunk candidates, and the default tiling
+    assert c in (8, 10, 12, 14, 16, 20, 24, 32, 48, 64, 96, p.nk - 4, default_chunk)
+    assert a.zchunk == c and a.step == 0
     assert a.tile_shape in (0, 1)
     a.run()
     b = Simulation(p)
