@@ -11,6 +11,7 @@ from typing import Optional
 
 import numpy as np
 
+CGFD_MEDIUM_ACOUSTIC_ISO = 1
 CGFD_MEDIUM_ELASTIC_ISO = 2
 CGFD_MEDIUM_ELASTIC_VTI = 3
 CGFD_MEDIUM_ELASTIC_ANISO = 4
@@ -62,7 +63,8 @@ class ProblemDesc(C.Structure):
 
 
 def medium_ncmp(medium_type):
-    return {CGFD_MEDIUM_ELASTIC_ISO: 3, CGFD_MEDIUM_ELASTIC_VTI: 6, CGFD_MEDIUM_ELASTIC_ANISO: 22}[medium_type]
+    return {CGFD_MEDIUM_ACOUSTIC_ISO: 2, CGFD_MEDIUM_ELASTIC_ISO: 3, CGFD_MEDIUM_ELASTIC_VTI: 6,
+            CGFD_MEDIUM_ELASTIC_ANISO: 22}[medium_type]
 
 
 def ref_shape(ni, nj, nk):

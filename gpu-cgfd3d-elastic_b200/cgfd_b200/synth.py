@@ -9,7 +9,7 @@ import ctypes as C
 
 import numpy as np
 
-from .abi import (CGFD_MEDIUM_ELASTIC_ISO, CGFD_MEDIUM_ELASTIC_VTI, CGFD_MEDIUM_ELASTIC_ANISO, WAVELETS,
+from .abi import (CGFD_MEDIUM_ACOUSTIC_ISO, CGFD_MEDIUM_ELASTIC_ISO, CGFD_MEDIUM_ELASTIC_VTI, CGFD_MEDIUM_ELASTIC_ANISO, WAVELETS,
                   Problem, Sources, Stations, lib, ref_shape, ProblemDesc)
 
 LAYERS_3 = [(4000.0, 2300.0, 2500.0), (5500.0, 3200.0, 2700.0), (6500.0, 3750.0, 2900.0)]
@@ -130,6 +130,16 @@ def layered_iso(coord, layers=LAYERS_3, interfaces=INTERFACES_3, perturb=None):
     med[0] = rho
     med[1] = rho * (vp * vp - 2.0 * vs * vs)
     med[2] = rho * vs * vs
+    return med
+
+
+def layered_ac(coord, layers=LAYERS_3, interfaces=INTERFACES_3):
+    """Acoustic iso medium [2, nz, ny, nx] (rho, kappa = rho vp^2) from the flat layers of
+    layered_iso (their vp and rho)."""
+    iso = layered_iso(coord, layers, interfaces)
+    med = np.zeros((2,) + iso.shape[1:], np.float32)
+    med[0] = iso[0]
+    med[1] = iso[1] + 2.0 * iso[2]  # lambda + 2 mu = rho vp^2
     return med
 
 
@@ -330,6 +340,33 @@ def dc_sources(coord, ni, nj, n, rng, depth_range=(2000.0, 2000.0), fc_range=(2.
                    cmp_type=2, mechanism_type=1, loc_coord_type=0, loc_3dim=1)
 
 
+def ac_sources(coord, ni, nj, n, rng, depth_range=(2000.0, 2000.0), fc_range=(2.0, 2.0), m0=1e16, center=False,
+               stf_length=None, dt=None):
+    """Sources of acoustic problems: a pressure term (moment components given directly, Mxx
+    drives P; the others are set too and must stay without effect) and a random force
+    (cmp_type 3), located by grid index with the depth flag, Ricker source time functions."""
+    loc = np.zeros((n, 3), np.float32)
+    cmp = np.zeros((n, 9), np.float32)
+    coefs = np.zeros((n, 10), np.float32)
+    tstart = np.zeros(n, np.float32)
+    for s in range(n):
+        if center:
+            i, j = ni // 2, nj // 2
+        else:
+            i = int(rng.integers(ni // 4, 3 * ni // 4))
+            j = int(rng.integers(nj // 4, 3 * nj // 4))
+        dep = rng.uniform(*depth_range)
+        loc[s] = (i, j, column_depth_index(coord, i, j, dep))
+        f = rng.normal(size=3)
+        cmp[s, 0:3] = (m0 * 1e-3) * f / np.linalg.norm(f)
+        cmp[s, 3:9] = m0 * np.array([1.0, 0.7, 0.4, 0.3, -0.2, 0.1])
+        fc = rng.uniform(*fc_range)
+        coefs[s, 0], coefs[s, 1] = fc, 1.2 / fc
+    return Sources(loc=loc, t_start=tstart, wavelet=np.full(n, WAVELETS["ricker"], np.int32),
+                   wavelet_coefs=coefs, cmp=cmp, stf_given=0, stf_length=float(stf_length),
+                   cmp_type=3, mechanism_type=0, loc_coord_type=0, loc_3dim=1)
+
+
 def surface_stations(ni, nj, nx_sta, ny_sta, margin=0.15):
     """nx_sta*ny_sta stations on the surface (1-based grid index, depth flag, z = 0)."""
     xs = np.round(np.linspace(margin * (ni - 1), (1 - margin) * (ni - 1), nx_sta)) + 1
@@ -363,7 +400,8 @@ def make_problem(ni, nj, nk, dh, nsteps, dt=None, medium="iso", npml=12, nsrc=1,
     """Build a seeded Problem of the benchmark family.
 
     medium: "iso" (3 flat layers, optional von Karman perturbation), "vti" (layered Thomsen),
-    "aniso" (Bond-rotated tilted TI). dt=None -> keep_three_digits(0.9 * dtmax).
+    "aniso" (Bond-rotated tilted TI), "ac" (acoustic, the iso layers' vp and rho; sources with
+    a force and an Mxx pressure term). dt=None -> keep_three_digits(0.9 * dtmax).
     """
     coord = curvilinear_grid(ni, nj, nk, dh, seed=seed)
     metric = metrics(coord) if metric_fn is None else metric_fn(coord)
@@ -382,6 +420,10 @@ def make_problem(ni, nj, nk, dh, nsteps, dt=None, medium="iso", npml=12, nsrc=1,
         med = tilted_aniso(coord, seed=seed + 3)
         mtype = CGFD_MEDIUM_ELASTIC_ANISO
         vmax = float(np.sqrt(np.maximum(np.maximum(med[1], med[7]), med[12]) / np.maximum(med[0], 1e-9))[3:-3, 3:-3, 3:-3].max())
+    elif medium == "ac":
+        med = layered_ac(coord)
+        mtype = CGFD_MEDIUM_ACOUSTIC_ISO
+        vmax = float(np.sqrt(med[1] / np.maximum(med[0], 1e-9))[3:-3, 3:-3, 3:-3].max())
     else:
         raise ValueError(medium)
     prob = Problem(ni=ni, nj=nj, nk=nk, medium_type=mtype, coord=coord, metric=metric, medium=med,
@@ -395,8 +437,9 @@ def make_problem(ni, nj, nk, dh, nsteps, dt=None, medium="iso", npml=12, nsrc=1,
     prob.dt = float(dt)
     rng = np.random.default_rng(seed + 7)
     if nsrc:
-        prob.src = dc_sources(coord, ni, nj, nsrc, rng, depth_range=src_depth, fc_range=(fc, fc) if np.isscalar(fc) else fc,
-                              center=center_src, stf_length=stf_length if stf_length else (nsteps + 1) * dt)
+        mk = ac_sources if medium == "ac" else dc_sources
+        prob.src = mk(coord, ni, nj, nsrc, rng, depth_range=src_depth, fc_range=(fc, fc) if np.isscalar(fc) else fc,
+                      center=center_src, stf_length=stf_length if stf_length else (nsteps + 1) * dt)
     if sta_grid:
         prob.sta = surface_stations(ni, nj, *sta_grid)
     return prob

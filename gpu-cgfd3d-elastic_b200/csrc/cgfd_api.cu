@@ -134,6 +134,7 @@ struct cgfd_problem {
   int device = 0;
   cudaStream_t stream = nullptr;
   int ni = 0, nj = 0, nk = 0, med = 0, ncoef = 0, nt_total = 0, free_top = 0;
+  int nbulk = 0;  // planes [0, nbulk) of the bulk kernel (elastic: below the surface slab; acoustic: all)
   int nshot = 1;  // wavefields sharing the grid, coefficients and stations
   int shot_group = 8;  // bulk kernel: shots per block group of a batch (cgfd_set_shot_group)
   // FP64 build (CGFD_PREC_FP64): every real-typed device array below holds doubles (esz 8)
@@ -294,7 +295,7 @@ struct cgfd_problem {
     p.jac = rptr<R>(jac); p.matx = rptr<R>(matx); p.maty = rptr<R>(maty);
     p.flux = rptr<R>(d_flux);
     p.free_top = free_top;
-    p.nbulk = free_top ? nk - cgfd::NSURF : nk;
+    p.nbulk = nbulk;
     p.err = d_flag;
     p.nshot = nshot;
     p.wsc = d_wsc;
@@ -383,7 +384,49 @@ struct cgfd_problem {
     return n;
   }
 
+  // One time step of an acoustic problem (drv_rk_curv_col.cu:193-541 with
+  // sv_curv_col_ac_iso_onestage): per stage the free-surface pressure image of the stage input,
+  // then the fused stage of every cell, then the sources; R float, or double in the FP64 build.
+  template <typename R>
+  int enqueue_step_ac(int step) {
+    cudaStream_t st = stream;
+    int n = 0;
+    if (rec.n > 0) {
+      cgfd::RecvPT<R> r;
+      r.nsta = rec.n; r.nshot = nshot; r.nt_total = nt_total; r.idx8 = d_idx8; r.w8 = d_w8;
+      r.pre = rptr<R>(wbuf[step & 1]); r.sf = sf; r.seis = d_seis; r.d_it = d_it; r.d_flag = d_flag;
+      n += timed(6, [&] { return cgfd::launch_recv(r, st); });
+    }
+    n += enqueue_outputs<R>(step);
+    for (int s = 0; s < 4; s++) {
+      const cgfd::StagePT<R> p = stage_params_t<R>(step, s);
+      n += timed(s, [&] { return cgfd::launch_ac_image(p, st) + cgfd::launch_stage_ac(p, nzc, st); });
+      if (src.nsrc > 0) {
+        cgfd::SrcPT<R> q;
+        memset(&q, 0, sizeof(q));
+        q.nsrc = src.nsrc; q.max_ext = src.max_ext; q.max_nt = src.max_nt;
+        q.force = src.force; q.moment = src.moment; q.stage = s;
+        q.ca = p.ca; q.cb = p.cb;
+        q.it_begin = d_it_begin; q.ext_num = d_ext_num; q.ext_idx = d_ext_idx;
+        q.ext_wv = d_ext_wv; q.ext_wt = d_ext_wt; q.stf = d_stf; q.src_shot = d_src_shot;
+        q.tmp_out = p.tmp_out; q.end = p.end; q.sf = sf; q.d_it = d_it;
+        n += timed(5, [&] { return cgfd::launch_source(q, st); });
+      }
+    }
+    if (free_top) {
+      cgfd::PgPT<R> q;
+      q.ni = ni; q.nj = nj; q.nshot = nshot; q.sx = sx; q.sf = sf;
+      q.off_top = off0 + (long long)(nk - 1) * sz;
+      q.w_end = rptr<R>(wbuf[(step + 1) & 1]); q.w_pre = rptr<R>(wbuf[step & 1]);
+      q.pg = d_pg; q.dis = rptr<R>(d_dis); q.dt = dt;
+      n += cgfd::launch_peak_motion(q, st);
+    }
+    n += cgfd::launch_advance(d_it, st);
+    return n;
+  }
+
   int enqueue_step(int step) {
+    if (med == cgfd::MED_AC) return fp64 ? enqueue_step_ac<double>(step) : enqueue_step_ac<float>(step);
     if (fp64) return enqueue_step64(step);
     cudaStream_t st = stream;
     int n = 0;
@@ -737,7 +780,8 @@ void problem_bytes(const cgfd_problem_desc *d, int nshot, const cgfd_source_desc
   if (nshot < 1 || nshot > 32767) throw cgfd::Error(CGFD_ERR_INVALID, "nshot must be in [1, 32767]");
   long long sx, sz, sf, off0;
   layout(d->ni, d->nj, d->nk, sx, sz, sf, off0);
-  const int ncoef = d->medium_type == CGFD_MEDIUM_ELASTIC_ISO ? 12 : (d->medium_type == CGFD_MEDIUM_ELASTIC_VTI ? 15 : 31);
+  const bool ac = d->medium_type == CGFD_MEDIUM_ACOUSTIC_ISO;
+  const int ncoef = ac ? 11 : (d->medium_type == CGFD_MEDIUM_ELASTIC_ISO ? 12 : (d->medium_type == CGFD_MEDIUM_ELASTIC_VTI ? 15 : 31));
   const bool f64 = d->precision == CGFD_PREC_FP64;
   const bool c16 = d->precision != CGFD_PREC_FP32 && !f64, w16 = d->precision == CGFD_PREC_FP16_WAVE;
   const size_t F = f64 ? sizeof(double) : sizeof(float);  // real-typed arrays
@@ -749,7 +793,7 @@ void problem_bytes(const cgfd_problem_desc *d, int nshot, const cgfd_source_desc
   // reference layout are held beside the staging buffer while the metric is repacked
   const size_t upload = stage_buf * (d->metric ? 1 : 14);
   const size_t high = waves + jac + coef32 + (c16 ? std::max(upload, coef16 + 8 * (size_t)ncoef) : upload);
-  if (d->free_top)
+  if (d->free_top && !ac)  // conversion matrices and traction-image fluxes (elastic media)
     r += (size_t)2 * 9 * d->ni * d->nj * F + (size_t)9 * cgfd::kFluxPlanes * (d->ni + 6) * (d->nj + 6) * nshot * F;
   cgfd::PmlFaceHost fh[3][2];
   cgfd::pml_setup(d, fh);
@@ -856,13 +900,16 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   CK(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
   p->ni = d->ni; p->nj = d->nj; p->nk = d->nk;
-  p->med = d->medium_type == CGFD_MEDIUM_ELASTIC_ISO ? cgfd::MED_ISO
+  p->med = d->medium_type == CGFD_MEDIUM_ACOUSTIC_ISO ? cgfd::MED_AC
+           : d->medium_type == CGFD_MEDIUM_ELASTIC_ISO ? cgfd::MED_ISO
            : (d->medium_type == CGFD_MEDIUM_ELASTIC_VTI ? cgfd::MED_VTI : cgfd::MED_ANISO);
-  p->ncoef = p->med == cgfd::MED_ISO ? 12 : (p->med == cgfd::MED_VTI ? 15 : 31);
+  p->ncoef = p->med == cgfd::MED_AC ? 11 : (p->med == cgfd::MED_ISO ? 12 : (p->med == cgfd::MED_VTI ? 15 : 31));
+  if (p->med == cgfd::MED_AC) p->use_tma = false;  // acoustic media run their own stage kernel
   p->nt_total = d->nt_total;
   p->dt = d->dt;
   p->free_top = d->free_top ? 1 : 0;
   if (p->free_top && p->nk < cgfd::NSURF + 4) throw cgfd::Error(CGFD_ERR_INVALID, "nk too small for the free surface");
+  p->nbulk = p->med == cgfd::MED_AC || !p->free_top ? p->nk : p->nk - cgfd::NSURF;
   // device layout
   layout(p->ni, p->nj, p->nk, p->sx, p->sz, p->sf, p->off0);
   // default tiling (cgfd_set_tile_shape / cgfd_set_zchunk / the autotuner refine it): 32x4
@@ -871,9 +918,8 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   // short chunks keep the resident blocks on neighbouring planes)
   p->shape = p->med == cgfd::MED_ISO ? 1 : 0;
   {
-    int nbulk = p->free_top ? p->nk - cgfd::NSURF : p->nk;
-    int chunks = std::max(1, (nbulk + 11) / 12);
-    p->nzc = (nbulk + chunks - 1) / chunks;
+    int chunks = std::max(1, (p->nbulk + 11) / 12);
+    p->nzc = (p->nbulk + chunks - 1) / chunks;
   }
 
   size_t &B = p->bytes;
@@ -923,9 +969,9 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   if (p->coef_type != cgfd::COEF_F32) to_16bit_coefficients(p);
 
   // TMA tensor maps of the four wavefield levels and of the coefficients
-  if (!p->fp64) make_maps(p);
-  // free surface
-  if (p->free_top) {
+  if (p->use_tma) make_maps(p);
+  // free surface of elastic media: velocity-gradient conversion and traction-image fluxes
+  if (p->free_top && p->med != cgfd::MED_AC) {
     std::vector<float> mx, my;
     cgfd::dvh2dvz(d, mx, my);
     p->matx = dalloc_real(p, mx.size(), B);
@@ -993,6 +1039,13 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
         all.nsrc++;
       }
     }
+  }
+  if (p->med == cgfd::MED_AC) {
+    // the acoustic source term takes the force and Mxx only (sv_curv_col_ac_iso_rhs_src_gpu,
+    // sv_curv_col_ac_iso_gpu.cu:823-887); the other moment components would land in the unused
+    // fields 4-8
+    for (size_t q = 0; q < p->src.stf.size(); q += 9)
+      for (int c = 4; c < 9; c++) p->src.stf[q + c] = 0.f;
   }
   if (p->src.nsrc > 0) {
     cgfd::SrcHost &s = p->src;
@@ -1126,7 +1179,8 @@ void make_maps(cgfd_problem *p) {
 // layers run in the march direction of the stage's z operator: upwards for backward operators
 // (tiles), downwards for forward ones (tiles_dn).
 void make_tiles(cgfd_problem *p) {
-  const int ty = cgfd::tma_tile_y(p->med, p->shape), nbulk = p->free_top ? p->nk - cgfd::NSURF : p->nk;
+  if (p->med == cgfd::MED_AC) return;  // no TMA kernel for acoustic media
+  const int ty = cgfd::tma_tile_y(p->med, p->shape), nbulk = p->nbulk;
   const int nbx = (p->ni + cgfd::TX - 1) / cgfd::TX, nby = (p->nj + ty - 1) / ty;
   if (nbx > cgfd::kTileBxMask + 1) throw cgfd::Error(CGFD_ERR_INVALID, "grid too wide for the bulk tile list");
   std::vector<int> cuts = {0, nbulk};
@@ -1656,7 +1710,9 @@ int cgfd_set_wavefield_shot(cgfd_problem *p, int shot, const float *in) {
     {
       PinnedStager &ps = PinnedStager::for_device(p->device);
       std::lock_guard<std::mutex> lk(ps.mutex());
-      for (int c = 0; c < 9; c++)
+      // acoustic media: Vx Vy Vz P; components 4-8 are not part of the state and stay 0
+      const int nf = p->med == cgfd::MED_AC ? 4 : 9;
+      for (int c = 0; c < nf; c++)
         upload_field(p, in + (size_t)c * g.siz_icmp, p->rvoid(p->wbuf[p->it & 1], ((size_t)shot * 9 + c) * p->sf), tmp, 0,
                      0, &ps);
     }
@@ -1731,7 +1787,7 @@ int cgfd_autotune(cgfd_problem *p, int steps, int *chosen) {
   if (p->it != 0) { set_err("autotuning runs on a problem that has not stepped yet (step 0)"); return CGFD_ERR_INVALID; }
   return guarded([&] {
     CK(cudaSetDevice(p->device));
-    const int nbulk = p->free_top ? p->nk - cgfd::NSURF : p->nk;
+    const int nbulk = p->nbulk;
     std::vector<int> zc;
     for (int c : {8, 10, 12, 14, 16, 20, 24, 32, 48, 64, 96, nbulk})
       if (c >= 1 && c <= nbulk && std::find(zc.begin(), zc.end(), c) == zc.end()) zc.push_back(c);
@@ -1837,6 +1893,10 @@ int cgfd_set_bulk_variant(cgfd_problem *p, int tma) {
   if (!tma && p->nshot > 1) { set_err("the direct-load bulk kernel handles one shot"); return CGFD_ERR_UNSUPPORTED; }
   if (tma && p->fp64) {
     set_err("the FP64 build runs the direct-load bulk kernel");
+    return CGFD_ERR_UNSUPPORTED;
+  }
+  if (p->med == cgfd::MED_AC) {
+    set_err("acoustic media run their own stage kernel");
     return CGFD_ERR_UNSUPPORTED;
   }
   if (!tma && p->precision != CGFD_PREC_FP32 && !p->fp64) {

@@ -32,18 +32,21 @@ constexpr int GX = 32;
 // the traction image rewrites up to 4 layers, vlow 3 (sv_curv_col_el_iso_gpu.cu:212-249).
 constexpr int NSURF = 4;
 
-enum { MED_ISO = 0, MED_VTI = 1, MED_ANISO = 2 };
+// elastic media; MED_AC: acoustic (fields Vx Vy Vz P, P in the Txx slot; cgfd_acoustic.cu)
+enum { MED_ISO = 0, MED_VTI = 1, MED_ANISO = 2, MED_AC = 3 };
 
 // Coefficient fields in the device coefficient array, in this order:
 //   0..8  xi_x xi_y xi_z eta_x eta_y eta_z zeta_x zeta_y zeta_z
 //   9     1/rho
 //   10..  iso: lambda mu | vti: c11 c13 c33 c55 c66 | aniso: c11 c12 .. c66 (21, row-major upper)
+//         | acoustic: kappa
 constexpr int CF_SLW = 9;
 constexpr int CF_MED = 10;
 template <int MED> struct MedInfo;
 template <> struct MedInfo<MED_ISO>   { static constexpr int NCOEF = 12; };
 template <> struct MedInfo<MED_VTI>   { static constexpr int NCOEF = 15; };
 template <> struct MedInfo<MED_ANISO> { static constexpr int NCOEF = 31; };
+template <> struct MedInfo<MED_AC>    { static constexpr int NCOEF = 11; };
 
 // Real type R of the stored solution, coefficients and arithmetic: float (the reference's
 // precision, every production mode) or double (the FP64 build, CGFD_PREC_FP64).
@@ -300,39 +303,40 @@ constexpr int kErrWaveNonfinite = 4;     // the RK combine produced a NaN/Inf so
 __device__ __forceinline__ bool nonfinite(float v) { return !(fabsf(v) <= 3.402823466e38f); }
 __device__ __forceinline__ bool nonfinite(double v) { return !(fabs(v) <= 1.7976931348623157e308); }
 
-// RK combine of 9 values at one point (wav_update / wav_update_end, wav_t.cu:362-378).
+// RK combine of N values at one point (wav_update / wav_update_end, wav_t.cu:362-378): the 9
+// elastic components, or the 4 acoustic ones (Vx Vy Vz P).
 // cur_c: the stage input at the point (== pre at stage 0). err (may be null): at stage 3,
 // a non-finite new solution value sets kErrWaveNonfinite there -- the blow-up sentinel the
 // reference leaves stubbed (drv_rk_curv_col.cu:507-510, wav_check_value wav_t.cu:260-279).
-template <typename R>
+template <int N = 9, typename R>
 __device__ __forceinline__ void rk_store(int stage, R ca, R cb, long long comp_stride, long long idx,
-                                         const R cur_c[9], const R h[9], const R *pre,
+                                         const R cur_c[N], const R h[N], const R *pre,
                                          R *tmp_out, R *end, int *err = nullptr) {
   if (stage == 0) {
 #pragma unroll
-    for (int c = 0; c < 9; c++) {
+    for (int c = 0; c < N; c++) {
       tmp_out[c * comp_stride + idx] = cur_c[c] + ca * h[c];
       end[c * comp_stride + idx] = cur_c[c] + cb * h[c];
     }
   } else if (stage < 3) {
-    R p[9], e[9];
+    R p[N], e[N];
 #pragma unroll
-    for (int c = 0; c < 9; c++) {
+    for (int c = 0; c < N; c++) {
       p[c] = __ldg(pre + c * comp_stride + idx);
       e[c] = end[c * comp_stride + idx];
     }
 #pragma unroll
-    for (int c = 0; c < 9; c++) {
+    for (int c = 0; c < N; c++) {
       tmp_out[c * comp_stride + idx] = p[c] + ca * h[c];
       end[c * comp_stride + idx] = e[c] + cb * h[c];
     }
   } else {
-    R e[9];
+    R e[N];
     bool bad = false;
 #pragma unroll
-    for (int c = 0; c < 9; c++) e[c] = end[c * comp_stride + idx];
+    for (int c = 0; c < N; c++) e[c] = end[c * comp_stride + idx];
 #pragma unroll
-    for (int c = 0; c < 9; c++) {
+    for (int c = 0; c < N; c++) {
       const R v = e[c] + cb * h[c];
       end[c * comp_stride + idx] = v;
       bad |= nonfinite(v);

@@ -103,6 +103,13 @@ void launch_metric(const float *x, const float *y, const float *z, float *const 
 template <typename R>
 int launch_stage_bulk(int med, const StagePT<R> &p, int nzc, cudaStream_t st);
 int launch_stage_surface(int med, int coef_type, int wave16, const StageP &p, cudaStream_t st);
+// Acoustic media (cgfd_acoustic.cu), R float or double: the free-surface pressure image of the
+// stage input (before the stage; no launch without a free surface), and the fused stage of
+// every cell in z chunks of nzc planes.
+template <typename R>
+int launch_ac_image(const StagePT<R> &p, cudaStream_t st);
+template <typename R>
+int launch_stage_ac(const StagePT<R> &p, int nzc, cudaStream_t st);
 // FP64 build: the surface slab with double storage and arithmetic
 int launch_stage_surface64(int med, const StagePT<double> &p, cudaStream_t st);
 // traction-image fluxes of the stage input for the surface slab (before it, same stream)

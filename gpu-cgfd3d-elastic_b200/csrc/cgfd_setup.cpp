@@ -15,6 +15,7 @@ static const double kPi = 3.1415926535897;  // constants.h:14
 
 int medium_ncmp(int medium_type) {
   switch (medium_type) {
+    case CGFD_MEDIUM_ACOUSTIC_ISO: return 2;
     case CGFD_MEDIUM_ELASTIC_ISO: return 3;
     case CGFD_MEDIUM_ELASTIC_VTI: return 6;
     case CGFD_MEDIUM_ELASTIC_ANISO: return 22;
@@ -25,7 +26,10 @@ int medium_ncmp(int medium_type) {
 void validate_desc(const cgfd_problem_desc *d) {
   if (!d) throw Error(CGFD_ERR_INVALID, "desc is NULL");
   if (d->ni < 8 || d->nj < 8 || d->nk < 8) throw Error(CGFD_ERR_INVALID, "grid must have at least 8 points per axis");
-  if (medium_ncmp(d->medium_type) < 0) throw Error(CGFD_ERR_UNSUPPORTED, "medium_type must be elastic iso/vti/aniso");
+  if (medium_ncmp(d->medium_type) < 0)
+    throw Error(CGFD_ERR_UNSUPPORTED, "medium_type must be acoustic iso or elastic iso/vti/aniso");
+  if (d->medium_type == CGFD_MEDIUM_ACOUSTIC_ISO && d->precision != CGFD_PREC_FP32 && d->precision != CGFD_PREC_FP64)
+    throw Error(CGFD_ERR_UNSUPPORTED, "acoustic media run in FP32 or FP64 (CGFD_PREC_FP32 / CGFD_PREC_FP64)");
   if (!d->medium) throw Error(CGFD_ERR_INVALID, "the medium array is required");
   if (!d->metric && !d->coord) throw Error(CGFD_ERR_INVALID, "coordinates are required when no metric is given");
   if (!(d->dt > 0.0f)) throw Error(CGFD_ERR_INVALID, "dt must be > 0");
@@ -562,7 +566,7 @@ int cgfd_metric_calc(int ni, int nj, int nk, const float *coord, float *metric) 
 // Largest stable time step in FP64 (blk_t.cu:673-763): CFL * (min distance from a point
 // to the 8 planes through its neighbours) / Vp, over physical points except the last
 // index of each axis. Vp: iso sqrt((lambda+2mu)/rho), VTI max(sqrt(c11/rho),
-// sqrt(c33/rho)), aniso sqrt(c11/rho).
+// sqrt(c33/rho)), aniso sqrt(c11/rho), acoustic sqrt(kappa/rho).
 int cgfd_dt_estimate(const cgfd_problem_desc *d, double cfl, double *dtmax) {
   if (!d || !d->coord || !d->medium || !dtmax) return CGFD_ERR_INVALID;
   cgfd::RefGrid g(d->ni, d->nj, d->nk);
@@ -575,7 +579,8 @@ int cgfd_dt_estimate(const cgfd_problem_desc *d, double cfl, double *dtmax) {
       for (int i = 0; i < d->ni - 1; i++) {
         size_t p = g.at(i, j, k);
         double rho = m[p], vp;
-        if (d->medium_type == CGFD_MEDIUM_ELASTIC_ISO) vp = std::sqrt((m[g.siz_icmp + p] + 2.0 * m[2 * g.siz_icmp + p]) / rho);
+        if (d->medium_type == CGFD_MEDIUM_ACOUSTIC_ISO) vp = std::sqrt(m[g.siz_icmp + p] / rho);
+        else if (d->medium_type == CGFD_MEDIUM_ELASTIC_ISO) vp = std::sqrt((m[g.siz_icmp + p] + 2.0 * m[2 * g.siz_icmp + p]) / rho);
         else if (d->medium_type == CGFD_MEDIUM_ELASTIC_VTI)
           vp = std::fmax(std::sqrt(m[g.siz_icmp + p] / rho), std::sqrt(m[3 * g.siz_icmp + p] / rho));
         else vp = std::sqrt(m[g.siz_icmp + p] / rho);

@@ -14,9 +14,15 @@
  *  - Host arrays use the reference layout var[cmp][k][j][i] with i fastest and CGFD_NGHOST
  *    ghost points on every side: nx = ni+6, ny = nj+6, nz = nk+6 (gd_t.cu:1888-2043).
  *  - Wavefield components are ordered Vx,Vy,Vz,Txx,Tyy,Tzz,Tyz,Txz,Txy (wav_t.cu:100-143).
+ *    Acoustic media (sv_curv_col_ac_iso_gpu.cu, wav_ac_init wav_t.cu:190-250) use Vx,Vy,Vz,P:
+ *    P takes the Txx slot (component 3) and components 4-8 stay 0, so every wavefield,
+ *    seismogram, slice and snapshot array keeps the 9-component layout. Acoustic sources use
+ *    the force and the Mxx moment component (the pressure source of
+ *    sv_curv_col_ac_iso_rhs_src_gpu); acoustic problems run in CGFD_PREC_FP32 or CGFD_PREC_FP64.
  *  - Metric components are ordered jac,xi_x,xi_y,xi_z,eta_x,eta_y,eta_z,zeta_x,zeta_y,zeta_z
  *    (gd_t.cu:140-200, gd_curv_metric_init).
  *  - Medium components are ordered as the media_*.nc variables (md_t.cu:16-268):
+ *      acoustic_iso : rho, kappa
  *      elastic_iso  : rho, lambda, mu
  *      elastic_vti  : rho, c11, c13, c33, c55, c66
  *      elastic_aniso: rho, c11,c12,c13,c14,c15,c16, c22,c23,c24,c25,c26, c33,c34,c35,c36,
@@ -40,6 +46,7 @@ extern "C" {
 #define CGFD_NCMP   9
 
 /* medium ids: src/forward/constants.h:20-24 */
+#define CGFD_MEDIUM_ACOUSTIC_ISO  1
 #define CGFD_MEDIUM_ELASTIC_ISO   2
 #define CGFD_MEDIUM_ELASTIC_VTI   3
 #define CGFD_MEDIUM_ELASTIC_ANISO 4
@@ -122,7 +129,7 @@ typedef struct cgfd_station_desc {
  */
 typedef struct cgfd_problem_desc {
   int ni, nj, nk;           /* physical points incl. PML layers (ghosts excluded)          */
-  int medium_type;          /* CGFD_MEDIUM_ELASTIC_*                                        */
+  int medium_type;          /* CGFD_MEDIUM_ACOUSTIC_ISO or CGFD_MEDIUM_ELASTIC_*               */
   const float *coord;       /* [3][nz][ny][nx] x,y,z with ghosts filled; used for the PML
                                length/spacing average (bdry_t.cu:334-451). May be NULL when
                                no PML face is enabled and metric is given.                   */
@@ -206,7 +213,7 @@ int cgfd_station_info(const cgfd_problem *p, int *input_index, int *ijk);
  */
 int cgfd_get_wavefield(cgfd_problem *p, float *out);
 
-/* Overwrite w_pre (physical points only; ghosts stay 0). */
+/* Overwrite w_pre (physical points only; ghosts stay 0; acoustic media take components 0-3). */
 int cgfd_set_wavefield(cgfd_problem *p, const float *in);
 
 /*

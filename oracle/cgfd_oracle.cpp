@@ -449,6 +449,7 @@ struct Oracle {
   const T *med_c(int c) const { return med.data() + (size_t)c * g.siz_icmp; }
 
   int ncmp_medium() const {
+    if (medium_type == CGFD_MEDIUM_ACOUSTIC_ISO) return 2;  // rho, kappa
     return medium_type == CGFD_MEDIUM_ELASTIC_ISO ? 3 : (medium_type == CGFD_MEDIUM_ELASTIC_VTI ? 6 : 22);
   }
 
@@ -535,7 +536,7 @@ struct Oracle {
     if (d->ni < 8 || d->nj < 8 || d->nk < 8) throw std::runtime_error("grid too small");
     medium_type = d->medium_type;
     if (medium_type != CGFD_MEDIUM_ELASTIC_ISO && medium_type != CGFD_MEDIUM_ELASTIC_VTI &&
-        medium_type != CGFD_MEDIUM_ELASTIC_ANISO)
+        medium_type != CGFD_MEDIUM_ELASTIC_ANISO && medium_type != CGFD_MEDIUM_ACOUSTIC_ISO)
       throw std::runtime_error("unsupported medium_type");
     g.set(d->ni, d->nj, d->nk);
     dt = (T)d->dt; t0 = (T)d->t0; nt_total = d->nt_total;
@@ -548,7 +549,7 @@ struct Oracle {
     for (size_t n = 0; n < g.siz_icmp; n++) med[n] = med[n] > (T)1e-10 ? (T)(1.0 / med[n]) : (T)0;
     wave.assign(4 * 9 * g.siz_icmp, (T)0);
     free_top = d->free_top;
-    if (free_top) dvh2dvz();
+    if (free_top && medium_type != CGFD_MEDIUM_ACOUSTIC_ISO) dvh2dvz();  // drv_rk_curv_col.cu:89: "not need"
     pml_set(d);
     src_set(d);
     recv_set(d);
@@ -1230,6 +1231,142 @@ struct Oracle {
     }
   }
 
+  // ---------------------------------------------------------------------------------------
+  // acoustic media, sv_curv_col_ac_iso_gpu.cu: fields Vx Vy Vz P with P in the Txx slot
+  // (wav_ac_init, wav_t.cu:190-250), medium slowness and kappa
+  // ---------------------------------------------------------------------------------------
+  // pressure image of the free surface, in place on the stage input (:376-410)
+  void ac_timg(T *w) {
+    T *P = w + TXX * g.siz_icmp;
+    for (int j = g.nj1; j <= g.nj2; j++)
+      for (int i = g.ni1; i <= g.ni2; i++) {
+        size_t top = i + j * g.siz_iy + (size_t)g.nk2 * g.siz_iz;
+        P[top] = 0;
+        for (int k = g.nk2 + 1; k < g.nz; k++)
+          P[i + j * g.siz_iy + (size_t)k * g.siz_iz] = -P[i + j * g.siz_iy + (size_t)(2 * g.nk2 - k) * g.siz_iz];
+      }
+  }
+
+  // inner points (:277-366)
+  void ac_inner(const T *w, T *h, const Ops &o) {
+    const Grid &G = g;
+    const long sy = (long)G.siz_iy, sz = (long)G.siz_iz;
+#pragma omp parallel for schedule(static)
+    for (int k = G.nk1; k <= G.nk2; k++)
+      for (int j = G.nj1; j <= G.nj2; j++)
+        for (int i = G.ni1; i <= G.ni2; i++) {
+          size_t iptr = i + j * G.siz_iy + k * G.siz_iz;
+          const T *Vx = w + VX * G.siz_icmp, *Vy = w + VY * G.siz_icmp, *Vz = w + VZ * G.siz_icmp,
+                  *P = w + TXX * G.siz_icmp;
+          T DxVx = fd_apply(o.x, Vx, iptr, 1), DyVx = fd_apply(o.y, Vx, iptr, sy), DzVx = fd_apply(o.z, Vx, iptr, sz);
+          T DxVy = fd_apply(o.x, Vy, iptr, 1), DyVy = fd_apply(o.y, Vy, iptr, sy), DzVy = fd_apply(o.z, Vy, iptr, sz);
+          T DxVz = fd_apply(o.x, Vz, iptr, 1), DyVz = fd_apply(o.y, Vz, iptr, sy), DzVz = fd_apply(o.z, Vz, iptr, sz);
+          T DxP = fd_apply(o.x, P, iptr, 1), DyP = fd_apply(o.y, P, iptr, sy), DzP = fd_apply(o.z, P, iptr, sz);
+          T xix = metric_c(1)[iptr], xiy = metric_c(2)[iptr], xiz = metric_c(3)[iptr];
+          T etx = metric_c(4)[iptr], ety = metric_c(5)[iptr], etz = metric_c(6)[iptr];
+          T ztx = metric_c(7)[iptr], zty = metric_c(8)[iptr], ztz = metric_c(9)[iptr];
+          T kappa = med_c(1)[iptr], slw = med_c(0)[iptr];
+          h[VX * G.siz_icmp + iptr] = -slw * (xix * DxP + etx * DyP + ztx * DzP);
+          h[VY * G.siz_icmp + iptr] = -slw * (xiy * DxP + ety * DyP + zty * DzP);
+          h[VZ * G.siz_icmp + iptr] = -slw * (xiz * DxP + etz * DyP + ztz * DzP);
+          h[TXX * G.siz_icmp + iptr] = -kappa * (xix * DxVx + etx * DyVx + ztx * DzVx + xiy * DxVy + ety * DyVy +
+                                                 zty * DzVy + xiz * DxVz + etz * DyVz + ztz * DzVz);
+        }
+  }
+
+  // low-order pressure rows of the top 3 planes (:413-521): 0 on the surface, 2nd / 4th-order
+  // velocity z-derivatives below it
+  void ac_vlow(const T *w, T *h, const Ops &o) {
+    const Grid &G = g;
+    for (int n = 0; n < 3; n++) {
+      const int k = G.nk2 - n;
+      const Op &oz = o.zlay[n];
+#pragma omp parallel for schedule(static)
+      for (int j = G.nj1; j <= G.nj2; j++)
+        for (int i = G.ni1; i <= G.ni2; i++) {
+          size_t iptr = i + j * G.siz_iy + k * G.siz_iz;
+          if (k == G.nk2) {
+            h[TXX * G.siz_icmp + iptr] = 0;
+            continue;
+          }
+          const T *V[3] = {w + VX * G.siz_icmp, w + VY * G.siz_icmp, w + VZ * G.siz_icmp};
+          T Dx[3], Dy[3], Dz[3];
+          for (int c = 0; c < 3; c++) {
+            Dx[c] = fd_apply(o.x, V[c], iptr, 1);
+            Dy[c] = fd_apply(o.y, V[c], iptr, (long)G.siz_iy);
+            Dz[c] = fd_apply(oz, V[c], iptr, (long)G.siz_iz);
+          }
+          T xix = metric_c(1)[iptr], xiy = metric_c(2)[iptr], xiz = metric_c(3)[iptr];
+          T etx = metric_c(4)[iptr], ety = metric_c(5)[iptr], etz = metric_c(6)[iptr];
+          T ztx = metric_c(7)[iptr], zty = metric_c(8)[iptr], ztz = metric_c(9)[iptr];
+          T kappa = med_c(1)[iptr];
+          h[TXX * G.siz_icmp + iptr] = -kappa * (xix * Dx[0] + etx * Dy[0] + ztx * Dz[0] + xiy * Dx[1] + ety * Dy[1] +
+                                                 zty * Dz[1] + xiz * Dx[2] + etz * Dy[2] + ztz * Dz[2]);
+        }
+    }
+  }
+
+  // CFS-PML (:579-802): per face, the 1-D terms of its axis correct the RHS and drive the 4
+  // auxiliary variables
+  void ac_cfspml(const T *w, T *h, const Ops &o, int cur_lvl_aux_is_pre) {
+    const Grid &G = g;
+    const Op *opa[3] = {&o.x, &o.y, &o.z};
+    const long sh[3] = {1, (long)G.siz_iy, (long)G.siz_iz};
+    const int fld[4] = {VX, VY, VZ, TXX};
+    for (int idim = 0; idim < 3; idim++)
+      for (int iside = 0; iside < 2; iside++) {
+        Face &f = face[idim][iside];
+        if (!f.enable) continue;
+        T *aux_cur = f.aux.data() + (size_t)(cur_lvl_aux_is_pre ? f.lvl_pre : 1) * 9 * f.siz_icmp;
+        T *aux_rhs = f.aux.data() + (size_t)2 * 9 * f.siz_icmp;
+#pragma omp parallel for schedule(static)
+        for (int iz = 0; iz < f.nz; iz++)
+          for (int iy = 0; iy < f.ny; iy++)
+            for (int ix = 0; ix < f.nx; ix++) {
+              size_t ia = (size_t)iz * f.ny * f.nx + (size_t)iy * f.nx + ix;
+              size_t iptr = (ix + f.ni1) + (iy + f.nj1) * G.siz_iy + (iz + f.nk1) * G.siz_iz;
+              int ab = idim == 0 ? ix : (idim == 1 ? iy : iz);
+              T cD = f.D[ab], cA = f.A[ab], cB = f.B[ab];
+              T cB1 = (T)(cB - 1.0);
+              T m0 = metric_c(1 + 3 * idim)[iptr], m1 = metric_c(2 + 3 * idim)[iptr], m2 = metric_c(3 + 3 * idim)[iptr];
+              T kappa = med_c(1)[iptr], slw = med_c(0)[iptr];
+              T D[4];
+              for (int c = 0; c < 4; c++) D[c] = fd_apply(*opa[idim], w + fld[c] * G.siz_icmp, iptr, sh[idim]);
+              T rhs[4];
+              rhs[0] = -slw * (m0 * D[3]);
+              rhs[1] = -slw * (m1 * D[3]);
+              rhs[2] = -slw * (m2 * D[3]);
+              rhs[3] = -kappa * (m0 * D[0] + m1 * D[1] + m2 * D[2]);
+              for (int c = 0; c < 4; c++) {
+                T a = aux_cur[fld[c] * f.siz_icmp + ia];
+                h[fld[c] * G.siz_icmp + iptr] += cB1 * rhs[c] - cB * a;
+                aux_rhs[fld[c] * f.siz_icmp + ia] = cD * rhs[c] - cA * a;
+              }
+            }
+      }
+  }
+
+  // sources (:823-887): forces on the velocities, Mxx on the pressure
+  void ac_src(T *h, int it, int istage) {
+    const T *jac = metric_c(0), *slw = med_c(0);
+    for (int is = 0; is < nsrc; is++) {
+      if (!(it >= it_begin[is] && it <= it_end[is])) continue;
+      size_t ip = (size_t)is * max_nt * 4 + (size_t)(it - it_begin[is]) * 4 + istage;
+      for (int e = 0; e < ext_num[is]; e++) {
+        size_t iptr = ext_indx[(size_t)is * max_ext + e];
+        T coef = ext_coef[(size_t)is * max_ext + e];
+        if (force_actived) {
+          T V = coef * slw[iptr] / jac[iptr];
+          for (int c = 0; c < 3; c++) h[c * g.siz_icmp + iptr] += F[c][ip] * V;
+        }
+        if (moment_actived) {
+          T rjac = coef / jac[iptr];
+          h[TXX * g.siz_icmp + iptr] += -M[0][ip] * rjac;
+        }
+      }
+    }
+  }
+
   // io_recv_keep, io_funcs.cu:1624-1666 (corner 5 used twice, corner 4 never)
   void recv_keep(const T *w, int it) {
     for (size_t n = 0; n < recv.size(); n++) {
@@ -1306,15 +1443,23 @@ struct Oracle {
       if (it < nt_total) recv_keep(w_pre, it);
       int ipair = it % 8;
       for (int istage = 0; istage < 4; istage++) {
-        const T *w_cur = istage == 0 ? w_pre : w_tmp;
+        T *w_cur = istage == 0 ? w_pre : w_tmp;
         Ops o = make_ops(ipair, istage);
-        rhs_inner(w_cur, w_rhs, o);
-        if (free_top) {
-          rhs_timg(w_cur, w_rhs, o);
-          rhs_vlow(w_cur, w_rhs, o);
+        if (medium_type == CGFD_MEDIUM_ACOUSTIC_ISO) {  // sv_curv_col_ac_iso_onestage, :21-270
+          if (free_top) ac_timg(w_cur);
+          ac_inner(w_cur, w_rhs, o);
+          if (free_top) ac_vlow(w_cur, w_rhs, o);
+          ac_cfspml(w_cur, w_rhs, o, istage == 0);
+          ac_src(w_rhs, it, istage);
+        } else {
+          rhs_inner(w_cur, w_rhs, o);
+          if (free_top) {
+            rhs_timg(w_cur, w_rhs, o);
+            rhs_vlow(w_cur, w_rhs, o);
+          }
+          rhs_cfspml(w_cur, w_rhs, o, istage == 0);
+          rhs_src(w_rhs, it, istage);
         }
-        rhs_cfspml(w_cur, w_rhs, o, istage == 0);
-        rhs_src(w_rhs, it, istage);
         // RK combine (float coefficients as in the reference)
         if (istage == 0) {
           T ca = (T)(rk_a[istage] * (float)dt), cb = (T)(rk_b[istage] * (float)dt);

@@ -8,7 +8,8 @@
  * gd_curv_metric_cal -> media -> src_read_locate_file -> wav_init -> io_recv_read_locate ->
  * bdry_pml_set -> bdry_free_set -> md_rho_to_slow), and the time loop restates
  * drv_rk_curv_col.cu:75-541 for one rank without halo exchange, slices, snapshots, PGV or the
- * exponential sponge, calling the reference's sv_curv_col_el_*_onestage, wav_update and
+ * exponential sponge, calling the reference's sv_curv_col_el_*_onestage (sv_curv_col_ac_iso_onestage
+ * for acoustic media), wav_update and
  * io_recv_keep.
  *
  * usage: ref_harness <dir>   (dir holds params.txt, coord.bin, medium.bin, src.src, station.list)
@@ -28,6 +29,7 @@
 #include "io_funcs.h"
 #include "md_t.h"
 #include "src_t.h"
+#include "sv_curv_col_ac_iso_gpu.h"
 #include "sv_curv_col_el_aniso_gpu.h"
 #include "sv_curv_col_el_gpu.h"
 #include "sv_curv_col_el_iso_gpu.h"
@@ -144,7 +146,8 @@ int main(int argc, char **argv) {
 
   wav_t wav;
   memset(&wav, 0, sizeof(wav));
-  wav_init(&gd, &wav, fd.num_rk_stages, 0, 0);
+  if (medium_type == CONST_MEDIUM_ACOUSTIC_ISO) wav_ac_init(&gd, &wav, fd.num_rk_stages);  // main:676-681
+  else wav_init(&gd, &wav, fd.num_rk_stages, 0, 0);
 
   iorecv_t iorecv;
   memset(&iorecv, 0, sizeof(iorecv));
@@ -166,7 +169,7 @@ int main(int argc, char **argv) {
   md_rho_to_slow(md.rho, md.siz_icmp);
 
   // ---- time loop: drv_rk_curv_col.cu:75-541 on one rank
-  if (bdryfree.is_sides_free[CONST_NDIM - 1][1] == 1) {
+  if (bdryfree.is_sides_free[CONST_NDIM - 1][1] == 1 && md.medium_type != CONST_MEDIUM_ACOUSTIC_ISO) {  // :73-95
     if (md.medium_type == CONST_MEDIUM_ELASTIC_ISO) sv_curv_col_el_iso_dvh2dvz(&gd, &metric, &md, &bdryfree);
     else if (md.medium_type == CONST_MEDIUM_ELASTIC_VTI) sv_curv_col_el_vti_dvh2dvz(&gd, &metric, &md, &bdryfree);
     else sv_curv_col_el_aniso_dvh2dvz(&gd, &metric, &md, &bdryfree);
@@ -219,9 +222,8 @@ int main(int argc, char **argv) {
   // Statement by statement against drv_rk_curv_col.cu (line numbers of that file). Left out:
   // io_line_keep / io_slice_nc_put / io_snap_nc_put (:203-215; outputs the harness does not
   // write), the MPI message pack / start / wait / unpack (:336, :353-355, :407-408, :461-462,
-  // :492-501; one rank, no neighbours), the acoustic and visco-elastic branches (:265-276,
-  // :317-331, :479-490), the stubbed NaN check (:507-510) and the exponential sponge (:513-515,
-  // not enabled by the cases). The per-stage cudaDeviceSynchronize (:333) is implied by the
+  // :492-501; one rank, no neighbours), the visco-elastic branches (:317-331, :479-490), the
+  // stubbed NaN check (:507-510) and the exponential sponge (:513-515, not enabled by the cases). The per-stage cudaDeviceSynchronize (:333) is implied by the
   // default stream's ordering.
   for (int it = 0; it < nsteps; it++) {  // :193
     io_recv_keep(&iorecv, w_pre_d, w_buff, it, wav.ncmp, wav.siz_icmp);  // :200
@@ -233,8 +235,13 @@ int main(int argc, char **argv) {
           for (int s = 0; s < 2; s++)
             bdrypml_d.auxvar[a][s].cur = istage == 0 ? bdrypml_d.auxvar[a][s].pre : bdrypml_d.auxvar[a][s].tmp;
       src_set_time(&src_d, it, istage);  // :260
-      // :263-315, the three elastic media
-      if (md_d.medium_type == CONST_MEDIUM_ELASTIC_ISO)
+      // :263-315, the acoustic and the three elastic media
+      if (md_d.medium_type == CONST_MEDIUM_ACOUSTIC_ISO)
+        sv_curv_col_ac_iso_onestage(w_cur_d, w_rhs_d, wav_d, fd_wav_d, gd_d, metric_d, md_d, bdrypml_d, bdryfree_d, src_d,
+                                    fd.num_of_fdx_op, fd.pair_fdx_op[ipair][istage], fd.num_of_fdy_op,
+                                    fd.pair_fdy_op[ipair][istage], fd.num_of_fdz_op, fd.pair_fdz_op[ipair][istage],
+                                    fd.fdz_max_len, myid);
+      else if (md_d.medium_type == CONST_MEDIUM_ELASTIC_ISO)
         sv_curv_col_el_iso_onestage(w_cur_d, w_rhs_d, wav_d, fd_wav_d, gd_d, metric_d, md_d, bdrypml_d, bdryfree_d, src_d,
                                     fd.num_of_fdx_op, fd.pair_fdx_op[ipair][istage], fd.num_of_fdy_op,
                                     fd.pair_fdy_op[ipair][istage], fd.num_of_fdz_op, fd.pair_fdz_op[ipair][istage],
@@ -304,17 +311,17 @@ int main(int argc, char **argv) {
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) die(cudaGetErrorString(err));
 
-  // ---- outputs
+  // ---- outputs, in the 9-component layout (acoustic: Vx Vy Vz P, components 4-8 left 0)
   std::vector<float> seis((size_t)iorecv.total_number * 9 * nt_total, 0.f);
   // samples of steps that were not run stay 0 (the reference leaves them uninitialised)
   for (int r = 0; r < iorecv.total_number; r++)
-    for (int c = 0; c < 9; c++)
+    for (int c = 0; c < wav.ncmp; c++)
       for (int t = 0; t < nsteps && t < nt_total; t++)
         seis[((size_t)r * 9 + c) * nt_total + t] = iorecv.recvone[r].seismo[(size_t)c * nt_total + t];
   snprintf(path, sizeof(path), "%s/ref_seismo.bin", dir);
   write_bin(path, seis.data(), seis.size());
-  std::vector<float> w((size_t)9 * gd.siz_icmp);
-  cudaMemcpy(w.data(), w_pre_d, sizeof(float) * w.size(), cudaMemcpyDeviceToHost);
+  std::vector<float> w((size_t)9 * gd.siz_icmp, 0.f);
+  cudaMemcpy(w.data(), w_pre_d, sizeof(float) * wav.ncmp * gd.siz_icmp, cudaMemcpyDeviceToHost);
   snprintf(path, sizeof(path), "%s/ref_wave.bin", dir);
   write_bin(path, w.data(), w.size());
   if (free_top) {

@@ -7,6 +7,7 @@ GOLDEN_CASES = {
     "iso_small": ("iso", 28, 26, 22, 120, 5, 1),
     "vti_small": ("vti", 28, 26, 22, 120, 5, 2),
     "aniso_small": ("aniso", 28, 26, 22, 120, 5, 3),
+    "ac_small": ("ac", 28, 26, 22, 120, 5, 4),
 }
 
 

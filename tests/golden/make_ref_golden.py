@@ -1,7 +1,7 @@
 """Generates tests/golden/ref_<case>.npz by running the reference's own solver code
 (oracle/_ref/ref_harness, built by `make -f oracle/Makefile.ref`) on a B200.
 
-    python tests/golden/make_ref_golden.py <out_dir>
+    python tests/golden/make_ref_golden.py <out_dir> [case ...]   (default: every case)
 
 The fixtures hold the reference-computed metrics, seismograms, final wavefield and free-surface
 peak ground motion (PG_calcu_gpu) of small seeded problems (tests/golden/cases.py); tests/test_cpu_golden.py checks the oracle against
@@ -21,9 +21,9 @@ from golden.cases import GOLDEN_CASES, golden_problem  # noqa: E402
 from golden import ref_io  # noqa: E402
 
 
-def main(out_dir):
+def main(out_dir, names=None):
     os.makedirs(out_dir, exist_ok=True)
-    for name in GOLDEN_CASES:
+    for name in names or list(GOLDEN_CASES):
         p, nsteps = golden_problem(name)
         with tempfile.TemporaryDirectory() as d:
             r = ref_io.run(p, d, nsteps)
@@ -35,4 +35,4 @@ def main(out_dir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else HERE)
+    main(sys.argv[1] if len(sys.argv) > 1 else HERE, sys.argv[2:])

@@ -92,9 +92,14 @@ def test_invalid_descriptions_are_rejected():
     rc, msg = _create(d)
     assert rc == -1 and "at least 8" in msg
     d = p.desc()
-    d.medium_type = 1  # acoustic: not on this path
+    d.medium_type = 5  # visco-elastic iso: not built
     rc, msg = _create(d)
     assert rc == -5
+    d = p.desc()
+    d.medium_type = 1  # acoustic: FP32 and FP64 only
+    d.precision = cgfd_b200.CGFD_PREC_U16_COEF
+    rc, msg = _create(d)
+    assert rc == -5 and "acoustic" in msg
     d = p.desc()
     d.dt = 0.0
     rc, msg = _create(d)
