@@ -301,14 +301,16 @@ def batched_mixed(local, steps=16):
 def media_bench(local, steps=2000):
     """The anisotropic precision workload at its full size: 320x320x160 (50 m, CFS-PML 20, free
     surface), layered Thomsen VTI and Bond-rotated tilted-TI 21-Cij media, one double-couple
-    source (fc 3 Hz) at 2 km, 100 surface stations, 2000 steps. The FP64 build of the kernels
+    source (fc 3 Hz) at 2 km, 100 surface stations, 2000 steps; and the same grid with a layered
+    acoustic medium (pressure and force source; FP32 only, its 16-bit modes are not built). The FP64 build of the kernels
     runs first; then every storage-precision mode runs the same 2000 steps (graph-replayed, timed
     with CUDA events: Gcell-stage/s) and reports its seismogram error against the FP64 build
     (relative L2 of the gather, largest per-station relative L2 with the tests' 1e-3 floor,
     relative error of the peak amplitude). FP32 and 16-bit fixed-point coefficients also report
     the bulk stage's algorithmic bytes (36 wavefield + NCOEF coefficient accesses per
-    cell-stage) per event-timed duration against the measured HBM peak. Each mode's problem is
-    autotuned (tile shape, z chunk) before it runs."""
+    cell-stage; acoustic: 16 wavefield + 11 coefficient accesses over every plane) per event-timed
+    duration against the measured HBM peak. Each mode's problem is autotuned (tile shape, z chunk)
+    before it runs."""
     import torch
     from cgfd_b200 import (synth, Simulation, CGFD_PREC_FP32, CGFD_PREC_U16_COEF, CGFD_PREC_FP16_WAVE,
                            CGFD_PREC_FP16_COEF, CGFD_PREC_BF16_COEF, CGFD_PREC_FP64)
@@ -319,7 +321,8 @@ def media_bench(local, steps=2000):
     out = {"workload": f"{ni}x{nj}x{nk}", "steps": steps, "reference": "FP64 build of the same kernels (GPU)"}
     modes = (("fp32", CGFD_PREC_FP32, 4), ("u16coef", CGFD_PREC_U16_COEF, 2), ("mixed_fp16wave", CGFD_PREC_FP16_WAVE, 2),
              ("fp16coef", CGFD_PREC_FP16_COEF, 2), ("bf16coef", CGFD_PREC_BF16_COEF, 2))
-    for med, ncoef in (("vti", 15), ("aniso", 31)):
+    for med, ncoef in (("vti", 15), ("aniso", 31), ("ac", 11)):
+        nf, nplanes = (4, nk) if med == "ac" else (9, nk - 4)  # fields; planes of the bulk kernel
         p = synth.make_problem(ni, nj, nk, 50.0, steps, dt=None, medium=med, npml=20, nsrc=1, sta_grid=(10, 10),
                                fc=3.0, seed=31, src_depth=(2000.0, 2000.0), center_src=True)
         p.device = local
@@ -332,7 +335,7 @@ def media_bench(local, steps=2000):
         sim.close()
         pk = float(np.abs(ref).max())
         out[f"{med}_fp64"] = {"value": ni * nj * nk * 4 * steps / t64 / 1e9, "unit": UNIT, "wall_s": t64}
-        for name, prec, cbytes in modes:
+        for name, prec, cbytes in modes[:1] if med == "ac" else modes:
             p.precision = prec
             sim = Simulation(p)
             sim.autotune(4)  # tile shape and z chunk for this medium and storage mode
@@ -356,8 +359,8 @@ def media_bench(local, steps=2000):
                 sim.synchronize()
                 bulk_ms, bulk_n = sim.timing(reset=True)["bulk"]
                 sim.set_timing(False)
-                bpc = 36 * 4 + ncoef * cbytes
-                achieved = bpc * ni * nj * (nk - 4) / (bulk_ms / bulk_n * 1e-3) / 1e9
+                bpc = 4 * nf * 4 + ncoef * cbytes
+                achieved = bpc * ni * nj * nplanes / (bulk_ms / bulk_n * 1e-3) / 1e9
                 rec.update({"bulk_ms_per_stage": bulk_ms / bulk_n, "bytes_per_cell_stage": bpc,
                             "roofline_frac": achieved / peak})
             sim.close()

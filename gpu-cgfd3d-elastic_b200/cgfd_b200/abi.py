@@ -213,16 +213,16 @@ class LayerMediaDesc(C.Structure):
 
 
 def media_layer_any_gpu(coord, model, medium_type, method=CGFD_MEDIA_LOC, device=0):
-    """cgfd_media_layer_gpu: the medium of medium_type (CGFD_MEDIUM_ELASTIC_*: [3 | 6 | 22, nz, ny,
-    nx] in the problem description's order) from the layer file model (formats.LayerMedia) on the
-    grid coord [3, nz, ny, nx]."""
+    """cgfd_media_layer_gpu: the medium of medium_type (CGFD_MEDIUM_ACOUSTIC_ISO / _ELASTIC_*:
+    [2 | 3 | 6 | 22, nz, ny, nx] in the problem description's order) from the layer file model
+    (formats.LayerMedia) on the grid coord [3, nz, ny, nx]."""
     _, nz, ny, nx = coord.shape
     el = np.ascontiguousarray(model.elevation, np.float32)
     pa = np.ascontiguousarray(model.param, np.float32)
     d = LayerMediaDesc(int(model.type), int(el.shape[0]), int(model.nx), int(model.ny), float(model.x0),
                        float(model.y0), float(model.dx), float(model.dy), el.ctypes.data, pa.ctypes.data)
     c = np.ascontiguousarray(coord, np.float32)
-    nf = {2: 3, 3: 6, 4: 22}[int(medium_type)]
+    nf = {1: 2, 2: 3, 3: 6, 4: 22}[int(medium_type)]
     out = np.zeros((nf, nz, ny, nx), np.float32)
     check(lib().cgfd_media_layer_gpu(int(device), nx - 6, ny - 6, nz - 6, c.ctypes.data, C.byref(d), int(medium_type),
                                      int(method), out.ctypes.data))

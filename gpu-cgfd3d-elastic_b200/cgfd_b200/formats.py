@@ -142,11 +142,12 @@ def _write_nc(path, names, fields, ni, nj, nk, version=2):
 
 
 MEDIUM_NAMES = {
+    1: ["rho", "kappa"],
     2: ["rho", "lambda", "mu"],
     3: ["rho", "c11", "c13", "c33", "c55", "c66"],
     4: ["rho"] + [f"c{a}{b}" for a in range(1, 7) for b in range(a, 7)],
 }
-MEDIUM_TYPES = {2: "elastic_iso", 3: "elastic_vti", 4: "elastic_aniso"}
+MEDIUM_TYPES = {1: "acoustic_iso", 2: "elastic_iso", 3: "elastic_vti", 4: "elastic_aniso"}
 
 
 def write_case(d, p, nsteps, metric="calculate", check_stability=1, snapshots=None, extra=None):
@@ -245,6 +246,7 @@ def write_layer_file(path, m: LayerModel):
 
 # Layer file types (the reference's media type numbers) and their parameters in file order
 LAYER_TYPES = {
+    10: ("acoustic_isotropic", ("rho", "vp")),
     21: ("elastic_isotropic", ("rho", "vp", "vs")),
     22: ("elastic_vti_prem", ("rho", "vph", "vpv", "vsh", "vsv", "eta")),
     23: ("elastic_vti_thomsen", ("rho", "vp0", "vs0", "epsilon", "delta", "gamma")),
@@ -257,7 +259,8 @@ LAYER_TYPES = {
 
 
 class LayerMedia:
-    """A layer file of any elastic type (read_interface_file, src/media/media_read_file.cpp:22-700):
+    """A layer file of the acoustic or any elastic type (read_interface_file,
+    src/media/media_read_file.cpp:22-700):
     interfaces top first on a uniform nx x ny mesh; `elevation` [num_interfaces, ny, nx] and
     `param` [npar, 3, num_interfaces, ny, nx]: value, gradient and power of each parameter of
     LAYER_TYPES[type], in the file's order, for the layer below each interface."""

@@ -149,6 +149,40 @@ __device__ void lame(const float var[3], float &lam, float &mu) {
   lam = (float)__dsub_rn((double)__fmul_rn(__fmul_rn(var[1], var[1]), var[0]), __dmul_rn(2.0, (double)mu));
 }
 
+// AssignLayerMediaPara2Point + CalPointValue_layer for acoustic_isotropic
+// (media_layer2model.cpp:1177-1207): rho, vp at point a (var[0], var[1]). On an interface the
+// layer above is evaluated at the same dz (the branch does not recompute it). Returns 0, or 1
+// when the point is outside the interface mesh.
+__device__ int point_value_ac(const LayerDev &m, P3 a, float var[2]) {
+  const float maxx = __fadd_rn(m.x0, __fmul_rn(m.dx, (float)(m.nx - 1)));
+  const float maxy = __fadd_rn(m.y0, __fmul_rn(m.dy, (float)(m.ny - 1)));
+  if (a.x < m.x0 || a.x > maxx || a.y < m.y0 || a.y > maxy) return 1;
+  float e[kMaxInterfaces];
+  const size_t sl = (size_t)m.nx * m.ny;
+  for (int n = 0; n < m.ni_; n++) e[n] = bilinear(m, m.elev + n * sl, a.x, a.y);
+  int mi = last_ge(a.z, e, m.ni_);
+  if (mi == -1) {  // above the top interface: the top layer's values
+    mi = last_ge(e[0], e, m.ni_);
+    for (int q = 0; q < 2; q++) var[q] = bilinear(m, m.p[3 * q] + mi * sl, a.x, a.y);
+    return 0;
+  }
+  const float dz = __fsub_rn(e[mi], a.z);
+  var[0] = layer_val(m, 0, mi, a.x, a.y, dz);
+  var[1] = layer_val(m, 1, mi, a.x, a.y, dz);
+  if ((int)dz == 0) {  // isEqual(dz, 0.0) with the integer abs()
+    const int mt = first_ge(a.z, e, m.ni_) - 1;
+    if (mt >= 0) {
+      const float rhot = layer_val(m, 0, mt, a.x, a.y, dz), vpt = layer_val(m, 1, mt, a.x, a.y, dz);
+      var[0] = (float)__ddiv_rn((double)__fadd_rn(var[0], rhot), 2.0);
+      var[1] = (float)__ddiv_rn((double)__fadd_rn(var[1], vpt), 2.0);
+    }
+  }
+  return 0;
+}
+
+// kappa = vp vp rho (float, parametrization_layer_ac_iso_loc, media_layer2model.cpp:1302-1305)
+__device__ float kappa_of(const float var[2]) { return __fmul_rn(__fmul_rn(var[1], var[1]), var[0]); }
+
 struct GridDev {
   int nx, ny, nz;  // extended grid (ghosts included)
   const float *x, *y, *z;
@@ -158,9 +192,22 @@ struct GridDev {
   int *err;
 };
 
+// AC: acoustic files (rho, vp) into rho and kappa (g.lam holds kappa)
+template <bool AC>
 __global__ void k_media_loc(const __grid_constant__ LayerDev m, const __grid_constant__ GridDev g) {
   const long long n = (long long)g.nx * g.ny * g.nz;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    if constexpr (AC) {
+      float var[2];
+      const int rc = point_value_ac(m, P3{g.x[t], g.y[t], g.z[t]}, var);
+      if (rc) {
+        atomicOr(g.err, rc);
+        continue;
+      }
+      g.lam[t] = kappa_of(var);
+      g.rho[t] = var[0];
+      continue;
+    }
     float var[3];
     const int rc = point_value(m, P3{g.x[t], g.y[t], g.z[t]}, var);
     if (rc) {
@@ -217,7 +264,9 @@ __global__ void k_mark(const __grid_constant__ LayerDev m, const __grid_constant
 
 // Equivalent medium where the 8 surrounding half-grid points fall in more than one layer
 // (parametrization_layer_el_iso_har / _ari): 9^3 sub-points of the half-grid cell.
-template <bool HAR>
+// AC: acoustic (parametrization_layer_ac_iso_har / _ari, media_layer2model.cpp:1765-1960): rho
+// arithmetically, kappa harmonically (har) or arithmetically (ari); g.lam holds kappa.
+template <bool HAR, bool AC>
 __global__ void k_media_avg(const __grid_constant__ LayerDev m, const __grid_constant__ GridDev g) {
   const long long sl = g.nx, ss = (long long)g.nx * g.ny;
   const long long n = (long long)(g.nx - 2) * (g.ny - 2) * (g.nz - 2);
@@ -252,6 +301,15 @@ __global__ void k_media_avg(const __grid_constant__ LayerDev m, const __grid_con
           const P3 lx01 = lerp(M[4], M[5], ii), lx11 = lerp(M[7], M[6], ii);
           const P3 lxy0 = lerp(lx00, lx10, jj), lxy1 = lerp(lx01, lx11, jj);
           float var[3];
+          if constexpr (AC) {
+            const int rc = point_value_ac(m, lerp(lxy0, lxy1, kk), var);
+            if (rc) { bad |= rc; continue; }
+            const float kap = kappa_of(var);
+            if (HAR) acc1 = (float)__dadd_rn((double)acc1, __ddiv_rn(1.0, (double)kap));
+            else acc1 = __fadd_rn(acc1, kap);
+            acc0 = __fadd_rn(acc0, var[0]);
+            continue;
+          }
           const int rc = point_value(m, lerp(lxy0, lxy1, kk), var);
           if (rc) { bad |= rc; continue; }
           float lam, mu;
@@ -267,6 +325,11 @@ __global__ void k_media_avg(const __grid_constant__ LayerDev m, const __grid_con
         }
     if (bad) { atomicOr(g.err, bad); continue; }
     const double nsg = (double)((kSub + 1) * (kSub + 1) * (kSub + 1));
+    if constexpr (AC) {
+      g.rho[indx] = (float)__ddiv_rn((double)acc0, nsg);
+      g.lam[indx] = HAR ? (float)__ddiv_rn(nsg, (double)acc1) : (float)__ddiv_rn((double)acc1, nsg);
+      continue;
+    }
     if (HAR) {
       const float hmu = (float)__ddiv_rn(nsg, (double)acc2);
       const float hkap = (float)__ddiv_rn(nsg, (double)acc1);
@@ -538,22 +601,17 @@ void launch_media_gen(const LayerDev &m, const GridDev &g, const OutDev &o, int 
 }  // namespace
 }  // namespace cgfd
 
-extern "C" int cgfd_media_layer_el_iso_gpu(int device, int ni, int nj, int nk, const float *coord,
-                                           const cgfd_layer_model *lm, int method, float *medium) {
-  using namespace cgfd;
-  if (!coord || !lm || !medium || ni < 4 || nj < 4 || nk < 4 || method < CGFD_MEDIA_LOC || method > CGFD_MEDIA_ARI) {
-    set_last_error("invalid argument");
-    return CGFD_ERR_INVALID;
-  }
-  if (lm->num_interfaces < 1 || lm->num_interfaces > kMaxInterfaces || lm->nx < 2 || lm->ny < 2 || !lm->elevation) {
-    set_last_error("layer model: 1 to 64 interfaces on a mesh of at least 2 x 2 points are required");
-    return CGFD_ERR_INVALID;
-  }
-  const float *hp[9] = {lm->rho, lm->rho_grad, lm->rho_pow, lm->vp, lm->vp_grad, lm->vp_pow, lm->vs, lm->vs_grad, lm->vs_pow};
-  for (const float *q : hp)
-    if (!q) { set_last_error("layer model: a parameter array is missing"); return CGFD_ERR_INVALID; }
+namespace cgfd {
+namespace {
+// The isotropic families on the GPU: elastic_isotropic files (hp: rho, vp, vs with gradient and
+// power each, 9 arrays) into rho, lambda, mu, or acoustic_isotropic files (ac; rho, vp: 6 arrays)
+// into rho, kappa; medium gets 3 or 2 fields of (ni+6)(nj+6)(nk+6) points.
+int layer_iso_family(int device, int ni, int nj, int nk, const float *coord, int num_interfaces, int mnx, int mny,
+                     float x0, float y0, float dx, float dy, const float *elevation, const float *const *hp, bool ac,
+                     int method, float *medium) {
+  const int nq = ac ? 6 : 9, nout = ac ? 2 : 3;
   const size_t nx = ni + 6, ny = nj + 6, nz = nk + 6, n = nx * ny * nz;
-  const size_t msz = (size_t)lm->num_interfaces * lm->nx * lm->ny;
+  const size_t msz = (size_t)num_interfaces * mnx * mny;
   std::vector<void *> owned;
   cudaStream_t st = nullptr;
   auto cleanup = [&] {
@@ -573,15 +631,15 @@ extern "C" int cgfd_media_layer_el_iso_gpu(int device, int ni, int nj, int nk, c
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return fail(e, "cudaSetDevice");
   if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "cudaStreamCreate");
-  LayerDev m;
-  m.ni_ = lm->num_interfaces; m.nx = lm->nx; m.ny = lm->ny;
-  m.x0 = lm->x0; m.y0 = lm->y0; m.dx = lm->dx; m.dy = lm->dy;
+  LayerDev m{};
+  m.ni_ = num_interfaces; m.nx = mnx; m.ny = mny;
+  m.x0 = x0; m.y0 = y0; m.dx = dx; m.dy = dy;
   float *dm = nullptr;
-  if ((e = dalloc(10 * msz * sizeof(float), (void **)&dm)) != cudaSuccess) return fail(e, "cudaMalloc");
-  if ((e = cudaMemcpyAsync(dm, lm->elevation, msz * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+  if ((e = dalloc((1 + nq) * msz * sizeof(float), (void **)&dm)) != cudaSuccess) return fail(e, "cudaMalloc");
+  if ((e = cudaMemcpyAsync(dm, elevation, msz * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess)
     return fail(e, "cudaMemcpy");
   m.elev = dm;
-  for (int q = 0; q < 9; q++) {
+  for (int q = 0; q < nq; q++) {
     if ((e = cudaMemcpyAsync(dm + (1 + q) * msz, hp[q], msz * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess)
       return fail(e, "cudaMemcpy");
     m.p[q] = dm + (1 + q) * msz;
@@ -591,17 +649,19 @@ extern "C" int cgfd_media_layer_el_iso_gpu(int device, int ni, int nj, int nk, c
   float *dc = nullptr, *dout = nullptr;
   int *derr = nullptr;
   if ((e = dalloc(3 * n * sizeof(float), (void **)&dc)) != cudaSuccess) return fail(e, "cudaMalloc");
-  if ((e = dalloc(3 * n * sizeof(float), (void **)&dout)) != cudaSuccess) return fail(e, "cudaMalloc");
+  if ((e = dalloc((size_t)nout * n * sizeof(float), (void **)&dout)) != cudaSuccess) return fail(e, "cudaMalloc");
   if ((e = dalloc(sizeof(int), (void **)&derr)) != cudaSuccess) return fail(e, "cudaMalloc");
   if ((e = cudaMemcpyAsync(dc, coord, 3 * n * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess)
     return fail(e, "cudaMemcpy");
   cudaMemsetAsync(derr, 0, sizeof(int), st);
   g.x = dc; g.y = dc + n; g.z = dc + 2 * n;
-  g.rho = dout; g.lam = dout + n; g.mu = dout + 2 * n;  // the medium order rho, lambda, mu
+  // the medium order: rho, lambda, mu (elastic) or rho, kappa (acoustic, kappa in g.lam)
+  g.rho = dout; g.lam = dout + n; g.mu = ac ? nullptr : dout + 2 * n;
   g.err = derr;
   g.hx = g.hy = g.hz = nullptr;
   g.mat = nullptr;
-  k_media_loc<<<148 * 8, 256, 0, st>>>(m, g);
+  if (ac) k_media_loc<true><<<148 * 8, 256, 0, st>>>(m, g);
+  else k_media_loc<false><<<148 * 8, 256, 0, st>>>(m, g);
   if (method != CGFD_MEDIA_LOC) {
     float *dh = nullptr;
     int *dmat = nullptr;
@@ -611,14 +671,20 @@ extern "C" int cgfd_media_layer_el_iso_gpu(int device, int ni, int nj, int nk, c
     g.mat = dmat;
     k_half_grid<<<148 * 8, 256, 0, st>>>(g);
     k_mark<<<148 * 8, 256, 0, st>>>(m, g);
-    if (method == CGFD_MEDIA_HAR) k_media_avg<true><<<148 * 8, 128, 0, st>>>(m, g);
-    else k_media_avg<false><<<148 * 8, 128, 0, st>>>(m, g);
+    if (method == CGFD_MEDIA_HAR) {
+      if (ac) k_media_avg<true, true><<<148 * 8, 128, 0, st>>>(m, g);
+      else k_media_avg<true, false><<<148 * 8, 128, 0, st>>>(m, g);
+    } else {
+      if (ac) k_media_avg<false, true><<<148 * 8, 128, 0, st>>>(m, g);
+      else k_media_avg<false, false><<<148 * 8, 128, 0, st>>>(m, g);
+    }
   }
   if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "media kernels");
   int herr = 0;
   if ((e = cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
     return fail(e, "cudaMemcpy");
-  if ((e = cudaMemcpyAsync(medium, dout, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+  if ((e = cudaMemcpyAsync(medium, dout, (size_t)nout * n * sizeof(float), cudaMemcpyDeviceToHost, st)) !=
+      cudaSuccess)
     return fail(e, "cudaMemcpy");
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail(e, "cudaStreamSynchronize");
   cleanup();
@@ -628,6 +694,26 @@ extern "C" int cgfd_media_layer_el_iso_gpu(int device, int ni, int nj, int nk, c
     return CGFD_ERR_INVALID;
   }
   return CGFD_OK;
+}
+}  // namespace
+}  // namespace cgfd
+
+extern "C" int cgfd_media_layer_el_iso_gpu(int device, int ni, int nj, int nk, const float *coord,
+                                           const cgfd_layer_model *lm, int method, float *medium) {
+  using namespace cgfd;
+  if (!coord || !lm || !medium || ni < 4 || nj < 4 || nk < 4 || method < CGFD_MEDIA_LOC || method > CGFD_MEDIA_ARI) {
+    set_last_error("invalid argument");
+    return CGFD_ERR_INVALID;
+  }
+  if (lm->num_interfaces < 1 || lm->num_interfaces > kMaxInterfaces || lm->nx < 2 || lm->ny < 2 || !lm->elevation) {
+    set_last_error("layer model: 1 to 64 interfaces on a mesh of at least 2 x 2 points are required");
+    return CGFD_ERR_INVALID;
+  }
+  const float *hp[9] = {lm->rho, lm->rho_grad, lm->rho_pow, lm->vp, lm->vp_grad, lm->vp_pow, lm->vs, lm->vs_grad, lm->vs_pow};
+  for (const float *q : hp)
+    if (!q) { set_last_error("layer model: a parameter array is missing"); return CGFD_ERR_INVALID; }
+  return layer_iso_family(device, ni, nj, nk, coord, lm->num_interfaces, lm->nx, lm->ny, lm->x0, lm->y0, lm->dx, lm->dy,
+                          lm->elevation, hp, false, method, medium);
 }
 
 extern "C" int cgfd_media_layer_gpu(int device, int ni, int nj, int nk, const float *coord, const cgfd_layer_media *lm,
@@ -643,6 +729,18 @@ extern "C" int cgfd_media_layer_gpu(int device, int ni, int nj, int nk, const fl
     return CGFD_ERR_INVALID;
   }
   const int T = lm->type;
+  // acoustic_isotropic files into acoustic media (media_layer2model_ac_iso, media_layer2model.cpp:70-118)
+  if (T == CGFD_LAYER_ACOUSTIC_ISO || medium_type == CGFD_MEDIUM_ACOUSTIC_ISO) {
+    if (T != CGFD_LAYER_ACOUSTIC_ISO || medium_type != CGFD_MEDIUM_ACOUSTIC_ISO) {
+      set_last_error("layer file type not usable for this medium type");
+      return CGFD_ERR_INVALID;
+    }
+    const size_t lv = (size_t)lm->num_interfaces * lm->nx * lm->ny;
+    const float *hp[6];
+    for (int q = 0; q < 6; q++) hp[q] = lm->param + (size_t)q * lv;  // rho, rho_grad, rho_pow, vp, vp_grad, vp_pow
+    return layer_iso_family(device, ni, nj, nk, coord, lm->num_interfaces, lm->nx, lm->ny, lm->x0, lm->y0, lm->dx,
+                            lm->dy, lm->elevation, hp, true, method, medium);
+  }
   // the file types each target medium accepts (media_layer2model_el_iso / _el_vti / _el_aniso)
   const bool ok = (medium_type == CGFD_MEDIUM_ELASTIC_ISO && T == CGFD_LAYER_ELASTIC_ISO) ||
                   (medium_type == CGFD_MEDIUM_ELASTIC_VTI && T >= CGFD_LAYER_VTI_PREM && T <= CGFD_LAYER_VTI_CIJ) ||

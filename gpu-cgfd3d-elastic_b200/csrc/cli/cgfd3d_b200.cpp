@@ -4,10 +4,11 @@
 // for the elastic time-loop path on one GPU: reads the same parameter file keys, grid /
 // metric / medium NetCDF files, .src source file and station list, checks the time step
 // (FP64), runs the B200 time loop through the C ABI and writes the same SAC files
-// (<output_dir>/<station>.<Vx..Txy>.sac, plus <station>.E**.sac strain for isotropic media),
-// and with a free surface the peak ground motion file PG_V_A_D_px0_py0_pz0.nc.
-// Options outside this path (MPI decomposition, media discretisation, slices, ablexp,
-// acoustic / visco-elastic media) are rejected with a message.
+// (<output_dir>/<station>.<Vx..Txy>.sac, plus <station>.E**.sac strain for isotropic media;
+// <station>.<Vx Vy Vz P>.sac for acoustic media), line receivers, slices and snapshots, and
+// with a free surface the peak ground motion file PG_V_A_D_px0_py0_pz0.nc. Media come from
+// media_*.nc files or layer files discretised on the GPU. Options outside this path (MPI
+// decomposition, ablexp, visco-elastic media) are rejected with a message.
 #include <sys/stat.h>
 
 #include <algorithm>
@@ -31,6 +32,11 @@ namespace {
 
 const char *kFnamePart = "px0_py0_pz0";  // blk_set_output (blk_t.cu:54) for one rank
 const char *kCmpNames[9] = {"Vx", "Vy", "Vz", "Txx", "Tyy", "Tzz", "Tyz", "Txz", "Txy"};
+// Output components of the medium (wav_init / wav_ac_init, wav_t.cu:14-250): the 9 elastic
+// ones, or Vx Vy Vz P for acoustic media (P in the device's Txx slot).
+const char *kAcNames[4] = {"Vx", "Vy", "Vz", "P"};
+int g_ncmp = 9;
+const char *const *g_names = kCmpNames;
 
 [[noreturn]] void fail(const std::string &m) { throw std::runtime_error(m); }
 
@@ -120,8 +126,13 @@ void open_snapshot(Snap &s, const std::string &out) {
   };
   var("time", true);
   if (s.vel == 1) for (const char *n : {"Vx", "Vy", "Vz"}) var(n, false);
-  if (s.stress == 1) for (const char *n : {"Txx", "Tyy", "Tzz", "Txz", "Tyz", "Txy"}) var(n, false);
-  if (s.strain == 1) for (const char *n : {"Exx", "Eyy", "Ezz", "Exz", "Eyz", "Exy"}) var(n, false);
+  if (g_ncmp == 4) {  // acoustic (io_snap_nc_create_ac, io_funcs.cu:1258-1350): the pressure as "Tii"
+    if (s.strain == 1) fail("snapshot strain of acoustic media is not computed (io_snap_nc_put_ac leaves it unwritten)");
+    if (s.stress == 1) var("Tii", false);
+  } else {
+    if (s.stress == 1) for (const char *n : {"Txx", "Tyy", "Tzz", "Txz", "Tyz", "Txy"}) var(n, false);
+    if (s.strain == 1) for (const char *n : {"Exx", "Eyy", "Ezz", "Exz", "Eyz", "Exy"}) var(n, false);
+  }
   f.gatts.push_back({"first_index_to_snapshot_output", cgfd::nc::INT,
                      {(double)s.first_in_nc[0], (double)s.first_in_nc[1], (double)s.first_in_nc[2]}, ""});
   f.gatts.push_back({"first_index_in_this_thread_with_ghosts", cgfd::nc::INT,
@@ -148,7 +159,8 @@ void put_snapshot(Snap &s, cgfd_problem *p, const Grid &g, const std::vector<flo
   for (int q = 0; q < 9; q++) c[q] = box.data() + q * n;
   std::vector<const float *> data = {&time};
   if (s.vel == 1) data.insert(data.end(), {c[0], c[1], c[2]});
-  if (s.stress == 1) data.insert(data.end(), {c[3], c[4], c[5], c[7], c[6], c[8]});
+  if (s.stress == 1 && g_ncmp == 4) data.push_back(c[3]);  // acoustic: P (io_snap_nc_put_ac)
+  else if (s.stress == 1) data.insert(data.end(), {c[3], c[4], c[5], c[7], c[6], c[8]});
   std::vector<float> E;
   if (s.strain == 1) {
     if (!iso) fail("snapshot strain is computed for elastic_iso media only (io_snap_stress_to_strain_eliso)");
@@ -204,7 +216,8 @@ std::vector<LinePoint> parse_lines(const Value *lv, const Grid &g) {
 // The x / y / z slices of the "slice" entry inside the grid (io_slice_locate,
 // io_funcs.cu:418-528), each a NetCDF file of record variables on an unlimited time dimension
 // (io_slice_nc_create, io_funcs.cu:531-664): slicex_i<gi+1>_<part>.nc with dims (time, k, j),
-// slicey_j<gj+1> (time, k, i), slicez_k<gk+1> (time, j, i); variable "time" and the 9 components.
+// slicey_j<gj+1> (time, k, i), slicez_k<gk+1> (time, j, i); variable "time" and the medium's
+// components (9 elastic, 4 acoustic).
 struct Slices {
   std::vector<int> idx[3];
   std::vector<std::unique_ptr<cgfd::nc::RecordWriter>> files[3];
@@ -233,9 +246,9 @@ Slices open_slices(const Value *sv, const Grid &g, const std::string &out) {
       tv.name = "time";
       tv.dimids = {0};
       f.vars.push_back(tv);
-      for (int c = 0; c < 9; c++) {
+      for (int c = 0; c < g_ncmp; c++) {
         cgfd::nc::Var v3;
-        v3.name = kCmpNames[c];
+        v3.name = g_names[c];
         v3.dimids = {0, 1, 2};
         f.vars.push_back(v3);
       }
@@ -259,7 +272,7 @@ void put_slices(Slices &S, cgfd_problem *p, const Grid &g, int it, float time, s
   for (int a = 0; a < 3; a++)
     for (size_t s = 0; s < S.idx[a].size(); s++) {
       std::vector<const float *> data = {&time};
-      for (int c = 0; c < 9; c++) data.push_back(buf.data() + off + c * plane[a]);
+      for (int c = 0; c < g_ncmp; c++) data.push_back(buf.data() + off + c * plane[a]);
       S.files[a][s]->append(data);
       off += 9 * plane[a];
     }
@@ -369,14 +382,19 @@ int run(int argc, char **argv) {
   const Value &md = need(par, "medium");
   std::string type = need(md, "type").as_str();
   std::vector<std::string> mnames;
-  if (type == "elastic_iso") { d.medium_type = CGFD_MEDIUM_ELASTIC_ISO; mnames = {"rho", "lambda", "mu"}; }
+  if (type == "acoustic_iso") {
+    d.medium_type = CGFD_MEDIUM_ACOUSTIC_ISO;
+    mnames = {"rho", "kappa"};
+    g_ncmp = 4;
+    g_names = kAcNames;
+  } else if (type == "elastic_iso") { d.medium_type = CGFD_MEDIUM_ELASTIC_ISO; mnames = {"rho", "lambda", "mu"}; }
   else if (type == "elastic_vti") { d.medium_type = CGFD_MEDIUM_ELASTIC_VTI; mnames = {"rho", "c11", "c13", "c33", "c55", "c66"}; }
   else if (type == "elastic_aniso") {
     d.medium_type = CGFD_MEDIUM_ELASTIC_ANISO;
     mnames = {"rho"};
     for (int a = 1; a <= 6; a++)
       for (int b = a; b <= 6; b++) mnames.push_back("c" + std::to_string(a) + std::to_string(b));
-  } else fail("medium type '" + type + "' is not on this path (elastic_iso/vti/aniso)");
+  } else fail("medium type '" + type + "' is not on this path (acoustic_iso, elastic_iso/vti/aniso)");
   std::string way = need(md, "input_way").as_str();
   std::vector<float> medium(mnames.size() * g.siz, 0.f);
   if (way == "import") {
@@ -501,8 +519,8 @@ int run(int argc, char **argv) {
     for (size_t r = 0; r < lines.size(); r++) {
       const LinePoint &l = lines[r];
       const size_t c0 = g.at(l.i, l.j, l.k);
-      for (int c = 0; c < 9; c++)
-        cgfd::fmt::write_sac(out + "/" + l.line + ".no" + std::to_string(l.seq) + "." + kCmpNames[c] + ".sac",
+      for (int c = 0; c < g_ncmp; c++)
+        cgfd::fmt::write_sac(out + "/" + l.line + ".no" + std::to_string(l.seq) + "." + g_names[c] + ".sac",
                              &ls[(r * 9 + c) * nt_total], nt_total, (float)dt, coord[c0], coord[g.siz + c0],
                              coord[2 * g.siz + c0], (float)dt);
     }
@@ -546,8 +564,8 @@ int run(int argc, char **argv) {
     float x = coord[c0], y = coord[g.siz + c0], z = coord[2 * g.siz + c0];
     const std::string &name = stf.names[idx[r]];
     float *tr = &seis[(size_t)r * 9 * nt_total];
-    for (int c = 0; c < 9; c++)
-      cgfd::fmt::write_sac(out + "/" + name + "." + kCmpNames[c] + ".sac", tr + (size_t)c * nt_total, nt_total,
+    for (int c = 0; c < g_ncmp; c++)
+      cgfd::fmt::write_sac(out + "/" + name + "." + g_names[c] + ".sac", tr + (size_t)c * nt_total, nt_total,
                            (float)dt, x, y, z, (float)dt);
     if (d.medium_type == CGFD_MEDIUM_ELASTIC_ISO) {
       // strain from stress in place (io_recv_output_sac_el_iso_strain, io_funcs.cu:1821-1902)

@@ -158,6 +158,7 @@ LayerFile read_layer_file(const std::string &path) {
   std::string type;
   if (!(body >> type)) throw std::runtime_error(path + ": no media type");
   static const struct { const char *name; int type, npar; } kTypes[] = {
+      {"acoustic_isotropic", CGFD_LAYER_ACOUSTIC_ISO, 2},
       {"elastic_isotropic", CGFD_LAYER_ELASTIC_ISO, 3},  {"elastic_vti_prem", CGFD_LAYER_VTI_PREM, 6},
       {"elastic_vti_thomsen", CGFD_LAYER_VTI_THOMSEN, 6}, {"elastic_vti_cij", CGFD_LAYER_VTI_CIJ, 6},
       {"elastic_tti_thomsen", CGFD_LAYER_TTI_THOMSEN, 8}, {"elastic_tti_bond", CGFD_LAYER_TTI_BOND, 8},
@@ -165,7 +166,7 @@ LayerFile read_layer_file(const std::string &path) {
   for (const auto &t : kTypes)
     if (type == t.name) { L.type = t.type; L.npar = t.npar; }
   if (!L.type)
-    throw std::runtime_error(path + ": media type '" + type + "' is not on this path (the elastic types)");
+    throw std::runtime_error(path + ": media type '" + type + "' is not on this path (acoustic and elastic types)");
   if (!(body >> L.ni) || L.ni < 1) throw std::runtime_error(path + ": number of interfaces missing or < 1");
   if (!(body >> L.nx >> L.ny >> L.x0 >> L.y0 >> L.dx >> L.dy) || L.nx < 2 || L.ny < 2)
     throw std::runtime_error(path + ": interface mesh line must be NX NY MINX MINY DX DY with NX, NY >= 2");

@@ -490,9 +490,11 @@ int cgfd_media_layer_el_iso_gpu(int device, int ni, int nj, int nk, const float 
                                 int method, float *medium);
 
 /*
- * Layer files of every elastic media type (read_interface_file, media_read_file.cpp:22-560),
- * by the reference's type numbers; the parameters of each, in the file's order:
+ * Layer files of the acoustic and every elastic media type (read_interface_file,
+ * media_read_file.cpp:22-560), by the reference's type numbers; the parameters of each, in the
+ * file's order:
  */
+#define CGFD_LAYER_ACOUSTIC_ISO  10  /* rho vp (into CGFD_MEDIUM_ACOUSTIC_ISO: rho, kappa)     */
 #define CGFD_LAYER_ELASTIC_ISO   21  /* rho vp vs                                              */
 #define CGFD_LAYER_VTI_PREM      22  /* rho vph vpv vsh vsv eta                                */
 #define CGFD_LAYER_VTI_THOMSEN   23  /* rho vp0 vs0 epsilon delta gamma                        */
@@ -512,7 +514,9 @@ typedef struct cgfd_layer_media {
 
 /*
  * Media discretisation of any layer file on the GPU `device` into the cgfd_problem_desc medium
- * of medium_type (CGFD_MEDIUM_ELASTIC_*): iso from an elastic_isotropic file (as
+ * of medium_type: acoustic [rho kappa] from an acoustic_isotropic file (kappa = vp vp rho; har
+ * averages kappa harmonically, ari arithmetically, rho arithmetically: media_layer2model_ac_iso,
+ * media_layer2model.cpp:70-118, 1263-1310, 1765-1960); iso from an elastic_isotropic file (as
  * cgfd_media_layer_el_iso_gpu); VTI [rho c11 c13 c33 c55 c66] from the three VTI files; 21-Cij
  * [rho c11 c12 ... c66] from any of the seven (iso and VTI files expanded to the full tensor).
  * method CGFD_MEDIA_LOC / _HAR / _ARI; har and ari average every c_ij harmonically /

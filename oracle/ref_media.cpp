@@ -13,6 +13,13 @@ extern "C" int ref_media_layer2model_el_iso(float *lam3d, float *mu3d, float *rh
   return media_layer2model_el_iso(lam3d, mu3d, rho3d, x3d, y3d, z3d, nx, ny, nz, GRID_CURV, in_3lay_file, method, 1);
 }
 
+// media_layer2model_ac_iso (media_layer2model.cpp:70-118): rho, kappa
+extern "C" int ref_media_layer2model_ac_iso(float *rho3d, float *kappa3d, const float *x3d, const float *y3d,
+                                            const float *z3d, size_t nx, size_t ny, size_t nz, const char *in_3lay_file,
+                                            const char *method) {
+  return media_layer2model_ac_iso(rho3d, kappa3d, x3d, y3d, z3d, nx, ny, nz, GRID_CURV, in_3lay_file, method, 1);
+}
+
 // media_layer2model_el_vti (media_layer2model.cpp:173-228): rho, c11, c33, c55, c66, c13
 extern "C" int ref_media_layer2model_el_vti(float *rho, float *c11, float *c33, float *c55, float *c66, float *c13,
                                             const float *x3d, const float *y3d, const float *z3d, size_t nx,

@@ -36,16 +36,24 @@ def layer2model_el_iso(coord, model, method=0):
 
 
 def layer2model(coord, model, medium_type, method=0):
-    """The medium of medium_type (2 iso [rho lambda mu], 3 VTI [rho c11 c13 c33 c55 c66], 4 21-Cij
-    [rho c11 ... c66]) from the layer file model (formats.LayerMedia) by the reference's
-    media_layer2model_el_iso / _el_vti / _el_aniso on the grid coord."""
+    """The medium of medium_type (1 acoustic [rho kappa], 2 iso [rho lambda mu], 3 VTI [rho c11 c13
+    c33 c55 c66], 4 21-Cij [rho c11 ... c66]) from the layer file model (formats.LayerMedia) by the
+    reference's media_layer2model_ac_iso / _el_iso / _el_vti / _el_aniso on the grid coord."""
     L = C.CDLL(LIB)
     _, nz, ny, nx = coord.shape
     c = np.ascontiguousarray(coord, np.float32)
     with tempfile.TemporaryDirectory() as d:
         path = os.path.join(d, "model.lay")
         formats.write_layer_media_file(path, model)
-        if medium_type == 2:
+        if medium_type == 1:
+            fn = L.ref_media_layer2model_ac_iso
+            fn.restype = C.c_int
+            fn.argtypes = [C.c_void_p] * 5 + [C.c_size_t] * 3 + [C.c_char_p, C.c_char_p]
+            rho, kappa = (np.zeros((nz, ny, nx), np.float32) for _ in range(2))
+            rc = fn(rho.ctypes.data, kappa.ctypes.data, c[0].ctypes.data, c[1].ctypes.data, c[2].ctypes.data,
+                    nx, ny, nz, path.encode(), METHODS[method])
+            out = np.stack([rho, kappa])
+        elif medium_type == 2:
             fn = L.ref_media_layer2model_el_iso
             fn.restype = C.c_int
             fn.argtypes = [C.c_void_p] * 6 + [C.c_size_t] * 3 + [C.c_char_p, C.c_char_p]

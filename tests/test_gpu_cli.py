@@ -142,18 +142,20 @@ def test_cli_layered_medium_matches_oracle(tmp_path):
     assert per_station_rel_l2(got, ref) <= 1e-4
 
 
-@pytest.mark.parametrize("mtype,ftype,method", [("elastic_vti", 23, "ari"), ("elastic_aniso", 26, "loc")])
+@pytest.mark.parametrize("mtype,ftype,method", [("elastic_vti", 23, "ari"), ("elastic_aniso", 26, "loc"),
+                                               ("acoustic_iso", 10, "har")])
 def test_cli_layered_anisotropic_medium_matches_oracle(tmp_path, mtype, ftype, method):
-    """infile_layer for the anisotropic media: a Thomsen VTI layer file into a VTI medium (ari
-    equivalent medium) and a Bond-rotated TI file into a 21-Cij medium. The CLI discretises the
-    file on the GPU; its seismograms equal the oracle's run on the medium the reference's own
-    media code builds from the same file (per-station rel L2 <= 1e-4)."""
+    """infile_layer for the anisotropic and acoustic media: a Thomsen VTI layer file into a VTI
+    medium (ari equivalent medium), a Bond-rotated TI file into a 21-Cij medium, an
+    acoustic_isotropic file into an acoustic medium (har). The CLI discretises the file on the
+    GPU; its seismograms equal the oracle's run on the medium the reference's own media code
+    builds from the same file (per-station rel L2 <= 1e-4; acoustic: per group Vx Vy Vz / P)."""
     import media_ref
     if not media_ref.available():
         pytest.skip("oracle/_ref/libref_media.so not built")
     from cgfd_b200 import synth
     nsteps = 60
-    med = {"elastic_vti": "vti", "elastic_aniso": "aniso"}[mtype]
+    med = {"elastic_vti": "vti", "elastic_aniso": "aniso", "acoustic_iso": "ac"}[mtype]
     p = small_problem(med, nsteps=nsteps)
     model = synth.layer_media(p.coord, ftype, seed=4, depths=(-1200.0, -2200.0))
     lay = os.path.join(str(tmp_path), "model.lay")
@@ -164,15 +166,60 @@ def test_cli_layered_anisotropic_medium_matches_oracle(tmp_path, mtype, ftype, m
     r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     p.metric = synth.metrics(p.coord)
-    p.medium = media_ref.layer2model(p.coord, model, {"elastic_vti": 3, "elastic_aniso": 4}[mtype],
+    p.medium = media_ref.layer2model(p.coord, model, {"elastic_vti": 3, "elastic_aniso": 4, "acoustic_iso": 1}[mtype],
                                      {"loc": 0, "har": 1, "ari": 2}[method])
     orc = Oracle(p)
     orc.run()
     ref = orc.seismograms()
     out = os.path.join(str(tmp_path), "output")
     got = np.zeros_like(ref)
+    cmps = ["Vx", "Vy", "Vz", "P"] if med == "ac" else CMPS
     for n, name in enumerate(p.sta.names):
-        for c, cn in enumerate(CMPS):
+        for c, cn in enumerate(cmps):
             got[n, c] = formats.read_sac(os.path.join(out, f"{name}.{cn}.sac"))[1]
     assert np.abs(ref).max() > 0
-    assert per_station_rel_l2(got, ref) <= 1e-4
+    if med == "ac":
+        assert per_station_rel_l2(got[:, :3], ref[:, :3]) <= 1e-4
+        assert per_station_rel_l2(got[:, 3:4], ref[:, 3:4]) <= 1e-4
+    else:
+        assert per_station_rel_l2(got, ref) <= 1e-4
+
+
+def test_cli_acoustic_medium_matches_oracle(tmp_path):
+    """An acoustic_iso par file (media_*.nc with rho and kappa): SAC files of Vx Vy Vz P per
+    station (wav_ac_init's components) against the oracle, a z slice with the 4 components and
+    a snapshot whose stress group is the pressure "Tii" (io_snap_nc_create_ac)."""
+    nsteps = 60
+    p = small_problem("ac", nsteps=nsteps, nsrc=2)
+    snaps = [{"name": "below", "grid_index_start": [1, 1, p.nk - 1], "grid_index_count": [p.ni, p.nj, 1],
+              "grid_index_incre": [1, 1, 1], "time_index_start": 0, "time_index_incre": 20,
+              "save_velocity": 1, "save_stress": 1, "save_strain": 0}]
+    par = formats.write_case(str(tmp_path), p, nsteps, metric="import", snapshots=snaps,
+                             extra={"slice": {"z_index": [p.nk - 5]}})
+    r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    orc = Oracle(p)
+    orc.run()
+    ref = orc.seismograms()
+    out = os.path.join(str(tmp_path), "output")
+    got = np.zeros_like(ref)
+    for n, name in enumerate(p.sta.names):
+        for c, cn in enumerate(["Vx", "Vy", "Vz", "P"]):
+            hdr, data = formats.read_sac(os.path.join(out, f"{name}.{cn}.sac"))
+            assert hdr["npts"] == p.nt_total
+            got[n, c] = data
+        assert not os.path.exists(os.path.join(out, f"{name}.Txx.sac"))
+    assert per_station_rel_l2(got[:, :3], ref[:, :3]) <= 1e-4
+    assert per_station_rel_l2(got[:, 3:4], ref[:, 3:4]) <= 1e-4
+    from scipy.io import netcdf_file
+    with netcdf_file(os.path.join(out, f"slicez_k{p.nk - 5}_px0_py0_pz0.nc"), "r", mmap=False) as f:
+        assert [v for v in f.variables if v != "time"] == ["Vx", "Vy", "Vz", "P"]
+        assert f.variables["P"][:].shape[1:] == (p.nj, p.ni)
+    with netcdf_file(os.path.join(out, "below_px0_py0_pz0.nc"), "r", mmap=False) as f:
+        assert sorted(v for v in f.variables if v != "time") == ["Tii", "Vx", "Vy", "Vz"]
+        # the state at the start of step 40 = the oracle's after 40 steps
+        o40 = Oracle(p)
+        o40.run(40)
+        w = o40.wavefield()
+        tii = f.variables["Tii"][2]
+        assert np.linalg.norm(tii[0] - w[3, -5, 3:-3, 3:-3]) <= 1e-4 * np.linalg.norm(w[3, -5, 3:-3, 3:-3])

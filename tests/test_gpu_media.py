@@ -38,8 +38,9 @@ def test_gpu_media_rejects_points_outside_the_mesh():
     assert e.value.code == -1
 
 
-# (layer file type, target medium type): VTI files into VTI media, every file type into 21-Cij
-CASES = [(22, 3), (23, 3), (24, 3), (21, 4), (23, 4), (25, 4), (26, 4), (27, 4)]
+# (layer file type, target medium type): acoustic files into acoustic media, VTI files into VTI
+# media, every elastic file type into 21-Cij
+CASES = [(10, 1), (22, 3), (23, 3), (24, 3), (21, 4), (23, 4), (25, 4), (26, 4), (27, 4)]
 
 
 @pytest.mark.parametrize("method", [0, 1, 2])
@@ -84,3 +85,7 @@ def test_gpu_layer_media_rejects_wrong_file_type():
     with pytest.raises(CgfdError) as e:
         media_layer_any_gpu(coord, synth.layer_media(coord, 25, seed=9), 3, 0)  # a TTI file into a VTI medium
     assert e.value.code == -1
+    for ftype, medium in ((10, 2), (21, 1)):  # acoustic files only into acoustic media, and back
+        with pytest.raises(CgfdError) as e:
+            media_layer_any_gpu(coord, synth.layer_media(coord, ftype, seed=9), medium, 0)
+        assert e.value.code == -1
