@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--shots", type=int, default=1, help="profiling case: shots of a batched problem")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "u16coef", "fp16wave", "fp64"],
                     help="profiling case: storage precision")
+    ap.add_argument("--medium", default="iso", choices=["iso", "ac"],
+                    help="profiling case: elastic iso or acoustic medium (the same layers' vp and rho)")
     return ap.parse_args()
 
 
@@ -89,8 +91,9 @@ def profile_run(args):
                    "fp64": CGFD_PREC_FP64}[args.precision]
     if args.shots > 1:
         rng = np.random.default_rng(78)
-        shots = [synth.dc_sources(p.coord, p.ni, p.nj, 1, rng, depth_range=(1000.0, 3000.0), fc_range=(2.0, 5.0),
-                                  stf_length=p.nt_total * p.dt) for _ in range(args.shots)]
+        mk = synth.ac_sources if args.medium == "ac" else synth.dc_sources
+        shots = [mk(p.coord, p.ni, p.nj, 1, rng, depth_range=(1000.0, 3000.0), fc_range=(2.0, 5.0),
+                    stf_length=p.nt_total * p.dt) for _ in range(args.shots)]
         sim = Simulation(p, shots=shots)
     else:
         sim = Simulation(p)
@@ -101,9 +104,10 @@ def profile_run(args):
         n = [p.ni, p.nj, p.nk]
         n[slots[f][0]] = nl + 1
         pts += n[0] * n[1] * n[2]
-    print(f"profile case {p.ni}x{p.nj}x{p.nk} faces={names or 'none'} layers={nl} shots={args.shots} "
-          f"precision={args.precision}: {args.profile_steps} steps, face points {pts}, "
-          f"bulk cells {p.ni * p.nj * (p.nk - 4)}", flush=True)
+    bulk = p.ni * p.nj * (p.nk if args.medium == "ac" or not p.free_top else p.nk - 4)
+    print(f"profile case {p.ni}x{p.nj}x{p.nk} medium={args.medium} faces={names or 'none'} layers={nl} "
+          f"shots={args.shots} precision={args.precision}: {args.profile_steps} steps, face points {pts}, "
+          f"bulk cells {bulk}", flush=True)
     sim.close()
     return 0
 
@@ -137,7 +141,8 @@ def build_problem(args, device=0, nk_override=None):
         ni, nj, nk = args.grid
     if nk_override:
         nk = nk_override
-    p = synth.make_problem(ni, nj, nk, dh, nsteps, dt=None, medium="iso", npml=npml, nsrc=1, sta_grid=(sx, sy),
+    p = synth.make_problem(ni, nj, nk, dh, nsteps, dt=None, medium=getattr(args, "medium", "iso"), npml=npml,
+                           nsrc=1, sta_grid=(sx, sy),
                            fc=fc, seed=2024, perturb_std=pert, corr=1000.0, hurst=0.3,
                            src_depth=(2000.0, 2000.0), center_src=True)
     p.device = device
@@ -506,6 +511,8 @@ def run_reference(args):
 
 def main():
     args = parse()
+    if args.medium != "iso" and args.profile_steps <= 0:
+        raise SystemExit("--medium applies to the profiling case (--profile-steps); the bench line is the iso workload")
     if args.impl == "reference":
         return run_reference(args)
     if args.profile_steps > 0:

@@ -16,6 +16,7 @@
 
 #include "cgfd_dev.cuh"
 #include "cgfd_launch.h"
+#include "cgfd_tma.cuh"
 
 namespace cgfd {
 
@@ -268,6 +269,260 @@ __global__ void __launch_bounds__(TX *TY, AcTile<R>::MINB)
     }
     __syncthreads();  // the next chunk's first plane reuses buffer kb & 1
   }
+}
+
+// -----------------------------------------------------------------------------------------
+// TMA-pipelined form (FP32): thread 0 streams, with mbarrier completion and one plane ahead of the
+// computation, the stage input of one plane with its x-y halo (4 fields, one 4-D box of
+// 40 x (TYT+4) x 1 x 4, x halo 16 bytes on both sides for the TMA alignment) into a 3-slot ring,
+// and the 11 coefficients plus the w_pre / w_end values the RK combine reads (centre boxes) into
+// a 2-slot ring. The z march runs upwards for backward z operators and downwards for forward
+// ones, so that the one-sided operator needs exactly one plane ahead: the current plane and the
+// one ahead come from the ring, the 3 planes behind from a per-thread register queue. The
+// stage-input map covers the physical cells and the 3 ghost planes above the top (the pressure
+// image); the halo beyond the grid's sides and bottom is zero fill, as the ghosts hold 0 there.
+// -----------------------------------------------------------------------------------------
+struct AcSmem {
+  static constexpr int TYT = TY;
+  static constexpr int XO = 4;             // x halo of the box: 16 bytes of floats
+  static constexpr int WX = TX + 2 * XO;   // x box [-XO, 32+XO) around the tile
+  static constexpr int WY = TYT + 4;       // y box [-1, TYT+3) (forward) or [-3, TYT+1) (backward)
+  static constexpr int CELLS = TX * TYT;
+  static constexpr int WAVE_ELEMS = kAcF * WY * WX;
+  static constexpr int WAVE_SLOT = ((WAVE_ELEMS * 4 + 127) / 128) * 128;  // bytes
+  static constexpr int COEF_BYTES = 11 * CELLS * 4;
+  static constexpr int FLD_BYTES = kAcF * CELLS * 4;
+  static constexpr int OFF_PRE = COEF_BYTES, OFF_END = COEF_BYTES + FLD_BYTES;  // within a cpe slot
+  static constexpr int CPE_SLOT = COEF_BYTES + 2 * FLD_BYTES;
+  static constexpr int NW = 3;  // wave ring slots: this plane, the one ahead, one in flight
+  static constexpr int OFF_CPE = NW * WAVE_SLOT;
+  static constexpr int OFF_BAR = OFF_CPE + 2 * CPE_SLOT;
+  static constexpr int BYTES = OFF_BAR + 8 * 8;
+  static constexpr int MINB = 3;
+  static_assert(COEF_BYTES % 128 == 0 && FLD_BYTES % 128 == 0, "TMA destinations stay 128-byte aligned");
+  static_assert(MINB * (BYTES + 1024) <= 228 * 1024, "MINB blocks must fit one SM's shared memory");
+};
+
+template <int DX, int DY, int DZ>
+__global__ void __launch_bounds__(TX *AcSmem::TYT, AcSmem::MINB)
+    k_stage_ac_tma(const __grid_constant__ StageP p, const __grid_constant__ TmaP tm, int nzc, int nchunk) {
+  using S = AcSmem;
+  constexpr int TYT = S::TYT;
+  constexpr int LX = op_left(DX), LY = op_left(DY);
+  constexpr int SD = DZ ? -1 : 1;  // march direction
+  extern __shared__ __align__(128) unsigned char smem[];
+  float *wave = reinterpret_cast<float *>(smem);
+  unsigned char *cpe = smem + S::OFF_CPE;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + S::OFF_BAR);  // NW wave, then 2 cpe
+
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int bx = blockIdx.x, by = blockIdx.y;
+  const int shot = blockIdx.z / nchunk, kb = (blockIdx.z % nchunk) * nzc;
+  const int ke = min(kb + nzc, p.nk);
+  if (kb >= ke) return;
+  const int n = ke - kb;
+  const int i = bx * TX + tx, j = by * TYT + ty;
+  const bool act = i < p.ni && j < p.nj;
+  const int k0 = SD > 0 ? kb : ke - 1;
+  const long long sf = p.sf;
+  const long long woff = (long long)shot * 9 * sf;
+  const float *__restrict__ cur = p.cur + woff;
+  float *__restrict__ tmp_out = p.tmp_out ? p.tmp_out + woff : nullptr;
+  float *__restrict__ endw = p.end + woff;
+  const int stage = p.stage;
+  const bool need_pre = stage == 1 || stage == 2;
+  const bool need_end = stage >= 1;
+  const uint32_t wave_bytes = S::WAVE_ELEMS * 4;
+  const uint32_t cpe_bytes = S::COEF_BYTES + (need_pre ? S::FLD_BYTES : 0) + (need_end ? S::FLD_BYTES : 0);
+  // box origins (x a multiple of 4 floats): the stage-input map counts physical cells from
+  // (0, 0, 0); the centre-box maps count device-layout (padded) coordinates
+  const int xw = bx * TX - S::XO, yw = by * TYT - LY;  // box row r = tile row r - LY
+  const int xc = GX + bx * TX, yc = 3 + by * TYT;
+
+  if (tid == 0) {
+    for (int b = 0; b < S::NW + 2; b++) mbar_init(&bar[b], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  auto issue_wave = [&](int m) {
+    const int kk = k0 + m * SD;
+    uint64_t *b = &bar[m % S::NW];
+    mbar_expect_tx(b, wave_bytes);
+    tma_load_4d(wave + (m % S::NW) * (S::WAVE_SLOT / 4), &tm.cur, xw, yw, kk, 9 * shot, b);
+  };
+  auto issue_cpe = [&](int m) {
+    const int kk = k0 + m * SD;
+    const int sl = m & 1;
+    uint64_t *b = &bar[S::NW + sl];
+    unsigned char *base = cpe + sl * S::CPE_SLOT;
+    mbar_expect_tx(b, cpe_bytes);
+    tma_load_4d(base, &tm.coef, xc, yc, kk + 3, 0, b);
+    if (need_pre) tma_load_4d(base + S::OFF_PRE, &tm.pre, xc, yc, kk + 3, 9 * shot, b);
+    if (need_end) tma_load_4d(base + S::OFF_END, &tm.end, xc, yc, kk + 3, 9 * shot, b);
+  };
+  if (tid == 0) {
+    for (int m = 0; m + 1 < S::NW && m <= n; m++) issue_wave(m);  // planes 0..n exist
+    issue_cpe(0);
+  }
+
+  // PML faces that intersect this block (uniform)
+  unsigned fmask = 0;
+  for (int fi = 0; fi < p.nface; fi++) {
+    const FaceP &f = p.face[fi];
+    const bool xo = f.lo[0] <= bx * TX + TX - 1 && f.hi[0] >= bx * TX;
+    const bool yo = f.lo[1] <= by * TYT + TYT - 1 && f.hi[1] >= by * TYT;
+    const bool zo = f.lo[2] <= ke - 1 && f.hi[2] >= kb;
+    if (xo && yo && zo) fmask |= 1u << fi;
+  }
+
+  // register queue of the planes behind, in march order: q[f][n] = plane k + (n - 3) * SD
+  float q[kAcF][3];
+#pragma unroll
+  for (int f = 0; f < kAcF; f++)
+#pragma unroll
+    for (int m = 0; m < 3; m++) q[f][m] = 0.f;
+  if (act) {
+#pragma unroll
+    for (int m = 0; m < 3; m++) {
+      const long long id = didx(p, i, j, k0 + (m - 3) * SD);
+#pragma unroll
+      for (int f = 0; f < kAcF; f++) q[f][m] = __ldg(cur + f * sf + id);
+    }
+  }
+  const int wc = (ty + LY) * S::WX + tx + S::XO;  // centre of this thread in a wave slot (per field)
+  mbar_wait(&bar[0], 0, p.err);
+  bool bad = false;  // stage 3: a new solution value is NaN/Inf
+
+  const int cell = ty * TX + tx;
+  for (int m = 0; m < n; m++) {
+    const int k = k0 + m * SD;
+    if (tid == 0) {
+      if (m + S::NW - 1 <= n) issue_wave(m + S::NW - 1);
+      if (m + 1 < n) issue_cpe(m + 1);
+    }
+    const int ws = m % S::NW, wn = (m + 1) % S::NW, cs = m & 1;
+    mbar_wait(&bar[wn], ((m + 1) / S::NW) & 1, p.err);
+    mbar_wait(&bar[S::NW + cs], (m >> 1) & 1, p.err);
+    const float *W = wave + ws * (S::WAVE_SLOT / 4);
+    const float *Wn = wave + wn * (S::WAVE_SLOT / 4);
+
+    if (act) {
+      const float *Cc = reinterpret_cast<const float *>(cpe + cs * S::CPE_SLOT) + cell;
+      float mt[3][3];
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) mt[a][b] = Cc[(3 * a + b) * S::CELLS];
+      const float slw = Cc[CF_SLW * S::CELLS], kappa = Cc[CF_MED * S::CELLS];
+      // derivatives along x, y, z of Vx Vy Vz (dv[axis][comp]) and of P (dp[axis])
+      float dv[3][3], dp[3];
+#pragma unroll
+      for (int f = 0; f < kAcF; f++) {
+        const float *r = W + f * S::WY * S::WX + (ty + LY) * S::WX + tx + S::XO - LX;
+        const float dx = drp5<DX>(r[0], r[1], r[2], r[3], r[4]);
+        const float *c = W + f * S::WY * S::WX + ty * S::WX + tx + S::XO;
+        const float dy = drp5<DY>(c[0], c[S::WX], c[2 * S::WX], c[3 * S::WX], c[4 * S::WX]);
+        const float c0 = W[f * S::WY * S::WX + wc], c1 = Wn[f * S::WY * S::WX + wc];
+        const float dz = SD > 0 ? drp5<DZ>(q[f][0], q[f][1], q[f][2], c0, c1) : drp5<DZ>(c1, c0, q[f][2], q[f][1], q[f][0]);
+        if (f < 3) { dv[0][f] = dx; dv[1][f] = dy; dv[2][f] = dz; }
+        else { dp[0] = dx; dp[1] = dy; dp[2] = dz; }
+      }
+      float h[kAcF];
+#pragma unroll
+      for (int c = 0; c < 3; c++) h[c] = -slw * (mt[0][c] * dp[0] + mt[1][c] * dp[1] + mt[2][c] * dp[2]);
+      // vlow rows of the top 3 planes (as k_stage_ac): planes k, k+1, k+2 are c0, q[2], q[1] when
+      // marching down (forward operators), k-2, k-1, k are q[1], q[2], c0 when marching up
+      float dvz[3] = {dv[2][0], dv[2][1], dv[2][2]};
+      const int nl = p.free_top ? p.nk - 1 - k : 3;
+      if (nl == 1 || nl == 2) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          const float c0 = W[c * S::WY * S::WX + wc];
+          if constexpr (DZ) {
+            dvz[c] = nl == 1 ? -c0 + q[c][2]
+                             : -7.0f / 6.0f * c0 + 8.0f / 6.0f * q[c][2] - 1.0f / 6.0f * q[c][1];
+          } else {
+            dvz[c] = nl == 1 ? -q[c][2] + c0
+                             : 1.0f / 6.0f * q[c][1] - 8.0f / 6.0f * q[c][2] + 7.0f / 6.0f * c0;
+          }
+        }
+      }
+      h[kAcP] = nl == 0 ? 0.f
+                        : -kappa * (mt[0][0] * dv[0][0] + mt[1][0] * dv[1][0] + mt[2][0] * dvz[0] +
+                                    mt[0][1] * dv[0][1] + mt[1][1] * dv[1][1] + mt[2][1] * dvz[1] +
+                                    mt[0][2] * dv[0][2] + mt[1][2] * dv[1][2] + mt[2][2] * dvz[2]);
+      if (fmask) {
+        float hc[kAcF] = {0.f, 0.f, 0.f, 0.f};
+        for (int fi = 0; fi < p.nface; fi++) {
+          const FaceP &fc = p.face[fi];
+          if ((fmask >> fi & 1) && in_face(fc, i, j, k))
+            ac_pml_face(p, fc, i, j, k, shot, slw, kappa, mt[fc.axis], dv[fc.axis], dp[fc.axis], hc);
+        }
+#pragma unroll
+        for (int c = 0; c < kAcF; c++) h[c] += hc[c];
+      }
+      // RK combine (wav_update / wav_update_end)
+      const long long id = didx(p, i, j, k);
+      const float *PR = reinterpret_cast<const float *>(cpe + cs * S::CPE_SLOT + S::OFF_PRE) + cell;
+      const float *EN = reinterpret_cast<const float *>(cpe + cs * S::CPE_SLOT + S::OFF_END) + cell;
+      const float ca = p.ca, cb = p.cb;
+      if (stage == 0) {
+#pragma unroll
+        for (int f = 0; f < kAcF; f++) {
+          const float c0 = W[f * S::WY * S::WX + wc];  // stage input = w_pre at stage 0
+          tmp_out[f * sf + id] = c0 + ca * h[f];
+          endw[f * sf + id] = c0 + cb * h[f];
+        }
+      } else if (stage < 3) {
+#pragma unroll
+        for (int f = 0; f < kAcF; f++) {
+          tmp_out[f * sf + id] = PR[f * S::CELLS] + ca * h[f];
+          endw[f * sf + id] = EN[f * S::CELLS] + cb * h[f];
+        }
+      } else {
+#pragma unroll
+        for (int f = 0; f < kAcF; f++) {
+          const float e = EN[f * S::CELLS] + cb * h[f];
+          endw[f * sf + id] = e;
+          bad |= nonfinite(e);
+        }
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < kAcF; f++) {
+      q[f][0] = q[f][1];
+      q[f][1] = q[f][2];
+      q[f][2] = W[f * S::WY * S::WX + wc];
+    }
+    // the slots read in this plane are refilled by TMA after the barrier
+    fence_proxy_async_smem();
+    __syncthreads();
+  }
+  if (bad) atomicOr(p.err, kErrWaveNonfinite);
+}
+
+int launch_stage_ac_tma(const StageP &p, const TmaP &tm, int nzc, cudaStream_t st) {
+  nzc = std::max(1, std::min(nzc, p.nk));
+  const int nchunk = (p.nk + nzc - 1) / nzc;
+  if ((long long)nchunk * p.nshot > 65535) return -1;  // the caller runs the direct-load kernel
+  const dim3 block(TX, AcSmem::TYT);
+  const dim3 grid((p.ni + TX - 1) / TX, (p.nj + AcSmem::TYT - 1) / AcSmem::TYT, nchunk * p.nshot);
+  static bool attr_done[8] = {};  // the opt-in above 48 KB of dynamic shared memory, once per instantiation
+  switch (p.dir[0] | (p.dir[1] << 1) | (p.dir[2] << 2)) {
+#define CASE(c)                                                                                           \
+  case c:                                                                                                 \
+    if (!attr_done[c]) {                                                                                  \
+      cudaFuncSetAttribute(k_stage_ac_tma<(c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1>,                         \
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, AcSmem::BYTES);                   \
+      attr_done[c] = true;                                                                                \
+    }                                                                                                     \
+    k_stage_ac_tma<(c)&1, ((c) >> 1) & 1, ((c) >> 2) & 1><<<grid, block, AcSmem::BYTES, st>>>(p, tm, nzc, nchunk); \
+    break;
+    CASE(0) CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7)
+#undef CASE
+  }
+  return 1;
 }
 
 template <typename R>

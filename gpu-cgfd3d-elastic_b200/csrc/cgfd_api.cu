@@ -208,7 +208,8 @@ struct cgfd_problem {
 
   bool use_graph = true;
   bool use_tma = true;
-  CUtensorMap map_halo[4], map_ctr[4], map_coef;
+  CUtensorMap map_halo[4], map_ctr[4], map_coef;  // acoustic media: the 4-field forms (make_ac_maps)
+  bool ac_tma = false;  // acoustic FP32: the TMA-pipelined stage kernel (else the direct-load one)
   cudaGraphExec_t graph[8] = {};
   bool graph_ok[8] = {};
   int graph_launches[8] = {};
@@ -400,7 +401,23 @@ struct cgfd_problem {
     n += enqueue_outputs<R>(step);
     for (int s = 0; s < 4; s++) {
       const cgfd::StagePT<R> p = stage_params_t<R>(step, s);
-      n += timed(s, [&] { return cgfd::launch_ac_image(p, st) + cgfd::launch_stage_ac(p, nzc, st); });
+      n += timed(s, [&] {
+        int k = cgfd::launch_ac_image(p, st);
+        int t = -1;
+        if constexpr (std::is_same<R, float>::value) {
+          if (ac_tma) {
+            cgfd::TmaP tm;
+            const int pre = step & 1, end = (step + 1) & 1;
+            const int curs[4] = {pre, 2, 3, 2};
+            tm.cur = map_halo[curs[s]];
+            tm.pre = map_ctr[pre];
+            tm.end = map_ctr[end];
+            tm.coef = map_coef;
+            t = cgfd::launch_stage_ac_tma(p, tm, nzc, st);
+          }
+        }
+        return k + (t >= 0 ? t : cgfd::launch_stage_ac(p, nzc, st));
+      });
       if (src.nsrc > 0) {
         cgfd::SrcPT<R> q;
         memset(&q, 0, sizeof(q));
@@ -863,6 +880,7 @@ std::vector<float> source_bounds(const cgfd_problem *p) {
 
 void make_tiles(cgfd_problem *p);
 void make_maps(cgfd_problem *p);
+void make_ac_maps(cgfd_problem *p);
 float *noalloc_scratch(int device);
 
 // sources given by physical coordinates: located on the current device (nullptr otherwise)
@@ -904,7 +922,10 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
            : d->medium_type == CGFD_MEDIUM_ELASTIC_ISO ? cgfd::MED_ISO
            : (d->medium_type == CGFD_MEDIUM_ELASTIC_VTI ? cgfd::MED_VTI : cgfd::MED_ANISO);
   p->ncoef = p->med == cgfd::MED_AC ? 11 : (p->med == cgfd::MED_ISO ? 12 : (p->med == cgfd::MED_VTI ? 15 : 31));
-  if (p->med == cgfd::MED_AC) p->use_tma = false;  // acoustic media run their own stage kernel
+  if (p->med == cgfd::MED_AC) {  // acoustic media run their own stage kernel (TMA-pipelined in FP32)
+    p->use_tma = false;
+    p->ac_tma = !p->fp64;
+  }
   p->nt_total = d->nt_total;
   p->dt = d->dt;
   p->free_top = d->free_top ? 1 : 0;
@@ -970,6 +991,7 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
 
   // TMA tensor maps of the four wavefield levels and of the coefficients
   if (p->use_tma) make_maps(p);
+  if (p->ac_tma) make_ac_maps(p);
   // free surface of elastic media: velocity-gradient conversion and traction-image fluxes
   if (p->free_top && p->med != cgfd::MED_AC) {
     std::vector<float> mx, my;
@@ -1166,6 +1188,21 @@ void make_maps(cgfd_problem *p) {
                2);
     CK(cgfd::tma_prepare(p->med, p->coef_type, p->wave16, p->shape));
   }
+}
+
+// TMA tensor maps of the acoustic stage kernel: the stage input of each level (physical cells and
+// the 3 ghost planes above the top, which hold the free surface's pressure image; 4 fields of a
+// shot), w_pre / w_end centre boxes (levels 0-1, 4 fields) and the 11 coefficient fields.
+void make_ac_maps(cgfd_problem *p) {
+  const int nshot = p->nshot;
+  for (int l = 0; l < 4; l++) {
+    make_map(&p->map_halo[l], p->wbuf[l] + p->off0, p->ni, p->nj, p->nk + 3, 9 * nshot, p->sx, p->sz, p->sf,
+             cgfd::TX + 8, cgfd::TY + 4, 4);
+    make_map(&p->map_ctr[l], p->wbuf[l], p->sx, p->nj + 6, p->nk + 6, 9 * nshot, p->sx, p->sz, p->sf, cgfd::TX,
+             cgfd::TY, 4);
+  }
+  make_map(&p->map_coef, p->coef, p->sx, p->nj + 6, p->nk + 6, p->ncoef, p->sx, p->sz, p->sf, cgfd::TX, cgfd::TY,
+           p->ncoef);
 }
 
 // Tile lists of the TMA bulk kernel: 32 x TY columns, split along z into chunks of about
@@ -1890,14 +1927,19 @@ int cgfd_autotune(cgfd_problem *p, int steps, int *chosen) {
 /* Bulk kernel variant: 1 = TMA-pipelined (default), 0 = direct loads. */
 int cgfd_set_bulk_variant(cgfd_problem *p, int tma) {
   if (!p) return CGFD_ERR_INVALID;
-  if (!tma && p->nshot > 1) { set_err("the direct-load bulk kernel handles one shot"); return CGFD_ERR_UNSUPPORTED; }
+  if (!tma && p->nshot > 1 && p->med != cgfd::MED_AC) {
+    set_err("the direct-load bulk kernel handles one shot");
+    return CGFD_ERR_UNSUPPORTED;
+  }
   if (tma && p->fp64) {
     set_err("the FP64 build runs the direct-load bulk kernel");
     return CGFD_ERR_UNSUPPORTED;
   }
-  if (p->med == cgfd::MED_AC) {
-    set_err("acoustic media run their own stage kernel");
-    return CGFD_ERR_UNSUPPORTED;
+  if (p->med == cgfd::MED_AC) {  // acoustic: the TMA-pipelined (1) or direct-load (0) stage kernel
+    p->ac_tma = tma != 0;
+    for (int s = 0; s < 8; s++)
+      if (p->graph_ok[s]) { cudaGraphExecDestroy(p->graph[s]); p->graph_ok[s] = false; }
+    return CGFD_OK;
   }
   if (!tma && p->precision != CGFD_PREC_FP32 && !p->fp64) {
     set_err("the direct-load bulk kernel handles FP32 storage only");

@@ -110,6 +110,9 @@ template <typename R>
 int launch_ac_image(const StagePT<R> &p, cudaStream_t st);
 template <typename R>
 int launch_stage_ac(const StagePT<R> &p, int nzc, cudaStream_t st);
+// the TMA-pipelined acoustic stage (FP32; tm: the acoustic maps of the stage input, w_pre,
+// w_end and the coefficients); -1 when the grid does not fit one launch (run launch_stage_ac)
+int launch_stage_ac_tma(const StageP &p, const TmaP &tm, int nzc, cudaStream_t st);
 // FP64 build: the surface slab with double storage and arithmetic
 int launch_stage_surface64(int med, const StagePT<double> &p, cudaStream_t st);
 // traction-image fluxes of the stage input for the surface slab (before it, same stream)

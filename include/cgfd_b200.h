@@ -369,7 +369,8 @@ int cgfd_get_shot_group(const cgfd_problem *p);
  */
 int cgfd_autotune(cgfd_problem *p, int steps, int *chosen);
 
-/* Bulk stage kernel variant: 1 = TMA-pipelined (default), 0 = direct global loads. */
+/* Bulk stage kernel variant: 1 = TMA-pipelined (default), 0 = direct global loads. Acoustic
+   media: their stage kernel in the same two forms (FP32; the FP64 build runs direct loads). */
 int cgfd_set_bulk_variant(cgfd_problem *p, int tma);
 
 /* Per-kernel CUDA-event timing of subsequent steps (uses direct launches while on). */
