@@ -229,6 +229,26 @@ def media_layer_any_gpu(coord, model, medium_type, method=CGFD_MEDIA_LOC, device
     return out
 
 
+class BinModelDesc(C.Structure):
+    """cgfd_bin_model: the three volumes of a binary model, file order."""
+    _fields_ = [("order", C.c_int * 3), ("size", C.c_int * 3), ("spacing", C.c_float * 3), ("origin", C.c_float * 3),
+                ("rho", C.c_void_p), ("vp", C.c_void_p), ("vs", C.c_void_p)]
+
+
+def media_bin_gpu(coord, model, device=0):
+    """cgfd_media_bin_el_iso_gpu: medium [3, nz, ny, nx] (rho, lambda, mu) of the binary model
+    (formats.BinModel) on the grid coord [3, nz, ny, nx]."""
+    _, nz, ny, nx = coord.shape
+    vols = [np.ascontiguousarray(v, np.float32) for v in (model.rho, model.vp, model.vs)]
+    d = BinModelDesc((C.c_int * 3)(*model.order), (C.c_int * 3)(*model.size), (C.c_float * 3)(*model.spacing),
+                     (C.c_float * 3)(*model.origin), vols[0].ctypes.data, vols[1].ctypes.data, vols[2].ctypes.data)
+    c = np.ascontiguousarray(coord, np.float32)
+    out = np.zeros((3, nz, ny, nx), np.float32)
+    check(lib().cgfd_media_bin_el_iso_gpu(int(device), nx - 6, ny - 6, nz - 6, c.ctypes.data, C.byref(d),
+                                          out.ctypes.data))
+    return out
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("device", C.c_int), ("hbm_budget", C.c_size_t), ("max_active", C.c_int), ("max_batch", C.c_int),
                 ("steps_per_slice", C.c_int)]
@@ -337,6 +357,7 @@ def lib():
         "cgfd_metric_calc_gpu": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, P]),
         "cgfd_media_layer_el_iso_gpu": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, P, C.c_int, P]),
         "cgfd_media_layer_gpu": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, P, C.c_int, C.c_int, P]),
+        "cgfd_media_bin_el_iso_gpu": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, P, P]),
         "cgfd_dt_estimate": (C.c_int, [C.POINTER(ProblemDesc), C.c_double, C.POINTER(C.c_double)]),
         "cgfd_keep_three_digits": (C.c_double, [C.c_double]),
         "cgfd_problem_bytes": (C.c_int, [C.POINTER(ProblemDesc), C.c_int, P, C.POINTER(C.c_size_t),

@@ -289,3 +289,32 @@ def write_layer_media_file(path, m: LayerMedia):
                 cols.append(m.param[q, c].reshape(-1))
         for row in np.stack(cols, axis=-1):
             f.write(" ".join(f"{v:.9g}" for v in row) + "\n")
+
+
+class BinModel:
+    """A 3-D binary model (the par file's medium input_way "binfile"): volumes rho, vp, vs with
+    size[0] x size[1] x size[2] samples, file dimension 0 fastest (numpy shape (size[2], size[1],
+    size[0])); order[d] is the grid axis (0 x, 1 y, 2 z) of file dimension d."""
+
+    def __init__(self, order, size, spacing, origin, rho, vp, vs):
+        self.order, self.size = [int(v) for v in order], [int(v) for v in size]
+        self.spacing, self.origin = [float(v) for v in spacing], [float(v) for v in origin]
+        shape = (self.size[2], self.size[1], self.size[0])
+        self.rho, self.vp, self.vs = (np.ascontiguousarray(v, np.float32).reshape(shape) for v in (rho, vp, vs))
+
+
+def write_bin_model(d, m: BinModel):
+    """The three raw float32 files (rho.bin, vp.bin, vs.bin) into directory d and the par-file
+    "medium" entry that reads them; returns that entry (medium type elastic_iso)."""
+    import os
+    os.makedirs(d, exist_ok=True)
+    files = {}
+    for name, v in (("rho", m.rho), ("Vp", m.vp), ("Vs", m.vs)):
+        path = os.path.join(d, name.lower() + ".bin")
+        np.ascontiguousarray(v, "<f4").tofile(path)
+        files[name] = path
+    axes = "xyz"
+    entry = {"size": list(m.size), "spacing": list(m.spacing), "origin": list(m.origin),
+             "dim1": axes[m.order[0]], "dim2": axes[m.order[1]], "dim3": axes[m.order[2]]}
+    entry.update(files)
+    return {"type": "elastic_iso", "input_way": "binfile", "binfile": entry}

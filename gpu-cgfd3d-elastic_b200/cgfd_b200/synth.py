@@ -172,6 +172,36 @@ def layer_model(coord, seed=5, layers=LAYERS_3, depths=(-1500.0, -3500.0), relie
     return LayerModel(x0, y0, dx, dy, **f)
 
 
+def bin_model(coord, seed=5, order=(2, 0, 1), spacing=(60.0, 90.0, 80.0), margin=300.0):
+    """A binary model (formats.BinModel) over the grid's extent plus `margin`: vp, vs, rho
+    rising smoothly with depth across the interfaces of INTERFACES_3 (below the speeds of the
+    deepest of LAYERS_3), with a seeded lateral variation of 2%, sampled on a regular mesh whose file dimensions run along the grid axes `order`
+    (default z fastest, then x, then y) with `spacing` per grid axis x, y, z; z decreasing from the
+    top of the grid (origin at the top, negative spacing), as depth models are stored."""
+    from .formats import BinModel
+    rng = np.random.default_rng(seed)
+    lo = [float(coord[a].min()) - margin for a in range(3)]
+    hi = [float(coord[a].max()) + margin for a in range(3)]
+    sp = [float(spacing[0]), float(spacing[1]), -float(spacing[2])]
+    org = [lo[0], lo[1], hi[2]]
+    n = [int(np.ceil((hi[a] - lo[a]) / abs(sp[a]))) + 1 for a in range(3)]
+    ax = [org[a] + sp[a] * np.arange(n[a]) for a in range(3)]
+    Z, Y, X = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")  # grid-axis order (z, y, x)
+    # 0 above the first interface, 1 below the second; speeds stay below the deepest layer's
+    t = 0.25 * (1 + np.tanh((-Z - 1500.0) / 300.0)) + 0.25 * (1 + np.tanh((-Z - 3500.0) / 300.0))
+    vp = LAYERS_3[0][0] + t * (LAYERS_3[2][0] - LAYERS_3[0][0]) * 0.9
+    vs = LAYERS_3[0][1] + t * (LAYERS_3[2][1] - LAYERS_3[0][1]) * 0.9
+    rho = LAYERS_3[0][2] + t * (LAYERS_3[2][2] - LAYERS_3[0][2]) * 0.9
+    k = rng.uniform(1.0, 3.0, 2) * 2 * np.pi / max(hi[0] - lo[0], 1.0)
+    lat = 1.0 + 0.02 * np.sin(k[0] * X + rng.uniform(0, 6.3)) * np.cos(k[1] * Y + rng.uniform(0, 6.3))
+    vols = [np.asarray(v * lat, np.float32) for v in (rho, vp, vs)]
+    # file order: file dimension d runs along grid axis order[d], dimension 0 fastest
+    perm = [2 - order[2], 2 - order[1], 2 - order[0]]  # numpy axes (z=0, y=1, x=2) of file dims 2, 1, 0
+    vols = [np.ascontiguousarray(np.transpose(v, perm)) for v in vols]
+    size = [n[order[d]] for d in range(3)]
+    return BinModel(order, size, [sp[order[d]] for d in range(3)], [org[order[d]] for d in range(3)], *vols)
+
+
 def layer_media(coord, type, seed=5, depths=(-1500.0, -3500.0), relief=150.0, grad=True):
     """A layer file of media type `type` (formats.LAYER_TYPES) over the grid's horizontal extent,
     with the interfaces of layer_model (a free top interface, undulating interfaces around the

@@ -14,7 +14,9 @@
 // result matches the reference's own host code. Kept alike on purpose: the reference's test
 // for "on an interface" compares the truncated integer part of dz with 0 (|dz| < 1 in model
 // units), because its isEqual() calls the integer abs().
+#include <algorithm>
 #include <cfloat>
+#include <cmath>
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -875,5 +877,189 @@ extern "C" int cgfd_media_layer_gpu(int device, int ni, int nj, int nk, const fl
       M(C44)[t] = c55; M(C55)[t] = c55; M(C66)[t] = c66;
     }
   }
+  return CGFD_OK;
+}
+
+// -----------------------------------------------------------------------------------------
+// Binary models (media_bin2model_el_iso, src/media/media_bin2model.cpp:27-233): the model cut to
+// the grid's x / y range is sampled at every grid point by TrilinearInterpolation
+// (src/media/media_utility.cpp:189-283), float arithmetic in the reference's order. The volumes
+// stay in file order on the device; the cut model is addressed through the file strides of its
+// x, y and z samples, which reads the same values as the reference's re-ordered copy.
+// -----------------------------------------------------------------------------------------
+namespace cgfd {
+namespace {
+
+struct BinDev {
+  int n[3];                    // samples of the cut model along x, y, z
+  long long st[3];             // file strides of one sample along x, y, z
+  long long off;               // file offset of the cut model's first sample
+  const float *xv, *yv, *zv;   // sample coordinates of the cut model
+  const float *rho, *vp, *vs;  // file-order volumes
+};
+
+__device__ __forceinline__ float lerp_rn(float a, float b, float w) { return __fadd_rn(a, __fmul_rn(w, __fsub_rn(b, a))); }
+
+// floor / ceil sample indices of q on the axis (first sample v0, spacing d), clamped to [0, n-1]
+__device__ __forceinline__ void bracket(float q, float v0, float d, int n, int &i0, int &i2) {
+  const float f = __fdiv_rn(__fsub_rn(q, v0), d);
+  i0 = (int)floorf(f);
+  i2 = (int)ceilf(f);
+  i0 = i0 < 0 ? 0 : (i0 > n - 1 ? n - 1 : i0);
+  i2 = i2 < 0 ? 0 : (i2 > n - 1 ? n - 1 : i2);
+}
+
+__device__ float trilinear(const BinDev &b, const float *v, float xq, float yq, float zq) {
+  int ix0, ix2, iy0, iy2, iz0, iz2;
+  bracket(xq, b.xv[0], __fsub_rn(b.xv[1], b.xv[0]), b.n[0], ix0, ix2);
+  bracket(yq, b.yv[0], __fsub_rn(b.yv[1], b.yv[0]), b.n[1], iy0, iy2);
+  bracket(zq, b.zv[0], __fsub_rn(b.zv[1], b.zv[0]), b.n[2], iz0, iz2);
+  auto at = [&](int ix, int iy, int iz) { return __ldg(v + b.off + ix * b.st[0] + iy * b.st[1] + iz * b.st[2]); };
+  if (ix0 == ix2 && iy0 == iy2 && iz0 == iz2) return at(ix0, iy0, iz0);
+  const float v000 = at(ix0, iy0, iz0), v002 = at(ix0, iy0, iz2), v200 = at(ix2, iy0, iz0), v202 = at(ix2, iy0, iz2);
+  const float v020 = at(ix0, iy2, iz0), v022 = at(ix0, iy2, iz2), v220 = at(ix2, iy2, iz0), v222 = at(ix2, iy2, iz2);
+  float v100 = v000, v102 = v002, v122 = v022, v120 = v020;
+  if (ix0 != ix2) {
+    const float w = __fdiv_rn(__fsub_rn(xq, b.xv[ix0]), __fsub_rn(b.xv[ix2], b.xv[ix0]));
+    v100 = lerp_rn(v000, v200, w);
+    v102 = lerp_rn(v002, v202, w);
+    v122 = lerp_rn(v022, v222, w);
+    v120 = lerp_rn(v020, v220, w);
+  }
+  float v110 = v100, v112 = v102;
+  if (iy0 != iy2) {
+    const float w = __fdiv_rn(__fsub_rn(yq, b.yv[iy0]), __fsub_rn(b.yv[iy2], b.yv[iy0]));
+    v110 = lerp_rn(v100, v120, w);
+    v112 = lerp_rn(v102, v122, w);
+  }
+  if (iz0 == iz2) return v110;
+  const float w = __fdiv_rn(__fsub_rn(zq, b.zv[iz0]), __fsub_rn(b.zv[iz2], b.zv[iz0]));
+  return __fadd_rn(v110, __fmul_rn(w, __fsub_rn(v112, v110)));
+}
+
+// parameterization_bin_el_iso_loc (media_bin2model.cpp:185-233): every grid point, ghosts included
+__global__ void k_media_bin(const __grid_constant__ BinDev b, const __grid_constant__ GridDev g) {
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const float xq = g.x[t], yq = g.y[t], zq = g.z[t];
+    float var[3];
+    var[0] = trilinear(b, b.rho, xq, yq, zq);
+    var[1] = trilinear(b, b.vp, xq, yq, zq);
+    var[2] = trilinear(b, b.vs, xq, yq, zq);
+    float lam, mu;
+    lame(var, lam, mu);
+    g.mu[t] = mu;
+    g.lam[t] = lam;
+    g.rho[t] = var[0];
+  }
+}
+
+}  // namespace
+}  // namespace cgfd
+
+extern "C" int cgfd_media_bin_el_iso_gpu(int device, int ni, int nj, int nk, const float *coord,
+                                         const cgfd_bin_model *bm, float *medium) {
+  using namespace cgfd;
+  if (!coord || !bm || !medium || !bm->rho || !bm->vp || !bm->vs || ni < 4 || nj < 4 || nk < 4) {
+    set_last_error("invalid argument");
+    return CGFD_ERR_INVALID;
+  }
+  // the grid axis of each file dimension (bin_order): dim[a] = the file dimension of axis a
+  int dim[3] = {-1, -1, -1};
+  for (int d = 0; d < 3; d++) {
+    const int o = bm->order[d];
+    if (o < 0 || o > 2 || dim[o] != -1) {
+      set_last_error("binary model: order must name x (0), y (1) and z (2) once each");
+      return CGFD_ERR_INVALID;
+    }
+    dim[o] = d;
+    if (bm->size[d] < 2) {
+      set_last_error("binary model: every dimension needs at least 2 samples");
+      return CGFD_ERR_INVALID;
+    }
+  }
+  const size_t nx = ni + 6, ny = nj + 6, nz = nk + 6, n = nx * ny * nz;
+  const float *X = coord, *Y = coord + n, *Z = coord + 2 * n;
+  // gd_curv_set_minmax (gd_t.cu:949-970): every point, ghosts included
+  float xmin = X[0], xmax = X[0], ymin = Y[0], ymax = Y[0], zmin = FLT_MAX, zmax = -FLT_MAX;
+  for (size_t t = 0; t < n; t++) {
+    xmin = std::min(xmin, X[t]); xmax = std::max(xmax, X[t]);
+    ymin = std::min(ymin, Y[t]); ymax = std::max(ymax, Y[t]);
+    zmin = std::min(zmin, Z[t]); zmax = std::max(zmax, Z[t]);
+  }
+  // the read range along x and y (media_bin2model.cpp:82-110), float arithmetic as there
+  const float x0 = bm->origin[dim[0]], y0 = bm->origin[dim[1]], z0 = bm->origin[dim[2]];
+  const float dxb = bm->spacing[dim[0]], dyb = bm->spacing[dim[1]], dzb = bm->spacing[dim[2]];
+  const int sx = bm->size[dim[0]], sy = bm->size[dim[1]], sz = bm->size[dim[2]];
+  const int ix_start = xmin < x0 ? 0 : (int)((xmin - x0) / dxb);
+  const int iy_start = ymin < y0 ? 0 : (int)((ymin - y0) / dyb);
+  const float zn = z0 + dzb * (float)(sz - 1);
+  if (ix_start >= sx || xmax < x0 || iy_start >= sy || ymax < y0 || zmin >= std::max(zn, z0) ||
+      zmax <= std::min(z0, zn)) {
+    set_last_error("binary model: the model does not coincide with the calculation area");
+    return CGFD_ERR_INVALID;
+  }
+  const int ix_end = std::min((int)std::ceil((xmax - x0) / dxb), sx - 1);
+  const int iy_end = std::min((int)std::ceil((ymax - y0) / dyb), sy - 1);
+  const int bnx = ix_end - ix_start + 1, bny = iy_end - iy_start + 1;
+  if (bnx < 2 || bny < 2) {
+    set_last_error("binary model: the cut model needs at least 2 samples along x and y");
+    return CGFD_ERR_INVALID;
+  }
+  std::vector<float> xv(bnx), yv(bny), zv(sz);
+  for (int q = 0; q < bnx; q++) xv[q] = x0 + (float)(ix_start + q) * dxb;
+  for (int q = 0; q < bny; q++) yv[q] = y0 + (float)(iy_start + q) * dyb;
+  for (int q = 0; q < sz; q++) zv[q] = z0 + (float)q * dzb;
+  const long long fst[3] = {1, (long long)bm->size[0], (long long)bm->size[0] * bm->size[1]};
+  const size_t nvol = (size_t)bm->size[0] * bm->size[1] * bm->size[2];
+
+  std::vector<void *> owned;
+  cudaStream_t st = nullptr;
+  auto cleanup = [&] {
+    for (void *q : owned) cudaFree(q);
+    if (st) cudaStreamDestroy(st);
+  };
+  auto fail = [&](cudaError_t e, const char *what) {
+    cleanup();
+    set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? CGFD_ERR_NOMEM : CGFD_ERR_CUDA;
+  };
+  auto dalloc = [&](size_t bytes, void **out) {
+    cudaError_t e = cudaMalloc(out, bytes);
+    if (e == cudaSuccess) owned.push_back(*out);
+    return e;
+  };
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return fail(e, "cudaSetDevice");
+  if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "cudaStreamCreate");
+  float *dvol = nullptr, *dvec = nullptr, *dc = nullptr, *dout = nullptr;
+  if ((e = dalloc(3 * nvol * sizeof(float), (void **)&dvol)) != cudaSuccess) return fail(e, "cudaMalloc");
+  if ((e = dalloc((size_t)(bnx + bny + sz) * sizeof(float), (void **)&dvec)) != cudaSuccess) return fail(e, "cudaMalloc");
+  if ((e = dalloc(3 * n * sizeof(float), (void **)&dc)) != cudaSuccess) return fail(e, "cudaMalloc");
+  if ((e = dalloc(3 * n * sizeof(float), (void **)&dout)) != cudaSuccess) return fail(e, "cudaMalloc");
+  const float *src[3] = {bm->rho, bm->vp, bm->vs};
+  for (int q = 0; q < 3 && e == cudaSuccess; q++)
+    e = cudaMemcpyAsync(dvol + q * nvol, src[q], nvol * sizeof(float), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dvec, xv.data(), bnx * sizeof(float), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dvec + bnx, yv.data(), bny * sizeof(float), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dvec + bnx + bny, zv.data(), sz * sizeof(float), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dc, coord, 3 * n * sizeof(float), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return fail(e, "cudaMemcpy");
+  BinDev b;
+  b.n[0] = bnx; b.n[1] = bny; b.n[2] = sz;
+  for (int a = 0; a < 3; a++) b.st[a] = fst[dim[a]];
+  b.off = (long long)ix_start * b.st[0] + (long long)iy_start * b.st[1];
+  b.xv = dvec; b.yv = dvec + bnx; b.zv = dvec + bnx + bny;
+  b.rho = dvol; b.vp = dvol + nvol; b.vs = dvol + 2 * nvol;
+  GridDev g{};
+  g.nx = (int)nx; g.ny = (int)ny; g.nz = (int)nz;
+  g.x = dc; g.y = dc + n; g.z = dc + 2 * n;
+  g.rho = dout; g.lam = dout + n; g.mu = dout + 2 * n;  // the medium order rho, lambda, mu
+  k_media_bin<<<148 * 8, 256, 0, st>>>(b, g);
+  if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "media kernel");
+  if ((e = cudaMemcpyAsync(medium, dout, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return fail(e, "cudaMemcpy");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail(e, "cudaStreamSynchronize");
+  cleanup();
   return CGFD_OK;
 }

@@ -7,7 +7,7 @@
 // (<output_dir>/<station>.<Vx..Txy>.sac, plus <station>.E**.sac strain for isotropic media;
 // <station>.<Vx Vy Vz P>.sac for acoustic media), line receivers, slices and snapshots, and
 // with a free surface the peak ground motion file PG_V_A_D_px0_py0_pz0.nc. Media come from
-// media_*.nc files or layer files discretised on the GPU. Options outside this path (MPI
+// media_*.nc files, or from layer files or binary models discretised on the GPU. Options outside this path (MPI
 // decomposition, ablexp, visco-elastic media) are rejected with a message.
 #include <sys/stat.h>
 
@@ -408,8 +408,37 @@ int run(int argc, char **argv) {
     if (method < 0) fail("equivalent_medium_method '" + em + "' must be loc, har or ari");
     if (cgfd_media_layer_gpu(gpu, g.ni, g.nj, g.nk, coord.data(), &lf.media(), d.medium_type, method, medium.data()))
       fail(std::string("media on the GPU: ") + cgfd_last_error());
+  } else if (way == "binfile") {
+    // 3-D binary model discretised on the GPU (media_bin2model_el_iso, main_curv_col_el_3d.cu:439-458;
+    // the reference reads binary models for elastic_iso media only)
+    if (d.medium_type != CGFD_MEDIUM_ELASTIC_ISO) fail("medium input_way 'binfile' is read for elastic_iso media only");
+    const Value &bf = need(md, "binfile");
+    cgfd_bin_model bm{};
+    const char *keys[3] = {"dim1", "dim2", "dim3"};
+    for (int q = 0; q < 3; q++) {
+      const std::string a = need(bf, keys[q]).as_str();
+      bm.order[q] = a == "x" ? 0 : a == "y" ? 1 : a == "z" ? 2 : -1;
+      bm.size[q] = need(bf, "size").arr.at(q).as_int();
+      bm.spacing[q] = (float)need(bf, "spacing").arr.at(q).as_num();
+      bm.origin[q] = (float)need(bf, "origin").arr.at(q).as_num();
+    }
+    const size_t nvol = (size_t)bm.size[0] * bm.size[1] * bm.size[2];
+    std::vector<float> vol[3];
+    const char *files[3] = {"rho", "Vp", "Vs"};
+    for (int q = 0; q < 3; q++) {  // raw float32, file order (read_bin_file, media_read_file.cpp:1274-1320)
+      const std::string path = need(bf, files[q]).as_str();
+      FILE *fp = fopen(path.c_str(), "rb");
+      if (!fp) fail("cannot open " + path);
+      vol[q].resize(nvol);
+      const size_t got = fread(vol[q].data(), sizeof(float), nvol, fp);
+      fclose(fp);
+      if (got < nvol) fail("Insufficient data in " + path);
+    }
+    bm.rho = vol[0].data(); bm.vp = vol[1].data(); bm.vs = vol[2].data();
+    if (cgfd_media_bin_el_iso_gpu(gpu, g.ni, g.nj, g.nk, coord.data(), &bm, medium.data()))
+      fail(std::string("media on the GPU: ") + cgfd_last_error());
   } else {
-    fail("medium input_way '" + way + "' is not on this path (import media_*.nc, or infile_layer)");
+    fail("medium input_way '" + way + "' is not on this path (import media_*.nc, infile_layer or binfile)");
   }
 
   d.ni = g.ni; d.nj = g.nj; d.nk = g.nk;

@@ -532,6 +532,32 @@ int cgfd_media_layer_gpu(int device, int ni, int nj, int nk, const float *coord,
                          int medium_type, int method, float *medium);
 
 /*
+ * A 3-D binary model (the par file's medium input_way "binfile", par_t.cu:495-600): raw float32
+ * volumes of rho, Vp and Vs, size[0] x size[1] x size[2] samples with file dimension 0 fastest.
+ * order[d] is the grid axis of file dimension d (0 x, 1 y, 2 z: the par file's dim1..dim3);
+ * spacing and origin are per file dimension (z may decrease).
+ */
+typedef struct cgfd_bin_model {
+  int   order[3];
+  int   size[3];
+  float spacing[3], origin[3];
+  const float *rho, *vp, *vs;  /* size[0] * size[1] * size[2] values each, in file order */
+} cgfd_bin_model;
+
+/*
+ * Media discretisation of a binary model on the GPU `device` into the elastic_iso medium
+ * [3][nz][ny][nx] = rho, lambda, mu (ghosts included): the model is cut to the grid's x / y range
+ * (all points, ghosts included) and sampled at every grid point by the reference's trilinear
+ * interpolation (samples clamped to the cut model), mu = vs vs rho, lambda = vp vp rho - 2 mu.
+ * CGFD_ERR_INVALID when order is not a permutation of 0, 1, 2, a dimension has fewer than 2
+ * samples, or the model does not coincide with the grid in x, y or z (the reference exits there).
+ * Replaces: media_bin2model_el_iso, src/media/media_bin2model.cpp:27-233, with
+ * TrilinearInterpolation (src/media/media_utility.cpp:189-283).
+ */
+int cgfd_media_bin_el_iso_gpu(int device, int ni, int nj, int nk, const float *coord, const cgfd_bin_model *model,
+                              float *medium);
+
+/*
  * Largest stable time step (FP64): CFL * min distance to the 8 neighbour planes / Vp.
  * Uses desc->coord and desc->medium (density form). The reference's CFL is 1.3.
  * Replaces: blk_dt_esti_curv, blk_t.cu:673-763.

@@ -4,6 +4,7 @@
 // links it.
 #include <cstddef>
 
+#include "media_bin2model.hpp"
 #include "media_layer2model.hpp"
 
 extern "C" int ref_media_layer2model_el_iso(float *lam3d, float *mu3d, float *rho3d, const float *x3d,
@@ -37,4 +38,15 @@ extern "C" int ref_media_layer2model_el_aniso(float *const *out, const float *x3
                                     out[10], out[11], out[12], out[13], out[14], out[15], out[16], out[17], out[18],
                                     out[19], out[20], out[21], x3d, y3d, z3d, nx, ny, nz, GRID_CURV, in_3lay_file,
                                     method, 1);
+}
+
+// media_bin2model_el_iso (media_bin2model.cpp:27-183): rho, lambda, mu from three binary volumes,
+// with the grid's x / y range as gd_curv_set_minmax computes it
+extern "C" int ref_media_bin2model_el_iso(float *rho3d, float *lam3d, float *mu3d, const float *x3d, const float *y3d,
+                                          const float *z3d, size_t nx, size_t ny, size_t nz, float xmin, float xmax,
+                                          float ymin, float ymax, int *bin_order, int *bin_size, float *bin_spacing,
+                                          float *bin_origin, const char *file_rho, const char *file_vp,
+                                          const char *file_vs) {
+  return media_bin2model_el_iso(rho3d, lam3d, mu3d, x3d, y3d, z3d, nx, ny, nz, xmin, xmax, ymin, ymax, GRID_CURV,
+                                bin_order, bin_size, bin_spacing, bin_origin, file_rho, file_vp, file_vs);
 }

@@ -80,3 +80,32 @@ def layer2model(coord, model, medium_type, method=0):
             out = np.stack(f)
     assert rc == 0
     return out
+
+
+def bin2model_el_iso(coord, model):
+    """medium [3, nz, ny, nx] = rho, lambda, mu by the reference's media_bin2model_el_iso from the
+    binary model (formats.BinModel) on the grid coord, with the grid's x / y range as
+    gd_curv_set_minmax computes it (every point, ghosts included)."""
+    L = C.CDLL(LIB)
+    fn = L.ref_media_bin2model_el_iso
+    fn.restype = C.c_int
+    fn.argtypes = ([C.c_void_p] * 6 + [C.c_size_t] * 3 + [C.c_float] * 4 + [C.c_void_p] * 4 +
+                   [C.c_char_p] * 3)
+    _, nz, ny, nx = coord.shape
+    c = np.ascontiguousarray(coord, np.float32)
+    rho, lam, mu = (np.zeros((nz, ny, nx), np.float32) for _ in range(3))
+    order = (C.c_int * 3)(*model.order)
+    size = (C.c_int * 3)(*model.size)
+    spacing = (C.c_float * 3)(*model.spacing)
+    origin = (C.c_float * 3)(*model.origin)
+    with tempfile.TemporaryDirectory() as d:
+        paths = []
+        for name, v in (("rho", model.rho), ("vp", model.vp), ("vs", model.vs)):
+            path = os.path.join(d, name + ".bin")
+            np.ascontiguousarray(v, np.float32).tofile(path)
+            paths.append(path.encode())
+        rc = fn(rho.ctypes.data, lam.ctypes.data, mu.ctypes.data, c[0].ctypes.data, c[1].ctypes.data,
+                c[2].ctypes.data, nx, ny, nz, float(c[0].min()), float(c[0].max()), float(c[1].min()),
+                float(c[1].max()), order, size, spacing, origin, *paths)
+    assert rc == 0
+    return np.stack([rho, lam, mu])

@@ -223,3 +223,33 @@ def test_cli_acoustic_medium_matches_oracle(tmp_path):
         w = o40.wavefield()
         tii = f.variables["Tii"][2]
         assert np.linalg.norm(tii[0] - w[3, -5, 3:-3, 3:-3]) <= 1e-4 * np.linalg.norm(w[3, -5, 3:-3, 3:-3])
+
+
+def test_cli_binary_medium_matches_oracle(tmp_path):
+    """medium input_way "binfile" (elastic_iso): three raw float32 volumes, file dimensions z, x,
+    y. The CLI discretises them on the GPU; its seismograms equal the oracle's run on the medium
+    the reference's own media_bin2model_el_iso builds from the same files (per-station rel L2
+    <= 1e-4)."""
+    import media_ref
+    if not media_ref.available():
+        pytest.skip("oracle/_ref/libref_media.so not built")
+    from cgfd_b200 import synth
+    nsteps = 60
+    p = small_problem("iso", nsteps=nsteps)
+    model = synth.bin_model(p.coord, seed=4)
+    medium = formats.write_bin_model(os.path.join(str(tmp_path), "bin"), model)
+    par = formats.write_case(str(tmp_path), p, nsteps, extra={"medium": medium})
+    r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    p.metric = synth.metrics(p.coord)
+    p.medium = media_ref.bin2model_el_iso(p.coord, model)
+    orc = Oracle(p)
+    orc.run()
+    ref = orc.seismograms()
+    out = os.path.join(str(tmp_path), "output")
+    got = np.zeros_like(ref)
+    for n, name in enumerate(p.sta.names):
+        for c, cn in enumerate(CMPS):
+            got[n, c] = formats.read_sac(os.path.join(out, f"{name}.{cn}.sac"))[1]
+    assert np.abs(ref).max() > 0
+    assert per_station_rel_l2(got, ref) <= 1e-4

@@ -1,6 +1,7 @@
-"""Media discretisation on the GPU (cgfd_media_layer_el_iso_gpu, cgfd_media_layer_gpu) against the
-reference's own host code (media_layer2model_el_iso / _el_vti / _el_aniso from the reference's
-src/media, oracle/_ref/libref_media.so)
+"""Media discretisation on the GPU (cgfd_media_layer_el_iso_gpu, cgfd_media_layer_gpu,
+cgfd_media_bin_el_iso_gpu) against the reference's own host code (media_layer2model_ac_iso /
+_el_iso / _el_vti / _el_aniso and media_bin2model_el_iso from the reference's src/media,
+oracle/_ref/libref_media.so)
 on the same curvilinear grid and layered model with undulating interfaces and depth gradients,
 for the three methods (loc, har, ari). Bar: every value equal to the reference's within 1e-6
 relative (both evaluate the same float / double expressions in the same order; the one
@@ -89,3 +90,33 @@ def test_gpu_layer_media_rejects_wrong_file_type():
         with pytest.raises(CgfdError) as e:
             media_layer_any_gpu(coord, synth.layer_media(coord, ftype, seed=9), medium, 0)
         assert e.value.code == -1
+
+
+def test_gpu_bin_media_matches_reference():
+    """cgfd_media_bin_el_iso_gpu against the reference's media_bin2model_el_iso on the same grid and
+    binary model (file dimensions z, x, y; z stored downwards): the same float operations in the
+    same order, so at least 99.9% of the values bitwise equal and all within 1e-6 relative."""
+    from cgfd_b200 import media_bin_gpu
+    coord = synth.curvilinear_grid(40, 36, 32, 100.0, seed=7)
+    model = synth.bin_model(coord, seed=3)
+    ref = media_ref.bin2model_el_iso(coord, model)
+    got = media_bin_gpu(coord, model)
+    assert np.isfinite(ref).all() and (ref[0] > 0).all()
+    rel = np.abs(got.astype(np.float64) - ref) / np.abs(ref).astype(np.float64)
+    assert rel.max() <= 1e-6, rel.max()
+    assert (got == ref).mean() >= 0.999
+
+
+def test_gpu_bin_media_rejects_a_model_beside_the_grid():
+    from cgfd_b200 import media_bin_gpu
+    coord = synth.curvilinear_grid(24, 24, 20, 100.0, seed=7)
+    model = synth.bin_model(coord, seed=3)
+    model.origin[1] += 1e6  # file dimension 1 runs along x: the model lies beyond the grid
+    with pytest.raises(CgfdError) as e:
+        media_bin_gpu(coord, model)
+    assert e.value.code == -1
+    model = synth.bin_model(coord, seed=3)
+    model.order = [0, 0, 1]
+    with pytest.raises(CgfdError) as e:
+        media_bin_gpu(coord, model)
+    assert e.value.code == -1
