@@ -1063,3 +1063,316 @@ extern "C" int cgfd_media_bin_el_iso_gpu(int device, int ni, int nj, int nk, con
   cleanup();
   return CGFD_OK;
 }
+
+// -----------------------------------------------------------------------------------------
+// Grid models (media_grid2model_el_iso, src/media/media_grid2model.cpp:133-188, the par file's
+// "infile_grid"): NL layers, layer l described by ngz[l] surfaces (elevation and rho vp vs on the
+// mesh, top first). A point takes the values of the surfaces above and below it, interpolated
+// linearly in elevation (CalPointValue_grid, :486-957); a point within the reference's isEqual of
+// a layer top takes the average of the two layers there. har / ari: where the 8 surrounding
+// half-grid points fall in more than one layer (MarkLayerNumber, :1269-1355), 9^3 sub-points of
+// the half-grid cell are averaged (:1819-2078), those on a layer top left out.
+// -----------------------------------------------------------------------------------------
+namespace cgfd {
+namespace {
+
+constexpr int kMaxGridLayers = 64;
+
+struct GridMediaDev {
+  LayerDev m;             // mesh (x0 .. dy of the cut mesh), elev [NI][ny][nx], p[0..2] rho vp vs [NI][ny][nx]
+  int nl;                 // layers
+  int tops[kMaxGridLayers];  // surface index of each layer's top (tops[0] = 0)
+};
+
+// last_ge over the NI surfaces with the elevations evaluated on the fly (no per-point array)
+__device__ int last_ge_grid(const LayerDev &m, float value, float x, float y) {
+  const size_t sl = (size_t)m.nx * m.ny;
+  if (value > bilinear(m, m.elev, x, y)) return -1;
+  float dist = FLT_MAX;
+  int indx = -1;
+  for (int i = 0; i < m.ni_; i++) {
+    const float e = bilinear(m, m.elev + i * sl, x, y);
+    if (e == -FLT_MAX) continue;
+    const float nd = __fsub_rn(e, value);
+    if (nd < 0.f) break;
+    if (nd <= dist) { dist = nd; indx = i; }
+  }
+  return indx;
+}
+
+__device__ __forceinline__ bool is_layer_top(const GridMediaDev &g, int mi) {
+  for (int l = 1; l < g.nl; l++)
+    if (g.tops[l] == mi) return true;
+  return false;
+}
+
+// AssignGridMediaPara2Point + CalPointValue_grid (elastic_isotropic): rho, vp, vs at a; on_inter:
+// the point lies on a layer top. Returns 0, 1 outside the mesh, or 2 vp <= sqrt(2) vs.
+__device__ int grid_point_value(const GridMediaDev &g, P3 a, float var[3], bool &on_inter) {
+  const LayerDev &m = g.m;
+  const float maxx = __fadd_rn(m.x0, __fmul_rn(m.dx, (float)(m.nx - 1)));
+  const float maxy = __fadd_rn(m.y0, __fmul_rn(m.dy, (float)(m.ny - 1)));
+  if (a.x < m.x0 || a.x > maxx || a.y < m.y0 || a.y > maxy) return 1;
+  const size_t sl = (size_t)m.nx * m.ny;
+  int mi = last_ge_grid(m, a.z, a.x, a.y);
+  const float em = mi >= 0 ? bilinear(m, m.elev + mi * sl, a.x, a.y) : 0.f;
+  on_inter = mi >= 0 && is_layer_top(g, mi) && (int)__fsub_rn(a.z, em) == 0;  // isEqual, integer abs
+  auto val = [&](int q, int s) { return bilinear(m, m.p[q] + s * sl, a.x, a.y); };
+  if (mi == -1) {
+    mi = last_ge_grid(m, bilinear(m, m.elev, a.x, a.y), a.x, a.y);
+    for (int q = 0; q < 3; q++) var[q] = val(q, mi);
+    return 0;
+  }
+  if (mi == m.ni_ - 1) {
+    for (int q = 0; q < 3; q++) var[q] = val(q, mi);
+    return 0;
+  }
+  const float ep = bilinear(m, m.elev + (mi + 1) * sl, a.x, a.y);
+  float dis_r = 0.5f;
+  if ((double)fabsf(__fsub_rn(ep, em)) > 1e-6) dis_r = __fdiv_rn(__fsub_rn(a.z, em), __fsub_rn(ep, em));
+  if (mi > 0 && (int)__fsub_rn(em, a.z) == 0 && is_layer_top(g, mi)) {
+    mi--;
+    dis_r = 0.5f;
+  }
+  for (int q = 0; q < 3; q++) {
+    const float v0 = val(q, mi), v1 = val(q, mi + 1);
+    var[q] = __fadd_rn(v0, __fmul_rn(__fsub_rn(v1, v0), dis_r));
+  }
+  if ((double)var[1] <= __dmul_rn(1.4142135623730951, (double)var[2])) return 2;
+  return 0;
+}
+
+// LayerNumberAtPoint (:1269-1310): the layer whose top is the last at or above the point
+__device__ int grid_layer_at(const GridMediaDev &g, float x, float y, float z) {
+  const size_t sl = (size_t)g.m.nx * g.m.ny;
+  float e[kMaxGridLayers];
+  for (int l = 0; l < g.nl; l++) e[l] = bilinear(g.m, g.m.elev + g.tops[l] * sl, x, y);
+  int mi = last_ge(z, e, g.nl);
+  if (mi == -1) mi = last_ge(e[0], e, g.nl);
+  return mi;
+}
+
+}  // namespace
+}  // namespace cgfd
+
+namespace cgfd {
+namespace {
+
+// parametrization_grid_el_iso_loc (:1067-1125)
+__global__ void k_grid_loc(const __grid_constant__ GridMediaDev gm, const __grid_constant__ GridDev g) {
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    float var[3];
+    bool on;
+    const int rc = grid_point_value(gm, P3{g.x[t], g.y[t], g.z[t]}, var, on);
+    if (rc) {
+      atomicOr(g.err, rc);
+      continue;
+    }
+    float lam, mu;
+    lame(var, lam, mu);
+    g.mu[t] = mu;
+    g.lam[t] = lam;
+    g.rho[t] = var[0];
+  }
+}
+
+// MarkLayerNumber, curvilinear: the layer of every half-grid point
+__global__ void k_grid_mark(const __grid_constant__ GridMediaDev gm, const __grid_constant__ GridDev g) {
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    g.mat[t] = grid_layer_at(gm, g.hx[t], g.hy[t], g.hz[t]);
+}
+
+// parametrization_grid_el_iso_har / _ari (:1819-2078): sub-points on a layer top are left out
+// (num_dis); har: rho arithmetic (float mean), kappa and mu harmonic; ari: rho, lambda, mu
+// arithmetic (double means)
+template <bool HAR>
+__global__ void k_grid_avg(const __grid_constant__ GridMediaDev gm, const __grid_constant__ GridDev g) {
+  const long long sl = g.nx, ss = (long long)g.nx * g.ny;
+  const long long n = (long long)(g.nx - 2) * (g.ny - 2) * (g.nz - 2);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(t % (g.nx - 2)), j = 1 + (int)((t / (g.nx - 2)) % (g.ny - 2));
+    const int k = 1 + (int)(t / ((long long)(g.nx - 2) * (g.ny - 2)));
+    const long long indx = i + j * sl + k * ss;
+    const long long c[8] = {indx - 1 - sl - ss, indx - sl - ss, indx - ss, indx - 1 - ss,
+                            indx - 1 - sl,      indx - sl,      indx,      indx - 1};
+    bool above = false, mixed = false;  // NumOfValues (media_utility.cpp:404-418) > 1
+    for (int q = 0; q < 8; q++) {
+      const int v = g.mat[c[q]];
+      if (v == -1) above = true;
+      if (v != g.mat[c[0]]) mixed = true;
+    }
+    if (above || !mixed) continue;
+    P3 M[8];
+    for (int q = 0; q < 8; q++) M[q] = P3{g.hx[c[q]], g.hy[c[q]], g.hz[c[q]]};
+    float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f;  // rho; kappa^-1 and mu^-1 (har) or lambda and mu (ari)
+    int num_dis = (kSub + 1) * (kSub + 1) * (kSub + 1), bad = 0;
+    auto lerp = [](P3 a, P3 b, int s) {  // a + (b - a) / ng * s, one rounding per step (Point3 operators)
+      return P3{__fadd_rn(a.x, __fmul_rn(__fdiv_rn(__fsub_rn(b.x, a.x), (float)kSub), (float)s)),
+                __fadd_rn(a.y, __fmul_rn(__fdiv_rn(__fsub_rn(b.y, a.y), (float)kSub), (float)s)),
+                __fadd_rn(a.z, __fmul_rn(__fdiv_rn(__fsub_rn(b.z, a.z), (float)kSub), (float)s))};
+    };
+    for (int kk = 0; kk <= kSub; kk++)
+      for (int jj = 0; jj <= kSub; jj++)
+        for (int ii = 0; ii <= kSub; ii++) {
+          const P3 lx00 = lerp(M[0], M[1], ii), lx10 = lerp(M[3], M[2], ii);
+          const P3 lx01 = lerp(M[4], M[5], ii), lx11 = lerp(M[7], M[6], ii);
+          const P3 lxy0 = lerp(lx00, lx10, jj), lxy1 = lerp(lx01, lx11, jj);
+          float var[3];
+          bool on = false;
+          const int rc = grid_point_value(gm, lerp(lxy0, lxy1, kk), var, on);
+          if (rc) { bad |= rc; continue; }
+          if (on) { num_dis--; continue; }
+          float lam, mu;
+          lame(var, lam, mu);
+          acc0 = __fadd_rn(acc0, var[0]);
+          if (HAR) {
+            acc1 = (float)__dadd_rn((double)acc1, __ddiv_rn(1.0, __dadd_rn((double)lam, __dmul_rn(2.0 / 3.0, (double)mu))));
+            acc2 = (float)__dadd_rn((double)acc2, __ddiv_rn(1.0, (double)mu));
+          } else {
+            acc1 = __fadd_rn(acc1, lam);
+            acc2 = __fadd_rn(acc2, mu);
+          }
+        }
+    if (bad) { atomicOr(g.err, bad); continue; }
+    if (HAR) {
+      const float hmu = (float)__ddiv_rn((double)num_dis, (double)acc2);
+      const float hkap = (float)__ddiv_rn((double)num_dis, (double)acc1);
+      g.rho[indx] = __fdiv_rn(acc0, (float)num_dis);
+      g.lam[indx] = (float)__dsub_rn((double)hkap, __dmul_rn(2.0 / 3.0, (double)hmu));
+      g.mu[indx] = hmu;
+    } else {
+      g.lam[indx] = (float)__ddiv_rn((double)acc1, (double)num_dis);
+      g.mu[indx] = (float)__ddiv_rn((double)acc2, (double)num_dis);
+      g.rho[indx] = (float)__ddiv_rn((double)acc0, (double)num_dis);
+    }
+  }
+}
+
+}  // namespace
+}  // namespace cgfd
+
+extern "C" int cgfd_media_grid_el_iso_gpu(int device, int ni, int nj, int nk, const float *coord,
+                                          const cgfd_grid_media *gmd, int method, float *medium) {
+  using namespace cgfd;
+  if (!coord || !gmd || !medium || !gmd->ngz || !gmd->elevation || !gmd->param || ni < 4 || nj < 4 || nk < 4 ||
+      method < CGFD_MEDIA_LOC || method > CGFD_MEDIA_ARI) {
+    set_last_error("invalid argument");
+    return CGFD_ERR_INVALID;
+  }
+  const int NL = gmd->num_layers;
+  if (NL < 1 || NL > kMaxGridLayers || gmd->nx < 2 || gmd->ny < 2) {
+    set_last_error("grid model: 1 to 64 layers on a mesh of at least 2 x 2 points are required");
+    return CGFD_ERR_INVALID;
+  }
+  GridMediaDev gm{};
+  gm.nl = NL;
+  int NI = 0;
+  for (int l = 0; l < NL; l++) {
+    if (gmd->ngz[l] < 1) {
+      set_last_error("grid model: every layer needs at least one surface");
+      return CGFD_ERR_INVALID;
+    }
+    gm.tops[l] = NI;
+    NI += gmd->ngz[l];
+  }
+  const size_t nx = ni + 6, ny = nj + 6, nz = nk + 6, n = nx * ny * nz;
+  const float *X = coord, *Y = coord + n;
+  float xmin = X[0], xmax = X[0], ymin = Y[0], ymax = Y[0];  // gd_curv_set_minmax
+  for (size_t t = 0; t < n; t++) {
+    xmin = std::min(xmin, X[t]); xmax = std::max(xmax, X[t]);
+    ymin = std::min(ymin, Y[t]); ymax = std::max(ymax, Y[t]);
+  }
+  // the part of the mesh read_grid_file keeps (media_read_file.cpp:774-800), float arithmetic as
+  // there; a grid beyond the mesh is refused (where the reference's check lets it through, it
+  // reads values it never stored)
+  const float MINX = gmd->x0, MINY = gmd->y0, DX = gmd->dx, DY = gmd->dy;
+  if (xmin < MINX || ymin < MINY) {
+    set_last_error("grid model: the given media range is smaller than the calculation grid range");
+    return CGFD_ERR_INVALID;
+  }
+  const size_t ix0 = (size_t)((xmin - MINX) / DX), iy0 = (size_t)((ymin - MINY) / DY);
+  const size_t ix1 = (size_t)std::ceil((xmax - MINX) / DX), iy1 = (size_t)std::ceil((ymax - MINY) / DY);
+  if (ix1 > (size_t)gmd->nx - 1 || iy1 > (size_t)gmd->ny - 1) {
+    set_last_error("grid model: the given media range is smaller than the calculation grid range");
+    return CGFD_ERR_INVALID;
+  }
+  const size_t cnx = ix1 - ix0 + 1, cny = iy1 - iy0 + 1, csl = cnx * cny;
+  std::vector<float> cut((size_t)4 * NI * csl);  // elevation, rho, vp, vs of the kept mesh
+  const size_t fsl = (size_t)gmd->nx * gmd->ny;
+  for (int q = 0; q < 4; q++) {
+    const float *src = q == 0 ? gmd->elevation : gmd->param + (size_t)(q - 1) * NI * fsl;
+    for (int s = 0; s < NI; s++)
+      for (size_t iy = 0; iy < cny; iy++)
+        for (size_t ix = 0; ix < cnx; ix++)
+          cut[((size_t)q * NI + s) * csl + iy * cnx + ix] = src[s * fsl + (iy0 + iy) * gmd->nx + ix0 + ix];
+  }
+  gm.m.ni_ = NI; gm.m.nx = (int)cnx; gm.m.ny = (int)cny;
+  gm.m.x0 = (float)ix0 * DX + MINX;
+  gm.m.y0 = (float)iy0 * DY + MINY;
+  gm.m.dx = DX; gm.m.dy = DY;
+
+  std::vector<void *> owned;
+  cudaStream_t st = nullptr;
+  auto cleanup = [&] {
+    for (void *q : owned) cudaFree(q);
+    if (st) cudaStreamDestroy(st);
+  };
+  auto fail = [&](cudaError_t e, const char *what) {
+    cleanup();
+    set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? CGFD_ERR_NOMEM : CGFD_ERR_CUDA;
+  };
+  auto dalloc = [&](size_t bytes, void **out) {
+    cudaError_t e = cudaMalloc(out, bytes);
+    if (e == cudaSuccess) owned.push_back(*out);
+    return e;
+  };
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return fail(e, "cudaSetDevice");
+  if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "cudaStreamCreate");
+  float *dm = nullptr, *dc = nullptr, *dout = nullptr;
+  int *derr = nullptr;
+  if ((e = dalloc(cut.size() * sizeof(float), (void **)&dm)) != cudaSuccess) return fail(e, "cudaMalloc");
+  if ((e = dalloc(3 * n * sizeof(float), (void **)&dc)) != cudaSuccess) return fail(e, "cudaMalloc");
+  if ((e = dalloc(3 * n * sizeof(float), (void **)&dout)) != cudaSuccess) return fail(e, "cudaMalloc");
+  if ((e = dalloc(sizeof(int), (void **)&derr)) != cudaSuccess) return fail(e, "cudaMalloc");
+  if ((e = cudaMemcpyAsync(dm, cut.data(), cut.size() * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(dc, coord, 3 * n * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return fail(e, "cudaMemcpy");
+  cudaMemsetAsync(derr, 0, sizeof(int), st);
+  gm.m.elev = dm;
+  for (int q = 0; q < 3; q++) gm.m.p[q] = dm + (size_t)(1 + q) * NI * csl;  // rho, vp, vs
+  GridDev g{};
+  g.nx = (int)nx; g.ny = (int)ny; g.nz = (int)nz;
+  g.x = dc; g.y = dc + n; g.z = dc + 2 * n;
+  g.rho = dout; g.lam = dout + n; g.mu = dout + 2 * n;  // the medium order rho, lambda, mu
+  g.err = derr;
+  k_grid_loc<<<148 * 8, 256, 0, st>>>(gm, g);
+  if (method != CGFD_MEDIA_LOC && NL >= 2) {  // one layer: the local values (the reference does the same)
+    float *dh = nullptr;
+    int *dmat = nullptr;
+    if ((e = dalloc(3 * n * sizeof(float), (void **)&dh)) != cudaSuccess) return fail(e, "cudaMalloc");
+    if ((e = dalloc(n * sizeof(int), (void **)&dmat)) != cudaSuccess) return fail(e, "cudaMalloc");
+    g.hx = dh; g.hy = dh + n; g.hz = dh + 2 * n;
+    g.mat = dmat;
+    k_half_grid<<<148 * 8, 256, 0, st>>>(g);
+    k_grid_mark<<<148 * 8, 256, 0, st>>>(gm, g);
+    if (method == CGFD_MEDIA_HAR) k_grid_avg<true><<<148 * 8, 128, 0, st>>>(gm, g);
+    else k_grid_avg<false><<<148 * 8, 128, 0, st>>>(gm, g);
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "media kernels");
+  int herr = 0;
+  if ((e = cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(medium, dout, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return fail(e, "cudaMemcpy");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail(e, "cudaStreamSynchronize");
+  cleanup();
+  if (herr) {
+    set_last_error((herr & 1) ? "a grid point lies outside the media grid mesh"
+                              : "vp must be larger than sqrt(2) vs in every layer");
+    return CGFD_ERR_INVALID;
+  }
+  return CGFD_OK;
+}

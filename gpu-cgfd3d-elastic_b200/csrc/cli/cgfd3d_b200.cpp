@@ -7,7 +7,7 @@
 // (<output_dir>/<station>.<Vx..Txy>.sac, plus <station>.E**.sac strain for isotropic media;
 // <station>.<Vx Vy Vz P>.sac for acoustic media), line receivers, slices and snapshots, and
 // with a free surface the peak ground motion file PG_V_A_D_px0_py0_pz0.nc. Media come from
-// media_*.nc files, or from layer files or binary models discretised on the GPU. Options outside this path (MPI
+// media_*.nc files, or from layer files, grid files or binary models discretised on the GPU. Options outside this path (MPI
 // decomposition, ablexp, visco-elastic media) are rejected with a message.
 #include <sys/stat.h>
 
@@ -408,6 +408,15 @@ int run(int argc, char **argv) {
     if (method < 0) fail("equivalent_medium_method '" + em + "' must be loc, har or ari");
     if (cgfd_media_layer_gpu(gpu, g.ni, g.nj, g.nk, coord.data(), &lf.media(), d.medium_type, method, medium.data()))
       fail(std::string("media on the GPU: ") + cgfd_last_error());
+  } else if (way == "infile_grid") {
+    // grid model discretised on the GPU (media_grid2model_el_iso, main_curv_col_el_3d.cu:365-379)
+    if (d.medium_type != CGFD_MEDIUM_ELASTIC_ISO) fail("medium input_way 'infile_grid' is read for elastic_iso media only");
+    cgfd::fmt::GridFile gf = cgfd::fmt::read_grid_file(need(md, "infile_grid").as_str());
+    const std::string em = md.get("equivalent_medium_method") ? md.get("equivalent_medium_method")->as_str() : "loc";
+    const int method = em == "loc" ? CGFD_MEDIA_LOC : em == "har" ? CGFD_MEDIA_HAR : em == "ari" ? CGFD_MEDIA_ARI : -1;
+    if (method < 0) fail("equivalent_medium_method '" + em + "' must be loc, har or ari");
+    if (cgfd_media_grid_el_iso_gpu(gpu, g.ni, g.nj, g.nk, coord.data(), &gf.desc(), method, medium.data()))
+      fail(std::string("media on the GPU: ") + cgfd_last_error());
   } else if (way == "binfile") {
     // 3-D binary model discretised on the GPU (media_bin2model_el_iso, main_curv_col_el_3d.cu:439-458;
     // the reference reads binary models for elastic_iso media only)
@@ -438,7 +447,7 @@ int run(int argc, char **argv) {
     if (cgfd_media_bin_el_iso_gpu(gpu, g.ni, g.nj, g.nk, coord.data(), &bm, medium.data()))
       fail(std::string("media on the GPU: ") + cgfd_last_error());
   } else {
-    fail("medium input_way '" + way + "' is not on this path (import media_*.nc, infile_layer or binfile)");
+    fail("medium input_way '" + way + "' is not on this path (import, infile_layer, infile_grid or binfile)");
   }
 
   d.ni = g.ni; d.nj = g.nj; d.nk = g.nk;

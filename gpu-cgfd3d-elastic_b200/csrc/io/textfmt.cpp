@@ -181,6 +181,53 @@ LayerFile read_layer_file(const std::string &path) {
   return L;
 }
 
+GridFile read_grid_file(const std::string &path) {
+  std::ifstream in(path);
+  if (!in) throw std::runtime_error("cannot open " + path);
+  GridFile G;
+  std::string type;
+  if (!(in >> type)) throw std::runtime_error(path + ": no media type");
+  if (type != "elastic_isotropic")
+    throw std::runtime_error(path + ": grid media of type '" + type + "' are not on this path (elastic_isotropic)");
+  int nl = 0;
+  if (!(in >> nl) || nl < 1) throw std::runtime_error(path + ": number of layers missing or < 1");
+  for (int l = 0; l < nl; l++) {
+    int ng = 0;
+    if (!(in >> ng) || ng < 1) throw std::runtime_error(path + ": surfaces of a layer missing or < 1");
+    G.ngz.push_back(ng);
+    G.ni += ng;
+  }
+  if (!(in >> G.nx >> G.ny >> G.x0 >> G.y0 >> G.dx >> G.dy) || G.nx < 2 || G.ny < 2)
+    throw std::runtime_error(path + ": mesh line must be NX NY MINX MINY DX DY with NX, NY >= 2");
+  const size_t sl = (size_t)G.nx * G.ny, n = (size_t)G.ni * sl;
+  G.elevation.resize(n);
+  G.param.resize(3 * n);
+  for (size_t p = 0; p < n; p++) {
+    if (!(in >> G.elevation[p])) throw std::runtime_error(path + ": insufficient data");
+    for (int q = 0; q < 3; q++)
+      if (!(in >> G.param[(size_t)q * n + p])) throw std::runtime_error(path + ": insufficient data");
+  }
+  int s = 0;
+  for (int l = 0; l + 1 < nl; l++) {
+    s += G.ngz[l];
+    for (size_t p = 0; p < sl; p++)
+      if (G.elevation[(size_t)(s - 1) * sl + p] != G.elevation[(size_t)s * sl + p])
+        throw std::runtime_error(path + ": the last elevations of layer " + std::to_string(l) +
+                                 " must equal the first elevations of layer " + std::to_string(l + 1));
+  }
+  return G;
+}
+
+const cgfd_grid_media &GridFile::desc() {
+  d.num_layers = (int)ngz.size();
+  d.ngz = ngz.data();
+  d.nx = nx; d.ny = ny;
+  d.x0 = x0; d.y0 = y0; d.dx = dx; d.dy = dy;
+  d.elevation = elevation.data();
+  d.param = param.data();
+  return d;
+}
+
 const cgfd_layer_model &LayerFile::desc() {
   const size_t n = (size_t)ni * nx * ny;
   d.num_interfaces = ni; d.nx = nx; d.ny = ny;

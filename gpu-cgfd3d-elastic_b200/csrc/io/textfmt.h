@@ -50,6 +50,21 @@ struct LayerFile {
 };
 LayerFile read_layer_file(const std::string &path);
 
+// Grid media file of elastic_isotropic type (read_grid_file, media_read_file.cpp:670-960): the type
+// name, the number of layers, the surfaces of each layer, "NX NY MINX MINY DX DY", then per
+// surface and mesh point (x fastest) elevation rho vp vs; a layer's last surface must lie on the
+// next layer's first (checkGridData, :1242-1266).
+struct GridFile {
+  std::vector<int> ngz;
+  int ni = 0, nx = 0, ny = 0;
+  float x0 = 0, y0 = 0, dx = 0, dy = 0;
+  std::vector<float> elevation;  // [ni][ny][nx]
+  std::vector<float> param;      // [3][ni][ny][nx]: rho vp vs
+  cgfd_grid_media d{};
+  const cgfd_grid_media &desc();
+};
+GridFile read_grid_file(const std::string &path);
+
 // One-component SAC file with the header fields the reference sets (sacLib.cu:8-100):
 // delta, b = 0, e = delta*(npts-1), npts, nvhdr = 6, iftype = ITIME, leven = 1, station
 // and event positions; every other field "undefined" (-12345).

@@ -558,6 +558,35 @@ int cgfd_media_bin_el_iso_gpu(int device, int ni, int nj, int nk, const float *c
                               float *medium);
 
 /*
+ * A grid model of elastic_isotropic type (the par file's medium input_way "infile_grid",
+ * read_grid_file, media_read_file.cpp:670-960): num_layers layers, layer l described by ngz[l]
+ * surfaces (NI = sum of ngz) on a uniform nx x ny mesh, top first; per surface and mesh point the
+ * elevation and rho, vp, vs (no gradients).
+ */
+typedef struct cgfd_grid_media {
+  int   num_layers;
+  const int *ngz;                /* [num_layers] */
+  int   nx, ny;
+  float x0, y0, dx, dy;
+  const float *elevation;        /* [NI][ny][nx] */
+  const float *param;            /* [3][NI][ny][nx]: rho, vp, vs */
+} cgfd_grid_media;
+
+/*
+ * Media discretisation of a grid model on the GPU `device` into the elastic_iso medium
+ * [3][nz][ny][nx] = rho, lambda, mu (ghosts included). A point takes the values of the two
+ * surfaces around it interpolated linearly in elevation, the average of the two layers on a layer
+ * top; har / ari average the 9^3 sub-points of a half-grid cell that a layer top crosses (those on
+ * the top left out): rho arithmetically, kappa and mu harmonically (har) or lambda and mu
+ * arithmetically (ari). CGFD_ERR_INVALID when the mesh does not cover the grid, a point falls
+ * outside it or vp <= sqrt(2) vs (the reference exits there).
+ * Replaces: media_grid2model_el_iso, src/media/media_grid2model.cpp:133-188 with
+ * parametrization_grid_el_iso_loc / _har / _ari (:1067-1125, 1819-2078).
+ */
+int cgfd_media_grid_el_iso_gpu(int device, int ni, int nj, int nk, const float *coord, const cgfd_grid_media *model,
+                               int method, float *medium);
+
+/*
  * Largest stable time step (FP64): CFL * min distance to the 8 neighbour planes / Vp.
  * Uses desc->coord and desc->medium (density form). The reference's CFL is 1.3.
  * Replaces: blk_dt_esti_curv, blk_t.cu:673-763.

@@ -3,8 +3,10 @@
 // TEST INFRASTRUCTURE: the checker of cgfd_media_layer_el_iso_gpu and cgfd_media_layer_gpu; nothing in the product
 // links it.
 #include <cstddef>
+#include <set>  // media_grid2model.hpp names std::set without including it
 
 #include "media_bin2model.hpp"
+#include "media_grid2model.hpp"
 #include "media_layer2model.hpp"
 
 extern "C" int ref_media_layer2model_el_iso(float *lam3d, float *mu3d, float *rho3d, const float *x3d,
@@ -49,4 +51,13 @@ extern "C" int ref_media_bin2model_el_iso(float *rho3d, float *lam3d, float *mu3
                                           const char *file_vs) {
   return media_bin2model_el_iso(rho3d, lam3d, mu3d, x3d, y3d, z3d, nx, ny, nz, xmin, xmax, ymin, ymax, GRID_CURV,
                                 bin_order, bin_size, bin_spacing, bin_origin, file_rho, file_vp, file_vs);
+}
+
+// media_grid2model_el_iso (media_grid2model.cpp:133-188): rho, lambda, mu from a grid media file,
+// with the grid's x / y range as gd_curv_set_minmax computes it
+extern "C" int ref_media_grid2model_el_iso(float *rho3d, float *lam3d, float *mu3d, const float *x3d, const float *y3d,
+                                           const float *z3d, int nx, int ny, int nz, float xmin, float xmax,
+                                           float ymin, float ymax, const char *in_media_file, const char *method) {
+  return media_grid2model_el_iso(rho3d, lam3d, mu3d, x3d, y3d, z3d, nx, ny, nz, xmin, xmax, ymin, ymax, GRID_CURV,
+                                 in_media_file, method, 1);
 }

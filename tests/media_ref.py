@@ -109,3 +109,24 @@ def bin2model_el_iso(coord, model):
                 float(c[1].max()), order, size, spacing, origin, *paths)
     assert rc == 0
     return np.stack([rho, lam, mu])
+
+
+def grid2model_el_iso(coord, model, method=0):
+    """medium [3, nz, ny, nx] = rho, lambda, mu by the reference's media_grid2model_el_iso from the
+    grid model (formats.GridMedia) on the grid coord, with the grid's x / y range as
+    gd_curv_set_minmax computes it."""
+    L = C.CDLL(LIB)
+    fn = L.ref_media_grid2model_el_iso
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p] * 6 + [C.c_int] * 3 + [C.c_float] * 4 + [C.c_char_p, C.c_char_p]
+    _, nz, ny, nx = coord.shape
+    c = np.ascontiguousarray(coord, np.float32)
+    rho, lam, mu = (np.zeros((nz, ny, nx), np.float32) for _ in range(3))
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "model.grd")
+        formats.write_grid_media_file(path, model)
+        rc = fn(rho.ctypes.data, lam.ctypes.data, mu.ctypes.data, c[0].ctypes.data, c[1].ctypes.data,
+                c[2].ctypes.data, nx, ny, nz, float(c[0].min()), float(c[0].max()), float(c[1].min()),
+                float(c[1].max()), path.encode(), METHODS[method])
+    assert rc == 0
+    return np.stack([rho, lam, mu])

@@ -41,7 +41,7 @@ def test_cli_rejects_off_path_options(tmp_path):
     par = formats.write_case(str(tmp_path), p, 2)
     import json
     cfg = json.load(open(par))
-    cfg["medium"]["input_way"] = "infile_grid"
+    cfg["medium"]["input_way"] = "code"  # the reference's built-in test media
     json.dump(cfg, open(par, "w"))
     r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "not on this path" in r.stderr

@@ -253,3 +253,35 @@ def test_cli_binary_medium_matches_oracle(tmp_path):
             got[n, c] = formats.read_sac(os.path.join(out, f"{name}.{cn}.sac"))[1]
     assert np.abs(ref).max() > 0
     assert per_station_rel_l2(got, ref) <= 1e-4
+
+
+def test_cli_grid_medium_matches_oracle(tmp_path):
+    """medium input_way "infile_grid" (elastic_iso, har): the CLI discretises the grid file on the
+    GPU; its seismograms equal the oracle's run on the medium the reference's own
+    media_grid2model_el_iso builds from the same file (per-station rel L2 <= 1e-4)."""
+    import media_ref
+    if not media_ref.available():
+        pytest.skip("oracle/_ref/libref_media.so not built")
+    from cgfd_b200 import synth
+    nsteps = 60
+    p = small_problem("iso", nsteps=nsteps)
+    model = synth.grid_media(p.coord, seed=4)
+    path = os.path.join(str(tmp_path), "model.grd")
+    formats.write_grid_media_file(path, model)
+    medium = {"type": "elastic_iso", "input_way": "infile_grid", "infile_grid": path,
+              "equivalent_medium_method": "har"}
+    par = formats.write_case(str(tmp_path), p, nsteps, extra={"medium": medium})
+    r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    p.metric = synth.metrics(p.coord)
+    p.medium = media_ref.grid2model_el_iso(p.coord, model, 1)
+    orc = Oracle(p)
+    orc.run()
+    ref = orc.seismograms()
+    out = os.path.join(str(tmp_path), "output")
+    got = np.zeros_like(ref)
+    for n, name in enumerate(p.sta.names):
+        for c, cn in enumerate(CMPS):
+            got[n, c] = formats.read_sac(os.path.join(out, f"{name}.{cn}.sac"))[1]
+    assert np.abs(ref).max() > 0
+    assert per_station_rel_l2(got, ref) <= 1e-4

@@ -1,6 +1,7 @@
 """Media discretisation on the GPU (cgfd_media_layer_el_iso_gpu, cgfd_media_layer_gpu,
-cgfd_media_bin_el_iso_gpu) against the reference's own host code (media_layer2model_ac_iso /
-_el_iso / _el_vti / _el_aniso and media_bin2model_el_iso from the reference's src/media,
+cgfd_media_bin_el_iso_gpu, cgfd_media_grid_el_iso_gpu) against the reference's own host code
+(media_layer2model_ac_iso / _el_iso / _el_vti / _el_aniso, media_bin2model_el_iso and
+media_grid2model_el_iso from the reference's src/media,
 oracle/_ref/libref_media.so)
 on the same curvilinear grid and layered model with undulating interfaces and depth gradients,
 for the three methods (loc, har, ari). Bar: every value equal to the reference's within 1e-6
@@ -119,4 +120,32 @@ def test_gpu_bin_media_rejects_a_model_beside_the_grid():
     model.order = [0, 0, 1]
     with pytest.raises(CgfdError) as e:
         media_bin_gpu(coord, model)
+    assert e.value.code == -1
+
+
+@pytest.mark.parametrize("method", [0, 1, 2])
+def test_gpu_grid_media_matches_reference(method):
+    """cgfd_media_grid_el_iso_gpu against the reference's media_grid2model_el_iso on the same grid
+    and grid model (3 layers of 3, 4, 3 surfaces with undulating layer tops): at least 99.9% of the
+    values bitwise equal and all within 1e-6 relative, for loc, har and ari."""
+    from cgfd_b200 import media_grid_gpu
+    coord = synth.curvilinear_grid(40, 36, 32, 100.0, seed=7)
+    model = synth.grid_media(coord, seed=3)
+    ref = media_ref.grid2model_el_iso(coord, model, method)
+    got = media_grid_gpu(coord, model, method)
+    assert np.isfinite(ref).all() and (ref[0] > 0).all()
+    rel = np.abs(got.astype(np.float64) - ref) / np.abs(ref).astype(np.float64)
+    assert rel.max() <= 1e-6, rel.max()
+    assert (got == ref).mean() >= 0.999
+    if method:
+        assert (ref != media_ref.grid2model_el_iso(coord, model, 0)).any()
+
+
+def test_gpu_grid_media_rejects_a_mesh_smaller_than_the_grid():
+    from cgfd_b200 import media_grid_gpu
+    coord = synth.curvilinear_grid(24, 24, 20, 100.0, seed=7)
+    model = synth.grid_media(coord, seed=3, margin=0.0)
+    model.x0 += 500.0  # the mesh no longer covers the grid's first columns
+    with pytest.raises(CgfdError) as e:
+        media_grid_gpu(coord, model, 0)
     assert e.value.code == -1
