@@ -251,24 +251,30 @@ def media_bin_gpu(coord, model, device=0):
 
 class GridMediaDesc(C.Structure):
     """cgfd_grid_media: a grid model of elastic_isotropic type."""
-    _fields_ = [("num_layers", C.c_int), ("ngz", C.c_void_p), ("nx", C.c_int), ("ny", C.c_int),
+    _fields_ = [("type", C.c_int), ("num_layers", C.c_int), ("ngz", C.c_void_p), ("nx", C.c_int), ("ny", C.c_int),
                 ("x0", C.c_float), ("y0", C.c_float), ("dx", C.c_float), ("dy", C.c_float),
                 ("elevation", C.c_void_p), ("param", C.c_void_p)]
 
 
-def media_grid_gpu(coord, model, method=CGFD_MEDIA_LOC, device=0):
+def media_grid_gpu(coord, model, method=CGFD_MEDIA_LOC, device=0, medium_type=None):
     """cgfd_media_grid_el_iso_gpu: medium [3, nz, ny, nx] (rho, lambda, mu) of the grid model
-    (formats.GridMedia) on the grid coord [3, nz, ny, nx]."""
+    (formats.GridMedia) on the grid coord [3, nz, ny, nx]; with medium_type (CGFD_MEDIUM_ELASTIC_*)
+    cgfd_media_grid_gpu: that medium in the problem description's order."""
     _, nz, ny, nx = coord.shape
     ngz = np.ascontiguousarray(model.ngz, np.int32)
     el = np.ascontiguousarray(model.elevation, np.float32)
     pa = np.ascontiguousarray(model.param, np.float32)
-    d = GridMediaDesc(len(model.ngz), ngz.ctypes.data, int(model.nx), int(model.ny), float(model.x0),
+    d = GridMediaDesc(int(model.type), len(model.ngz), ngz.ctypes.data, int(model.nx), int(model.ny), float(model.x0),
                       float(model.y0), float(model.dx), float(model.dy), el.ctypes.data, pa.ctypes.data)
     c = np.ascontiguousarray(coord, np.float32)
     out = np.zeros((3, nz, ny, nx), np.float32)
-    check(lib().cgfd_media_grid_el_iso_gpu(int(device), nx - 6, ny - 6, nz - 6, c.ctypes.data, C.byref(d),
-                                           int(method), out.ctypes.data))
+    if medium_type is None:
+        check(lib().cgfd_media_grid_el_iso_gpu(int(device), nx - 6, ny - 6, nz - 6, c.ctypes.data, C.byref(d),
+                                               int(method), out.ctypes.data))
+        return out
+    out = np.zeros(({2: 3, 3: 6, 4: 22}[int(medium_type)], nz, ny, nx), np.float32)
+    check(lib().cgfd_media_grid_gpu(int(device), nx - 6, ny - 6, nz - 6, c.ctypes.data, C.byref(d), int(medium_type),
+                                    int(method), out.ctypes.data))
     return out
 
 
@@ -382,6 +388,7 @@ def lib():
         "cgfd_media_layer_gpu": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, P, C.c_int, C.c_int, P]),
         "cgfd_media_bin_el_iso_gpu": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, P, P]),
         "cgfd_media_grid_el_iso_gpu": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, P, C.c_int, P]),
+        "cgfd_media_grid_gpu": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, P, C.c_int, C.c_int, P]),
         "cgfd_dt_estimate": (C.c_int, [C.POINTER(ProblemDesc), C.c_double, C.POINTER(C.c_double)]),
         "cgfd_keep_three_digits": (C.c_double, [C.c_double]),
         "cgfd_problem_bytes": (C.c_int, [C.POINTER(ProblemDesc), C.c_int, P, C.POINTER(C.c_size_t),

@@ -321,27 +321,30 @@ def write_bin_model(d, m: BinModel):
 
 
 class GridMedia:
-    """A grid model of elastic_isotropic type (read_grid_file, src/media/media_read_file.cpp:670-960):
-    `ngz[l]` surfaces per layer, top first, on a uniform nx x ny mesh; `elevation` [NI, ny, nx]
-    and `param` [3, NI, ny, nx] (rho, vp, vs) per surface."""
+    """A grid model (read_grid_file, src/media/media_read_file.cpp:670-1266): `ngz[l]` surfaces per
+    layer, top first, on a uniform nx x ny mesh; `elevation` [NI, ny, nx] and `param` [npar, NI,
+    ny, nx], the parameters of LAYER_TYPES[type] in file order (values only)."""
 
-    def __init__(self, ngz, x0, y0, dx, dy, elevation, param):
+    def __init__(self, ngz, x0, y0, dx, dy, elevation, param, type=21):
+        self.type = int(type)
         self.ngz = [int(v) for v in ngz]
         self.x0, self.y0, self.dx, self.dy = float(x0), float(y0), float(dx), float(dy)
         self.elevation = np.ascontiguousarray(elevation, np.float32)
         self.param = np.ascontiguousarray(param, np.float32)
         self.ny, self.nx = self.elevation.shape[1:]
-        assert self.elevation.shape[0] == sum(self.ngz) and self.param.shape == (3,) + self.elevation.shape
+        npar = len(LAYER_TYPES[self.type][1])
+        assert self.elevation.shape[0] == sum(self.ngz) and self.param.shape == (npar,) + self.elevation.shape
 
 
 def write_grid_media_file(path, m: GridMedia):
     """The grid media file of m in the reference's format: the type name, the number of layers,
     the surfaces of each layer, "NX NY MINX MINY DX DY", then per surface and mesh point (x
-    fastest) the elevation, rho, vp and vs (values written so that they read back exactly)."""
+    fastest) the elevation and the type's parameters (values written so that they read back
+    exactly)."""
     with open(path, "w") as f:
-        f.write("elastic_isotropic\n")
+        f.write(LAYER_TYPES[m.type][0] + "\n")
         f.write(f"{len(m.ngz)}\n" + " ".join(str(v) for v in m.ngz) + "\n")
         f.write(f"{m.nx} {m.ny} {m.x0:.9g} {m.y0:.9g} {m.dx:.9g} {m.dy:.9g}\n")
-        cols = [m.elevation.reshape(-1)] + [m.param[q].reshape(-1) for q in range(3)]
+        cols = [m.elevation.reshape(-1)] + [m.param[q].reshape(-1) for q in range(m.param.shape[0])]
         for row in np.stack(cols, axis=-1):
             f.write(" ".join(f"{v:.9g}" for v in row) + "\n")

@@ -202,14 +202,15 @@ def bin_model(coord, seed=5, order=(2, 0, 1), spacing=(60.0, 90.0, 80.0), margin
     return BinModel(order, size, [sp[order[d]] for d in range(3)], [org[order[d]] for d in range(3)], *vols)
 
 
-def grid_media(coord, seed=5, ngz=(3, 4, 3), depths=(-1200.0, -2400.0), relief=150.0, margin=300.0):
+def grid_media(coord, seed=5, ngz=(3, 4, 3), depths=(-1200.0, -2400.0), relief=150.0, margin=300.0, type=21):
     """A grid model (formats.GridMedia) over the grid's extent plus `margin`: len(ngz) layers whose
     tops lie above the grid and undulate around `depths`, each layer given by ngz[l] >= 2 surfaces
     evenly spaced from its top down to the next layer's top (the last layer's down to 1.5 km below
     its top), so that a layer's last surface lies on the next layer's first, as the format asks;
-    rho, vp, vs of LAYERS_3 per layer, rising a few percent from a layer's top surface to its last
-    one, with a seeded lateral variation."""
-    from .formats import GridMedia
+    rho, vp, vs of LAYERS_3 per layer (other file types: the per-layer parameters of layer_media),
+    the speeds and stiffnesses rising a few percent from a layer's top surface to its last one,
+    with a seeded lateral variation."""
+    from .formats import GridMedia, LAYER_TYPES
     rng = np.random.default_rng(seed)
     dx = dy = 100.0
     x0 = float(coord[0].min()) - margin
@@ -221,21 +222,25 @@ def grid_media(coord, seed=5, ngz=(3, 4, 3), depths=(-1200.0, -2400.0), relief=1
     def surface(z, n):
         k = rng.uniform(1.0, 3.0, 2) * 2 * np.pi / max(nx * dx, 1.0)
         return z + relief * np.sin(k[0] * X + rng.uniform(0, 6.3)) * np.cos(k[1] * Y + rng.uniform(0, 6.3)) * (n > 0)
+    names = LAYER_TYPES[type][1]
+    lm = layer_media(coord, type, seed=seed) if type != 21 else None
     surf = [np.asarray(surface(tops[l], l), np.float32) for l in range(len(ngz))]
     surf.append(surf[-1] - np.float32(1500.0))
     elev, par = [], []
     for l, ng in enumerate(ngz):
         top, bot = surf[l], surf[l + 1]
         vp, vs, rho = LAYERS_3[min(l, len(LAYERS_3) - 1)]
+        base = [rho, vp, vs] if type == 21 else [float(v) for v in lm.param[:, 0, min(l, lm.param.shape[2] - 1), 0, 0]]
         for s in range(ng):
             f = s / max(ng - 1, 1)
             elev.append(bot if s == ng - 1 else top + (bot - top) * np.float32(f))
             lat = 1.0 + 0.01 * np.sin(X / 700.0 + l) * np.cos(Y / 900.0 + s)
             g = 1.0 + 0.04 * f
-            par.append([rho * g * lat, vp * g * lat, vs * g * lat])
+            par.append([b * g * lat if (nm == "rho" or nm[0] in "vc") else b + 0 * X
+                        for b, nm in zip(base, names)])
     elev = np.asarray(elev, np.float32)
     param = np.asarray(par, np.float32).transpose(1, 0, 2, 3)
-    return GridMedia(ngz, x0, y0, dx, dy, elev, param)
+    return GridMedia(ngz, x0, y0, dx, dy, elev, param, type)
 
 
 def layer_media(coord, type, seed=5, depths=(-1500.0, -3500.0), relief=150.0, grad=True):

@@ -718,6 +718,56 @@ extern "C" int cgfd_media_layer_el_iso_gpu(int device, int ni, int nj, int nk, c
                           lm->elevation, hp, false, method, medium);
 }
 
+namespace cgfd {
+namespace {
+// The family's fields (iso rho lambda mu | VTI rho c11 c33 c55 c66 c13 | 22 Cij) into the
+// cgfd_problem_desc medium of medium_type; iso and VTI families into a 21-Cij medium by the
+// reference's expansion (media_layer2model_el_aniso / media_grid2model_el_aniso).
+int family_to_medium(const std::vector<float> &fam, int nfam, int medium_type, size_t n, float *medium) {
+  const int nout_med = medium_type == CGFD_MEDIUM_ELASTIC_ISO ? 3 : (medium_type == CGFD_MEDIUM_ELASTIC_VTI ? 6 : 22);
+  auto M = [&](int f) { return medium + (size_t)f * n; };
+  if (medium_type == CGFD_MEDIUM_ELASTIC_ISO) {
+    std::memcpy(medium, fam.data(), 3 * n * sizeof(float));
+    return CGFD_OK;
+  }
+  auto F = [&](int f) { return fam.data() + (size_t)f * n; };
+  if (medium_type == CGFD_MEDIUM_ELASTIC_VTI) {  // rho c11 c33 c55 c66 c13 -> rho c11 c13 c33 c55 c66
+    const int from[6] = {0, 1, 5, 2, 3, 4};
+    for (int f = 0; f < 6; f++) std::memcpy(M(f), F(from[f]), n * sizeof(float));
+    return CGFD_OK;
+  }
+  // 21-Cij medium (desc order rho c11 c12 c13 c14 c15 c16 c22 c23 c24 c25 c26 c33 c34 c35 c36 c44
+  // c45 c46 c55 c56 c66)
+  if (nfam == 22) {
+    std::memcpy(medium, fam.data(), 22 * n * sizeof(float));
+    return CGFD_OK;
+  }
+  std::memset(medium, 0, (size_t)nout_med * n * sizeof(float));
+  enum { RHO = 0, C11 = 1, C12 = 2, C13 = 3, C22 = 7, C23 = 8, C33 = 12, C44 = 16, C55 = 19, C66 = 21 };
+  const bool iso = nfam == 3;
+#pragma omp parallel for schedule(static)
+  for (long long t = 0; t < (long long)n; t++) {
+    if (iso) {  // el_aniso's elastic_isotropic branch: lambda -> c13, mu -> c44
+      const float c13 = F(1)[t], c44 = F(2)[t];
+      const float c11 = (float)((double)c13 + 2.0 * (double)c44);
+      M(RHO)[t] = F(0)[t];
+      M(C11)[t] = c11; M(C22)[t] = c11; M(C33)[t] = c11;
+      M(C12)[t] = c13; M(C13)[t] = c13; M(C23)[t] = c13;
+      M(C44)[t] = c44; M(C55)[t] = c44; M(C66)[t] = c44;
+    } else {  // its VTI branch
+      const float c11 = F(1)[t], c33 = F(2)[t], c55 = F(3)[t], c66 = F(4)[t], c13 = F(5)[t];
+      M(RHO)[t] = F(0)[t];
+      M(C11)[t] = c11; M(C22)[t] = c11; M(C33)[t] = c33;
+      M(C12)[t] = (float)((double)c11 - 2.0 * (double)c66);
+      M(C13)[t] = c13; M(C23)[t] = c13;
+      M(C44)[t] = c55; M(C55)[t] = c55; M(C66)[t] = c66;
+    }
+  }
+  return CGFD_OK;
+}
+}  // namespace
+}  // namespace cgfd
+
 extern "C" int cgfd_media_layer_gpu(int device, int ni, int nj, int nk, const float *coord, const cgfd_layer_media *lm,
                                     int medium_type, int method, float *medium) {
   using namespace cgfd;
@@ -753,8 +803,6 @@ extern "C" int cgfd_media_layer_gpu(int device, int ni, int nj, int nk, const fl
   }
   const size_t nx = ni + 6, ny = nj + 6, nz = nk + 6, n = nx * ny * nz;
   const size_t lv = (size_t)lm->num_interfaces * lm->nx * lm->ny;
-  const int nout_med = medium_type == CGFD_MEDIUM_ELASTIC_ISO ? 3 : (medium_type == CGFD_MEDIUM_ELASTIC_VTI ? 6 : 22);
-  auto M = [&](int f) { return medium + (size_t)f * n; };  // field f of the output, desc order
 
   // the family's fields on the device: iso (rho lambda mu), VTI (rho c11 c33 c55 c66 c13), 22 Cij
   std::vector<float> fam;
@@ -844,40 +892,7 @@ extern "C" int cgfd_media_layer_gpu(int device, int ni, int nj, int nk, const fl
       return CGFD_ERR_INVALID;
     }
   }
-  auto F = [&](int f) { return fam.data() + (size_t)f * n; };
-  if (medium_type == CGFD_MEDIUM_ELASTIC_VTI) {  // rho c11 c33 c55 c66 c13 -> rho c11 c13 c33 c55 c66
-    const int from[6] = {0, 1, 5, 2, 3, 4};
-    for (int f = 0; f < 6; f++) std::memcpy(M(f), F(from[f]), n * sizeof(float));
-    return CGFD_OK;
-  }
-  // 21-Cij medium (desc order rho c11 c12 c13 c14 c15 c16 c22 c23 c24 c25 c26 c33 c34 c35 c36 c44
-  // c45 c46 c55 c56 c66)
-  if (nfam == 22) {
-    std::memcpy(medium, fam.data(), 22 * n * sizeof(float));
-    return CGFD_OK;
-  }
-  std::memset(medium, 0, (size_t)nout_med * n * sizeof(float));
-  enum { RHO = 0, C11 = 1, C12 = 2, C13 = 3, C22 = 7, C23 = 8, C33 = 12, C44 = 16, C55 = 19, C66 = 21 };
-  const bool iso = nfam == 3;
-#pragma omp parallel for schedule(static)
-  for (long long t = 0; t < (long long)n; t++) {
-    if (iso) {  // el_aniso's elastic_isotropic branch: lambda -> c13, mu -> c44
-      const float c13 = F(1)[t], c44 = F(2)[t];
-      const float c11 = (float)((double)c13 + 2.0 * (double)c44);
-      M(RHO)[t] = F(0)[t];
-      M(C11)[t] = c11; M(C22)[t] = c11; M(C33)[t] = c11;
-      M(C12)[t] = c13; M(C13)[t] = c13; M(C23)[t] = c13;
-      M(C44)[t] = c44; M(C55)[t] = c44; M(C66)[t] = c44;
-    } else {  // its VTI branch
-      const float c11 = F(1)[t], c33 = F(2)[t], c55 = F(3)[t], c66 = F(4)[t], c13 = F(5)[t];
-      M(RHO)[t] = F(0)[t];
-      M(C11)[t] = c11; M(C22)[t] = c11; M(C33)[t] = c33;
-      M(C12)[t] = (float)((double)c11 - 2.0 * (double)c66);
-      M(C13)[t] = c13; M(C23)[t] = c13;
-      M(C44)[t] = c55; M(C55)[t] = c55; M(C66)[t] = c66;
-    }
-  }
-  return CGFD_OK;
+  return family_to_medium(fam, nfam, medium_type, n, medium);
 }
 
 // -----------------------------------------------------------------------------------------
@@ -1253,20 +1268,126 @@ __global__ void k_grid_avg(const __grid_constant__ GridMediaDev gm, const __grid
 }  // namespace
 }  // namespace cgfd
 
-extern "C" int cgfd_media_grid_el_iso_gpu(int device, int ni, int nj, int nk, const float *coord,
-                                          const cgfd_grid_media *gmd, int method, float *medium) {
-  using namespace cgfd;
-  if (!coord || !gmd || !medium || !gmd->ngz || !gmd->elevation || !gmd->param || ni < 4 || nj < 4 || nk < 4 ||
-      method < CGFD_MEDIA_LOC || method > CGFD_MEDIA_ARI) {
-    set_last_error("invalid argument");
-    return CGFD_ERR_INVALID;
+namespace cgfd {
+namespace {
+
+// CalPointValue_grid for the VTI / TTI / Cij file types: the NPAR parameters of the surfaces
+// around a, interpolated in elevation (par: [NPAR][NI][ny][nx]); on_inter as grid_point_value.
+template <int NPAR>
+__device__ int grid_point_params(const GridMediaDev &g, P3 a, float var[NPAR], bool &on_inter) {
+  const LayerDev &m = g.m;
+  const float maxx = __fadd_rn(m.x0, __fmul_rn(m.dx, (float)(m.nx - 1)));
+  const float maxy = __fadd_rn(m.y0, __fmul_rn(m.dy, (float)(m.ny - 1)));
+  if (a.x < m.x0 || a.x > maxx || a.y < m.y0 || a.y > maxy) return 1;
+  const size_t sl = (size_t)m.nx * m.ny, ps = (size_t)m.ni_ * sl;
+  int mi = last_ge_grid(m, a.z, a.x, a.y);
+  const float em = mi >= 0 ? bilinear(m, m.elev + mi * sl, a.x, a.y) : 0.f;
+  on_inter = mi >= 0 && is_layer_top(g, mi) && (int)__fsub_rn(a.z, em) == 0;
+  auto val = [&](int q, int s) { return bilinear(m, m.par + q * ps + s * sl, a.x, a.y); };
+  if (mi == -1 || mi == m.ni_ - 1) {
+    if (mi == -1) mi = last_ge_grid(m, bilinear(m, m.elev, a.x, a.y), a.x, a.y);
+    for (int q = 0; q < NPAR; q++) var[q] = val(q, mi);
+    return 0;
   }
+  const float ep = bilinear(m, m.elev + (mi + 1) * sl, a.x, a.y);
+  float dis_r = 0.5f;
+  if ((double)fabsf(__fsub_rn(ep, em)) > 1e-6) dis_r = __fdiv_rn(__fsub_rn(a.z, em), __fsub_rn(ep, em));
+  if (mi > 0 && (int)__fsub_rn(em, a.z) == 0 && is_layer_top(g, mi)) {
+    mi--;
+    dis_r = 0.5f;
+  }
+  for (int q = 0; q < NPAR; q++) {
+    const float v0 = val(q, mi), v1 = val(q, mi + 1);
+    var[q] = __fadd_rn(v0, __fmul_rn(__fsub_rn(v1, v0), dis_r));
+  }
+  return 0;
+}
+
+// parametrization_grid_el_{vti,aniso}_loc (:1127-1267)
+template <int T>
+__global__ void k_grid_loc_gen(const __grid_constant__ GridMediaDev gm, const __grid_constant__ GridDev g,
+                               const __grid_constant__ OutDev out) {
+  constexpr int NP = LayerFile<T>::NPAR, NO = LayerFile<T>::NOUT;
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    float var[NP], o[NO];
+    bool on;
+    if (grid_point_params<NP>(gm, P3{g.x[t], g.y[t], g.z[t]}, var, on)) {
+      atomicOr(out.err, 1);
+      continue;
+    }
+    para2out<T>(var, o);
+    for (int q = 0; q < NO; q++) out.f[q * out.n + t] = o[q];
+  }
+}
+
+// parametrization_grid_el_{vti,aniso}_{har,ari} (:2080-2793): every c_ij harmonically (double
+// sum of 1/c into a float, num_dis / sum in double) or arithmetically (float sum / num_dis), rho
+// arithmetically; the sub-points on a layer top left out
+template <int T, bool HAR>
+__global__ void k_grid_avg_gen(const __grid_constant__ GridMediaDev gm, const __grid_constant__ GridDev g,
+                               const __grid_constant__ OutDev out) {
+  constexpr int NP = LayerFile<T>::NPAR, NO = LayerFile<T>::NOUT;
+  const long long sl = g.nx, ss = (long long)g.nx * g.ny;
+  const long long n = (long long)(g.nx - 2) * (g.ny - 2) * (g.nz - 2);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(t % (g.nx - 2)), j = 1 + (int)((t / (g.nx - 2)) % (g.ny - 2));
+    const int k = 1 + (int)(t / ((long long)(g.nx - 2) * (g.ny - 2)));
+    const long long indx = i + j * sl + k * ss;
+    const long long c[8] = {indx - 1 - sl - ss, indx - sl - ss, indx - ss, indx - 1 - ss,
+                            indx - 1 - sl,      indx - sl,      indx,      indx - 1};
+    bool above = false, mixed = false;
+    for (int q = 0; q < 8; q++) {
+      const int v = g.mat[c[q]];
+      if (v == -1) above = true;
+      if (v != g.mat[c[0]]) mixed = true;
+    }
+    if (above || !mixed) continue;
+    P3 M[8];
+    for (int q = 0; q < 8; q++) M[q] = P3{g.hx[c[q]], g.hy[c[q]], g.hz[c[q]]};
+    float acc[NO];
+    for (int q = 0; q < NO; q++) acc[q] = 0.f;
+    int num_dis = (kSub + 1) * (kSub + 1) * (kSub + 1), bad = 0;
+    auto lerp = [](P3 a, P3 b, int s) {
+      return P3{__fadd_rn(a.x, __fmul_rn(__fdiv_rn(__fsub_rn(b.x, a.x), (float)kSub), (float)s)),
+                __fadd_rn(a.y, __fmul_rn(__fdiv_rn(__fsub_rn(b.y, a.y), (float)kSub), (float)s)),
+                __fadd_rn(a.z, __fmul_rn(__fdiv_rn(__fsub_rn(b.z, a.z), (float)kSub), (float)s))};
+    };
+    for (int kk = 0; kk <= kSub; kk++)
+      for (int jj = 0; jj <= kSub; jj++)
+        for (int ii = 0; ii <= kSub; ii++) {
+          const P3 lx00 = lerp(M[0], M[1], ii), lx10 = lerp(M[3], M[2], ii);
+          const P3 lx01 = lerp(M[4], M[5], ii), lx11 = lerp(M[7], M[6], ii);
+          const P3 lxy0 = lerp(lx00, lx10, jj), lxy1 = lerp(lx01, lx11, jj);
+          float var[NP], o[NO];
+          bool on = false;
+          if (grid_point_params<NP>(gm, lerp(lxy0, lxy1, kk), var, on)) { bad = 1; continue; }
+          if (on) { num_dis--; continue; }
+          para2out<T>(var, o);
+          acc[0] = __fadd_rn(acc[0], o[0]);
+          for (int q = 1; q < NO; q++)
+            acc[q] = HAR ? (float)__dadd_rn((double)acc[q], __ddiv_rn(1.0, (double)o[q])) : __fadd_rn(acc[q], o[q]);
+        }
+    if (bad) { atomicOr(out.err, 1); continue; }
+    out.f[indx] = __fdiv_rn(acc[0], (float)num_dis);
+    for (int q = 1; q < NO; q++)
+      out.f[q * out.n + indx] =
+          HAR ? (float)__ddiv_rn((double)num_dis, (double)acc[q]) : __fdiv_rn(acc[q], (float)num_dis);
+  }
+}
+
+// The part of the grid file's mesh read_grid_file keeps (media_read_file.cpp:774-800), float
+// arithmetic as there: cut[0] elevation, cut[1 ..] the npar parameters, each [NI][cny][cnx];
+// gm gets the cut mesh. A grid beyond the mesh is refused (where the reference's check lets it
+// through, it reads values it never stored).
+int grid_setup(const cgfd_grid_media *gmd, int npar, const float *coord, size_t n, std::vector<float> &cut,
+               GridMediaDev &gm) {
   const int NL = gmd->num_layers;
-  if (NL < 1 || NL > kMaxGridLayers || gmd->nx < 2 || gmd->ny < 2) {
+  if (NL < 1 || NL > kMaxGridLayers || gmd->nx < 2 || gmd->ny < 2 || !gmd->ngz || !gmd->elevation || !gmd->param) {
     set_last_error("grid model: 1 to 64 layers on a mesh of at least 2 x 2 points are required");
     return CGFD_ERR_INVALID;
   }
-  GridMediaDev gm{};
+  gm = GridMediaDev{};
   gm.nl = NL;
   int NI = 0;
   for (int l = 0; l < NL; l++) {
@@ -1277,16 +1398,12 @@ extern "C" int cgfd_media_grid_el_iso_gpu(int device, int ni, int nj, int nk, co
     gm.tops[l] = NI;
     NI += gmd->ngz[l];
   }
-  const size_t nx = ni + 6, ny = nj + 6, nz = nk + 6, n = nx * ny * nz;
   const float *X = coord, *Y = coord + n;
   float xmin = X[0], xmax = X[0], ymin = Y[0], ymax = Y[0];  // gd_curv_set_minmax
   for (size_t t = 0; t < n; t++) {
     xmin = std::min(xmin, X[t]); xmax = std::max(xmax, X[t]);
     ymin = std::min(ymin, Y[t]); ymax = std::max(ymax, Y[t]);
   }
-  // the part of the mesh read_grid_file keeps (media_read_file.cpp:774-800), float arithmetic as
-  // there; a grid beyond the mesh is refused (where the reference's check lets it through, it
-  // reads values it never stored)
   const float MINX = gmd->x0, MINY = gmd->y0, DX = gmd->dx, DY = gmd->dy;
   if (xmin < MINX || ymin < MINY) {
     set_last_error("grid model: the given media range is smaller than the calculation grid range");
@@ -1298,20 +1415,43 @@ extern "C" int cgfd_media_grid_el_iso_gpu(int device, int ni, int nj, int nk, co
     set_last_error("grid model: the given media range is smaller than the calculation grid range");
     return CGFD_ERR_INVALID;
   }
-  const size_t cnx = ix1 - ix0 + 1, cny = iy1 - iy0 + 1, csl = cnx * cny;
-  std::vector<float> cut((size_t)4 * NI * csl);  // elevation, rho, vp, vs of the kept mesh
-  const size_t fsl = (size_t)gmd->nx * gmd->ny;
-  for (int q = 0; q < 4; q++) {
+  const size_t cnx = ix1 - ix0 + 1, cny = iy1 - iy0 + 1, csl = cnx * cny, fsl = (size_t)gmd->nx * gmd->ny;
+  cut.assign((size_t)(1 + npar) * NI * csl, 0.f);
+  for (int q = 0; q <= npar; q++) {
     const float *src = q == 0 ? gmd->elevation : gmd->param + (size_t)(q - 1) * NI * fsl;
-    for (int s = 0; s < NI; s++)
+    for (int sfc = 0; sfc < NI; sfc++)
       for (size_t iy = 0; iy < cny; iy++)
         for (size_t ix = 0; ix < cnx; ix++)
-          cut[((size_t)q * NI + s) * csl + iy * cnx + ix] = src[s * fsl + (iy0 + iy) * gmd->nx + ix0 + ix];
+          cut[((size_t)q * NI + sfc) * csl + iy * cnx + ix] = src[sfc * fsl + (iy0 + iy) * gmd->nx + ix0 + ix];
   }
   gm.m.ni_ = NI; gm.m.nx = (int)cnx; gm.m.ny = (int)cny;
   gm.m.x0 = (float)ix0 * DX + MINX;
   gm.m.y0 = (float)iy0 * DY + MINY;
   gm.m.dx = DX; gm.m.dy = DY;
+  return CGFD_OK;
+}
+
+}  // namespace
+}  // namespace cgfd
+
+extern "C" int cgfd_media_grid_el_iso_gpu(int device, int ni, int nj, int nk, const float *coord,
+                                          const cgfd_grid_media *gmd, int method, float *medium) {
+  using namespace cgfd;
+  if (!coord || !gmd || !medium || !gmd->ngz || !gmd->elevation || !gmd->param || ni < 4 || nj < 4 || nk < 4 ||
+      method < CGFD_MEDIA_LOC || method > CGFD_MEDIA_ARI) {
+    set_last_error("invalid argument");
+    return CGFD_ERR_INVALID;
+  }
+  if (gmd->type != CGFD_LAYER_ELASTIC_ISO) {
+    set_last_error("grid model: an elastic_isotropic file is required");
+    return CGFD_ERR_INVALID;
+  }
+  const size_t nx = ni + 6, ny = nj + 6, nz = nk + 6, n = nx * ny * nz;
+  GridMediaDev gm;
+  std::vector<float> cut;
+  if (const int rc = grid_setup(gmd, 3, coord, n, cut, gm)) return rc;
+  const int NL = gm.nl, NI = gm.m.ni_;
+  const size_t csl = (size_t)gm.m.nx * gm.m.ny;
 
   std::vector<void *> owned;
   cudaStream_t st = nullptr;
@@ -1375,4 +1515,113 @@ extern "C" int cgfd_media_grid_el_iso_gpu(int device, int ni, int nj, int nk, co
     return CGFD_ERR_INVALID;
   }
   return CGFD_OK;
+}
+
+extern "C" int cgfd_media_grid_gpu(int device, int ni, int nj, int nk, const float *coord,
+                                   const cgfd_grid_media *gmd, int medium_type, int method, float *medium) {
+  using namespace cgfd;
+  if (!coord || !gmd || !medium || ni < 4 || nj < 4 || nk < 4 || method < CGFD_MEDIA_LOC || method > CGFD_MEDIA_ARI) {
+    set_last_error("invalid argument");
+    return CGFD_ERR_INVALID;
+  }
+  const int T = gmd->type;
+  // the file types each target medium accepts (media_grid2model_el_iso / _el_vti / _el_aniso; the
+  // grid reader has no TTI-Bond branch)
+  const bool vti_file = T >= CGFD_LAYER_VTI_PREM && T <= CGFD_LAYER_VTI_CIJ;
+  const bool ok = (medium_type == CGFD_MEDIUM_ELASTIC_ISO && T == CGFD_LAYER_ELASTIC_ISO) ||
+                  (medium_type == CGFD_MEDIUM_ELASTIC_VTI && vti_file) ||
+                  (medium_type == CGFD_MEDIUM_ELASTIC_ANISO &&
+                   (T == CGFD_LAYER_ELASTIC_ISO || vti_file || T == CGFD_LAYER_TTI_THOMSEN || T == CGFD_LAYER_ANISO_CIJ));
+  if (!ok) {
+    set_last_error("grid file type not usable for this medium type");
+    return CGFD_ERR_INVALID;
+  }
+  if (medium_type == CGFD_MEDIUM_ELASTIC_ISO) return cgfd_media_grid_el_iso_gpu(device, ni, nj, nk, coord, gmd, method, medium);
+  const size_t nx = ni + 6, ny = nj + 6, nz = nk + 6, n = nx * ny * nz;
+  std::vector<float> fam;
+  int nfam = 0;
+  if (T == CGFD_LAYER_ELASTIC_ISO) {
+    fam.resize(3 * n);
+    nfam = 3;
+    if (const int rc = cgfd_media_grid_el_iso_gpu(device, ni, nj, nk, coord, gmd, method, fam.data())) return rc;
+    return family_to_medium(fam, nfam, medium_type, n, medium);
+  }
+  nfam = vti_file ? 6 : 22;
+  const int npar = vti_file ? 6 : (T == CGFD_LAYER_ANISO_CIJ ? 22 : 8);
+  GridMediaDev gm;
+  std::vector<float> cut;
+  if (const int rc = grid_setup(gmd, npar, coord, n, cut, gm)) return rc;
+  const size_t ps = (size_t)gm.m.ni_ * gm.m.nx * gm.m.ny;
+
+  std::vector<void *> owned;
+  cudaStream_t st = nullptr;
+  auto cleanup = [&] {
+    for (void *q : owned) cudaFree(q);
+    if (st) cudaStreamDestroy(st);
+  };
+  auto fail = [&](cudaError_t e, const char *what) {
+    cleanup();
+    set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? CGFD_ERR_NOMEM : CGFD_ERR_CUDA;
+  };
+  auto dalloc = [&](size_t bytes, void **out) {
+    cudaError_t e = cudaMalloc(out, bytes);
+    if (e == cudaSuccess) owned.push_back(*out);
+    return e;
+  };
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return fail(e, "cudaSetDevice");
+  if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "cudaStreamCreate");
+  float *dm = nullptr, *dc = nullptr, *dout = nullptr, *dh = nullptr;
+  int *derr = nullptr, *dmat = nullptr;
+  if ((e = dalloc(cut.size() * sizeof(float), (void **)&dm)) != cudaSuccess) return fail(e, "cudaMalloc");
+  if ((e = dalloc(3 * n * sizeof(float), (void **)&dc)) != cudaSuccess) return fail(e, "cudaMalloc");
+  if ((e = dalloc((size_t)nfam * n * sizeof(float), (void **)&dout)) != cudaSuccess) return fail(e, "cudaMalloc");
+  if ((e = dalloc(sizeof(int), (void **)&derr)) != cudaSuccess) return fail(e, "cudaMalloc");
+  if ((e = cudaMemcpyAsync(dm, cut.data(), cut.size() * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(dc, coord, 3 * n * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return fail(e, "cudaMemcpy");
+  cudaMemsetAsync(derr, 0, sizeof(int), st);
+  gm.m.elev = dm;
+  gm.m.par = dm + ps;
+  GridDev g{};
+  g.nx = (int)nx; g.ny = (int)ny; g.nz = (int)nz;
+  g.x = dc; g.y = dc + n; g.z = dc + 2 * n;
+  const bool avg = method != CGFD_MEDIA_LOC && gm.nl >= 2;
+  if (avg) {
+    if ((e = dalloc(3 * n * sizeof(float), (void **)&dh)) != cudaSuccess) return fail(e, "cudaMalloc");
+    if ((e = dalloc(n * sizeof(int), (void **)&dmat)) != cudaSuccess) return fail(e, "cudaMalloc");
+    g.hx = dh; g.hy = dh + n; g.hz = dh + 2 * n;
+    g.mat = dmat;
+  }
+  OutDev o{(long long)n, dout, derr};
+  auto run = [&](auto tag) {
+    constexpr int TT = decltype(tag)::value;
+    k_grid_loc_gen<TT><<<148 * 8, 256, 0, st>>>(gm, g, o);
+    if (!avg) return;
+    k_half_grid<<<148 * 8, 256, 0, st>>>(g);
+    k_grid_mark<<<148 * 8, 256, 0, st>>>(gm, g);
+    if (method == CGFD_MEDIA_HAR) k_grid_avg_gen<TT, true><<<148 * 8, 128, 0, st>>>(gm, g, o);
+    else k_grid_avg_gen<TT, false><<<148 * 8, 128, 0, st>>>(gm, g, o);
+  };
+  switch (T) {
+    case CGFD_LAYER_VTI_PREM: run(std::integral_constant<int, 22>()); break;
+    case CGFD_LAYER_VTI_THOMSEN: run(std::integral_constant<int, 23>()); break;
+    case CGFD_LAYER_VTI_CIJ: run(std::integral_constant<int, 24>()); break;
+    case CGFD_LAYER_TTI_THOMSEN: run(std::integral_constant<int, 25>()); break;
+    default: run(std::integral_constant<int, 27>()); break;
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "media kernels");
+  int herr = 0;
+  fam.resize((size_t)nfam * n);
+  if ((e = cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(fam.data(), dout, (size_t)nfam * n * sizeof(float), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return fail(e, "cudaMemcpy");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail(e, "cudaStreamSynchronize");
+  cleanup();
+  if (herr) {
+    set_last_error("a grid point lies outside the media grid mesh");
+    return CGFD_ERR_INVALID;
+  }
+  return family_to_medium(fam, nfam, medium_type, n, medium);
 }

@@ -409,13 +409,14 @@ int run(int argc, char **argv) {
     if (cgfd_media_layer_gpu(gpu, g.ni, g.nj, g.nk, coord.data(), &lf.media(), d.medium_type, method, medium.data()))
       fail(std::string("media on the GPU: ") + cgfd_last_error());
   } else if (way == "infile_grid") {
-    // grid model discretised on the GPU (media_grid2model_el_iso, main_curv_col_el_3d.cu:365-379)
-    if (d.medium_type != CGFD_MEDIUM_ELASTIC_ISO) fail("medium input_way 'infile_grid' is read for elastic_iso media only");
+    // grid model discretised on the GPU (media_grid2model_el_iso / _el_vti / _el_aniso,
+    // main_curv_col_el_3d.cu:365-420; the reference reads no acoustic grid files there)
+    if (d.medium_type == CGFD_MEDIUM_ACOUSTIC_ISO) fail("medium input_way 'infile_grid' is read for elastic media only");
     cgfd::fmt::GridFile gf = cgfd::fmt::read_grid_file(need(md, "infile_grid").as_str());
     const std::string em = md.get("equivalent_medium_method") ? md.get("equivalent_medium_method")->as_str() : "loc";
     const int method = em == "loc" ? CGFD_MEDIA_LOC : em == "har" ? CGFD_MEDIA_HAR : em == "ari" ? CGFD_MEDIA_ARI : -1;
     if (method < 0) fail("equivalent_medium_method '" + em + "' must be loc, har or ari");
-    if (cgfd_media_grid_el_iso_gpu(gpu, g.ni, g.nj, g.nk, coord.data(), &gf.desc(), method, medium.data()))
+    if (cgfd_media_grid_gpu(gpu, g.ni, g.nj, g.nk, coord.data(), &gf.desc(), d.medium_type, method, medium.data()))
       fail(std::string("media on the GPU: ") + cgfd_last_error());
   } else if (way == "binfile") {
     // 3-D binary model discretised on the GPU (media_bin2model_el_iso, main_curv_col_el_3d.cu:439-458;

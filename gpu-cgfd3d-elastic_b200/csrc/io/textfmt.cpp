@@ -187,8 +187,13 @@ GridFile read_grid_file(const std::string &path) {
   GridFile G;
   std::string type;
   if (!(in >> type)) throw std::runtime_error(path + ": no media type");
-  if (type != "elastic_isotropic")
-    throw std::runtime_error(path + ": grid media of type '" + type + "' are not on this path (elastic_isotropic)");
+  static const struct { const char *name; int type, npar; } kTypes[] = {
+      {"elastic_isotropic", CGFD_LAYER_ELASTIC_ISO, 3},     {"elastic_vti_prem", CGFD_LAYER_VTI_PREM, 6},
+      {"elastic_vti_thomsen", CGFD_LAYER_VTI_THOMSEN, 6}, {"elastic_vti_cij", CGFD_LAYER_VTI_CIJ, 6},
+      {"elastic_tti_thomsen", CGFD_LAYER_TTI_THOMSEN, 8}, {"elastic_aniso_cij", CGFD_LAYER_ANISO_CIJ, 22}};
+  for (const auto &t : kTypes)
+    if (type == t.name) { G.type = t.type; G.npar = t.npar; }
+  if (!G.type) throw std::runtime_error(path + ": grid media of type '" + type + "' are not on this path");
   int nl = 0;
   if (!(in >> nl) || nl < 1) throw std::runtime_error(path + ": number of layers missing or < 1");
   for (int l = 0; l < nl; l++) {
@@ -201,10 +206,10 @@ GridFile read_grid_file(const std::string &path) {
     throw std::runtime_error(path + ": mesh line must be NX NY MINX MINY DX DY with NX, NY >= 2");
   const size_t sl = (size_t)G.nx * G.ny, n = (size_t)G.ni * sl;
   G.elevation.resize(n);
-  G.param.resize(3 * n);
+  G.param.resize((size_t)G.npar * n);
   for (size_t p = 0; p < n; p++) {
     if (!(in >> G.elevation[p])) throw std::runtime_error(path + ": insufficient data");
-    for (int q = 0; q < 3; q++)
+    for (int q = 0; q < G.npar; q++)
       if (!(in >> G.param[(size_t)q * n + p])) throw std::runtime_error(path + ": insufficient data");
   }
   int s = 0;
@@ -219,6 +224,7 @@ GridFile read_grid_file(const std::string &path) {
 }
 
 const cgfd_grid_media &GridFile::desc() {
+  d.type = type;
   d.num_layers = (int)ngz.size();
   d.ngz = ngz.data();
   d.nx = nx; d.ny = ny;

@@ -50,16 +50,17 @@ struct LayerFile {
 };
 LayerFile read_layer_file(const std::string &path);
 
-// Grid media file of elastic_isotropic type (read_grid_file, media_read_file.cpp:670-960): the type
+// Grid media file (read_grid_file, media_read_file.cpp:670-1266) of the elastic types: the type
 // name, the number of layers, the surfaces of each layer, "NX NY MINX MINY DX DY", then per
-// surface and mesh point (x fastest) elevation rho vp vs; a layer's last surface must lie on the
-// next layer's first (checkGridData, :1242-1266).
+// surface and mesh point (x fastest) the elevation and the type's parameters; a layer's last
+// surface must lie on the next layer's first (checkGridData, :1242-1266).
 struct GridFile {
+  int type = 0, npar = 0;  // CGFD_LAYER_*
   std::vector<int> ngz;
   int ni = 0, nx = 0, ny = 0;
   float x0 = 0, y0 = 0, dx = 0, dy = 0;
   std::vector<float> elevation;  // [ni][ny][nx]
-  std::vector<float> param;      // [3][ni][ny][nx]: rho vp vs
+  std::vector<float> param;      // [npar][ni][ny][nx]
   cgfd_grid_media d{};
   const cgfd_grid_media &desc();
 };

@@ -558,18 +558,20 @@ int cgfd_media_bin_el_iso_gpu(int device, int ni, int nj, int nk, const float *c
                               float *medium);
 
 /*
- * A grid model of elastic_isotropic type (the par file's medium input_way "infile_grid",
- * read_grid_file, media_read_file.cpp:670-960): num_layers layers, layer l described by ngz[l]
- * surfaces (NI = sum of ngz) on a uniform nx x ny mesh, top first; per surface and mesh point the
- * elevation and rho, vp, vs (no gradients).
+ * A grid model (the par file's medium input_way "infile_grid", read_grid_file,
+ * media_read_file.cpp:670-1266): num_layers layers, layer l described by ngz[l] surfaces (NI = sum
+ * of ngz) on a uniform nx x ny mesh, top first; per surface and mesh point the elevation and the
+ * parameters of the file type (CGFD_LAYER_ELASTIC_ISO, _VTI_PREM, _VTI_THOMSEN, _VTI_CIJ,
+ * _TTI_THOMSEN or _ANISO_CIJ: the parameters listed above, values only, no gradients).
  */
 typedef struct cgfd_grid_media {
+  int   type;                    /* CGFD_LAYER_*                                            */
   int   num_layers;
   const int *ngz;                /* [num_layers] */
   int   nx, ny;
   float x0, y0, dx, dy;
   const float *elevation;        /* [NI][ny][nx] */
-  const float *param;            /* [3][NI][ny][nx]: rho, vp, vs */
+  const float *param;            /* [npar][NI][ny][nx], the type's parameters in file order */
 } cgfd_grid_media;
 
 /*
@@ -585,6 +587,19 @@ typedef struct cgfd_grid_media {
  */
 int cgfd_media_grid_el_iso_gpu(int device, int ni, int nj, int nk, const float *coord, const cgfd_grid_media *model,
                                int method, float *medium);
+
+/*
+ * A grid model of any type on the GPU `device` into the cgfd_problem_desc medium of medium_type:
+ * iso from an elastic_isotropic file (as cgfd_media_grid_el_iso_gpu); VTI [rho c11 c13 c33 c55
+ * c66] from the PREM, Thomsen and Cij VTI files; 21-Cij from any of the six file types (iso and VTI
+ * results expanded to the full tensor). The surfaces' parameters are interpolated in elevation,
+ * then converted to stiffness as for layer files; har / ari average every c_ij harmonically /
+ * arithmetically over the sub-points off the layer tops (rho arithmetically).
+ * Replaces: media_grid2model_el_vti / _el_aniso (src/media/media_grid2model.cpp:190-422) with
+ * parametrization_grid_el_{vti,aniso}_{loc,har,ari} (:1127-1267, 2080-2793).
+ */
+int cgfd_media_grid_gpu(int device, int ni, int nj, int nk, const float *coord, const cgfd_grid_media *model,
+                        int medium_type, int method, float *medium);
 
 /*
  * Largest stable time step (FP64): CFL * min distance to the 8 neighbour planes / Vp.

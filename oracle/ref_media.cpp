@@ -61,3 +61,21 @@ extern "C" int ref_media_grid2model_el_iso(float *rho3d, float *lam3d, float *mu
   return media_grid2model_el_iso(rho3d, lam3d, mu3d, x3d, y3d, z3d, nx, ny, nz, xmin, xmax, ymin, ymax, GRID_CURV,
                                  in_media_file, method, 1);
 }
+
+// media_grid2model_el_vti (media_grid2model.cpp:190-248): rho, c11, c33, c55, c66, c13
+extern "C" int ref_media_grid2model_el_vti(float *const *out, const float *x3d, const float *y3d, const float *z3d,
+                                           int nx, int ny, int nz, float xmin, float xmax, float ymin, float ymax,
+                                           const char *in_media_file, const char *method) {
+  return media_grid2model_el_vti(out[0], out[1], out[2], out[3], out[4], out[5], x3d, y3d, z3d, nx, ny, nz, xmin,
+                                 xmax, ymin, ymax, GRID_CURV, in_media_file, method, 1);
+}
+
+// media_grid2model_el_aniso (media_grid2model.cpp:250-422): out[0] rho, out[1..21] c11 .. c66
+extern "C" int ref_media_grid2model_el_aniso(float *const *out, const float *x3d, const float *y3d, const float *z3d,
+                                             int nx, int ny, int nz, float xmin, float xmax, float ymin, float ymax,
+                                             const char *in_media_file, const char *method) {
+  return media_grid2model_el_aniso(out[0], out[1], out[2], out[3], out[4], out[5], out[6], out[7], out[8], out[9],
+                                   out[10], out[11], out[12], out[13], out[14], out[15], out[16], out[17], out[18],
+                                   out[19], out[20], out[21], x3d, y3d, z3d, nx, ny, nz, xmin, xmax, ymin, ymax,
+                                   GRID_CURV, in_media_file, method, 1);
+}

@@ -130,3 +130,29 @@ def grid2model_el_iso(coord, model, method=0):
                 float(c[1].max()), path.encode(), METHODS[method])
     assert rc == 0
     return np.stack([rho, lam, mu])
+
+
+def grid2model(coord, model, medium_type, method=0):
+    """The medium of medium_type (2 iso, 3 VTI [rho c11 c13 c33 c55 c66], 4 21-Cij [rho c11 ... c66])
+    from the grid model (formats.GridMedia) by the reference's media_grid2model_el_iso / _el_vti /
+    _el_aniso on the grid coord."""
+    if medium_type == 2:
+        return grid2model_el_iso(coord, model, method)
+    L = C.CDLL(LIB)
+    fn = L.ref_media_grid2model_el_vti if medium_type == 3 else L.ref_media_grid2model_el_aniso
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p] * 4 + [C.c_int] * 3 + [C.c_float] * 4 + [C.c_char_p, C.c_char_p]
+    _, nz, ny, nx = coord.shape
+    c = np.ascontiguousarray(coord, np.float32)
+    nf = 6 if medium_type == 3 else 22
+    f = [np.zeros((nz, ny, nx), np.float32) for _ in range(nf)]
+    ptrs = (C.c_void_p * nf)(*[a.ctypes.data for a in f])
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "model.grd")
+        formats.write_grid_media_file(path, model)
+        rc = fn(ptrs, c[0].ctypes.data, c[1].ctypes.data, c[2].ctypes.data, nx, ny, nz, float(c[0].min()),
+                float(c[0].max()), float(c[1].min()), float(c[1].max()), path.encode(), METHODS[method])
+    assert rc == 0
+    if medium_type == 3:  # rho c11 c33 c55 c66 c13 -> the description's rho c11 c13 c33 c55 c66
+        return np.stack([f[0], f[1], f[5], f[2], f[3], f[4]])
+    return np.stack(f)

@@ -255,26 +255,28 @@ def test_cli_binary_medium_matches_oracle(tmp_path):
     assert per_station_rel_l2(got, ref) <= 1e-4
 
 
-def test_cli_grid_medium_matches_oracle(tmp_path):
-    """medium input_way "infile_grid" (elastic_iso, har): the CLI discretises the grid file on the
-    GPU; its seismograms equal the oracle's run on the medium the reference's own
-    media_grid2model_el_iso builds from the same file (per-station rel L2 <= 1e-4)."""
+@pytest.mark.parametrize("med,ftype", [("iso", 21), ("vti", 23)])
+def test_cli_grid_medium_matches_oracle(tmp_path, med, ftype):
+    """medium input_way "infile_grid" (har): an elastic_isotropic grid file into an iso medium and
+    a Thomsen VTI grid file into a VTI medium. The CLI discretises the file on the GPU; its
+    seismograms equal the oracle's run on the medium the reference's own media_grid2model_el_iso /
+    _el_vti builds from the same file (per-station rel L2 <= 1e-4)."""
     import media_ref
     if not media_ref.available():
         pytest.skip("oracle/_ref/libref_media.so not built")
     from cgfd_b200 import synth
     nsteps = 60
-    p = small_problem("iso", nsteps=nsteps)
-    model = synth.grid_media(p.coord, seed=4)
+    p = small_problem(med, nsteps=nsteps)
+    model = synth.grid_media(p.coord, seed=4, type=ftype)
     path = os.path.join(str(tmp_path), "model.grd")
     formats.write_grid_media_file(path, model)
-    medium = {"type": "elastic_iso", "input_way": "infile_grid", "infile_grid": path,
+    medium = {"type": "elastic_" + med, "input_way": "infile_grid", "infile_grid": path,
               "equivalent_medium_method": "har"}
     par = formats.write_case(str(tmp_path), p, nsteps, extra={"medium": medium})
     r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     p.metric = synth.metrics(p.coord)
-    p.medium = media_ref.grid2model_el_iso(p.coord, model, 1)
+    p.medium = media_ref.grid2model(p.coord, model, {"iso": 2, "vti": 3}[med], 1)
     orc = Oracle(p)
     orc.run()
     ref = orc.seismograms()

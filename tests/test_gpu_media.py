@@ -149,3 +149,36 @@ def test_gpu_grid_media_rejects_a_mesh_smaller_than_the_grid():
     with pytest.raises(CgfdError) as e:
         media_grid_gpu(coord, model, 0)
     assert e.value.code == -1
+
+
+# (grid file type, target medium type): VTI files into VTI media, the other types into 21-Cij
+GRID_CASES = [(22, 3), (23, 3), (24, 3), (21, 4), (23, 4), (25, 4), (27, 4)]
+
+
+@pytest.mark.parametrize("method", [0, 1, 2])
+@pytest.mark.parametrize("ftype,medium", GRID_CASES)
+def test_gpu_grid_media_any_type_matches_reference(ftype, medium, method):
+    """cgfd_media_grid_gpu against the reference's media_grid2model_el_vti / _el_aniso on the same
+    grid and grid file: every field within 1e-6 of its largest magnitude (the TTI file: 2e-5, its
+    sines and cosines from another math library), at least 99% bitwise equal without a rotation.
+    As for the layer files, under the harmonic average the c_ij of the TTI file whose values
+    change sign across the grid are left out (their harmonic mean divides by sums near zero)."""
+    from cgfd_b200 import media_grid_gpu
+    coord = synth.curvilinear_grid(40, 36, 32, 100.0, seed=7)
+    model = synth.grid_media(coord, seed=3, type=ftype)
+    ref = media_ref.grid2model(coord, model, medium, method)
+    got = media_grid_gpu(coord, model, method, medium_type=medium)
+    assert got.shape == ref.shape and np.isfinite(ref).all() and (ref[0] > 0).all()
+    tol = 2e-5 if ftype == 25 else 1e-6
+    loc = media_ref.grid2model(coord, model, medium, 0) if method == 1 and ftype == 25 else None
+    for f in range(ref.shape[0]):
+        if loc is not None and (loc[f] > 0).any() and (loc[f] < 0).any():
+            assert np.isfinite(got[f]).all()
+            continue
+        scale = float(np.abs(ref[f]).max())
+        if scale == 0.0:
+            assert not got[f].any(), f
+            continue
+        assert float(np.abs(got[f].astype(np.float64) - ref[f]).max()) <= tol * scale, f
+    if ftype != 25:
+        assert (got == ref).mean() >= 0.99
