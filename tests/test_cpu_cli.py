@@ -58,3 +58,30 @@ def test_cli_dt_check_rejects_unstable_step(tmp_path):
     par = formats.write_case(str(tmp_path), p, 2)
     r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "> dtmax" in r.stderr
+
+
+def test_cli_reads_grid_and_binary_media_files(tmp_path):
+    """The media file readers run before the device: a grid file whose layer boundary surfaces
+    differ is refused as read_grid_file's checkGridData does, and a binary model file shorter than
+    its size is refused ("Insufficient data", read_bin_file)."""
+    import json
+    from cgfd_b200 import synth
+    p = small_problem("iso", nsteps=2)
+    par = formats.write_case(str(tmp_path), p, 2)
+    cfg = json.load(open(par))
+    model = synth.grid_media(p.coord, seed=4)
+    model.elevation[model.ngz[0]] += 1.0  # the second layer's first surface leaves the first's last
+    grd = os.path.join(str(tmp_path), "model.grd")
+    formats.write_grid_media_file(grd, model)
+    cfg["medium"] = {"type": "elastic_iso", "input_way": "infile_grid", "infile_grid": grd,
+                     "equivalent_medium_method": "loc"}
+    json.dump(cfg, open(par, "w"))
+    r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "must equal the first elevations" in r.stderr, r.stderr
+    medium = formats.write_bin_model(os.path.join(str(tmp_path), "bin"), synth.bin_model(p.coord, seed=4))
+    with open(medium["binfile"]["Vs"], "r+b") as f:
+        f.truncate(100)
+    cfg["medium"] = medium
+    json.dump(cfg, open(par, "w"))
+    r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "Insufficient data" in r.stderr, r.stderr
