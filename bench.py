@@ -99,6 +99,13 @@ def profile_run(args):
         sim = Simulation(p)
     sim.set_graph_mode(0)
     sim.run(args.profile_steps)
+    # per-kernel CUDA-event times of 8 more steps (not for use under ncu)
+    sim.set_timing(True)
+    sim.timing(reset=True)
+    sim.run(8)
+    sim.synchronize()
+    bulk_ms, bulk_n = sim.timing(reset=True)["bulk"]
+    sim.set_timing(False)
     pts = 0
     for f in names:
         n = [p.ni, p.nj, p.nk]
@@ -107,7 +114,7 @@ def profile_run(args):
     bulk = p.ni * p.nj * (p.nk if args.medium == "ac" or not p.free_top else p.nk - 4)
     print(f"profile case {p.ni}x{p.nj}x{p.nk} medium={args.medium} faces={names or 'none'} layers={nl} "
           f"shots={args.shots} precision={args.precision}: {args.profile_steps} steps, face points {pts}, "
-          f"bulk cells {bulk}", flush=True)
+          f"bulk cells {bulk}; event-timed bulk stage {bulk_ms / max(bulk_n, 1):.4f} ms", flush=True)
     sim.close()
     return 0
 
