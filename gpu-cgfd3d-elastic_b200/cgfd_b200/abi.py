@@ -15,6 +15,7 @@ CGFD_MEDIUM_ACOUSTIC_ISO = 1
 CGFD_MEDIUM_ELASTIC_ISO = 2
 CGFD_MEDIUM_ELASTIC_VTI = 3
 CGFD_MEDIUM_ELASTIC_ANISO = 4
+CGFD_MEDIUM_VISCO_ISO = 5
 CGFD_ERR_BUSY = -7
 CGFD_ERR_NOMEM = -3
 CGFD_PREC_FP32 = 0
@@ -54,17 +55,23 @@ class StationDesc(C.Structure):
                 ("loc", C.c_void_p)]
 
 
+class ViscoDesc(C.Structure):
+    """cgfd_visco_desc: GMB parameters of a visco-elastic medium (par_t.cu:728-770)."""
+    _fields_ = [("nmaxwell", C.c_int), ("fr", C.c_float), ("fmin", C.c_float), ("fmax", C.c_float)]
+
+
 class ProblemDesc(C.Structure):
     _fields_ = [("ni", C.c_int), ("nj", C.c_int), ("nk", C.c_int), ("medium_type", C.c_int),
                 ("coord", C.c_void_p), ("metric", C.c_void_p), ("medium", C.c_void_p),
                 ("pml", (PmlFace * 2) * 3), ("free_top", C.c_int), ("dt", C.c_float),
                 ("t0", C.c_float), ("nt_total", C.c_int), ("src", SourceDesc),
-                ("sta", StationDesc), ("precision", C.c_int), ("device", C.c_int)]
+                ("sta", StationDesc), ("precision", C.c_int), ("device", C.c_int),
+                ("visco", C.POINTER(ViscoDesc))]
 
 
 def medium_ncmp(medium_type):
     return {CGFD_MEDIUM_ACOUSTIC_ISO: 2, CGFD_MEDIUM_ELASTIC_ISO: 3, CGFD_MEDIUM_ELASTIC_VTI: 6,
-            CGFD_MEDIUM_ELASTIC_ANISO: 22}[medium_type]
+            CGFD_MEDIUM_ELASTIC_ANISO: 22, CGFD_MEDIUM_VISCO_ISO: 5}[medium_type]
 
 
 def ref_shape(ni, nj, nk):
@@ -130,6 +137,8 @@ class Problem:
     sta: Optional[Stations] = None
     precision: int = CGFD_PREC_FP32
     device: int = 0
+    # visco-elastic media (medium rho lambda mu Qp Qs): {"nmaxwell", "fr", "fmin", "fmax"}
+    visco: Optional[dict] = None
 
     def desc(self):
         """Build the C description; the returned object keeps every array alive."""
@@ -172,6 +181,11 @@ class Problem:
             d.sta.loc = _ptr(arr(t.loc, np.float32))
         d.precision = int(self.precision)
         d.device = int(self.device)
+        if self.visco is not None:
+            v = self.visco
+            vd = ViscoDesc(int(v["nmaxwell"]), float(v["fr"]), float(v["fmin"]), float(v["fmax"]))
+            d._visco = vd
+            d.visco = C.pointer(vd)
         return d
 
 
@@ -382,6 +396,7 @@ def lib():
         "cgfd_set_bulk_variant": (C.c_int, [P, C.c_int]),
         "cgfd_get_timing": (C.c_int, [P, P, P, P, C.c_int]),
         "cgfd_fill_ghosts": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P]),
+        "cgfd_visco_gmb": (C.c_int, [P, C.c_longlong, P, P, P, P, P, P, P, P, P]),
         "cgfd_metric_calc": (C.c_int, [C.c_int, C.c_int, C.c_int, P, P]),
         "cgfd_metric_calc_gpu": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, P]),
         "cgfd_media_layer_el_iso_gpu": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, P, C.c_int, P]),
@@ -666,3 +681,17 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def visco_gmb(visco, lam, mu, qp, qs):
+    """cgfd_visco_gmb: the GMB fit of n points. Returns (lam_u, mu_u, Ylam [nmax, n], Ymu [nmax, n],
+    wl [nmax])."""
+    lam, mu, qp, qs = (np.ascontiguousarray(np.ravel(a), np.float32) for a in (lam, mu, qp, qs))
+    n, nm = lam.size, int(visco["nmaxwell"])
+    vd = ViscoDesc(nm, float(visco["fr"]), float(visco["fmin"]), float(visco["fmax"]))
+    lu, mu_u = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    yl, ym = np.zeros((max(nm, 1), n), np.float32), np.zeros((max(nm, 1), n), np.float32)
+    wl = np.zeros(max(nm, 1), np.float32)
+    check(lib().cgfd_visco_gmb(C.addressof(vd), n, lam.ctypes.data, mu.ctypes.data, qp.ctypes.data, qs.ctypes.data,
+                               lu.ctypes.data, mu_u.ctypes.data, yl.ctypes.data, ym.ctypes.data, wl.ctypes.data))
+    return lu, mu_u, yl, ym, wl

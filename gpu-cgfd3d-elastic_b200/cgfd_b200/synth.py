@@ -10,6 +10,7 @@ import ctypes as C
 import numpy as np
 
 from .abi import (CGFD_MEDIUM_ACOUSTIC_ISO, CGFD_MEDIUM_ELASTIC_ISO, CGFD_MEDIUM_ELASTIC_VTI, CGFD_MEDIUM_ELASTIC_ANISO, WAVELETS,
+                  CGFD_MEDIUM_VISCO_ISO,
                   Problem, Sources, Stations, lib, ref_shape, ProblemDesc)
 
 LAYERS_3 = [(4000.0, 2300.0, 2500.0), (5500.0, 3200.0, 2700.0), (6500.0, 3750.0, 2900.0)]
@@ -476,7 +477,7 @@ def make_problem(ni, nj, nk, dh, nsteps, dt=None, medium="iso", npml=12, nsrc=1,
     """
     coord = curvilinear_grid(ni, nj, nk, dh, seed=seed)
     metric = metrics(coord) if metric_fn is None else metric_fn(coord)
-    if medium == "iso":
+    if medium in ("iso", "vis"):
         pert = None
         if perturb_std > 0:
             pert = von_karman((nk, nj, ni), dh, corr=corr, hurst=hurst, std=perturb_std, seed=seed + 1)
@@ -506,6 +507,15 @@ def make_problem(ni, nj, nk, dh, nsteps, dt=None, medium="iso", npml=12, nsrc=1,
     if dt is None:
         dt = keep_three_digits(0.9 * dt_estimate(prob))
     prob.dt = float(dt)
+    if medium == "vis":
+        # visco-elastic: the iso layers with Qs = 20 + vs / 50 and Qp = 2 Qs, three GMB mechanisms
+        # over 0.2-20 Hz with the moduli given at 2 Hz (the time step above is the elastic one;
+        # the unrelaxed moduli are a few per cent stiffer, inside its 0.9 margin)
+        vs = np.sqrt(med[2] / np.maximum(med[0], 1e-9))
+        qs = np.round(20.0 + vs / 50.0).astype(np.float32)
+        prob.medium = np.concatenate([med, (2.0 * qs)[None], qs[None]]).astype(np.float32)
+        prob.medium_type = CGFD_MEDIUM_VISCO_ISO
+        prob.visco = {"nmaxwell": 3, "fr": 2.0, "fmin": 0.2, "fmax": 20.0}
     rng = np.random.default_rng(seed + 7)
     if nsrc:
         mk = ac_sources if medium == "ac" else dc_sources

@@ -147,6 +147,13 @@ struct cgfd_problem {
   int shape = 0;  // tile shape of the bulk kernel (cgfd_set_tile_shape; set per medium at creation)
 
   float *wbuf[4] = {nullptr, nullptr, nullptr, nullptr};  // [0],[1]: pre/end by parity; [2],[3]: tmpA/tmpB
+  // visco-elastic media (CGFD_MEDIUM_VISCO_ISO, run as iso media plus the attenuation pass):
+  // memory variables [nmax][6][sf] per level (same roles as wbuf), the anelastic weights
+  // [2 nmax][sf] (Ylam, then Ymu), the stage right-hand side [9][sf], the surface frame [nj][ni][9]
+  int vis = 0, nmax = 0;
+  float wl[10] = {};
+  float *jbuf[4] = {nullptr, nullptr, nullptr, nullptr};
+  float *d_y = nullptr, *d_rhs = nullptr, *d_matD = nullptr;
   // (real-typed arrays -- wbuf, coef, jac, matx/maty, PML A/B/D/aux, d_dis -- are held as float*
   // and hold doubles in the FP64 build; rptr() gives the typed, element-offset pointer)
   float *coef = nullptr, *jac = nullptr, *matx = nullptr, *maty = nullptr;
@@ -385,6 +392,69 @@ struct cgfd_problem {
     return n;
   }
 
+  // One time step of a visco-elastic problem (drv_rk_curv_col.cu:193-541 with
+  // sv_curv_col_vis_iso_onestage): per stage the iso kernels write the right-hand side (bulk
+  // planes, then the traction-image fluxes and the surface slab), the attenuation pass combines it
+  // with the memory variables, then the sources; after the last stage the surface stress fix.
+  int enqueue_step_vis(int step) {
+    cudaStream_t st = stream;
+    int n = 0;
+    if (rec.n > 0) {
+      cgfd::RecvPT<float> r;
+      r.nsta = rec.n; r.nshot = nshot; r.nt_total = nt_total; r.idx8 = d_idx8; r.w8 = d_w8;
+      r.pre = wbuf[step & 1]; r.sf = sf; r.seis = d_seis; r.d_it = d_it; r.d_flag = d_flag;
+      n += timed(6, [&] { return cgfd::launch_recv(r, st); });
+    }
+    n += enqueue_outputs<float>(step);
+    float *jpre = jbuf[step & 1], *jend = jbuf[(step + 1) & 1];
+    const float *jcurs[4] = {jpre, jbuf[2], jbuf[3], jbuf[2]};
+    float *jouts[4] = {jbuf[2], jbuf[3], jbuf[2], nullptr};
+    for (int s = 0; s < 4; s++) {
+      cgfd::StagePT<float> p = stage_params_t<float>(step, s);
+      p.rhs = d_rhs;
+      n += timed(s, [&] { return cgfd::launch_stage_bulk(cgfd::MED_ISO, p, nzc, st); });
+      if (free_top)
+        n += timed(4, [&] {
+          return cgfd::launch_timg_flux(coef_type, 0, p, st) + cgfd::launch_stage_surface(cgfd::MED_ISO, coef_type, 0, p, st);
+        });
+      cgfd::VisP v;
+      memset(&v, 0, sizeof(v));
+      v.ni = ni; v.nj = nj; v.nk = nk; v.nmax = nmax; v.stage = s;
+      v.sx = sx; v.sz = sz; v.sf = sf; v.off0 = off0;
+      v.rhs = d_rhs; v.cur = p.cur; v.pre = p.pre; v.tmp_out = p.tmp_out; v.end = p.end;
+      v.jcur = jcurs[s]; v.jpre = jpre; v.jtmp = jouts[s]; v.jend = jend;
+      v.coef = coef; v.y = d_y;
+      for (int m = 0; m < nmax; m++) v.wl[m] = wl[m];
+      v.ca = p.ca; v.cb = p.cb; v.err = d_flag;
+      n += timed(s, [&] { return cgfd::launch_vis_atten(v, st); });
+      if (src.nsrc > 0) {
+        cgfd::SrcPT<float> q;
+        memset(&q, 0, sizeof(q));
+        q.nsrc = src.nsrc; q.max_ext = src.max_ext; q.max_nt = src.max_nt;
+        q.force = src.force; q.moment = src.moment; q.stage = s;
+        q.ca = p.ca; q.cb = p.cb;
+        q.it_begin = d_it_begin; q.ext_num = d_ext_num; q.ext_idx = d_ext_idx;
+        q.ext_wv = d_ext_wv; q.ext_wt = d_ext_wt; q.stf = d_stf; q.src_shot = d_src_shot;
+        q.tmp_out = p.tmp_out; q.end = p.end; q.sf = sf; q.d_it = d_it;
+        n += timed(5, [&] { return cgfd::launch_source(q, st); });
+      }
+    }
+    if (free_top) {
+      cgfd::VisFreeP f;
+      f.ni = ni; f.nj = nj; f.sx = sx; f.sf = sf; f.off_top = off0 + (long long)(nk - 1) * sz;
+      f.w_end = wbuf[(step + 1) & 1]; f.matD = d_matD;
+      n += timed(4, [&] { return cgfd::launch_vis_free(f, st); });
+      cgfd::PgPT<float> q;
+      q.ni = ni; q.nj = nj; q.nshot = nshot; q.sx = sx; q.sf = sf;
+      q.off_top = off0 + (long long)(nk - 1) * sz;
+      q.w_end = wbuf[(step + 1) & 1]; q.w_pre = wbuf[step & 1];
+      q.pg = d_pg; q.dis = d_dis; q.dt = dt;
+      n += cgfd::launch_peak_motion(q, st);
+    }
+    n += cgfd::launch_advance(d_it, st);
+    return n;
+  }
+
   // One time step of an acoustic problem (drv_rk_curv_col.cu:193-541 with
   // sv_curv_col_ac_iso_onestage): per stage the free-surface pressure image of the stage input,
   // then the fused stage of every cell, then the sources; R float, or double in the FP64 build.
@@ -443,6 +513,7 @@ struct cgfd_problem {
   }
 
   int enqueue_step(int step) {
+    if (vis) return enqueue_step_vis(step);
     if (med == cgfd::MED_AC) return fp64 ? enqueue_step_ac<double>(step) : enqueue_step_ac<float>(step);
     if (fp64) return enqueue_step64(step);
     cudaStream_t st = stream;
@@ -552,6 +623,8 @@ struct cgfd_problem {
     if (stream) {  // everything below was allocated in the order of this stream
       const cudaStream_t st = stream;
       for (auto *p : wbuf) dfree(p, st);
+      for (auto *p : jbuf) dfree(p, st);
+      dfree(d_y, st); dfree(d_rhs, st); dfree(d_matD, st);
       dfree(coef, st); dfree(coef16, st); dfree(jac, st); dfree(matx, st); dfree(maty, st); dfree(d_flux, st);
       for (Face &f : faces) { dfree(f.A, st); dfree(f.B, st); dfree(f.D, st); dfree(f.aux, st); }
       dfree(d_it_begin, st); dfree(d_ext_num, st); dfree(d_src_shot, st); dfree(d_ext_idx, st); dfree(d_ext_wv, st);
@@ -798,7 +871,8 @@ void problem_bytes(const cgfd_problem_desc *d, int nshot, const cgfd_source_desc
   long long sx, sz, sf, off0;
   layout(d->ni, d->nj, d->nk, sx, sz, sf, off0);
   const bool ac = d->medium_type == CGFD_MEDIUM_ACOUSTIC_ISO;
-  const int ncoef = ac ? 11 : (d->medium_type == CGFD_MEDIUM_ELASTIC_ISO ? 12 : (d->medium_type == CGFD_MEDIUM_ELASTIC_VTI ? 15 : 31));
+  const bool vis = d->medium_type == CGFD_MEDIUM_VISCO_ISO;
+  const int ncoef = ac ? 11 : (d->medium_type == CGFD_MEDIUM_ELASTIC_ISO || vis ? 12 : (d->medium_type == CGFD_MEDIUM_ELASTIC_VTI ? 15 : 31));
   const bool f64 = d->precision == CGFD_PREC_FP64;
   const bool c16 = d->precision != CGFD_PREC_FP32 && !f64, w16 = d->precision == CGFD_PREC_FP16_WAVE;
   const size_t F = f64 ? sizeof(double) : sizeof(float);  // real-typed arrays
@@ -812,6 +886,8 @@ void problem_bytes(const cgfd_problem_desc *d, int nshot, const cgfd_source_desc
   const size_t high = waves + jac + coef32 + (c16 ? std::max(upload, coef16 + 8 * (size_t)ncoef) : upload);
   if (d->free_top && !ac)  // conversion matrices and traction-image fluxes (elastic media)
     r += (size_t)2 * 9 * d->ni * d->nj * F + (size_t)9 * cgfd::kFluxPlanes * (d->ni + 6) * (d->nj + 6) * nshot * F;
+  if (vis)  // memory variables (4 levels), anelastic weights, stage right-hand side, surface frame
+    r += (size_t)(4 * 6 + 2) * d->visco->nmaxwell * sf * F + (size_t)9 * sf * F + (size_t)9 * d->ni * d->nj * F;
   cgfd::PmlFaceHost fh[3][2];
   cgfd::pml_setup(d, fh);
   for (int a = 0; a < 3; a++)
@@ -895,6 +971,50 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   cgfd::validate_desc(d);
   if (nshot < 1 || nshot > 32767) throw cgfd::Error(CGFD_ERR_INVALID, "nshot must be in [1, 32767]");
   p->nshot = nshot;
+  // visco-elastic media: the GMB fit of the physical points on the host (cgfd_visco_gmb); the
+  // kernels then see the iso medium of the unrelaxed moduli plus the anelastic weights
+  cgfd_problem_desc dvis;
+  std::vector<float> vis_med, vis_y;
+  if (d->medium_type == CGFD_MEDIUM_VISCO_ISO) {
+    if (nshot != 1) throw cgfd::Error(CGFD_ERR_UNSUPPORTED, "visco-elastic media run one shot per problem");
+    cgfd::RefGrid g(d->ni, d->nj, d->nk);
+    const size_t N = g.siz_icmp;
+    const int nm = d->visco->nmaxwell;
+    const long long np = (long long)d->ni * d->nj * d->nk;
+    std::vector<float> l(np), m(np), qp(np), qs(np), lu(np), mu(np), yl((size_t)np * std::max(nm, 1)),
+        ym((size_t)np * std::max(nm, 1));
+    long long t = 0;
+    for (int k = 0; k < d->nk; k++)
+      for (int j = 0; j < d->nj; j++)
+        for (int i = 0; i < d->ni; i++, t++) {
+          const size_t ip = g.at(i, j, k);
+          l[t] = d->medium[N + ip]; m[t] = d->medium[2 * N + ip];
+          qp[t] = d->medium[3 * N + ip]; qs[t] = d->medium[4 * N + ip];
+        }
+    cgfd::visco_gmb(d->visco, np, l.data(), m.data(), qp.data(), qs.data(), lu.data(), mu.data(), yl.data(),
+                    ym.data(), p->wl);
+    p->vis = 1;
+    p->nmax = nm;
+    vis_med.assign(d->medium, d->medium + 3 * N);  // rho, lambda, mu; ghosts as given
+    vis_y.assign((size_t)2 * nm * N, 0.f);
+    t = 0;
+    for (int k = 0; k < d->nk; k++)
+      for (int j = 0; j < d->nj; j++)
+        for (int i = 0; i < d->ni; i++, t++) {
+          const size_t ip = g.at(i, j, k);
+          vis_med[N + ip] = lu[t];
+          vis_med[2 * N + ip] = mu[t];
+          for (int q = 0; q < nm; q++) {
+            vis_y[(size_t)q * N + ip] = yl[(size_t)q * np + t];
+            vis_y[(size_t)(nm + q) * N + ip] = ym[(size_t)q * np + t];
+          }
+        }
+    dvis = *d;
+    dvis.medium_type = CGFD_MEDIUM_ELASTIC_ISO;
+    dvis.medium = vis_med.data();
+    dvis.visco = nullptr;
+    d = &dvis;
+  }
   p->precision = d->precision;
   switch (d->precision) {
     case CGFD_PREC_BF16_COEF: p->coef_type = cgfd::COEF_BF16; break;
@@ -906,7 +1026,7 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   p->wave16 = d->precision == CGFD_PREC_FP16_WAVE ? 1 : 0;
   p->fp64 = d->precision == CGFD_PREC_FP64 ? 1 : 0;
   p->esz = p->fp64 ? sizeof(double) : sizeof(float);
-  if (p->fp64) p->use_tma = false;  // the FP64 build runs the direct-load bulk kernel
+  if (p->fp64 || p->vis) p->use_tma = false;  // the FP64 build and visco-elastic media run the direct-load bulk kernel
   p->device = d->device;
   CK(cudaSetDevice(p->device));
   keep_pool_memory(p->device);
@@ -983,6 +1103,12 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
     for (int c = 0; c < nmed; c++)
       upload_field(p, d->medium + (size_t)(1 + c) * g.siz_icmp, p->rvoid(p->coef, (size_t)(cgfd::CF_MED + c) * p->sf),
                    stage_buf, 0, 0, &ps);
+    if (p->vis) {
+      p->d_y = dalloc_real(p, (size_t)2 * p->nmax * p->sf, B);
+      CK(cudaMemsetAsync(p->d_y, 0, sizeof(float) * 2 * p->nmax * p->sf, p->stream));
+      for (int c = 0; c < 2 * p->nmax; c++)
+        upload_field(p, vis_y.data() + (size_t)c * g.siz_icmp, p->d_y + (size_t)c * p->sf, stage_buf, 0, 0, &ps);
+    }
   }
   CK(cudaStreamSynchronize(p->stream));
   dfree(stage_buf, p->stream);
@@ -1001,6 +1127,20 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
     upload_real(p, p->matx, mx);
     upload_real(p, p->maty, my);
     p->d_flux = dalloc_real(p, (size_t)9 * cgfd::kFluxPlanes * (p->ni + 6) * (p->nj + 6) * nshot, B);
+  }
+  if (p->vis) {
+    for (int l = 0; l < 4; l++) {
+      p->jbuf[l] = dalloc_real(p, (size_t)6 * p->nmax * p->sf, B);
+      CK(cudaMemsetAsync(p->jbuf[l], 0, sizeof(float) * 6 * p->nmax * p->sf, p->stream));
+    }
+    p->d_rhs = dalloc_real(p, (size_t)9 * p->sf, B);
+    CK(cudaMemsetAsync(p->d_rhs, 0, sizeof(float) * 9 * p->sf, p->stream));
+    if (p->free_top) {
+      std::vector<float> md;
+      cgfd::vis_free_matrix(d, md);
+      p->d_matD = dalloc_real(p, md.size(), B);
+      upload_real(p, p->d_matD, md);
+    }
   }
   // PML
   cgfd::PmlFaceHost fh[3][2];
@@ -1290,6 +1430,8 @@ void reset_state(cgfd_problem *p) {
   const size_t lev_bytes[4] = {E, E, p->wave16 ? 2u : E, p->wave16 ? 2u : E};
   for (int l = 0; l < 4; l++) CK(cudaMemsetAsync(p->wbuf[l], 0, lev_bytes[l] * 9 * p->sf * p->nshot, p->stream));
   for (auto &f : p->faces) CK(cudaMemsetAsync(f.aux, 0, E * 3 * 9 * f.n * p->nshot, p->stream));
+  for (auto *jb : p->jbuf)
+    if (jb) CK(cudaMemsetAsync(jb, 0, sizeof(float) * 6 * p->nmax * p->sf, p->stream));
   if (p->rec.n > 0)
     CK(cudaMemsetAsync(p->d_seis, 0, sizeof(float) * p->rec.n * 9 * p->nt_total * p->nshot, p->stream));
   if (p->nline > 0)
@@ -1933,6 +2075,10 @@ int cgfd_set_bulk_variant(cgfd_problem *p, int tma) {
   }
   if (tma && p->fp64) {
     set_err("the FP64 build runs the direct-load bulk kernel");
+    return CGFD_ERR_UNSUPPORTED;
+  }
+  if (tma && p->vis) {
+    set_err("visco-elastic media run the direct-load bulk kernel");
     return CGFD_ERR_UNSUPPORTED;
   }
   if (p->med == cgfd::MED_AC) {  // acoustic: the TMA-pipelined (1) or direct-load (0) stage kernel

@@ -82,6 +82,9 @@ struct StagePT {
   const R *pre;           // w_pre (stages 1-2)
   R *tmp_out;             // next stage input (stages 0-2); __half in FP16-stage mode
   R *end;                 // accumulator (written at every stage)
+  R *rhs;                 // non-null (visco-elastic media): the wave fields' right-hand side
+                          // [9][sf] is written here instead of the RK combine (PML auxiliaries
+                          // are still combined); the attenuation pass combines them
   R ca, cb;               // rk_a[stage]*dt, rk_b[stage]*dt
   const void *coef;       // [ncoef][sf] of R, __half, __nv_bfloat16 or uint16_t
   float cscale[32];       // 16-bit coefficients: value = cscale[f] * stored + coffset[f]

@@ -165,10 +165,15 @@ __global__ void __launch_bounds__(TX *TY, DirectTile<R>::MINB)
       md.hooke(acc.G, h + 3);
 #pragma unroll
       for (int c = 3; c < 9; c++) h[c] += acc.hc[c];
-      R cc[9];
+      if (p.rhs) {
 #pragma unroll
-      for (int f = 0; f < 9; f++) cc[f] = q[f][LZ];
-      rk_store(p.stage, p.ca, p.cb, sf, id, cc, h, p.pre, p.tmp_out, p.end, p.err);
+        for (int f = 0; f < 9; f++) p.rhs[f * sf + id] = h[f];
+      } else {
+        R cc[9];
+#pragma unroll
+        for (int f = 0; f < 9; f++) cc[f] = q[f][LZ];
+        rk_store(p.stage, p.ca, p.cb, sf, id, cc, h, p.pre, p.tmp_out, p.end, p.err);
+      }
     }
 #pragma unroll
     for (int f = 0; f < 9; f++)
@@ -379,7 +384,10 @@ __global__ void __launch_bounds__(32 * 2 * NSURF, 2) k_stage_surface(const __gri
     }
 #pragma unroll
     for (int c = 0; c < 9; c++) h[c] += hc[c];
-    if constexpr (WP == 0) {
+    if (WP == 0 && p.rhs) {
+#pragma unroll
+      for (int f = 0; f < 9; f++) p.rhs[woff + f * sf + id] = h[f];
+    } else if constexpr (WP == 0) {
       R cc[9];
 #pragma unroll
       for (int f = 0; f < 9; f++) cc[f] = cur(f, id);

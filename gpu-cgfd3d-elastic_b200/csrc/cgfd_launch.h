@@ -58,6 +58,35 @@ using PgP = PgPT<float>;
 template <typename R>
 int launch_peak_motion(const PgPT<R> &q, cudaStream_t st);
 
+// Visco-elastic media (generalized Maxwell body), cgfd_visco.cu. The attenuation pass of one
+// RK stage (sv_curv_col_vis_iso_atten_gpu, sv_curv_col_vis_iso_gpu.cu:285-433) on the elastic
+// right-hand side `rhs`, then the RK combine of the 9 wave fields and the 6 nmax memory variables.
+struct VisP {
+  int ni, nj, nk, nmax, stage;
+  long long sx, sz, sf, off0;
+  const float *rhs;                   // [9][sf] elastic right-hand side (no sources)
+  const float *cur, *pre;             // wave levels: stage input, w_pre
+  float *tmp_out, *end;               // next stage input (stages 0-2), w_end
+  const float *jcur, *jpre;           // memory variables [nmax][6][sf], xx yy zz yz xz xy
+  float *jtmp, *jend;
+  const float *coef;                  // coefficient fields: lambda at 10, mu at 11 (unrelaxed)
+  const float *y;                     // [2 nmax][sf]: Ylam[n], then Ymu[n]
+  float wl[10];                       // relaxation angular frequencies
+  float ca, cb;
+  int *err;                           // kErrWaveNonfinite when w_end turns non-finite (stage 3)
+};
+int launch_vis_atten(const VisP &q, cudaStream_t st);
+// The stress rotation of w_end at the free surface after the last stage
+// (sv_curv_col_vis_iso_free_gpu, sv_curv_col_vis_iso_gpu.cu:435-531): the stress in the local
+// frame D (rows: tangent x normal, tangent along eta, normal), its normal components zeroed.
+struct VisFreeP {
+  int ni, nj;
+  long long sx, sf, off_top;          // off_top: device index of physical (0, 0, nk-1)
+  float *w_end;
+  const float *matD;                  // [nj][ni][9] row-major
+};
+int launch_vis_free(const VisFreeP &q, cudaStream_t st);
+
 // Station sampling of w_pre (io_funcs.cu:1624-1666).
 template <typename R>
 struct RecvPT {

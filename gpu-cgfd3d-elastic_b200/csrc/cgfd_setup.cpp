@@ -8,6 +8,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <utility>
 
 namespace cgfd {
 
@@ -19,6 +21,7 @@ int medium_ncmp(int medium_type) {
     case CGFD_MEDIUM_ELASTIC_ISO: return 3;
     case CGFD_MEDIUM_ELASTIC_VTI: return 6;
     case CGFD_MEDIUM_ELASTIC_ANISO: return 22;
+    case CGFD_MEDIUM_VISCO_ISO: return 5;  // rho lambda mu Qp Qs
   }
   return -1;
 }
@@ -27,9 +30,13 @@ void validate_desc(const cgfd_problem_desc *d) {
   if (!d) throw Error(CGFD_ERR_INVALID, "desc is NULL");
   if (d->ni < 8 || d->nj < 8 || d->nk < 8) throw Error(CGFD_ERR_INVALID, "grid must have at least 8 points per axis");
   if (medium_ncmp(d->medium_type) < 0)
-    throw Error(CGFD_ERR_UNSUPPORTED, "medium_type must be acoustic iso or elastic iso/vti/aniso");
+    throw Error(CGFD_ERR_UNSUPPORTED, "medium_type must be acoustic iso, elastic iso/vti/aniso or visco-elastic iso");
   if (d->medium_type == CGFD_MEDIUM_ACOUSTIC_ISO && d->precision != CGFD_PREC_FP32 && d->precision != CGFD_PREC_FP64)
     throw Error(CGFD_ERR_UNSUPPORTED, "acoustic media run in FP32 or FP64 (CGFD_PREC_FP32 / CGFD_PREC_FP64)");
+  if (d->medium_type == CGFD_MEDIUM_VISCO_ISO && d->precision != CGFD_PREC_FP32)
+    throw Error(CGFD_ERR_UNSUPPORTED, "visco-elastic media run in FP32 (CGFD_PREC_FP32)");
+  if (d->medium_type == CGFD_MEDIUM_VISCO_ISO && !d->visco)
+    throw Error(CGFD_ERR_INVALID, "visco-elastic media need desc->visco");
   if (!d->medium) throw Error(CGFD_ERR_INVALID, "the medium array is required");
   if (!d->metric && !d->coord) throw Error(CGFD_ERR_INVALID, "coordinates are required when no metric is given");
   if (!(d->dt > 0.0f)) throw Error(CGFD_ERR_INVALID, "dt must be > 0");
@@ -235,6 +242,132 @@ void dvh2dvz(const cgfd_problem_desc *d, std::vector<float> &matx, std::vector<f
         }
     }
   if (singular) throw Error(CGFD_ERR_INVALID, "singular free-surface traction matrix");
+}
+
+// ---------------------------------------------------------------------------------------
+// Visco-elastic media: the generalized-Maxwell-body fit (md_vis_GMB_cal_Y, md_t.cu:657-781).
+// Frequencies wk[m] = wmin (wmax/wmin)^(m/(kmax-1)), m < kmax = 2 nmax - 1 (angular), the
+// relaxation frequencies wl[n] = wk[2n]. For Q^-1 = 1/round(Q) the weights Y solve, in the least-
+// squares sense, sum_n G[m][n] Y[n] = Q^-1 with G[m][n] = (wl_n wk_m + wl_n^2 Q^-1) /
+// (wl_n^2 + wk_m^2) (md_visco_LS: the normal equations). At wr = 2 pi fr,
+// theta1 = 1 - sum_n Y_n / (1 + (wr/wl_n)^2), theta2 = sum_n Y_n (wr/wl_n) / (1 + (wr/wl_n)^2),
+// R = |theta|, and a modulus M given at fr is unrelaxed as M (R + theta1) / (2 R^2): the P modulus
+// lambda + 2 mu with Y of Qp, mu with Y of Qs. Ylam = (1 + 2 mu_u / lam_u) YP - 2 mu_u / lam_u YS,
+// Ymu = YS. Y and the factor depend on Q alone, so they are solved once per distinct Q.
+// ---------------------------------------------------------------------------------------
+namespace {
+struct GmbQ {
+  double y[10];
+  double fac;
+};
+
+GmbQ gmb_solve(double qinv, int nmax, const double *wl, const double *wk, int kmax, double wr) {
+  double A[10][10] = {}, r[10] = {};
+  for (int m = 0; m < kmax; m++) {
+    double g[10];
+    for (int n = 0; n < nmax; n++) g[n] = (wl[n] * wk[m] + wl[n] * wl[n] * qinv) / (wl[n] * wl[n] + wk[m] * wk[m]);
+    for (int a = 0; a < nmax; a++) {
+      r[a] += g[a] * qinv;
+      for (int b = 0; b < nmax; b++) A[a][b] += g[a] * g[b];
+    }
+  }
+  // Gauss-Jordan elimination with partial pivoting on the normal equations
+  for (int c = 0; c < nmax; c++) {
+    int piv = c;
+    for (int a = c + 1; a < nmax; a++)
+      if (std::fabs(A[a][c]) > std::fabs(A[piv][c])) piv = a;
+    if (A[piv][c] == 0.0) throw Error(CGFD_ERR_INVALID, "singular GMB least-squares system");
+    if (piv != c) {
+      for (int b = 0; b < nmax; b++) std::swap(A[c][b], A[piv][b]);
+      std::swap(r[c], r[piv]);
+    }
+    for (int a = 0; a < nmax; a++) {
+      if (a == c) continue;
+      const double f = A[a][c] / A[c][c];
+      for (int b = c; b < nmax; b++) A[a][b] -= f * A[c][b];
+      r[a] -= f * r[c];
+    }
+  }
+  GmbQ o;
+  double t1 = 0, t2 = 0;
+  for (int n = 0; n < nmax; n++) {
+    o.y[n] = r[n] / A[n][n];
+    const double x = wr / wl[n], den = 1.0 + x * x;
+    t1 += o.y[n] / den;
+    t2 += o.y[n] * x / den;
+  }
+  t1 = 1.0 - t1;
+  const double R = std::sqrt(t1 * t1 + t2 * t2);
+  o.fac = (R + t1) / (2.0 * R * R);
+  return o;
+}
+}  // namespace
+
+void visco_gmb(const cgfd_visco_desc *v, long long n, const float *lambda, const float *mu, const float *Qp,
+               const float *Qs, float *lam_u, float *mu_u, float *Ylam, float *Ymu, float *wl_out) {
+  if (!v) throw Error(CGFD_ERR_INVALID, "visco parameters are required");
+  if (v->nmaxwell < 1 || v->nmaxwell > 10) throw Error(CGFD_ERR_INVALID, "nmaxwell must be in [1, 10]");
+  if (!(v->fmin > 0.f) || !(v->fmax > v->fmin) || !(v->fr > 0.f))
+    throw Error(CGFD_ERR_INVALID, "visco frequencies must satisfy 0 < fmin < fmax and fr > 0");
+  const int nmax = v->nmaxwell, kmax = 2 * nmax - 1;
+  const double wmin = 2 * kPi * v->fmin, wmax = 2 * kPi * v->fmax, wr = 2 * kPi * v->fr;
+  double wk[19], wl[10];
+  for (int m = 0; m < kmax; m++) wk[m] = kmax > 1 ? wmin * std::pow(wmax / wmin, m / (double)(kmax - 1)) : wmin;
+  for (int q = 0; q < nmax; q++) {
+    wl[q] = wk[2 * q];
+    if (wl_out) wl_out[q] = (float)wl[q];
+  }
+  std::map<long long, GmbQ> cache;
+  auto fit = [&](float Q) -> const GmbQ & {
+    const double rq = std::round((double)Q);
+    if (!(rq >= 1.0)) throw Error(CGFD_ERR_INVALID, "Q values must round to >= 1");
+    auto it = cache.find((long long)rq);
+    if (it == cache.end()) it = cache.emplace((long long)rq, gmb_solve(1.0 / rq, nmax, wl, wk, kmax, wr)).first;
+    return it->second;
+  };
+  for (long long t = 0; t < n; t++) {
+    const GmbQ &P = fit(Qp[t]);
+    const GmbQ &S = fit(Qs[t]);
+    const double m_u = (double)mu[t] * S.fac;
+    const double l_u = ((double)lambda[t] + 2.0 * mu[t]) * P.fac - 2.0 * m_u;
+    lam_u[t] = (float)l_u;
+    mu_u[t] = (float)m_u;
+    const double r = l_u != 0.0 ? 2.0 * m_u / l_u : 0.0;
+    for (int q = 0; q < nmax; q++) {
+      Ylam[(size_t)q * n + t] = (float)((1.0 + r) * P.y[q] - r * S.y[q]);
+      Ymu[(size_t)q * n + t] = (float)S.y[q];
+    }
+  }
+}
+
+// Local frame of the free surface for the visco-elastic stress fix
+// (sv_curv_col_vis_iso_dvh2dvz, sv_curv_col_vis_iso_gpu.cu:632-706): with the surface normal
+// zeta / |zeta| and the tangent r_eta / |r_eta| (the centered operator along j on the
+// coordinates), D = [tangent x normal scaled by 1/(|r_eta||zeta|) ; r_eta / |r_eta| ;
+// zeta / |zeta|], row-major per surface column.
+void vis_free_matrix(const cgfd_problem_desc *d, std::vector<float> &matD) {
+  if (!d->coord) throw Error(CGFD_ERR_INVALID, "visco-elastic media with a free surface need the coordinates");
+  static const double c7[7] = {-0.02084, 0.1667, -0.7709, 0.0, 0.7709, -0.1667, 0.02084};  // fd_t.cu:162
+  RefGrid g(d->ni, d->nj, d->nk);
+  matD.assign((size_t)d->ni * d->nj * 9, 0.f);
+  const int k = d->nk - 1;
+  for (int j = 0; j < d->nj; j++)
+    for (int i = 0; i < d->ni; i++) {
+      const size_t iptr = g.at(i, j, k);
+      double r[3] = {0, 0, 0};
+      for (int a = 0; a < 3; a++)
+        for (int t = 0; t < 7; t++)
+          r[a] += c7[t] * d->coord[(size_t)a * g.siz_icmp + iptr + (size_t)((long long)(t - 3) * (long long)g.siz_iy)];
+      double e[3];
+      for (int a = 0; a < 3; a++) e[a] = d->metric[(size_t)(7 + a) * g.siz_icmp + iptr];
+      const double en = 1.0 / std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+      const double em = 1.0 / std::sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+      const double enm = en * em;
+      const double D[9] = {(r[1] * e[2] - r[2] * e[1]) * enm, (r[2] * e[0] - r[0] * e[2]) * enm,
+                           (r[0] * e[1] - r[1] * e[0]) * enm, r[0] * en, r[1] * en, r[2] * en,
+                           e[0] * em, e[1] * em, e[2] * em};
+      for (int q = 0; q < 9; q++) matD[((size_t)j * d->ni + i) * 9 + q] = (float)D[q];
+    }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -490,6 +623,21 @@ thread_local std::string g_setup_err;
 }
 
 extern "C" {
+
+int cgfd_visco_gmb(const cgfd_visco_desc *v, long long n, const float *lambda, const float *mu, const float *Qp,
+                   const float *Qs, float *lam_u, float *mu_u, float *Ylam, float *Ymu, float *wl) {
+  if (n < 0 || (n > 0 && (!lambda || !mu || !Qp || !Qs || !lam_u || !mu_u || !Ylam || !Ymu))) {
+    cgfd::set_last_error("invalid argument");
+    return CGFD_ERR_INVALID;
+  }
+  try {
+    cgfd::visco_gmb(v, n, lambda, mu, Qp, Qs, lam_u, mu_u, Ylam, Ymu, wl);
+  } catch (const cgfd::Error &e) {
+    cgfd::set_last_error(e.what());
+    return e.code;
+  }
+  return CGFD_OK;
+}
 
 // Fill the 3 ghost layers of ncmp fields by linear extrapolation (gd_t.cu:404-502).
 int cgfd_fill_ghosts(int ni, int nj, int nk, int ncmp, float *v4d) {

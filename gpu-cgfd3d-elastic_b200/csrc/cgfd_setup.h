@@ -40,6 +40,11 @@ void pml_setup(const cgfd_problem_desc *d, PmlFaceHost faces[3][2]);
 
 // [nj][ni][9] matVx2Vz / matVy2Vz at the top layer
 void dvh2dvz(const cgfd_problem_desc *d, std::vector<float> &matx, std::vector<float> &maty);
+// Visco-elastic media: the GMB fit (cgfd_visco_gmb) and the free-surface frame matrices
+// [nj][ni][9] of the stress fix after each time step.
+void visco_gmb(const cgfd_visco_desc *v, long long n, const float *lambda, const float *mu, const float *Qp,
+               const float *Qs, float *lam_u, float *mu_u, float *Ylam, float *Ymu, float *wl);
+void vis_free_matrix(const cgfd_problem_desc *d, std::vector<float> &matD);
 
 // Points given by physical coordinates, located like the reference: global physical index
 // (-1000 when outside the grid), fractional shift, and the coordinates after a depth was

@@ -50,6 +50,7 @@ extern "C" {
 #define CGFD_MEDIUM_ELASTIC_ISO   2
 #define CGFD_MEDIUM_ELASTIC_VTI   3
 #define CGFD_MEDIUM_ELASTIC_ANISO 4
+#define CGFD_MEDIUM_VISCO_ISO     5  /* visco-elastic iso, generalized Maxwell body (CONST_VISCO_GMB) */
 
 /* wavelet names accepted in .src files: src_t.cu:873-903 (src_cal_wavelet) */
 #define CGFD_WAVELET_RICKER         0
@@ -127,9 +128,19 @@ typedef struct cgfd_station_desc {
 /*
  * Everything drv_rk_curv_col_allstep() consumes, in the reference's host layout.
  */
+/*
+ * Visco-elastic media (CGFD_MEDIUM_VISCO_ISO; the par file's visco_config, par_t.cu:728-770):
+ * a generalized Maxwell body of nmaxwell relaxation mechanisms fitted to the per-point Qp and Qs
+ * over [fmin, fmax] with the moduli given at the reference frequency fr (md_vis_GMB_cal_Y).
+ */
+typedef struct cgfd_visco_desc {
+  int   nmaxwell;           /* 1..10                                                          */
+  float fr, fmin, fmax;     /* Hz; 0 < fmin < fmax                                           */
+} cgfd_visco_desc;
+
 typedef struct cgfd_problem_desc {
   int ni, nj, nk;           /* physical points incl. PML layers (ghosts excluded)          */
-  int medium_type;          /* CGFD_MEDIUM_ACOUSTIC_ISO or CGFD_MEDIUM_ELASTIC_*               */
+  int medium_type;          /* CGFD_MEDIUM_ACOUSTIC_ISO, CGFD_MEDIUM_ELASTIC_* or _VISCO_ISO   */
   const float *coord;       /* [3][nz][ny][nx] x,y,z with ghosts filled; used for the PML
                                length/spacing average (bdry_t.cu:334-451). May be NULL when
                                no PML face is enabled and metric is given.                   */
@@ -148,6 +159,8 @@ typedef struct cgfd_problem_desc {
   cgfd_station_desc sta;
   int   precision;          /* CGFD_PREC_*                                                  */
   int   device;             /* CUDA device ordinal                                          */
+  const cgfd_visco_desc *visco; /* CGFD_MEDIUM_VISCO_ISO: the GMB parameters (medium [5] = rho,
+                               lambda, mu, Qp, Qs); NULL for the other media                 */
 } cgfd_problem_desc;
 
 typedef struct cgfd_problem cgfd_problem;
@@ -431,6 +444,18 @@ int cgfd_server_get_stats(cgfd_server *s, cgfd_server_stats *out);
 int cgfd_server_destroy(cgfd_server *s);
 
 /* ---- grid helpers (host, FP64) ------------------------------------------------------- */
+
+/*
+ * The generalized-Maxwell-body fit of visco-elastic media for n points (md_vis_GMB_cal_Y,
+ * md_t.cu:657-781, with its least-squares solve md_visco_LS): relaxation frequencies wl[nmaxwell]
+ * spread log-uniformly over [fmin, fmax], per point the anelastic weights Ylam[nmaxwell][n] /
+ * Ymu[nmaxwell][n] fitted to 1/round(Qp), 1/round(Qs), and the unrelaxed moduli lam_u[n], mu_u[n]
+ * that give lambda, mu at the reference frequency fr. cgfd_problem_create runs the same fit for a
+ * CGFD_MEDIUM_VISCO_ISO medium. Solved in FP64 (the reference solves in float).
+ * Returns CGFD_ERR_INVALID for Q values that round below 1 or parameters out of range.
+ */
+int cgfd_visco_gmb(const cgfd_visco_desc *v, long long n, const float *lambda, const float *mu, const float *Qp,
+                   const float *Qs, float *lam_u, float *mu_u, float *Ylam, float *Ymu, float *wl);
 
 /*
  * Fill the 3 ghost layers of ncmp fields [ncmp][nz][ny][nx] by linear extrapolation.

@@ -9,8 +9,8 @@
  * bdry_pml_set -> bdry_free_set -> md_rho_to_slow), and the time loop restates
  * drv_rk_curv_col.cu:75-541 for one rank without halo exchange, slices, snapshots, PGV or the
  * exponential sponge, calling the reference's sv_curv_col_el_*_onestage (sv_curv_col_ac_iso_onestage
- * for acoustic media), wav_update and
- * io_recv_keep.
+ * for acoustic media; sv_curv_col_vis_iso_onestage, md_vis_GMB_cal_Y, sv_curv_col_vis_iso_dvh2dvz and
+ * sv_curv_col_vis_iso_free_gpu for visco-elastic media), wav_update and io_recv_keep.
  *
  * usage: ref_harness <dir>   (dir holds params.txt, coord.bin, medium.bin, src.src, station.list)
  */
@@ -18,6 +18,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "alloc.h"
@@ -34,6 +35,7 @@
 #include "sv_curv_col_el_gpu.h"
 #include "sv_curv_col_el_iso_gpu.h"
 #include "sv_curv_col_el_vti_gpu.h"
+#include "sv_curv_col_vis_iso_gpu.h"
 #include "wav_t.h"
 
 static void die(const char *m) {
@@ -74,6 +76,12 @@ int main(int argc, char **argv) {
     for (int s = 0; s < 2; s++)
       if (fscanf(fp, "%d %d %f %f %f", &pml_on[a][s], &pml_n[a][s], &pml_a[a][s], &pml_b[a][s], &pml_v[a][s]) != 5)
         die("params pml");
+  // visco-elastic media (CONST_MEDIUM_VISCOELASTIC_ISO, GMB): an extra line
+  // "nmaxwell fr fmin fmax" (par_t.cu:736-770)
+  int nmaxwell = 0;
+  float vis_fr = 0.f, vis_fmin = 0.f, vis_fmax = 0.f;
+  const bool visco = medium_type == CONST_MEDIUM_VISCOELASTIC_ISO;
+  if (visco && fscanf(fp, "%d %f %f %f", &nmaxwell, &vis_fr, &vis_fmin, &vis_fmax) != 4) die("params visco");
   fclose(fp);
 
   int myid = 0;
@@ -122,12 +130,15 @@ int main(int argc, char **argv) {
   // medium: physical points as md_import does (md_t.cu:269-326), ghosts left at 0
   md_t md;
   memset(&md, 0, sizeof(md));
-  md_init(&gd, &md, medium_type, 0, 0);
+  md_init(&gd, &md, medium_type, visco ? CONST_VISCO_GMB : 0, nmaxwell);
   {
-    std::vector<float> m((size_t)md.ncmp * gd.siz_icmp);
+    // visco-elastic: rho lambda mu Qp Qs (the first five of md_init's components); the Ylam /
+    // Ymu components come from md_vis_GMB_cal_Y below
+    const int nread = visco ? 5 : md.ncmp;
+    std::vector<float> m((size_t)nread * gd.siz_icmp);
     snprintf(path, sizeof(path), "%s/medium.bin", dir);
     read_bin(path, m.data(), m.size());
-    for (int c = 0; c < md.ncmp; c++) {
+    for (int c = 0; c < nread; c++) {
       float *ptr = md.v4d + md.cmp_pos[c];
       for (int k = gd.nk1; k <= gd.nk2; k++)
         for (int j = gd.nj1; j <= gd.nj2; j++)
@@ -136,6 +147,22 @@ int main(int argc, char **argv) {
             ptr[p] = m[c * gd.siz_icmp + p];
           }
     }
+  }
+
+  if (visco) {  // main_curv_col_el_3d.cu:558-561
+    md_vis_GMB_cal_Y(&md, vis_fr, vis_fmin, vis_fmax);
+    // the fitted medium: lambda, mu (unrelaxed), Ylam[n], Ymu[n], then wl[n] (relaxation
+    // frequencies)
+    std::vector<float> fit((size_t)(2 + 2 * nmaxwell) * gd.siz_icmp + nmaxwell);
+    memcpy(fit.data(), md.lambda, sizeof(float) * gd.siz_icmp);
+    memcpy(fit.data() + gd.siz_icmp, md.mu, sizeof(float) * gd.siz_icmp);
+    for (int n = 0; n < nmaxwell; n++) {
+      memcpy(fit.data() + (2 + n) * gd.siz_icmp, md.Ylam[n], sizeof(float) * gd.siz_icmp);
+      memcpy(fit.data() + (2 + nmaxwell + n) * gd.siz_icmp, md.Ymu[n], sizeof(float) * gd.siz_icmp);
+    }
+    memcpy(fit.data() + (2 + 2 * nmaxwell) * gd.siz_icmp, md.wl, sizeof(float) * nmaxwell);
+    snprintf(path, sizeof(path), "%s/ref_gmb.bin", dir);
+    write_bin(path, fit.data(), fit.size());
   }
 
   src_t src;
@@ -147,7 +174,7 @@ int main(int argc, char **argv) {
   wav_t wav;
   memset(&wav, 0, sizeof(wav));
   if (medium_type == CONST_MEDIUM_ACOUSTIC_ISO) wav_ac_init(&gd, &wav, fd.num_rk_stages);  // main:676-681
-  else wav_init(&gd, &wav, fd.num_rk_stages, 0, 0);
+  else wav_init(&gd, &wav, fd.num_rk_stages, visco ? CONST_VISCO_GMB : 0, nmaxwell);
 
   iorecv_t iorecv;
   memset(&iorecv, 0, sizeof(iorecv));
@@ -172,6 +199,8 @@ int main(int argc, char **argv) {
   if (bdryfree.is_sides_free[CONST_NDIM - 1][1] == 1 && md.medium_type != CONST_MEDIUM_ACOUSTIC_ISO) {  // :73-95
     if (md.medium_type == CONST_MEDIUM_ELASTIC_ISO) sv_curv_col_el_iso_dvh2dvz(&gd, &metric, &md, &bdryfree);
     else if (md.medium_type == CONST_MEDIUM_ELASTIC_VTI) sv_curv_col_el_vti_dvh2dvz(&gd, &metric, &md, &bdryfree);
+    else if (visco)
+      sv_curv_col_vis_iso_dvh2dvz(&gd, &metric, &md, &bdryfree, fd.fdc_len, fd.fdc_indx, fd.fdc_coef);
     else sv_curv_col_el_aniso_dvh2dvz(&gd, &metric, &md, &bdryfree);
   }
   gd_t gd_d;
@@ -222,7 +251,7 @@ int main(int argc, char **argv) {
   // Statement by statement against drv_rk_curv_col.cu (line numbers of that file). Left out:
   // io_line_keep / io_slice_nc_put / io_snap_nc_put (:203-215; outputs the harness does not
   // write), the MPI message pack / start / wait / unpack (:336, :353-355, :407-408, :461-462,
-  // :492-501; one rank, no neighbours), the visco-elastic branches (:317-331, :479-490), the
+  // :492-501; one rank, no neighbours), the
   // stubbed NaN check (:507-510) and the exponential sponge (:513-515, not enabled by the cases). The per-stage cudaDeviceSynchronize (:333) is implied by the
   // default stream's ordering.
   for (int it = 0; it < nsteps; it++) {  // :193
@@ -246,6 +275,11 @@ int main(int argc, char **argv) {
                                     fd.num_of_fdx_op, fd.pair_fdx_op[ipair][istage], fd.num_of_fdy_op,
                                     fd.pair_fdy_op[ipair][istage], fd.num_of_fdz_op, fd.pair_fdz_op[ipair][istage],
                                     fd.fdz_max_len, myid);
+      else if (visco)  // :317-331
+        sv_curv_col_vis_iso_onestage(w_cur_d, w_rhs_d, wav_d, fd_wav_d, gd_d, metric_d, md_d, bdrypml_d, bdryfree_d, src_d,
+                                     fd.num_of_fdx_op, fd.pair_fdx_op[ipair][istage], fd.num_of_fdy_op,
+                                     fd.pair_fdy_op[ipair][istage], fd.num_of_fdz_op, fd.pair_fdz_op[ipair][istage],
+                                     fd.fdz_max_len, myid);
       else if (md_d.medium_type == CONST_MEDIUM_ELASTIC_VTI)
         sv_curv_col_el_vti_onestage(w_cur_d, w_rhs_d, wav_d, fd_wav_d, gd_d, metric_d, md_d, bdrypml_d, bdryfree_d, src_d,
                                     fd.num_of_fdx_op, fd.pair_fdx_op[ipair][istage], fd.num_of_fdy_op,
@@ -286,6 +320,10 @@ int main(int argc, char **argv) {
         float cb = fd.rk_b[istage] * dt;
         wav_update_end<<<grid, block>>>(wav_d.siz_ilevel, cb, w_end_d, w_rhs_d);  // :456
         aux_update(2, cb);                                                         // :464-478
+        if (visco && free_top) {                                                   // :479-490
+          dim3 fb(32, 16), fg((ni + fb.x - 1) / fb.x, (nj + fb.y - 1) / fb.y);
+          sv_curv_col_vis_iso_free_gpu<<<fg, fb>>>(w_end_d, wav_d, gd_d, metric_d, md_d, bdryfree_d, myid);
+        }
       }
     }
     if (free_top) {  // drv_rk_curv_col.cu:519-527
@@ -315,13 +353,14 @@ int main(int argc, char **argv) {
   std::vector<float> seis((size_t)iorecv.total_number * 9 * nt_total, 0.f);
   // samples of steps that were not run stay 0 (the reference leaves them uninitialised)
   for (int r = 0; r < iorecv.total_number; r++)
-    for (int c = 0; c < wav.ncmp; c++)
+    for (int c = 0; c < wav.ncmp && c < 9; c++)
       for (int t = 0; t < nsteps && t < nt_total; t++)
         seis[((size_t)r * 9 + c) * nt_total + t] = iorecv.recvone[r].seismo[(size_t)c * nt_total + t];
   snprintf(path, sizeof(path), "%s/ref_seismo.bin", dir);
   write_bin(path, seis.data(), seis.size());
   std::vector<float> w((size_t)9 * gd.siz_icmp, 0.f);
-  cudaMemcpy(w.data(), w_pre_d, sizeof(float) * wav.ncmp * gd.siz_icmp, cudaMemcpyDeviceToHost);
+  // (visco-elastic: the 9 wave fields; the memory variables follow them in the level)
+  cudaMemcpy(w.data(), w_pre_d, sizeof(float) * std::min(wav.ncmp, 9) * gd.siz_icmp, cudaMemcpyDeviceToHost);
   snprintf(path, sizeof(path), "%s/ref_wave.bin", dir);
   write_bin(path, w.data(), w.size());
   if (free_top) {

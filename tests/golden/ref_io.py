@@ -22,6 +22,9 @@ def write_inputs(p, d, nsteps):
                     f.write(f"1 {fc['num_layers']} {fc['alpha_max']:.9g} {fc['beta_max']:.9g} {fc['ref_vel']:.9g}\n")
                 else:
                     f.write("0 0 0 0 0\n")
+        if p.medium_type == 5:  # visco-elastic: "nmaxwell fr fmin fmax"
+            v = p.visco
+            f.write(f"{int(v['nmaxwell'])} {v['fr']:.9g} {v['fmin']:.9g} {v['fmax']:.9g}\n")
     np.ascontiguousarray(p.coord, np.float32).tofile(os.path.join(d, "coord.bin"))
     np.ascontiguousarray(p.medium, np.float32).tofile(os.path.join(d, "medium.bin"))
     formats.write_src(os.path.join(d, "src.src"), p.src)
@@ -41,5 +44,12 @@ def run(p, d, nsteps, timeout=600):
     metric = np.fromfile(os.path.join(d, "ref_metric.bin"), np.float32).reshape((10,) + shp)
     pg_path = os.path.join(d, "ref_pg.bin")
     pg = np.fromfile(pg_path, np.float32).reshape((15,) + shp[1:]) if os.path.exists(pg_path) else None
-    return {"seismo": seis, "wave": wave, "metric": metric, "pg": pg, "loop_ms": float(info["loop_ms"]),
+    gmb = None
+    gmb_path = os.path.join(d, "ref_gmb.bin")
+    if os.path.exists(gmb_path):  # visco-elastic: lambda, mu, Ylam[n], Ymu[n] (unrelaxed), then wl[n]
+        nm = int(p.visco["nmaxwell"])
+        raw = np.fromfile(gmb_path, np.float32)
+        n3 = shp[0] * shp[1] * shp[2]
+        gmb = {"fields": raw[:(2 + 2 * nm) * n3].reshape((2 + 2 * nm,) + shp), "wl": raw[(2 + 2 * nm) * n3:]}
+    return {"gmb": gmb, "seismo": seis, "wave": wave, "metric": metric, "pg": pg, "loop_ms": float(info["loop_ms"]),
             "cell_stages": int(info["cell_stages"]), "nsrc": int(info["nsrc"])}

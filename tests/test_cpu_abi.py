@@ -92,9 +92,17 @@ def test_invalid_descriptions_are_rejected():
     rc, msg = _create(d)
     assert rc == -1 and "at least 8" in msg
     d = p.desc()
-    d.medium_type = 5  # visco-elastic iso: not built
+    d.medium_type = 6  # no such medium
     rc, msg = _create(d)
     assert rc == -5
+    d = p.desc()
+    d.medium_type = 5  # visco-elastic iso without its GMB parameters
+    rc, msg = _create(d)
+    assert rc == -1 and "visco" in msg
+    pv = small_problem("vis", nsteps=2)
+    pv.precision = cgfd_b200.CGFD_PREC_FP64  # visco-elastic: FP32 only
+    rc, msg = _create(pv.desc())
+    assert rc == -5 and "visco" in msg
     d = p.desc()
     d.medium_type = 1  # acoustic: FP32 and FP64 only
     d.precision = cgfd_b200.CGFD_PREC_U16_COEF
@@ -147,3 +155,23 @@ def test_server_without_gpu_fails_cleanly():
     with pytest.raises(CgfdError) as e:
         Server()
     assert e.value.code == -2
+
+
+def test_visco_gmb_fit_properties():
+    """cgfd_visco_gmb (md_vis_GMB_cal_Y): log-uniform relaxation frequencies, weights of order 1/Q,
+    moduli unchanged at Q -> infinity, rejection of Q < 1."""
+    v = {"nmaxwell": 3, "fr": 2.0, "fmin": 0.2, "fmax": 20.0}
+    lam = np.full(4, 8e9, np.float32)
+    mu = np.full(4, 6e9, np.float32)
+    qs = np.array([20, 50, 100, 1e7], np.float32)
+    lu, mu_u, yl, ym, wl = cgfd_b200.visco_gmb(v, lam, mu, 2 * qs, qs)
+    assert np.allclose(wl, 2 * np.pi * np.array([0.2, 2.0, 20.0]), rtol=1e-6)
+    assert np.all(mu_u[:3] > mu[:3]) and abs(mu_u[3] / mu[3] - 1) < 1e-5
+    assert np.all(np.abs(ym[:, :3] * qs[:3]) < 3.0) and np.all(np.abs(ym[:, 3]) < 1e-5)
+    # the fitted Q^-1(w) = sum Y_n (wl_n w + wl_n^2 Q^-1) / (wl_n^2 + w^2) matches 1/Qs inside the band
+    w = 2 * np.pi * np.geomspace(0.3, 15.0, 9)
+    for t in range(3):
+        fit = sum(ym[n, t] * (wl[n] * w + wl[n] ** 2 / qs[t]) / (wl[n] ** 2 + w ** 2) for n in range(3))
+        assert np.all(np.abs(fit * qs[t] - 1.0) < 0.1), t
+    with pytest.raises(cgfd_b200.CgfdError):
+        cgfd_b200.visco_gmb(v, lam, mu, 2 * qs, np.zeros(4, np.float32))
