@@ -310,7 +310,7 @@ def batched_mixed(local, steps=16):
     return out
 
 
-def media_bench(local, steps=2000):
+def media_bench(local, steps=2000, media=("vti", "aniso", "ac", "vis")):
     """The anisotropic precision workload at its full size: 320x320x160 (50 m, CFS-PML 20, free
     surface), layered Thomsen VTI and Bond-rotated tilted-TI 21-Cij media, one double-couple
     source (fc 3 Hz) at 2 km, 100 surface stations, 2000 steps; and the same grid with a layered
@@ -333,7 +333,9 @@ def media_bench(local, steps=2000):
     out = {"workload": f"{ni}x{nj}x{nk}", "steps": steps, "reference": "FP64 build of the same kernels (GPU)"}
     modes = (("fp32", CGFD_PREC_FP32, 4), ("u16coef", CGFD_PREC_U16_COEF, 2), ("mixed_fp16wave", CGFD_PREC_FP16_WAVE, 2),
              ("fp16coef", CGFD_PREC_FP16_COEF, 2), ("bf16coef", CGFD_PREC_BF16_COEF, 2))
-    for med, ncoef in (("vti", 15), ("aniso", 31), ("ac", 11)):
+    for med, ncoef in (("vti", 15), ("aniso", 31), ("ac", 11)):  # visco-elastic after the loop
+        if med not in media:
+            continue
         nf, nplanes = (4, nk) if med == "ac" else (9, nk - 4)  # fields; planes of the bulk kernel
         p = synth.make_problem(ni, nj, nk, 50.0, steps, dt=None, medium=med, npml=20, nsrc=1, sta_grid=(10, 10),
                                fc=3.0, seed=31, src_depth=(2000.0, 2000.0), center_src=True)
@@ -377,6 +379,42 @@ def media_bench(local, steps=2000):
                             "roofline_frac": achieved / peak})
             sim.close()
             out[f"{med}_{name}"] = rec
+    # visco-elastic (GMB, 3 mechanisms; FP32 only, no FP64 build): the iso layers with Q, the
+    # same source and stations; the stage time covers the iso kernels in their right-hand-side
+    # mode and the attenuation pass. Bytes per cell-stage of this two-pass form, averaged over
+    # the 4 stages: the iso pass 30 floats (9 stage-input fields, 12 coefficients, 9 RHS) and the
+    # attenuation pass 118.25 (RHS, wave levels, 2 moduli, 6 weights and 18 memory variables per
+    # level touched: 98 / 143 / 143 / 89 floats at stages 0-3) = 593 B.
+    if "vis" not in media:
+        return out
+    p = synth.make_problem(ni, nj, nk, 50.0, steps, dt=None, medium="vis", npml=20, nsrc=1, sta_grid=(10, 10),
+                           fc=3.0, seed=31, src_depth=(2000.0, 2000.0), center_src=True)
+    p.device = local
+    sim = Simulation(p)
+    sim.autotune(4)
+    st = torch.cuda.ExternalStream(sim.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    sim.enqueue(steps)
+    e1.record(st)
+    e1.synchronize()
+    sim.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    sim.set_timing(True)
+    sim.timing(reset=True)
+    sim.enqueue(8)
+    sim.synchronize()
+    bulk_ms, _ = sim.timing(reset=True)["bulk"]  # both passes of the 32 stages
+    sim.set_timing(False)
+    s = sim.seismograms()[:, :, :steps]
+    zc = sim.zchunk
+    sim.close()
+    bpc = 593.0
+    stage_ms = bulk_ms / 32
+    achieved = bpc * ni * nj * nk / (stage_ms * 1e-3) / 1e9
+    out["vis_fp32"] = {"value": ni * nj * nk * 4 / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": ms,
+                       "nmaxwell": 3, "stage_ms": stage_ms, "bytes_per_cell_stage": bpc,
+                       "roofline_frac": achieved / peak, "finite": bool(np.isfinite(s).all()), "zchunk": zc}
     return out
 
 
