@@ -977,6 +977,8 @@ void build(cgfd_problem *p, const cgfd_problem_desc *d, int nshot, const cgfd_so
   std::vector<float> vis_med, vis_y;
   if (d->medium_type == CGFD_MEDIUM_VISCO_ISO) {
     if (nshot != 1) throw cgfd::Error(CGFD_ERR_UNSUPPORTED, "visco-elastic media run one shot per problem");
+    if (d->nj > 65535 || d->nk > 65535)  // the attenuation pass runs one block row per (j, k)
+      throw cgfd::Error(CGFD_ERR_UNSUPPORTED, "visco-elastic media take nj, nk <= 65535");
     cgfd::RefGrid g(d->ni, d->nj, d->nk);
     const size_t N = g.siz_icmp;
     const int nm = d->visco->nmaxwell;

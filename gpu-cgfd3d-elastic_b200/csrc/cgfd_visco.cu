@@ -19,14 +19,16 @@
 
 namespace cgfd {
 
-// Stress rows of the wave fields (components 3..8): xx yy zz yz xz xy.
-__global__ void __launch_bounds__(256) k_vis_atten(const __grid_constant__ VisP q) {
-  const long long n = (long long)q.ni * q.nj * q.nk;
+// Stress rows of the wave fields (components 3..8): xx yy zz yz xz xy. One thread per physical
+// point: x from the block's x index, one block row per (j, k); NM mechanisms unrolled so that
+// every load of a point is issued before its arithmetic.
+template <int NM>
+__global__ void __launch_bounds__(128) k_vis_atten(const __grid_constant__ VisP q) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= q.ni) return;
+  const int j = blockIdx.y, k = blockIdx.z;
   const long long sf = q.sf;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % q.ni);
-    const int j = (int)((t / q.ni) % q.nj);
-    const int k = (int)(t / ((long long)q.ni * q.nj));
+  {
     const long long id = q.off0 + (long long)k * q.sz + (long long)j * q.sx + i;
     float h[9];
 #pragma unroll
@@ -44,9 +46,10 @@ __global__ void __launch_bounds__(256) k_vis_atten(const __grid_constant__ VisP 
     ev[4] = (float)((double)(h[7] / mu) * 0.5);
     ev[5] = (float)((double)(h[8] / mu) * 0.5);
     float sl = 0.f, sm[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    for (int m = 0; m < q.nmax; m++) {
+#pragma unroll
+    for (int m = 0; m < NM; m++) {
       const float ylam = __ldg(q.y + (long long)m * sf + id);
-      const float ymu = __ldg(q.y + (long long)(q.nmax + m) * sf + id);
+      const float ymu = __ldg(q.y + (long long)(NM + m) * sf + id);
       float jc[6], hj[6];
 #pragma unroll
       for (int c = 0; c < 6; c++) jc[c] = q.jcur[(long long)(6 * m + c) * sf + id];
@@ -147,7 +150,19 @@ static unsigned grid_for(long long n) {
 }
 
 int launch_vis_atten(const VisP &q, cudaStream_t st) {
-  k_vis_atten<<<grid_for((long long)q.ni * q.nj * q.nk), 256, 0, st>>>(q);
+  const dim3 grid((q.ni + 127) / 128, q.nj, q.nk);
+  switch (q.nmax) {
+    case 1: k_vis_atten<1><<<grid, 128, 0, st>>>(q); break;
+    case 2: k_vis_atten<2><<<grid, 128, 0, st>>>(q); break;
+    case 3: k_vis_atten<3><<<grid, 128, 0, st>>>(q); break;
+    case 4: k_vis_atten<4><<<grid, 128, 0, st>>>(q); break;
+    case 5: k_vis_atten<5><<<grid, 128, 0, st>>>(q); break;
+    case 6: k_vis_atten<6><<<grid, 128, 0, st>>>(q); break;
+    case 7: k_vis_atten<7><<<grid, 128, 0, st>>>(q); break;
+    case 8: k_vis_atten<8><<<grid, 128, 0, st>>>(q); break;
+    case 9: k_vis_atten<9><<<grid, 128, 0, st>>>(q); break;
+    default: k_vis_atten<10><<<grid, 128, 0, st>>>(q); break;
+  }
   return 1;
 }
 
