@@ -61,6 +61,7 @@ struct Request {
 // requests on the same grid (same model arrays and run parameters) batch together
 bool same_grid(const cgfd_problem_desc &a, const cgfd_problem_desc &b) {
   if (a.ni != b.ni || a.nj != b.nj || a.nk != b.nk || a.medium_type != b.medium_type) return false;
+  if (a.medium_type == CGFD_MEDIUM_VISCO_ISO) return false;  // visco-elastic problems run one shot each
   if (a.coord != b.coord || a.metric != b.metric || a.medium != b.medium) return false;
   if (memcmp(a.pml, b.pml, sizeof(a.pml)) != 0) return false;
   if (a.free_top != b.free_top || a.dt != b.dt || a.t0 != b.t0 || a.nt_total != b.nt_total) return false;
