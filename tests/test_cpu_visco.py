@@ -33,3 +33,14 @@ def test_gmb_fit_matches_restatement_over_q():
     mu = np.full(qs.size, 6.5e9, np.float32)
     for nm in (1, 2, 3, 5):
         _compare(dict(VIS, nmaxwell=nm), lam, mu, 2 * qs, qs)
+
+
+def test_problem_bytes_counts_memory_variables():
+    """cgfd_problem_bytes of a visco-elastic problem adds at least the 4 levels of 6 nmax memory
+    variables and the anelastic weights to the elastic problem's bytes."""
+    pi = small_problem("iso", nsteps=2)
+    pv = small_problem("vis", nsteps=2)
+    ri, _ = cgfd_b200.problem_bytes(pi)
+    rv, _ = cgfd_b200.problem_bytes(pv)
+    cells = (pv.ni + 6) * (pv.nj + 6) * (pv.nk + 6)
+    assert rv - ri >= (4 * 6 + 2) * 3 * cells * 4
