@@ -394,8 +394,24 @@ int run(int argc, char **argv) {
     mnames = {"rho"};
     for (int a = 1; a <= 6; a++)
       for (int b = a; b <= 6; b++) mnames.push_back("c" + std::to_string(a) + std::to_string(b));
-  } else fail("medium type '" + type + "' is not on this path (acoustic_iso, elastic_iso/vti/aniso)");
+  } else if (type == "viscoelastic_iso") {
+    // generalized Maxwell body (par_t.cu:730-770; only visco_type gmb reaches the time loop)
+    d.medium_type = CGFD_MEDIUM_VISCO_ISO;
+    mnames = {"rho", "lambda", "mu", "Qp", "Qs"};
+    const Value &vc = need(par, "visco_config");
+    if (need(vc, "visco_type").as_str() != "gmb") fail("visco_type must be gmb (graves_Qs is not applied by the time loop)");
+    static cgfd_visco_desc vd;
+    vd.nmaxwell = need(vc, "number_of_maxwell").as_int();
+    vd.fmin = (float)need(vc, "min_freq").as_num();
+    vd.fmax = (float)need(vc, "max_freq").as_num();
+    vd.fr = (float)need(vc, "refer_freq").as_num();
+    d.visco = &vd;
+  } else fail("medium type '" + type + "' is not on this path (acoustic_iso, elastic_iso/vti/aniso, viscoelastic_iso)");
   std::string way = need(md, "input_way").as_str();
+  // visco-elastic Q volumes come from one-component media files (media_*2model_onecmp), not built
+  if (d.medium_type == CGFD_MEDIUM_VISCO_ISO && way != "import")
+    fail("viscoelastic_iso media are read with input_way 'import' (rho lambda mu Qp Qs); their one-component "
+         "Qp / Qs files are not on this path");
   std::vector<float> medium(mnames.size() * g.siz, 0.f);
   if (way == "import") {
     import_vars(need(md, "import").as_str() + "/media_" + kFnamePart + ".nc", g, mnames, medium.data());

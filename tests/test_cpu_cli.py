@@ -50,6 +50,20 @@ def test_cli_rejects_off_path_options(tmp_path):
     json.dump(cfg, open(par, "w"))
     r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "ablexp" in r.stderr
+    # visco-elastic media: GMB only, and Q volumes through the media import only
+    cfg = json.load(open(par))
+    cfg.pop("boundary_x_left", None)
+    cfg["medium"]["type"] = "viscoelastic_iso"
+    cfg["medium"]["input_way"] = "infile_layer"
+    cfg["visco_config"] = {"visco_type": "gmb", "number_of_maxwell": 3, "min_freq": 0.2, "max_freq": 20.0,
+                           "refer_freq": 2.0}
+    json.dump(cfg, open(par, "w"))
+    r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "one-component" in r.stderr, r.stderr
+    cfg["visco_config"]["visco_type"] = "graves_Qs"
+    json.dump(cfg, open(par, "w"))
+    r = subprocess.run([CLI, par, "0"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "gmb" in r.stderr, r.stderr
 
 
 def test_cli_dt_check_rejects_unstable_step(tmp_path):
