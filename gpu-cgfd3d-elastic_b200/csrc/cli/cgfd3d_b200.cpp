@@ -8,7 +8,8 @@
 // <station>.<Vx Vy Vz P>.sac for acoustic media), line receivers, slices and snapshots, and
 // with a free surface the peak ground motion file PG_V_A_D_px0_py0_pz0.nc. Media come from
 // media_*.nc files, or from layer files, grid files or binary models discretised on the GPU. Options outside this path (MPI
-// decomposition, ablexp, visco-elastic media) are rejected with a message.
+// decomposition, ablexp, visco-elastic Q volumes from one-component media files) are rejected
+// with a message; visco-elastic media (visco_type gmb) are read through the media import.
 #include <sys/stat.h>
 
 #include <algorithm>
