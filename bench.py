@@ -322,7 +322,9 @@ def media_bench(local, steps=2000, media=("vti", "aniso", "ac", "vis")):
     the bulk stage's algorithmic bytes (36 wavefield + NCOEF coefficient accesses per
     cell-stage; acoustic: 16 wavefield + 11 coefficient accesses over every plane) per event-timed
     duration against the measured HBM peak. Each mode's problem is autotuned (tile shape, z chunk)
-    before it runs."""
+    before it runs. Last, the same grid with a visco-elastic medium (3 GMB mechanisms, FP32):
+    Gcell-stage/s and the event-timed stage (both passes) against its 593 B per cell-stage.
+    `media` picks the legs."""
     import torch
     from cgfd_b200 import (synth, Simulation, CGFD_PREC_FP32, CGFD_PREC_U16_COEF, CGFD_PREC_FP16_WAVE,
                            CGFD_PREC_FP16_COEF, CGFD_PREC_BF16_COEF, CGFD_PREC_FP64)
